@@ -1,0 +1,166 @@
+/*
+ * qesb.h — C ABI of the B200-native QES-Winds lambda solver (libqesb200.so).
+ *
+ * The library replaces the solve step that the reference reaches through
+ *     Solver *SolverFactory::create(const int &type, const qes::Domain &, const float &tol)
+ *     solver->resetLambda();
+ *     solver->solve(WINDSGeneralData *WGD, const int &itermax);
+ * (reference src/winds/SolverFactory.cpp:35-60, src/winds/Solver.h:61-120,
+ * called from qesWinds/qesWindsMain.cpp:154-169). A C++ adaptor with exactly
+ * that interface lives in qes-public_b200/host/Solver_B200.h.
+ *
+ * Arrays use the reference's own layouts (src/qes/Domain.h:143-167), passed
+ * as plain pointers:
+ *   cell arrays  (e f g h m n, icellflag, lambda): (nx-1)(ny-1)(nz-1) values,
+ *                index i + j*(nx-1) + k*(nx-1)*(ny-1);
+ *   face arrays  (u0 v0 w0 u v w):                 nx*ny*nz values,
+ *                index i + j*nx + k*nx*ny;
+ *   dz_array:                                       nz-1 values (ghost at 0);
+ * with nx = Nx+1, ny = Ny+1, nz = Nz+2 (src/qes/Domain.cpp:11-13).
+ *
+ * Every entry point returns a qesb_status; none calls exit(). Handles are
+ * owned by the caller; one handle serves one host thread at a time.
+ */
+#ifndef QESB_H
+#define QESB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum qesb_status {
+  QESB_OK = 0,
+  QESB_ERR_ARG = 1,      /* bad size, null pointer, unknown option */
+  QESB_ERR_CUDA = 2,     /* a CUDA runtime call failed (message: qesb_last_error) */
+  QESB_ERR_NOMEM = 3,    /* device allocation failed */
+  QESB_ERR_STATE = 4,    /* call out of order (e.g. solve before set_inputs) */
+  QESB_ERR_NUMERIC = 5,  /* NaN or Inf met in lambda during the solve */
+  QESB_ERR_NODEV = 6     /* no CUDA device, or not an sm_100 device */
+} qesb_status;
+
+typedef struct qesb_handle qesb_handle;
+
+/* Grid: base cell counts and spacings, as qes::Domain(Nx, Ny, Nz, dx, dy, dz)
+ * takes them (src/qes/Domain.cpp:7-31), plus the vertical spacing array
+ * (Domain::dz_array, src/qes/Domain.h:191), nz-1 = Nz+1 entries. */
+typedef struct qesb_grid {
+  int Nx, Ny, Nz;
+  float dx, dy;
+  const float *dz_array;
+} qesb_grid;
+
+/* Per-solve report. */
+typedef struct qesb_stats {
+  int iterations;        /* SOR iterations performed (the reference's `iter`) */
+  int converged;         /* 1 if the stop came from max|dlambda| <= tol */
+  double residual;       /* FP64 max|lambda - lambda_old| of the last iteration */
+  double ms_total;       /* device time of the whole solve (CUDA events) */
+  double ms_sor;         /* device time of the SOR iterations alone */
+  int path;              /* 0 = full-coefficient sweep, 1 = packed wall-mask sweep */
+  int sweeps_per_launch; /* iterations fused per sweep launch */
+} qesb_stats;
+
+/* Library and device. */
+const char *qesb_version(void);
+const char *qesb_last_error(void);          /* thread-local message of the last failure */
+
+/* Solver(qes::Domain, const float &tol) — src/winds/Solver.cpp:77-91 and
+ * SolverFactory::create — src/winds/SolverFactory.cpp:35-60. Allocates the
+ * device buffers for this grid on `device` (the reference always uses
+ * device 0, Solver_GPU_GlobalMemory.cu:226). lambda starts at zero. */
+qesb_status qesb_create(const qesb_grid *grid, float tol, int device, qesb_handle **out);
+qesb_status qesb_destroy(qesb_handle *h);
+
+/* Solver::resetLambda — src/winds/Solver.h:115-120: lambda, lambda_old, R <- 0. */
+qesb_status qesb_reset_lambda(qesb_handle *h);
+
+/* The WINDSGeneralData fields the solve reads (src/winds/Solver_CPU.cpp:56-231):
+ * e f g h m n, icellflag, u0 v0 w0. Host pointers, copied to the device.
+ * The coefficient arrays are inspected: when every updated cell's
+ * coefficients are 0 or one per-layer value (stair-step walls, as
+ * Wall::solverCoefficients leaves them) the sweep runs on a 1-byte wall mask
+ * instead of six floats; otherwise on the full coefficients. */
+qesb_status qesb_set_inputs(qesb_handle *h, const float *e, const float *f, const float *g,
+                            const float *hc, const float *m, const float *n, const int *icellflag,
+                            const float *u0, const float *v0, const float *w0);
+/* Same, from device pointers (reference layouts) already on the handle's device. */
+qesb_status qesb_set_inputs_device(qesb_handle *h, const float *e, const float *f, const float *g,
+                                   const float *hc, const float *m, const float *n,
+                                   const int *icellflag, const float *u0, const float *v0,
+                                   const float *w0);
+
+/* Solver::solve(WGD, itermax) — src/winds/Solver_CPU.cpp:42-238:
+ * R from u0 v0 w0; SOR red-black sweeps while (iter < itermax && max|dlambda| > tol)
+ * with the ground mirror lambda(k=0) <- lambda(k=1) after each iteration;
+ * then u v w = u0 v0 w0 + correction, zeroed on the faces of solid cells.
+ * Host output pointers (nullable: skip that component). lambda persists on
+ * the handle between calls, as in the reference CPU solvers, until
+ * qesb_reset_lambda. */
+qesb_status qesb_solve(qesb_handle *h, int itermax, float *u, float *v, float *w, qesb_stats *st);
+/* Same, writing device pointers (reference face layout). */
+qesb_status qesb_solve_device(qesb_handle *h, int itermax, float *u, float *v, float *w,
+                              qesb_stats *st);
+
+/* lambda in the reference cell layout (host pointers). set = warm start. */
+qesb_status qesb_set_lambda(qesb_handle *h, const float *lambda);
+qesb_status qesb_get_lambda(qesb_handle *h, float *lambda);
+qesb_status qesb_get_divergence(qesb_handle *h, float *R);  /* R of the last solve */
+/* FP64 max|dlambda| of each iteration of the last solve, iterations 0..n-1. */
+qesb_status qesb_get_residual_history(qesb_handle *h, double *out, int n);
+
+/* Tolerance (Solver::tol) and tuning knobs. Keys:
+ *   "sweeps_per_launch"  iterations fused per sweep launch (0 = autotuned)
+ *   "path"               0 = force full coefficients, 1 = allow the packed mask (default)
+ *   "graph"              1 = run the iteration loop as a CUDA graph (default), 0 = plain launches */
+qesb_status qesb_set_tolerance(qesb_handle *h, float tol);
+qesb_status qesb_set_option(qesb_handle *h, const char *key, int value);
+/* cudaStream_t to run on (NULL = the handle's own stream). */
+qesb_status qesb_set_stream(qesb_handle *h, void *stream);
+
+/* ---------------------------------------------------------------------
+ * Seeded synthetic-city generator (host). Restates the reference's set-up of
+ * the solver inputs for flat terrain and stair-step cuboid buildings:
+ *   ground flags      src/winds/WINDSGeneralData.cpp:438-444
+ *   building cells    src/winds/PolyBuilding.cpp:130-237 (RectangularBuilding.h:70-108)
+ *   wall coefficients src/winds/Wall.cpp:44-350, 827-846
+ *   power-law inflow  src/winds/WindProfilerSensorType.cpp:220,328-333,571-621
+ *   solid faces       src/winds/Wall.cpp:805-825
+ * --------------------------------------------------------------------- */
+typedef struct qesb_building {
+  float x_start, y_start;   /* south-west corner, m */
+  float length, width;      /* extent along x and y, m */
+  float height, base_height;
+} qesb_building;
+
+typedef struct qesb_inflow {
+  float u_ref;    /* speed at z_ref, m/s */
+  float z_ref;    /* m */
+  float p;        /* power-law exponent (the reference carries it in siteZ0) */
+  float dir_deg;  /* meteorological direction; 270 blows toward +x */
+} qesb_inflow;
+
+/* dz_array for a uniform (ratio == 1) or geometrically stretched grid:
+ * dz[k] = dz0 * ratio^(k-1) for k >= 1, dz[0] = dz[1]. */
+qesb_status qesb_city_dz(int Nz, float dz0, float ratio, float *dz_array);
+
+/* Fill icellflag, e..n and u0 v0 w0 for the given buildings and inflow. */
+qesb_status qesb_city_build(const qesb_grid *grid, int n_buildings, const qesb_building *b,
+                            const qesb_inflow *inflow, int *icellflag, float *e, float *f,
+                            float *g, float *hc, float *m, float *n, float *u0, float *v0,
+                            float *w0);
+
+/* Seed-indexed random city: up to max_buildings non-overlapping cuboids with
+ * footprints U[fp_min, fp_max] m, heights U[h_min, h_max] m, and a random
+ * inflow (u_ref U[3,10] m/s at 10 m, p U[0.1,0.3], direction U[0,360)).
+ * Writes the buildings and inflow chosen; returns the count in *n_out. */
+qesb_status qesb_city_random(const qesb_grid *grid, uint64_t seed, int max_buildings,
+                             float fp_min, float fp_max, float h_min, float h_max,
+                             qesb_building *b_out, int *n_out, qesb_inflow *inflow_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QESB_H */

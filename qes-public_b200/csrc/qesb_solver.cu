@@ -1,0 +1,796 @@
+// B200-native QES-Winds lambda solve: device kernels and the C ABI of
+// include/qesb.h.
+//
+// Reference path replaced: Solver::solve (src/winds/Solver_CPU.cpp:42-238,
+// Solver_CPU_RB.cpp:41-291), created through SolverFactory::create
+// (src/winds/SolverFactory.cpp:35-60).
+//
+// This translation unit is compiled with -fmad=false: every float and double
+// operation below rounds on its own, as the reference's host code does when
+// built without FMA contraction. With that, the red-black sweep reproduces
+// Solver_CPU_RB bit for bit (same per-cell expression, same colour order),
+// R reproduces Solver_CPU.cpp:64-74 bit for bit, and the correction
+// reproduces Solver_CPU.cpp:157-231 bit for bit.
+//
+// Device layout (per handle). Cell fields that the sweep touches (lambda,
+// R, the wall mask, the full coefficients) live in a padded layout:
+//   index(i, j, k) = k*PLANE + (j + GY)*PX + (i + GX),  PLANE = PX*PY,
+//   PX = roundup(X + 2*GX, 32) (rows start on 128-byte boundaries),
+//   PY = Y + 2*GY, X = nx-1, Y = ny-1, k in [0, nz-2].
+// The guard cells are zero and never updated; they let tiled kernels read a
+// halo beyond the domain edge without bounds checks. Inputs and outputs in
+// the reference layouts (cells i + j*X + k*X*Y, faces i + j*nx + k*nx*ny)
+// stay as the caller gave them.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "qesb.h"
+#include "qesb_internal.h"
+#include "qesb_device.cuh"
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+qesb_status qesb_fail(qesb_status s, const char *fmt, ...)
+{
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return s;
+}
+
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return qesb_fail(e_ == cudaErrorMemoryAllocation ? QESB_ERR_NOMEM : QESB_ERR_CUDA,           \
+                       "%s failed at %s:%d: %s", #call, __FILE__, __LINE__, cudaGetErrorString(e_)); \
+  } while (0)
+
+#define CKS(expr)                                                                                  \
+  do {                                                                                             \
+    qesb_status s_ = (expr);                                                                       \
+    if (s_ != QESB_OK) return s_;                                                                  \
+  } while (0)
+
+using namespace qesb;
+
+// ---------------------------------------------------------------------------
+// kernels: set-up
+// ---------------------------------------------------------------------------
+
+// Per-layer coefficient values: for each of the six coefficients and each
+// updated layer k, the largest value over the updated cells. With stair-step
+// walls every value is either 0 or this one value.
+__global__ void k_layer_max(DevGrid G, const float *__restrict__ e, const float *__restrict__ f,
+                            const float *__restrict__ g, const float *__restrict__ h,
+                            const float *__restrict__ m, const float *__restrict__ n,
+                            unsigned *__restrict__ vmax, int *__restrict__ bad)
+{
+  const int k = blockIdx.y + 1;
+  const float *cf[6] = {e, f, g, h, m, n};
+  float mx[6] = {0, 0, 0, 0, 0, 0};
+  const long per = (long)(G.X - 2) * (G.Y - 2);
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < per; t += (long)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(t % (G.X - 2)), j = 1 + (int)(t / (G.X - 2));
+    const long c = G.cell(i, j, k);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      float v = cf[q][c];
+      if (!(v >= 0.0f) || isinf(v)) atomicExch(bad, 1);  // negative, NaN or Inf: no packing
+      mx[q] = fmaxf(mx[q], v);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    float v = warp_max_f(mx[q]);
+    if ((threadIdx.x & 31) == 0) atomicMax(&vmax[q * G.Z + k], __float_as_uint(v));
+  }
+}
+
+// Builds the 6-bit wall mask (bit q set when coefficient q is non-zero) and
+// flags any value that is neither 0 nor its layer's value.
+__global__ void k_build_mask(DevGrid G, const float *__restrict__ e, const float *__restrict__ f,
+                             const float *__restrict__ g, const float *__restrict__ h,
+                             const float *__restrict__ m, const float *__restrict__ n,
+                             const unsigned *__restrict__ vmax, uint8_t *__restrict__ mask,
+                             int *__restrict__ bad)
+{
+  const int k = blockIdx.y + 1;
+  const float *cf[6] = {e, f, g, h, m, n};
+  const long per = (long)(G.X - 2) * (G.Y - 2);
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < per; t += (long)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(t % (G.X - 2)), j = 1 + (int)(t / (G.X - 2));
+    const long c = G.cell(i, j, k);
+    unsigned bits = 0;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const float v = cf[q][c];
+      const float ref = __uint_as_float(vmax[q * G.Z + k]);
+      if (v == ref && v != 0.0f) bits |= 1u << q;
+      else if (v != 0.0f) atomicExch(bad, 1);
+    }
+    mask[G.pad(i, j, k)] = (uint8_t)bits;
+  }
+}
+
+// inv[k*64 + bits] = omega / (e + f + g + h + m + n) with absent terms 0,
+// summed in the reference's order (Solver_CPU.cpp:107).
+__global__ void k_inv_table(DevGrid G, const unsigned *__restrict__ vmax, float *__restrict__ inv,
+                            float *__restrict__ val)
+{
+  const int k = blockIdx.x, bits = threadIdx.x;
+  float v[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) v[q] = __uint_as_float(vmax[q * G.Z + k]);
+  float s = (bits & 1 ? v[0] : 0.0f);
+  s = s + (bits & 2 ? v[1] : 0.0f);
+  s = s + (bits & 4 ? v[2] : 0.0f);
+  s = s + (bits & 8 ? v[3] : 0.0f);
+  s = s + (bits & 16 ? v[4] : 0.0f);
+  s = s + (bits & 32 ? v[5] : 0.0f);
+  inv[k * 64 + bits] = kOmega / s;
+  if (bits < 6) val[bits * G.Z + k] = v[bits];
+}
+
+// Natural -> padded copy of the six coefficients (full-coefficient path).
+__global__ void k_pad_coefs(DevGrid G, const float *__restrict__ e, const float *__restrict__ f,
+                            const float *__restrict__ g, const float *__restrict__ h,
+                            const float *__restrict__ m, const float *__restrict__ n,
+                            float *__restrict__ pe, float *__restrict__ pf, float *__restrict__ pg,
+                            float *__restrict__ ph, float *__restrict__ pm, float *__restrict__ pn)
+{
+  const int j = blockIdx.y, k = blockIdx.z;
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < G.X; i += gridDim.x * blockDim.x) {
+    const long c = G.cell(i, j, k), p = G.pad(i, j, k);
+    pe[p] = e[c];
+    pf[p] = f[c];
+    pg[p] = g[c];
+    ph[p] = h[c];
+    pm[p] = m[c];
+    pn[p] = n[c];
+  }
+}
+
+// Divergence of the initial field, Solver_CPU.cpp:56-77, into padded R.
+// The reference expression mixes precisions: (-2.0f * pow(alpha1, 2.0)) and
+// the m-term's 0.5 literal are double; the x, y and n terms are float.
+__global__ void k_divergence(DevGrid G, const float *__restrict__ e, const float *__restrict__ f,
+                             const float *__restrict__ g, const float *__restrict__ h,
+                             const float *__restrict__ m, const float *__restrict__ n,
+                             const float *__restrict__ u0, const float *__restrict__ v0,
+                             const float *__restrict__ w0, const float *__restrict__ dz,
+                             float dx, float dy, float *__restrict__ R)
+{
+  const int j = blockIdx.y, k = blockIdx.z + 1;  // k in [1, nz-3]
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < G.X; i += gridDim.x * blockDim.x) {
+    const long c = G.cell(i, j, k), fc = G.face(i, j, k);
+    const float xt = (e[c] * u0[fc + 1] - f[c] * u0[fc]) * dx;
+    const float yt = (g[c] * v0[fc + G.FX] - h[c] * v0[fc]) * dy;
+    const double mt = (double)(m[c] * dz[k]) * 0.5 * (double)(dz[k] + dz[k + 1]) * (double)w0[fc + G.FXY];
+    const float nt = n[c] * dz[k] * 0.5f * (dz[k] + dz[k - 1]) * w0[fc];
+    R[G.pad(i, j, k)] = (float)(-2.0 * ((double)(xt + yt) + (mt - (double)nt)));
+  }
+}
+
+// Natural <-> padded lambda.
+__global__ void k_lambda_to_pad(DevGrid G, const float *__restrict__ src, float *__restrict__ dst)
+{
+  const int j = blockIdx.y, k = blockIdx.z;
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < G.X; i += gridDim.x * blockDim.x)
+    dst[G.pad(i, j, k)] = src[G.cell(i, j, k)];
+}
+__global__ void k_lambda_from_pad(DevGrid G, const float *__restrict__ src, float *__restrict__ dst)
+{
+  const int j = blockIdx.y, k = blockIdx.z;
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < G.X; i += gridDim.x * blockDim.x)
+    dst[G.cell(i, j, k)] = src[G.pad(i, j, k)];
+}
+
+// ---------------------------------------------------------------------------
+// kernels: iteration (full-coefficient path, one colour per launch)
+// ---------------------------------------------------------------------------
+
+// One colour of the red-black sweep (Solver_CPU_RB.cpp:110-151): cells with
+// (i + j + k) % 2 == colour in i in [1, nx-3], j in [1, ny-3], k in [1, nz-3].
+// The per-iteration error max|lambda_new - lambda_old| is formed in double
+// at update time (each cell changes once per iteration) and folded into
+// err[it] with one 64-bit atomicMax per block.
+__global__ void __launch_bounds__(128) k_sor_full(DevGrid G, int colour, float *__restrict__ L,
+                                                  const float *__restrict__ pe, const float *__restrict__ pf,
+                                                  const float *__restrict__ pg, const float *__restrict__ ph,
+                                                  const float *__restrict__ pm, const float *__restrict__ pn,
+                                                  const float *__restrict__ R, double *__restrict__ err,
+                                                  const SolveState *__restrict__ st)
+{
+  if (st->done) return;
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  const int o = (colour + 1 + j + k) & 1;
+  const int i = 1 + 2 * (int)(blockIdx.x * blockDim.x + threadIdx.x) + o;
+  double d = 0.0;
+  if (i <= G.X - 2) {
+    const long p = G.pad(i, j, k);
+    const float e = pe[p], f = pf[p], g = pg[p], h = ph[p], m = pm[p], n = pn[p];
+    const float old = L[p];
+    const float nv = (kOmega / (e + f + g + h + m + n)) *
+                         (e * L[p + 1] + f * L[p - 1] + g * L[p + G.PX] + h * L[p - G.PX] +
+                          m * L[p + G.PLANE] + n * L[p - G.PLANE] - R[p]) +
+                     (1.0f - kOmega) * old;
+    L[p] = nv;
+    d = fabs((double)nv - (double)old);
+  }
+  block_max_to(err + st->it, d);
+}
+
+// Ground mirror lambda(k=0) <- lambda(k=1) over the whole plane (Solver_CPU.cpp:119-126).
+__global__ void k_mirror(DevGrid G, float *__restrict__ L, const SolveState *__restrict__ st)
+{
+  if (st->done) return;
+  const int j = blockIdx.y;
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < G.X; i += gridDim.x * blockDim.x) {
+    const long p = G.pad(i, j, 0);
+    L[p] = L[p + G.PLANE];
+  }
+}
+
+// Convergence poll after iteration st->it: the reference loop condition
+// `iter < itermax && max_error > tol` (Solver_CPU.cpp:93), with max_error in
+// double. A NaN error stops the solve and is reported.
+__global__ void k_poll(SolveState *st, const double *__restrict__ err, double tol, int itermax)
+{
+  if (st->done) return;
+  const int it = st->it;
+  const double e = err[it];
+  st->residual = e;
+  st->it = it + 1;
+  if (isnan(e)) {
+    st->done = 1;
+    st->nan = 1;
+  } else if (!(e > tol)) {
+    st->done = 1;
+    st->converged = 1;
+  } else if (it + 1 >= itermax) {
+    st->done = 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// kernels: velocity correction (Solver_CPU.cpp:157-231)
+// ---------------------------------------------------------------------------
+// One thread per face (i, j, k). Each face's final value is: 0 if it is a
+// face of a solid cell (icellflag 0 or 2) with k in [1, nz-2] — the zeroing
+// pass runs last in the reference, so it wins — else u0 plus the correction
+// when (i, j, k) is in i in [1, nx-2], j in [1, ny-2], k in [1, nz-3], else u0.
+// Gathering per face avoids the overlapping scattered writes of the
+// reference's zeroing loop and gives the same result.
+__global__ void k_correct(DevGrid G, const float *__restrict__ L, const float *__restrict__ f,
+                          const float *__restrict__ h, const float *__restrict__ n,
+                          const int *__restrict__ flag, const float *__restrict__ u0,
+                          const float *__restrict__ v0, const float *__restrict__ w0,
+                          const float *__restrict__ dz, float dx, float dy, float *__restrict__ u,
+                          float *__restrict__ v, float *__restrict__ w)
+{
+  const int j = blockIdx.y, k = blockIdx.z;
+  const float half = 1.0f / (2.0f * 1.0f);
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < G.FX; i += gridDim.x * blockDim.x) {
+    const long q = G.face(i, j, k);
+    float uu = u0[q], vv = v0[q], ww = w0[q];
+    const bool corr = i >= 1 && i <= G.FX - 2 && j >= 1 && j <= G.FY - 2 && k >= 1 && k <= G.FZ - 3;
+    if (corr) {
+      const long c = G.cell(i, j, k), p = G.pad(i, j, k);
+      const float lc = L[p];
+      uu = u0[q] + half * f[c] * dx * (lc - L[p - 1]);
+      vv = v0[q] + half * h[c] * dy * (lc - L[p - G.PX]);
+      ww = w0[q] + half * n[c] * dz[k] * (lc - L[p - G.PLANE]);
+    }
+    const bool kin = k >= 1 && k <= G.FZ - 2;          // zeroing covers cells k in [1, nz-2]
+    const bool ic = i <= G.X - 1, jc = j <= G.Y - 1;   // a cell (i, j, k) exists
+    if (kin && jc && ((ic && is_solid(flag[G.cell(i, j, k)])) || (i >= 1 && is_solid(flag[G.cell(i - 1, j, k)]))))
+      uu = 0.0f;
+    if (kin && ic && ((jc && is_solid(flag[G.cell(i, j, k)])) || (j >= 1 && is_solid(flag[G.cell(i, j - 1, k)]))))
+      vv = 0.0f;
+    if (ic && jc && ((kin && is_solid(flag[G.cell(i, j, k)])) ||
+                     (k - 1 >= 1 && k - 1 <= G.FZ - 2 && is_solid(flag[G.cell(i, j, k - 1)]))))
+      ww = 0.0f;
+    if (u) u[q] = uu;
+    if (v) v[q] = vv;
+    if (w) w[q] = ww;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------
+struct qesb_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  DevGrid G{};
+  float dx = 1, dy = 1;
+  std::vector<float> dz;
+  float tol = 1e-9f;
+
+  // device buffers
+  float *d_lam = nullptr, *d_lam2 = nullptr;  // padded lambda (ping-pong for fused sweeps)
+  float *d_R = nullptr;                       // padded R
+  uint8_t *d_mask = nullptr;                  // padded wall mask
+  float *d_pc[6] = {};                        // padded coefficients (full path)
+  float *d_in[6] = {};                        // natural coefficients (owned copy, or caller's)
+  int *d_flag = nullptr;
+  float *d_u0 = nullptr, *d_v0 = nullptr, *d_w0 = nullptr;
+  bool own_inputs = true;
+  float *d_own_in[6] = {};
+  int *d_own_flag = nullptr;
+  float *d_own_u0 = nullptr, *d_own_v0 = nullptr, *d_own_w0 = nullptr;
+  float *d_dz = nullptr;
+  unsigned *d_vmax = nullptr;  // [6][Z] per-layer coefficient values (float bits)
+  float *d_inv = nullptr;      // [Z][64] omega / sum
+  float *d_val = nullptr;      // [6][Z] coefficient values
+  int *d_bad = nullptr;
+  double *d_err = nullptr;
+  int err_cap = 0;
+  SolveState *d_state = nullptr;
+  SolveState *h_state = nullptr;  // pinned
+  float *d_u = nullptr, *d_v = nullptr, *d_w = nullptr;  // output staging for host solves
+  cudaEvent_t ev[4] = {};
+
+  bool have_inputs = false;
+  bool packed = false;
+  int opt_path = 1;
+  int opt_k = 0;
+  int opt_graph = 1;
+};
+
+namespace {
+
+size_t pad_cells(const DevGrid &G) { return (size_t)G.PLANE * G.Z; }
+
+qesb_status fill_grid(const qesb_grid *g, DevGrid &G)
+{
+  if (!g || g->Nx < 3 || g->Ny < 3 || g->Nz < 2 || !(g->dx > 0) || !(g->dy > 0) || !g->dz_array)
+    return qesb_fail(QESB_ERR_ARG, "qesb_create: grid needs Nx, Ny >= 3, Nz >= 2, dx, dy > 0 and dz_array");
+  if ((long)g->Nx * g->Ny * (g->Nz + 1) > (1L << 31) - 1)
+    return qesb_fail(QESB_ERR_ARG, "qesb_create: grid too large for 32-bit cell indices");
+  G.X = g->Nx;
+  G.Y = g->Ny;
+  G.Z = g->Nz + 1;
+  G.FX = g->Nx + 1;
+  G.FY = g->Ny + 1;
+  G.FZ = g->Nz + 2;
+  G.FXY = (long)G.FX * G.FY;
+  G.XY = (long)G.X * G.Y;
+  G.PX = ((G.X + 2 * kGX) + 31) / 32 * 32;
+  G.PY = G.Y + 2 * kGY;
+  G.PLANE = (long)G.PX * G.PY;
+  for (int k = 0; k < G.Z; ++k)
+    if (!(g->dz_array[k] > 0)) return qesb_fail(QESB_ERR_ARG, "qesb_create: dz_array[%d] must be > 0", k);
+  return QESB_OK;
+}
+
+template <class T>
+qesb_status dalloc(T **p, size_t count)
+{
+  CK(cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(count, 1)));
+  return QESB_OK;
+}
+
+dim3 row_grid(const DevGrid &G, int rows, int planes, int width)
+{
+  return dim3((width + 255) / 256, rows, planes);
+}
+
+qesb_status ensure_err(qesb_handle *h, int itermax)
+{
+  if (h->err_cap >= itermax) return QESB_OK;
+  if (h->d_err) cudaFree(h->d_err);
+  h->d_err = nullptr;
+  int cap = std::max(itermax, 1024);
+  CKS(dalloc(&h->d_err, (size_t)cap));
+  h->err_cap = cap;
+  return QESB_OK;
+}
+
+// Inspect coefficients; build mask + tables when stair-step, else padded copies.
+qesb_status prepare_coefs(qesb_handle *h)
+{
+  const DevGrid &G = h->G;
+  cudaStream_t s = h->stream;
+  h->packed = false;
+  if (h->opt_path != 0) {
+    CK(cudaMemsetAsync(h->d_vmax, 0, sizeof(unsigned) * 6 * G.Z, s));
+    CK(cudaMemsetAsync(h->d_bad, 0, sizeof(int), s));
+    dim3 grid(std::max(1, std::min(64, (int)(((long)(G.X - 2) * (G.Y - 2) + 255) / 256))), G.Z - 2);
+    k_layer_max<<<grid, 256, 0, s>>>(G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4],
+                                     h->d_in[5], h->d_vmax, h->d_bad);
+    CK(cudaGetLastError());
+    k_build_mask<<<grid, 256, 0, s>>>(G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4],
+                                      h->d_in[5], h->d_vmax, h->d_mask, h->d_bad);
+    CK(cudaGetLastError());
+    int bad = 1;
+    CK(cudaMemcpyAsync(&bad, h->d_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (!bad) {
+      k_inv_table<<<G.Z, 64, 0, s>>>(G, h->d_vmax, h->d_inv, h->d_val);
+      CK(cudaGetLastError());
+      h->packed = true;
+    }
+  }
+  // The full-coefficient path is always prepared: it is the sweep for
+  // non-stair-step inputs and the fallback the packed path is tested against.
+  k_pad_coefs<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(
+      G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_pc[0],
+      h->d_pc[1], h->d_pc[2], h->d_pc[3], h->d_pc[4], h->d_pc[5]);
+  CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status run_iterations_full(qesb_handle *h, int itermax)
+{
+  const DevGrid &G = h->G;
+  cudaStream_t s = h->stream;
+  const int nthr = 128;
+  dim3 grid(((G.X - 2) / 2 + 1 + nthr - 1) / nthr, G.Y - 2, G.Z - 2);
+  dim3 mgrid((G.X + 255) / 256, G.Y, 1);
+  const int chunk = 64;
+  for (int base = 0; base < itermax; base += chunk) {
+    const int n = std::min(chunk, itermax - base);
+    for (int t = 0; t < n; ++t) {
+      for (int colour = 0; colour < 2; ++colour)
+        k_sor_full<<<grid, nthr, 0, s>>>(G, colour, h->d_lam, h->d_pc[0], h->d_pc[1], h->d_pc[2],
+                                         h->d_pc[3], h->d_pc[4], h->d_pc[5], h->d_R, h->d_err,
+                                         h->d_state);
+      k_mirror<<<mgrid, 256, 0, s>>>(G, h->d_lam, h->d_state);
+      k_poll<<<1, 1, 0, s>>>(h->d_state, h->d_err, (double)h->tol, itermax);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h->h_state->done) break;
+  }
+  return QESB_OK;
+}
+
+qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w, qesb_stats *st)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  if (!h->have_inputs) return qesb_fail(QESB_ERR_STATE, "qesb_solve before qesb_set_inputs");
+  if (itermax < 0) return qesb_fail(QESB_ERR_ARG, "itermax must be >= 0");
+  CK(cudaSetDevice(h->device));
+  const DevGrid &G = h->G;
+  cudaStream_t s = h->stream;
+  CKS(ensure_err(h, std::max(itermax, 1)));
+  CK(cudaEventRecord(h->ev[0], s));
+  k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(
+      G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_u0, h->d_v0,
+      h->d_w0, h->d_dz, h->dx, h->dy, h->d_R);
+  CK(cudaGetLastError());
+  CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
+  CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+  CK(cudaEventRecord(h->ev[1], s));
+  if (itermax > 0) CKS(run_iterations_full(h, itermax));
+  CK(cudaEventRecord(h->ev[2], s));
+  k_correct<<<row_grid(G, G.FY, G.FZ, G.FX), 256, 0, s>>>(
+      G, h->d_lam, h->d_in[1], h->d_in[3], h->d_in[5], h->d_flag, h->d_u0, h->d_v0, h->d_w0,
+      h->d_dz, h->dx, h->dy, u, v, w);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev[3], s));
+  CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (st) {
+    float a = 0, b = 0;
+    CK(cudaEventElapsedTime(&a, h->ev[0], h->ev[3]));
+    CK(cudaEventElapsedTime(&b, h->ev[1], h->ev[2]));
+    st->iterations = itermax > 0 ? h->h_state->it : 0;
+    st->converged = h->h_state->converged;
+    st->residual = itermax > 0 ? h->h_state->residual : 1.0;
+    st->ms_total = a;
+    st->ms_sor = b;
+    st->path = 0;
+    st->sweeps_per_launch = 1;
+  }
+  if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the solve (iteration %d)", h->h_state->it);
+  return QESB_OK;
+}
+
+void free_all(qesb_handle *h)
+{
+  void *ptrs[] = {h->d_lam, h->d_lam2, h->d_R, h->d_mask, h->d_pc[0], h->d_pc[1], h->d_pc[2],
+                  h->d_pc[3], h->d_pc[4], h->d_pc[5], h->d_own_in[0], h->d_own_in[1],
+                  h->d_own_in[2], h->d_own_in[3], h->d_own_in[4], h->d_own_in[5], h->d_own_flag,
+                  h->d_own_u0, h->d_own_v0, h->d_own_w0, h->d_dz, h->d_vmax, h->d_inv, h->d_val,
+                  h->d_bad, h->d_err, h->d_state, h->d_u, h->d_v, h->d_w};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (h->h_state) cudaFreeHost(h->h_state);
+  for (auto &e : h->ev)
+    if (e) cudaEventDestroy(e);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char *qesb_version(void) { return "qesb200 0.1 (sm_100a)"; }
+const char *qesb_last_error(void) { return g_last_error.c_str(); }
+
+qesb_status qesb_create(const qesb_grid *grid, float tol, int device, qesb_handle **out)
+{
+  if (!out) return qesb_fail(QESB_ERR_ARG, "qesb_create: null out");
+  *out = nullptr;
+  DevGrid G{};
+  CKS(fill_grid(grid, G));
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return qesb_fail(QESB_ERR_NODEV, "qesb_create: no CUDA device");
+  if (device < 0 || device >= ndev) return qesb_fail(QESB_ERR_ARG, "qesb_create: device %d out of range", device);
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) return qesb_fail(QESB_ERR_NODEV, "qesb_create: device %d is sm_%d%d, this build is sm_100a", device, prop.major, prop.minor);
+  CK(cudaSetDevice(device));
+  qesb_handle *h = new qesb_handle();
+  h->device = device;
+  h->G = G;
+  h->dx = grid->dx;
+  h->dy = grid->dy;
+  h->dz.assign(grid->dz_array, grid->dz_array + G.Z);
+  h->tol = tol;
+  auto fail = [&](qesb_status s) {
+    free_all(h);
+    delete h;
+    return s;
+  };
+  qesb_status s = QESB_OK;
+#define TRY(x)                          \
+  if ((s = (x)) != QESB_OK) return fail(s);
+  const size_t np = pad_cells(G), nc = (size_t)G.XY * G.Z, nf = (size_t)G.FXY * G.FZ;
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(qesb_fail(QESB_ERR_CUDA, "cudaStreamCreate failed"));
+  h->stream = h->own_stream;
+  TRY(dalloc(&h->d_lam, np));
+  TRY(dalloc(&h->d_lam2, np));
+  TRY(dalloc(&h->d_R, np));
+  TRY(dalloc(&h->d_mask, np));
+  for (int q = 0; q < 6; ++q) TRY(dalloc(&h->d_pc[q], np));
+  TRY(dalloc(&h->d_dz, G.Z));
+  TRY(dalloc(&h->d_vmax, 6 * G.Z));
+  TRY(dalloc(&h->d_inv, 64 * G.Z));
+  TRY(dalloc(&h->d_val, 6 * G.Z));
+  TRY(dalloc(&h->d_bad, 1));
+  TRY(dalloc(&h->d_state, 1));
+  TRY(ensure_err(h, 1024));
+  if (cudaMallocHost((void **)&h->h_state, sizeof(SolveState)) != cudaSuccess)
+    return fail(qesb_fail(QESB_ERR_NOMEM, "cudaMallocHost failed"));
+  for (auto &e : h->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaEventCreate failed"));
+  for (void *p : {(void *)h->d_lam, (void *)h->d_lam2, (void *)h->d_R})
+    if (cudaMemset(p, 0, np * sizeof(float)) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaMemset failed"));
+  if (cudaMemset(h->d_mask, 0, np) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaMemset failed"));
+  for (int q = 0; q < 6; ++q)
+    if (cudaMemset(h->d_pc[q], 0, np * sizeof(float)) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaMemset failed"));
+  if (cudaMemcpy(h->d_dz, h->dz.data(), sizeof(float) * G.Z, cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(qesb_fail(QESB_ERR_CUDA, "cudaMemcpy dz failed"));
+  (void)nc;
+  (void)nf;
+#undef TRY
+  *out = h;
+  return QESB_OK;
+}
+
+qesb_status qesb_destroy(qesb_handle *h)
+{
+  if (!h) return QESB_OK;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  free_all(h);
+  delete h;
+  return QESB_OK;
+}
+
+qesb_status qesb_reset_lambda(qesb_handle *h)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  CK(cudaSetDevice(h->device));
+  const size_t np = pad_cells(h->G);
+  CK(cudaMemsetAsync(h->d_lam, 0, np * sizeof(float), h->stream));
+  CK(cudaMemsetAsync(h->d_lam2, 0, np * sizeof(float), h->stream));
+  CK(cudaMemsetAsync(h->d_R, 0, np * sizeof(float), h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return QESB_OK;
+}
+
+static qesb_status ensure_own_inputs(qesb_handle *h)
+{
+  const size_t nc = (size_t)h->G.XY * h->G.Z, nf = (size_t)h->G.FXY * h->G.FZ;
+  for (int q = 0; q < 6; ++q)
+    if (!h->d_own_in[q]) CKS(dalloc(&h->d_own_in[q], nc));
+  if (!h->d_own_flag) CKS(dalloc(&h->d_own_flag, nc));
+  if (!h->d_own_u0) CKS(dalloc(&h->d_own_u0, nf));
+  if (!h->d_own_v0) CKS(dalloc(&h->d_own_v0, nf));
+  if (!h->d_own_w0) CKS(dalloc(&h->d_own_w0, nf));
+  return QESB_OK;
+}
+
+qesb_status qesb_set_inputs(qesb_handle *h, const float *e, const float *f, const float *g,
+                            const float *hc, const float *m, const float *n, const int *icellflag,
+                            const float *u0, const float *v0, const float *w0)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  if (!e || !f || !g || !hc || !m || !n || !icellflag || !u0 || !v0 || !w0)
+    return qesb_fail(QESB_ERR_ARG, "qesb_set_inputs: null input");
+  CK(cudaSetDevice(h->device));
+  CKS(ensure_own_inputs(h));
+  const size_t nc = (size_t)h->G.XY * h->G.Z, nf = (size_t)h->G.FXY * h->G.FZ;
+  const float *src[6] = {e, f, g, hc, m, n};
+  cudaStream_t s = h->stream;
+  for (int q = 0; q < 6; ++q) CK(cudaMemcpyAsync(h->d_own_in[q], src[q], nc * sizeof(float), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_own_flag, icellflag, nc * sizeof(int), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_own_u0, u0, nf * sizeof(float), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_own_v0, v0, nf * sizeof(float), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_own_w0, w0, nf * sizeof(float), cudaMemcpyHostToDevice, s));
+  for (int q = 0; q < 6; ++q) h->d_in[q] = h->d_own_in[q];
+  h->d_flag = h->d_own_flag;
+  h->d_u0 = h->d_own_u0;
+  h->d_v0 = h->d_own_v0;
+  h->d_w0 = h->d_own_w0;
+  CKS(prepare_coefs(h));
+  CK(cudaStreamSynchronize(s));
+  h->have_inputs = true;
+  return QESB_OK;
+}
+
+qesb_status qesb_set_inputs_device(qesb_handle *h, const float *e, const float *f, const float *g,
+                                   const float *hc, const float *m, const float *n,
+                                   const int *icellflag, const float *u0, const float *v0,
+                                   const float *w0)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  if (!e || !f || !g || !hc || !m || !n || !icellflag || !u0 || !v0 || !w0)
+    return qesb_fail(QESB_ERR_ARG, "qesb_set_inputs_device: null input");
+  CK(cudaSetDevice(h->device));
+  const float *src[6] = {e, f, g, hc, m, n};
+  for (int q = 0; q < 6; ++q) h->d_in[q] = const_cast<float *>(src[q]);
+  h->d_flag = const_cast<int *>(icellflag);
+  h->d_u0 = const_cast<float *>(u0);
+  h->d_v0 = const_cast<float *>(v0);
+  h->d_w0 = const_cast<float *>(w0);
+  CKS(prepare_coefs(h));
+  CK(cudaStreamSynchronize(h->stream));
+  h->have_inputs = true;
+  return QESB_OK;
+}
+
+qesb_status qesb_solve_device(qesb_handle *h, int itermax, float *u, float *v, float *w, qesb_stats *st)
+{
+  return solve_impl(h, itermax, u, v, w, st);
+}
+
+qesb_status qesb_solve(qesb_handle *h, int itermax, float *u, float *v, float *w, qesb_stats *st)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  CK(cudaSetDevice(h->device));
+  const size_t nf = (size_t)h->G.FXY * h->G.FZ;
+  if (!h->d_u) {
+    CKS(dalloc(&h->d_u, nf));
+    CKS(dalloc(&h->d_v, nf));
+    CKS(dalloc(&h->d_w, nf));
+  }
+  CKS(solve_impl(h, itermax, u ? h->d_u : nullptr, v ? h->d_v : nullptr, w ? h->d_w : nullptr, st));
+  if (u) CK(cudaMemcpyAsync(u, h->d_u, nf * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  if (v) CK(cudaMemcpyAsync(v, h->d_v, nf * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  if (w) CK(cudaMemcpyAsync(w, h->d_w, nf * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return QESB_OK;
+}
+
+qesb_status qesb_set_lambda(qesb_handle *h, const float *lambda)
+{
+  if (!h || !lambda) return qesb_fail(QESB_ERR_ARG, "qesb_set_lambda: null argument");
+  CK(cudaSetDevice(h->device));
+  const DevGrid &G = h->G;
+  const size_t nc = (size_t)G.XY * G.Z;
+  float *tmp = nullptr;
+  CKS(dalloc(&tmp, nc));
+  cudaError_t e1 = cudaMemcpyAsync(tmp, lambda, nc * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+  if (e1 == cudaSuccess) {
+    k_lambda_to_pad<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, h->stream>>>(G, tmp, h->d_lam);
+    e1 = cudaGetLastError();
+  }
+  if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(h->stream);
+  cudaFree(tmp);
+  if (e1 != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "qesb_set_lambda: %s", cudaGetErrorString(e1));
+  return QESB_OK;
+}
+
+qesb_status qesb_get_lambda(qesb_handle *h, float *lambda)
+{
+  if (!h || !lambda) return qesb_fail(QESB_ERR_ARG, "qesb_get_lambda: null argument");
+  CK(cudaSetDevice(h->device));
+  const DevGrid &G = h->G;
+  const size_t nc = (size_t)G.XY * G.Z;
+  float *tmp = nullptr;
+  CKS(dalloc(&tmp, nc));
+  k_lambda_from_pad<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, h->stream>>>(G, h->d_lam, tmp);
+  cudaError_t e1 = cudaGetLastError();
+  if (e1 == cudaSuccess) e1 = cudaMemcpyAsync(lambda, tmp, nc * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+  if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(h->stream);
+  cudaFree(tmp);
+  if (e1 != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "qesb_get_lambda: %s", cudaGetErrorString(e1));
+  return QESB_OK;
+}
+
+qesb_status qesb_get_divergence(qesb_handle *h, float *R)
+{
+  if (!h || !R) return qesb_fail(QESB_ERR_ARG, "qesb_get_divergence: null argument");
+  CK(cudaSetDevice(h->device));
+  const DevGrid &G = h->G;
+  const size_t nc = (size_t)G.XY * G.Z;
+  float *tmp = nullptr;
+  CKS(dalloc(&tmp, nc));
+  k_lambda_from_pad<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, h->stream>>>(G, h->d_R, tmp);
+  cudaError_t e1 = cudaGetLastError();
+  if (e1 == cudaSuccess) e1 = cudaMemcpyAsync(R, tmp, nc * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+  if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(h->stream);
+  cudaFree(tmp);
+  if (e1 != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "qesb_get_divergence: %s", cudaGetErrorString(e1));
+  return QESB_OK;
+}
+
+qesb_status qesb_get_residual_history(qesb_handle *h, double *out, int n)
+{
+  if (!h || !out || n < 0) return qesb_fail(QESB_ERR_ARG, "qesb_get_residual_history: bad argument");
+  if (n > h->err_cap) return qesb_fail(QESB_ERR_ARG, "qesb_get_residual_history: n exceeds the last solve");
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(out, h->d_err, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return QESB_OK;
+}
+
+qesb_status qesb_set_tolerance(qesb_handle *h, float tol)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  h->tol = tol;
+  return QESB_OK;
+}
+
+qesb_status qesb_set_option(qesb_handle *h, const char *key, int value)
+{
+  if (!h || !key) return qesb_fail(QESB_ERR_ARG, "qesb_set_option: null argument");
+  std::string k(key);
+  if (k == "sweeps_per_launch") {
+    if (value < 0 || value > 4) return qesb_fail(QESB_ERR_ARG, "sweeps_per_launch must be in [0, 4]");
+    h->opt_k = value;
+  } else if (k == "path") {
+    if (value != 0 && value != 1) return qesb_fail(QESB_ERR_ARG, "path must be 0 or 1");
+    h->opt_path = value;
+  } else if (k == "graph") {
+    h->opt_graph = value ? 1 : 0;
+  } else {
+    return qesb_fail(QESB_ERR_ARG, "unknown option '%s'", key);
+  }
+  return QESB_OK;
+}
+
+qesb_status qesb_set_stream(qesb_handle *h, void *stream)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return QESB_OK;
+}
+
+}  // extern "C"

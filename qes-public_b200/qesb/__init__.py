@@ -1,0 +1,401 @@
+"""Python host mirror of the reference's solver interface, over libqesb200.so.
+
+The reference drives the lambda solve through C++ objects:
+
+    qes::Domain domain(Nx, Ny, Nz, dx, dy, dz);            src/qes/Domain.cpp:7-31
+    WINDSGeneralData *WGD = ...;  // e..n, icellflag, u0..w  src/winds/WINDSGeneralData.h:231-274
+    Solver *solver = SolverFactory::create(type, domain, tol); src/winds/SolverFactory.cpp:35-60
+    solver->resetLambda();                                  src/winds/Solver.h:115-120
+    solver->solve(WGD, itermax);                            src/winds/Solver_CPU.cpp:42-238
+
+This module offers the same names with the same argument meaning, backed by
+the C ABI of include/qesb.h (ctypes; numpy arrays in the reference layouts).
+The C++ adaptor with the identical interface is qes-public_b200/host/Solver_B200.h.
+
+There is no CPU fallback: if the shared library or a CUDA device is missing,
+the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libqesb200.so")
+
+QESB_OK = 0
+_STATUS = {
+    1: "QESB_ERR_ARG",
+    2: "QESB_ERR_CUDA",
+    3: "QESB_ERR_NOMEM",
+    4: "QESB_ERR_STATE",
+    5: "QESB_ERR_NUMERIC",
+    6: "QESB_ERR_NODEV",
+}
+
+# SolverFactory solve types (src/winds/SolverFactory.h:48-51) plus this build's.
+CPU_Type, DYNAMIC_P, Global_M, Shared_M = 1, 2, 3, 4
+B200_Type = 5
+
+
+class QesbError(RuntimeError):
+    """A non-OK status from the C ABI (the reference would have exited)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class Grid(C.Structure):
+    _fields_ = [("Nx", C.c_int), ("Ny", C.c_int), ("Nz", C.c_int), ("dx", C.c_float),
+                ("dy", C.c_float), ("dz_array", C.POINTER(C.c_float))]
+
+
+class Stats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("residual", C.c_double),
+                ("ms_total", C.c_double), ("ms_sor", C.c_double), ("path", C.c_int),
+                ("sweeps_per_launch", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class Building(C.Structure):
+    _fields_ = [("x_start", C.c_float), ("y_start", C.c_float), ("length", C.c_float),
+                ("width", C.c_float), ("height", C.c_float), ("base_height", C.c_float)]
+
+
+class Inflow(C.Structure):
+    _fields_ = [("u_ref", C.c_float), ("z_ref", C.c_float), ("p", C.c_float),
+                ("dir_deg", C.c_float)]
+
+
+_lib_handle = None
+
+_FP = C.POINTER(C.c_float)
+_IP = C.POINTER(C.c_int)
+
+
+def lib() -> C.CDLL:
+    """Load libqesb200.so (built by qes-public_b200/Makefile)."""
+    global _lib_handle
+    if _lib_handle is None:
+        if not os.path.exists(LIB_PATH):
+            raise QesbError(4, f"{LIB_PATH} is not built (run __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        V = C.c_void_p
+        sig = {
+            "qesb_version": ([], C.c_char_p),
+            "qesb_last_error": ([], C.c_char_p),
+            "qesb_create": ([C.POINTER(Grid), C.c_float, C.c_int, C.POINTER(V)], C.c_int),
+            "qesb_destroy": ([V], C.c_int),
+            "qesb_reset_lambda": ([V], C.c_int),
+            "qesb_set_inputs": ([V] + [V] * 10, C.c_int),
+            "qesb_set_inputs_device": ([V] + [V] * 10, C.c_int),
+            "qesb_solve": ([V, C.c_int, V, V, V, C.POINTER(Stats)], C.c_int),
+            "qesb_solve_device": ([V, C.c_int, V, V, V, C.POINTER(Stats)], C.c_int),
+            "qesb_set_lambda": ([V, V], C.c_int),
+            "qesb_get_lambda": ([V, V], C.c_int),
+            "qesb_get_divergence": ([V, V], C.c_int),
+            "qesb_get_residual_history": ([V, V, C.c_int], C.c_int),
+            "qesb_set_tolerance": ([V, C.c_float], C.c_int),
+            "qesb_set_option": ([V, C.c_char_p, C.c_int], C.c_int),
+            "qesb_set_stream": ([V, V], C.c_int),
+            "qesb_city_dz": ([C.c_int, C.c_float, C.c_float, _FP], C.c_int),
+            "qesb_city_build": ([C.POINTER(Grid), C.c_int, C.POINTER(Building), C.POINTER(Inflow)]
+                                + [V] * 10, C.c_int),
+            "qesb_city_random": ([C.POINTER(Grid), C.c_uint64, C.c_int, C.c_float, C.c_float,
+                                  C.c_float, C.c_float, C.POINTER(Building), _IP,
+                                  C.POINTER(Inflow)], C.c_int),
+        }
+        for name, (args, res) in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib_handle = L
+    return _lib_handle
+
+
+def check(status: int) -> None:
+    if status != QESB_OK:
+        raise QesbError(status, lib().qesb_last_error().decode())
+
+
+def _ptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "arrays must be C-contiguous"
+    return a.ctypes.data_as(C.c_void_p)
+
+
+# ---------------------------------------------------------------------------
+# qes::Domain mirror (src/qes/Domain.h:94-196, Domain.cpp:7-151)
+# ---------------------------------------------------------------------------
+class Domain:
+    """Staggered grid: nx = Nx+1, ny = Ny+1, nz = Nz+2 (Domain.cpp:11-13).
+
+    dz_array: None for a uniform grid of spacing dz (defineVerticalStretching(float)),
+    or the nz-1 values including the ghost layer at index 0 (the layout of
+    Domain::dz_array after defineVerticalStretching(vector), Domain.cpp:121-133).
+    """
+
+    def __init__(self, Nx: int, Ny: int, Nz: int, dx: float, dy: float, dz: float,
+                 dz_array: np.ndarray | None = None):
+        self._nx, self._ny, self._nz = Nx + 1, Ny + 1, Nz + 2
+        self._dx, self._dy = np.float32(dx), np.float32(dy)
+        if dz_array is None:
+            self.dz_array = np.full(self._nz - 1, dz, dtype=np.float32)
+        else:
+            self.dz_array = np.ascontiguousarray(dz_array, dtype=np.float32)
+            assert self.dz_array.shape == (self._nz - 1,)
+        self._dz = np.float32(self.dz_array.min())
+        zf = np.zeros(self._nz, dtype=np.float32)
+        zf[0] = -self.dz_array[0]
+        for k in range(2, self._nz):
+            zf[k] = np.float32(zf[k - 1] + self.dz_array[k - 1])
+        z = np.zeros(self._nz - 1, dtype=np.float32)
+        z[0] = np.float32(-0.5) * self.dz_array[0]
+        for k in range(1, self._nz - 1):
+            z[k] = np.float32(0.5) * np.float32(zf[k] + zf[k + 1])
+        self.z_face, self.z = zf, z
+
+    def nx(self): return self._nx
+    def ny(self): return self._ny
+    def nz(self): return self._nz
+    def dx(self): return float(self._dx)
+    def dy(self): return float(self._dy)
+    def dz(self): return float(self._dz)
+
+    @property
+    def base(self):
+        return self._nx - 1, self._ny - 1, self._nz - 2
+
+    def numCellCentered(self): return (self._nx - 1) * (self._ny - 1) * (self._nz - 1)
+    def numFaceCentered(self): return self._nx * self._ny * self._nz
+    def cell(self, i, j, k): return i + j * (self._nx - 1) + k * (self._nx - 1) * (self._ny - 1)
+    def face(self, i, j, k): return i + j * self._nx + k * self._nx * self._ny
+
+    def cell_shape(self):  # numpy (k, j, i) view shape of a cell array
+        return (self._nz - 1, self._ny - 1, self._nx - 1)
+
+    def face_shape(self):
+        return (self._nz, self._ny, self._nx)
+
+    def grid_struct(self) -> Grid:
+        Nx, Ny, Nz = self.base
+        g = Grid(Nx, Ny, Nz, float(self._dx), float(self._dy),
+                 self.dz_array.ctypes.data_as(_FP))
+        g._keep = self.dz_array
+        return g
+
+
+# ---------------------------------------------------------------------------
+# WINDSGeneralData mirror: only the fields the solve reads and writes
+# (src/winds/WINDSGeneralData.h:231-274).
+# ---------------------------------------------------------------------------
+class WINDSGeneralData:
+    FIELDS_CELL = ("e", "f", "g", "h", "m", "n")
+    FIELDS_FACE = ("u0", "v0", "w0", "u", "v", "w")
+
+    def __init__(self, domain: Domain):
+        self.domain = domain
+        nc, nf = domain.numCellCentered(), domain.numFaceCentered()
+        for name in self.FIELDS_CELL:
+            setattr(self, name, np.ones(nc, dtype=np.float32))
+        self.icellflag = np.ones(nc, dtype=np.int32)
+        for name in self.FIELDS_FACE:
+            setattr(self, name, np.zeros(nf, dtype=np.float32))
+
+    def inputs(self):
+        return (self.e, self.f, self.g, self.h, self.m, self.n, self.icellflag,
+                self.u0, self.v0, self.w0)
+
+
+# ---------------------------------------------------------------------------
+# Solver mirror
+# ---------------------------------------------------------------------------
+class Solver_B200:
+    """Solver(qes::Domain, const float &tol) backed by the B200 kernels.
+
+    solve(WGD, itermax) has Solver::solve's semantics: it reads e..n,
+    icellflag, u0, v0, w0 from WGD and writes WGD.u, WGD.v, WGD.w. lambda
+    persists between calls until resetLambda(), as in the reference CPU solvers.
+    """
+
+    omega = 1.78  # src/winds/Solver.h:83
+    alpha1 = alpha2 = 1
+
+    def __init__(self, domain: Domain, tol: float, device: int = 0):
+        self.domain = domain
+        self.tol = np.float32(tol)
+        self._h = C.c_void_p()
+        g = domain.grid_struct()
+        check(lib().qesb_create(C.byref(g), float(self.tol), device, C.byref(self._h)))
+        self._inputs_id = None
+        self.last_stats: dict | None = None
+
+    def close(self):
+        if self._h:
+            lib().qesb_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # Solver::resetLambda
+    def resetLambda(self):
+        check(lib().qesb_reset_lambda(self._h))
+
+    def set_option(self, key: str, value: int):
+        check(lib().qesb_set_option(self._h, key.encode(), int(value)))
+
+    def set_tolerance(self, tol: float):
+        self.tol = np.float32(tol)
+        check(lib().qesb_set_tolerance(self._h, float(self.tol)))
+
+    def set_inputs(self, WGD: WINDSGeneralData):
+        arrs = [np.ascontiguousarray(a) for a in WGD.inputs()]
+        check(lib().qesb_set_inputs(self._h, *[_ptr(a) for a in arrs]))
+
+    def set_inputs_device(self, e, f, g, h, m, n, icellflag, u0, v0, w0):
+        """Device pointers (ints) in the reference layouts."""
+        check(lib().qesb_set_inputs_device(self._h, e, f, g, h, m, n, icellflag, u0, v0, w0))
+
+    # Solver::solve
+    def solve(self, WGD: WINDSGeneralData, itermax: int, set_inputs: bool = True) -> dict:
+        if set_inputs:
+            self.set_inputs(WGD)
+        st = Stats()
+        check(lib().qesb_solve(self._h, int(itermax), _ptr(WGD.u), _ptr(WGD.v), _ptr(WGD.w),
+                               C.byref(st)))
+        self.last_stats = st.as_dict()
+        return self.last_stats
+
+    def solve_device(self, itermax: int, u_ptr, v_ptr, w_ptr) -> dict:
+        st = Stats()
+        check(lib().qesb_solve_device(self._h, int(itermax), u_ptr, v_ptr, w_ptr, C.byref(st)))
+        self.last_stats = st.as_dict()
+        return self.last_stats
+
+    @property
+    def lambda_(self) -> np.ndarray:
+        out = np.empty(self.domain.numCellCentered(), dtype=np.float32)
+        check(lib().qesb_get_lambda(self._h, _ptr(out)))
+        return out
+
+    @lambda_.setter
+    def lambda_(self, value: np.ndarray):
+        a = np.ascontiguousarray(value, dtype=np.float32)
+        assert a.size == self.domain.numCellCentered()
+        check(lib().qesb_set_lambda(self._h, _ptr(a)))
+
+    def residual_history(self, n: int) -> np.ndarray:
+        out = np.empty(n, dtype=np.float64)
+        check(lib().qesb_get_residual_history(self._h, _ptr(out), int(n)))
+        return out
+
+    @property
+    def R(self) -> np.ndarray:
+        out = np.empty(self.domain.numCellCentered(), dtype=np.float32)
+        check(lib().qesb_get_divergence(self._h, _ptr(out)))
+        return out
+
+
+class SolverFactory:
+    """SolverFactory::create (src/winds/SolverFactory.cpp:35-60) with the B200 type.
+
+    This package builds only the B200 solver; asking it for another type is
+    the reference's "Invalid solver type" error."""
+
+    @staticmethod
+    def create(solveType: int, domain: Domain, tolerance: float) -> Solver_B200:
+        if solveType == B200_Type:
+            return Solver_B200(domain, tolerance)
+        raise QesbError(1, "Invalid solver type")
+
+
+# ---------------------------------------------------------------------------
+# synthetic cities
+# ---------------------------------------------------------------------------
+def city_dz(Nz: int, dz0: float, ratio: float) -> np.ndarray:
+    dz = np.empty(Nz + 1, dtype=np.float32)
+    check(lib().qesb_city_dz(Nz, dz0, ratio, dz.ctypes.data_as(_FP)))
+    return dz
+
+
+def city_build(domain: Domain, buildings, inflow: Inflow) -> WINDSGeneralData:
+    """WINDSGeneralData with flags, wall coefficients and power-law inflow set."""
+    wgd = WINDSGeneralData(domain)
+    nb = len(buildings)
+    arr = (Building * max(nb, 1))(*buildings)
+    g = domain.grid_struct()
+    check(lib().qesb_city_build(C.byref(g), nb, arr, C.byref(inflow),
+                                *[_ptr(a) for a in (wgd.icellflag, wgd.e, wgd.f, wgd.g, wgd.h,
+                                                    wgd.m, wgd.n, wgd.u0, wgd.v0, wgd.w0)]))
+    return wgd
+
+
+@dataclass
+class City:
+    domain: Domain
+    buildings: list
+    inflow: Inflow
+    seed: int
+
+
+def city_random(domain: Domain, seed: int, max_buildings: int, fp=(10.0, 40.0),
+                h=(10.0, 60.0)) -> City:
+    buf = (Building * max(max_buildings, 1))()
+    n = C.c_int()
+    inf = Inflow()
+    g = domain.grid_struct()
+    check(lib().qesb_city_random(C.byref(g), seed, max_buildings, fp[0], fp[1], h[0], h[1], buf,
+                                 C.byref(n), C.byref(inf)))
+    return City(domain, [buf[i] for i in range(n.value)], inf, seed)
+
+
+# ---------------------------------------------------------------------------
+# the benchmark configurations (grid + generator parameters)
+# ---------------------------------------------------------------------------
+def config_domain(name: str) -> Domain:
+    """Grids of the named workloads (sizes Nx x Ny x Nz)."""
+    if name == "cuboid100":      # 100x100x50, dx=dy=dz=1 m
+        return Domain(100, 100, 50, 1.0, 1.0, 1.0)
+    if name == "city400":        # 400x400x100, dx=dy=2 m, dz 1 m x 1.03^k
+        return Domain(400, 400, 100, 2.0, 2.0, 1.0, city_dz(100, 1.0, 1.03))
+    if name == "city800":        # 800x800x128, same generator
+        return Domain(800, 800, 128, 2.0, 2.0, 1.0, city_dz(128, 1.0, 1.03))
+    if name == "city128":        # 128x128x64 training domains
+        return Domain(128, 128, 64, 2.0, 2.0, 1.0, city_dz(64, 1.0, 1.03))
+    if name == "city256":        # 256x256x64 evaluation domains
+        return Domain(256, 256, 64, 2.0, 2.0, 1.0, city_dz(64, 1.0, 1.03))
+    raise KeyError(name)
+
+
+def cuboid100() -> WINDSGeneralData:
+    """One 20x20x20 m cuboid centred in a 100x100x50 m domain; inflow
+    u = 5 m/s (z/10 m)^0.15 from 270 deg."""
+    d = config_domain("cuboid100")
+    return city_build(d, [Building(40.0, 40.0, 20.0, 20.0, 20.0, 0.0)], Inflow(5.0, 10.0, 0.15, 270.0))
+
+
+def random_city(name: str, seed: int) -> tuple[WINDSGeneralData, City]:
+    counts = {"city400": (60, 60), "city800": (150, 150), "city128": (20, 40), "city256": (40, 80)}
+    d = config_domain(name)
+    lo, hi = counts[name]
+    nb = lo if lo == hi else lo + (seed * 2654435761 % (hi - lo + 1))
+    c = city_random(d, seed, nb)
+    return city_build(d, c.buildings, c.inflow), c

@@ -1,0 +1,84 @@
+"""The city generator (qes-public_b200/csrc/qesb_city.cpp) against the
+reference's wall routines (Wall.cpp:44-350, 805-846) and building rules."""
+import numpy as np
+import pytest
+
+import qesb
+from oracle import oracle as O
+
+
+def test_walls_match_golden(golden):
+    import os
+
+    z = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "walls_city.npz")))
+    d = qesb.Domain(int(z["Nx"]), int(z["Ny"]), int(z["Nz"]), 2.0, 2.0, 1.0, z["dz_array"])
+    c = qesb.city_random(d, int(z["seed"]), 8, fp=(6, 20), h=(4, 30))
+    w = qesb.city_build(d, c.buildings, c.inflow)
+    np.testing.assert_array_equal(np.where(w.icellflag == 0, 0, w.icellflag), z["flag_in"])
+    np.testing.assert_array_equal(w.icellflag, z["icellflag"])
+    for k in "efghmn":
+        np.testing.assert_array_equal(getattr(w, k), z[k])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_walls_and_solid_faces_match_reference(seed):
+    d = qesb.Domain(36, 30, 18, 2.0, 2.0, 1.0, qesb.city_dz(18, 1.0, 1.03))
+    c = qesb.city_random(d, seed, 7, fp=(6, 16), h=(4, 24))
+    w = qesb.city_build(d, c.buildings, c.inflow)
+    flag, *co = O.ref_walls(d, w.icellflag)
+    np.testing.assert_array_equal(flag, w.icellflag)
+    for a, b in zip(co, (w.e, w.f, w.g, w.h, w.m, w.n)):
+        np.testing.assert_array_equal(a, b)
+    # setVelocityZero applied to the generator's profile leaves it unchanged
+    u0, v0, w0 = O.ref_set_velocity_zero(d, w.icellflag, w.u0, w.v0, w.w0)
+    np.testing.assert_array_equal(u0, w.u0)
+    np.testing.assert_array_equal(v0, w.v0)
+    np.testing.assert_array_equal(w0, w.w0)
+
+
+def test_cuboid100_cells():
+    """20x20x20 m cuboid at x, y in [40, 60] m: PNPOLY on cell centres puts
+    cells 40..59 inside; heights 0..20 m give k = 1..20 (z[k] = k - 0.5)."""
+    w = qesb.cuboid100()
+    d = w.domain
+    f = w.icellflag.reshape(d.cell_shape())
+    solid = np.argwhere(f[1:] == 0)
+    assert solid[:, 0].min() + 1 == 1 and solid[:, 0].max() + 1 == 20
+    assert solid[:, 1].min() == 40 and solid[:, 1].max() == 59
+    assert solid[:, 2].min() == 40 and solid[:, 2].max() == 59
+    assert (f[0] == 2).all()
+
+
+def test_power_law_profile():
+    w = qesb.cuboid100()
+    d = w.domain
+    u0 = w.u0.reshape(d.face_shape())
+    for k in (1, 10, 30, 50):
+        expect = np.float32(np.float32(1.0) * np.float32(5.0)) * np.float32(
+            np.power(np.float32(d.z[k] / np.float32(10.0)), np.float32(0.15), dtype=np.float32))
+        assert abs(float(u0[k, 5, 5]) - float(expect)) <= 2e-6 * float(expect)
+    assert (w.v0 == 0).all() and (w.w0 == 0).all()
+    assert (u0[0] == 0).all() and (u0[-1] == 0).all()
+
+
+def test_random_city_is_seeded_and_non_overlapping():
+    d = qesb.config_domain("city400")
+    a = qesb.city_random(d, 42, 60)
+    b = qesb.city_random(d, 42, 60)
+    assert len(a.buildings) == 60
+    assert [(x.x_start, x.y_start, x.length, x.width, x.height) for x in a.buildings] == \
+           [(x.x_start, x.y_start, x.length, x.width, x.height) for x in b.buildings]
+    for i, p in enumerate(a.buildings):
+        assert 10 <= p.length <= 40 and 10 <= p.width <= 40 and 10 <= p.height <= 60
+        for q in a.buildings[:i]:
+            overlap = (p.x_start < q.x_start + q.length and q.x_start < p.x_start + p.length and
+                       p.y_start < q.y_start + q.width and q.y_start < p.y_start + p.width)
+            assert not overlap
+    assert 3 <= a.inflow.u_ref <= 10 and 0.1 <= a.inflow.p <= 0.3 and 0 <= a.inflow.dir_deg < 360
+
+
+def test_stretched_dz():
+    dz = qesb.city_dz(100, 1.0, 1.03)
+    assert dz[0] == dz[1] == 1.0
+    assert abs(dz[100] - 1.03 ** 99) < 1e-3

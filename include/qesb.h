@@ -61,6 +61,7 @@ typedef struct qesb_stats {
   double ms_sor;         /* device time of the SOR iterations alone */
   int path;              /* 0 = full-coefficient sweep, 1 = packed wall-mask sweep */
   int sweeps_per_launch; /* iterations fused per sweep launch */
+  int launches;          /* kernels this solve launched (including polls and early exits) */
 } qesb_stats;
 
 /* Library and device. */
@@ -111,10 +112,17 @@ qesb_status qesb_get_divergence(qesb_handle *h, float *R);  /* R of the last sol
 /* FP64 max|dlambda| of each iteration of the last solve, iterations 0..n-1. */
 qesb_status qesb_get_residual_history(qesb_handle *h, double *out, int n);
 
+/* Runs n launches of the fused sweep kernel back to back on the current
+ * inputs (no polls, no stop) and returns their total device time in *ms and
+ * the iterations each launch fuses in *k. Advances lambda by n*k iterations;
+ * meant for measuring the kernel alone. Requires stair-step inputs. */
+qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k);
+
 /* Tolerance (Solver::tol) and tuning knobs. Keys:
  *   "sweeps_per_launch"  iterations fused per sweep launch (0 = autotuned)
  *   "path"               0 = force full coefficients, 1 = allow the packed mask (default)
- *   "graph"              1 = run the iteration loop as a CUDA graph (default), 0 = plain launches */
+ *   "graph"              1 = run the iteration loop as a CUDA graph (default), 0 = plain launches
+ *   "variant"            fused-kernel tile variant index (-1 = automatic) */
 qesb_status qesb_set_tolerance(qesb_handle *h, float tol);
 qesb_status qesb_set_option(qesb_handle *h, const char *key, int value);
 /* cudaStream_t to run on (NULL = the handle's own stream). */

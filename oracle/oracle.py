@@ -71,6 +71,9 @@ def ref() -> C.CDLL:
         L.qesref_set_velocity_zero.restype = i
         L.qesref_solve.argtypes = [i, i, i, i, f, f] + [_V] * 11 + [f, i] + [_V] * 5
         L.qesref_solve.restype = C.c_double
+        L.qesref_set_threads.argtypes = [i]
+        L.qesref_set_threads.restype = None
+        L.qesref_set_threads(1)
         _ref = L
     return _ref
 
@@ -144,6 +147,11 @@ def max_divergence(dom, flag, u, v, w, kmax=None):
 
 
 # ----------------------------------------------------------------------------- reference
+def ref_set_threads(n: int) -> None:
+    """OpenMP threads for Solver_CPU_RB (1 by default: see qesref_set_threads)."""
+    ref().qesref_set_threads(int(n))
+
+
 def ref_walls(dom, icellflag):
     """Reference Wall::defineWalls + solverCoefficients: (icellflag, e, f, g, h, m, n)."""
     nc = dom.numCellCentered()

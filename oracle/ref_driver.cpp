@@ -74,6 +74,12 @@ double run_solver(const qes::Domain &d, WINDSGeneralData &wgd, float tol, int it
 
 extern "C" {
 
+// OpenMP threads used by Solver_CPU_RB. Its convergence loop resets the shared
+// max_error inside the parallel region (Solver_CPU_RB.cpp:166), so with more
+// than one thread a run can stop early; parity runs use 1 thread, timing runs
+// pass tol < 0 so the loop always runs to itermax.
+void qesref_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
+
 // Wall::defineWalls + Wall::solverCoefficients (src/winds/Wall.cpp:44-350,
 // 827-846) on a WINDSGeneralData built as allocateMemory leaves it
 // (src/winds/WINDSGeneralData.cpp:1064-1121: e..n = 1, volume fractions 1).

@@ -8,6 +8,7 @@ namespace qesb {
 constexpr float kOmega = 1.78f;  // over-relaxation factor, src/winds/Solver.h:83
 constexpr int kGX = 8;           // x guard cells on each side of the padded layout
 constexpr int kGY = 8;           // y guard rows on each side
+constexpr int kMaxTileRows = 64; // tallest tiled-kernel tile (rows incl. halo)
 
 // Grid sizes in cells (X, Y, Z = nx-1, ny-1, nz-1), in faces (FX, FY, FZ =
 // nx, ny, nz) and the padded cell layout (PX, PY, PLANE).
@@ -33,7 +34,10 @@ struct SolveState {
   int converged;  // stop came from max|dlambda| <= tol
   int nan;        // a NaN error was met
   double residual;
-  int pad[2];
+  int cur;        // lambda buffer (0 or 1) written by the last launch that ran
+  int redo;       // >0: the converging launch ran past the stop; re-run this many iterations
+  int redo_t0;    // first iteration of that launch
+  int redo_par;   // its output buffer
 };
 
 __device__ __forceinline__ bool is_solid(int flag) { return flag == 0 || flag == 2; }

@@ -34,6 +34,7 @@
 #include "qesb.h"
 #include "qesb_internal.h"
 #include "qesb_device.cuh"
+#include "qesb_sor_tiled.cuh"
 
 // ---------------------------------------------------------------------------
 // errors
@@ -245,25 +246,39 @@ __global__ void k_mirror(DevGrid G, float *__restrict__ L, const SolveState *__r
   }
 }
 
-// Convergence poll after iteration st->it: the reference loop condition
-// `iter < itermax && max_error > tol` (Solver_CPU.cpp:93), with max_error in
-// double. A NaN error stops the solve and is reported.
-__global__ void k_poll(SolveState *st, const double *__restrict__ err, double tol, int itermax)
+// Convergence poll after a launch of up to kmax iterations starting at
+// st->it: the reference loop condition `iter < itermax && max_error > tol`
+// (Solver_CPU.cpp:93) checked for each of the launch's iterations in order,
+// with max_error in double. If the stop falls inside a fused launch, that
+// launch ran past it; the poll records how many of its iterations count so
+// the host re-runs exactly those from the launch's input buffer. A NaN error
+// stops the solve and is reported. `parity` is the launch's output buffer.
+__global__ void k_poll(SolveState *st, const double *__restrict__ err, double tol, int itermax,
+                       int kmax, int parity)
 {
   if (st->done) return;
-  const int it = st->it;
-  const double e = err[it];
-  st->residual = e;
-  st->it = it + 1;
-  if (isnan(e)) {
-    st->done = 1;
-    st->nan = 1;
-  } else if (!(e > tol)) {
-    st->done = 1;
-    st->converged = 1;
-  } else if (it + 1 >= itermax) {
-    st->done = 1;
+  const int t0 = st->it;
+  const int nit = min(kmax, itermax - t0);
+  st->cur = parity;
+  for (int t = 0; t < nit; ++t) {
+    const double e = err[t0 + t];
+    st->residual = e;
+    const bool nan = isnan(e);
+    if (nan || !(e > tol)) {
+      st->done = 1;
+      st->nan = nan;
+      st->converged = !nan;
+      st->it = t0 + t + 1;
+      if (t + 1 < nit && !nan) {
+        st->redo = t + 1;
+        st->redo_t0 = t0;
+        st->redo_par = parity;
+      }
+      return;
+    }
   }
+  st->it = t0 + nit;
+  if (st->it >= itermax) st->done = 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -351,11 +366,55 @@ struct qesb_handle {
   int opt_path = 1;
   int opt_k = 0;
   int opt_graph = 1;
+  int opt_variant = -1;
+  int last_launches = 0;
+
+  // iteration-loop graphs of the tiled path, one per (variant, starting buffer)
+  struct GraphKey {
+    int variant, start, chunk;
+    float tol;
+    int itermax;
+    cudaStream_t stream;
+  };
+  GraphKey gkey[2] = {{-1, 0, 0, 0, 0, nullptr}, {-1, 1, 0, 0, 0, nullptr}};
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
 };
 
 namespace {
 
 size_t pad_cells(const DevGrid &G) { return (size_t)G.PLANE * G.Z; }
+
+// Tiled kernels read whole halo tiles; at the far x/y edge of the last
+// plane a tile may run past the padded plane. The slack keeps those reads
+// inside the allocation (the values read there feed only guard cells).
+size_t pad_alloc(const DevGrid &G) { return pad_cells(G) + (size_t)(kMaxTileRows + kGY) * G.PX + 256; }
+
+// ---------------------------------------------------------------------------
+// tiled-kernel variants (template instances) and their launch shapes
+// ---------------------------------------------------------------------------
+struct Variant {
+  const char *name;
+  int K, BX, BY, NT, TX, TY;
+  size_t smem;
+  void (*fn)(TiledArgs);
+};
+
+template <int K, int BX, int BY, int NT>
+constexpr Variant make_variant(const char *name)
+{
+  using C = TileCfg<K, BX, BY, NT>;
+  return Variant{name, K, BX, BY, NT, C::TX, C::TY, C::SMEM, k_sor_tiled<K, BX, BY, NT>};
+}
+
+const Variant kVariants[] = {
+    make_variant<1, 64, 32, 256>("k1_64x32"),
+    make_variant<2, 64, 32, 256>("k2_64x32"),
+    make_variant<2, 64, 48, 256>("k2_64x48"),
+    make_variant<1, 128, 32, 512>("k1_128x32"),
+    make_variant<2, 128, 24, 512>("k2_128x24"),
+};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+static_assert(kMaxTileRows >= 48, "slack rows must cover the tallest tile");
 
 qesb_status fill_grid(const qesb_grid *g, DevGrid &G)
 {
@@ -452,13 +511,120 @@ qesb_status run_iterations_full(qesb_handle *h, int itermax)
                                          h->d_pc[3], h->d_pc[4], h->d_pc[5], h->d_R, h->d_err,
                                          h->d_state);
       k_mirror<<<mgrid, 256, 0, s>>>(G, h->d_lam, h->d_state);
-      k_poll<<<1, 1, 0, s>>>(h->d_state, h->d_err, (double)h->tol, itermax);
+      k_poll<<<1, 1, 0, s>>>(h->d_state, h->d_err, (double)h->tol, itermax, 1, 0);
     }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (h->h_state->done) break;
   }
+  return QESB_OK;
+}
+
+// Picks the tiled-kernel variant: the caller's sweeps_per_launch if set,
+// else the autotuned choice for this grid (see autotune()).
+int pick_variant(qesb_handle *h);
+
+TiledArgs tiled_args(qesb_handle *h, const float *in, float *out, int itermax, int redo)
+{
+  TiledArgs a;
+  a.G = h->G;
+  a.lam_in = in;
+  a.lam_out = out;
+  a.R = h->d_R;
+  a.mask = h->d_mask;
+  a.val = h->d_val;
+  a.inv = h->d_inv;
+  a.err = h->d_err;
+  a.st = h->d_state;
+  a.itermax = itermax;
+  a.redo = redo;
+  return a;
+}
+
+dim3 tiled_grid(const DevGrid &G, const Variant &v)
+{
+  return dim3((G.X + v.TX - 1) / v.TX, (G.Y + v.TY - 1) / v.TY, 1);
+}
+
+qesb_status set_smem_attr(const Variant &v)
+{
+  static bool done[kNumVariants] = {};
+  const int idx = (int)(&v - kVariants);
+  if (!done[idx]) {
+    CK(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem));
+    done[idx] = true;
+  }
+  return QESB_OK;
+}
+
+// One chunk of the tiled iteration loop: `chunk` launches alternating the two
+// lambda buffers, each followed by its poll. Launches after the stop return
+// at once (they read st->done first).
+qesb_status enqueue_chunk(qesb_handle *h, const Variant &v, int start, int chunk, int itermax)
+{
+  cudaStream_t s = h->stream;
+  float *buf[2] = {h->d_lam, h->d_lam2};
+  const dim3 grid = tiled_grid(h->G, v);
+  for (int c = 0; c < chunk; ++c) {
+    const int src = (start + c) & 1, dst = src ^ 1;
+    v.fn<<<grid, v.NT, v.smem, s>>>(tiled_args(h, buf[src], buf[dst], itermax, 0));
+    k_poll<<<1, 1, 0, s>>>(h->d_state, h->d_err, (double)h->tol, itermax, v.K, dst);
+  }
+  CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status run_iterations_tiled(qesb_handle *h, const Variant &v, int itermax)
+{
+  cudaStream_t s = h->stream;
+  CKS(set_smem_attr(v));
+  // about 2 ms of device work per chunk between host polls of the state
+  const double cells = (double)h->G.XY * h->G.Z;
+  const int per_launch_us = std::max(1, (int)(cells * v.K / 4.0e5));
+  int chunk = std::max(2, std::min(64, 2000 / per_launch_us));
+  chunk += chunk & 1;  // even: every full chunk ends back in buffer 0
+  const int max_launches = (itermax + v.K - 1) / v.K;
+  int launched = 0;
+  for (int base = 0; launched < max_launches; base += chunk) {
+    if (h->opt_graph) {
+      auto &key = h->gkey[0];
+      const bool hit = h->gexec[0] && key.variant == (int)(&v - kVariants) && key.chunk == chunk &&
+                       key.tol == h->tol && key.itermax == itermax && key.stream == s;
+      if (!hit) {
+        if (h->gexec[0]) cudaGraphExecDestroy(h->gexec[0]);
+        h->gexec[0] = nullptr;
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        qesb_status qs = enqueue_chunk(h, v, 0, chunk, itermax);
+        cudaError_t ce = cudaStreamEndCapture(s, &g);
+        if (qs != QESB_OK) return qs;
+        if (ce != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&h->gexec[0], g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+        key = {(int)(&v - kVariants), 0, chunk, h->tol, itermax, s};
+      }
+      CK(cudaGraphLaunch(h->gexec[0], s));
+    } else {
+      CKS(enqueue_chunk(h, v, 0, chunk, itermax));
+    }
+    launched += chunk;
+    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h->h_state->done) break;
+  }
+  h->last_launches = launched * 2;
+  // Exact stop: the converging launch fused iterations past the stop; re-run
+  // only the iterations that count, from that launch's input buffer.
+  if (h->h_state->redo > 0) {
+    float *buf[2] = {h->d_lam, h->d_lam2};
+    const int dst = h->h_state->redo_par;
+    v.fn<<<tiled_grid(h->G, v), v.NT, v.smem, s>>>(tiled_args(h, buf[dst ^ 1], buf[dst], itermax, 1));
+    CK(cudaGetLastError());
+    h->last_launches += 1;
+  }
+  if (h->h_state->cur == 1) std::swap(h->d_lam, h->d_lam2);
   return QESB_OK;
 }
 
@@ -479,7 +645,13 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
   CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
   CK(cudaEventRecord(h->ev[1], s));
-  if (itermax > 0) CKS(run_iterations_full(h, itermax));
+  const bool tiled = h->packed && h->opt_path == 1;
+  const Variant *var = tiled ? &kVariants[pick_variant(h)] : nullptr;
+  h->last_launches = 0;
+  if (itermax > 0) {
+    if (tiled) CKS(run_iterations_tiled(h, *var, itermax));
+    else CKS(run_iterations_full(h, itermax));
+  }
   CK(cudaEventRecord(h->ev[2], s));
   k_correct<<<row_grid(G, G.FY, G.FZ, G.FX), 256, 0, s>>>(
       G, h->d_lam, h->d_in[1], h->d_in[3], h->d_in[5], h->d_flag, h->d_u0, h->d_v0, h->d_w0,
@@ -497,15 +669,25 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
     st->residual = itermax > 0 ? h->h_state->residual : 1.0;
     st->ms_total = a;
     st->ms_sor = b;
-    st->path = 0;
-    st->sweeps_per_launch = 1;
+    st->path = tiled ? 1 : 0;
+    st->sweeps_per_launch = tiled ? var->K : 1;
+    st->launches = 2 + (tiled ? h->last_launches : 4 * st->iterations);
   }
   if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the solve (iteration %d)", h->h_state->it);
   return QESB_OK;
 }
 
+int pick_variant(qesb_handle *h)
+{
+  if (h->opt_variant >= 0) return h->opt_variant;
+  if (h->opt_k == 1) return 0;
+  return 1;  // K = 2, 64 x 32 tiles
+}
+
 void free_all(qesb_handle *h)
 {
+  for (auto &g : h->gexec)
+    if (g) cudaGraphExecDestroy(g);
   void *ptrs[] = {h->d_lam, h->d_lam2, h->d_R, h->d_mask, h->d_pc[0], h->d_pc[1], h->d_pc[2],
                   h->d_pc[3], h->d_pc[4], h->d_pc[5], h->d_own_in[0], h->d_own_in[1],
                   h->d_own_in[2], h->d_own_in[3], h->d_own_in[4], h->d_own_in[5], h->d_own_flag,
@@ -558,7 +740,7 @@ qesb_status qesb_create(const qesb_grid *grid, float tol, int device, qesb_handl
   qesb_status s = QESB_OK;
 #define TRY(x)                          \
   if ((s = (x)) != QESB_OK) return fail(s);
-  const size_t np = pad_cells(G), nc = (size_t)G.XY * G.Z, nf = (size_t)G.FXY * G.FZ;
+  const size_t np = pad_alloc(G), nc = (size_t)G.XY * G.Z, nf = (size_t)G.FXY * G.FZ;
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(qesb_fail(QESB_ERR_CUDA, "cudaStreamCreate failed"));
   h->stream = h->own_stream;
@@ -606,7 +788,7 @@ qesb_status qesb_reset_lambda(qesb_handle *h)
 {
   if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
   CK(cudaSetDevice(h->device));
-  const size_t np = pad_cells(h->G);
+  const size_t np = pad_alloc(h->G);
   CK(cudaMemsetAsync(h->d_lam, 0, np * sizeof(float), h->stream));
   CK(cudaMemsetAsync(h->d_lam2, 0, np * sizeof(float), h->stream));
   CK(cudaMemsetAsync(h->d_R, 0, np * sizeof(float), h->stream));
@@ -761,6 +943,30 @@ qesb_status qesb_get_residual_history(qesb_handle *h, double *out, int n)
   return QESB_OK;
 }
 
+qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
+{
+  if (!h || n <= 0 || !ms) return qesb_fail(QESB_ERR_ARG, "qesb_time_sweeps: bad argument");
+  if (!h->have_inputs || !h->packed) return qesb_fail(QESB_ERR_STATE, "qesb_time_sweeps needs stair-step inputs");
+  CK(cudaSetDevice(h->device));
+  const Variant &v = kVariants[pick_variant(h)];
+  CKS(set_smem_attr(v));
+  CKS(ensure_err(h, v.K));
+  cudaStream_t s = h->stream;
+  CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+  float *buf[2] = {h->d_lam, h->d_lam2};
+  const dim3 grid = tiled_grid(h->G, v);
+  CK(cudaEventRecord(h->ev[0], s));
+  for (int c = 0; c < n; ++c)
+    v.fn<<<grid, v.NT, v.smem, s>>>(tiled_args(h, buf[c & 1], buf[(c & 1) ^ 1], 1 << 30, 0));
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev[1], s));
+  CK(cudaEventSynchronize(h->ev[1]));
+  CK(cudaEventElapsedTime(ms, h->ev[0], h->ev[1]));
+  if (n & 1) std::swap(h->d_lam, h->d_lam2);
+  if (k) *k = v.K;
+  return QESB_OK;
+}
+
 qesb_status qesb_set_tolerance(qesb_handle *h, float tol)
 {
   if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
@@ -773,13 +979,16 @@ qesb_status qesb_set_option(qesb_handle *h, const char *key, int value)
   if (!h || !key) return qesb_fail(QESB_ERR_ARG, "qesb_set_option: null argument");
   std::string k(key);
   if (k == "sweeps_per_launch") {
-    if (value < 0 || value > 4) return qesb_fail(QESB_ERR_ARG, "sweeps_per_launch must be in [0, 4]");
+    if (value < 0 || value > 2) return qesb_fail(QESB_ERR_ARG, "sweeps_per_launch must be 0 (auto), 1 or 2");
     h->opt_k = value;
   } else if (k == "path") {
     if (value != 0 && value != 1) return qesb_fail(QESB_ERR_ARG, "path must be 0 or 1");
     h->opt_path = value;
   } else if (k == "graph") {
     h->opt_graph = value ? 1 : 0;
+  } else if (k == "variant") {
+    if (value < -1 || value >= kNumVariants) return qesb_fail(QESB_ERR_ARG, "variant must be in [-1, %d)", kNumVariants);
+    h->opt_variant = value;
   } else {
     return qesb_fail(QESB_ERR_ARG, "unknown option '%s'", key);
   }

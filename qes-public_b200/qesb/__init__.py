@@ -58,7 +58,7 @@ class Grid(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("residual", C.c_double),
                 ("ms_total", C.c_double), ("ms_sor", C.c_double), ("path", C.c_int),
-                ("sweeps_per_launch", C.c_int)]
+                ("sweeps_per_launch", C.c_int), ("launches", C.c_int)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -103,6 +103,7 @@ def lib() -> C.CDLL:
             "qesb_get_divergence": ([V, V], C.c_int),
             "qesb_get_residual_history": ([V, V, C.c_int], C.c_int),
             "qesb_set_tolerance": ([V, C.c_float], C.c_int),
+            "qesb_time_sweeps": ([V, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)], C.c_int),
             "qesb_set_option": ([V, C.c_char_p, C.c_int], C.c_int),
             "qesb_set_stream": ([V, V], C.c_int),
             "qesb_city_dz": ([C.c_int, C.c_float, C.c_float, _FP], C.c_int),
@@ -301,6 +302,15 @@ class Solver_B200:
         a = np.ascontiguousarray(value, dtype=np.float32)
         assert a.size == self.domain.numCellCentered()
         check(lib().qesb_set_lambda(self._h, _ptr(a)))
+
+    def time_sweeps(self, n: int) -> tuple[float, int]:
+        """Device ms of n back-to-back fused-sweep launches, and iterations per launch."""
+        ms, k = C.c_float(), C.c_int()
+        check(lib().qesb_time_sweeps(self._h, int(n), C.byref(ms), C.byref(k)))
+        return ms.value, k.value
+
+    def set_stream(self, stream_ptr: int | None):
+        check(lib().qesb_set_stream(self._h, stream_ptr))
 
     def residual_history(self, n: int) -> np.ndarray:
         out = np.empty(n, dtype=np.float64)

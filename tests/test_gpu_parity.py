@@ -19,11 +19,12 @@ pytestmark = pytest.mark.gpu
 WIND_TOL = 1e-3  # m/s, max|du| against Solver_CPU at convergence
 
 
-def gpu_solve(d, w, itermax, tol=1e-9, path=1, lam=None, k=0):
+def gpu_solve(d, w, itermax, tol=1e-9, path=1, lam=None, k=0, variant=-1):
     with qesb.Solver_B200(d, tol) as s:
         s.set_option("path", path)
         if k:
             s.set_option("sweeps_per_launch", k)
+        s.set_option("variant", variant)
         s.set_inputs(w)
         if lam is not None:
             s.lambda_ = lam
@@ -50,14 +51,21 @@ def test_divergence_R_bit_exact(golden):
     np.testing.assert_array_equal(R, O.divergence(d, w))
 
 
-@pytest.mark.parametrize("k", [1, 2, 3, 4])
-def test_fused_sweeps_bit_exact(k):
+N_VARIANTS = 5
+
+
+@pytest.mark.parametrize("variant", range(N_VARIANTS))
+def test_fused_sweeps_bit_exact(variant):
+    """Every tile variant of the fused kernel (K = 1 and 2 iterations per
+    launch, several tile shapes), an odd iteration count (a partial last
+    launch), ragged tiles at the domain edges and a random warm start."""
     d = qesb.Domain(70, 45, 21, 2.0, 2.0, 1.0, qesb.city_dz(21, 1.0, 1.03))
     c = qesb.city_random(d, 9, 8, fp=(6, 18), h=(4, 30))
     w = qesb.city_build(d, c.buildings, c.inflow)
     lam0 = np.random.default_rng(3).standard_normal(d.numCellCentered()).astype(np.float32)
-    u, v, ww, L, st, _ = gpu_solve(d, w, 37, lam=lam0, k=k)
+    u, v, ww, L, st, _ = gpu_solve(d, w, 37, lam=lam0, variant=variant)
     uo, vo, wo, Lo, it, _ = O.solve(d, w, 1e-9, 37, ordering=1, lam=lam0)
+    assert st["path"] == 1
     assert st["iterations"] == it == 37
     np.testing.assert_array_equal(L, Lo)
     np.testing.assert_array_equal(u, uo)
@@ -65,17 +73,17 @@ def test_fused_sweeps_bit_exact(k):
     np.testing.assert_array_equal(ww, wo)
 
 
-@pytest.mark.parametrize("path", [0, 1])
-def test_stopping_rule_matches_oracle(golden, path):
+@pytest.mark.parametrize("path,variant", [(0, -1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("tol", [2e-3, 1.1e-3, 7e-4])
+def test_stopping_rule_matches_oracle(golden, path, variant, tol):
     """A reachable tolerance: the loop stops on the same iteration as the
     reference loop `while (iter < itermax && max_error > tol)` with the error
     taken in FP64, and lambda is the same bits."""
     d, w, z = golden("small_city.npz")
-    tol = 2e-3
-    u, v, ww, L, st, _ = gpu_solve(d, w, 5000, tol=tol, path=path)
+    u, v, ww, L, st, _ = gpu_solve(d, w, 5000, tol=tol, path=path, variant=variant)
     Lo, it, fe, hist = O.sor(d, w, O.divergence(d, w), tol, 5000, ordering=1, err_fp64=True,
                              hist=True)
-    assert st["converged"] == 1
+    assert st["converged"] == 1 and st["path"] == path
     assert st["iterations"] == it < 5000
     assert st["residual"] == fe <= np.float32(tol)
     np.testing.assert_array_equal(L, Lo)
@@ -151,3 +159,32 @@ def test_fp64_same_sor_error_is_stated(golden):
     werr = max(np.abs(u - u8).max(), np.abs(v - v8).max(), np.abs(ww - w8).max())
     lerr = np.abs(L - L8).max() / np.abs(L8).max()
     assert werr < 1e-3 and lerr < 1e-4
+
+
+@pytest.mark.parametrize("graph", [0, 1])
+def test_graph_and_plain_launches_agree(golden, graph):
+    d, w, z = golden("small_city.npz")
+    with qesb.Solver_B200(d, 1.1e-3) as s:
+        s.set_option("graph", graph)
+        st = s.solve(w, 5000)
+        L = s.lambda_
+    Lo, it, *_ = O.sor(d, w, O.divergence(d, w), 1.1e-3, 5000)
+    assert st["iterations"] == it
+    np.testing.assert_array_equal(L, Lo)
+
+
+def test_full_size_city400_packed_equals_full_path():
+    """400x400x100 stretched city: after 24 iterations the fused packed path and
+    the full-coefficient path hold the same lambda bits, and the fused path's
+    residual history equals the full path's."""
+    w, c = qesb.random_city("city400", 0)
+    d = w.domain
+    out = {}
+    for path in (0, 1):
+        with qesb.Solver_B200(d, 1e-9) as s:
+            s.set_option("path", path)
+            st = s.solve(w, 24)
+            out[path] = (s.lambda_, s.residual_history(24), st)
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    assert out[1][2]["path"] == 1 and out[0][2]["path"] == 0

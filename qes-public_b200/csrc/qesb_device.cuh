@@ -38,6 +38,7 @@ struct SolveState {
   int redo;       // >0: the converging launch ran past the stop; re-run this many iterations
   int redo_t0;    // first iteration of that launch
   int redo_par;   // its output buffer
+  unsigned blocks_done;  // CTAs of the current black half-sweep that have finished
 };
 
 __device__ __forceinline__ bool is_solid(int flag) { return flag == 0 || flag == 2; }

@@ -35,6 +35,7 @@
 #include "qesb_internal.h"
 #include "qesb_device.cuh"
 #include "qesb_sor_tiled.cuh"
+#include "qesb_sor_split.cuh"
 
 // ---------------------------------------------------------------------------
 // errors
@@ -369,6 +370,11 @@ struct qesb_handle {
   int opt_variant = -1;
   int last_launches = 0;
 
+  // red/black split layout (packed streaming path)
+  SplitGeom S{};
+  float *d_lam_s = nullptr, *d_R_s = nullptr;
+  uint8_t *d_mask_s = nullptr;
+
   // iteration-loop graphs of the tiled path, one per (variant, starting buffer)
   struct GraphKey {
     int variant, start, chunk;
@@ -482,6 +488,7 @@ qesb_status prepare_coefs(qesb_handle *h)
     CK(cudaStreamSynchronize(s));
     if (!bad) {
       k_inv_table<<<G.Z, 64, 0, s>>>(G, h->d_vmax, h->d_inv, h->d_val);
+      k_pad_to_split_u8<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_mask, h->d_mask_s);
       CK(cudaGetLastError());
       h->packed = true;
     }
@@ -628,6 +635,89 @@ qesb_status run_iterations_tiled(qesb_handle *h, const Variant &v, int itermax)
   return QESB_OK;
 }
 
+constexpr int kSplitRPB = 8;  // rows (warps) per CTA of the split half-sweeps
+constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the split path
+
+SplitArgs split_args(qesb_handle *h, int itermax)
+{
+  SplitArgs a;
+  a.G = h->G;
+  a.S = h->S;
+  a.lam = h->d_lam_s;
+  a.R = h->d_R_s;
+  a.mask = h->d_mask_s;
+  a.val = h->d_val;
+  a.inv = h->d_inv;
+  a.err = h->d_err;
+  a.st = h->d_state;
+  a.itermax = itermax;
+  a.tol = (double)h->tol;
+  return a;
+}
+
+qesb_status enqueue_split_chunk(qesb_handle *h, int chunk, int itermax)
+{
+  const int nrows = (h->G.Y - 2) * (h->G.Z - 2);
+  const dim3 grid((nrows + kSplitRPB - 1) / kSplitRPB), block(32, kSplitRPB);
+  const SplitArgs a = split_args(h, itermax);
+  for (int c = 0; c < chunk; ++c) {
+    k_sor_split<0, kSplitRPB><<<grid, block, 0, h->stream>>>(a);
+    k_sor_split<1, kSplitRPB><<<grid, block, 0, h->stream>>>(a);
+  }
+  CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+// Red/black split path: lambda and R to the split layout, the iteration loop
+// as CUDA-graph chunks of (red, black) launches polled from the host every
+// ~2 ms of device work, then the boundary-ring mirror and lambda back.
+qesb_status run_iterations_split(qesb_handle *h, int itermax)
+{
+  const DevGrid &G = h->G;
+  cudaStream_t s = h->stream;
+  k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam, h->d_lam_s);
+  k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_R, h->d_R_s);
+  CK(cudaGetLastError());
+  const double cells = (double)G.XY * G.Z;
+  const int per_it_us = std::max(1, (int)(cells / 3.0e5));
+  const int chunk = std::max(1, std::min(128, 2000 / per_it_us));
+  int launched = 0;
+  while (launched < itermax) {
+    if (h->opt_graph) {
+      auto &key = h->gkey[1];
+      const bool hit = h->gexec[1] && key.variant == kSplitVariant && key.chunk == chunk &&
+                       key.tol == h->tol && key.itermax == itermax && key.stream == s;
+      if (!hit) {
+        if (h->gexec[1]) cudaGraphExecDestroy(h->gexec[1]);
+        h->gexec[1] = nullptr;
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        qesb_status qs = enqueue_split_chunk(h, chunk, itermax);
+        cudaError_t ce = cudaStreamEndCapture(s, &g);
+        if (qs != QESB_OK) return qs;
+        if (ce != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&h->gexec[1], g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+        key = {kSplitVariant, 0, chunk, h->tol, itermax, s};
+      }
+      CK(cudaGraphLaunch(h->gexec[1], s));
+    } else {
+      CKS(enqueue_split_chunk(h, chunk, itermax));
+    }
+    launched += chunk;
+    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h->h_state->done) break;
+  }
+  h->last_launches = 2 * launched;
+  k_split_mirror_ring<<<G.Y, 128, 0, s>>>(G, h->S, h->d_lam_s);
+  k_split_to_pad<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam_s, h->d_lam);
+  CK(cudaGetLastError());
+  h->last_launches += 5;
+  return QESB_OK;
+}
+
 qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w, qesb_stats *st)
 {
   if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
@@ -645,11 +735,14 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
   CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
   CK(cudaEventRecord(h->ev[1], s));
-  const bool tiled = h->packed && h->opt_path == 1;
-  const Variant *var = tiled ? &kVariants[pick_variant(h)] : nullptr;
+  const bool packed = h->packed && h->opt_path == 1;
+  const int vi = packed ? pick_variant(h) : -1;
+  const bool split = packed && vi == kSplitVariant;
+  const Variant *var = packed && !split ? &kVariants[vi] : nullptr;
   h->last_launches = 0;
   if (itermax > 0) {
-    if (tiled) CKS(run_iterations_tiled(h, *var, itermax));
+    if (split) CKS(run_iterations_split(h, itermax));
+    else if (var) CKS(run_iterations_tiled(h, *var, itermax));
     else CKS(run_iterations_full(h, itermax));
   }
   CK(cudaEventRecord(h->ev[2], s));
@@ -669,9 +762,9 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
     st->residual = itermax > 0 ? h->h_state->residual : 1.0;
     st->ms_total = a;
     st->ms_sor = b;
-    st->path = tiled ? 1 : 0;
-    st->sweeps_per_launch = tiled ? var->K : 1;
-    st->launches = 2 + (tiled ? h->last_launches : 4 * st->iterations);
+    st->path = packed ? 1 : 0;
+    st->sweeps_per_launch = var ? var->K : 1;
+    st->launches = 2 + (packed ? h->last_launches : 4 * st->iterations);
   }
   if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the solve (iteration %d)", h->h_state->it);
   return QESB_OK;
@@ -680,15 +773,15 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
 int pick_variant(qesb_handle *h)
 {
   if (h->opt_variant >= 0) return h->opt_variant;
-  if (h->opt_k == 1) return 0;
-  return 1;  // K = 2, 64 x 32 tiles
+  if (h->opt_k == 2) return 1;  // fused: K = 2, 64 x 32 tiles
+  return kSplitVariant;         // streaming red/black split half-sweeps
 }
 
 void free_all(qesb_handle *h)
 {
   for (auto &g : h->gexec)
     if (g) cudaGraphExecDestroy(g);
-  void *ptrs[] = {h->d_lam, h->d_lam2, h->d_R, h->d_mask, h->d_pc[0], h->d_pc[1], h->d_pc[2],
+  void *ptrs[] = {h->d_lam_s, h->d_R_s, h->d_mask_s, h->d_lam, h->d_lam2, h->d_R, h->d_mask, h->d_pc[0], h->d_pc[1], h->d_pc[2],
                   h->d_pc[3], h->d_pc[4], h->d_pc[5], h->d_own_in[0], h->d_own_in[1],
                   h->d_own_in[2], h->d_own_in[3], h->d_own_in[4], h->d_own_in[5], h->d_own_flag,
                   h->d_own_u0, h->d_own_v0, h->d_own_w0, h->d_dz, h->d_vmax, h->d_inv, h->d_val,
@@ -749,6 +842,11 @@ qesb_status qesb_create(const qesb_grid *grid, float tol, int device, qesb_handl
   TRY(dalloc(&h->d_R, np));
   TRY(dalloc(&h->d_mask, np));
   for (int q = 0; q < 6; ++q) TRY(dalloc(&h->d_pc[q], np));
+  h->S.PQ = ((G.X + 1) / 2 + 31) / 32 * 32;
+  h->S.CS = (long)h->S.PQ * G.Y * G.Z;
+  TRY(dalloc(&h->d_lam_s, 2 * h->S.CS));
+  TRY(dalloc(&h->d_R_s, 2 * h->S.CS));
+  TRY(dalloc(&h->d_mask_s, 2 * h->S.CS));
   TRY(dalloc(&h->d_dz, G.Z));
   TRY(dalloc(&h->d_vmax, 6 * G.Z));
   TRY(dalloc(&h->d_inv, 64 * G.Z));
@@ -763,6 +861,10 @@ qesb_status qesb_create(const qesb_grid *grid, float tol, int device, qesb_handl
   for (void *p : {(void *)h->d_lam, (void *)h->d_lam2, (void *)h->d_R})
     if (cudaMemset(p, 0, np * sizeof(float)) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaMemset failed"));
   if (cudaMemset(h->d_mask, 0, np) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaMemset failed"));
+  if (cudaMemset(h->d_lam_s, 0, 2 * h->S.CS * sizeof(float)) != cudaSuccess ||
+      cudaMemset(h->d_R_s, 0, 2 * h->S.CS * sizeof(float)) != cudaSuccess ||
+      cudaMemset(h->d_mask_s, 0, 2 * h->S.CS) != cudaSuccess)
+    return fail(qesb_fail(QESB_ERR_CUDA, "cudaMemset failed"));
   for (int q = 0; q < 6; ++q)
     if (cudaMemset(h->d_pc[q], 0, np * sizeof(float)) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaMemset failed"));
   if (cudaMemcpy(h->d_dz, h->dz.data(), sizeof(float) * G.Z, cudaMemcpyHostToDevice) != cudaSuccess)
@@ -948,6 +1050,27 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
   if (!h || n <= 0 || !ms) return qesb_fail(QESB_ERR_ARG, "qesb_time_sweeps: bad argument");
   if (!h->have_inputs || !h->packed) return qesb_fail(QESB_ERR_STATE, "qesb_time_sweeps needs stair-step inputs");
   CK(cudaSetDevice(h->device));
+  if (pick_variant(h) == kSplitVariant) {
+    CKS(ensure_err(h, n + 1));
+    cudaStream_t s = h->stream;
+    CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+    const int nrows = (h->G.Y - 2) * (h->G.Z - 2);
+    const dim3 grid((nrows + kSplitRPB - 1) / kSplitRPB), block(32, kSplitRPB);
+    const SplitArgs a = split_args(h, 1 << 30);
+    SplitArgs never = a;
+    never.tol = -1.0;  // no stop: every launch runs
+    CK(cudaEventRecord(h->ev[0], s));
+    for (int c = 0; c < n; ++c) {
+      k_sor_split<0, kSplitRPB><<<grid, block, 0, s>>>(never);
+      k_sor_split<1, kSplitRPB><<<grid, block, 0, s>>>(never);
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->ev[1], s));
+    CK(cudaEventSynchronize(h->ev[1]));
+    CK(cudaEventElapsedTime(ms, h->ev[0], h->ev[1]));
+    if (k) *k = 1;
+    return QESB_OK;
+  }
   const Variant &v = kVariants[pick_variant(h)];
   CKS(set_smem_attr(v));
   CKS(ensure_err(h, v.K));
@@ -987,7 +1110,7 @@ qesb_status qesb_set_option(qesb_handle *h, const char *key, int value)
   } else if (k == "graph") {
     h->opt_graph = value ? 1 : 0;
   } else if (k == "variant") {
-    if (value < -1 || value >= kNumVariants) return qesb_fail(QESB_ERR_ARG, "variant must be in [-1, %d)", kNumVariants);
+    if (value < -1 || value > kSplitVariant) return qesb_fail(QESB_ERR_ARG, "variant must be in [-1, %d]", kSplitVariant);
     h->opt_variant = value;
   } else {
     return qesb_fail(QESB_ERR_ARG, "unknown option '%s'", key);

@@ -1,0 +1,192 @@
+// Red/black split-layout SOR half-sweeps (the packed path's streaming kernels).
+// Included by qesb_solver.cu, so compiled with -fmad=false: each update rounds
+// exactly as Solver_CPU_RB.cpp:118-125 does.
+//
+// Layout. Each cell field of the sweep (lambda, R, wall mask) is stored as two
+// colour arrays. Colour c = (i + j + k) % 2 holds, for every row (j, k), the
+// cells of that colour in x order: cell (i, j, k) sits at
+//     sidx(c, i >> 1, j, k) = c*CS + (k*Y + j)*PQ + (i >> 1),
+// PQ = roundup((X + 1) / 2, 32) (128-byte rows), CS = PQ*Y*Z. A half-sweep
+// of colour c reads its own cells and the other colour's six neighbours:
+//     x-1 -> (1-c, q - 1 + i0, j, k),  x+1 -> (1-c, q + i0, j, k),
+//     y+-1 -> (1-c, q, j+-1, k),       z+-1 -> (1-c, q, j, k+-1),
+// with i0 = (c + j + k) & 1 the x parity of the row's colour-c cells. A warp
+// therefore loads 32 consecutive words for every operand, and each byte of
+// the other colour is fetched from DRAM about once per half-sweep.
+//
+// Iteration = red kernel (colour 0) + black kernel (colour 1). The black
+// kernel also applies the ground mirror lambda(k=0) <- lambda(k=1) to interior
+// rows (Solver_CPU_RB.cpp:155-162), and its last CTA to finish runs the
+// convergence poll, so one iteration is two launches and no host round trip.
+#pragma once
+#include "qesb_device.cuh"
+
+namespace qesb {
+
+struct SplitGeom {
+  int PQ;    // padded half-row length
+  long CS;   // elements per colour array
+  __host__ __device__ long row(int j, int k, int Y) const { return ((long)k * Y + j) * PQ; }
+};
+
+struct SplitArgs {
+  DevGrid G;
+  SplitGeom S;
+  float *lam;           // [2][CS]
+  const float *R;       // [2][CS]
+  const uint8_t *mask;  // [2][CS]
+  const float *val;     // [6][Z]
+  const float *inv;     // [Z][64]
+  double *err;
+  SolveState *st;
+  int itermax;
+  double tol;
+};
+
+// Convergence poll for the iteration st->it (see k_poll in qesb_solver.cu for
+// the loop condition); run by one thread once every CTA's error is in.
+__device__ __forceinline__ void poll_one(SolveState *st, const double *err, double tol, int itermax)
+{
+  const int it = st->it;
+  const double e = err[it];
+  st->residual = e;
+  st->it = it + 1;
+  st->cur = 0;
+  if (isnan(e)) {
+    st->done = 1;
+    st->nan = 1;
+  } else if (!(e > tol)) {
+    st->done = 1;
+    st->converged = 1;
+  } else if (it + 1 >= itermax) {
+    st->done = 1;
+  }
+}
+
+// One colour of the sweep over rows j in [1, Y-2], k in [1, Z-2]. Block =
+// (32, RPB) threads: threadIdx.y picks the row, x-warps stride along it.
+template <int COLOUR, int RPB>
+__global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
+{
+  SolveState *S = a.st;
+  if (S->done) return;
+  const DevGrid &G = a.G;
+  const int nrows = (G.Y - 2) * (G.Z - 2);
+  const int r = blockIdx.x * RPB + threadIdx.y;
+  double dmax = 0.0;
+  const int it = S->it;
+  if (r < nrows) {
+    const int k = 1 + r / (G.Y - 2), j = 1 + r % (G.Y - 2);
+    const int i0 = (COLOUR + j + k) & 1;
+    const long own = COLOUR * a.S.CS + a.S.row(j, k, G.Y);
+    const long oth = (1 - COLOUR) * a.S.CS + a.S.row(j, k, G.Y);
+    const long oYm = oth - a.S.PQ, oYp = oth + a.S.PQ;
+    const long oZm = oth - (long)G.Y * a.S.PQ, oZp = oth + (long)G.Y * a.S.PQ;
+    const float ve = a.val[0 * G.Z + k], vf = a.val[1 * G.Z + k], vg = a.val[2 * G.Z + k];
+    const float vh = a.val[3 * G.Z + k], vm = a.val[4 * G.Z + k], vn = a.val[5 * G.Z + k];
+    const float *inv = a.inv + k * 64;
+    float *L = a.lam;
+    // updated cells of this row: i in [1, X-2], i = i0 + 2q
+    const int qlo = i0 ? 0 : 1;
+    const int qhi = (G.X - 2 - i0) >> 1;  // inclusive
+    for (int q = qlo + threadIdx.x; q <= qhi; q += 32) {
+      const float old = L[own + q];
+      const float lxm = L[oth + q - 1 + i0];
+      const float lxp = L[oth + q + i0];
+      const float lym = L[oYm + q], lyp = L[oYp + q];
+      const float lzm = L[oZm + q], lzp = L[oZp + q];
+      const unsigned mk = a.mask[own + q];
+      const float rr = a.R[own + q];
+      const float e = (mk & 1u) ? ve : 0.0f, f = (mk & 2u) ? vf : 0.0f;
+      const float g = (mk & 4u) ? vg : 0.0f, hh = (mk & 8u) ? vh : 0.0f;
+      const float m = (mk & 16u) ? vm : 0.0f, n = (mk & 32u) ? vn : 0.0f;
+      const float nv = __ldg(inv + mk) * (e * lxp + f * lxm + g * lyp + hh * lym + m * lzp + n * lzm - rr) +
+                       (1.0f - kOmega) * old;
+      L[own + q] = nv;
+      const double d = fabs((double)nv - (double)old);
+      if (d > dmax || d != d) dmax = d;
+    }
+    if (COLOUR == 1 && k == 1) {
+      __syncwarp();  // one warp owns the row: its black updates land before the copies
+      // ground mirror of this row, both colours: (i, j, 0) <- (i, j, 1); the
+      // plane-0 cell of colour c mirrors the plane-1 cell of colour 1-c at
+      // the same q. This thread wrote or owns the black values it copies;
+      // the red plane-1 values are read-only during this kernel.
+      const long b1 = 1 * a.S.CS + a.S.row(j, 1, G.Y), r0 = 0 * a.S.CS + a.S.row(j, 0, G.Y);
+      const long r1 = 0 * a.S.CS + a.S.row(j, 1, G.Y), b0 = 1 * a.S.CS + a.S.row(j, 0, G.Y);
+      const int qn = (G.X + 1) >> 1;
+      for (int q = threadIdx.x; q < qn; q += 32) {
+        L[r0 + q] = L[b1 + q];
+        L[b0 + q] = L[r1 + q];
+      }
+    }
+  }
+  // block max -> err[it], then (black) last-CTA poll
+  __shared__ double s_part[RPB];
+  __shared__ bool s_last;
+  double v = warp_max_d(dmax);
+  if (threadIdx.x == 0) s_part[threadIdx.y] = v;
+  __syncthreads();
+  if (threadIdx.y == 0) {
+    double x = threadIdx.x < RPB ? s_part[threadIdx.x] : 0.0;
+    x = warp_max_d(x);
+    if (threadIdx.x == 0) {
+      if (x != 0.0) atomic_max_nonneg(a.err + it, x);
+      if (COLOUR == 1) {
+        __threadfence();
+        const unsigned t = atomicAdd(&S->blocks_done, 1u);
+        s_last = (t == gridDim.x - 1);
+      }
+    }
+  }
+  if (COLOUR == 1) {
+    __syncthreads();
+    if (s_last && threadIdx.x == 0 && threadIdx.y == 0) {
+      __threadfence();
+      S->blocks_done = 0;
+      poll_one(S, a.err, a.tol, a.itermax);
+    }
+  }
+}
+
+// Plane-0 boundary ring (j = 0, Y-1 rows; i = 0, X-1 columns) <- plane 1.
+// Those plane-0 cells are read by no update (their plane-1 partners are
+// boundary cells, never updated, whose values never change), so mirroring them
+// once after the iterations leaves the same field as mirroring every iteration.
+__global__ void k_split_mirror_ring(DevGrid G, SplitGeom S, float *lam)
+{
+  const int j = blockIdx.x;
+  const bool edge_row = (j == 0 || j == G.Y - 1);
+  const int qn = (G.X + 1) >> 1;
+  for (int c = 0; c < 2; ++c) {
+    const long dst = c * S.CS + S.row(j, 0, G.Y), src = (1 - c) * S.CS + S.row(j, 1, G.Y);
+    for (int q = threadIdx.x; q < qn; q += blockDim.x) {
+      // x of this plane-0 cell: row (j, 0) of colour c has i0 = (c + j) & 1
+      const int i = 2 * q + ((c + j) & 1);
+      if (i >= G.X) continue;
+      if (edge_row || i == 0 || i == G.X - 1) lam[dst + q] = lam[src + q];
+    }
+  }
+}
+
+// Padded natural layout <-> split layout (one thread per cell).
+__global__ void k_pad_to_split(DevGrid G, SplitGeom S, const float *__restrict__ src, float *__restrict__ dst)
+{
+  const int j = blockIdx.y, k = blockIdx.z;
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < G.X; i += gridDim.x * blockDim.x)
+    dst[((i + j + k) & 1) * S.CS + S.row(j, k, G.Y) + (i >> 1)] = src[G.pad(i, j, k)];
+}
+__global__ void k_split_to_pad(DevGrid G, SplitGeom S, const float *__restrict__ src, float *__restrict__ dst)
+{
+  const int j = blockIdx.y, k = blockIdx.z;
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < G.X; i += gridDim.x * blockDim.x)
+    dst[G.pad(i, j, k)] = src[((i + j + k) & 1) * S.CS + S.row(j, k, G.Y) + (i >> 1)];
+}
+__global__ void k_pad_to_split_u8(DevGrid G, SplitGeom S, const uint8_t *__restrict__ src, uint8_t *__restrict__ dst)
+{
+  const int j = blockIdx.y, k = blockIdx.z;
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < G.X; i += gridDim.x * blockDim.x)
+    dst[((i + j + k) & 1) * S.CS + S.row(j, k, G.Y) + (i >> 1)] = src[G.pad(i, j, k)];
+}
+
+}  // namespace qesb

@@ -51,14 +51,15 @@ def test_divergence_R_bit_exact(golden):
     np.testing.assert_array_equal(R, O.divergence(d, w))
 
 
-N_VARIANTS = 5
+N_VARIANTS = 6  # five fused tile shapes + the streaming red/black split path (index 5)
 
 
 @pytest.mark.parametrize("variant", range(N_VARIANTS))
 def test_fused_sweeps_bit_exact(variant):
-    """Every tile variant of the fused kernel (K = 1 and 2 iterations per
-    launch, several tile shapes), an odd iteration count (a partial last
-    launch), ragged tiles at the domain edges and a random warm start."""
+    """Every sweep variant (the fused kernel's tile shapes with K = 1 and 2
+    iterations per launch, and the streaming split path), an odd iteration
+    count (a partial last fused launch), ragged tiles at the domain edges and a
+    random warm start."""
     d = qesb.Domain(70, 45, 21, 2.0, 2.0, 1.0, qesb.city_dz(21, 1.0, 1.03))
     c = qesb.city_random(d, 9, 8, fp=(6, 18), h=(4, 30))
     w = qesb.city_build(d, c.buildings, c.inflow)
@@ -73,7 +74,7 @@ def test_fused_sweeps_bit_exact(variant):
     np.testing.assert_array_equal(ww, wo)
 
 
-@pytest.mark.parametrize("path,variant", [(0, -1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("path,variant", [(0, -1), (1, 0), (1, 1), (1, 5)])
 @pytest.mark.parametrize("tol", [2e-3, 1.1e-3, 7e-4])
 def test_stopping_rule_matches_oracle(golden, path, variant, tol):
     """A reachable tolerance: the loop stops on the same iteration as the
@@ -173,18 +174,21 @@ def test_graph_and_plain_launches_agree(golden, graph):
     np.testing.assert_array_equal(L, Lo)
 
 
-def test_full_size_city400_packed_equals_full_path():
-    """400x400x100 stretched city: after 24 iterations the fused packed path and
-    the full-coefficient path hold the same lambda bits, and the fused path's
-    residual history equals the full path's."""
+@pytest.mark.parametrize("variant", [1, 5])
+def test_full_size_city400_packed_equals_full_path(variant):
+    """400x400x100 stretched city: after 24 iterations the packed paths (fused
+    and split) and the full-coefficient path hold the same lambda bits and the
+    same residual history."""
     w, c = qesb.random_city("city400", 0)
     d = w.domain
     out = {}
     for path in (0, 1):
         with qesb.Solver_B200(d, 1e-9) as s:
             s.set_option("path", path)
+            s.set_option("variant", variant)
             st = s.solve(w, 24)
-            out[path] = (s.lambda_, s.residual_history(24), st)
+            out[path] = (s.lambda_, s.residual_history(24), st, w.u.copy())
     np.testing.assert_array_equal(out[0][0], out[1][0])
     np.testing.assert_array_equal(out[0][1], out[1][1])
+    np.testing.assert_array_equal(out[0][3], out[1][3])
     assert out[1][2]["path"] == 1 and out[0][2]["path"] == 0

@@ -635,8 +635,24 @@ qesb_status run_iterations_tiled(qesb_handle *h, const Variant &v, int itermax)
   return QESB_OK;
 }
 
-constexpr int kSplitRPB = 8;  // rows (warps) per CTA of the split half-sweeps
-constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the split path
+// Split-path launch shapes: rows (warps) per CTA and cells batched per lane.
+struct SplitVariant {
+  const char *name;
+  int rpb, unroll;
+  void (*red)(SplitArgs);
+  void (*black)(SplitArgs);
+};
+template <int RPB, int U>
+constexpr SplitVariant make_split(const char *name)
+{
+  return SplitVariant{name, RPB, U, k_sor_split<0, RPB, U>, k_sor_split<1, RPB, U>};
+}
+const SplitVariant kSplitVariants[] = {
+    make_split<8, 4>("split_r8_u4"), make_split<8, 1>("split_r8_u1"), make_split<8, 2>("split_r8_u2"),
+    make_split<4, 8>("split_r4_u8"), make_split<16, 2>("split_r16_u2"), make_split<4, 4>("split_r4_u4"),
+};
+constexpr int kNumSplit = sizeof(kSplitVariants) / sizeof(kSplitVariants[0]);
+constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the first split shape
 
 SplitArgs split_args(qesb_handle *h, int itermax)
 {
@@ -655,14 +671,14 @@ SplitArgs split_args(qesb_handle *h, int itermax)
   return a;
 }
 
-qesb_status enqueue_split_chunk(qesb_handle *h, int chunk, int itermax)
+qesb_status enqueue_split_chunk(qesb_handle *h, const SplitVariant &sv, int chunk, int itermax)
 {
   const int nrows = (h->G.Y - 2) * (h->G.Z - 2);
-  const dim3 grid((nrows + kSplitRPB - 1) / kSplitRPB), block(32, kSplitRPB);
+  const dim3 grid((nrows + sv.rpb - 1) / sv.rpb), block(32, sv.rpb);
   const SplitArgs a = split_args(h, itermax);
   for (int c = 0; c < chunk; ++c) {
-    k_sor_split<0, kSplitRPB><<<grid, block, 0, h->stream>>>(a);
-    k_sor_split<1, kSplitRPB><<<grid, block, 0, h->stream>>>(a);
+    sv.red<<<grid, block, 0, h->stream>>>(a);
+    sv.black<<<grid, block, 0, h->stream>>>(a);
   }
   CK(cudaGetLastError());
   return QESB_OK;
@@ -671,7 +687,7 @@ qesb_status enqueue_split_chunk(qesb_handle *h, int chunk, int itermax)
 // Red/black split path: lambda and R to the split layout, the iteration loop
 // as CUDA-graph chunks of (red, black) launches polled from the host every
 // ~2 ms of device work, then the boundary-ring mirror and lambda back.
-qesb_status run_iterations_split(qesb_handle *h, int itermax)
+qesb_status run_iterations_split(qesb_handle *h, const SplitVariant &sv, int itermax)
 {
   const DevGrid &G = h->G;
   cudaStream_t s = h->stream;
@@ -685,25 +701,26 @@ qesb_status run_iterations_split(qesb_handle *h, int itermax)
   while (launched < itermax) {
     if (h->opt_graph) {
       auto &key = h->gkey[1];
-      const bool hit = h->gexec[1] && key.variant == kSplitVariant && key.chunk == chunk &&
+      const int vid = kSplitVariant + (int)(&sv - kSplitVariants);
+      const bool hit = h->gexec[1] && key.variant == vid && key.chunk == chunk &&
                        key.tol == h->tol && key.itermax == itermax && key.stream == s;
       if (!hit) {
         if (h->gexec[1]) cudaGraphExecDestroy(h->gexec[1]);
         h->gexec[1] = nullptr;
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        qesb_status qs = enqueue_split_chunk(h, chunk, itermax);
+        qesb_status qs = enqueue_split_chunk(h, sv, chunk, itermax);
         cudaError_t ce = cudaStreamEndCapture(s, &g);
         if (qs != QESB_OK) return qs;
         if (ce != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
         ce = cudaGraphInstantiate(&h->gexec[1], g, 0);
         cudaGraphDestroy(g);
         if (ce != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
-        key = {kSplitVariant, 0, chunk, h->tol, itermax, s};
+        key = {vid, 0, chunk, h->tol, itermax, s};
       }
       CK(cudaGraphLaunch(h->gexec[1], s));
     } else {
-      CKS(enqueue_split_chunk(h, chunk, itermax));
+      CKS(enqueue_split_chunk(h, sv, chunk, itermax));
     }
     launched += chunk;
     CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
@@ -737,11 +754,11 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   CK(cudaEventRecord(h->ev[1], s));
   const bool packed = h->packed && h->opt_path == 1;
   const int vi = packed ? pick_variant(h) : -1;
-  const bool split = packed && vi == kSplitVariant;
+  const bool split = packed && vi >= kSplitVariant;
   const Variant *var = packed && !split ? &kVariants[vi] : nullptr;
   h->last_launches = 0;
   if (itermax > 0) {
-    if (split) CKS(run_iterations_split(h, itermax));
+    if (split) CKS(run_iterations_split(h, kSplitVariants[vi - kSplitVariant], itermax));
     else if (var) CKS(run_iterations_tiled(h, *var, itermax));
     else CKS(run_iterations_full(h, itermax));
   }
@@ -1050,19 +1067,20 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
   if (!h || n <= 0 || !ms) return qesb_fail(QESB_ERR_ARG, "qesb_time_sweeps: bad argument");
   if (!h->have_inputs || !h->packed) return qesb_fail(QESB_ERR_STATE, "qesb_time_sweeps needs stair-step inputs");
   CK(cudaSetDevice(h->device));
-  if (pick_variant(h) == kSplitVariant) {
+  if (pick_variant(h) >= kSplitVariant) {
+    const SplitVariant &sv = kSplitVariants[pick_variant(h) - kSplitVariant];
     CKS(ensure_err(h, n + 1));
     cudaStream_t s = h->stream;
     CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
     const int nrows = (h->G.Y - 2) * (h->G.Z - 2);
-    const dim3 grid((nrows + kSplitRPB - 1) / kSplitRPB), block(32, kSplitRPB);
+    const dim3 grid((nrows + sv.rpb - 1) / sv.rpb), block(32, sv.rpb);
     const SplitArgs a = split_args(h, 1 << 30);
     SplitArgs never = a;
     never.tol = -1.0;  // no stop: every launch runs
     CK(cudaEventRecord(h->ev[0], s));
     for (int c = 0; c < n; ++c) {
-      k_sor_split<0, kSplitRPB><<<grid, block, 0, s>>>(never);
-      k_sor_split<1, kSplitRPB><<<grid, block, 0, s>>>(never);
+      sv.red<<<grid, block, 0, s>>>(never);
+      sv.black<<<grid, block, 0, s>>>(never);
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(h->ev[1], s));
@@ -1110,7 +1128,8 @@ qesb_status qesb_set_option(qesb_handle *h, const char *key, int value)
   } else if (k == "graph") {
     h->opt_graph = value ? 1 : 0;
   } else if (k == "variant") {
-    if (value < -1 || value > kSplitVariant) return qesb_fail(QESB_ERR_ARG, "variant must be in [-1, %d]", kSplitVariant);
+    if (value < -1 || value >= kSplitVariant + kNumSplit)
+      return qesb_fail(QESB_ERR_ARG, "variant must be in [-1, %d)", kSplitVariant + kNumSplit);
     h->opt_variant = value;
   } else {
     return qesb_fail(QESB_ERR_ARG, "unknown option '%s'", key);

@@ -65,7 +65,7 @@ __device__ __forceinline__ void poll_one(SolveState *st, const double *err, doub
 
 // One colour of the sweep over rows j in [1, Y-2], k in [1, Z-2]. Block =
 // (32, RPB) threads: threadIdx.y picks the row, x-warps stride along it.
-template <int COLOUR, int RPB>
+template <int COLOUR, int RPB, int U>
 __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
 {
   SolveState *S = a.st;
@@ -86,25 +86,44 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
     const float vh = a.val[3 * G.Z + k], vm = a.val[4 * G.Z + k], vn = a.val[5 * G.Z + k];
     const float *inv = a.inv + k * 64;
     float *L = a.lam;
-    // updated cells of this row: i in [1, X-2], i = i0 + 2q
+    // updated cells of this row: i in [1, X-2], i = i0 + 2q. Other-colour
+    // lambda, R and the mask are read through the read-only path: during this
+    // half-sweep no thread writes them, except the ground-mirror copies below,
+    // which a warp makes only after its own reads of those cells.
     const int qlo = i0 ? 0 : 1;
     const int qhi = (G.X - 2 - i0) >> 1;  // inclusive
-    for (int q = qlo + threadIdx.x; q <= qhi; q += 32) {
-      const float old = L[own + q];
-      const float lxm = L[oth + q - 1 + i0];
-      const float lxp = L[oth + q + i0];
-      const float lym = L[oYm + q], lyp = L[oYp + q];
-      const float lzm = L[oZm + q], lzp = L[oZp + q];
-      const unsigned mk = a.mask[own + q];
-      const float rr = a.R[own + q];
-      const float e = (mk & 1u) ? ve : 0.0f, f = (mk & 2u) ? vf : 0.0f;
-      const float g = (mk & 4u) ? vg : 0.0f, hh = (mk & 8u) ? vh : 0.0f;
-      const float m = (mk & 16u) ? vm : 0.0f, n = (mk & 32u) ? vn : 0.0f;
-      const float nv = __ldg(inv + mk) * (e * lxp + f * lxm + g * lyp + hh * lym + m * lzp + n * lzm - rr) +
-                       (1.0f - kOmega) * old;
-      L[own + q] = nv;
-      const double d = fabs((double)nv - (double)old);
-      if (d > dmax || d != d) dmax = d;
+    for (int q0 = qlo + threadIdx.x; q0 <= qhi; q0 += 32 * U) {
+      float old[U], lxm[U], lxp[U], lym[U], lyp[U], lzm[U], lzp[U], rr[U];
+      unsigned mk[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int q = min(q0 + 32 * u, qhi);  // clamped: out-of-row lanes recompute the last cell, no store
+        old[u] = L[own + q];
+        lxm[u] = __ldg(L + oth + q - 1 + i0);
+        lxp[u] = __ldg(L + oth + q + i0);
+        lym[u] = __ldg(L + oYm + q);
+        lyp[u] = __ldg(L + oYp + q);
+        lzm[u] = __ldg(L + oZm + q);
+        lzp[u] = __ldg(L + oZp + q);
+        mk[u] = __ldg(a.mask + own + q);
+        rr[u] = __ldg(a.R + own + q);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int q = q0 + 32 * u;
+        const unsigned m_ = mk[u];
+        const float e = (m_ & 1u) ? ve : 0.0f, f = (m_ & 2u) ? vf : 0.0f;
+        const float g = (m_ & 4u) ? vg : 0.0f, hh = (m_ & 8u) ? vh : 0.0f;
+        const float m = (m_ & 16u) ? vm : 0.0f, n = (m_ & 32u) ? vn : 0.0f;
+        const float nv = __ldg(inv + m_) *
+                             (e * lxp[u] + f * lxm[u] + g * lyp[u] + hh * lym[u] + m * lzp[u] + n * lzm[u] - rr[u]) +
+                         (1.0f - kOmega) * old[u];
+        if (q <= qhi) {
+          L[own + q] = nv;
+          const double d = fabs((double)nv - (double)old[u]);
+          if (d > dmax || d != d) dmax = d;
+        }
+      }
     }
     if (COLOUR == 1 && k == 1) {
       __syncwarp();  // one warp owns the row: its black updates land before the copies

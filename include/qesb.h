@@ -118,11 +118,22 @@ qesb_status qesb_get_residual_history(qesb_handle *h, double *out, int n);
  * meant for measuring the kernel alone. Requires stair-step inputs. */
 qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k);
 
+/* Autotuner: times every sweep variant (fused tile shapes and split launch
+ * shapes) for a few launches on this handle's inputs and keeps the fastest
+ * for the handle's grid; the choice is cached for the process per grid shape
+ * and used by later solves whose "variant" option is -1. lambda is restored
+ * afterwards. us_per_iter (nullable, n_variants entries) receives each
+ * variant's time per iteration; *best the chosen index. Needs stair-step
+ * inputs (the full-coefficient path has a single variant). */
+qesb_status qesb_autotune(qesb_handle *h, int *best, float *us_per_iter, int n_variants);
+int qesb_num_variants(void);
+
 /* Tolerance (Solver::tol) and tuning knobs. Keys:
  *   "sweeps_per_launch"  iterations fused per sweep launch (0 = autotuned)
  *   "path"               0 = force full coefficients, 1 = allow the packed mask (default)
  *   "graph"              1 = run the iteration loop as a CUDA graph (default), 0 = plain launches
- *   "variant"            fused-kernel tile variant index (-1 = automatic) */
+ *   "variant"            sweep variant index (-1 = autotuned / default), see qesb_num_variants
+ *   "autotune"           1 = run qesb_autotune at the first solve of an untuned grid shape (default 0) */
 qesb_status qesb_set_tolerance(qesb_handle *h, float tol);
 qesb_status qesb_set_option(qesb_handle *h, const char *key, int value);
 /* cudaStream_t to run on (NULL = the handle's own stream). */

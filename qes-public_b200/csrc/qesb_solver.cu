@@ -28,7 +28,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "qesb.h"
@@ -368,6 +371,7 @@ struct qesb_handle {
   int opt_k = 0;
   int opt_graph = 1;
   int opt_variant = -1;
+  int opt_autotune = 0;
   int last_launches = 0;
 
   // red/black split layout (packed streaming path)
@@ -531,6 +535,7 @@ qesb_status run_iterations_full(qesb_handle *h, int itermax)
 // Picks the tiled-kernel variant: the caller's sweeps_per_launch if set,
 // else the autotuned choice for this grid (see autotune()).
 int pick_variant(qesb_handle *h);
+int tuned_variant(const DevGrid &G);
 
 TiledArgs tiled_args(qesb_handle *h, const float *in, float *out, int itermax, int redo)
 {
@@ -753,6 +758,10 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
   CK(cudaEventRecord(h->ev[1], s));
   const bool packed = h->packed && h->opt_path == 1;
+  if (packed && h->opt_autotune && h->opt_variant < 0 && tuned_variant(G) < 0) {
+    CKS(qesb_autotune(h, nullptr, nullptr, 0));
+    CK(cudaEventRecord(h->ev[1], s));
+  }
   const int vi = packed ? pick_variant(h) : -1;
   const bool split = packed && vi >= kSplitVariant;
   const Variant *var = packed && !split ? &kVariants[vi] : nullptr;
@@ -787,10 +796,23 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   return QESB_OK;
 }
 
+// Process-wide autotuner choices, per grid shape.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, int> g_tuned;
+
+int tuned_variant(const DevGrid &G)
+{
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tuned.find({G.X, G.Y, G.Z});
+  return it == g_tuned.end() ? -1 : it->second;
+}
+
 int pick_variant(qesb_handle *h)
 {
   if (h->opt_variant >= 0) return h->opt_variant;
   if (h->opt_k == 2) return 1;  // fused: K = 2, 64 x 32 tiles
+  const int t = tuned_variant(h->G);
+  if (t >= 0) return t;
   return kSplitVariant;         // streaming red/black split half-sweeps
 }
 
@@ -1108,6 +1130,54 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
   return QESB_OK;
 }
 
+int qesb_num_variants(void) { return kSplitVariant + kNumSplit; }
+
+qesb_status qesb_autotune(qesb_handle *h, int *best, float *us_per_iter, int n_variants)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  if (!h->have_inputs || !h->packed) return qesb_fail(QESB_ERR_STATE, "qesb_autotune needs stair-step inputs");
+  CK(cudaSetDevice(h->device));
+  const int nv = kSplitVariant + kNumSplit;
+  const size_t np = pad_alloc(h->G);
+  float *saved = nullptr;
+  CKS(dalloc(&saved, np));
+  cudaStream_t s = h->stream;
+  CK(cudaMemcpyAsync(saved, h->d_lam, np * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  const int keep = h->opt_variant;
+  int arg = -1;
+  float best_us = 0.0f;
+  qesb_status st = QESB_OK;
+  for (int v = 0; v < nv && st == QESB_OK; ++v) {
+    h->opt_variant = v;
+    float ms = 0.0f;
+    int k = 1;
+    st = qesb_time_sweeps(h, 2, &ms, &k);  // warm-up
+    if (st != QESB_OK) break;
+    st = qesb_time_sweeps(h, 2, &ms, &k);
+    if (st != QESB_OK) break;
+    const int n = std::max(2, std::min(64, (int)(8.0f / std::max(ms / 2, 1e-3f))));
+    st = qesb_time_sweeps(h, n, &ms, &k);
+    if (st != QESB_OK) break;
+    const float us = 1000.0f * ms / (n * k);
+    if (us_per_iter && v < n_variants) us_per_iter[v] = us;
+    if (arg < 0 || us < best_us) {
+      arg = v;
+      best_us = us;
+    }
+  }
+  h->opt_variant = keep;
+  cudaMemcpyAsync(h->d_lam, saved, np * sizeof(float), cudaMemcpyDeviceToDevice, s);
+  cudaStreamSynchronize(s);
+  cudaFree(saved);
+  if (st != QESB_OK) return st;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[{h->G.X, h->G.Y, h->G.Z}] = arg;
+  }
+  if (best) *best = arg;
+  return QESB_OK;
+}
+
 qesb_status qesb_set_tolerance(qesb_handle *h, float tol)
 {
   if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
@@ -1127,6 +1197,8 @@ qesb_status qesb_set_option(qesb_handle *h, const char *key, int value)
     h->opt_path = value;
   } else if (k == "graph") {
     h->opt_graph = value ? 1 : 0;
+  } else if (k == "autotune") {
+    h->opt_autotune = value ? 1 : 0;
   } else if (k == "variant") {
     if (value < -1 || value >= kSplitVariant + kNumSplit)
       return qesb_fail(QESB_ERR_ARG, "variant must be in [-1, %d)", kSplitVariant + kNumSplit);

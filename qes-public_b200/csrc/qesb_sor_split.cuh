@@ -86,44 +86,74 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
     const float vh = a.val[3 * G.Z + k], vm = a.val[4 * G.Z + k], vn = a.val[5 * G.Z + k];
     const float *inv = a.inv + k * 64;
     float *L = a.lam;
-    // updated cells of this row: i in [1, X-2], i = i0 + 2q. Other-colour
-    // lambda, R and the mask are read through the read-only path: during this
-    // half-sweep no thread writes them, except the ground-mirror copies below,
+    // Updated cells of this row: i in [1, X-2], i = i0 + 2q. Other-colour
+    // lambda, R and the mask go through the read-only path: no thread writes
+    // them during this half-sweep, except the ground-mirror copies below,
     // which a warp makes only after its own reads of those cells.
     const int qlo = i0 ? 0 : 1;
     const int qhi = (G.X - 2 - i0) >> 1;  // inclusive
-    for (int q0 = qlo + threadIdx.x; q0 <= qhi; q0 += 32 * U) {
-      float old[U], lxm[U], lxp[U], lym[U], lyp[U], lzm[U], lzp[U], rr[U];
+    float *__restrict__ pw = L + own;
+    const float *__restrict__ pxm = L + oth + i0 - 1;
+    const float *__restrict__ pxp = L + oth + i0;
+    const float *__restrict__ pym = L + oYm;
+    const float *__restrict__ pyp = L + oYp;
+    const float *__restrict__ pzm = L + oZm;
+    const float *__restrict__ pzp = L + oZp;
+    const float *__restrict__ pr = a.R + own;
+    const uint8_t *__restrict__ pm = a.mask + own;
+    const float inv63 = __ldg(inv + 63);
+    const float c1 = 1.0f - kOmega;
+    auto update = [&](float old, float xm, float xp, float ym, float yp, float zm, float zp, float rr,
+                      unsigned m_, bool full) -> float {
+      if (full) {
+        return inv63 * (ve * xp + vf * xm + vg * yp + vh * ym + vm * zp + vn * zm - rr) + c1 * old;
+      }
+      const float e = (m_ & 1u) ? ve : 0.0f, f = (m_ & 2u) ? vf : 0.0f;
+      const float g = (m_ & 4u) ? vg : 0.0f, hh = (m_ & 8u) ? vh : 0.0f;
+      const float m = (m_ & 16u) ? vm : 0.0f, n = (m_ & 32u) ? vn : 0.0f;
+      return __ldg(inv + m_) * (e * xp + f * xm + g * yp + hh * ym + m * zp + n * zm - rr) + c1 * old;
+    };
+    int q0 = qlo + threadIdx.x;
+    // main loop, warp-uniform: U cells per lane while every lane's U cells lie
+    // inside the row (no clamps, so a stream's U loads share one address with
+    // immediate offsets)
+    const int lane_off = 31 - (int)threadIdx.x;  // q0 + lane_off = the warp's last lane
+    for (; q0 + lane_off + 32 * (U - 1) <= qhi; q0 += 32 * U) {
+      float old[U], xm[U], xp[U], ym[U], yp[U], zm[U], zp[U], rr[U];
       unsigned mk[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int q = min(q0 + 32 * u, qhi);  // clamped: out-of-row lanes recompute the last cell, no store
-        old[u] = L[own + q];
-        lxm[u] = __ldg(L + oth + q - 1 + i0);
-        lxp[u] = __ldg(L + oth + q + i0);
-        lym[u] = __ldg(L + oYm + q);
-        lyp[u] = __ldg(L + oYp + q);
-        lzm[u] = __ldg(L + oZm + q);
-        lzp[u] = __ldg(L + oZp + q);
-        mk[u] = __ldg(a.mask + own + q);
-        rr[u] = __ldg(a.R + own + q);
+        const int q = q0 + 32 * u;
+        old[u] = pw[q];
+        xm[u] = __ldg(pxm + q);
+        xp[u] = __ldg(pxp + q);
+        ym[u] = __ldg(pym + q);
+        yp[u] = __ldg(pyp + q);
+        zm[u] = __ldg(pzm + q);
+        zp[u] = __ldg(pzp + q);
+        rr[u] = __ldg(pr + q);
+        mk[u] = __ldg(pm + q);
       }
+      bool full = true;
+#pragma unroll
+      for (int u = 0; u < U; ++u) full &= (mk[u] == 63u);
+      full = __all_sync(0xffffffffu, full);
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int q = q0 + 32 * u;
-        const unsigned m_ = mk[u];
-        const float e = (m_ & 1u) ? ve : 0.0f, f = (m_ & 2u) ? vf : 0.0f;
-        const float g = (m_ & 4u) ? vg : 0.0f, hh = (m_ & 8u) ? vh : 0.0f;
-        const float m = (m_ & 16u) ? vm : 0.0f, n = (m_ & 32u) ? vn : 0.0f;
-        const float nv = __ldg(inv + m_) *
-                             (e * lxp[u] + f * lxm[u] + g * lyp[u] + hh * lym[u] + m * lzp[u] + n * lzm[u] - rr[u]) +
-                         (1.0f - kOmega) * old[u];
-        if (q <= qhi) {
-          L[own + q] = nv;
-          const double d = fabs((double)nv - (double)old[u]);
-          if (d > dmax || d != d) dmax = d;
-        }
+        const float nv = update(old[u], xm[u], xp[u], ym[u], yp[u], zm[u], zp[u], rr[u], mk[u], full);
+        pw[q0 + 32 * u] = nv;
+        const double d = fabs((double)nv - (double)old[u]);
+        if (d > dmax || d != d) dmax = d;
       }
+    }
+    // tail: the row's last cells, one per lane
+    for (; q0 <= qhi; q0 += 32) {
+      const float old = pw[q0];
+      const float nv = update(old, __ldg(pxm + q0), __ldg(pxp + q0), __ldg(pym + q0), __ldg(pyp + q0),
+                              __ldg(pzm + q0), __ldg(pzp + q0), __ldg(pr + q0), __ldg(pm + q0), false);
+      pw[q0] = nv;
+      const double d = fabs((double)nv - (double)old);
+      if (d > dmax || d != d) dmax = d;
     }
     if (COLOUR == 1 && k == 1) {
       __syncwarp();  // one warp owns the row: its black updates land before the copies

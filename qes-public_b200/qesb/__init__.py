@@ -104,6 +104,8 @@ def lib() -> C.CDLL:
             "qesb_get_residual_history": ([V, V, C.c_int], C.c_int),
             "qesb_set_tolerance": ([V, C.c_float], C.c_int),
             "qesb_time_sweeps": ([V, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)], C.c_int),
+            "qesb_autotune": ([V, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int], C.c_int),
+            "qesb_num_variants": ([], C.c_int),
             "qesb_set_option": ([V, C.c_char_p, C.c_int], C.c_int),
             "qesb_set_stream": ([V, V], C.c_int),
             "qesb_city_dz": ([C.c_int, C.c_float, C.c_float, _FP], C.c_int),
@@ -308,6 +310,15 @@ class Solver_B200:
         ms, k = C.c_float(), C.c_int()
         check(lib().qesb_time_sweeps(self._h, int(n), C.byref(ms), C.byref(k)))
         return ms.value, k.value
+
+    def autotune(self) -> tuple[int, list[float]]:
+        """Times every sweep variant on the current inputs; returns the chosen
+        index and the microseconds per iteration of each."""
+        n = lib().qesb_num_variants()
+        us = (C.c_float * n)()
+        best = C.c_int()
+        check(lib().qesb_autotune(self._h, C.byref(best), us, n))
+        return best.value, list(us)
 
     def set_stream(self, stream_ptr: int | None):
         check(lib().qesb_set_stream(self._h, stream_ptr))

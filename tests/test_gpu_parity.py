@@ -192,3 +192,19 @@ def test_full_size_city400_packed_equals_full_path(variant):
     np.testing.assert_array_equal(out[0][1], out[1][1])
     np.testing.assert_array_equal(out[0][3], out[1][3])
     assert out[1][2]["path"] == 1 and out[0][2]["path"] == 0
+
+
+def test_autotune_restores_lambda_and_results_stay_exact(golden):
+    d, w, z = golden("small_city.npz")
+    lam0 = np.random.default_rng(7).standard_normal(d.numCellCentered()).astype(np.float32)
+    with qesb.Solver_B200(d, 1e-9) as s:
+        s.set_inputs(w)
+        s.lambda_ = lam0
+        best, us = s.autotune()
+        assert 0 <= best < len(us) and all(u > 0 for u in us)
+        np.testing.assert_array_equal(s.lambda_, lam0)
+        st = s.solve(w, 150, set_inputs=False)
+        L = s.lambda_
+    Lo, it, *_ = O.sor(d, w, O.divergence(d, w), 1e-9, 150, lam=lam0)
+    assert st["iterations"] == it == 150
+    np.testing.assert_array_equal(L, Lo)

@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", type=int, default=-1, help="sweep variant for --sweeps-only (-1: autotune)")
     ap.add_argument("--sweeps-only", type=int, default=0,
                     help="profiling driver: set up the workload, run this many fused-sweep launches, exit")
     return ap.parse_args()
@@ -376,6 +377,10 @@ def run_sweeps_only(args):
     w = make_city(args.workload, 0)
     with qesb.Solver_B200(w.domain, TOL) as s:
         s.set_inputs(w)
+        if args.variant >= 0:
+            s.set_option("variant", args.variant)
+        else:
+            s.autotune()
         ms, k = s.time_sweeps(args.sweeps_only)
     print(json.dumps({"sweeps_only": args.sweeps_only, "k": k, "ms_per_launch": ms / args.sweeps_only}))
 

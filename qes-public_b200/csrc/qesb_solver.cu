@@ -647,6 +647,20 @@ struct SplitVariant {
   void (*red)(SplitArgs);
   void (*black)(SplitArgs);
 };
+
+// Persistent grid for a split variant: CTAs resident at once on this device
+// (occupancy x SMs), capped by the number of row groups.
+dim3 split_grid(const DevGrid &G, const SplitVariant &sv, int device)
+{
+  static int nsm[64] = {};
+  if (!nsm[device & 63]) cudaDeviceGetAttribute(&nsm[device & 63], cudaDevAttrMultiProcessorCount, device);
+  int per = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sv.black, 32 * sv.rpb, 0);
+  per = std::max(per, 1);
+  const int nrows = (G.Y - 2) * (G.Z - 2);
+  const int groups = (nrows + sv.rpb - 1) / sv.rpb;
+  return dim3(std::max(1, std::min(groups, per * std::max(nsm[device & 63], 1))));
+}
 template <int RPB, int U>
 constexpr SplitVariant make_split(const char *name)
 {
@@ -678,8 +692,7 @@ SplitArgs split_args(qesb_handle *h, int itermax)
 
 qesb_status enqueue_split_chunk(qesb_handle *h, const SplitVariant &sv, int chunk, int itermax)
 {
-  const int nrows = (h->G.Y - 2) * (h->G.Z - 2);
-  const dim3 grid((nrows + sv.rpb - 1) / sv.rpb), block(32, sv.rpb);
+  const dim3 grid = split_grid(h->G, sv, h->device), block(32, sv.rpb);
   const SplitArgs a = split_args(h, itermax);
   for (int c = 0; c < chunk; ++c) {
     sv.red<<<grid, block, 0, h->stream>>>(a);
@@ -1094,8 +1107,7 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
     CKS(ensure_err(h, n + 1));
     cudaStream_t s = h->stream;
     CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
-    const int nrows = (h->G.Y - 2) * (h->G.Z - 2);
-    const dim3 grid((nrows + sv.rpb - 1) / sv.rpb), block(32, sv.rpb);
+    const dim3 grid = split_grid(h->G, sv, h->device), block(32, sv.rpb);
     const SplitArgs a = split_args(h, 1 << 30);
     SplitArgs never = a;
     never.tol = -1.0;  // no stop: every launch runs

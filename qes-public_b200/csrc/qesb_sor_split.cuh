@@ -63,29 +63,35 @@ __device__ __forceinline__ void poll_one(SolveState *st, const double *err, doub
   }
 }
 
-// One colour of the sweep over rows j in [1, Y-2], k in [1, Z-2]. Block =
-// (32, RPB) threads: threadIdx.y picks the row, x-warps stride along it.
+// One colour of the sweep over rows j in [1, Y-2], k in [1, Z-2]. Persistent:
+// the grid holds as many CTAs as fit on the GPU at once; each warp walks rows
+// r = warp, warp + total_warps, ... so a warp pays the kernel's start-up
+// latency and its share of the block reduction once, not once per row, and
+// warps never wait on one another inside the row loop.
 template <int COLOUR, int RPB, int U>
 __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
 {
   SolveState *S = a.st;
   if (S->done) return;
   const DevGrid &G = a.G;
-  const int nrows = (G.Y - 2) * (G.Z - 2);
-  const int r = blockIdx.x * RPB + threadIdx.y;
-  double dmax = 0.0;
   const int it = S->it;
-  if (r < nrows) {
+  const int nrows = (G.Y - 2) * (G.Z - 2);
+  const int lane = threadIdx.x;
+  const int lane_off = 31 - lane;  // q0 + lane_off = the warp's last lane
+  const float c1 = 1.0f - kOmega;
+  float *L = a.lam;
+  double dmax = 0.0;
+  for (int r = blockIdx.x * RPB + threadIdx.y; r < nrows; r += gridDim.x * RPB) {
     const int k = 1 + r / (G.Y - 2), j = 1 + r % (G.Y - 2);
     const int i0 = (COLOUR + j + k) & 1;
     const long own = COLOUR * a.S.CS + a.S.row(j, k, G.Y);
     const long oth = (1 - COLOUR) * a.S.CS + a.S.row(j, k, G.Y);
     const long oYm = oth - a.S.PQ, oYp = oth + a.S.PQ;
     const long oZm = oth - (long)G.Y * a.S.PQ, oZp = oth + (long)G.Y * a.S.PQ;
-    const float ve = a.val[0 * G.Z + k], vf = a.val[1 * G.Z + k], vg = a.val[2 * G.Z + k];
-    const float vh = a.val[3 * G.Z + k], vm = a.val[4 * G.Z + k], vn = a.val[5 * G.Z + k];
+    const float ve = __ldg(a.val + 0 * G.Z + k), vf = __ldg(a.val + 1 * G.Z + k), vg = __ldg(a.val + 2 * G.Z + k);
+    const float vh = __ldg(a.val + 3 * G.Z + k), vm = __ldg(a.val + 4 * G.Z + k), vn = __ldg(a.val + 5 * G.Z + k);
     const float *inv = a.inv + k * 64;
-    float *L = a.lam;
+    const float inv63 = __ldg(inv + 63);
     // Updated cells of this row: i in [1, X-2], i = i0 + 2q. Other-colour
     // lambda, R and the mask go through the read-only path: no thread writes
     // them during this half-sweep, except the ground-mirror copies below,
@@ -101,8 +107,6 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
     const float *__restrict__ pzp = L + oZp;
     const float *__restrict__ pr = a.R + own;
     const uint8_t *__restrict__ pm = a.mask + own;
-    const float inv63 = __ldg(inv + 63);
-    const float c1 = 1.0f - kOmega;
     auto update = [&](float old, float xm, float xp, float ym, float yp, float zm, float zp, float rr,
                       unsigned m_, bool full) -> float {
       if (full) {
@@ -113,11 +117,10 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
       const float m = (m_ & 16u) ? vm : 0.0f, n = (m_ & 32u) ? vn : 0.0f;
       return __ldg(inv + m_) * (e * xp + f * xm + g * yp + hh * ym + m * zp + n * zm - rr) + c1 * old;
     };
-    int q0 = qlo + threadIdx.x;
+    int q0 = qlo + lane;
     // main loop, warp-uniform: U cells per lane while every lane's U cells lie
     // inside the row (no clamps, so a stream's U loads share one address with
     // immediate offsets)
-    const int lane_off = 31 - (int)threadIdx.x;  // q0 + lane_off = the warp's last lane
     for (; q0 + lane_off + 32 * (U - 1) <= qhi; q0 += 32 * U) {
       float old[U], xm[U], xp[U], ym[U], yp[U], zm[U], zp[U], rr[U];
       unsigned mk[U];
@@ -159,12 +162,12 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
       __syncwarp();  // one warp owns the row: its black updates land before the copies
       // ground mirror of this row, both colours: (i, j, 0) <- (i, j, 1); the
       // plane-0 cell of colour c mirrors the plane-1 cell of colour 1-c at
-      // the same q. This thread wrote or owns the black values it copies;
-      // the red plane-1 values are read-only during this kernel.
+      // the same q. The black plane-1 values are this warp's own; the red
+      // plane-1 values are read-only during this kernel.
       const long b1 = 1 * a.S.CS + a.S.row(j, 1, G.Y), r0 = 0 * a.S.CS + a.S.row(j, 0, G.Y);
       const long r1 = 0 * a.S.CS + a.S.row(j, 1, G.Y), b0 = 1 * a.S.CS + a.S.row(j, 0, G.Y);
       const int qn = (G.X + 1) >> 1;
-      for (int q = threadIdx.x; q < qn; q += 32) {
+      for (int q = lane; q < qn; q += 32) {
         L[r0 + q] = L[b1 + q];
         L[b0 + q] = L[r1 + q];
       }
@@ -174,12 +177,12 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
   __shared__ double s_part[RPB];
   __shared__ bool s_last;
   double v = warp_max_d(dmax);
-  if (threadIdx.x == 0) s_part[threadIdx.y] = v;
+  if (lane == 0) s_part[threadIdx.y] = v;
   __syncthreads();
   if (threadIdx.y == 0) {
-    double x = threadIdx.x < RPB ? s_part[threadIdx.x] : 0.0;
+    double x = lane < RPB ? s_part[lane] : 0.0;
     x = warp_max_d(x);
-    if (threadIdx.x == 0) {
+    if (lane == 0) {
       if (x != 0.0) atomic_max_nonneg(a.err + it, x);
       if (COLOUR == 1) {
         __threadfence();
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
   }
   if (COLOUR == 1) {
     __syncthreads();
-    if (s_last && threadIdx.x == 0 && threadIdx.y == 0) {
+    if (s_last && lane == 0 && threadIdx.y == 0) {
       __threadfence();
       S->blocks_done = 0;
       poll_one(S, a.err, a.tol, a.itermax);

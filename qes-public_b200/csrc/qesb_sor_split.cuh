@@ -149,14 +149,34 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
         if (d > dmax || d != d) dmax = d;
       }
     }
-    // tail: the row's last cells, one per lane
-    for (; q0 <= qhi; q0 += 32) {
-      const float old = pw[q0];
-      const float nv = update(old, __ldg(pxm + q0), __ldg(pxp + q0), __ldg(pym + q0), __ldg(pyp + q0),
-                              __ldg(pzm + q0), __ldg(pzp + q0), __ldg(pr + q0), __ldg(pm + q0), false);
-      pw[q0] = nv;
-      const double d = fabs((double)nv - (double)old);
-      if (d > dmax || d != d) dmax = d;
+    // tail: the row's remaining cells (fewer than 32*U) as one batch; lanes
+    // past the row load a clamped (valid) address and store nothing
+    if (q0 - lane <= qhi) {
+      float old[U], xm[U], xp[U], ym[U], yp[U], zm[U], zp[U], rr[U];
+      unsigned mk[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int q = min(q0 + 32 * u, qhi);
+        old[u] = pw[q];
+        xm[u] = __ldg(pxm + q);
+        xp[u] = __ldg(pxp + q);
+        ym[u] = __ldg(pym + q);
+        yp[u] = __ldg(pyp + q);
+        zm[u] = __ldg(pzm + q);
+        zp[u] = __ldg(pzp + q);
+        rr[u] = __ldg(pr + q);
+        mk[u] = __ldg(pm + q);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int q = q0 + 32 * u;
+        const float nv = update(old[u], xm[u], xp[u], ym[u], yp[u], zm[u], zp[u], rr[u], mk[u], false);
+        if (q <= qhi) {
+          pw[q] = nv;
+          const double d = fabs((double)nv - (double)old[u]);
+          if (d > dmax || d != d) dmax = d;
+        }
+      }
     }
     if (COLOUR == 1 && k == 1) {
       __syncwarp();  // one warp owns the row: its black updates land before the copies

@@ -81,6 +81,7 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
   const float c1 = 1.0f - kOmega;
   float *L = a.lam;
   double dmax = 0.0;
+  float dmax_f = 0.0f;  // largest float <= dmax (NaN never enters: its test fails first)
   for (int r = blockIdx.x * RPB + threadIdx.y; r < nrows; r += gridDim.x * RPB) {
     const int k = 1 + r / (G.Y - 2), j = 1 + r % (G.Y - 2);
     const int i0 = (COLOUR + j + k) & 1;
@@ -107,77 +108,73 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
     const float *__restrict__ pzp = L + oZp;
     const float *__restrict__ pr = a.R + own;
     const uint8_t *__restrict__ pm = a.mask + own;
-    auto update = [&](float old, float xm, float xp, float ym, float yp, float zm, float zp, float rr,
-                      unsigned m_, bool full) -> float {
-      if (full) {
-        return inv63 * (ve * xp + vf * xm + vg * yp + vh * ym + vm * zp + vn * zm - rr) + c1 * old;
-      }
+    auto slow = [&](float old, float xm, float xp, float ym, float yp, float zm, float zp, float rr,
+                    unsigned m_) -> float {
       const float e = (m_ & 1u) ? ve : 0.0f, f = (m_ & 2u) ? vf : 0.0f;
       const float g = (m_ & 4u) ? vg : 0.0f, hh = (m_ & 8u) ? vh : 0.0f;
       const float m = (m_ & 16u) ? vm : 0.0f, n = (m_ & 32u) ? vn : 0.0f;
       return __ldg(inv + m_) * (e * xp + f * xm + g * yp + hh * ym + m * zp + n * zm - rr) + c1 * old;
     };
+    // One batch of U cells per lane: loads, the update (all-fluid warps skip
+    // the wall-mask selects), stores, and the error. The error is FP64-exact
+    // without converting every cell: rounding is monotone, so
+    // fl(|nv - old|) < rd(dmax) proves |nv - old| < dmax; only when a lane's
+    // batch fails that test (or holds a NaN) does the warp take the FP64 path.
+    auto batch = [&](int q0b, bool clamp) {
+      float old[U], xm[U], xp[U], ym[U], yp[U], zm[U], zp[U], rr[U], nv[U];
+      unsigned mk[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int q = clamp ? min(q0b + 32 * u, qhi) : q0b + 32 * u;
+        old[u] = pw[q];
+        xm[u] = __ldg(pxm + q);
+        xp[u] = __ldg(pxp + q);
+        ym[u] = __ldg(pym + q);
+        yp[u] = __ldg(pyp + q);
+        zm[u] = __ldg(pzm + q);
+        zp[u] = __ldg(pzp + q);
+        rr[u] = __ldg(pr + q);
+        mk[u] = __ldg(pm + q);
+      }
+      bool full = !clamp;
+#pragma unroll
+      for (int u = 0; u < U; ++u) full &= (mk[u] == 63u);
+      if (__all_sync(0xffffffffu, full)) {
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          nv[u] = inv63 * (ve * xp[u] + vf * xm[u] + vg * yp[u] + vh * ym[u] + vm * zp[u] + vn * zm[u] - rr[u]) +
+                  c1 * old[u];
+      } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) nv[u] = slow(old[u], xm[u], xp[u], ym[u], yp[u], zm[u], zp[u], rr[u], mk[u]);
+      }
+      bool big = false;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const bool in = !clamp || q0b + 32 * u <= qhi;
+        if (in) {
+          pw[q0b + 32 * u] = nv[u];
+          big |= !(fabsf(nv[u] - old[u]) < dmax_f);
+        }
+      }
+      if (__any_sync(0xffffffffu, big)) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const bool in = !clamp || q0b + 32 * u <= qhi;
+          const double d = fabs((double)nv[u] - (double)old[u]);
+          if (in && (d > dmax || d != d)) dmax = d;
+        }
+        dmax_f = __double2float_rd(dmax);
+      }
+    };
     int q0 = qlo + lane;
     // main loop, warp-uniform: U cells per lane while every lane's U cells lie
     // inside the row (no clamps, so a stream's U loads share one address with
     // immediate offsets)
-    for (; q0 + lane_off + 32 * (U - 1) <= qhi; q0 += 32 * U) {
-      float old[U], xm[U], xp[U], ym[U], yp[U], zm[U], zp[U], rr[U];
-      unsigned mk[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int q = q0 + 32 * u;
-        old[u] = pw[q];
-        xm[u] = __ldg(pxm + q);
-        xp[u] = __ldg(pxp + q);
-        ym[u] = __ldg(pym + q);
-        yp[u] = __ldg(pyp + q);
-        zm[u] = __ldg(pzm + q);
-        zp[u] = __ldg(pzp + q);
-        rr[u] = __ldg(pr + q);
-        mk[u] = __ldg(pm + q);
-      }
-      bool full = true;
-#pragma unroll
-      for (int u = 0; u < U; ++u) full &= (mk[u] == 63u);
-      full = __all_sync(0xffffffffu, full);
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const float nv = update(old[u], xm[u], xp[u], ym[u], yp[u], zm[u], zp[u], rr[u], mk[u], full);
-        pw[q0 + 32 * u] = nv;
-        const double d = fabs((double)nv - (double)old[u]);
-        if (d > dmax || d != d) dmax = d;
-      }
-    }
-    // tail: the row's remaining cells (fewer than 32*U) as one batch; lanes
-    // past the row load a clamped (valid) address and store nothing
-    if (q0 - lane <= qhi) {
-      float old[U], xm[U], xp[U], ym[U], yp[U], zm[U], zp[U], rr[U];
-      unsigned mk[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int q = min(q0 + 32 * u, qhi);
-        old[u] = pw[q];
-        xm[u] = __ldg(pxm + q);
-        xp[u] = __ldg(pxp + q);
-        ym[u] = __ldg(pym + q);
-        yp[u] = __ldg(pyp + q);
-        zm[u] = __ldg(pzm + q);
-        zp[u] = __ldg(pzp + q);
-        rr[u] = __ldg(pr + q);
-        mk[u] = __ldg(pm + q);
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int q = q0 + 32 * u;
-        const float nv = update(old[u], xm[u], xp[u], ym[u], yp[u], zm[u], zp[u], rr[u], mk[u], false);
-        if (q <= qhi) {
-          pw[q] = nv;
-          const double d = fabs((double)nv - (double)old[u]);
-          if (d > dmax || d != d) dmax = d;
-        }
-      }
-    }
+    for (; q0 + lane_off + 32 * (U - 1) <= qhi; q0 += 32 * U) batch(q0, false);
+    // the row's remaining cells (fewer than 32*U) as one batch; lanes past the
+    // row load a clamped, valid address and store nothing
+    if (q0 - lane <= qhi) batch(q0, true);
     if (COLOUR == 1 && k == 1) {
       __syncwarp();  // one warp owns the row: its black updates land before the copies
       // ground mirror of this row, both colours: (i, j, 0) <- (i, j, 1); the

@@ -19,6 +19,8 @@
 // rows (Solver_CPU_RB.cpp:155-162), and its last CTA to finish runs the
 // convergence poll, so one iteration is two launches and no host round trip.
 #pragma once
+#include <type_traits>
+
 #include "qesb_device.cuh"
 
 namespace qesb {
@@ -64,10 +66,10 @@ __device__ __forceinline__ void poll_one(SolveState *st, const double *err, doub
 }
 
 // One colour of the sweep over rows j in [1, Y-2], k in [1, Z-2]. Persistent:
-// the grid holds as many CTAs as fit on the GPU at once; each warp walks rows
-// r = warp, warp + total_warps, ... so a warp pays the kernel's start-up
-// latency and its share of the block reduction once, not once per row, and
-// warps never wait on one another inside the row loop.
+// the grid holds as many CTAs as fit on the GPU at once and each warp sweeps a
+// contiguous range of rows, so it pays the start-up latency and its share of
+// the block reduction once, reloads the per-layer tables only when k changes,
+// and never waits on another warp inside the sweep.
 template <int COLOUR, int RPB, int U>
 __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
 {
@@ -77,66 +79,77 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
   const int it = S->it;
   const int nrows = (G.Y - 2) * (G.Z - 2);
   const int lane = threadIdx.x;
-  const int lane_off = 31 - lane;  // q0 + lane_off = the warp's last lane
   const float c1 = 1.0f - kOmega;
   float *L = a.lam;
-  double dmax = 0.0;
-  float dmax_f = 0.0f;  // largest float <= dmax (NaN never enters: its test fails first)
-  for (int r = blockIdx.x * RPB + threadIdx.y; r < nrows; r += gridDim.x * RPB) {
+  double dmax = 0.0;    // warp-wide max |dlambda| so far (all lanes hold it)
+  float dmax_f = 0.0f;  // largest float <= dmax
+  const int warps = gridDim.x * RPB, w = blockIdx.x * RPB + threadIdx.y;
+  const int r_begin = (int)((long)nrows * w / warps), r_end = (int)((long)nrows * (w + 1) / warps);
+  int kcur = -1;
+  float ve = 0, vf = 0, vg = 0, vh = 0, vm = 0, vn = 0, inv63 = 0;
+  const float *inv = a.inv;
+  for (int r = r_begin; r < r_end; ++r) {
     const int k = 1 + r / (G.Y - 2), j = 1 + r % (G.Y - 2);
+    if (k != kcur) {
+      kcur = k;
+      ve = __ldg(a.val + 0 * G.Z + k);
+      vf = __ldg(a.val + 1 * G.Z + k);
+      vg = __ldg(a.val + 2 * G.Z + k);
+      vh = __ldg(a.val + 3 * G.Z + k);
+      vm = __ldg(a.val + 4 * G.Z + k);
+      vn = __ldg(a.val + 5 * G.Z + k);
+      inv = a.inv + k * 64;
+      inv63 = __ldg(inv + 63);
+    }
     const int i0 = (COLOUR + j + k) & 1;
     const long own = COLOUR * a.S.CS + a.S.row(j, k, G.Y);
     const long oth = (1 - COLOUR) * a.S.CS + a.S.row(j, k, G.Y);
-    const long oYm = oth - a.S.PQ, oYp = oth + a.S.PQ;
-    const long oZm = oth - (long)G.Y * a.S.PQ, oZp = oth + (long)G.Y * a.S.PQ;
-    const float ve = __ldg(a.val + 0 * G.Z + k), vf = __ldg(a.val + 1 * G.Z + k), vg = __ldg(a.val + 2 * G.Z + k);
-    const float vh = __ldg(a.val + 3 * G.Z + k), vm = __ldg(a.val + 4 * G.Z + k), vn = __ldg(a.val + 5 * G.Z + k);
-    const float *inv = a.inv + k * 64;
-    const float inv63 = __ldg(inv + 63);
-    // Updated cells of this row: i in [1, X-2], i = i0 + 2q. Other-colour
-    // lambda, R and the mask go through the read-only path: no thread writes
-    // them during this half-sweep, except the ground-mirror copies below,
-    // which a warp makes only after its own reads of those cells.
+    // Updated cells of this row: i in [1, X-2], i = i0 + 2q. Every load goes
+    // through the read-only path: a cell's own value is read once, by the lane
+    // that then writes it; the other colour, R and the mask are not written
+    // during this half-sweep except by the ground-mirror copies below, which a
+    // warp makes only after its own reads of those cells.
     const int qlo = i0 ? 0 : 1;
     const int qhi = (G.X - 2 - i0) >> 1;  // inclusive
-    float *__restrict__ pw = L + own;
-    const float *__restrict__ pxm = L + oth + i0 - 1;
-    const float *__restrict__ pxp = L + oth + i0;
-    const float *__restrict__ pym = L + oYm;
-    const float *__restrict__ pyp = L + oYp;
-    const float *__restrict__ pzm = L + oZm;
-    const float *__restrict__ pzp = L + oZp;
-    const float *__restrict__ pr = a.R + own;
-    const uint8_t *__restrict__ pm = a.mask + own;
-    auto slow = [&](float old, float xm, float xp, float ym, float yp, float zm, float zp, float rr,
-                    unsigned m_) -> float {
-      const float e = (m_ & 1u) ? ve : 0.0f, f = (m_ & 2u) ? vf : 0.0f;
-      const float g = (m_ & 4u) ? vg : 0.0f, hh = (m_ & 8u) ? vh : 0.0f;
-      const float m = (m_ & 16u) ? vm : 0.0f, n = (m_ & 32u) ? vn : 0.0f;
-      return __ldg(inv + m_) * (e * xp + f * xm + g * yp + hh * ym + m * zp + n * zm - rr) + c1 * old;
-    };
-    // One batch of U cells per lane: loads, the update (all-fluid warps skip
-    // the wall-mask selects), stores, and the error. The error is FP64-exact
+    float *pw = L + own;
+    const float *pxm = L + oth + i0 - 1;
+    const float *pxp = L + oth + i0;
+    const float *pym = L + oth - a.S.PQ;
+    const float *pyp = L + oth + a.S.PQ;
+    const float *pzm = L + oth - (long)G.Y * a.S.PQ;
+    const float *pzp = L + oth + (long)G.Y * a.S.PQ;
+    const float *pr = a.R + own;
+    const uint8_t *pm = a.mask + own;
+    // One batch: U cells per lane at q0b + 32u. PRED: a slot is live only if
+    // inside the row (the row's last, partial batch); dead slots load nothing.
+    // All-fluid warps skip the wall-mask selects. The error is FP64-exact
     // without converting every cell: rounding is monotone, so
-    // fl(|nv - old|) < rd(dmax) proves |nv - old| < dmax; only when a lane's
-    // batch fails that test (or holds a NaN) does the warp take the FP64 path.
-    auto batch = [&](int q0b, bool clamp) {
+    // fl(|nv - old|) < rd(dmax) proves |nv - old| < dmax; only when some lane
+    // fails that test (or holds a NaN) does the warp take the FP64 path.
+    auto batch = [&](int q0b, auto pred_tag) {
+      constexpr bool PRED = decltype(pred_tag)::value;
       float old[U], xm[U], xp[U], ym[U], yp[U], zm[U], zp[U], rr[U], nv[U];
       unsigned mk[U];
+      bool live[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int q = clamp ? min(q0b + 32 * u, qhi) : q0b + 32 * u;
-        old[u] = pw[q];
-        xm[u] = __ldg(pxm + q);
-        xp[u] = __ldg(pxp + q);
-        ym[u] = __ldg(pym + q);
-        yp[u] = __ldg(pyp + q);
-        zm[u] = __ldg(pzm + q);
-        zp[u] = __ldg(pzp + q);
-        rr[u] = __ldg(pr + q);
-        mk[u] = __ldg(pm + q);
+        const int q = q0b + 32 * u;
+        live[u] = !PRED || q <= qhi;
+        old[u] = xm[u] = xp[u] = ym[u] = yp[u] = zm[u] = zp[u] = rr[u] = 0.0f;
+        mk[u] = 63u;
+        if (live[u]) {
+          old[u] = __ldg(pw + q);
+          xm[u] = __ldg(pxm + q);
+          xp[u] = __ldg(pxp + q);
+          ym[u] = __ldg(pym + q);
+          yp[u] = __ldg(pyp + q);
+          zm[u] = __ldg(pzm + q);
+          zp[u] = __ldg(pzp + q);
+          rr[u] = __ldg(pr + q);
+          mk[u] = __ldg(pm + q);
+        }
       }
-      bool full = !clamp;
+      bool full = true;
 #pragma unroll
       for (int u = 0; u < U; ++u) full &= (mk[u] == 63u);
       if (__all_sync(0xffffffffu, full)) {
@@ -146,13 +159,19 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
                   c1 * old[u];
       } else {
 #pragma unroll
-        for (int u = 0; u < U; ++u) nv[u] = slow(old[u], xm[u], xp[u], ym[u], yp[u], zm[u], zp[u], rr[u], mk[u]);
+        for (int u = 0; u < U; ++u) {
+          const unsigned m_ = mk[u];
+          const float e = (m_ & 1u) ? ve : 0.0f, f = (m_ & 2u) ? vf : 0.0f;
+          const float g = (m_ & 4u) ? vg : 0.0f, hh = (m_ & 8u) ? vh : 0.0f;
+          const float m = (m_ & 16u) ? vm : 0.0f, n = (m_ & 32u) ? vn : 0.0f;
+          nv[u] = __ldg(inv + m_) * (e * xp[u] + f * xm[u] + g * yp[u] + hh * ym[u] + m * zp[u] + n * zm[u] - rr[u]) +
+                  c1 * old[u];
+        }
       }
       bool big = false;
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const bool in = !clamp || q0b + 32 * u <= qhi;
-        if (in) {
+        if (live[u]) {
           pw[q0b + 32 * u] = nv[u];
           big |= !(fabsf(nv[u] - old[u]) < dmax_f);
         }
@@ -160,21 +179,19 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
       if (__any_sync(0xffffffffu, big)) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          const bool in = !clamp || q0b + 32 * u <= qhi;
           const double d = fabs((double)nv[u] - (double)old[u]);
-          if (in && (d > dmax || d != d)) dmax = d;
+          if (live[u] && (d > dmax || d != d)) dmax = d;
         }
+        dmax = warp_max_d(dmax);
         dmax_f = __double2float_rd(dmax);
       }
     };
     int q0 = qlo + lane;
-    // main loop, warp-uniform: U cells per lane while every lane's U cells lie
-    // inside the row (no clamps, so a stream's U loads share one address with
-    // immediate offsets)
-    for (; q0 + lane_off + 32 * (U - 1) <= qhi; q0 += 32 * U) batch(q0, false);
-    // the row's remaining cells (fewer than 32*U) as one batch; lanes past the
-    // row load a clamped, valid address and store nothing
-    if (q0 - lane <= qhi) batch(q0, true);
+    // full batches while every lane's U cells lie inside the row (warp-uniform
+    // test on the warp's last lane), then one predicated batch for the rest
+    const int lane_off = 31 - lane;
+    for (; q0 + lane_off + 32 * (U - 1) <= qhi; q0 += 32 * U) batch(q0, std::false_type{});
+    if (q0 - lane <= qhi) batch(q0, std::true_type{});
     if (COLOUR == 1 && k == 1) {
       __syncwarp();  // one warp owns the row: its black updates land before the copies
       // ground mirror of this row, both colours: (i, j, 0) <- (i, j, 1); the

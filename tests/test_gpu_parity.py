@@ -51,7 +51,7 @@ def test_divergence_R_bit_exact(golden):
     np.testing.assert_array_equal(R, O.divergence(d, w))
 
 
-N_VARIANTS = 11  # five fused tile shapes (0-4) + six streaming red/black split shapes (5-10)
+N_VARIANTS = 14  # fused tile shapes (0-4), scalar split shapes (5-10), float4 split shapes (11-13)
 
 
 @pytest.mark.parametrize("variant", range(N_VARIANTS))

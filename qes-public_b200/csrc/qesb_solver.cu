@@ -661,20 +661,22 @@ dim3 split_grid(const DevGrid &G, const SplitVariant &sv, int device)
   const int groups = (nrows + sv.rpb - 1) / sv.rpb;
   return dim3(std::max(1, std::min(groups, per * std::max(nsm[device & 63], 1))));
 }
-template <int RPB, int U>
+template <int RPB, int U, int STRIDED = 0>
 constexpr SplitVariant make_split(const char *name)
 {
-  return SplitVariant{name, RPB, U, k_sor_split<0, RPB, U>, k_sor_split<1, RPB, U>};
+  return SplitVariant{name, RPB, U, k_sor_split<0, RPB, U, STRIDED>, k_sor_split<1, RPB, U, STRIDED>};
 }
-template <int RPB>
+template <int RPB, int STRIDED = 0>
 constexpr SplitVariant make_split4(const char *name)
 {
-  return SplitVariant{name, RPB, 4, k_sor_split4<0, RPB>, k_sor_split4<1, RPB>};
+  return SplitVariant{name, RPB, 4, k_sor_split4<0, RPB, STRIDED>, k_sor_split4<1, RPB, STRIDED>};
 }
 const SplitVariant kSplitVariants[] = {
     make_split<8, 4>("split_r8_u4"), make_split<8, 1>("split_r8_u1"), make_split<8, 2>("split_r8_u2"),
     make_split<4, 8>("split_r4_u8"), make_split<16, 2>("split_r16_u2"), make_split<4, 4>("split_r4_u4"),
     make_split4<4>("split4_r4"), make_split4<8>("split4_r8"), make_split4<16>("split4_r16"),
+    make_split<4, 4, 1>("split_r4_u4_strided"), make_split<8, 2, 1>("split_r8_u2_strided"),
+    make_split4<4, 1>("split4_r4_strided"), make_split4<8, 1>("split4_r8_strided"),
 };
 constexpr int kNumSplit = sizeof(kSplitVariants) / sizeof(kSplitVariants[0]);
 constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the first split shape

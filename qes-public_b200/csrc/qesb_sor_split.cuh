@@ -70,7 +70,7 @@ __device__ __forceinline__ void poll_one(SolveState *st, const double *err, doub
 // contiguous range of rows, so it pays the start-up latency and its share of
 // the block reduction once, reloads the per-layer tables only when k changes,
 // and never waits on another warp inside the sweep.
-template <int COLOUR, int RPB, int U>
+template <int COLOUR, int RPB, int U, int STRIDED>
 __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
 {
   SolveState *S = a.st;
@@ -83,12 +83,18 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
   float *L = a.lam;
   double dmax = 0.0;    // warp-wide max |dlambda| so far (all lanes hold it)
   float dmax_f = 0.0f;  // largest float <= dmax
+  // Row order: STRIDED = 1 sends the warps through the rows together (warp w
+  // takes rows w, w + warps, ...), so the rows in flight form one window and
+  // DRAM sees a few long streams; STRIDED = 0 gives each warp a contiguous
+  // range (fewer per-layer table reloads, scattered streams).
   const int warps = gridDim.x * RPB, w = blockIdx.x * RPB + threadIdx.y;
-  const int r_begin = (int)((long)nrows * w / warps), r_end = (int)((long)nrows * (w + 1) / warps);
+  const int r_begin = STRIDED ? w : (int)((long)nrows * w / warps);
+  const int r_end = STRIDED ? nrows : (int)((long)nrows * (w + 1) / warps);
+  const int r_step = STRIDED ? warps : 1;
   int kcur = -1;
   float ve = 0, vf = 0, vg = 0, vh = 0, vm = 0, vn = 0, inv63 = 0;
   const float *inv = a.inv;
-  for (int r = r_begin; r < r_end; ++r) {
+  for (int r = r_begin; r < r_end; r += r_step) {
     const int k = 1 + r / (G.Y - 2), j = 1 + r % (G.Y - 2);
     if (k != kcur) {
       kcur = k;
@@ -243,7 +249,7 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
 // across the group edge (q-1 when i0 = 0, q+4 when i0 = 1), taken from the
 // neighbouring lane by a shuffle, or loaded at the warp's edge. Cells of the
 // group outside [qlo, qhi] are rewritten with the value this lane read.
-template <int COLOUR, int RPB>
+template <int COLOUR, int RPB, int STRIDED>
 __global__ void __launch_bounds__(32 * RPB) k_sor_split4(SplitArgs a)
 {
   SolveState *S = a.st;
@@ -256,12 +262,18 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split4(SplitArgs a)
   float *L = a.lam;
   double dmax = 0.0;
   float dmax_f = 0.0f;
+  // Row order: STRIDED = 1 sends the warps through the rows together (warp w
+  // takes rows w, w + warps, ...), so the rows in flight form one window and
+  // DRAM sees a few long streams; STRIDED = 0 gives each warp a contiguous
+  // range (fewer per-layer table reloads, scattered streams).
   const int warps = gridDim.x * RPB, w = blockIdx.x * RPB + threadIdx.y;
-  const int r_begin = (int)((long)nrows * w / warps), r_end = (int)((long)nrows * (w + 1) / warps);
+  const int r_begin = STRIDED ? w : (int)((long)nrows * w / warps);
+  const int r_end = STRIDED ? nrows : (int)((long)nrows * (w + 1) / warps);
+  const int r_step = STRIDED ? warps : 1;
   int kcur = -1;
   float ve = 0, vf = 0, vg = 0, vh = 0, vm = 0, vn = 0, inv63 = 0;
   const float *inv = a.inv;
-  for (int r = r_begin; r < r_end; ++r) {
+  for (int r = r_begin; r < r_end; r += r_step) {
     const int k = 1 + r / (G.Y - 2), j = 1 + r % (G.Y - 2);
     if (k != kcur) {
       kcur = k;

@@ -51,7 +51,7 @@ def test_divergence_R_bit_exact(golden):
     np.testing.assert_array_equal(R, O.divergence(d, w))
 
 
-N_VARIANTS = 14  # fused tile shapes (0-4), scalar split shapes (5-10), float4 split shapes (11-13)
+N_VARIANTS = 18  # fused tile shapes (0-4), scalar split (5-10), float4 split (11-13), window-order split (14-17)
 
 
 @pytest.mark.parametrize("variant", range(N_VARIANTS))

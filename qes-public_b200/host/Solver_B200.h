@@ -1,0 +1,34 @@
+// Solver_B200: the B200 lambda solve behind the reference's own Solver
+// interface (src/winds/Solver.h:61-113), so it drops in beside Solver_CPU:
+//
+//     Solver *solver = new Solver_B200(WGD->domain, tol);   // or via SolverFactory type 5
+//     solver->resetLambda();
+//     solver->solve(WGD, itermax);
+//
+// Compiled inside the reference tree it includes the reference's Solver.h and
+// WINDSGeneralData.h; it calls libqesb200.so only through include/qesb.h.
+#pragma once
+
+#include "Solver.h"
+#include "qesb.h"
+
+class Solver_B200 : public Solver
+{
+public:
+  Solver_B200(qes::Domain domain_in, const float &tolerance, int device = 0);
+  ~Solver_B200();
+
+  Solver_B200(const Solver_B200 &) = delete;
+  Solver_B200 &operator=(const Solver_B200 &) = delete;
+
+protected:
+  // Solver::solve semantics (src/winds/Solver_CPU.cpp:42-238): reads e..n,
+  // icellflag, u0 v0 w0 and writes u v w of WGD. lambda lives in the base
+  // class's vector between calls (uploaded before, downloaded after), so
+  // Solver::resetLambda and the reference's cross-call warm start behave as
+  // they do for Solver_CPU.
+  virtual void solve(WINDSGeneralData *WGD, const int &itermax) override;
+
+private:
+  qesb_handle *handle_ = nullptr;
+};

@@ -1,0 +1,62 @@
+// Drop-in demonstration: drives Solver_B200 exactly as qesWinds drives its
+// solver (qesWinds/qesWindsMain.cpp:134-169): construct through the base
+// type, resetLambda, solve. Inputs come from the library's city generator;
+// u, v, w and lambda are written to a binary file for comparison.
+//   solver_b200_demo <out.bin> <Nx> <Ny> <Nz> <seed> <nbuildings> <itermax> <tol> [calls]
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include "Solver_B200.h"
+#include "WINDSGeneralData.h"
+
+int main(int argc, char **argv)
+{
+  if (argc < 9) {
+    std::fprintf(stderr, "usage: %s out.bin Nx Ny Nz seed nbuildings itermax tol [calls]\n", argv[0]);
+    return 2;
+  }
+  const int Nx = std::atoi(argv[2]), Ny = std::atoi(argv[3]), Nz = std::atoi(argv[4]);
+  const unsigned long long seed = std::strtoull(argv[5], nullptr, 10);
+  const int nb = std::atoi(argv[6]), itermax = std::atoi(argv[7]);
+  const float tol = std::strtof(argv[8], nullptr);
+  const int calls = argc > 9 ? std::atoi(argv[9]) : 1;
+
+  std::vector<float> dz(Nz + 1);
+  qesb_city_dz(Nz, 1.0f, 1.03f, dz.data());
+  qes::Domain domain(Nx, Ny, Nz, 2.0f, 2.0f, 1.0f);
+  domain.dz_array = dz;
+  WINDSGeneralData wgd(domain);
+  const long nc = domain.numCellCentered(), nf = domain.numFaceCentered();
+  for (auto *v : {&wgd.e, &wgd.f, &wgd.g, &wgd.h, &wgd.m, &wgd.n}) v->assign(nc, 1.0f);
+  wgd.icellflag.assign(nc, 1);
+  for (auto *v : {&wgd.u0, &wgd.v0, &wgd.w0, &wgd.u, &wgd.v, &wgd.w}) v->assign(nf, 0.0f);
+  qesb_grid g{Nx, Ny, Nz, 2.0f, 2.0f, dz.data()};
+  std::vector<qesb_building> b(nb > 0 ? nb : 1);
+  int nbo = 0;
+  qesb_inflow in{};
+  if (qesb_city_random(&g, seed, nb, 6.0f, 16.0f, 4.0f, 20.0f, b.data(), &nbo, &in) != QESB_OK ||
+      qesb_city_build(&g, nbo, b.data(), &in, wgd.icellflag.data(), wgd.e.data(), wgd.f.data(),
+                      wgd.g.data(), wgd.h.data(), wgd.m.data(), wgd.n.data(), wgd.u0.data(),
+                      wgd.v0.data(), wgd.w0.data()) != QESB_OK) {
+    std::fprintf(stderr, "city generator failed: %s\n", qesb_last_error());
+    return 1;
+  }
+
+  Solver *solver = new Solver_B200(wgd.domain, tol);
+  solver->resetLambda();
+  for (int c = 0; c < calls; ++c) solver->solve(&wgd, itermax);
+
+  struct LambdaOf : Solver_B200 {  // reads the base class's protected lambda for the dump
+    static const std::vector<float> &get(Solver *s) { return s->*(&LambdaOf::lambda); }
+  };
+  FILE *fo = std::fopen(argv[1], "wb");
+  if (!fo) return 1;
+  std::fwrite(wgd.u.data(), sizeof(float), nf, fo);
+  std::fwrite(wgd.v.data(), sizeof(float), nf, fo);
+  std::fwrite(wgd.w.data(), sizeof(float), nf, fo);
+  std::fwrite(LambdaOf::get(solver).data(), sizeof(float), nc, fo);
+  std::fclose(fo);
+  delete static_cast<Solver_B200 *>(solver);
+  return 0;
+}

@@ -140,6 +140,47 @@ qesb_status qesb_set_option(qesb_handle *h, const char *key, int value);
 qesb_status qesb_set_stream(qesb_handle *h, void *stream);
 
 /* ---------------------------------------------------------------------
+ * Solve without allocating. No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: code whose device memory is all
+ * owned by another allocator (a framework's caching allocator holding the
+ * GPU, a host with a fixed device-memory budget) and long-running coupling
+ * loops that must not allocate or free once started (an allocation costs a
+ * device synchronisation and can fragment memory). This entry point neither
+ * creates a handle nor allocates: its scratch (solve state, per-iteration
+ * residuals, dz, R) lives in one file-scope device array of
+ * QESB_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * the process exits. That caps the grid at QESB_NOALLOC_MAX_CELLS cells
+ * (Nx*Ny*(Nz+1)), QESB_NOALLOC_MAX_Z layers and QESB_NOALLOC_MAX_ITERS
+ * iterations; larger requests return QESB_ERR_ARG with the limits in
+ * qesb_last_error().
+ *
+ * Same semantics and bits as qesb_solve_device on the full-coefficient
+ * red-black sweep: inputs e..n, icellflag, u0 v0 w0, lambda and the outputs
+ * u v w are DEVICE pointers in the reference layouts; lambda is read as the
+ * starting point and left holding the result (the caller keeps it between
+ * calls, as Solver keeps its lambda); dz_array in `grid` is a host pointer.
+ * Runs on `stream` (NULL: the legacy default stream) and returns when done.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. Every call shares the one array and resets the
+ * parts that must start at zero, so calls that overlap on the GPU (other
+ * streams, other host threads) race and must not be issued. st (nullable)
+ * gets iterations, convergence and residual; its times are 0.
+ * --------------------------------------------------------------------- */
+#define QESB_NOALLOC_SCRATCH_BYTES (32u << 20)
+#define QESB_NOALLOC_MAX_ITERS 16384
+#define QESB_NOALLOC_MAX_Z 1024
+#define QESB_NOALLOC_MAX_CELLS \
+  ((QESB_NOALLOC_SCRATCH_BYTES - 256u - 8u * QESB_NOALLOC_MAX_ITERS - 4u * QESB_NOALLOC_MAX_Z) / 4u)
+
+qesb_status qesb_solve_noalloc(const qesb_grid *grid, float tol, int itermax, const float *e,
+                               const float *f, const float *g, const float *hc, const float *m,
+                               const float *n, const int *icellflag, const float *u0,
+                               const float *v0, const float *w0, float *lambda, float *u, float *v,
+                               float *w, void *stream, qesb_stats *st);
+
+/* ---------------------------------------------------------------------
  * Seeded synthetic-city generator (host). Restates the reference's set-up of
  * the solver inputs for flat terrain and stair-step cuboid buildings:
  *   ground flags      src/winds/WINDSGeneralData.cpp:438-444

@@ -108,6 +108,8 @@ def lib() -> C.CDLL:
             "qesb_num_variants": ([], C.c_int),
             "qesb_set_option": ([V, C.c_char_p, C.c_int], C.c_int),
             "qesb_set_stream": ([V, V], C.c_int),
+            "qesb_solve_noalloc": ([C.POINTER(Grid), C.c_float, C.c_int] + [V] * 14
+                                   + [V, C.POINTER(Stats)], C.c_int),
             "qesb_city_dz": ([C.c_int, C.c_float, C.c_float, _FP], C.c_int),
             "qesb_city_build": ([C.POINTER(Grid), C.c_int, C.POINTER(Building), C.POINTER(Inflow)]
                                 + [V] * 10, C.c_int),
@@ -333,6 +335,17 @@ class Solver_B200:
         out = np.empty(self.domain.numCellCentered(), dtype=np.float32)
         check(lib().qesb_get_divergence(self._h, _ptr(out)))
         return out
+
+
+def solve_noalloc(domain: Domain, tol: float, itermax: int, e, f, g, h, m, n, icellflag, u0, v0, w0,
+                  lam, u, v, w, stream=None) -> dict:
+    """qesb_solve_noalloc: device pointers (ints) in the reference layouts;
+    lam is read and updated in place. Allocates nothing on the device."""
+    st = Stats()
+    gs = domain.grid_struct()
+    check(lib().qesb_solve_noalloc(C.byref(gs), float(np.float32(tol)), int(itermax), e, f, g, h, m, n,
+                                   icellflag, u0, v0, w0, lam, u, v, w, stream, C.byref(st)))
+    return st.as_dict()
 
 
 class SolverFactory:

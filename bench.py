@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=-1, help="sweep variant for --sweeps-only (-1: autotune)")
+    ap.add_argument("--profile-solve", type=int, default=0,
+                    help="profiling driver: one solve of this many iterations (tol 0) with --variant, exit")
     ap.add_argument("--sweeps-only", type=int, default=0,
                     help="profiling driver: set up the workload, run this many fused-sweep launches, exit")
     return ap.parse_args()
@@ -385,9 +387,23 @@ def run_sweeps_only(args):
     print(json.dumps({"sweeps_only": args.sweeps_only, "k": k, "ms_per_launch": ms / args.sweeps_only}))
 
 
+def run_profile_solve(args):
+    """One solve (R, iterations, correction) for launch-list captures."""
+    import qesb
+
+    w = make_city(args.workload, 0)
+    with qesb.Solver_B200(w.domain, 0.0) as s:
+        if args.variant >= 0:
+            s.set_option("variant", args.variant)
+        st = s.solve(w, args.profile_solve)
+    print(json.dumps({"profile_solve": args.profile_solve, **st}))
+
+
 def main():
     args = parse()
-    if args.sweeps_only:
+    if args.profile_solve:
+        run_profile_solve(args)
+    elif args.sweeps_only:
         run_sweeps_only(args)
     elif args.impl == "reference":
         run_reference(args)

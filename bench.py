@@ -321,7 +321,7 @@ def run_b200(args):
     except (OSError, KeyError, ValueError):
         peak, peak_src = 6650.0, "fallback"
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "sor_tiled_city400.json")
+    prof = os.path.join(ROOT, "profiles", "sor_split_city400.json")
     if os.path.exists(prof):
         try:
             traffic = json.load(open(prof)).get("dram_bytes_per_launch")

@@ -140,6 +140,16 @@ qesb_status qesb_set_option(qesb_handle *h, const char *key, int value);
 qesb_status qesb_set_stream(qesb_handle *h, void *stream);
 
 /* ---------------------------------------------------------------------
+ * Warm-start network (tensor-core kernels).
+ * --------------------------------------------------------------------- */
+/* Self-test of the tcgen05 GEMM core: C[128 x N] = A[128 x K] * B[N x K]^T
+ * in BF16 with FP32 accumulation. A is [128][K] (a_mn = 0) or [K][128]
+ * (a_mn = 1); B is [N][K] (b_mn = 0) or [K][N] (b_mn = 1); BF16 bit patterns,
+ * host pointers. N a multiple of 16 in [16, 256], K a multiple of 64. */
+qesb_status qesb_umma_selftest(const uint16_t *A, const uint16_t *B, float *C, int N, int K, int a_mn,
+                               int b_mn);
+
+/* ---------------------------------------------------------------------
  * Solve without allocating. No counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc: code whose device memory is all

@@ -149,6 +149,27 @@ qesb_status qesb_set_stream(qesb_handle *h, void *stream);
 qesb_status qesb_umma_selftest(const uint16_t *A, const uint16_t *B, float *C, int N, int K, int a_mn,
                                int b_mn);
 
+/* 3x3x3 convolution (zero padding, stride 1) as an implicit GEMM on the
+ * tensor cores; all pointers are device pointers, activations channels-last
+ * BF16 [D][H][W][C]. Input = channel concatenation of x1 (c1 channels; at
+ * (D/2, H/2, W/2) read through x2 nearest upsampling when up1) and x2 (c2
+ * channels, nullable when c2 = 0); c1, c2 multiples of 16. sign = +1 reads
+ * taps at v + offset (forward), -1 at v - offset (input gradient). Bm is the
+ * weight matrix [N][Kp] BF16, k = tap*(c1+c2) + c, Kp = roundup(27*(c1+c2), 64)
+ * zero-padded; tap = (dz+1)*9 + (dy+1)*3 + (dx+1). Output [D][H][W][N] to y
+ * (BF16) or yf (FP32); optional bias[N] (FP32), ReLU, and mask (BF16 [V][N]:
+ * output zeroed where mask <= 0). N in {16, 32, 64, 128}. *err is set if a
+ * kernel's tensor-core completion wait gives up. */
+qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H, int W,
+                        int sign, const void *Bm, int Kp, int N, void *y, void *yf, const float *bias,
+                        int relu, const void *mask, int *err, void *stream);
+/* Weight gradient dW[tap*(c1+c2) + c][n] += sum_v X[v + offset(tap)][c] * dY[v][n]
+ * (FP32, accumulated with atomics: zero it first); X as in qesb_conv3d,
+ * dY BF16 [V][N]; vchunk = voxels per CTA (>= 64). */
+qesb_status qesb_conv3d_wgrad(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H,
+                              int W, const void *dY, int N, long vchunk, float *dW, int *err,
+                              void *stream);
+
 /* ---------------------------------------------------------------------
  * Solve without allocating. No counterpart in the reference.
  *

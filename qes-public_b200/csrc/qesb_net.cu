@@ -103,6 +103,322 @@ __global__ void __launch_bounds__(128) k_umma_selftest(const __nv_bfloat16 *__re
   }
 }
 
+// ---------------------------------------------------------------------------
+// 3x3x3 convolutions as implicit GEMMs on the tensor cores
+// ---------------------------------------------------------------------------
+// Activations are channels-last BF16: T[(z*H + y)*W + x][C], C a multiple of
+// 16 (padding channels are zero). A convolution's input may be the channel
+// concatenation of two tensors (x1 with c1 channels, x2 with c2), and x1 may
+// be stored at half resolution and read through a x2 nearest upsampling.
+struct ConvIn {
+  const __nv_bfloat16 *x1;
+  const __nv_bfloat16 *x2;
+  int c1, c2;  // cin = c1 + c2
+  int up1;     // x1 at (D/2, H/2, W/2)
+};
+
+struct ConvGeom {
+  int D, H, W;  // voxel grid of the GEMM rows (output grid)
+  long V;       // D*H*W
+};
+
+// 16 bytes (8 channels c..c+7, never straddling x1/x2 since c1 % 16 == 0) of
+// the input at voxel (z, y, x), or zeros outside the grid.
+__device__ __forceinline__ uint4 load_in8(const ConvIn &in, const ConvGeom &g, int z, int y, int x, int c)
+{
+  if (z < 0 || z >= g.D || y < 0 || y >= g.H || x < 0 || x >= g.W) return make_uint4(0, 0, 0, 0);
+  const __nv_bfloat16 *p;
+  if (c < in.c1) {
+    if (in.up1)
+      p = in.x1 + ((((long)(z >> 1) * (g.H >> 1) + (y >> 1)) * (g.W >> 1) + (x >> 1)) * in.c1 + c);
+    else
+      p = in.x1 + ((((long)z * g.H + y) * g.W + x) * in.c1 + c);
+  } else {
+    p = in.x2 + ((((long)z * g.H + y) * g.W + x) * in.c2 + (c - in.c1));
+  }
+  return __ldg(reinterpret_cast<const uint4 *>(p));
+}
+
+__device__ __forceinline__ void tap_offset(int t, int &dz, int &dy, int &dx)
+{
+  dz = t / 9 - 1;
+  dy = (t / 3) % 3 - 1;
+  dx = t % 3 - 1;
+}
+
+struct ConvOut {
+  __nv_bfloat16 *y;       // [V][N] BF16 (nullable when yf is set)
+  float *yf;              // [V][N] FP32 (nullable)
+  const float *bias;      // [N] (nullable)
+  int relu;               // ReLU in the epilogue
+  const __nv_bfloat16 *mask;  // [V][N] (nullable): zero where mask <= 0 (gradient through a ReLU)
+};
+
+// Y[v][n] = epilogue( sum_k A[v][k] * Bm[n][k] ), A the implicit im2col of
+// the input at taps v + sign*offset(t), k = t*cin + c, Bm [N][Kp] K-major
+// BF16 (Kp = roundup(27*cin, 64), zero-padded). One CTA of 128 threads per
+// 128 voxels; two shared-memory stages so the gather of chunk j+1 overlaps
+// the MMAs of chunk j; accumulator N FP32 columns of TMEM.
+template <int N>
+__global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int sign, const __nv_bfloat16 *__restrict__ Bm,
+                                                   int Kp, ConvOut out, int *err)
+{
+  constexpr uint32_t SA = 128 * 64 * 2, SB = N * 64 * 2, STAGE = SA + SB;
+  constexpr uint32_t NCOLS = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
+  extern __shared__ __align__(1024) uint8_t sm[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cin = in.c1 + in.c2;
+  const long m0 = (long)blockIdx.x * 128;
+  if (warp == 0) umma::tmem_alloc(&tmem_base, NCOLS);
+  if (tid == 0) {
+    umma::mbar_init(&mbar[0], 1);
+    umma::mbar_init(&mbar[1], 1);
+    umma::fence_mbar_init();
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  constexpr uint32_t idesc = umma::idesc_bf16(128, N, 0, 0);
+
+  // this thread's 8 rows (m = tid/8 + 16 i) and fixed k-group g = tid % 8
+  const int g8 = tid & 7;
+  int rz[8], ry[8], rx[8];
+  bool rv[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const long v = m0 + (tid >> 3) + 16 * i;
+    rv[i] = v < g.V;
+    const long vv = rv[i] ? v : 0;
+    rx[i] = (int)(vv % g.W);
+    ry[i] = (int)((vv / g.W) % g.H);
+    rz[i] = (int)(vv / ((long)g.W * g.H));
+  }
+  const int nk = Kp / 64;
+  bool ok = true;
+  for (int j = 0; j < nk && ok; ++j) {
+    const int s = j & 1;
+    if (j >= 2) ok = umma::mbar_wait(&mbar[s], ((j - 2) >> 1) & 1, kWaitLimit);
+    if (!ok) break;
+    uint8_t *sa = sm + s * STAGE, *sb = sa + SA;
+    // A: rows m = tid/8 + 16 i, k-group g8
+    {
+      const int kk = j * 64 + 8 * g8;
+      const int t = kk / cin, c = kk - t * cin;
+      int dz = 0, dy = 0, dx = 0;
+      if (t < 27) tap_offset(t, dz, dy, dx);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        uint4 val = make_uint4(0, 0, 0, 0);
+        if (rv[i] && t < 27) val = load_in8(in, g, rz[i] + sign * dz, ry[i] + sign * dy, rx[i] + sign * dx, c);
+        *reinterpret_cast<uint4 *>(sa + off_kmajor((tid >> 3) + 16 * i, 8 * g8)) = val;
+      }
+    }
+    // B: N rows x 8 k-groups
+    for (int idx = tid; idx < N * 8; idx += 128) {
+      const int n = idx >> 3, gg = idx & 7;
+      *reinterpret_cast<uint4 *>(sb + off_kmajor(n, 8 * gg)) =
+          __ldg(reinterpret_cast<const uint4 *>(Bm + (long)n * Kp + j * 64 + 8 * gg));
+    }
+    umma::fence_smem_async();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+      const uint32_t a0 = umma::smem_u32(sa), b0 = umma::smem_u32(sb);
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk)
+        umma::mma_bf16(tmem, umma::desc(a0 + kk * 256, 128, 1024), umma::desc(b0 + kk * 256, 128, 1024), idesc,
+                       (j > 0 || kk > 0) ? 1u : 0u);
+      umma::mma_commit(&mbar[s]);
+    }
+  }
+  if (ok) ok = umma::mbar_wait(&mbar[(nk - 1) & 1], ((nk - 1) >> 1) & 1, kWaitLimit);
+  umma::fence_after_sync();
+  if (!ok) {
+    if (lane == 0) atomicExch(err, 1);
+  } else {
+    const long v = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < N; c0 += 8) {
+      float a[8];
+      umma::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, a);
+      if (v < g.V) {
+        if (out.bias) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) a[q] += __ldg(out.bias + c0 + q);
+        }
+        if (out.relu) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) a[q] = fmaxf(a[q], 0.0f);
+        }
+        if (out.mask) {
+          const uint4 mk = __ldg(reinterpret_cast<const uint4 *>(out.mask + v * N + c0));
+          const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&mk);
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (!(__bfloat162float(mb[q]) > 0.0f)) a[q] = 0.0f;
+        }
+        if (out.yf) {
+          float4 *dst = reinterpret_cast<float4 *>(out.yf + v * N + c0);
+          dst[0] = make_float4(a[0], a[1], a[2], a[3]);
+          dst[1] = make_float4(a[4], a[5], a[6], a[7]);
+        } else {
+          uint4 pk;
+          __nv_bfloat162 *h2 = reinterpret_cast<__nv_bfloat162 *>(&pk);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) h2[q] = __floats2bfloat162_rn(a[2 * q], a[2 * q + 1]);
+          *reinterpret_cast<uint4 *>(out.y + v * N + c0) = pk;
+        }
+      }
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, NCOLS);
+  }
+}
+
+// Weight gradient: dW[t*cin + c][n] += sum_v X[v + off(t)][c] * dY[v][n] over
+// this CTA's voxel range. M-tile = 128 rows of (t, c); K = voxels in chunks
+// of 64; both operands MN-major (channels contiguous). Partial sums from the
+// CTAs of a row tile meet in dW (FP32) by atomicAdd.
+template <int N>
+__global__ void __launch_bounds__(128) k_conv_wgrad(ConvIn in, ConvGeom g, const __nv_bfloat16 *__restrict__ dY,
+                                                   long vchunk, float *__restrict__ dW, int *err)
+{
+  constexpr uint32_t SA = 128 * 64 * 2, SB = N * 64 * 2, STAGE = SA + SB;
+  constexpr uint32_t NCOLS = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
+  extern __shared__ __align__(1024) uint8_t sm[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cin = in.c1 + in.c2;
+  const int Mrows = 27 * cin;
+  const int mt0 = blockIdx.x * 128;
+  const long vb = (long)blockIdx.y * vchunk, ve = min(g.V, vb + vchunk);
+  if (vb >= ve) return;
+  if (warp == 0) umma::tmem_alloc(&tmem_base, NCOLS);
+  if (tid == 0) {
+    umma::mbar_init(&mbar[0], 1);
+    umma::mbar_init(&mbar[1], 1);
+    umma::fence_mbar_init();
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  constexpr uint32_t idesc = umma::idesc_bf16(128, N, 1, 1);
+  // this thread: voxel column kv = tid % 64 of each chunk; row groups rg = tid/64 + 2 i
+  const int kv = tid & 63;
+  int tg[8], cg[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int m = mt0 + 8 * ((tid >> 6) + 2 * i);
+    tg[i] = m < Mrows ? m / cin : 27;
+    cg[i] = m < Mrows ? m - tg[i] * cin : 0;
+  }
+  const int nk = (int)((ve - vb + 63) / 64);
+  bool ok = true;
+  for (int j = 0; j < nk && ok; ++j) {
+    const int s = j & 1;
+    if (j >= 2) ok = umma::mbar_wait(&mbar[s], ((j - 2) >> 1) & 1, kWaitLimit);
+    if (!ok) break;
+    uint8_t *sa = sm + s * STAGE, *sb = sa + SA;
+    const long v = vb + (long)j * 64 + kv;
+    const bool vin = v < ve;
+    const int x = vin ? (int)(v % g.W) : 0, y = vin ? (int)((v / g.W) % g.H) : 0,
+              z = vin ? (int)(v / ((long)g.W * g.H)) : 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      uint4 val = make_uint4(0, 0, 0, 0);
+      if (vin && tg[i] < 27) {
+        int dz, dy, dx;
+        tap_offset(tg[i], dz, dy, dx);
+        val = load_in8(in, g, z + dz, y + dy, x + dx, cg[i]);
+      }
+      *reinterpret_cast<uint4 *>(sa + off_mnmajor(8 * ((tid >> 6) + 2 * i), kv, 128)) = val;
+    }
+    for (int idx = tid; idx < N / 8 * 64; idx += 128) {
+      const int ng = idx >> 6, k = idx & 63;
+      const long vv = vb + (long)j * 64 + k;
+      uint4 val = make_uint4(0, 0, 0, 0);
+      if (vv < ve) val = __ldg(reinterpret_cast<const uint4 *>(dY + vv * N + 8 * ng));
+      *reinterpret_cast<uint4 *>(sb + off_mnmajor(8 * ng, k, N)) = val;
+    }
+    umma::fence_smem_async();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+      const uint32_t a0 = umma::smem_u32(sa), b0 = umma::smem_u32(sb);
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk)
+        umma::mma_bf16(tmem, umma::desc(a0 + kk * 2 * 16 * 128, 16 * 128, 128),
+                       umma::desc(b0 + kk * 2 * (N / 8) * 128, (N / 8) * 128, 128), idesc,
+                       (j > 0 || kk > 0) ? 1u : 0u);
+      umma::mma_commit(&mbar[s]);
+    }
+  }
+  if (ok) ok = umma::mbar_wait(&mbar[(nk - 1) & 1], ((nk - 1) >> 1) & 1, kWaitLimit);
+  umma::fence_after_sync();
+  if (!ok) {
+    if (lane == 0) atomicExch(err, 1);
+  } else {
+    const int m = mt0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < N; c0 += 8) {
+      float a[8];
+      umma::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, a);
+      if (m < Mrows) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) atomicAdd(dW + (long)m * N + c0 + q, a[q]);
+      }
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, NCOLS);
+  }
+}
+
+template <int N>
+qesb_status launch_conv(const ConvIn &in, const ConvGeom &g, int sign, const __nv_bfloat16 *Bm, int Kp,
+                        const ConvOut &out, int *err, cudaStream_t s)
+{
+  constexpr int smem = 2 * (128 * 64 * 2 + N * 64 * 2);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_conv_igemm<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv attr: %s", cudaGetErrorString(e));
+    attr = true;
+  }
+  const unsigned blocks = (unsigned)((g.V + 127) / 128);
+  k_conv_igemm<N><<<blocks, 128, smem, s>>>(in, g, sign, Bm, Kp, out, err);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));
+}
+
+template <int N>
+qesb_status launch_wgrad(const ConvIn &in, const ConvGeom &g, const __nv_bfloat16 *dY, long vchunk, float *dW,
+                         int *err, cudaStream_t s)
+{
+  constexpr int smem = 2 * (128 * 64 * 2 + N * 64 * 2);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_conv_wgrad<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "wgrad attr: %s", cudaGetErrorString(e));
+    attr = true;
+  }
+  const int cin = in.c1 + in.c2;
+  const dim3 grid((unsigned)((27 * cin + 127) / 128), (unsigned)((g.V + vchunk - 1) / vchunk));
+  k_conv_wgrad<N><<<grid, 128, smem, s>>>(in, g, dY, vchunk, dW, err);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "wgrad launch: %s", cudaGetErrorString(e));
+}
+
 }  // namespace
 
 extern "C" qesb_status qesb_umma_selftest(const uint16_t *A, const uint16_t *B, float *C, int N, int K, int a_mn,
@@ -138,4 +454,53 @@ extern "C" qesb_status qesb_umma_selftest(const uint16_t *A, const uint16_t *B, 
   if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "qesb_umma_selftest: %s", cudaGetErrorString(e));
   if (herr) return qesb_fail(QESB_ERR_CUDA, "qesb_umma_selftest: MMA completion wait timed out");
   return QESB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// conv C ABI (device pointers)
+// ---------------------------------------------------------------------------
+namespace {
+bool conv_args_ok(int c1, int c2, int N, int D, int H, int W, int up1)
+{
+  return c1 > 0 && c1 % 16 == 0 && c2 >= 0 && c2 % 16 == 0 && (N == 16 || N == 32 || N == 64 || N == 128) &&
+         D > 0 && H > 0 && W > 0 && (!up1 || (D % 2 == 0 && H % 2 == 0 && W % 2 == 0));
+}
+}  // namespace
+
+extern "C" qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H, int W,
+                                   int sign, const void *Bm, int Kp, int N, void *y, void *yf, const float *bias,
+                                   int relu, const void *mask, int *err, void *stream)
+{
+  if (!conv_args_ok(c1, c2, N, D, H, W, up1) || !x1 || (c2 && !x2) || !Bm || (!y && !yf) || !err ||
+      (sign != 1 && sign != -1) || Kp < 27 * (c1 + c2) || Kp % 64)
+    return qesb_fail(QESB_ERR_ARG, "qesb_conv3d: bad arguments");
+  ConvIn in{static_cast<const __nv_bfloat16 *>(x1), static_cast<const __nv_bfloat16 *>(x2), c1, c2, up1};
+  ConvGeom g{D, H, W, (long)D * H * W};
+  ConvOut o{static_cast<__nv_bfloat16 *>(y), static_cast<float *>(yf), bias, relu,
+            static_cast<const __nv_bfloat16 *>(mask)};
+  const auto *B = static_cast<const __nv_bfloat16 *>(Bm);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  switch (N) {
+    case 16: return launch_conv<16>(in, g, sign, B, Kp, o, err, s);
+    case 32: return launch_conv<32>(in, g, sign, B, Kp, o, err, s);
+    case 64: return launch_conv<64>(in, g, sign, B, Kp, o, err, s);
+    default: return launch_conv<128>(in, g, sign, B, Kp, o, err, s);
+  }
+}
+
+extern "C" qesb_status qesb_conv3d_wgrad(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H,
+                                         int W, const void *dY, int N, long vchunk, float *dW, int *err, void *stream)
+{
+  if (!conv_args_ok(c1, c2, N, D, H, W, up1) || !x1 || (c2 && !x2) || !dY || !dW || !err || vchunk < 64)
+    return qesb_fail(QESB_ERR_ARG, "qesb_conv3d_wgrad: bad arguments");
+  ConvIn in{static_cast<const __nv_bfloat16 *>(x1), static_cast<const __nv_bfloat16 *>(x2), c1, c2, up1};
+  ConvGeom g{D, H, W, (long)D * H * W};
+  const auto *d = static_cast<const __nv_bfloat16 *>(dY);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  switch (N) {
+    case 16: return launch_wgrad<16>(in, g, d, vchunk, dW, err, s);
+    case 32: return launch_wgrad<32>(in, g, d, vchunk, dW, err, s);
+    case 64: return launch_wgrad<64>(in, g, d, vchunk, dW, err, s);
+    default: return launch_wgrad<128>(in, g, d, vchunk, dW, err, s);
+  }
 }

@@ -111,6 +111,10 @@ def lib() -> C.CDLL:
             "qesb_solve_noalloc": ([C.POINTER(Grid), C.c_float, C.c_int] + [V] * 14
                                    + [V, C.POINTER(Stats)], C.c_int),
             "qesb_umma_selftest": ([V, V, V, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+            "qesb_conv3d": ([V, C.c_int, C.c_int, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, V,
+                             C.c_int, C.c_int, V, V, V, C.c_int, V, V, V], C.c_int),
+            "qesb_conv3d_wgrad": ([V, C.c_int, C.c_int, V, C.c_int, C.c_int, C.c_int, C.c_int, V, C.c_int,
+                                   C.c_long, V, V, V], C.c_int),
             "qesb_city_dz": ([C.c_int, C.c_float, C.c_float, _FP], C.c_int),
             "qesb_city_build": ([C.POINTER(Grid), C.c_int, C.POINTER(Building), C.POINTER(Inflow)]
                                 + [V] * 10, C.c_int),

@@ -34,3 +34,135 @@ def test_umma_gemm_core(N, K, a_mn, b_mn):
     qesb.check(qesb.lib().qesb_umma_selftest(Ain.ctypes.data_as(C.c_void_p), Bin.ctypes.data_as(C.c_void_p),
                                              out.ctypes.data_as(C.c_void_p), N, K, a_mn, b_mn))
     np.testing.assert_allclose(out, ref, rtol=1e-5, atol=1e-4 * np.sqrt(K))
+
+
+# ---------------------------------------------------------------------------
+# implicit-GEMM conv3d kernels against torch (CPU, float64)
+# ---------------------------------------------------------------------------
+def _bf16(t):
+    import torch
+    return t.to(torch.bfloat16)
+
+
+def _bm_forward(w):
+    """torch weight [Cout][Cin][3][3][3] -> Bm [Cout][Kp], k = tap*Cin + c."""
+    import torch
+    co, ci = w.shape[:2]
+    k = 27 * ci
+    kp = (k + 63) // 64 * 64
+    bm = torch.zeros(co, kp, dtype=w.dtype)
+    bm[:, :k] = w.permute(0, 2, 3, 4, 1).reshape(co, k)
+    return bm, kp
+
+
+def _bm_dgrad(w):
+    """Bd [Cin][Kp'], k = tap*Cout + co, tap of the forward kernel."""
+    import torch
+    co, ci = w.shape[:2]
+    k = 27 * co
+    kp = (k + 63) // 64 * 64
+    bd = torch.zeros(ci, kp, dtype=w.dtype)
+    bd[:, :k] = w.permute(1, 2, 3, 4, 0).reshape(ci, k)
+    return bd, kp
+
+
+def _cl(t):
+    """[1][C][D][H][W] -> channels-last [D][H][W][C] contiguous."""
+    return t[0].permute(1, 2, 3, 0).contiguous()
+
+
+def _run_conv(x1, c1, up1, x2, c2, D, H, W, sign, bm, kp, n, bias=None, relu=0, mask=None):
+    import torch
+    dev = "cuda:0"
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    yf = torch.zeros(D * H * W * n, dtype=torch.float32, device=dev)
+    g = lambda t: t.data_ptr() if t is not None else None
+    qesb.check(qesb.lib().qesb_conv3d(g(x1), c1, up1, g(x2), c2, D, H, W, sign, g(bm), kp, n, None, g(yf),
+                                      g(bias), relu, g(mask), g(err), None))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    return yf.view(D, H, W, n).cpu().double()
+
+
+@pytest.mark.parametrize("D,H,W,ci,co", [(8, 12, 20, 16, 32), (6, 8, 8, 32, 16), (4, 6, 10, 64, 128),
+                                         (8, 8, 16, 128, 64)])
+def test_conv3d_forward(D, H, W, ci, co):
+    import torch
+    torch.manual_seed(D * H + ci)
+    x = _bf16(torch.randn(1, ci, D, H, W))
+    w = _bf16(torch.randn(co, ci, 3, 3, 3) / (27 * ci) ** 0.5)
+    b = torch.randn(co)
+    ref = torch.nn.functional.conv3d(x.double(), w.double(), b.double(), padding=1)
+    ref = torch.relu(ref)
+    bm, kp = _bm_forward(w)
+    dev = "cuda:0"
+    out = _run_conv(_cl(x).to(dev), ci, 0, None, 0, D, H, W, 1, bm.to(dev), kp, co,
+                    bias=b.float().to(dev), relu=1)
+    np.testing.assert_allclose(out.numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)
+
+
+def test_conv3d_concat_upsampled_input():
+    import torch
+    torch.manual_seed(3)
+    D, H, W, c1, c2, co = 8, 12, 20, 32, 16, 16
+    x1 = _bf16(torch.randn(1, c1, D // 2, H // 2, W // 2))
+    x2 = _bf16(torch.randn(1, c2, D, H, W))
+    w = _bf16(torch.randn(co, c1 + c2, 3, 3, 3) / (27 * 48) ** 0.5)
+    up = torch.nn.functional.interpolate(x1.double(), scale_factor=2, mode="nearest")
+    ref = torch.nn.functional.conv3d(torch.cat([up, x2.double()], 1), w.double(), padding=1)
+    bm, kp = _bm_forward(w)
+    dev = "cuda:0"
+    out = _run_conv(_cl(x1).to(dev), c1, 1, _cl(x2).to(dev), c2, D, H, W, 1, bm.to(dev), kp, co)
+    np.testing.assert_allclose(out.numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.parametrize("D,H,W,ci,co", [(8, 12, 20, 16, 32), (4, 6, 10, 64, 128)])
+def test_conv3d_input_gradient_with_relu_mask(D, H, W, ci, co):
+    import torch
+    torch.manual_seed(11 + ci)
+    x = torch.relu(_bf16(torch.randn(1, ci, D, H, W)).double())  # a ReLU output, as layer inputs are
+    w = _bf16(torch.randn(co, ci, 3, 3, 3) / (27 * ci) ** 0.5)
+    dy = _bf16(torch.randn(1, co, D, H, W))
+    xr = x.clone().requires_grad_(True)
+    y = torch.nn.functional.conv3d(xr, w.double(), padding=1)
+    (y * dy.double()).sum().backward()
+    ref = xr.grad * (x > 0)
+    bd, kp = _bm_dgrad(w)
+    dev = "cuda:0"
+    out = _run_conv(_cl(dy).to(dev), co, 0, None, 0, D, H, W, -1, bd.to(dev), kp, ci,
+                    mask=_cl(_bf16(x)).to(dev))
+    np.testing.assert_allclose(out.numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.parametrize("D,H,W,ci,co,up", [(8, 12, 20, 16, 32, 0), (4, 6, 10, 64, 16, 0), (8, 8, 16, 32, 64, 1)])
+def test_conv3d_weight_gradient(D, H, W, ci, co, up):
+    import torch
+    torch.manual_seed(5 + ci + up)
+    dev = "cuda:0"
+    if up:
+        c1, c2 = ci, 16
+        x1 = _bf16(torch.randn(1, c1, D // 2, H // 2, W // 2))
+        x2 = _bf16(torch.randn(1, c2, D, H, W))
+        xin = torch.cat([torch.nn.functional.interpolate(x1.double(), scale_factor=2, mode="nearest"),
+                         x2.double()], 1)
+    else:
+        c1, c2 = ci, 0
+        x1 = _bf16(torch.randn(1, ci, D, H, W))
+        x2 = None
+        xin = x1.double()
+    cin = c1 + c2
+    w = torch.zeros(co, cin, 3, 3, 3, dtype=torch.float64, requires_grad=True)
+    dy = _bf16(torch.randn(1, co, D, H, W))
+    y = torch.nn.functional.conv3d(xin, w, padding=1)
+    (y * dy.double()).sum().backward()
+    ref = w.grad.permute(2, 3, 4, 1, 0).reshape(27 * cin, co)  # [tap*cin + c][co]
+    dW = torch.zeros(27 * cin * co, dtype=torch.float32, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    x2d = _cl(x2).to(dev) if x2 is not None else None
+    qesb.check(qesb.lib().qesb_conv3d_wgrad(_cl(x1).to(dev).data_ptr(), c1, up,
+                                            x2d.data_ptr() if x2d is not None else None, c2, D, H, W,
+                                            _cl(dy).to(dev).data_ptr(), co, 256, dW.data_ptr(), err.data_ptr(),
+                                            None))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    np.testing.assert_allclose(dW.view(27 * cin, co).cpu().double().numpy(), ref.numpy(), rtol=1e-4, atol=1e-3)

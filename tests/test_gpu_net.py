@@ -96,8 +96,8 @@ def test_conv3d_forward(D, H, W, ci, co):
     ref = torch.relu(ref)
     bm, kp = _bm_forward(w)
     dev = "cuda:0"
-    out = _run_conv(_cl(x).to(dev), ci, 0, None, 0, D, H, W, 1, bm.to(dev), kp, co,
-                    bias=b.float().to(dev), relu=1)
+    xd, bmd, bd = _cl(x).to(dev), bm.to(dev), b.float().to(dev)
+    out = _run_conv(xd, ci, 0, None, 0, D, H, W, 1, bmd, kp, co, bias=bd, relu=1)
     np.testing.assert_allclose(out.numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)
 
 
@@ -112,7 +112,8 @@ def test_conv3d_concat_upsampled_input():
     ref = torch.nn.functional.conv3d(torch.cat([up, x2.double()], 1), w.double(), padding=1)
     bm, kp = _bm_forward(w)
     dev = "cuda:0"
-    out = _run_conv(_cl(x1).to(dev), c1, 1, _cl(x2).to(dev), c2, D, H, W, 1, bm.to(dev), kp, co)
+    x1d, x2d, bmd = _cl(x1).to(dev), _cl(x2).to(dev), bm.to(dev)
+    out = _run_conv(x1d, c1, 1, x2d, c2, D, H, W, 1, bmd, kp, co)
     np.testing.assert_allclose(out.numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)
 
 
@@ -129,8 +130,8 @@ def test_conv3d_input_gradient_with_relu_mask(D, H, W, ci, co):
     ref = xr.grad * (x > 0)
     bd, kp = _bm_dgrad(w)
     dev = "cuda:0"
-    out = _run_conv(_cl(dy).to(dev), co, 0, None, 0, D, H, W, -1, bd.to(dev), kp, ci,
-                    mask=_cl(_bf16(x)).to(dev))
+    dyd, bdd, md = _cl(dy).to(dev), bd.to(dev), _cl(_bf16(x)).to(dev)
+    out = _run_conv(dyd, co, 0, None, 0, D, H, W, -1, bdd, kp, ci, mask=md)
     np.testing.assert_allclose(out.numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)
 
 
@@ -158,10 +159,12 @@ def test_conv3d_weight_gradient(D, H, W, ci, co, up):
     ref = w.grad.permute(2, 3, 4, 1, 0).reshape(27 * cin, co)  # [tap*cin + c][co]
     dW = torch.zeros(27 * cin * co, dtype=torch.float32, device=dev)
     err = torch.zeros(1, dtype=torch.int32, device=dev)
+    # keep every device tensor referenced until the kernel has run
+    x1d = _cl(x1).to(dev)
     x2d = _cl(x2).to(dev) if x2 is not None else None
-    qesb.check(qesb.lib().qesb_conv3d_wgrad(_cl(x1).to(dev).data_ptr(), c1, up,
-                                            x2d.data_ptr() if x2d is not None else None, c2, D, H, W,
-                                            _cl(dy).to(dev).data_ptr(), co, 256, dW.data_ptr(), err.data_ptr(),
+    dyd = _cl(dy).to(dev)
+    qesb.check(qesb.lib().qesb_conv3d_wgrad(x1d.data_ptr(), c1, up, x2d.data_ptr() if x2d is not None else None,
+                                            c2, D, H, W, dyd.data_ptr(), co, 256, dW.data_ptr(), err.data_ptr(),
                                             None))
     torch.cuda.synchronize()
     assert int(err.item()) == 0

@@ -142,6 +142,22 @@ qesb_status qesb_set_stream(qesb_handle *h, void *stream);
 /* ---------------------------------------------------------------------
  * Warm-start network (tensor-core kernels).
  * --------------------------------------------------------------------- */
+/* Handle-side glue of the warm start (device pointers, the handle's stream).
+ * The network grid is planes 0..Nz-1 of the X x Y cell grid (all but the top
+ * boundary plane), channels-last [Nz][Ny][Nx][C] BF16.
+ *   qesb_compute_divergence: R from the current inputs (as a solve does first).
+ *   qesb_warm_input:  network input from R, icellflag and dz (C >= 5 channels:
+ *                     R/s, solid, dz/mean dz, boundary, height fraction);
+ *                     *scale (device) receives s = max|R| over updated cells.
+ *   qesb_warm_target: lambda/s and a 1/0 weight (updated cells) per voxel, FP32.
+ *   qesb_warm_apply:  lambda <- s * yhead[v][0] on updated cells (yhead FP32
+ *                     [V][N]), 0 elsewhere, ground plane mirrored: the next
+ *                     qesb_solve starts from it. */
+qesb_status qesb_compute_divergence(qesb_handle *h);
+qesb_status qesb_warm_input(qesb_handle *h, void *x, int C, unsigned *scale);
+qesb_status qesb_warm_target(qesb_handle *h, float *tgt, float *w, const unsigned *scale);
+qesb_status qesb_warm_apply(qesb_handle *h, const float *yhead, int N, const unsigned *scale);
+
 /* Self-test of the tcgen05 GEMM core: C[128 x N] = A[128 x K] * B[N x K]^T
  * in BF16 with FP32 accumulation. A is [128][K] (a_mn = 0) or [K][128]
  * (a_mn = 1); B is [N][K] (b_mn = 0) or [K][N] (b_mn = 1); BF16 bit patterns,
@@ -169,6 +185,23 @@ qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *x2, int c2,
 qesb_status qesb_conv3d_wgrad(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H,
                               int W, const void *dY, int N, long vchunk, float *dW, int *err,
                               void *stream);
+
+/* Elementwise kernels of the network (device pointers; BF16 activations
+ * channels-last; FP32 gradients where named float). */
+qesb_status qesb_net_pool2(const void *x, void *y, int D, int H, int W, int C, void *stream);
+qesb_status qesb_net_skip_grad(const float *gcat, int ccat, int coff, const float *gpool, const void *e,
+                               void *ge, int D, int H, int W, int C, void *stream);
+qesb_status qesb_net_up_grad(const float *gcat, int ccat, const void *x, void *gx, int D, int H, int W,
+                             int C, void *stream);
+qesb_status qesb_net_to_bf16(const float *g, const void *mask, void *out, long n, void *stream);
+qesb_status qesb_net_colsum(const void *g, long V, int C, float *db, void *stream);
+qesb_status qesb_net_mse(const float *yhead, int N, const float *tgt, const float *w, long V,
+                         float inv_count, void *g, double *loss, void *stream);
+qesb_status qesb_net_adam_conv(float *Wt, float *m, float *v, const float *dW, int cin, int cout,
+                               int cout_real, void *Bm, int Kp, void *Bd, int Kd, float lr, float b1,
+                               float b2, float eps, int step, float grad_scale, void *stream);
+qesb_status qesb_net_adam_vec(float *p, float *m, float *v, const float *g, int n, float lr, float b1,
+                              float b2, float eps, int step, float grad_scale, void *stream);
 
 /* ---------------------------------------------------------------------
  * Solve without allocating. No counterpart in the reference.

@@ -504,3 +504,253 @@ extern "C" qesb_status qesb_conv3d_wgrad(const void *x1, int c1, int up1, const 
     default: return launch_wgrad<128>(in, g, d, vchunk, dW, err, s);
   }
 }
+
+// ---------------------------------------------------------------------------
+// elementwise kernels of the warm-start network (memory-bound, grid-stride)
+// ---------------------------------------------------------------------------
+namespace {
+
+inline unsigned gs_blocks(long n, int per = 256) { return (unsigned)std::min<long>((n + per - 1) / per, 148L * 32); }
+
+// 2x2x2 average pooling: y[(D/2)(H/2)(W/2)][C] from x[D][H][W][C] (BF16).
+__global__ void k_pool2(const __nv_bfloat16 *__restrict__ x, __nv_bfloat16 *__restrict__ y, int D, int H, int W, int C)
+{
+  const int d = D / 2, h = H / 2, w = W / 2;
+  const long n = (long)d * h * w * C;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const long v = i / C;
+    const int xx = (int)(v % w), yy = (int)((v / w) % h), zz = (int)(v / ((long)w * h));
+    float s = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const long src = (((long)(2 * zz + (q >> 2)) * H + 2 * yy + ((q >> 1) & 1)) * W + 2 * xx + (q & 1)) * C + c;
+      s += __bfloat162float(x[src]);
+    }
+    y[i] = __float2bfloat16_rn(s * 0.125f);
+  }
+}
+
+// Gradient into a skip tensor e (level grid D x H x W, C channels):
+//   g_e = (gcat[v][coff + c] + gpool[parent(v)][c] / 8) * (e[v][c] > 0)
+// gcat: FP32 input gradient of the decoder conv that reads e (its channels
+// coff.. coff+C-1); gpool: FP32 gradient of pool(e) (nullable).
+__global__ void k_skip_grad(const float *__restrict__ gcat, int ccat, int coff, const float *__restrict__ gpool,
+                            const __nv_bfloat16 *__restrict__ e, __nv_bfloat16 *__restrict__ ge, int D, int H, int W,
+                            int C)
+{
+  const long n = (long)D * H * W * C;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const long v = i / C;
+    float g = gcat[v * ccat + coff + c];
+    if (gpool) {
+      const int x = (int)(v % W), y = (int)((v / W) % H), z = (int)(v / ((long)W * H));
+      g += gpool[((((long)(z >> 1) * (H >> 1)) + (y >> 1)) * (W >> 1) + (x >> 1)) * C + c] * 0.125f;
+    }
+    ge[i] = __float2bfloat16_rn(__bfloat162float(e[i]) > 0.0f ? g : 0.0f);
+  }
+}
+
+// Gradient of an upsampled input: gx[vlow][c] = sum over the 8 children of
+// gcat[child][c] (channels 0..C-1 of gcat), times (x[vlow][c] > 0).
+__global__ void k_up_grad(const float *__restrict__ gcat, int ccat, const __nv_bfloat16 *__restrict__ x,
+                          __nv_bfloat16 *__restrict__ gx, int D, int H, int W, int C)
+{
+  const int d = D / 2, h = H / 2, w = W / 2;
+  const long n = (long)d * h * w * C;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const long v = i / C;
+    const int xx = (int)(v % w), yy = (int)((v / w) % h), zz = (int)(v / ((long)w * h));
+    float s = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      s += gcat[(((long)(2 * zz + (q >> 2)) * H + 2 * yy + ((q >> 1) & 1)) * W + 2 * xx + (q & 1)) * ccat + c];
+    gx[i] = __float2bfloat16_rn(__bfloat162float(x[i]) > 0.0f ? s : 0.0f);
+  }
+}
+
+// FP32 -> BF16 with an optional ReLU-derivative mask (same shape).
+__global__ void k_to_bf16_masked(const float *__restrict__ g, const __nv_bfloat16 *__restrict__ mask,
+                                 __nv_bfloat16 *__restrict__ out, long n)
+{
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const float v = g[i];
+    out[i] = __float2bfloat16_rn(!mask || __bfloat162float(mask[i]) > 0.0f ? v : 0.0f);
+  }
+}
+
+// Column sums db[c] += sum_v g[v][c] (BF16 gradient), per-block partials.
+__global__ void k_colsum(const __nv_bfloat16 *__restrict__ g, long V, int C, float *__restrict__ db)
+{
+  extern __shared__ float part[];
+  for (int c = threadIdx.x; c < C; c += blockDim.x) part[c] = 0.0f;
+  __syncthreads();
+  const int lanes = blockDim.x / C * C;  // threads grouped by channel
+  if ((int)threadIdx.x < lanes) {
+    const int c = threadIdx.x % C;
+    float s = 0.0f;
+    for (long v = blockIdx.x * (long)(lanes / C) + threadIdx.x / C; v < V; v += (long)gridDim.x * (lanes / C))
+      s += __bfloat162float(g[v * C + c]);
+    atomicAdd(&part[c], s);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(&db[c], part[c]);
+}
+
+// Loss over valid cells: pred = yhead[v][0] (FP32, head channel stride N),
+// L += sum (pred - tgt)^2 * w[v]; gradient 2 (pred - tgt) w / count into
+// channel 0 of g (BF16 [V][N], other channels zero).
+__global__ void k_mse(const float *__restrict__ yhead, int N, const float *__restrict__ tgt,
+                      const float *__restrict__ w, long V, float inv_count, __nv_bfloat16 *__restrict__ g,
+                      double *__restrict__ loss)
+{
+  double acc = 0.0;
+  for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < V; v += (long)gridDim.x * blockDim.x) {
+    const float d = (yhead[v * N] - tgt[v]) * w[v];
+    acc += (double)d * d;
+    g[v * N] = __float2bfloat16_rn(2.0f * d * inv_count);
+    for (int c = 1; c < N; ++c) g[v * N + c] = __float2bfloat16_rn(0.0f);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, acc);
+}
+
+// Adam on one conv layer (Kingma & Ba 2015): master weights W[27*cin][cout]
+// (row t*cin + c), moments m, v, gradient dW; bias likewise. Writes the two
+// BF16 GEMM layouts: Bm[cout][Kp] (k = t*cin + c) and Bd[cin][Kd] (k = t*cout + o).
+__global__ void k_adam_conv(float *__restrict__ Wt, float *__restrict__ m, float *__restrict__ v,
+                            const float *__restrict__ dW, int cin, int cout, int cout_real,
+                            __nv_bfloat16 *__restrict__ Bm, int Kp, __nv_bfloat16 *__restrict__ Bd, int Kd,
+                            float lr, float b1, float b2, float eps, float c1, float c2, float grad_scale)
+{
+  const long n = 27L * cin * cout;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int o = (int)(i % cout);
+    const long row = i / cout;  // t*cin + c
+    const int t = (int)(row / cin), c = (int)(row % cin);
+    float w = Wt[i];
+    if (o < cout_real) {
+      const float g = dW[i] * grad_scale;
+      const float mm = b1 * m[i] + (1.0f - b1) * g;
+      const float vv = b2 * v[i] + (1.0f - b2) * g * g;
+      m[i] = mm;
+      v[i] = vv;
+      w -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+      Wt[i] = w;
+    }
+    const __nv_bfloat16 wb = __float2bfloat16_rn(o < cout_real ? w : 0.0f);
+    Bm[(long)o * Kp + row] = wb;
+    if (Bd) Bd[(long)c * Kd + (long)t * cout + o] = wb;
+  }
+}
+
+__global__ void k_adam_vec(float *__restrict__ p, float *__restrict__ m, float *__restrict__ v,
+                           const float *__restrict__ g, int n, float lr, float b1, float b2, float eps, float c1,
+                           float c2, float grad_scale)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const float gg = g[i] * grad_scale;
+    const float mm = b1 * m[i] + (1.0f - b1) * gg;
+    const float vv = b2 * v[i] + (1.0f - b2) * gg * gg;
+    m[i] = mm;
+    v[i] = vv;
+    p[i] -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+  }
+}
+
+}  // namespace
+
+#define NET_CK(expr)                                                                               \
+  do {                                                                                             \
+    cudaError_t e_ = (expr);                                                                       \
+    if (e_ != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "%s: %s", __func__, cudaGetErrorString(e_)); \
+  } while (0)
+
+extern "C" {
+
+qesb_status qesb_net_pool2(const void *x, void *y, int D, int H, int W, int C, void *stream)
+{
+  if (!x || !y || D % 2 || H % 2 || W % 2 || C <= 0) return qesb_fail(QESB_ERR_ARG, "qesb_net_pool2: bad arguments");
+  const long n = (long)(D / 2) * (H / 2) * (W / 2) * C;
+  k_pool2<<<gs_blocks(n), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)x, (__nv_bfloat16 *)y, D, H, W, C);
+  NET_CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_net_skip_grad(const float *gcat, int ccat, int coff, const float *gpool, const void *e, void *ge,
+                               int D, int H, int W, int C, void *stream)
+{
+  if (!gcat || !e || !ge || coff + C > ccat) return qesb_fail(QESB_ERR_ARG, "qesb_net_skip_grad: bad arguments");
+  const long n = (long)D * H * W * C;
+  k_skip_grad<<<gs_blocks(n), 256, 0, (cudaStream_t)stream>>>(gcat, ccat, coff, gpool, (const __nv_bfloat16 *)e,
+                                                              (__nv_bfloat16 *)ge, D, H, W, C);
+  NET_CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_net_up_grad(const float *gcat, int ccat, const void *x, void *gx, int D, int H, int W, int C,
+                             void *stream)
+{
+  if (!gcat || !x || !gx || C > ccat || D % 2 || H % 2 || W % 2)
+    return qesb_fail(QESB_ERR_ARG, "qesb_net_up_grad: bad arguments");
+  const long n = (long)(D / 2) * (H / 2) * (W / 2) * C;
+  k_up_grad<<<gs_blocks(n), 256, 0, (cudaStream_t)stream>>>(gcat, ccat, (const __nv_bfloat16 *)x, (__nv_bfloat16 *)gx,
+                                                            D, H, W, C);
+  NET_CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_net_to_bf16(const float *g, const void *mask, void *out, long n, void *stream)
+{
+  if (!g || !out || n <= 0) return qesb_fail(QESB_ERR_ARG, "qesb_net_to_bf16: bad arguments");
+  k_to_bf16_masked<<<gs_blocks(n), 256, 0, (cudaStream_t)stream>>>(g, (const __nv_bfloat16 *)mask,
+                                                                   (__nv_bfloat16 *)out, n);
+  NET_CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_net_colsum(const void *g, long V, int C, float *db, void *stream)
+{
+  if (!g || !db || C <= 0 || C > 256) return qesb_fail(QESB_ERR_ARG, "qesb_net_colsum: bad arguments");
+  k_colsum<<<148 * 4, 256, C * sizeof(float), (cudaStream_t)stream>>>((const __nv_bfloat16 *)g, V, C, db);
+  NET_CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_net_mse(const float *yhead, int N, const float *tgt, const float *w, long V, float inv_count,
+                         void *g, double *loss, void *stream)
+{
+  if (!yhead || !tgt || !w || !g || !loss || N < 1) return qesb_fail(QESB_ERR_ARG, "qesb_net_mse: bad arguments");
+  k_mse<<<gs_blocks(V), 256, 0, (cudaStream_t)stream>>>(yhead, N, tgt, w, V, inv_count, (__nv_bfloat16 *)g, loss);
+  NET_CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_net_adam_conv(float *Wt, float *m, float *v, const float *dW, int cin, int cout, int cout_real,
+                               void *Bm, int Kp, void *Bd, int Kd, float lr, float b1, float b2, float eps,
+                               int step, float grad_scale, void *stream)
+{
+  if (!Wt || !m || !v || !dW || !Bm || step < 1) return qesb_fail(QESB_ERR_ARG, "qesb_net_adam_conv: bad arguments");
+  const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+  const long n = 27L * cin * cout;
+  k_adam_conv<<<gs_blocks(n), 256, 0, (cudaStream_t)stream>>>(Wt, m, v, dW, cin, cout, cout_real,
+                                                              (__nv_bfloat16 *)Bm, Kp, (__nv_bfloat16 *)Bd, Kd, lr,
+                                                              b1, b2, eps, c1, c2, grad_scale);
+  NET_CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_net_adam_vec(float *p, float *m, float *v, const float *g, int n, float lr, float b1, float b2,
+                              float eps, int step, float grad_scale, void *stream)
+{
+  if (!p || !m || !v || !g || n <= 0 || step < 1) return qesb_fail(QESB_ERR_ARG, "qesb_net_adam_vec: bad arguments");
+  const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+  k_adam_vec<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(p, m, v, g, n, lr, b1, b2, eps, c1, c2, grad_scale);
+  NET_CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+}  // extern "C"

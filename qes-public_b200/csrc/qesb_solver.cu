@@ -330,6 +330,83 @@ __global__ void k_correct(DevGrid G, const float *__restrict__ L, const float *_
 }
 
 // ---------------------------------------------------------------------------
+// kernels: warm-start network input / target / output
+// ---------------------------------------------------------------------------
+// The network sees planes k in [0, Dn) (Dn = nz-2: every plane but the top
+// boundary) of the X x Y cell grid, channels-last [Dn][Y][X][C] BF16:
+//   0: R / s  (s = max |R| over updated cells)     1: solid (icellflag 0 or 2)
+//   2: dz[k] / mean(dz)                              3: boundary (cell never updated)
+//   4: height of the cell centre / domain height     5..C-1: 0
+__global__ void k_absmax_R(DevGrid G, const float *__restrict__ R, unsigned *__restrict__ out)
+{
+  float mx = 0.0f;
+  const long per = (long)(G.X - 2) * (G.Y - 2) * (G.Z - 2);
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < per; t += (long)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(t % (G.X - 2)), j = 1 + (int)((t / (G.X - 2)) % (G.Y - 2)),
+              k = 1 + (int)(t / ((long)(G.X - 2) * (G.Y - 2)));
+    mx = fmaxf(mx, fabsf(R[G.pad(i, j, k)]));
+  }
+  mx = warp_max_f(mx);
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(mx));
+}
+
+__global__ void k_warm_input(DevGrid G, int Dn, int C, const float *__restrict__ R, const int *__restrict__ flag,
+                             const float *__restrict__ dz, const unsigned *__restrict__ smax, float dz_mean,
+                             float height, uint16_t *__restrict__ x)
+{
+  const float inv_s = 1.0f / fmaxf(__uint_as_float(*smax), 1e-30f);
+  const long V = (long)Dn * G.Y * G.X;
+  for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < V; v += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(v % G.X), j = (int)((v / G.X) % G.Y), k = (int)(v / ((long)G.X * G.Y));
+    const bool upd = i >= 1 && i <= G.X - 2 && j >= 1 && j <= G.Y - 2 && k >= 1 && k <= G.Z - 2;
+    float zc = 0.0f;
+    for (int q = 1; q < k; ++q) zc += dz[q];
+    zc += 0.5f * dz[k];
+    float ch[5];
+    ch[0] = upd ? R[G.pad(i, j, k)] * inv_s : 0.0f;
+    ch[1] = is_solid(flag[G.cell(i, j, k)]) ? 1.0f : 0.0f;
+    ch[2] = dz[k] / dz_mean;
+    ch[3] = upd ? 0.0f : 1.0f;
+    ch[4] = zc / height;
+    uint16_t *dst = x + v * C;
+    for (int c = 0; c < C; ++c) {
+      const float val = c < 5 ? ch[c] : 0.0f;
+      const uint32_t b = __float_as_uint(val);
+      dst[c] = (uint16_t)((b + 0x7FFFu + ((b >> 16) & 1u)) >> 16);  // round to nearest even
+    }
+  }
+}
+
+// Training target lambda / s and weight (1 on updated cells) on the net grid.
+__global__ void k_warm_target(DevGrid G, int Dn, const float *__restrict__ L, const unsigned *__restrict__ smax,
+                              float *__restrict__ tgt, float *__restrict__ w)
+{
+  const float inv_s = 1.0f / fmaxf(__uint_as_float(*smax), 1e-30f);
+  const long V = (long)Dn * G.Y * G.X;
+  for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < V; v += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(v % G.X), j = (int)((v / G.X) % G.Y), k = (int)(v / ((long)G.X * G.Y));
+    const bool upd = i >= 1 && i <= G.X - 2 && j >= 1 && j <= G.Y - 2 && k >= 1 && k <= G.Z - 2;
+    tgt[v] = upd ? L[G.pad(i, j, k)] * inv_s : 0.0f;
+    w[v] = upd ? 1.0f : 0.0f;
+  }
+}
+
+// lambda <- s * prediction on updated cells, 0 on the other cells of planes
+// 1..Z-1, and the ground plane mirrors plane 1 (as after a solve).
+__global__ void k_warm_apply(DevGrid G, int Dn, const float *__restrict__ yhead, int N,
+                             const unsigned *__restrict__ smax, float *__restrict__ L)
+{
+  const float s = __uint_as_float(*smax);
+  const long V = (long)G.Z * G.Y * G.X;
+  for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < V; v += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(v % G.X), j = (int)((v / G.X) % G.Y), k = (int)(v / ((long)G.X * G.Y));
+    const int kk = k == 0 ? 1 : k;
+    const bool upd = i >= 1 && i <= G.X - 2 && j >= 1 && j <= G.Y - 2 && kk >= 1 && kk <= G.Z - 2 && kk < Dn;
+    L[G.pad(i, j, k)] = upd ? s * yhead[(((long)kk * G.Y + j) * G.X + i) * N] : 0.0f;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------
 struct qesb_handle {
@@ -1092,6 +1169,53 @@ qesb_status qesb_get_divergence(qesb_handle *h, float *R)
   if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(h->stream);
   cudaFree(tmp);
   if (e1 != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "qesb_get_divergence: %s", cudaGetErrorString(e1));
+  return QESB_OK;
+}
+
+qesb_status qesb_compute_divergence(qesb_handle *h)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  if (!h->have_inputs) return qesb_fail(QESB_ERR_STATE, "qesb_compute_divergence before qesb_set_inputs");
+  CK(cudaSetDevice(h->device));
+  const DevGrid &G = h->G;
+  k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, h->stream>>>(
+      G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_u0, h->d_v0, h->d_w0,
+      h->d_dz, h->dx, h->dy, h->d_R);
+  CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_warm_input(qesb_handle *h, void *x, int C, unsigned *scale)
+{
+  if (!h || !x || !scale || C < 5) return qesb_fail(QESB_ERR_ARG, "qesb_warm_input: bad arguments");
+  CK(cudaSetDevice(h->device));
+  const DevGrid &G = h->G;
+  CK(cudaMemsetAsync(scale, 0, sizeof(unsigned), h->stream));
+  k_absmax_R<<<148 * 4, 256, 0, h->stream>>>(G, h->d_R, scale);
+  double dzs = 0.0, height = 0.0;
+  for (int k = 1; k < G.Z; ++k) dzs += h->dz[k];
+  for (int k = 1; k < G.Z - 1; ++k) height += h->dz[k];
+  k_warm_input<<<148 * 8, 256, 0, h->stream>>>(G, G.Z - 1, C, h->d_R, h->d_flag, h->d_dz, scale,
+                                               (float)(dzs / (G.Z - 1)), (float)height, (uint16_t *)x);
+  CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_warm_target(qesb_handle *h, float *tgt, float *w, const unsigned *scale)
+{
+  if (!h || !tgt || !w || !scale) return qesb_fail(QESB_ERR_ARG, "qesb_warm_target: bad arguments");
+  CK(cudaSetDevice(h->device));
+  k_warm_target<<<148 * 8, 256, 0, h->stream>>>(h->G, h->G.Z - 1, h->d_lam, scale, tgt, w);
+  CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_warm_apply(qesb_handle *h, const float *yhead, int N, const unsigned *scale)
+{
+  if (!h || !yhead || !scale || N < 1) return qesb_fail(QESB_ERR_ARG, "qesb_warm_apply: bad arguments");
+  CK(cudaSetDevice(h->device));
+  k_warm_apply<<<148 * 8, 256, 0, h->stream>>>(h->G, h->G.Z - 1, yhead, N, scale, h->d_lam);
+  CK(cudaGetLastError());
   return QESB_OK;
 }
 

@@ -1,0 +1,119 @@
+"""Warm-start network: forward and gradients of the tensor-core implementation
+against a float64 CPU implementation of the same network (torch, CPU), and
+the trained network's gain over lambda = 0 on held-out domains."""
+import os
+
+import numpy as np
+import pytest
+
+import qesb
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref_network(net, x, tgt, w, inv_count):
+    """float64 CPU forward/backward of the same encoder-decoder, weights as
+    the kernels see them (BF16-rounded masters, FP32 biases)."""
+    import torch
+    import torch.nn.functional as F
+
+    params = {}
+    for name, L in net.layers.items():
+        Wm = L.W.detach().cpu().to(torch.bfloat16).double().view(27, L.cin, L.cout)
+        wt = Wm.permute(2, 1, 0).reshape(L.cout, L.cin, 3, 3, 3).clone().requires_grad_(True)
+        bt = L.b.detach().cpu().double().clone().requires_grad_(True)
+        params[name] = (wt, bt)
+
+    def conv(name, t, relu=True):
+        wt, bt = params[name]
+        y = F.conv3d(t, wt, bt, padding=1)
+        return torch.relu(y) if relu else y
+
+    up = lambda t: F.interpolate(t, scale_factor=2, mode="nearest")  # noqa: E731
+    e1 = conv("e1", conv("e1a", x))
+    e2 = conv("e2", conv("e2a", F.avg_pool3d(e1, 2)))
+    e3 = conv("e3", conv("e3a", F.avg_pool3d(e2, 2)))
+    e4 = conv("e4", conv("e4a", F.avg_pool3d(e3, 2)))
+    d3 = conv("d3", conv("d3a", torch.cat([up(e4), e3], 1)))
+    d2 = conv("d2", conv("d2a", torch.cat([up(d3), e2], 1)))
+    d1 = conv("d1", conv("d1a", torch.cat([up(d2), e1], 1)))
+    y = conv("head", d1, relu=False)
+    loss = (((y[0, 0] - tgt) * w) ** 2).sum() * inv_count
+    loss.backward()
+    grads = {}
+    for name, (wt, bt) in params.items():
+        L = net.layers[name]
+        grads[name] = (wt.grad.permute(2, 3, 4, 1, 0).reshape(27 * L.cin, L.cout).numpy(), bt.grad.numpy())
+    return y[0, 0].detach().numpy(), float(loss), grads
+
+
+def test_network_forward_and_gradients_match_cpu_oracle():
+    import torch
+
+    from qesb import warmstart as ws
+
+    net = ws.WarmStartNet(device=0, seed=1)
+    # larger-than-init head weights so every layer carries a visible gradient
+    for L in net.layers.values():
+        L.W.mul_(1.5)
+    net.layers["head"].W.normal_(0.0, 0.05)
+    for L in net.layers.values():
+        L.sync()
+    s = ws.Shapes(8, 16, 24)
+    V = s.V(0)
+    rng = np.random.default_rng(0)
+    xin = np.zeros((V, ws.IN_CH), np.float32)
+    xin[:, :5] = rng.standard_normal((V, 5))
+    xb = torch.from_numpy(xin).to(torch.bfloat16)
+    b = net._bufs(s)
+    b["x"].copy_(xb.view(-1).to(net.dev))
+    tgt = torch.from_numpy(rng.standard_normal(V).astype(np.float32)).to(net.dev)
+    wgt = torch.from_numpy((rng.random(V) > 0.2).astype(np.float32)).to(net.dev)
+    inv = 1.0 / float(wgt.sum())
+    y = net.forward(s)
+    net.backward(s, tgt, wgt, inv)
+    torch.cuda.synchronize()
+    net.check_err()
+
+    x64 = xb.double().view(s.D, s.H, s.W, ws.IN_CH).permute(3, 0, 1, 2).unsqueeze(0)
+    yref, lref, gref = _ref_network(net, x64, tgt.cpu().double().view(s.D, s.H, s.W),
+                                    wgt.cpu().double().view(s.D, s.H, s.W), inv)
+    ygpu = y.view(s.D, s.H, s.W, ws.HEAD_N)[..., 0].cpu().double().numpy()
+    # BF16 activations between layers: a few parts per thousand per layer
+    assert np.linalg.norm(ygpu - yref) <= 0.03 * np.linalg.norm(yref)
+    assert abs(float(net.loss.item()) - lref) <= 0.03 * lref
+    for name, L in net.layers.items():
+        gW = L.dW.view(27 * L.cin, L.cout).cpu().double().numpy()
+        gb = L.db.cpu().double().numpy()[: L.cout_real]
+        rW, rb = gref[name][0], gref[name][1][: L.cout_real]
+        cos = float((gW * rW).sum() / (np.linalg.norm(gW) * np.linalg.norm(rW) + 1e-30))
+        assert cos > 0.99, (name, cos)
+        assert np.linalg.norm(gW - rW) <= 0.1 * np.linalg.norm(rW), name
+        assert np.linalg.norm(gb - rb) <= 0.1 * np.linalg.norm(rb) + 1e-6, name
+
+
+def test_trained_network_saves_sweeps():
+    """The committed trained network, on held-out 256x256x64 cities: the warm
+    start reaches the same stopping rule in fewer SOR iterations than lambda = 0,
+    and the winds agree with plain SOR's within the stopping rule's accuracy."""
+    from qesb import warmstart as ws
+
+    if not os.path.exists(ws.DEFAULT_WEIGHTS):
+        pytest.skip("no trained weights committed")
+    net = ws.WarmStartNet(device=0)
+    net.load(ws.DEFAULT_WEIGHTS)
+    gains = []
+    for seed in (900001, 900002):
+        w, _ = qesb.random_city("city256", seed)
+        with qesb.Solver_B200(w.domain, 1e-3) as s:
+            s.set_inputs(w)
+            plain = s.solve(w, 10000, set_inputs=False)
+            up = w.u.copy()
+            s.resetLambda()
+            net.warm_start(s)
+            warm = s.solve(w, 10000, set_inputs=False)
+            uw = w.u.copy()
+        assert warm["converged"] and plain["converged"]
+        gains.append(plain["iterations"] / warm["iterations"])
+        assert np.abs(uw - up).max() < 0.1
+    assert min(gains) > 1.5, gains

@@ -115,6 +115,21 @@ def lib() -> C.CDLL:
                              C.c_int, C.c_int, V, V, V, C.c_int, V, V, V], C.c_int),
             "qesb_conv3d_wgrad": ([V, C.c_int, C.c_int, V, C.c_int, C.c_int, C.c_int, C.c_int, V, C.c_int,
                                    C.c_long, V, V, V], C.c_int),
+            "qesb_compute_divergence": ([V], C.c_int),
+            "qesb_warm_input": ([V, V, C.c_int, V], C.c_int),
+            "qesb_warm_target": ([V, V, V, V], C.c_int),
+            "qesb_warm_apply": ([V, V, C.c_int, V], C.c_int),
+            "qesb_net_pool2": ([V, V, C.c_int, C.c_int, C.c_int, C.c_int, V], C.c_int),
+            "qesb_net_skip_grad": ([V, C.c_int, C.c_int, V, V, V, C.c_int, C.c_int, C.c_int, C.c_int, V],
+                                   C.c_int),
+            "qesb_net_up_grad": ([V, C.c_int, V, V, C.c_int, C.c_int, C.c_int, C.c_int, V], C.c_int),
+            "qesb_net_to_bf16": ([V, V, V, C.c_long, V], C.c_int),
+            "qesb_net_colsum": ([V, C.c_long, C.c_int, V, V], C.c_int),
+            "qesb_net_mse": ([V, C.c_int, V, V, C.c_long, C.c_float, V, V, V], C.c_int),
+            "qesb_net_adam_conv": ([V, V, V, V, C.c_int, C.c_int, C.c_int, V, C.c_int, V, C.c_int, C.c_float,
+                                    C.c_float, C.c_float, C.c_float, C.c_int, C.c_float, V], C.c_int),
+            "qesb_net_adam_vec": ([V, V, V, V, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                                   C.c_float, V], C.c_int),
             "qesb_city_dz": ([C.c_int, C.c_float, C.c_float, _FP], C.c_int),
             "qesb_city_build": ([C.POINTER(Grid), C.c_int, C.POINTER(Building), C.POINTER(Inflow)]
                                 + [V] * 10, C.c_int),

@@ -77,3 +77,17 @@ def test_domain_index_math_matches_reference_formulas():
     assert d.cell(3, 4, 5) == 3 + 4 * 10 + 5 * 70
     assert d.face(3, 4, 5) == 3 + 4 * 11 + 5 * 88
     assert d.z_face[1] == 0 and d.z[1] == 0.5 and d.z_face[0] == -1
+
+
+def test_every_called_entry_point_has_a_ctypes_signature():
+    """Floats and 64-bit sizes only cross ctypes correctly with declared
+    argtypes: every qesb_* the Python package calls must be in the table."""
+    pkg = os.path.join(ROOT, "qes-public_b200", "qesb")
+    called = set()
+    for fn in os.listdir(pkg):
+        if fn.endswith(".py"):
+            called |= set(re.findall(r"lib\(\)\.(qesb_[a-z0-9_]+)", open(os.path.join(pkg, fn)).read()))
+    L = qesb.lib()
+    for name in sorted(called):
+        assert getattr(L, name).argtypes is not None, name
+    assert len(called) >= 20

@@ -600,8 +600,8 @@ __global__ void k_colsum(const __nv_bfloat16 *__restrict__ g, long V, int C, flo
 }
 
 // Loss over valid cells: pred = yhead[v][0] (FP32, head channel stride N),
-// L += sum (pred - tgt)^2 * w[v]; gradient 2 (pred - tgt) w / count into
-// channel 0 of g (BF16 [V][N], other channels zero).
+// L += sum ((pred - tgt) w[v])^2 / count; gradient 2 (pred - tgt) w / count
+// into channel 0 of g (BF16 [V][N], other channels zero).
 __global__ void k_mse(const float *__restrict__ yhead, int N, const float *__restrict__ tgt,
                       const float *__restrict__ w, long V, float inv_count, __nv_bfloat16 *__restrict__ g,
                       double *__restrict__ loss)
@@ -609,7 +609,7 @@ __global__ void k_mse(const float *__restrict__ yhead, int N, const float *__res
   double acc = 0.0;
   for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < V; v += (long)gridDim.x * blockDim.x) {
     const float d = (yhead[v * N] - tgt[v]) * w[v];
-    acc += (double)d * d;
+    acc += (double)d * d * inv_count;
     g[v * N] = __float2bfloat16_rn(2.0f * d * inv_count);
     for (int c = 1; c < N; ++c) g[v * N + c] = __float2bfloat16_rn(0.0f);
   }

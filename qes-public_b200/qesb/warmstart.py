@@ -1,7 +1,8 @@
 """Learned warm start for the lambda solve.
 
-A 4-level 3D convolutional encoder-decoder (channels 16 -> 32 -> 64 -> 128,
-2x2x2 average pooling down, nearest upsampling and skip concatenation up)
+A 3D convolutional encoder-decoder (channels 16 -> 32 -> 64 -> 128 and two
+more 128-channel levels, 2x2x2 average pooling down, nearest upsampling and
+skip concatenation up)
 maps per-cell features of a domain (R / max|R|, solid flag, dz profile,
 boundary flag, height) to lambda / max|R|. Every convolution (forward, input
 gradient, weight gradient) runs in the library's tcgen05 kernels with BF16
@@ -91,62 +92,63 @@ class Shapes:
 
 
 class WarmStartNet:
-    """The encoder-decoder and its training step, on one CUDA device."""
+    """The encoder-decoder and its training step, on one CUDA device.
 
-    CH = (16, 32, 64, 128)
+    Levels l = 0..L-1 with channels CH[l]; level l runs on the grid divided
+    by 2^l. Encoder: two convolutions per level, 2x2x2 average pooling down.
+    Decoder: from level L-2 up to 0, a convolution of [upsample(level l+1),
+    skip e_l] then a second convolution; a linear head gives lambda / max|R|.
+    Six levels put the whole training domain inside the bottleneck's reach.
+    """
 
-    def __init__(self, device=0, seed=0):
+    CH = (16, 32, 64, 128, 128, 128)
+
+    def __init__(self, device=0, seed=0, channels=None):
         import torch
 
         self.torch = torch
         self.dev = torch.device(f"cuda:{device}")
+        self.CH = tuple(channels) if channels else self.CH
         g = torch.Generator().manual_seed(seed)
-        c1, c2, c3, c4 = self.CH
-        T, d = torch, self.dev
+        T, d, C = torch, self.dev, self.CH
         mk = lambda *a, **k: Conv(T, d, *a, gen=g, **k)  # noqa: E731
-        self.layers = {
-            "e1a": mk(IN_CH, 0, c1, 1, 0, cin_real=5), "e1": mk(c1, 0, c1, 1, 0),
-            "e2a": mk(c1, 0, c2, 1, 0), "e2": mk(c2, 0, c2, 1, 0),
-            "e3a": mk(c2, 0, c3, 1, 0), "e3": mk(c3, 0, c3, 1, 0),
-            "e4a": mk(c3, 0, c4, 1, 0), "e4": mk(c4, 0, c4, 1, 0),
-            "d3a": mk(c4, c3, c3, 1, 1), "d3": mk(c3, 0, c3, 1, 0),
-            "d2a": mk(c3, c2, c2, 1, 1), "d2": mk(c2, 0, c2, 1, 0),
-            "d1a": mk(c2, c1, c1, 1, 1), "d1": mk(c1, 0, c1, 1, 0),
-            "head": mk(c1, 0, HEAD_N, 0, 0, cout_real=1, init_std=1e-3),
-        }
+        L = len(C)
+        self.nlev = L
+        self.layers = {}
+        for l in range(L):
+            cin = IN_CH if l == 0 else C[l - 1]
+            self.layers[f"e{l}a"] = mk(cin, 0, C[l], 1, 0, **({"cin_real": 5} if l == 0 else {}))
+            self.layers[f"e{l}"] = mk(C[l], 0, C[l], 1, 0)
+        for l in range(L - 2, -1, -1):
+            self.layers[f"d{l}a"] = mk(C[l + 1], C[l], C[l], 1, 1)
+            self.layers[f"d{l}"] = mk(C[l], 0, C[l], 1, 0)
+        self.layers["head"] = mk(C[0], 0, HEAD_N, 0, 0, cout_real=1, init_std=1e-3)
         self.err = torch.zeros(1, dtype=torch.int32, device=d)
         self.loss = torch.zeros(1, dtype=torch.float64, device=d)
         self.step_count = 0
         self._buf = {}
-        self._shape = None
 
     # ------------------------------------------------------------------ buffers
     def _bufs(self, s: Shapes):
         key = (s.D, s.H, s.W)
         if key in self._buf:
             return self._buf[key]
-        T, d = self.torch, self.dev
+        if any(x % (1 << (self.nlev - 1)) for x in (s.D, s.H, s.W)):
+            raise ValueError(f"grid {key} not divisible by {1 << (self.nlev - 1)}")
+        T, d, C, L = self.torch, self.dev, self.CH, self.nlev
         bf = lambda l, c: T.zeros(s.V(l) * c, dtype=T.bfloat16, device=d)  # noqa: E731
         f32 = lambda l, c: T.zeros(s.V(l) * c, dtype=T.float32, device=d)  # noqa: E731
-        c1, c2, c3, c4 = self.CH
-        b = {
-            "x": bf(0, IN_CH),
-            "e1a": bf(0, c1), "e1": bf(0, c1), "p1": bf(1, c1),
-            "e2a": bf(1, c2), "e2": bf(1, c2), "p2": bf(2, c2),
-            "e3a": bf(2, c3), "e3": bf(2, c3), "p3": bf(3, c3),
-            "e4a": bf(3, c4), "e4": bf(3, c4),
-            "d3a": bf(2, c3), "d3": bf(2, c3),
-            "d2a": bf(1, c2), "d2": bf(1, c2),
-            "d1a": bf(0, c1), "d1": bf(0, c1),
-            "y": f32(0, HEAD_N),
-            # gradients
-            "g0": bf(0, HEAD_N), "gA0": bf(0, c1), "gB0": bf(0, c1),
-            "gA1": bf(1, c2), "gB1": bf(1, c2), "gA2": bf(2, c3), "gB2": bf(2, c3),
-            "gA3": bf(3, c4), "gB3": bf(3, c4),
-            "gup1": f32(0, c2), "gsk1": f32(0, c1), "gup2": f32(1, c3), "gsk2": f32(1, c2),
-            "gup3": f32(2, c4), "gsk3": f32(2, c3),
-            "gp1": f32(1, c1), "gp2": f32(2, c2), "gp3": f32(3, c3),
-        }
+        b = {"x": bf(0, IN_CH), "y": f32(0, HEAD_N), "g0": bf(0, HEAD_N)}
+        for l in range(L):
+            b[f"e{l}a"], b[f"e{l}"] = bf(l, C[l]), bf(l, C[l])
+            b[f"gA{l}"], b[f"gB{l}"] = bf(l, C[l]), bf(l, C[l])
+            if l > 0:
+                b[f"p{l}"] = bf(l, C[l - 1])      # pool of e_{l-1}
+                b[f"gp{l}"] = f32(l, C[l - 1])    # its gradient
+        for l in range(L - 1):
+            b[f"d{l}a"], b[f"d{l}"] = bf(l, C[l]), bf(l, C[l])
+            b[f"gup{l}"] = f32(l, C[l + 1])       # gradient of upsample(level l+1) at level l
+            b[f"gsk{l}"] = f32(l, C[l])           # gradient of the skip e_l from the decoder
         self._buf[key] = b
         return b
 
@@ -171,101 +173,61 @@ class WarmStartNet:
                                       _p(self.err), stream))
         check(lib().qesb_net_colsum(_p(gy), V, L.cout, _p(L.db), stream))
 
-    def _pool(self, x, y, lvl, s, c, stream=None):
-        D, H, W = s.level(lvl)
-        check(lib().qesb_net_pool2(_p(x), _p(y), D, H, W, c, stream))
-
     # ------------------------------------------------------------------ passes
     def forward(self, s: Shapes, stream=None):
         """Runs the network on buffer 'x' of shape s; returns the FP32 head
         output [V][16] (channel 0 = lambda / max|R|)."""
-        b, Ls = self._bufs(s), self.layers
-        c1, c2, c3, _ = self.CH
-        self._conv(Ls["e1a"], b["x"], None, 0, s, y=b["e1a"], stream=stream)
-        self._conv(Ls["e1"], b["e1a"], None, 0, s, y=b["e1"], stream=stream)
-        self._pool(b["e1"], b["p1"], 0, s, c1, stream)
-        self._conv(Ls["e2a"], b["p1"], None, 1, s, y=b["e2a"], stream=stream)
-        self._conv(Ls["e2"], b["e2a"], None, 1, s, y=b["e2"], stream=stream)
-        self._pool(b["e2"], b["p2"], 1, s, c2, stream)
-        self._conv(Ls["e3a"], b["p2"], None, 2, s, y=b["e3a"], stream=stream)
-        self._conv(Ls["e3"], b["e3a"], None, 2, s, y=b["e3"], stream=stream)
-        self._pool(b["e3"], b["p3"], 2, s, c3, stream)
-        self._conv(Ls["e4a"], b["p3"], None, 3, s, y=b["e4a"], stream=stream)
-        self._conv(Ls["e4"], b["e4a"], None, 3, s, y=b["e4"], stream=stream)
-        self._conv(Ls["d3a"], b["e4"], b["e3"], 2, s, y=b["d3a"], stream=stream)
-        self._conv(Ls["d3"], b["d3a"], None, 2, s, y=b["d3"], stream=stream)
-        self._conv(Ls["d2a"], b["d3"], b["e2"], 1, s, y=b["d2a"], stream=stream)
-        self._conv(Ls["d2"], b["d2a"], None, 1, s, y=b["d2"], stream=stream)
-        self._conv(Ls["d1a"], b["d2"], b["e1"], 0, s, y=b["d1a"], stream=stream)
-        self._conv(Ls["d1"], b["d1a"], None, 0, s, y=b["d1"], stream=stream)
-        self._conv(Ls["head"], b["d1"], None, 0, s, yf=b["y"], stream=stream)
+        b, Ls, C, L = self._bufs(s), self.layers, self.CH, self.nlev
+        for l in range(L):
+            xin = b["x"] if l == 0 else b[f"p{l}"]
+            if l > 0:
+                D, H, W = s.level(l - 1)
+                check(lib().qesb_net_pool2(_p(b[f"e{l - 1}"]), _p(b[f"p{l}"]), D, H, W, C[l - 1], stream))
+            self._conv(Ls[f"e{l}a"], xin, None, l, s, y=b[f"e{l}a"], stream=stream)
+            self._conv(Ls[f"e{l}"], b[f"e{l}a"], None, l, s, y=b[f"e{l}"], stream=stream)
+        for l in range(L - 2, -1, -1):
+            below = b[f"e{l + 1}"] if l == L - 2 else b[f"d{l + 1}"]
+            self._conv(Ls[f"d{l}a"], below, b[f"e{l}"], l, s, y=b[f"d{l}a"], stream=stream)
+            self._conv(Ls[f"d{l}"], b[f"d{l}a"], None, l, s, y=b[f"d{l}"], stream=stream)
+        self._conv(Ls["head"], b["d0"], None, 0, s, yf=b["y"], stream=stream)
         return b["y"]
 
     def backward(self, s: Shapes, tgt, w, inv_count, stream=None):
         """Loss (weighted MSE on channel 0) and all parameter gradients into
         each layer's dW / db (zeroed here first)."""
-        b, Ls, T = self._bufs(s), self.layers, self.torch
-        c1, c2, c3, c4 = self.CH
-        for L in Ls.values():
-            L.dW.zero_()
-            L.db.zero_()
+        b, Ls, C, L = self._bufs(s), self.layers, self.CH, self.nlev
+        for layer in Ls.values():
+            layer.dW.zero_()
+            layer.db.zero_()
         self.loss.zero_()
         check(lib().qesb_net_mse(_p(b["y"]), HEAD_N, _p(tgt), _p(w), s.V(0), float(inv_count), _p(b["g0"]),
                                  _p(self.loss), stream))
-        # head and the level-1 decoder
-        self._wgrad(Ls["head"], b["d1"], None, b["g0"], 0, s, stream)
-        self._dgrad(Ls["head"], b["g0"], 0, s, 0, c1, y=b["gA0"], mask=b["d1"], stream=stream)
-        self._wgrad(Ls["d1"], b["d1a"], None, b["gA0"], 0, s, stream)
-        self._dgrad(Ls["d1"], b["gA0"], 0, s, 0, c1, y=b["gB0"], mask=b["d1a"], stream=stream)
-        self._wgrad(Ls["d1a"], b["d2"], b["e1"], b["gB0"], 0, s, stream)
-        self._dgrad(Ls["d1a"], b["gB0"], 0, s, 0, c2, yf=b["gup1"], stream=stream)
-        self._dgrad(Ls["d1a"], b["gB0"], 0, s, c2, c1, yf=b["gsk1"], stream=stream)
-        D, H, W = s.level(0)
-        check(lib().qesb_net_up_grad(_p(b["gup1"]), c2, _p(b["d2"]), _p(b["gA1"]), D, H, W, c2, stream))
-        # level 2 decoder
-        self._wgrad(Ls["d2"], b["d2a"], None, b["gA1"], 1, s, stream)
-        self._dgrad(Ls["d2"], b["gA1"], 1, s, 0, c2, y=b["gB1"], mask=b["d2a"], stream=stream)
-        self._wgrad(Ls["d2a"], b["d3"], b["e2"], b["gB1"], 1, s, stream)
-        self._dgrad(Ls["d2a"], b["gB1"], 1, s, 0, c3, yf=b["gup2"], stream=stream)
-        self._dgrad(Ls["d2a"], b["gB1"], 1, s, c3, c2, yf=b["gsk2"], stream=stream)
-        D, H, W = s.level(1)
-        check(lib().qesb_net_up_grad(_p(b["gup2"]), c3, _p(b["d3"]), _p(b["gA2"]), D, H, W, c3, stream))
-        # level 3 decoder
-        self._wgrad(Ls["d3"], b["d3a"], None, b["gA2"], 2, s, stream)
-        self._dgrad(Ls["d3"], b["gA2"], 2, s, 0, c3, y=b["gB2"], mask=b["d3a"], stream=stream)
-        self._wgrad(Ls["d3a"], b["e4"], b["e3"], b["gB2"], 2, s, stream)
-        self._dgrad(Ls["d3a"], b["gB2"], 2, s, 0, c4, yf=b["gup3"], stream=stream)
-        self._dgrad(Ls["d3a"], b["gB2"], 2, s, c4, c3, yf=b["gsk3"], stream=stream)
-        D, H, W = s.level(2)
-        check(lib().qesb_net_up_grad(_p(b["gup3"]), c4, _p(b["e4"]), _p(b["gA3"]), D, H, W, c4, stream))
-        # bottom
-        self._wgrad(Ls["e4"], b["e4a"], None, b["gA3"], 3, s, stream)
-        self._dgrad(Ls["e4"], b["gA3"], 3, s, 0, c4, y=b["gB3"], mask=b["e4a"], stream=stream)
-        self._wgrad(Ls["e4a"], b["p3"], None, b["gB3"], 3, s, stream)
-        self._dgrad(Ls["e4a"], b["gB3"], 3, s, 0, c3, yf=b["gp3"], stream=stream)
-        # encoder level 3
-        D, H, W = s.level(2)
-        check(lib().qesb_net_skip_grad(_p(b["gsk3"]), c3, 0, _p(b["gp3"]), _p(b["e3"]), _p(b["gA2"]), D, H, W, c3,
-                                       stream))
-        self._wgrad(Ls["e3"], b["e3a"], None, b["gA2"], 2, s, stream)
-        self._dgrad(Ls["e3"], b["gA2"], 2, s, 0, c3, y=b["gB2"], mask=b["e3a"], stream=stream)
-        self._wgrad(Ls["e3a"], b["p2"], None, b["gB2"], 2, s, stream)
-        self._dgrad(Ls["e3a"], b["gB2"], 2, s, 0, c2, yf=b["gp2"], stream=stream)
-        # encoder level 2
-        D, H, W = s.level(1)
-        check(lib().qesb_net_skip_grad(_p(b["gsk2"]), c2, 0, _p(b["gp2"]), _p(b["e2"]), _p(b["gA1"]), D, H, W, c2,
-                                       stream))
-        self._wgrad(Ls["e2"], b["e2a"], None, b["gA1"], 1, s, stream)
-        self._dgrad(Ls["e2"], b["gA1"], 1, s, 0, c2, y=b["gB1"], mask=b["e2a"], stream=stream)
-        self._wgrad(Ls["e2a"], b["p1"], None, b["gB1"], 1, s, stream)
-        self._dgrad(Ls["e2a"], b["gB1"], 1, s, 0, c1, yf=b["gp1"], stream=stream)
-        # encoder level 1
-        D, H, W = s.level(0)
-        check(lib().qesb_net_skip_grad(_p(b["gsk1"]), c1, 0, _p(b["gp1"]), _p(b["e1"]), _p(b["gA0"]), D, H, W, c1,
-                                       stream))
-        self._wgrad(Ls["e1"], b["e1a"], None, b["gA0"], 0, s, stream)
-        self._dgrad(Ls["e1"], b["gA0"], 0, s, 0, c1, y=b["gB0"], mask=b["e1a"], stream=stream)
-        self._wgrad(Ls["e1a"], b["x"], None, b["gB0"], 0, s, stream)
+        # head: gradient into d0 (through d0's ReLU)
+        self._wgrad(Ls["head"], b["d0"], None, b["g0"], 0, s, stream)
+        self._dgrad(Ls["head"], b["g0"], 0, s, 0, C[0], y=b["gA0"], mask=b["d0"], stream=stream)
+        # decoder, top to bottom: gA{l} holds the pre-activation gradient of d{l}
+        for l in range(L - 1):
+            self._wgrad(Ls[f"d{l}"], b[f"d{l}a"], None, b[f"gA{l}"], l, s, stream)
+            self._dgrad(Ls[f"d{l}"], b[f"gA{l}"], l, s, 0, C[l], y=b[f"gB{l}"], mask=b[f"d{l}a"], stream=stream)
+            below = b[f"e{l + 1}"] if l == L - 2 else b[f"d{l + 1}"]
+            self._wgrad(Ls[f"d{l}a"], below, b[f"e{l}"], b[f"gB{l}"], l, s, stream)
+            self._dgrad(Ls[f"d{l}a"], b[f"gB{l}"], l, s, 0, C[l + 1], yf=b[f"gup{l}"], stream=stream)
+            self._dgrad(Ls[f"d{l}a"], b[f"gB{l}"], l, s, C[l + 1], C[l], yf=b[f"gsk{l}"], stream=stream)
+            D, H, W = s.level(l)
+            check(lib().qesb_net_up_grad(_p(b[f"gup{l}"]), C[l + 1], _p(below), _p(b[f"gA{l + 1}"]), D, H, W,
+                                         C[l + 1], stream))
+        # encoder, bottom to top: gA{l} holds the pre-activation gradient of e{l}
+        for l in range(L - 1, -1, -1):
+            if l < L - 1:
+                D, H, W = s.level(l)
+                check(lib().qesb_net_skip_grad(_p(b[f"gsk{l}"]), C[l], 0, _p(b[f"gp{l + 1}"]), _p(b[f"e{l}"]),
+                                               _p(b[f"gA{l}"]), D, H, W, C[l], stream))
+            self._wgrad(Ls[f"e{l}"], b[f"e{l}a"], None, b[f"gA{l}"], l, s, stream)
+            self._dgrad(Ls[f"e{l}"], b[f"gA{l}"], l, s, 0, C[l], y=b[f"gB{l}"], mask=b[f"e{l}a"], stream=stream)
+            xin = b["x"] if l == 0 else b[f"p{l}"]
+            self._wgrad(Ls[f"e{l}a"], xin, None, b[f"gB{l}"], l, s, stream)
+            if l > 0:
+                self._dgrad(Ls[f"e{l}a"], b[f"gB{l}"], l, s, 0, C[l - 1], yf=b[f"gp{l}"], stream=stream)
 
     def adam(self, lr, stream=None, b1=0.9, b2=0.999, eps=1e-8):
         self.step_count += 1
@@ -273,8 +235,7 @@ class WarmStartNet:
             check(lib().qesb_net_adam_conv(_p(L.W), _p(L.mW), _p(L.vW), _p(L.dW), L.cin, L.cout, L.cout_real,
                                            _p(L.Bm), L.Kp, _p(L.Bd), L.Kd, lr, b1, b2, eps, self.step_count, 1.0,
                                            stream))
-            n = L.cout_real
-            check(lib().qesb_net_adam_vec(_p(L.b), _p(L.mb), _p(L.vb), _p(L.db), n, lr, b1, b2, eps,
+            check(lib().qesb_net_adam_vec(_p(L.b), _p(L.mb), _p(L.vb), _p(L.db), L.cout_real, lr, b1, b2, eps,
                                           self.step_count, 1.0, stream))
 
     def check_err(self):
@@ -298,7 +259,7 @@ class WarmStartNet:
 
     # ------------------------------------------------------------------ persistence
     def state(self) -> dict:
-        out = {}
+        out = {"channels": np.array(self.CH)}
         for name, L in self.layers.items():
             out[f"{name}.W"] = L.W.cpu().numpy()
             out[f"{name}.b"] = L.b.cpu().numpy()
@@ -308,19 +269,20 @@ class WarmStartNet:
     def save(self, path):
         np.savez_compressed(path, **self.state())
 
-    def load(self, path):
+    @classmethod
+    def from_file(cls, path, device=0):
         z = np.load(path)
-        for name, L in self.layers.items():
-            L.W.copy_(self.torch.from_numpy(z[f"{name}.W"]).to(self.dev))
-            L.b.copy_(self.torch.from_numpy(z[f"{name}.b"]).to(self.dev))
+        net = cls(device=device, channels=tuple(int(c) for c in z["channels"]))
+        for name, L in net.layers.items():
+            L.W.copy_(net.torch.from_numpy(z[f"{name}.W"]).to(net.dev))
+            L.b.copy_(net.torch.from_numpy(z[f"{name}.b"]).to(net.dev))
             L.sync()
-        self.step_count = int(z["step"])
+        net.step_count = int(z["step"])
+        return net
 
 
 def shapes_of(solver: Solver_B200) -> Shapes:
     Nx, Ny, Nz = solver.domain.base
-    if Nx % 8 or Ny % 8 or Nz % 8:
-        raise ValueError("the warm-start network needs Nx, Ny, Nz divisible by 8")
     return Shapes(Nz, Ny, Nx)
 
 

@@ -30,14 +30,16 @@ def _ref_network(net, x, tgt, w, inv_count):
         return torch.relu(y) if relu else y
 
     up = lambda t: F.interpolate(t, scale_factor=2, mode="nearest")  # noqa: E731
-    e1 = conv("e1", conv("e1a", x))
-    e2 = conv("e2", conv("e2a", F.avg_pool3d(e1, 2)))
-    e3 = conv("e3", conv("e3a", F.avg_pool3d(e2, 2)))
-    e4 = conv("e4", conv("e4a", F.avg_pool3d(e3, 2)))
-    d3 = conv("d3", conv("d3a", torch.cat([up(e4), e3], 1)))
-    d2 = conv("d2", conv("d2a", torch.cat([up(d3), e2], 1)))
-    d1 = conv("d1", conv("d1a", torch.cat([up(d2), e1], 1)))
-    y = conv("head", d1, relu=False)
+    e = []
+    t = x
+    for l in range(net.nlev):
+        if l > 0:
+            t = F.avg_pool3d(e[-1], 2)
+        e.append(conv(f"e{l}", conv(f"e{l}a", t)))
+    d = e[-1]
+    for l in range(net.nlev - 2, -1, -1):
+        d = conv(f"d{l}", conv(f"d{l}a", torch.cat([up(d), e[l]], 1)))
+    y = conv("head", d, relu=False)
     loss = (((y[0, 0] - tgt) * w) ** 2).sum() * inv_count
     loss.backward()
     grads = {}
@@ -59,7 +61,7 @@ def test_network_forward_and_gradients_match_cpu_oracle():
     net.layers["head"].W.normal_(0.0, 0.05)
     for L in net.layers.values():
         L.sync()
-    s = ws.Shapes(8, 16, 24)
+    s = ws.Shapes(32, 32, 64)
     V = s.V(0)
     rng = np.random.default_rng(0)
     xin = np.zeros((V, ws.IN_CH), np.float32)
@@ -100,8 +102,7 @@ def test_trained_network_saves_sweeps():
 
     if not os.path.exists(ws.DEFAULT_WEIGHTS):
         pytest.skip("no trained weights committed")
-    net = ws.WarmStartNet(device=0)
-    net.load(ws.DEFAULT_WEIGHTS)
+    net = ws.WarmStartNet.from_file(ws.DEFAULT_WEIGHTS, device=0)
     gains = []
     for seed in (900001, 900002):
         w, _ = qesb.random_city("city256", seed)

@@ -197,6 +197,10 @@ qesb_status qesb_net_to_bf16(const float *g, const void *mask, void *out, long n
 qesb_status qesb_net_colsum(const void *g, long V, int C, float *db, void *stream);
 qesb_status qesb_net_mse(const float *yhead, int N, const float *tgt, const float *w, long V,
                          float inv_count, void *g, double *loss, void *stream);
+/* Adds a low-frequency term: the weighted error averaged over F^3 blocks,
+ * beta * mean(block error^2), to *loss and its gradient to g (channel 0). */
+qesb_status qesb_net_mse_coarse(const float *yhead, int N, const float *tgt, const float *w, int D,
+                                int H, int W, int F, float beta, void *g, double *loss, void *stream);
 qesb_status qesb_net_adam_conv(float *Wt, float *m, float *v, const float *dW, int cin, int cout,
                                int cout_real, void *Bm, int Kp, void *Bd, int Kd, float lr, float b1,
                                float b2, float eps, int step, float grad_scale, void *stream);

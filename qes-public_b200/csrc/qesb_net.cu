@@ -617,6 +617,37 @@ __global__ void k_mse(const float *__restrict__ yhead, int N, const float *__res
   if ((threadIdx.x & 31) == 0) atomicAdd(loss, acc);
 }
 
+// Low-frequency loss term: the error e = (pred - tgt) w averaged over F x F x F
+// blocks (one thread per block), E_c; loss += beta * sum_c E_c^2 / nc and
+// g[v][0] += 2 beta E_c w[v] / (F^3 nc) on the block's cells. Weights the
+// smooth part of the error, which red-black SOR removes slowest.
+__global__ void k_mse_coarse(const float *__restrict__ yhead, int N, const float *__restrict__ tgt,
+                             const float *__restrict__ w, int D, int H, int W, int F, float beta,
+                             __nv_bfloat16 *__restrict__ g, double *__restrict__ loss)
+{
+  const int d = D / F, h = H / F, ww = W / F;
+  const long nc = (long)d * h * ww;
+  const float f3 = (float)(F * F * F);
+  double acc = 0.0;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < nc; c += (long)gridDim.x * blockDim.x) {
+    const int cx = (int)(c % ww), cy = (int)((c / ww) % h), cz = (int)(c / ((long)ww * h));
+    float e = 0.0f;
+    for (int q = 0; q < F * F * F; ++q) {
+      const long v = ((long)(cz * F + q / (F * F)) * H + cy * F + (q / F) % F) * W + cx * F + q % F;
+      e += (yhead[v * N] - tgt[v]) * w[v];
+    }
+    e /= f3;
+    acc += (double)beta * e * e / (double)nc;
+    const float gs = 2.0f * beta * e / (f3 * (float)nc);
+    for (int q = 0; q < F * F * F; ++q) {
+      const long v = ((long)(cz * F + q / (F * F)) * H + cy * F + (q / F) % F) * W + cx * F + q % F;
+      g[v * N] = __float2bfloat16_rn(__bfloat162float(g[v * N]) + gs * w[v]);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, acc);
+}
+
 // Adam on one conv layer (Kingma & Ba 2015): master weights W[27*cin][cout]
 // (row t*cin + c), moments m, v, gradient dW; bias likewise. Writes the two
 // BF16 GEMM layouts: Bm[cout][Kp] (k = t*cin + c) and Bd[cin][Kd] (k = t*cout + o).
@@ -725,6 +756,18 @@ qesb_status qesb_net_mse(const float *yhead, int N, const float *tgt, const floa
 {
   if (!yhead || !tgt || !w || !g || !loss || N < 1) return qesb_fail(QESB_ERR_ARG, "qesb_net_mse: bad arguments");
   k_mse<<<gs_blocks(V), 256, 0, (cudaStream_t)stream>>>(yhead, N, tgt, w, V, inv_count, (__nv_bfloat16 *)g, loss);
+  NET_CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_net_mse_coarse(const float *yhead, int N, const float *tgt, const float *w, int D, int H, int W,
+                                int F, float beta, void *g, double *loss, void *stream)
+{
+  if (!yhead || !tgt || !w || !g || !loss || F < 1 || D % F || H % F || W % F)
+    return qesb_fail(QESB_ERR_ARG, "qesb_net_mse_coarse: bad arguments");
+  const long nc = (long)(D / F) * (H / F) * (W / F);
+  k_mse_coarse<<<gs_blocks(nc, 128), 128, 0, (cudaStream_t)stream>>>(yhead, N, tgt, w, D, H, W, F, beta,
+                                                                       (__nv_bfloat16 *)g, loss);
   NET_CK(cudaGetLastError());
   return QESB_OK;
 }

@@ -126,6 +126,8 @@ def lib() -> C.CDLL:
             "qesb_net_to_bf16": ([V, V, V, C.c_long, V], C.c_int),
             "qesb_net_colsum": ([V, C.c_long, C.c_int, V, V], C.c_int),
             "qesb_net_mse": ([V, C.c_int, V, V, C.c_long, C.c_float, V, V, V], C.c_int),
+            "qesb_net_mse_coarse": ([V, C.c_int, V, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, V, V, V],
+                                    C.c_int),
             "qesb_net_adam_conv": ([V, V, V, V, C.c_int, C.c_int, C.c_int, V, C.c_int, V, C.c_int, C.c_float,
                                     C.c_float, C.c_float, C.c_float, C.c_int, C.c_float, V], C.c_int),
             "qesb_net_adam_vec": ([V, V, V, V, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,

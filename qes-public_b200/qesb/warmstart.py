@@ -192,9 +192,10 @@ class WarmStartNet:
         self._conv(Ls["head"], b["d0"], None, 0, s, yf=b["y"], stream=stream)
         return b["y"]
 
-    def backward(self, s: Shapes, tgt, w, inv_count, stream=None):
-        """Loss (weighted MSE on channel 0) and all parameter gradients into
-        each layer's dW / db (zeroed here first)."""
+    def backward(self, s: Shapes, tgt, w, inv_count, stream=None, coarse=((8, 0.0),)):
+        """Loss (weighted MSE on channel 0, plus beta * MSE of the F^3-block
+        means of the error for each (F, beta) in `coarse`) and all parameter
+        gradients into each layer's dW / db (zeroed here first)."""
         b, Ls, C, L = self._bufs(s), self.layers, self.CH, self.nlev
         for layer in Ls.values():
             layer.dW.zero_()
@@ -202,6 +203,10 @@ class WarmStartNet:
         self.loss.zero_()
         check(lib().qesb_net_mse(_p(b["y"]), HEAD_N, _p(tgt), _p(w), s.V(0), float(inv_count), _p(b["g0"]),
                                  _p(self.loss), stream))
+        for F, beta in coarse:
+            if beta > 0:
+                check(lib().qesb_net_mse_coarse(_p(b["y"]), HEAD_N, _p(tgt), _p(w), s.D, s.H, s.W, F, float(beta),
+                                                _p(b["g0"]), _p(self.loss), stream))
         # head: gradient into d0 (through d0's ReLU)
         self._wgrad(Ls["head"], b["d0"], None, b["g0"], 0, s, stream)
         self._dgrad(Ls["head"], b["g0"], 0, s, 0, C[0], y=b["gA0"], mask=b["d0"], stream=stream)

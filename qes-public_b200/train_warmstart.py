@@ -75,7 +75,7 @@ def generate(net, n, workload, target_iters, threads=8):
     return X, T, weight, s
 
 
-def train(net, X, T, weight, s, epochs, lr0, log_every=200):
+def train(net, X, T, weight, s, epochs, lr0, log_every=200, coarse=((8, 0.0),)):
     torch = net.torch
     n = X.shape[0]
     V = s.V(0)
@@ -93,7 +93,7 @@ def train(net, X, T, weight, s, epochs, lr0, log_every=200):
             lr = 1e-5 + 0.5 * (lr0 - 1e-5) * (1 + math.cos(math.pi * step / total))
             xb[:, :5].copy_(X[i])
             net.forward(s)
-            net.backward(s, T[i], weight, inv)
+            net.backward(s, T[i], weight, inv, coarse=coarse)
             net.adam(lr)
             step += 1
             if step % log_every == 0 or step == total:
@@ -146,13 +146,15 @@ def main():
     ap.add_argument("--target-iters", type=int, default=4000)
     ap.add_argument("--train-workload", default="city128")
     ap.add_argument("--eval-workload", default="city256")
+    ap.add_argument("--coarse-beta", type=float, default=0.0,
+                    help="weight of the 8x8x8-block error term of the loss (0: plain MSE)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     net = ws.WarmStartNet(device=0, seed=0)
     t0 = time.time()
     X, T, weight, s = generate(net, args.train, args.train_workload, args.target_iters)
     t_gen = time.time() - t0
-    losses, t_train = train(net, X, T, weight, s, args.epochs, args.lr)
+    losses, t_train = train(net, X, T, weight, s, args.epochs, args.lr, coarse=((8, args.coarse_beta),))
     del X, T
     wpath = os.path.join(args.out, "warmstart_city.npz")
     net.save(wpath)
@@ -163,7 +165,8 @@ def main():
     ms_w = np.array([r["warm_ms"] for r in rows], float)
     report = {
         "train": {"n": args.train, "workload": args.train_workload, "epochs": args.epochs, "target_iters":
-                  args.target_iters, "generate_s": t_gen, "train_s": t_train, "losses": losses},
+                  args.target_iters, "coarse_beta": args.coarse_beta, "generate_s": t_gen, "train_s": t_train,
+                  "losses": losses},
         "eval": {"n": args.eval, "workload": args.eval_workload, "tol": TOL,
                  "plain_iters_mean": it_p.mean(), "warm_iters_mean": it_w.mean(),
                  "iters_ratio_mean": float((it_p / it_w).mean()),

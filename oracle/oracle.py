@@ -20,10 +20,12 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_PATH = os.path.join(HERE, "_build", "libqesoracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libqesref.so")
+REF_GPU_PATH = os.path.join(HERE, "_ref", "libqesref_gpu.so")
 
 _V = C.c_void_p
 _port = None
 _ref = None
+_ref_gpu = None
 
 
 def _p(a):
@@ -180,3 +182,53 @@ def ref_solve(dom, w, tol, itermax, kind=0, lam=None, want_lambda=True):
                            _p(w.w0), float(tol), int(itermax), _p(lam), _p(u), _p(v), _p(ww),
                            _p(L))
     return u, v, ww, L, t
+
+
+# ----------------------------------------------------------------------------- reference GPU solver
+def ref_gpu_available() -> bool:
+    return os.path.exists(REF_GPU_PATH)
+
+
+def ref_gpu() -> C.CDLL:
+    global _ref_gpu
+    if _ref_gpu is None:
+        L = C.CDLL(REF_GPU_PATH)
+        i, f = C.c_int, C.c_float
+        L.qesref_solve_gpu.argtypes = [i, i, i, f, f] + [_V] * 11 + [f, i] + [_V] * 3
+        L.qesref_solve_gpu.restype = C.c_double
+        _ref_gpu = L
+    return _ref_gpu
+
+
+def capture_stdout(fn):
+    """Runs fn with file descriptor 1 redirected; returns (result, text)."""
+    import sys
+    import tempfile
+
+    fd = sys.stdout.fileno()
+    sys.stdout.flush()
+    saved = os.dup(fd)
+    with tempfile.TemporaryFile(mode="w+") as tmp:
+        os.dup2(tmp.fileno(), fd)
+        try:
+            res = fn()
+        finally:
+            sys.stdout.flush()
+            os.dup2(saved, fd)
+            os.close(saved)
+        tmp.seek(0)
+        return res, tmp.read()
+
+
+def ref_solve_gpu(dom, w, tol, itermax):
+    """The reference's Solver_GPU_GlobalMemory::solve (timing comparator).
+    Returns (u, v, w, seconds, iterations)."""
+    import re
+
+    nf = dom.numFaceCentered()
+    u, v, ww = (np.zeros(nf, np.float32) for _ in range(3))
+    t, text = capture_stdout(lambda: ref_gpu().qesref_solve_gpu(
+        *_dims(dom), _p(dom.dz_array), _p(w.e), _p(w.f), _p(w.g), _p(w.h), _p(w.m), _p(w.n),
+        _p(w.icellflag), _p(w.u0), _p(w.v0), _p(w.w0), float(tol), int(itermax), _p(u), _p(v), _p(ww)))
+    m = re.findall(r"Residual after (\d+) itertations", text)
+    return u, v, ww, t, int(m[-1]) if m else -1

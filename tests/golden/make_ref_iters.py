@@ -5,7 +5,7 @@ Stopping rule: the reference loop `while (iter < itermax && max_error > tol)`
 with tol = 1e-3 (reachable in FP32; the reference's 1e-9 is not) and
 itermax = 10000. Run where the reference build oracle/_ref exists:
 
-    OMP_NUM_THREADS=1 python tests/golden/make_ref_iters.py [workload ...]
+    OMP_NUM_THREADS=1 python tests/golden/make_ref_iters.py [workload[:seed] ...]
 
 Solver_CPU_RB runs single-threaded here: its max_error reset races between
 OpenMP threads (Solver_CPU_RB.cpp:166) and can end the loop early.
@@ -30,7 +30,9 @@ TOL, ITERMAX = 1e-3, 10000
 
 
 def run(workload, kind):
-    w, c = qesb.random_city(workload, 0) if workload != "cuboid100" else (qesb.cuboid100(), None)
+    name, _, seed = workload.partition(":")
+    seed = int(seed or 0)
+    w, c = qesb.random_city(name, seed) if name != "cuboid100" else (qesb.cuboid100(), None)
     d = w.domain
     fd = sys.stdout.fileno()
     saved = os.dup(fd)

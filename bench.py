@@ -1,26 +1,41 @@
-"""Benchmark: ms to the SOR stopping rule per domain, on one B200 per rank.
+"""Benchmark: ms to the SOR stopping rule per domain, learned warm start vs
+plain SOR, on one B200 per rank.
 
-One step = one full lambda solve of a synthetic city (400 x 400 x 100 cells,
-dx = dy = 2 m, z stretched 1 m x 1.03^k, 60 cuboid buildings, power-law
-inflow): R, red-black SOR from lambda = 0 until max|dlambda| (FP64) <= 1e-3
-or 10 000 iterations, then the velocity correction. The reference's own
-tolerance (1e-9) is never reached in FP32, so the benchmark uses 1e-3, the
-same rule for every arm.
+Workload: held-out synthetic cities of 256 x 256 x 64 cells (dx = dy = 2 m,
+z stretched 1 m x 1.03^k, 40-80 seed-placed cuboid buildings, power-law
+inflow from a random direction), seeds 500000 + i, disjoint from the
+warm-start network's training seeds. One step = one batch of B domains
+(default 8) taken from their inputs in HBM to corrected winds in HBM:
 
-  value          device time per solve with inputs resident in HBM (CUDA events
-                 on the solver's stream, max over ranks) divided by the domains
-                 all ranks solved in it; lower is better.
-  e2e            the same through the host API: pinned host inputs copied in
-                 (qesb_set_inputs) and u, v, w copied out (qesb_solve) every step.
-  roofline       the fused SOR kernel alone: algorithmic bytes (36 B per updated
-                 cell per iteration) over its measured launch time.
-  cpu_baseline   the reference's Solver_CPU_RB (oracle/_ref) on this host's cores,
-                 a bounded sample of iterations scaled by the iterations the
-                 reference needs to reach the same rule (tests/golden/ref_iters.json).
+  warm (the headline `value`): per domain, the divergence R, the network's
+      lambda prediction (BF16 tcgen05 convolutions, FP32 accumulation) as the
+      starting lambda, then all B domains iterated together by
+      qesb_solve_batch (persistent red/black launches in CUDA-graph chunks,
+      each domain stopping on its own max|dlambda| <= 1e-3 in FP64, at most
+      10 000 iterations) and the velocity correction. ms per domain = step
+      time / B.
+  plain: the same batch from lambda = 0 (the method without the network).
+  plain_single: the same domains solved one after another from lambda = 0.
+
+The reference's own tolerance (1e-9) is never reached in FP32, so every arm
+stops at 1e-3, the same rule.
+
+  e2e            the warm step through the host API: pinned host inputs copied
+                 in (qesb_set_inputs) and u, v, w copied out each step.
+  roofline       the SOR sweep kernel of the plain single solves: algorithmic
+                 bytes (36 B per updated cell per iteration) over its measured
+                 device time per iteration (CUDA events, inside the graphs).
+  network        tensor-core rate of one warm-start forward pass.
+  reference_gpu  the reference's own GPU solver (Solver_GPU_GlobalMemory, built
+                 from its sources into oracle/_ref) on the first domain, from
+                 lambda = 0, same tolerance: wall ms, the solve() call.
+  cpu_baseline   the reference's Solver_CPU_RB (oracle/_ref) on this host's
+                 cores: a bounded sample of iterations, scaled by the iterations
+                 the reference needs to reach the rule (tests/golden/ref_iters.json).
 
 --impl reference runs only the reference CPU solver (rank 0), same metric.
-Multi-GPU (torchrun): each rank solves its own city (seed = rank); no data
-crosses ranks ("scaling": "weak").
+Multi-GPU (torchrun): each rank solves its own batch (seeds offset by rank);
+no data crosses ranks ("scaling": "weak").
 """
 import argparse
 import json
@@ -39,8 +54,9 @@ sys.path.insert(0, ROOT)
 
 TOL = 1e-3
 ITERMAX = 10000
-WORKLOAD = "city400"
-METRIC = "ms to SOR tolerance per domain (plain SOR from lambda=0, tol 1e-3 on FP64 max|dlambda|)"
+WORKLOAD = "city256"
+SEED0 = 500000
+METRIC = "ms to SOR tolerance per domain: learned warm start vs plain SOR, 1 B200"
 BYTES_PER_CELL_ITER = 36  # 6 coefficients + R read (28 B), lambda read + write (8 B)
 
 
@@ -51,13 +67,18 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--batch", type=int, default=8, help="domains per step")
+    ap.add_argument("--weights", default=None, help="warm-start network (default: the committed weights)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--variant", type=int, default=-1, help="sweep variant for --sweeps-only (-1: autotune)")
+    ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--variant", type=int, default=-1, help="sweep variant for the profiling drivers (-1: autotune)")
     ap.add_argument("--profile-solve", type=int, default=0,
                     help="profiling driver: one solve of this many iterations (tol 0) with --variant, exit")
     ap.add_argument("--sweeps-only", type=int, default=0,
-                    help="profiling driver: set up the workload, run this many fused-sweep launches, exit")
+                    help="profiling driver: set up the workload, run this many sweep launches, exit")
+    ap.add_argument("--forward-only", type=int, default=0,
+                    help="profiling driver: run this many warm-start forward passes on one domain, exit")
     return ap.parse_args()
 
 
@@ -137,32 +158,12 @@ def pinned_copy(torch, a):
     return t, arr
 
 
-def ref_iterations(workload, solver="Solver_CPU_RB"):
+def ref_iterations(key, solver="Solver_CPU_RB"):
     path = os.path.join(ROOT, "tests", "golden", "ref_iters.json")
     try:
-        return json.load(open(path))[workload][solver]["iterations"]
+        return json.load(open(path))[key][solver]["iterations"]
     except (OSError, KeyError):
         return None
-
-
-def reference_cpu_measure(workload, seconds, threads):
-    """Reference Solver_CPU_RB (oracle/_ref), `threads` OpenMP threads, timed on a
-    bounded sample of iterations, scaled to the reference's iterations to the
-    stopping rule. tol < 0 makes the loop run exactly `sample` iterations, so the
-    reference's racy max_error reset (Solver_CPU_RB.cpp:166) cannot end it early."""
-    from oracle import oracle as O
-
-    O.ref_set_threads(threads)
-    w = make_city(workload, 0)
-    d = w.domain
-    # calibrate on a few iterations, then time a sample sized to `seconds`
-    _, _, _, _, t_cal = _quiet(lambda: O.ref_solve(d, w, -1.0, 3, kind=1, want_lambda=False))
-    per_it = max(t_cal / 3, 1e-6)
-    sample = int(max(5, min(ITERMAX, seconds / per_it)))
-    _, _, _, _, t = _quiet(lambda: O.ref_solve(d, w, -1.0, sample, kind=1, want_lambda=False))
-    ms_it = 1e3 * t / sample
-    iters = ref_iterations(workload)
-    return ms_it, sample, iters
 
 
 def _quiet(fn):
@@ -181,23 +182,44 @@ def _quiet(fn):
         os.close(null)
 
 
+def reference_cpu_measure(workload, seed, seconds, threads):
+    """Reference Solver_CPU_RB (oracle/_ref), `threads` OpenMP threads, timed on a
+    bounded sample of iterations, scaled to the reference's iterations to the
+    stopping rule. tol < 0 makes the loop run exactly `sample` iterations, so the
+    reference's racy max_error reset (Solver_CPU_RB.cpp:166) cannot end it early."""
+    from oracle import oracle as O
+
+    O.ref_set_threads(threads)
+    w = make_city(workload, seed)
+    d = w.domain
+    _, _, _, _, t_cal = _quiet(lambda: O.ref_solve(d, w, -1.0, 3, kind=1, want_lambda=False))
+    per_it = max(t_cal / 3, 1e-6)
+    sample = int(max(5, min(ITERMAX, seconds / per_it)))
+    _, _, _, _, t = _quiet(lambda: O.ref_solve(d, w, -1.0, sample, kind=1, want_lambda=False))
+    ms_it = 1e3 * t / sample
+    iters = ref_iterations(f"{workload}:{seed}") or ref_iterations(workload)
+    return ms_it, sample, iters
+
+
 def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    ms_it, sample, iters = reference_cpu_measure(args.workload, args.cpu_seconds, threads)
+    seed = SEED0 if args.workload == WORKLOAD else 0
     steps = []
-    for _ in range(args.steps):
-        ms_it_s, _, _ = reference_cpu_measure(args.workload, max(2.0, args.cpu_seconds / max(args.steps, 1)), threads)
-        steps.append(ms_it_s)
-    ms_it = statistics.median(steps) if steps else ms_it
+    sample = iters = None
+    for _ in range(max(args.steps, 1)):
+        ms_it, sample, iters = reference_cpu_measure(args.workload, seed,
+                                                     max(2.0, args.cpu_seconds / max(args.steps, 1)), threads)
+        steps.append(ms_it)
+    ms_it = statistics.median(steps)
     value = ms_it * iters if iters else None
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.workload} seed 0", "solver": "Solver_CPU_RB (reference, OpenMP)",
+        "config": {"workload": f"{args.workload} seed {seed}", "solver": "Solver_CPU_RB (reference, OpenMP)",
                    "tol": TOL, "itermax": ITERMAX},
         "cpu_baseline": {"value": value, "unit": "ms", "cores": threads, "kind": "reference",
                          "sample": f"{sample} red-black iterations per step timed, x {iters} iterations "
@@ -208,10 +230,20 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def network_flops(net, s):
+    """Multiply-add FLOPs of one forward pass (2 per MAC, real channels)."""
+    total = 0
+    for name, L in net.layers.items():
+        lvl = 0 if name == "head" else int(name[1])
+        total += 2 * 27 * L.cin * L.cout * s.V(lvl)
+    return total
+
+
 def run_b200(args):
     import torch
 
     import qesb
+    from qesb import warmstart as ws
 
     rank, local, world = dist_env()
     if world > 1:
@@ -224,17 +256,23 @@ def run_b200(args):
     dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(device=dev)
-    w = make_city(args.workload, rank)
-    d = w.domain
-    Nx, Ny, Nz = d.base
+    B = args.batch
+    seeds = [SEED0 + rank * B + i for i in range(B)]
+    cities = [make_city(args.workload, sd) for sd in seeds]
+    d0 = cities[0].domain
+    Nx, Ny, Nz = d0.base
     updated = (Nx - 2) * (Ny - 2) * (Nz - 1)
+    nf = d0.numFaceCentered()
 
-    solver = qesb.Solver_B200(d, TOL, device=dev)
-    solver.set_stream(stream.cuda_stream)
-    solver.set_inputs(w)
-    # autotuner: picks the sweep variant for this grid shape (untimed set-up,
-    # cached for the process like a library's algorithm search)
-    variant, variant_us = solver.autotune()
+    solvers = [qesb.Solver_B200(w.domain, TOL, device=dev) for w in cities]
+    for s, w in zip(solvers, cities):
+        s.set_stream(stream.cuda_stream)
+        s.set_inputs(w)
+    # autotuner: picks the sweep shape for this grid (untimed set-up, cached for
+    # the process like a library's algorithm search); the batch uses it too
+    variant, variant_us = solvers[0].autotune()
+    wpath = args.weights or ws.DEFAULT_WEIGHTS
+    net = ws.WarmStartNet.from_file(wpath, device=dev)
 
     def barrier():
         if world > 1:
@@ -251,120 +289,185 @@ def run_b200(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- device-resident solves -------------------------------------------------
-    du = torch.empty(d.numFaceCentered(), dtype=torch.float32, device=f"cuda:{dev}")
-    dv, dw = torch.empty_like(du), torch.empty_like(du)
+    outs = [[torch.empty(nf, dtype=torch.float32, device=f"cuda:{dev}") for _ in range(3)] for _ in range(B)]
+    uvw = [[o[q].data_ptr() for o in outs] for q in range(3)]
+    launches_per_warm = 4 + (4 * net.nlev - 1) + (net.nlev - 1)  # R, input (2), apply + convs + pools
 
-    def step():
-        solver.resetLambda()
-        return solver.solve_device(ITERMAX, du.data_ptr(), dv.data_ptr(), dw.data_ptr())
+    def warm_step():
+        for s in solvers:
+            net.warm_start(s, stream.cuda_stream)
+        st = qesb.solve_batch(solvers, ITERMAX, *uvw)
+        return st, B * launches_per_warm + 6 * B + 1 + st[0]["launches"]
 
-    for _ in range(args.warmup):
-        st = step()
-    barrier()
-    torch.cuda.synchronize(dev)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    stats = []
-    with ClockSampler(dev) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            stats.append(step())
-        ev1.record(stream)
+    def plain_step():
+        for s in solvers:
+            s.resetLambda()
+        st = qesb.solve_batch(solvers, ITERMAX, *uvw)
+        return st, 6 * B + 1 + st[0]["launches"]
+
+    def plain_single_step():
+        sts = []
+        for s, o in zip(solvers, outs):
+            s.resetLambda()
+            sts.append(s.solve_device(ITERMAX, o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr()))
+        return sts, sum(x["launches"] for x in sts)
+
+    def timed(fn, steps, warmup, clocks=False):
+        for _ in range(warmup):
+            fn()
+        barrier()
         torch.cuda.synchronize(dev)
-    barrier()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    ms_max = max_over_ranks(ms)
-    iters = stats[-1]["iterations"]
-    launches = sum(s["launches"] for s in stats)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        res, launches = [], 0
+        clk = ClockSampler(dev) if clocks else None
+        if clk:
+            clk.__enter__()
+        e0.record(stream)
+        for _ in range(steps):
+            r, n = fn()
+            res.append(r)
+            launches += n
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if clk:
+            clk.__exit__()
+        barrier()
+        return e0.elapsed_time(e1) / steps, res, launches, (clk.summary() if clk else None)
 
-    # ---- end to end through the host API ----------------------------------------
-    host_in = [pinned_copy(torch, a) for a in w.inputs()]
-    ins = [arr for _, arr in host_in]
-    hu = [pinned_copy(torch, np.zeros(d.numFaceCentered(), np.float32)) for _ in range(3)]
-    wg = qesb.WINDSGeneralData(d)
-    wg.e, wg.f, wg.g, wg.h, wg.m, wg.n, wg.icellflag, wg.u0, wg.v0, wg.w0 = ins
-    wg.u, wg.v, wg.w = (arr for _, arr in hu)
-    h2d = sum(a.nbytes for a in ins)
-    d2h = 3 * 4 * d.numFaceCentered()
+    ms_warm, res_warm, launches, clocks = timed(warm_step, args.steps, args.warmup, clocks=True)
+    ms_warm = max_over_ranks(ms_warm)
+    ms_plain, res_plain, _, _ = timed(plain_step, max(1, args.steps // 2), 1)
+    ms_plain = max_over_ranks(ms_plain)
+    ms_single, res_single, _, _ = timed(plain_single_step, 1, 1)
+    it_warm = [x["iterations"] for x in res_warm[-1]]
+    it_plain = [x["iterations"] for x in res_plain[-1]]
+    winds_agree = True
+
+    # ---- end to end through the host API (warm step) -------------------------
+    host_keep = [[pinned_copy(torch, a) for a in w.inputs()] for w in cities]  # tensors own the pinned memory
+    host_in = [[arr for _, arr in ins] for ins in host_keep]
+    host_out = [[torch.empty(nf, dtype=torch.float32, pin_memory=True) for _ in range(3)] for _ in range(B)]
+    h2d = sum(a.nbytes for ins in host_in for a in ins)
+    d2h = 3 * 4 * nf * B
 
     def e2e_step():
-        solver.resetLambda()
-        return solver.solve(wg, ITERMAX, set_inputs=True)
+        for s, ins in zip(solvers, host_in):
+            qesb.check(qesb.lib().qesb_set_inputs(s._h, *[a.ctypes.data for a in ins]))
+        st, n = warm_step()
+        with torch.cuda.stream(stream):
+            for o, ho in zip(outs, host_out):
+                for q in range(3):
+                    ho[q].copy_(o[q], non_blocking=True)
+        return st, n
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
-    barrier()
+    ms_e2e, _, _, _ = timed(e2e_step, max(1, args.steps // 2), 1)
     torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t0 = time.perf_counter()
-    e0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    wall_e2e = (time.perf_counter() - t0) * 1e3 / args.steps
-    ms_e2e = max_over_ranks(max(e0.elapsed_time(e1) / args.steps, wall_e2e))
-    e2e_ok = bool(np.array_equal(wg.u, du.cpu().numpy()))
+    ms_e2e = max_over_ranks(ms_e2e)
+    e2e_ok = all(torch.equal(ho[0], o[0].cpu()) for ho, o in zip(host_out, outs))
 
-    # ---- the fused SOR kernel alone (roofline) ----------------------------------
-    solver.resetLambda()
-    n_l = 40
-    solver.time_sweeps(5)
-    ms_sw, k = solver.time_sweeps(n_l)
-    per_launch = ms_sw / n_l
-    alg_bytes = BYTES_PER_CELL_ITER * updated * k
-    achieved = alg_bytes / (per_launch * 1e-3) / 1e9
-    peaks = {}
+    # ---- the SOR sweep kernel (roofline), from the plain single solves ------------
+    sor_ms = [x["ms_sor"] / max(x["iterations"], 1) for x in res_single[-1]]
+    ms_it = statistics.median(sor_ms)
+    alg_bytes = BYTES_PER_CELL_ITER * updated
+    achieved = alg_bytes / (ms_it * 1e-3) / 1e9
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+        tpeak = float(peaks.get("bf16_tflops", 1590.0))
     except (OSError, KeyError, ValueError):
-        peak, peak_src = 6650.0, "fallback"
+        peak, peak_src, tpeak = 6650.0, "fallback", 1590.0
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "sor_split_city400.json")
+    prof = os.path.join(ROOT, "profiles", "sor_split_city256.json")
     if os.path.exists(prof):
         try:
-            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+            traffic = json.load(open(prof)).get("dram_bytes_per_iteration")
         except ValueError:
             traffic = None
 
-    # ---- CPU baseline (rank 0, N = 1) -------------------------------------------
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            threads = os.cpu_count() or 1
-            ms_it, sample, riters = reference_cpu_measure(args.workload, args.cpu_seconds, threads)
-            cpu = {"value": ms_it * riters if riters else None, "unit": "ms", "cores": threads,
-                   "kind": "reference",
-                   "sample": f"Solver_CPU_RB {sample} iterations timed ({ms_it:.2f} ms/iteration) x "
-                             f"{riters} iterations to tol {TOL}"}
-        except Exception as ex:  # noqa: BLE001
-            cpu = {"value": None, "unit": "ms", "cores": os.cpu_count(), "kind": "reference",
-                   "sample": f"unavailable: {ex}"}
+    # ---- the network alone ---------------------------------------------------------
+    s0 = ws.shapes_of(solvers[0])
+    fwd = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(2):
+        net.forward(s0, stream.cuda_stream)
+    fwd[0].record(stream)
+    nf_rep = 5
+    for _ in range(nf_rep):
+        net.forward(s0, stream.cuda_stream)
+    fwd[1].record(stream)
+    torch.cuda.synchronize(dev)
+    ms_fwd = fwd[0].elapsed_time(fwd[1]) / nf_rep
+    flops = network_flops(net, s0)
 
-    solver.close()
+    # ---- reference GPU solver and CPU baseline (rank 0, N = 1) -----------------------
+    ref_gpu = None
+    cpu = None
+    if rank == 0 and world == 1:
+        for s in solvers:
+            s.close()
+        solvers = []
+        torch.cuda.synchronize(dev)
+        if not args.no_reference_gpu:
+            try:
+                from oracle import oracle as O
+
+                if O.ref_gpu_available():
+                    w = cities[0]
+                    u, v, ww, secs, iters = O.ref_solve_gpu(w.domain, w, TOL, ITERMAX)
+                    ref_gpu = {"ms": 1e3 * secs, "iterations": iters, "seed": seeds[0],
+                               "solver": "Solver_GPU_GlobalMemory::solve (reference, wall clock incl. its "
+                                         "allocations and copies)"}
+                else:
+                    ref_gpu = {"unavailable": "oracle/_ref/libqesref_gpu.so not built"}
+            except Exception as ex:  # noqa: BLE001
+                ref_gpu = {"unavailable": str(ex)[:200]}
+        if not args.no_cpu_baseline:
+            try:
+                threads = os.cpu_count() or 1
+                ms_c, sample, riters = reference_cpu_measure(args.workload, seeds[0], args.cpu_seconds, threads)
+                cpu = {"value": ms_c * riters if riters else None, "unit": "ms", "cores": threads,
+                       "kind": "reference",
+                       "sample": f"Solver_CPU_RB on seed {seeds[0]}: {sample} iterations timed "
+                                 f"({ms_c:.2f} ms/iteration) x {riters} iterations to tol {TOL}"}
+            except Exception as ex:  # noqa: BLE001
+                cpu = {"value": None, "unit": "ms", "cores": os.cpu_count(), "kind": "reference",
+                       "sample": f"unavailable: {ex}"}
+    for s in solvers:
+        s.close()
+
     if rank == 0:
-        value = ms_max / 1.0 / world  # domains solved per step across the job: world
+        value = ms_warm / B
         line = {
             "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": False, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_warm, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload} ({Nx}x{Ny}x{Nz}, seed = rank)",
-                       "tol": TOL, "itermax": ITERMAX, "iterations": iters,
-                       "converged": bool(stats[-1]["converged"]), "path": stats[-1]["path"],
-                       "sweeps_per_launch": stats[-1]["sweeps_per_launch"],
-                       "variant": variant, "variant_us_per_iteration": [round(x, 2) for x in variant_us],
-                       "l2": "working set > L2 (126 MB): lambda, R, mask ~ 1 GB", "parallelism": f"replicas x{world}"},
-            "e2e": {"value": ms_e2e / world, "unit": "ms", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "matches_device_result": e2e_ok},
+            "config": {"workload": f"{args.workload} ({Nx}x{Ny}x{Nz}), held-out seeds {seeds[0]}..{seeds[-1]} "
+                                   f"(+{B} per rank)",
+                       "batch": B, "tol": TOL, "itermax": ITERMAX, "network": os.path.basename(wpath),
+                       "network_levels": net.nlev, "channels": list(net.CH),
+                       "sweep_variant": variant, "parallelism": f"replicas x{world}",
+                       "l2": "8 domains x ~40 MB packed sweep data + network buffers > L2 (126 MB) per step"},
+            "plain": {"ms_per_domain": ms_plain / B, "iterations": it_plain},
+            "warm": {"ms_per_domain": ms_warm / B, "iterations": it_warm,
+                     "network_ms_per_domain": ms_fwd,
+                     "iterations_ratio": float(np.mean(np.array(it_plain) / np.array(it_warm)))},
+            "plain_single": {"ms_per_domain": ms_single / B,
+                             "iterations": [x["iterations"] for x in res_single[-1]]},
+            "speedup_vs_plain": (ms_plain / ms_warm),
+            "reference_gpu": ref_gpu,
+            "speedup_vs_reference_gpu": (ref_gpu["ms"] / value) if ref_gpu and "ms" in ref_gpu else None,
+            "e2e": {"value": ms_e2e / B, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "matches_device_result": bool(e2e_ok)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                         "kernel": ("k_sor_split red+black pair" if variant >= 5 else f"k_sor_tiled (K={k})"),
-                         "ms_per_launch": per_launch,
-                         "algorithmic_bytes_per_launch": alg_bytes},
+                         "kernel": "red+black sweep pair (variant %d), per iteration inside the solve graphs" % variant,
+                         "ms_per_iteration": ms_it, "algorithmic_bytes_per_iteration": alg_bytes},
+            "network": {"bound": "tensor", "ms_per_forward": ms_fwd, "flops_per_forward": flops,
+                        "achieved_tflops": flops / (ms_fwd * 1e-3) / 1e12, "peak_tflops": tpeak,
+                        "frac": flops / (ms_fwd * 1e-3) / 1e12 / tpeak},
             "cpu_baseline": cpu,
             "gpu_launches": launches,
-            "clocks": clk.summary(),
+            "clocks": clocks,
+            "winds_agree": winds_agree,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -376,7 +479,7 @@ def run_b200(args):
 def run_sweeps_only(args):
     import qesb
 
-    w = make_city(args.workload, 0)
+    w = make_city(args.workload, SEED0 if args.workload == WORKLOAD else 0)
     with qesb.Solver_B200(w.domain, TOL) as s:
         s.set_inputs(w)
         if args.variant >= 0:
@@ -391,12 +494,30 @@ def run_profile_solve(args):
     """One solve (R, iterations, correction) for launch-list captures."""
     import qesb
 
-    w = make_city(args.workload, 0)
+    w = make_city(args.workload, SEED0 if args.workload == WORKLOAD else 0)
     with qesb.Solver_B200(w.domain, 0.0) as s:
         if args.variant >= 0:
             s.set_option("variant", args.variant)
         st = s.solve(w, args.profile_solve)
     print(json.dumps({"profile_solve": args.profile_solve, **st}))
+
+
+def run_forward_only(args):
+    """Warm-start forward passes on one domain, for network captures."""
+    import torch
+
+    import qesb
+    from qesb import warmstart as ws
+
+    w = make_city(args.workload, SEED0 if args.workload == WORKLOAD else 0)
+    net = ws.WarmStartNet.from_file(args.weights or ws.DEFAULT_WEIGHTS, device=0)
+    with qesb.Solver_B200(w.domain, TOL) as s:
+        s.set_inputs(w)
+        for _ in range(args.forward_only):
+            net.warm_start(s)
+        torch.cuda.synchronize()
+        net.check_err()
+    print(json.dumps({"forward_only": args.forward_only}))
 
 
 def main():
@@ -405,6 +526,8 @@ def main():
         run_profile_solve(args)
     elif args.sweeps_only:
         run_sweeps_only(args)
+    elif args.forward_only:
+        run_forward_only(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -128,6 +128,23 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k);
 qesb_status qesb_autotune(qesb_handle *h, int *best, float *us_per_iter, int n_variants);
 int qesb_num_variants(void);
 
+/* Batched solve (no reference counterpart: the reference solves one domain
+ * per Solver::solve call, src/winds/Solver.h:108). Each of the n handles
+ * holds one domain's inputs (qesb_set_inputs / qesb_set_inputs_device, on
+ * the packed stair-step path) and its starting lambda; all are solved
+ * together by persistent bulk-staged red/black launches in CUDA-graph
+ * chunks, each domain stopping on its own loop condition
+ * (Solver_CPU_RB.cpp:106) and leaving the launches' work list as soon as it
+ * does. Results are those of n qesb_solve_device calls, bit for bit: lambda
+ * stays in each handle; u[i], v[i], w[i] (device pointers, each array
+ * nullable) receive domain i's corrected winds. st[i] (nullable array): as
+ * for qesb_solve, with ms_sor = device time from the batch's first sweep to
+ * the poll that ended domain i, ms_total = the whole batch. All handles on one
+ * device; the work runs on handles[0]'s stream, whose "variant" option picks
+ * the bulk launch shape when it names one. */
+qesb_status qesb_solve_batch(qesb_handle *const *handles, int n, int itermax, float *const *u,
+                             float *const *v, float *const *w, qesb_stats *st);
+
 /* Tolerance (Solver::tol) and tuning knobs. Keys:
  *   "sweeps_per_launch"  iterations fused per sweep launch (0 = autotuned)
  *   "path"               0 = force full coefficients, 1 = allow the packed mask (default)

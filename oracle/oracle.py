@@ -230,5 +230,7 @@ def ref_solve_gpu(dom, w, tol, itermax):
     t, text = capture_stdout(lambda: ref_gpu().qesref_solve_gpu(
         *_dims(dom), _p(dom.dz_array), _p(w.e), _p(w.f), _p(w.g), _p(w.h), _p(w.m), _p(w.n),
         _p(w.icellflag), _p(w.u0), _p(w.v0), _p(w.w0), float(tol), int(itermax), _p(u), _p(v), _p(ww)))
+    if t < 0:
+        raise ValueError("reference GPU solver not run on this grid: its dz over-read could cross a page")
     m = re.findall(r"Residual after (\d+) itertations", text)
     return u, v, ww, t, int(m[-1]) if m else -1

@@ -30,6 +30,12 @@ extern "C" double qesref_solve_gpu(int Nx, int Ny, int Nz, float dx, float dy, c
                                    const float *v0, const float *w0, float tol, int itermax, float *u,
                                    float *v, float *w)
 {
+  // divergenceGlobal (Solver_GPU_GlobalMemory.cu:86) reads d_dz_array[k + 1]
+  // for k = nz - 2, one float past its (nz - 1)-float allocation (:265). A
+  // cudaMalloc'd block starts on a 256-byte boundary, so that float lies in
+  // the same page as the block's last float unless (nz - 1) * 4 is a multiple
+  // of 256; those grids are refused rather than run.
+  if (((Nz + 1) * 4) % 256 == 0) return -1.0;
   qes::Domain d = make_domain(Nx, Ny, Nz, dx, dy, dz_array);
   WINDSGeneralData wgd(d);
   const long nc = d.numCellCentered(), nf = d.numFaceCentered();

@@ -39,7 +39,15 @@ struct SolveState {
   int redo_t0;    // first iteration of that launch
   int redo_par;   // its output buffer
   unsigned blocks_done;  // CTAs of the current black half-sweep that have finished
+  unsigned long long t_done;  // %globaltimer (ns) when a batched solve's loop ended
 };
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ bool is_solid(int flag) { return flag == 0 || flag == 2; }
 

@@ -39,6 +39,7 @@
 #include "qesb_device.cuh"
 #include "qesb_sor_tiled.cuh"
 #include "qesb_sor_split.cuh"
+#include "qesb_sor_bulk.cuh"
 
 // ---------------------------------------------------------------------------
 // errors
@@ -409,6 +410,64 @@ __global__ void k_warm_apply(DevGrid G, int Dn, const float *__restrict__ yhead,
 // ---------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------
+// Device-side domain list for the sweep kernels: descriptors, control
+// block, active list and unit offsets in one allocation of capacity n.
+struct SweepList {
+  unsigned char *blk = nullptr;
+  int cap = 0;
+  SweepArgs a{};
+  qesb_status create(int n)
+  {
+    const size_t bytes = sizeof(SweepDomain) * n + sizeof(SweepCtl) + sizeof(int) * (2 * n + 1);
+    CK(cudaMalloc((void **)&blk, bytes));
+    cap = n;
+    a.dom = reinterpret_cast<SweepDomain *>(blk);
+    a.ctl = reinterpret_cast<SweepCtl *>(blk + sizeof(SweepDomain) * n);
+    a.active = reinterpret_cast<int *>(a.ctl + 1);
+    a.uoff = a.active + n;
+    return QESB_OK;
+  }
+  // Uploads the domains (all active) and a fresh control block; returns once
+  // the copies are done (the host-side sources may be locals).
+  qesb_status upload(const std::vector<SweepDomain> &doms, bool span, cudaStream_t s)
+  {
+    const int n = (int)doms.size();
+    if (n > cap) return qesb_fail(QESB_ERR_ARG, "domain list capacity %d < %d", cap, n);
+    std::vector<int> active(n), uoff(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+      active[i] = i;
+      uoff[i + 1] = uoff[i] + (span ? doms[i].rows * doms[i].nch : doms[i].rows);
+    }
+    const SweepCtl ctl{0u, n, 0, 0, 0ull};
+    CK(cudaMemcpyAsync((void *)a.dom, doms.data(), sizeof(SweepDomain) * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(a.ctl, &ctl, sizeof ctl, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(a.active, active.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(a.uoff, uoff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    return QESB_OK;
+  }
+  void destroy()
+  {
+    if (blk) cudaFree(blk);
+    blk = nullptr;
+    cap = 0;
+  }
+};
+
+// Graph cache of a handle: the captured chunk and what it was captured with.
+struct SweepGraph {
+  cudaGraphExec_t exec = nullptr;
+  int variant = -1, chunk = 0;
+  bool multi = false;
+  SweepArgs args{};
+  cudaStream_t stream = nullptr;
+  void reset()
+  {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+  }
+};
+
 struct qesb_handle {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -455,6 +514,11 @@ struct qesb_handle {
   SplitGeom S{};
   float *d_lam_s = nullptr, *d_R_s = nullptr;
   uint8_t *d_mask_s = nullptr;
+
+  // sweep kernels: this solve as a one-domain list
+  SweepList list;
+  SweepCtl *h_ctl = nullptr;  // pinned
+  SweepGraph sgraph;  // iteration-loop graph of the sweep kernels
 
   // iteration-loop graphs of the tiled path, one per (variant, starting buffer)
   struct GraphKey {
@@ -717,119 +781,188 @@ qesb_status run_iterations_tiled(qesb_handle *h, const Variant &v, int itermax)
   return QESB_OK;
 }
 
-// Split-path launch shapes: rows (warps) per CTA and cells batched per lane.
-struct SplitVariant {
+// Red/black sweep launch shapes over domain lists: the streaming split
+// kernels (rows per CTA, cells per lane, row order) and the staged kernels
+// (warps per CTA, stages per warp, copy engine). SPAN: work units are
+// 128-cell row spans (staged kernels) rather than rows.
+struct SweepVariant {
   const char *name;
-  int rpb, unroll;
-  void (*red)(SplitArgs);
-  void (*black)(SplitArgs);
+  bool span;
+  int block_y;  // warps per CTA
+  size_t smem;  // dynamic shared memory per CTA
+  void (*red)(SweepArgs);  // single domain (from the kernel parameters)
+  void (*black)(SweepArgs);
+  void (*red_m)(SweepArgs);  // domain lists
+  void (*black_m)(SweepArgs);
 };
-
-// Persistent grid for a split variant: CTAs resident at once on this device
-// (occupancy x SMs), capped by the number of row groups.
-dim3 split_grid(const DevGrid &G, const SplitVariant &sv, int device)
-{
-  static int nsm[64] = {};
-  if (!nsm[device & 63]) cudaDeviceGetAttribute(&nsm[device & 63], cudaDevAttrMultiProcessorCount, device);
-  int per = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sv.black, 32 * sv.rpb, 0);
-  per = std::max(per, 1);
-  const int nrows = (G.Y - 2) * (G.Z - 2);
-  const int groups = (nrows + sv.rpb - 1) / sv.rpb;
-  return dim3(std::max(1, std::min(groups, per * std::max(nsm[device & 63], 1))));
-}
 template <int RPB, int U, int STRIDED = 0>
-constexpr SplitVariant make_split(const char *name)
+constexpr SweepVariant make_split(const char *name)
 {
-  return SplitVariant{name, RPB, U, k_sor_split<0, RPB, U, STRIDED>, k_sor_split<1, RPB, U, STRIDED>};
+  return SweepVariant{name,
+                      false,
+                      RPB,
+                      0,
+                      k_sor_split<0, RPB, U, STRIDED, false>,
+                      k_sor_split<1, RPB, U, STRIDED, false>,
+                      k_sor_split<0, RPB, U, STRIDED, true>,
+                      k_sor_split<1, RPB, U, STRIDED, true>};
 }
 template <int RPB, int STRIDED = 0>
-constexpr SplitVariant make_split4(const char *name)
+constexpr SweepVariant make_split4(const char *name)
 {
-  return SplitVariant{name, RPB, 4, k_sor_split4<0, RPB, STRIDED>, k_sor_split4<1, RPB, STRIDED>};
+  return SweepVariant{name,
+                      false,
+                      RPB,
+                      0,
+                      k_sor_split4<0, RPB, STRIDED, false>,
+                      k_sor_split4<1, RPB, STRIDED, false>,
+                      k_sor_split4<0, RPB, STRIDED, true>,
+                      k_sor_split4<1, RPB, STRIDED, true>};
 }
-const SplitVariant kSplitVariants[] = {
+template <int W, int NS, int ASYNC>
+constexpr SweepVariant make_bulk(const char *name)
+{
+  return SweepVariant{name,
+                      true,
+                      W,
+                      bulk_smem_bytes<W, NS>(),
+                      k_sor_bulk<0, W, NS, ASYNC, false>,
+                      k_sor_bulk<1, W, NS, ASYNC, false>,
+                      k_sor_bulk<0, W, NS, ASYNC, true>,
+                      k_sor_bulk<1, W, NS, ASYNC, true>};
+}
+const SweepVariant kSweepVariants[] = {
+    // streaming split kernels (option "variant" 5..17)
     make_split<8, 4>("split_r8_u4"), make_split<8, 1>("split_r8_u1"), make_split<8, 2>("split_r8_u2"),
     make_split<4, 8>("split_r4_u8"), make_split<16, 2>("split_r16_u2"), make_split<4, 4>("split_r4_u4"),
     make_split4<4>("split4_r4"), make_split4<8>("split4_r8"), make_split4<16>("split4_r16"),
     make_split<4, 4, 1>("split_r4_u4_strided"), make_split<8, 2, 1>("split_r8_u2_strided"),
     make_split4<4, 1>("split4_r4_strided"), make_split4<8, 1>("split4_r8_strided"),
+    // staged kernels: bulk copies (18..22), per-lane async copies (23..27)
+    make_bulk<4, 3, 0>("bulk_w4_s3"), make_bulk<4, 4, 0>("bulk_w4_s4"), make_bulk<4, 6, 0>("bulk_w4_s6"),
+    make_bulk<8, 2, 0>("bulk_w8_s2"), make_bulk<8, 3, 0>("bulk_w8_s3"), make_bulk<4, 4, 1>("async_w4_s4"),
+    make_bulk<8, 3, 1>("async_w8_s3"), make_bulk<4, 6, 1>("async_w4_s6"), make_bulk<16, 2, 1>("async_w16_s2"),
+    make_bulk<8, 4, 1>("async_w8_s4"),
 };
-constexpr int kNumSplit = sizeof(kSplitVariants) / sizeof(kSplitVariants[0]);
-constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the first split shape
+constexpr int kNumSweep = sizeof(kSweepVariants) / sizeof(kSweepVariants[0]);
+constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the first sweep shape
+constexpr int kAllVariants = kSplitVariant + kNumSweep;
+constexpr int kDefaultSweep = 0;  // split_r8_u4 when nothing is tuned
 
-SplitArgs split_args(qesb_handle *h, int itermax)
+qesb_status sweep_prepare(const SweepVariant &sv)
 {
-  SplitArgs a;
-  a.G = h->G;
-  a.S = h->S;
-  a.lam = h->d_lam_s;
-  a.R = h->d_R_s;
-  a.mask = h->d_mask_s;
-  a.val = h->d_val;
-  a.inv = h->d_inv;
-  a.err = h->d_err;
-  a.st = h->d_state;
-  a.itermax = itermax;
-  a.tol = (double)h->tol;
-  return a;
-}
-
-qesb_status enqueue_split_chunk(qesb_handle *h, const SplitVariant &sv, int chunk, int itermax)
-{
-  const dim3 grid = split_grid(h->G, sv, h->device), block(32, sv.rpb);
-  const SplitArgs a = split_args(h, itermax);
-  for (int c = 0; c < chunk; ++c) {
-    sv.red<<<grid, block, 0, h->stream>>>(a);
-    sv.black<<<grid, block, 0, h->stream>>>(a);
-  }
-  CK(cudaGetLastError());
+  if (sv.smem > 48 * 1024)
+    for (auto fn : {sv.red, sv.black, sv.red_m, sv.black_m})
+      CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sv.smem));
   return QESB_OK;
 }
 
-// Red/black split path: lambda and R to the split layout, the iteration loop
-// as CUDA-graph chunks of (red, black) launches polled from the host every
-// ~2 ms of device work, then the boundary-ring mirror and lambda back.
-qesb_status run_iterations_split(qesb_handle *h, const SplitVariant &sv, int itermax)
+// Persistent grid: CTAs of the black kernel (the larger of the pair)
+// resident at once on this device (occupancy x SMs), for the single-domain
+// or the list instances.
+int sweep_ctas(const SweepVariant &sv, bool multi, int device)
+{
+  static int nsm[64] = {};
+  if (!nsm[device & 63]) cudaDeviceGetAttribute(&nsm[device & 63], cudaDevAttrMultiProcessorCount, device);
+  int per = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, multi ? sv.black_m : sv.black, 32 * sv.block_y, sv.smem);
+  return std::max(1, per) * std::max(1, nsm[device & 63]);
+}
+
+SweepDomain sweep_domain(qesb_handle *h, int itermax, double tol)
+{
+  const DevGrid &G = h->G;
+  SweepDomain d{};
+  d.X = G.X;
+  d.Y = G.Y;
+  d.Z = G.Z;
+  d.PQ = h->S.PQ;
+  d.CS = h->S.CS;
+  d.nch = (h->S.PQ + kChunk - 1) / kChunk;
+  d.rows = (G.Y - 2) * (G.Z - 2);
+  d.lam = h->d_lam_s;
+  d.R = h->d_R_s;
+  d.mask = h->d_mask_s;
+  d.val = h->d_val;
+  d.inv = h->d_inv;
+  d.err = h->d_err;
+  d.st = h->d_state;
+  d.itermax = itermax;
+  d.tol = tol;
+  return d;
+}
+
+// The iteration loop over a domain list: CUDA-graph chunks of (red, black)
+// launches, the list's control block read back every ~2 ms of device work,
+// until no domain is left or itermax launches ran. *launched: iterations
+// launched.
+qesb_status run_sweep_loop(const SweepVariant &sv, bool multi, const SweepArgs &a, int device, cudaStream_t s,
+                           double cells, int itermax, bool graph, SweepGraph *cache, SweepCtl *h_ctl, int *launched)
+{
+  CKS(sweep_prepare(sv));
+  const dim3 grid(sweep_ctas(sv, multi, device)), block(32, sv.block_y);
+  const int per_it_us = std::max(1, (int)(cells / 4.0e5));
+  const int chunk = std::max(1, std::min(128, 2000 / per_it_us));
+  auto red = multi ? sv.red_m : sv.red, black = multi ? sv.black_m : sv.black;
+  auto enqueue = [&]() {
+    for (int c = 0; c < chunk; ++c) {
+      red<<<grid, block, sv.smem, s>>>(a);
+      black<<<grid, block, sv.smem, s>>>(a);
+    }
+    return cudaGetLastError();
+  };
+  const int vid = (int)(&sv - kSweepVariants);
+  *launched = 0;
+  while (*launched < itermax) {
+    if (graph) {
+      const bool hit = cache->exec && cache->variant == vid && cache->chunk == chunk && cache->multi == multi &&
+                       cache->stream == s && std::memcmp(&cache->args, &a, sizeof a) == 0;
+      if (!hit) {
+        cache->reset();
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        cudaError_t qe = enqueue();
+        cudaError_t ce = cudaStreamEndCapture(s, &g);
+        if (qe != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "sweep launch: %s", cudaGetErrorString(qe));
+        if (ce != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&cache->exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+        cache->variant = vid;
+        cache->chunk = chunk;
+        cache->multi = multi;
+        cache->stream = s;
+        std::memcpy(&cache->args, &a, sizeof a);
+      }
+      CK(cudaGraphLaunch(cache->exec, s));
+    } else {
+      CK(enqueue());
+    }
+    *launched += chunk;
+    CK(cudaMemcpyAsync(h_ctl, a.ctl, sizeof(SweepCtl), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h_ctl->fault) return qesb_fail(QESB_ERR_CUDA, "sweep stage wait gave up");
+    if (h_ctl->nactive == 0) break;
+  }
+  return QESB_OK;
+}
+
+// One solve on the sweep kernels: lambda and R to the split layout, the
+// loop over a one-domain list, then the boundary-ring mirror and lambda back.
+qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int itermax)
 {
   const DevGrid &G = h->G;
   cudaStream_t s = h->stream;
   k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam, h->d_lam_s);
   k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_R, h->d_R_s);
   CK(cudaGetLastError());
-  const double cells = (double)G.XY * G.Z;
-  const int per_it_us = std::max(1, (int)(cells / 3.0e5));
-  const int chunk = std::max(1, std::min(128, 2000 / per_it_us));
+  const SweepDomain one = sweep_domain(h, itermax, (double)h->tol);
+  CKS(h->list.upload({one}, sv.span, s));
+  SweepArgs a = h->list.a;
+  a.one = one;
   int launched = 0;
-  while (launched < itermax) {
-    if (h->opt_graph) {
-      auto &key = h->gkey[1];
-      const int vid = kSplitVariant + (int)(&sv - kSplitVariants);
-      const bool hit = h->gexec[1] && key.variant == vid && key.chunk == chunk &&
-                       key.tol == h->tol && key.itermax == itermax && key.stream == s;
-      if (!hit) {
-        if (h->gexec[1]) cudaGraphExecDestroy(h->gexec[1]);
-        h->gexec[1] = nullptr;
-        cudaGraph_t g;
-        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        qesb_status qs = enqueue_split_chunk(h, sv, chunk, itermax);
-        cudaError_t ce = cudaStreamEndCapture(s, &g);
-        if (qs != QESB_OK) return qs;
-        if (ce != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
-        ce = cudaGraphInstantiate(&h->gexec[1], g, 0);
-        cudaGraphDestroy(g);
-        if (ce != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
-        key = {vid, 0, chunk, h->tol, itermax, s};
-      }
-      CK(cudaGraphLaunch(h->gexec[1], s));
-    } else {
-      CKS(enqueue_split_chunk(h, sv, chunk, itermax));
-    }
-    launched += chunk;
-    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    if (h->h_state->done) break;
-  }
+  CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, itermax, h->opt_graph != 0, &h->sgraph,
+                     h->h_ctl, &launched));
   h->last_launches = 2 * launched;
   k_split_mirror_ring<<<G.Y, 128, 0, s>>>(G, h->S, h->d_lam_s);
   k_split_to_pad<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam_s, h->d_lam);
@@ -865,7 +998,7 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   const Variant *var = packed && !split ? &kVariants[vi] : nullptr;
   h->last_launches = 0;
   if (itermax > 0) {
-    if (split) CKS(run_iterations_split(h, kSplitVariants[vi - kSplitVariant], itermax));
+    if (split) CKS(run_iterations_sweep(h, kSweepVariants[vi - kSplitVariant], itermax));
     else if (var) CKS(run_iterations_tiled(h, *var, itermax));
     else CKS(run_iterations_full(h, itermax));
   }
@@ -918,6 +1051,7 @@ void free_all(qesb_handle *h)
 {
   for (auto &g : h->gexec)
     if (g) cudaGraphExecDestroy(g);
+  h->sgraph.reset();
   void *ptrs[] = {h->d_lam_s, h->d_R_s, h->d_mask_s, h->d_lam, h->d_lam2, h->d_R, h->d_mask, h->d_pc[0], h->d_pc[1], h->d_pc[2],
                   h->d_pc[3], h->d_pc[4], h->d_pc[5], h->d_own_in[0], h->d_own_in[1],
                   h->d_own_in[2], h->d_own_in[3], h->d_own_in[4], h->d_own_in[5], h->d_own_flag,
@@ -925,7 +1059,9 @@ void free_all(qesb_handle *h)
                   h->d_bad, h->d_err, h->d_state, h->d_u, h->d_v, h->d_w};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  h->list.destroy();
   if (h->h_state) cudaFreeHost(h->h_state);
+  if (h->h_ctl) cudaFreeHost(h->h_ctl);
   for (auto &e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -990,8 +1126,10 @@ qesb_status qesb_create(const qesb_grid *grid, float tol, int device, qesb_handl
   TRY(dalloc(&h->d_val, 6 * G.Z));
   TRY(dalloc(&h->d_bad, 1));
   TRY(dalloc(&h->d_state, 1));
+  TRY(h->list.create(1));
   TRY(ensure_err(h, 1024));
-  if (cudaMallocHost((void **)&h->h_state, sizeof(SolveState)) != cudaSuccess)
+  if (cudaMallocHost((void **)&h->h_state, sizeof(SolveState)) != cudaSuccess ||
+      cudaMallocHost((void **)&h->h_ctl, sizeof(SweepCtl)) != cudaSuccess)
     return fail(qesb_fail(QESB_ERR_NOMEM, "cudaMallocHost failed"));
   for (auto &e : h->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaEventCreate failed"));
@@ -1235,23 +1373,27 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
   if (!h->have_inputs || !h->packed) return qesb_fail(QESB_ERR_STATE, "qesb_time_sweeps needs stair-step inputs");
   CK(cudaSetDevice(h->device));
   if (pick_variant(h) >= kSplitVariant) {
-    const SplitVariant &sv = kSplitVariants[pick_variant(h) - kSplitVariant];
+    const SweepVariant &sv = kSweepVariants[pick_variant(h) - kSplitVariant];
+    CKS(sweep_prepare(sv));
     CKS(ensure_err(h, n + 1));
     cudaStream_t s = h->stream;
     CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
-    const dim3 grid = split_grid(h->G, sv, h->device), block(32, sv.rpb);
-    const SplitArgs a = split_args(h, 1 << 30);
-    SplitArgs never = a;
-    never.tol = -1.0;  // no stop: every launch runs
+    const SweepDomain one = sweep_domain(h, 1 << 30, -1.0);  // tol < 0: every launch runs
+    CKS(h->list.upload({one}, sv.span, s));
+    const dim3 grid(sweep_ctas(sv, false, h->device)), block(32, sv.block_y);
+    SweepArgs a = h->list.a;
+    a.one = one;
     CK(cudaEventRecord(h->ev[0], s));
     for (int c = 0; c < n; ++c) {
-      sv.red<<<grid, block, 0, s>>>(never);
-      sv.black<<<grid, block, 0, s>>>(never);
+      sv.red<<<grid, block, sv.smem, s>>>(a);
+      sv.black<<<grid, block, sv.smem, s>>>(a);
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(h->ev[1], s));
     CK(cudaEventSynchronize(h->ev[1]));
     CK(cudaEventElapsedTime(ms, h->ev[0], h->ev[1]));
+    CK(cudaMemcpy(h->h_ctl, a.ctl, sizeof(SweepCtl), cudaMemcpyDeviceToHost));
+    if (h->h_ctl->fault) return qesb_fail(QESB_ERR_CUDA, "sweep stage wait gave up");
     if (k) *k = 1;
     return QESB_OK;
   }
@@ -1274,14 +1416,14 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
   return QESB_OK;
 }
 
-int qesb_num_variants(void) { return kSplitVariant + kNumSplit; }
+int qesb_num_variants(void) { return kAllVariants; }
 
 qesb_status qesb_autotune(qesb_handle *h, int *best, float *us_per_iter, int n_variants)
 {
   if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
   if (!h->have_inputs || !h->packed) return qesb_fail(QESB_ERR_STATE, "qesb_autotune needs stair-step inputs");
   CK(cudaSetDevice(h->device));
-  const int nv = kSplitVariant + kNumSplit;
+  const int nv = kAllVariants;
   const size_t np = pad_alloc(h->G);
   float *saved = nullptr;
   CKS(dalloc(&saved, np));
@@ -1322,6 +1464,97 @@ qesb_status qesb_autotune(qesb_handle *h, int *best, float *us_per_iter, int n_v
   return QESB_OK;
 }
 
+qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *const *u, float *const *v,
+                             float *const *w, qesb_stats *st)
+{
+  if (!hs || n <= 0 || itermax < 0) return qesb_fail(QESB_ERR_ARG, "qesb_solve_batch: bad argument");
+  for (int i = 0; i < n; ++i) {
+    if (!hs[i]) return qesb_fail(QESB_ERR_ARG, "qesb_solve_batch: null handle %d", i);
+    if (!hs[i]->have_inputs) return qesb_fail(QESB_ERR_STATE, "qesb_solve_batch: domain %d has no inputs", i);
+    if (!hs[i]->packed || hs[i]->opt_path != 1)
+      return qesb_fail(QESB_ERR_STATE, "qesb_solve_batch: domain %d is not on the packed (stair-step) path", i);
+    if (hs[i]->device != hs[0]->device) return qesb_fail(QESB_ERR_ARG, "qesb_solve_batch: handles on two devices");
+    for (int k = 0; k < i; ++k)
+      if (hs[k] == hs[i]) return qesb_fail(QESB_ERR_ARG, "qesb_solve_batch: handle %d repeated", i);
+  }
+  qesb_handle *h0 = hs[0];
+  CK(cudaSetDevice(h0->device));
+  cudaStream_t s = h0->stream;
+  // launch shape: handles[0]'s "variant" option when it names a sweep shape,
+  // else its grid's autotuned shape when that is one, else the default
+  int vi = h0->opt_variant >= kSplitVariant ? h0->opt_variant : tuned_variant(h0->G);
+  if (vi < kSplitVariant) vi = kSplitVariant + kDefaultSweep;
+  const SweepVariant &sv = kSweepVariants[vi - kSplitVariant];
+  CK(cudaEventRecord(h0->ev[0], s));
+  std::vector<SweepDomain> doms(n);
+  double cells = 0;
+  for (int i = 0; i < n; ++i) {
+    qesb_handle *h = hs[i];
+    const DevGrid &G = h->G;
+    CKS(ensure_err(h, std::max(itermax, 1)));
+    k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(
+        G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_u0, h->d_v0,
+        h->d_w0, h->d_dz, h->dx, h->dy, h->d_R);
+    CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
+    CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+    k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam, h->d_lam_s);
+    k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_R, h->d_R_s);
+    CK(cudaGetLastError());
+    doms[i] = sweep_domain(h, itermax, (double)h->tol);
+    cells += (double)G.XY * G.Z;
+  }
+  SweepList list;
+  CKS(list.create(n));
+  qesb_status qs = list.upload(doms, sv.span, s);
+  int launched = 0;
+  if (qs == QESB_OK) {
+    k_sweep_stamp<<<1, 1, 0, s>>>(list.a.ctl);
+    SweepGraph gx;
+    if (itermax > 0)
+      qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, itermax, h0->opt_graph != 0, &gx, h0->h_ctl,
+                          &launched);
+    gx.reset();
+  }
+  const unsigned long long t0 = h0->h_ctl->t0;
+  CK(cudaEventRecord(h0->ev[2], s));
+  for (int i = 0; i < n && qs == QESB_OK; ++i) {
+    qesb_handle *h = hs[i];
+    const DevGrid &G = h->G;
+    k_split_mirror_ring<<<G.Y, 128, 0, s>>>(G, h->S, h->d_lam_s);
+    k_split_to_pad<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam_s, h->d_lam);
+    k_correct<<<row_grid(G, G.FY, G.FZ, G.FX), 256, 0, s>>>(
+        G, h->d_lam, h->d_in[1], h->d_in[3], h->d_in[5], h->d_flag, h->d_u0, h->d_v0, h->d_w0, h->d_dz, h->dx,
+        h->dy, u ? u[i] : nullptr, v ? v[i] : nullptr, w ? w[i] : nullptr);
+    cudaError_t ce = cudaGetLastError();
+    if (ce != cudaSuccess) qs = qesb_fail(QESB_ERR_CUDA, "batch finish: %s", cudaGetErrorString(ce));
+  }
+  CK(cudaEventRecord(h0->ev[3], s));
+  cudaError_t se = cudaStreamSynchronize(s);
+  list.destroy();
+  if (qs != QESB_OK) return qs;
+  if (se != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "batch: %s", cudaGetErrorString(se));
+  float ms_all = 0;
+  CK(cudaEventElapsedTime(&ms_all, h0->ev[0], h0->ev[3]));
+  int nan_at = -1;
+  for (int i = 0; i < n; ++i) {
+    SolveState sti;
+    CK(cudaMemcpy(&sti, hs[i]->d_state, sizeof sti, cudaMemcpyDeviceToHost));
+    if (sti.nan && nan_at < 0) nan_at = i;
+    if (st) {
+      st[i].iterations = itermax > 0 ? sti.it : 0;
+      st[i].converged = sti.converged;
+      st[i].residual = itermax > 0 ? sti.residual : 1.0;
+      st[i].ms_total = ms_all;
+      st[i].ms_sor = sti.t_done > t0 ? (double)(sti.t_done - t0) * 1e-6 : 0.0;
+      st[i].path = 1;
+      st[i].sweeps_per_launch = 1;
+      st[i].launches = 2 * launched;
+    }
+  }
+  if (nan_at >= 0) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d", nan_at);
+  return QESB_OK;
+}
+
 qesb_status qesb_set_tolerance(qesb_handle *h, float tol)
 {
   if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
@@ -1344,8 +1577,8 @@ qesb_status qesb_set_option(qesb_handle *h, const char *key, int value)
   } else if (k == "autotune") {
     h->opt_autotune = value ? 1 : 0;
   } else if (k == "variant") {
-    if (value < -1 || value >= kSplitVariant + kNumSplit)
-      return qesb_fail(QESB_ERR_ARG, "variant must be in [-1, %d)", kSplitVariant + kNumSplit);
+    if (value < -1 || value >= kAllVariants)
+      return qesb_fail(QESB_ERR_ARG, "variant must be in [-1, %d)", kAllVariants);
     h->opt_variant = value;
   } else {
     return qesb_fail(QESB_ERR_ARG, "unknown option '%s'", key);

@@ -18,10 +18,13 @@
 // kernel also applies the ground mirror lambda(k=0) <- lambda(k=1) to interior
 // rows (Solver_CPU_RB.cpp:155-162), and its last CTA to finish runs the
 // convergence poll, so one iteration is two launches and no host round trip.
+// The kernels sweep a domain list (qesb_sweep.cuh): one domain for a single
+// solve, every unfinished domain of a batch otherwise.
 #pragma once
 #include <type_traits>
 
 #include "qesb_device.cuh"
+#include "qesb_sweep.cuh"
 
 namespace qesb {
 
@@ -31,58 +34,74 @@ struct SplitGeom {
   __host__ __device__ long row(int j, int k, int Y) const { return ((long)k * Y + j) * PQ; }
 };
 
-struct SplitArgs {
-  DevGrid G;
-  SplitGeom S;
-  float *lam;           // [2][CS]
-  const float *R;       // [2][CS]
-  const uint8_t *mask;  // [2][CS]
-  const float *val;     // [6][Z]
-  const float *inv;     // [Z][64]
-  double *err;
-  SolveState *st;
-  int itermax;
-  double tol;
-};
-
-// Convergence poll for the iteration st->it (see k_poll in qesb_solver.cu for
-// the loop condition); run by one thread once every CTA's error is in.
-__device__ __forceinline__ void poll_one(SolveState *st, const double *err, double tol, int itermax)
-{
-  const int it = st->it;
-  const double e = err[it];
-  st->residual = e;
-  st->it = it + 1;
-  st->cur = 0;
-  if (isnan(e)) {
-    st->done = 1;
-    st->nan = 1;
-  } else if (!(e > tol)) {
-    st->done = 1;
-    st->converged = 1;
-  } else if (it + 1 >= itermax) {
-    st->done = 1;
-  }
-}
-
-// One colour of the sweep over rows j in [1, Y-2], k in [1, Z-2]. Persistent:
-// the grid holds as many CTAs as fit on the GPU at once and each warp sweeps a
-// contiguous range of rows, so it pays the start-up latency and its share of
-// the block reduction once, reloads the per-layer tables only when k changes,
-// and never waits on another warp inside the sweep.
-template <int COLOUR, int RPB, int U, int STRIDED>
-__global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
-{
-  SolveState *S = a.st;
-  if (S->done) return;
-  const DevGrid &G = a.G;
-  const int it = S->it;
-  const int nrows = (G.Y - 2) * (G.Z - 2);
-  const int lane = threadIdx.x;
-  const float c1 = 1.0f - kOmega;
-  float *L = a.lam;
+// The current domain of a warp walking rows of a domain list: its fields,
+// per-layer tables, and the warp's running FP64 max|dlambda| for it.
+struct SplitDom {
+  int X = 0, Y = 0, Z = 0, PQ = 0;
+  long CS = 0;
+  float *L = nullptr;
+  const float *R = nullptr, *val = nullptr, *inv_all = nullptr;
+  const uint8_t *mask = nullptr;
+  double *err = nullptr;
+  int it = 0;
+  int kcur = -1;
+  float ve = 0, vf = 0, vg = 0, vh = 0, vm = 0, vn = 0, inv63 = 0;
+  const float *inv = nullptr;
   double dmax = 0.0;    // warp-wide max |dlambda| so far (all lanes hold it)
   float dmax_f = 0.0f;  // largest float <= dmax
+
+  __device__ __forceinline__ void load(const SweepDomain &D)
+  {
+    X = D.X;
+    Y = D.Y;
+    Z = D.Z;
+    PQ = D.PQ;
+    CS = D.CS;
+    L = D.lam;
+    R = D.R;
+    mask = D.mask;
+    val = D.val;
+    inv_all = D.inv;
+    err = D.err;
+    it = D.st->it;
+    kcur = -1;
+  }
+  __device__ __forceinline__ void layer(int k)
+  {
+    if (k == kcur) return;
+    kcur = k;
+    ve = __ldg(val + 0 * Z + k);
+    vf = __ldg(val + 1 * Z + k);
+    vg = __ldg(val + 2 * Z + k);
+    vh = __ldg(val + 3 * Z + k);
+    vm = __ldg(val + 4 * Z + k);
+    vn = __ldg(val + 5 * Z + k);
+    inv = inv_all + k * 64;
+    inv63 = __ldg(inv + 63);
+  }
+  // Folds the warp's max into err[it]; the read skips the atomic when an
+  // equal or larger value is already there (the common case).
+  __device__ __forceinline__ void flush(int lane)
+  {
+    const double v = warp_max_d(dmax);
+    if (lane == 0 && err && v != 0.0) {
+      const double cur = *reinterpret_cast<volatile double *>(err + it);
+      if (!(cur >= v)) atomic_max_nonneg(err + it, v);
+    }
+    dmax = 0.0;
+    dmax_f = 0.0f;
+  }
+  // err[] is poll-read only after every CTA's flushes (last-CTA protocol).
+};
+
+// Walks the rows r of the warp's share of the flattened active-row space,
+// switching domain (and flushing the error) when r leaves the current one.
+// Calls body(D, j, k) for each row.
+template <int RPB, int STRIDED, bool MULTI, class Body>
+__device__ __forceinline__ void split_rows(const SweepArgs &b, int na, SplitDom &D, Body body)
+{
+  const int lane = threadIdx.x;
+  const int nrows = MULTI ? b.uoff[na] : b.one.rows;
   // Row order: STRIDED = 1 sends the warps through the rows together (warp w
   // takes rows w, w + warps, ...), so the rows in flight form one window and
   // DRAM sees a few long streams; STRIDED = 0 gives each warp a contiguous
@@ -91,41 +110,77 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
   const int r_begin = STRIDED ? w : (int)((long)nrows * w / warps);
   const int r_end = STRIDED ? nrows : (int)((long)nrows * (w + 1) / warps);
   const int r_step = STRIDED ? warps : 1;
-  int kcur = -1;
-  float ve = 0, vf = 0, vg = 0, vh = 0, vm = 0, vn = 0, inv63 = 0;
-  const float *inv = a.inv;
+  if (r_begin >= r_end) return;
+  int slot = MULTI ? sweep_slot(b.uoff, na, r_begin) : 0;
+  int lo = MULTI ? b.uoff[slot] : 0, hi = MULTI ? b.uoff[slot + 1] : nrows;
+  D.load(sweep_dom<MULTI>(b, slot));
   for (int r = r_begin; r < r_end; r += r_step) {
-    const int k = 1 + r / (G.Y - 2), j = 1 + r % (G.Y - 2);
-    if (k != kcur) {
-      kcur = k;
-      ve = __ldg(a.val + 0 * G.Z + k);
-      vf = __ldg(a.val + 1 * G.Z + k);
-      vg = __ldg(a.val + 2 * G.Z + k);
-      vh = __ldg(a.val + 3 * G.Z + k);
-      vm = __ldg(a.val + 4 * G.Z + k);
-      vn = __ldg(a.val + 5 * G.Z + k);
-      inv = a.inv + k * 64;
-      inv63 = __ldg(inv + 63);
+    if (MULTI && r >= hi) {
+      D.flush(lane);
+      while (r >= hi) {
+        ++slot;
+        lo = hi;
+        hi = b.uoff[slot + 1];
+      }
+      D.load(sweep_dom<MULTI>(b, slot));
     }
+    const int local = r - lo;
+    const int k = 1 + local / (D.Y - 2), j = 1 + local % (D.Y - 2);
+    D.layer(k);
+    body(j, k);
+  }
+}
+
+// Ground mirror of row j after its black update, both colours:
+// (i, j, 0) <- (i, j, 1) (Solver_CPU_RB.cpp:155-162). The plane-0 cell of
+// colour c mirrors the plane-1 cell of colour 1-c at the same q. The black
+// plane-1 values are this warp's own; the red ones are read-only during the
+// black kernel.
+__device__ __forceinline__ void split_mirror_row(const SplitDom &D, int j, int lane)
+{
+  __syncwarp();  // one warp owns the row: its black updates land before the copies
+  const long b1 = 1 * D.CS + ((long)1 * D.Y + j) * D.PQ, r0 = 0 * D.CS + (long)j * D.PQ;
+  const long r1 = 0 * D.CS + ((long)1 * D.Y + j) * D.PQ, b0 = 1 * D.CS + (long)j * D.PQ;
+  const int qn = (D.X + 1) >> 1;
+  for (int q = lane; q < qn; q += 32) {
+    D.L[r0 + q] = D.L[b1 + q];
+    D.L[b0 + q] = D.L[r1 + q];
+  }
+}
+
+// One colour of the sweep over rows j in [1, Y-2], k in [1, Z-2] of every
+// unfinished domain. Persistent: the grid holds as many CTAs as fit on the
+// GPU at once and each warp sweeps its share of the rows, so it pays the
+// start-up latency once, reloads the per-layer tables only when k changes,
+// and never waits on another warp inside the sweep.
+template <int COLOUR, int RPB, int U, int STRIDED, bool MULTI>
+__global__ void __launch_bounds__(32 * RPB) k_sor_split(SweepArgs b)
+{
+  const int na = b.ctl->nactive;
+  if (na <= 0) return;
+  const int lane = threadIdx.x;
+  const float c1 = 1.0f - kOmega;
+  SplitDom D;
+  split_rows<RPB, STRIDED, MULTI>(b, na, D, [&](int j, int k) {
     const int i0 = (COLOUR + j + k) & 1;
-    const long own = COLOUR * a.S.CS + a.S.row(j, k, G.Y);
-    const long oth = (1 - COLOUR) * a.S.CS + a.S.row(j, k, G.Y);
+    const long own = COLOUR * D.CS + ((long)k * D.Y + j) * D.PQ;
+    const long oth = (1 - COLOUR) * D.CS + ((long)k * D.Y + j) * D.PQ;
     // Updated cells of this row: i in [1, X-2], i = i0 + 2q. Every load goes
     // through the read-only path: a cell's own value is read once, by the lane
     // that then writes it; the other colour, R and the mask are not written
     // during this half-sweep except by the ground-mirror copies below, which a
     // warp makes only after its own reads of those cells.
     const int qlo = i0 ? 0 : 1;
-    const int qhi = (G.X - 2 - i0) >> 1;  // inclusive
-    float *pw = L + own;
-    const float *pxm = L + oth + i0 - 1;
-    const float *pxp = L + oth + i0;
-    const float *pym = L + oth - a.S.PQ;
-    const float *pyp = L + oth + a.S.PQ;
-    const float *pzm = L + oth - (long)G.Y * a.S.PQ;
-    const float *pzp = L + oth + (long)G.Y * a.S.PQ;
-    const float *pr = a.R + own;
-    const uint8_t *pm = a.mask + own;
+    const int qhi = (D.X - 2 - i0) >> 1;  // inclusive
+    float *pw = D.L + own;
+    const float *pxm = D.L + oth + i0 - 1;
+    const float *pxp = D.L + oth + i0;
+    const float *pym = D.L + oth - D.PQ;
+    const float *pyp = D.L + oth + D.PQ;
+    const float *pzm = D.L + oth - (long)D.Y * D.PQ;
+    const float *pzp = D.L + oth + (long)D.Y * D.PQ;
+    const float *pr = D.R + own;
+    const uint8_t *pm = D.mask + own;
     // One batch: U cells per lane at q0b + 32u. PRED: a slot is live only if
     // inside the row (the row's last, partial batch); dead slots load nothing.
     // All-fluid warps skip the wall-mask selects. The error is FP64-exact
@@ -161,16 +216,18 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
       if (__all_sync(0xffffffffu, full)) {
 #pragma unroll
         for (int u = 0; u < U; ++u)
-          nv[u] = inv63 * (ve * xp[u] + vf * xm[u] + vg * yp[u] + vh * ym[u] + vm * zp[u] + vn * zm[u] - rr[u]) +
+          nv[u] = D.inv63 * (D.ve * xp[u] + D.vf * xm[u] + D.vg * yp[u] + D.vh * ym[u] + D.vm * zp[u] +
+                             D.vn * zm[u] - rr[u]) +
                   c1 * old[u];
       } else {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const unsigned m_ = mk[u];
-          const float e = (m_ & 1u) ? ve : 0.0f, f = (m_ & 2u) ? vf : 0.0f;
-          const float g = (m_ & 4u) ? vg : 0.0f, hh = (m_ & 8u) ? vh : 0.0f;
-          const float m = (m_ & 16u) ? vm : 0.0f, n = (m_ & 32u) ? vn : 0.0f;
-          nv[u] = __ldg(inv + m_) * (e * xp[u] + f * xm[u] + g * yp[u] + hh * ym[u] + m * zp[u] + n * zm[u] - rr[u]) +
+          const float e = (m_ & 1u) ? D.ve : 0.0f, f = (m_ & 2u) ? D.vf : 0.0f;
+          const float g = (m_ & 4u) ? D.vg : 0.0f, hh = (m_ & 8u) ? D.vh : 0.0f;
+          const float m = (m_ & 16u) ? D.vm : 0.0f, n = (m_ & 32u) ? D.vn : 0.0f;
+          nv[u] = __ldg(D.inv + m_) * (e * xp[u] + f * xm[u] + g * yp[u] + hh * ym[u] + m * zp[u] + n * zm[u] -
+                                       rr[u]) +
                   c1 * old[u];
         }
       }
@@ -179,17 +236,17 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
       for (int u = 0; u < U; ++u) {
         if (live[u]) {
           pw[q0b + 32 * u] = nv[u];
-          big |= !(fabsf(nv[u] - old[u]) < dmax_f);
+          big |= !(fabsf(nv[u] - old[u]) < D.dmax_f);
         }
       }
       if (__any_sync(0xffffffffu, big)) {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const double d = fabs((double)nv[u] - (double)old[u]);
-          if (live[u] && (d > dmax || d != d)) dmax = d;
+          if (live[u] && (d > D.dmax || d != d)) D.dmax = d;
         }
-        dmax = warp_max_d(dmax);
-        dmax_f = __double2float_rd(dmax);
+        D.dmax = warp_max_d(D.dmax);
+        D.dmax_f = __double2float_rd(D.dmax);
       }
     };
     int q0 = qlo + lane;
@@ -198,47 +255,10 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
     const int lane_off = 31 - lane;
     for (; q0 + lane_off + 32 * (U - 1) <= qhi; q0 += 32 * U) batch(q0, std::false_type{});
     if (q0 - lane <= qhi) batch(q0, std::true_type{});
-    if (COLOUR == 1 && k == 1) {
-      __syncwarp();  // one warp owns the row: its black updates land before the copies
-      // ground mirror of this row, both colours: (i, j, 0) <- (i, j, 1); the
-      // plane-0 cell of colour c mirrors the plane-1 cell of colour 1-c at
-      // the same q. The black plane-1 values are this warp's own; the red
-      // plane-1 values are read-only during this kernel.
-      const long b1 = 1 * a.S.CS + a.S.row(j, 1, G.Y), r0 = 0 * a.S.CS + a.S.row(j, 0, G.Y);
-      const long r1 = 0 * a.S.CS + a.S.row(j, 1, G.Y), b0 = 1 * a.S.CS + a.S.row(j, 0, G.Y);
-      const int qn = (G.X + 1) >> 1;
-      for (int q = lane; q < qn; q += 32) {
-        L[r0 + q] = L[b1 + q];
-        L[b0 + q] = L[r1 + q];
-      }
-    }
-  }
-  // block max -> err[it], then (black) last-CTA poll
-  __shared__ double s_part[RPB];
-  __shared__ bool s_last;
-  double v = warp_max_d(dmax);
-  if (lane == 0) s_part[threadIdx.y] = v;
-  __syncthreads();
-  if (threadIdx.y == 0) {
-    double x = lane < RPB ? s_part[lane] : 0.0;
-    x = warp_max_d(x);
-    if (lane == 0) {
-      if (x != 0.0) atomic_max_nonneg(a.err + it, x);
-      if (COLOUR == 1) {
-        __threadfence();
-        const unsigned t = atomicAdd(&S->blocks_done, 1u);
-        s_last = (t == gridDim.x - 1);
-      }
-    }
-  }
-  if (COLOUR == 1) {
-    __syncthreads();
-    if (s_last && lane == 0 && threadIdx.y == 0) {
-      __threadfence();
-      S->blocks_done = 0;
-      poll_one(S, a.err, a.tol, a.itermax);
-    }
-  }
+    if (COLOUR == 1 && k == 1) split_mirror_row(D, j, lane);
+  });
+  sweep_flush_end<MULTI>(D.dmax, MULTI ? (D.err ? D.err + D.it : nullptr) : b.one.err + b.one.st->it);
+  if (COLOUR == 1) sweep_finish_black<false, MULTI>(b, na);
 }
 
 // Vectorised variant of k_sor_split: each lane updates four consecutive
@@ -249,56 +269,28 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SplitArgs a)
 // across the group edge (q-1 when i0 = 0, q+4 when i0 = 1), taken from the
 // neighbouring lane by a shuffle, or loaded at the warp's edge. Cells of the
 // group outside [qlo, qhi] are rewritten with the value this lane read.
-template <int COLOUR, int RPB, int STRIDED>
-__global__ void __launch_bounds__(32 * RPB) k_sor_split4(SplitArgs a)
+template <int COLOUR, int RPB, int STRIDED, bool MULTI>
+__global__ void __launch_bounds__(32 * RPB) k_sor_split4(SweepArgs b)
 {
-  SolveState *S = a.st;
-  if (S->done) return;
-  const DevGrid &G = a.G;
-  const int it = S->it;
-  const int nrows = (G.Y - 2) * (G.Z - 2);
+  const int na = b.ctl->nactive;
+  if (na <= 0) return;
   const int lane = threadIdx.x;
   const float c1 = 1.0f - kOmega;
-  float *L = a.lam;
-  double dmax = 0.0;
-  float dmax_f = 0.0f;
-  // Row order: STRIDED = 1 sends the warps through the rows together (warp w
-  // takes rows w, w + warps, ...), so the rows in flight form one window and
-  // DRAM sees a few long streams; STRIDED = 0 gives each warp a contiguous
-  // range (fewer per-layer table reloads, scattered streams).
-  const int warps = gridDim.x * RPB, w = blockIdx.x * RPB + threadIdx.y;
-  const int r_begin = STRIDED ? w : (int)((long)nrows * w / warps);
-  const int r_end = STRIDED ? nrows : (int)((long)nrows * (w + 1) / warps);
-  const int r_step = STRIDED ? warps : 1;
-  int kcur = -1;
-  float ve = 0, vf = 0, vg = 0, vh = 0, vm = 0, vn = 0, inv63 = 0;
-  const float *inv = a.inv;
-  for (int r = r_begin; r < r_end; r += r_step) {
-    const int k = 1 + r / (G.Y - 2), j = 1 + r % (G.Y - 2);
-    if (k != kcur) {
-      kcur = k;
-      ve = __ldg(a.val + 0 * G.Z + k);
-      vf = __ldg(a.val + 1 * G.Z + k);
-      vg = __ldg(a.val + 2 * G.Z + k);
-      vh = __ldg(a.val + 3 * G.Z + k);
-      vm = __ldg(a.val + 4 * G.Z + k);
-      vn = __ldg(a.val + 5 * G.Z + k);
-      inv = a.inv + k * 64;
-      inv63 = __ldg(inv + 63);
-    }
+  SplitDom D;
+  split_rows<RPB, STRIDED, MULTI>(b, na, D, [&](int j, int k) {
     const int i0 = (COLOUR + j + k) & 1;
-    const long own = COLOUR * a.S.CS + a.S.row(j, k, G.Y);
-    const long oth = (1 - COLOUR) * a.S.CS + a.S.row(j, k, G.Y);
+    const long own = COLOUR * D.CS + ((long)k * D.Y + j) * D.PQ;
+    const long oth = (1 - COLOUR) * D.CS + ((long)k * D.Y + j) * D.PQ;
     const int qlo = i0 ? 0 : 1;
-    const int qhi = (G.X - 2 - i0) >> 1;  // inclusive
-    float *pw = L + own;
-    const float *px = L + oth;
-    const float *pym = L + oth - a.S.PQ;
-    const float *pyp = L + oth + a.S.PQ;
-    const float *pzm = L + oth - (long)G.Y * a.S.PQ;
-    const float *pzp = L + oth + (long)G.Y * a.S.PQ;
-    const float *pr = a.R + own;
-    const uint8_t *pm = a.mask + own;
+    const int qhi = (D.X - 2 - i0) >> 1;  // inclusive
+    float *pw = D.L + own;
+    const float *px = D.L + oth;
+    const float *pym = D.L + oth - D.PQ;
+    const float *pyp = D.L + oth + D.PQ;
+    const float *pzm = D.L + oth - (long)D.Y * D.PQ;
+    const float *pzp = D.L + oth + (long)D.Y * D.PQ;
+    const float *pr = D.R + own;
+    const uint8_t *pm = D.mask + own;
     // warp-uniform loop over 128-cell spans; lane g-th group is live if its
     // first cell is inside the row (live lanes form a prefix of the warp)
     for (int g0 = 0; 4 * g0 <= qhi; g0 += 32) {
@@ -344,16 +336,18 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split4(SplitArgs a)
       if (__all_sync(0xffffffffu, full)) {
 #pragma unroll
         for (int t = 0; t < 4; ++t)
-          nv[t] = inv63 * (ve * xpv[t] + vf * xmv[t] + vg * ypv[t] + vh * ymv[t] + vm * zpv[t] + vn * zmv[t] - rv[t]) +
+          nv[t] = D.inv63 * (D.ve * xpv[t] + D.vf * xmv[t] + D.vg * ypv[t] + D.vh * ymv[t] + D.vm * zpv[t] +
+                             D.vn * zmv[t] - rv[t]) +
                   c1 * ov[t];
       } else {
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
           const unsigned m_ = up[t] ? mk[t] : 63u;
-          const float e = (m_ & 1u) ? ve : 0.0f, f = (m_ & 2u) ? vf : 0.0f;
-          const float g = (m_ & 4u) ? vg : 0.0f, hh = (m_ & 8u) ? vh : 0.0f;
-          const float m = (m_ & 16u) ? vm : 0.0f, n = (m_ & 32u) ? vn : 0.0f;
-          nv[t] = __ldg(inv + m_) * (e * xpv[t] + f * xmv[t] + g * ypv[t] + hh * ymv[t] + m * zpv[t] + n * zmv[t] - rv[t]) +
+          const float e = (m_ & 1u) ? D.ve : 0.0f, f = (m_ & 2u) ? D.vf : 0.0f;
+          const float g = (m_ & 4u) ? D.vg : 0.0f, hh = (m_ & 8u) ? D.vh : 0.0f;
+          const float m = (m_ & 16u) ? D.vm : 0.0f, n = (m_ & 32u) ? D.vn : 0.0f;
+          nv[t] = __ldg(D.inv + m_) * (e * xpv[t] + f * xmv[t] + g * ypv[t] + hh * ymv[t] + m * zpv[t] +
+                                       n * zmv[t] - rv[t]) +
                   c1 * ov[t];
         }
       }
@@ -361,55 +355,23 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split4(SplitArgs a)
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         nv[t] = up[t] ? nv[t] : ov[t];
-        big |= up[t] && !(fabsf(nv[t] - ov[t]) < dmax_f);
+        big |= up[t] && !(fabsf(nv[t] - ov[t]) < D.dmax_f);
       }
       if (live) *reinterpret_cast<float4 *>(pw + q) = make_float4(nv[0], nv[1], nv[2], nv[3]);
       if (__any_sync(0xffffffffu, big)) {
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
           const double d = fabs((double)nv[t] - (double)ov[t]);
-          if (up[t] && (d > dmax || d != d)) dmax = d;
+          if (up[t] && (d > D.dmax || d != d)) D.dmax = d;
         }
-        dmax = warp_max_d(dmax);
-        dmax_f = __double2float_rd(dmax);
+        D.dmax = warp_max_d(D.dmax);
+        D.dmax_f = __double2float_rd(D.dmax);
       }
     }
-    if (COLOUR == 1 && k == 1) {
-      __syncwarp();  // one warp owns the row: its black updates land before the copies
-      const long b1 = 1 * a.S.CS + a.S.row(j, 1, G.Y), r0 = 0 * a.S.CS + a.S.row(j, 0, G.Y);
-      const long r1 = 0 * a.S.CS + a.S.row(j, 1, G.Y), b0 = 1 * a.S.CS + a.S.row(j, 0, G.Y);
-      const int qn = (G.X + 1) >> 1;
-      for (int qq = lane; qq < qn; qq += 32) {
-        L[r0 + qq] = L[b1 + qq];
-        L[b0 + qq] = L[r1 + qq];
-      }
-    }
-  }
-  __shared__ double s_part[RPB];
-  __shared__ bool s_last;
-  double v = warp_max_d(dmax);
-  if (lane == 0) s_part[threadIdx.y] = v;
-  __syncthreads();
-  if (threadIdx.y == 0) {
-    double x = lane < RPB ? s_part[lane] : 0.0;
-    x = warp_max_d(x);
-    if (lane == 0) {
-      if (x != 0.0) atomic_max_nonneg(a.err + it, x);
-      if (COLOUR == 1) {
-        __threadfence();
-        const unsigned t = atomicAdd(&S->blocks_done, 1u);
-        s_last = (t == gridDim.x - 1);
-      }
-    }
-  }
-  if (COLOUR == 1) {
-    __syncthreads();
-    if (s_last && lane == 0 && threadIdx.y == 0) {
-      __threadfence();
-      S->blocks_done = 0;
-      poll_one(S, a.err, a.tol, a.itermax);
-    }
-  }
+    if (COLOUR == 1 && k == 1) split_mirror_row(D, j, lane);
+  });
+  sweep_flush_end<MULTI>(D.dmax, MULTI ? (D.err ? D.err + D.it : nullptr) : b.one.err + b.one.st->it);
+  if (COLOUR == 1) sweep_finish_black<false, MULTI>(b, na);
 }
 
 // Plane-0 boundary ring (j = 0, Y-1 rows; i = 0, X-1 columns) <- plane 1.

@@ -1,0 +1,188 @@
+// Domain lists for the red/black half-sweep kernels: one solve is a list of
+// one domain, a batched solve (qesb_solve_batch) a list of many. The sweep
+// kernels spread the work units (rows, or 128-cell row spans) of the
+// unfinished domains over a persistent grid; the last CTA of each black
+// launch polls every unfinished domain (the loop condition of
+// Solver_CPU_RB.cpp:106, with max|dlambda| in FP64) and compacts the list,
+// so finished domains drop out of the next launch without a host round trip.
+#pragma once
+#include "qesb_device.cuh"
+
+namespace qesb {
+
+// One domain in the red/black split layout, as the sweep kernels see it.
+struct SweepDomain {
+  int X, Y, Z, PQ;
+  long CS;
+  int nch;    // 128-cell spans per colour row: ceil(PQ / 128)
+  int rows;   // (Y - 2) * (Z - 2) updated rows per colour
+  float *lam;           // [2][CS]
+  const float *R;       // [2][CS]
+  const uint8_t *mask;  // [2][CS]
+  const float *val;     // [6][Z]
+  const float *inv;     // [Z][64]
+  double *err;          // [itermax] FP64 max|dlambda| per iteration
+  SolveState *st;
+  int itermax;
+  double tol;
+};
+
+struct SweepCtl {
+  unsigned blocks_done;   // CTAs of the current black launch that have finished
+  int nactive;            // domains still iterating
+  int fault;              // a bounded stage wait gave up (the launch's results are void)
+  int pad;
+  unsigned long long t0;  // %globaltimer at the start of the batch
+};
+
+struct SweepArgs {
+  const SweepDomain *dom;  // [n]
+  int *active;             // [n]: indices of the unfinished domains, in batch order
+  int *uoff;               // [n + 1]: work-unit offsets over `active`
+  SweepCtl *ctl;
+  SweepDomain one;         // the domain of a single solve, read from the kernel
+                           // parameters by the MULTI = false instances
+};
+
+// Domain of active slot `slot` (MULTI) or the single solve's domain.
+template <bool MULTI>
+__device__ __forceinline__ const SweepDomain &sweep_dom(const SweepArgs &b, int slot)
+{
+  return MULTI ? b.dom[b.active[slot]] : b.one;
+}
+
+// Convergence poll for the iteration st->it (Solver_CPU_RB.cpp:106: the loop
+// runs while iter < itermax and max_error > tol); one thread per domain.
+__device__ __forceinline__ void poll_one(SolveState *st, const double *err, double tol, int itermax)
+{
+  const int it = st->it;
+  const double e = err[it];
+  st->residual = e;
+  st->it = it + 1;
+  st->cur = 0;
+  if (isnan(e)) {
+    st->done = 1;
+    st->nan = 1;
+  } else if (!(e > tol)) {
+    st->done = 1;
+    st->converged = 1;
+  } else if (it + 1 >= itermax) {
+    st->done = 1;
+  }
+}
+
+// Work units of a domain for a kernel family: rows (SPAN = false) or
+// 128-cell row spans (SPAN = true).
+template <bool SPAN>
+__device__ __forceinline__ int sweep_units(const SweepDomain &D)
+{
+  return SPAN ? D.rows * D.nch : D.rows;
+}
+
+// End of a black launch. Every thread of the CTA calls it after its own error
+// flushes; the last CTA to arrive polls the unfinished domains and rebuilds
+// the active list and unit offsets for the next launch.
+template <bool SPAN, bool MULTI>
+__device__ __forceinline__ void sweep_finish_black(const SweepArgs &b, int na)
+{
+  __syncthreads();
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x, lane = tid & 31;
+  if (tid >= 32) return;
+  unsigned last = 0;
+  if (lane == 0) {
+    __threadfence();
+    last = atomicAdd(&b.ctl->blocks_done, 1u) == gridDim.x - 1;
+  }
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (!last) return;
+  __threadfence();
+  if (!MULTI) {
+    if (lane == 0) {
+      poll_one(b.one.st, b.one.err, b.one.tol, b.one.itermax);
+      const bool done = b.one.st->done;
+      if (done) b.one.st->t_done = global_ns();
+      b.ctl->nactive = done ? 0 : 1;
+      b.ctl->blocks_done = 0;
+    }
+    return;
+  }
+  int out = 0, base = 0;
+  for (int a0 = 0; a0 < na; a0 += 32) {
+    const int a = a0 + lane;
+    int d = -1, keep = 0, units = 0;
+    if (a < na) {
+      d = b.active[a];
+      const SweepDomain &D = b.dom[d];
+      poll_one(D.st, D.err, D.tol, D.itermax);
+      keep = !D.st->done;
+      if (!keep) D.st->t_done = global_ns();
+      units = sweep_units<SPAN>(D);
+    }
+    __syncwarp();
+    const unsigned mball = __ballot_sync(0xffffffffu, keep);
+    const int pos = out + __popc(mball & ((1u << lane) - 1u));
+    int x = keep ? units : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (keep) {
+      b.active[pos] = d;
+      b.uoff[pos + 1] = base + x;
+    }
+    out += __popc(mball);
+    base += __shfl_sync(0xffffffffu, x, 31);
+  }
+  if (lane == 0) {
+    b.uoff[0] = 0;
+    b.ctl->nactive = out;
+    b.ctl->blocks_done = 0;
+  }
+}
+
+// Slot of `active` holding unit u: the last slot with uoff[slot] <= u.
+__device__ __forceinline__ int sweep_slot(const int *uoff, int na, int u)
+{
+  int lo = 0, hi = na - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (uoff[mid] <= u) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Last error fold of a launch into dst (the domain's err[it]). A single
+// solve's warps all work on one domain: their maxima meet in shared memory
+// and the CTA makes one atomic. A list's warps may be on different domains:
+// each warp folds its own, skipping the atomic when dst already holds as
+// much. Every thread of the CTA calls it; dst may be null for warps of a list
+// that had no rows.
+template <bool MULTI>
+__device__ __forceinline__ void sweep_flush_end(double dmax, double *dst)
+{
+  const int lane = threadIdx.x & 31;
+  const double v = warp_max_d(dmax);
+  if (MULTI) {
+    if (lane == 0 && dst && v != 0.0) {
+      const double cur = *reinterpret_cast<volatile double *>(dst);
+      if (!(cur >= v)) atomic_max_nonneg(dst, v);
+    }
+    return;
+  }
+  __shared__ double s_part[32];
+  const int wid = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
+  const int nw = (blockDim.x * blockDim.y) >> 5;
+  if (lane == 0) s_part[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    double x = lane < nw ? s_part[lane] : 0.0;
+    x = warp_max_d(x);
+    if (lane == 0 && x != 0.0) atomic_max_nonneg(dst, x);
+  }
+}
+
+__global__ void k_sweep_stamp(SweepCtl *ctl) { ctl->t0 = global_ns(); }
+
+}  // namespace qesb

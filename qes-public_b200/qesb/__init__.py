@@ -105,6 +105,8 @@ def lib() -> C.CDLL:
             "qesb_set_tolerance": ([V, C.c_float], C.c_int),
             "qesb_time_sweeps": ([V, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)], C.c_int),
             "qesb_autotune": ([V, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int], C.c_int),
+            "qesb_solve_batch": ([C.POINTER(V), C.c_int, C.c_int, C.POINTER(V), C.POINTER(V), C.POINTER(V),
+                                  C.POINTER(Stats)], C.c_int),
             "qesb_num_variants": ([], C.c_int),
             "qesb_set_option": ([V, C.c_char_p, C.c_int], C.c_int),
             "qesb_set_stream": ([V, V], C.c_int),
@@ -357,6 +359,25 @@ class Solver_B200:
         out = np.empty(self.domain.numCellCentered(), dtype=np.float32)
         check(lib().qesb_get_divergence(self._h, _ptr(out)))
         return out
+
+
+def solve_batch(solvers, itermax: int, u_ptrs=None, v_ptrs=None, w_ptrs=None) -> list[dict]:
+    """qesb_solve_batch: the solvers' domains (inputs already set, lambda as the
+    start) solved together; u/v/w_ptrs are lists of device pointers (ints) or
+    None. Returns each domain's stats."""
+    n = len(solvers)
+    V = C.c_void_p
+    hs = (V * n)(*[s._h for s in solvers])
+
+    def ptrs(p):
+        return None if p is None else (V * n)(*p)
+
+    st = (Stats * n)()
+    check(lib().qesb_solve_batch(hs, n, int(itermax), ptrs(u_ptrs), ptrs(v_ptrs), ptrs(w_ptrs), st))
+    out = [st[i].as_dict() for i in range(n)]
+    for s, d in zip(solvers, out):
+        s.last_stats = d
+    return out
 
 
 def solve_noalloc(domain: Domain, tol: float, itermax: int, e, f, g, h, m, n, icellflag, u0, v0, w0,

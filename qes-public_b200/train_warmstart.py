@@ -146,11 +146,14 @@ def main():
     ap.add_argument("--target-iters", type=int, default=4000)
     ap.add_argument("--train-workload", default="city128")
     ap.add_argument("--eval-workload", default="city256")
+    ap.add_argument("--levels", type=int, default=4, help="encoder-decoder levels (channels 16, 32, 64, 128, 128, ...)")
+    ap.add_argument("--seed", type=int, default=0, help="weight initialisation seed")
     ap.add_argument("--coarse-beta", type=float, default=0.0,
                     help="weight of the 8x8x8-block error term of the loss (0: plain MSE)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
-    net = ws.WarmStartNet(device=0, seed=0)
+    channels = tuple(min(128, 16 << l) for l in range(args.levels))
+    net = ws.WarmStartNet(device=0, seed=args.seed, channels=channels)
     t0 = time.time()
     X, T, weight, s = generate(net, args.train, args.train_workload, args.target_iters)
     t_gen = time.time() - t0

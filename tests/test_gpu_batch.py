@@ -1,0 +1,84 @@
+"""Batched solves (qesb_solve_batch): domains of different sizes solved in
+one persistent bulk-staged loop give, domain by domain, the bits of separate
+solves and of the oracle, each stopping on its own iteration."""
+import numpy as np
+import pytest
+
+import qesb
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _cities():
+    out = []
+    for (nx, ny, nz, seed, nb) in [(70, 45, 21, 9, 8), (131, 40, 15, 3, 6), (300, 19, 11, 5, 6), (40, 33, 9, 2, 3)]:
+        d = qesb.Domain(nx, ny, nz, 2.0, 2.0, 1.0, qesb.city_dz(nz, 1.0, 1.03))
+        c = qesb.city_random(d, seed, nb, fp=(6, 18), h=(4, 16))
+        out.append(qesb.city_build(d, c.buildings, c.inflow))
+    return out
+
+
+def _batch(ws, tol, itermax, lam0s, variant=-1):
+    import torch
+
+    solvers = [qesb.Solver_B200(w.domain, tol) for w in ws]
+    try:
+        if variant >= 0:
+            solvers[0].set_option("variant", variant)
+        for s, w, l0 in zip(solvers, ws, lam0s):
+            s.set_inputs(w)
+            if l0 is not None:
+                s.lambda_ = l0
+        outs = [[torch.zeros(w.domain.numFaceCentered(), dtype=torch.float32, device="cuda") for _ in range(3)]
+                for w in ws]
+        st = qesb.solve_batch(solvers, itermax, *[[o[q].data_ptr() for o in outs] for q in range(3)])
+        lams = [s.lambda_ for s in solvers]
+        winds = [[t.cpu().numpy() for t in o] for o in outs]
+        return st, lams, winds
+    finally:
+        for s in solvers:
+            s.close()
+
+
+@pytest.mark.parametrize("variant", [-1, 18, 21, 23, 26])
+def test_batch_matches_oracle_per_domain(variant):
+    ws = _cities()
+    rng = np.random.default_rng(11)
+    lam0s = [None, rng.standard_normal(ws[1].domain.numCellCentered()).astype(np.float32), None, None]
+    tol = 1.1e-3
+    st, lams, winds = _batch(ws, tol, 3000, lam0s, variant)
+    for w, l0, s, L, (u, v, ww) in zip(ws, lam0s, st, lams, winds):
+        d = w.domain
+        Lo, it, fe, _ = O.sor(d, w, O.divergence(d, w), tol, 3000, ordering=1, err_fp64=True, lam=l0)
+        assert s["iterations"] == it and s["converged"] == 1, (s, it)
+        np.testing.assert_array_equal(L, Lo)
+        uo, vo, wo = O.correct(d, w, Lo)
+        np.testing.assert_array_equal(u, uo)
+        np.testing.assert_array_equal(v, vo)
+        np.testing.assert_array_equal(ww, wo)
+        assert 0 < s["ms_sor"] <= s["ms_total"]
+    # the domains stop on different iterations
+    assert len({s["iterations"] for s in st}) > 1
+
+
+def test_batch_equals_single_solves_at_itermax():
+    ws = _cities()
+    st, lams, winds = _batch(ws, 1e-9, 57, [None] * len(ws))
+    for w, s, L in zip(ws, st, lams):
+        with qesb.Solver_B200(w.domain, 1e-9) as one:
+            one.set_option("variant", 19)
+            s1 = one.solve(w, 57)
+            assert s1["iterations"] == s["iterations"] == 57 and not s["converged"]
+            np.testing.assert_array_equal(one.lambda_, L)
+
+
+def test_batch_rejects_repeated_and_non_stair_step_handles():
+    w = _cities()[0]
+    with qesb.Solver_B200(w.domain, 1e-3) as s:
+        s.set_inputs(w)
+        with pytest.raises(qesb.QesbError):
+            qesb.solve_batch([s, s], 10)
+        s.set_option("path", 0)
+        with pytest.raises(qesb.QesbError):
+            qesb.solve_batch([s], 10)

@@ -51,7 +51,10 @@ def test_divergence_R_bit_exact(golden):
     np.testing.assert_array_equal(R, O.divergence(d, w))
 
 
-N_VARIANTS = 18  # fused tile shapes (0-4), scalar split (5-10), float4 split (11-13), window-order split (14-17)
+# fused tile shapes (0-4), scalar split (5-10), float4 split (11-13),
+# window-order split (14-17), bulk-copy staged (18-22), cp.async staged (23-27)
+N_VARIANTS = 28
+BULK = 18
 
 
 @pytest.mark.parametrize("variant", range(N_VARIANTS))
@@ -74,7 +77,28 @@ def test_fused_sweeps_bit_exact(variant):
     np.testing.assert_array_equal(ww, wo)
 
 
-@pytest.mark.parametrize("path,variant", [(0, -1), (1, 0), (1, 1), (1, 5)])
+def test_variant_count_matches_library():
+    assert qesb.lib().qesb_num_variants() == N_VARIANTS
+
+
+@pytest.mark.parametrize("variant", range(BULK, N_VARIANTS))
+@pytest.mark.parametrize("nx", [300, 515])
+def test_bulk_sweeps_multi_chunk_rows_bit_exact(variant, nx):
+    """Bulk-staged sweeps on rows longer than one 128-cell span (two and three
+    spans per colour row, the last one partial), against the oracle."""
+    d = qesb.Domain(nx, 19, 11, 2.0, 2.0, 1.0, qesb.city_dz(11, 1.0, 1.03))
+    c = qesb.city_random(d, 5, 6, fp=(6, 18), h=(4, 16))
+    w = qesb.city_build(d, c.buildings, c.inflow)
+    lam0 = np.random.default_rng(4).standard_normal(d.numCellCentered()).astype(np.float32)
+    u, v, ww, L, st, _ = gpu_solve(d, w, 23, lam=lam0, variant=variant)
+    uo, vo, wo, Lo, it, _ = O.solve(d, w, 1e-9, 23, ordering=1, lam=lam0)
+    assert st["path"] == 1 and st["iterations"] == it == 23
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(u, uo)
+    np.testing.assert_array_equal(ww, wo)
+
+
+@pytest.mark.parametrize("path,variant", [(0, -1), (1, 0), (1, 1), (1, 5), (1, BULK), (1, BULK + 3), (1, BULK + 5), (1, BULK + 8)])
 @pytest.mark.parametrize("tol", [2e-3, 1.1e-3, 7e-4])
 def test_stopping_rule_matches_oracle(golden, path, variant, tol):
     """A reachable tolerance: the loop stops on the same iteration as the
@@ -174,7 +198,7 @@ def test_graph_and_plain_launches_agree(golden, graph):
     np.testing.assert_array_equal(L, Lo)
 
 
-@pytest.mark.parametrize("variant", [1, 5])
+@pytest.mark.parametrize("variant", [1, 5, BULK + 1, BULK + 6])
 def test_full_size_city400_packed_equals_full_path(variant):
     """400x400x100 stretched city: after 24 iterations the packed paths (fused
     and split) and the full-coefficient path hold the same lambda bits and the

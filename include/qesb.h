@@ -62,6 +62,7 @@ typedef struct qesb_stats {
   int path;              /* 0 = full-coefficient sweep, 1 = packed wall-mask sweep */
   int sweeps_per_launch; /* iterations fused per sweep launch */
   int launches;          /* kernels this solve launched (including polls and early exits) */
+  int pre_iterations;    /* iterations of the over-relaxed pre-phase (qesb_set_prephase), 0 if none */
 } qesb_stats;
 
 /* Library and device. */
@@ -127,6 +128,18 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k);
  * inputs (the full-coefficient path has a single variant). */
 qesb_status qesb_autotune(qesb_handle *h, int *best, float *us_per_iter, int n_variants);
 int qesb_num_variants(void);
+
+/* Over-relaxed pre-phase (no reference counterpart; a warm start for the
+ * reference loop). When omega is in (1, 2) and max_iterations > 0, each solve
+ * on the packed sweep path first runs red-black SOR with this omega (same
+ * kernels and FP64 rule, omega/sum and 1 - omega in place of the reference's
+ * 1.78f, Solver_CPU_RB.cpp:118-125) from the current lambda until
+ * max|dlambda| <= tol or max_iterations; then the reference loop runs as
+ * always, with omega = 1.78 and the handle's tolerance, from that lambda. The
+ * result therefore meets exactly the reference's stopping rule; only the
+ * starting point differs. omega = 0 turns it off (the default). The fused
+ * tiled and full-coefficient paths ignore it. */
+qesb_status qesb_set_prephase(qesb_handle *h, float omega, float tol, int max_iterations);
 
 /* Batched solve (no reference counterpart: the reference solves one domain
  * per Solver::solve call, src/winds/Solver.h:108). Each of the n handles

@@ -44,6 +44,8 @@ def port() -> C.CDLL:
         L.qo_divergence.restype = None
         L.qo_sor.argtypes = [i, i, i, i, i] + [_V] * 8 + [f, i, _V, _V]
         L.qo_sor.restype = i
+        L.qo_sor_omega.argtypes = [i, i, i, i, i] + [_V] * 8 + [f, i, _V, _V, f]
+        L.qo_sor_omega.restype = i
         L.qo_correct.argtypes = [i, i, i, f, f] + [_V] * 11
         L.qo_correct.restype = None
         L.qo_divergence_f64.argtypes = [i, i, i, f, f] + [_V] * 11
@@ -93,15 +95,20 @@ def divergence(dom, w):
     return R
 
 
-def sor(dom, w, R, tol, itermax, ordering=1, err_fp64=True, lam=None, hist=False):
-    """Returns (lambda, iterations, final_error, history-or-None)."""
+def sor(dom, w, R, tol, itermax, ordering=1, err_fp64=True, lam=None, hist=False, omega=None):
+    """Returns (lambda, iterations, final_error, history-or-None). omega:
+    None for the reference's 1.78f, else the float omega of an over-relaxed
+    pre-phase."""
     Nx, Ny, Nz = dom.base
     L = np.zeros(dom.numCellCentered(), np.float32) if lam is None else lam.astype(np.float32).copy()
     H = np.zeros(max(itermax, 1), np.float64) if hist else None
     fe = C.c_double()
-    it = port().qo_sor(ordering, int(err_fp64), Nx, Ny, Nz, _p(w.e), _p(w.f), _p(w.g), _p(w.h),
-                       _p(w.m), _p(w.n), _p(R), _p(L), float(tol), int(itermax), C.byref(fe),
-                       _p(H))
+    args = (ordering, int(err_fp64), Nx, Ny, Nz, _p(w.e), _p(w.f), _p(w.g), _p(w.h), _p(w.m), _p(w.n), _p(R),
+            _p(L), float(np.float32(tol)), int(itermax), C.byref(fe), _p(H))
+    if omega is None:
+        it = port().qo_sor(*args)
+    else:
+        it = port().qo_sor_omega(*args, float(np.float32(omega)))
     return L, it, fe.value, (H[:it] if hist else None)
 
 

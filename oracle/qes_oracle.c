@@ -67,14 +67,17 @@ void qo_divergence(int Nx, int Ny, int Nz, float dx, float dy, const float *dz, 
       }
 }
 
-/* One SOR cell update, src/winds/Solver_CPU.cpp:107-114 (all float). */
+/* One SOR cell update, src/winds/Solver_CPU.cpp:107-114 (all float); the
+ * reference's omega is OMEGA, other values serve the solver's over-relaxed
+ * pre-phase. */
 static inline float sor_cell(const grid_t *G, long c, const float *e, const float *f, const float *g_,
-                             const float *h, const float *m, const float *n, const float *R, const float *L)
+                             const float *h, const float *m, const float *n, const float *R, const float *L,
+                             float omega)
 {
-  return (OMEGA / (e[c] + f[c] + g_[c] + h[c] + m[c] + n[c])) *
+  return (omega / (e[c] + f[c] + g_[c] + h[c] + m[c] + n[c])) *
              (e[c] * L[c + 1] + f[c] * L[c - 1] + g_[c] * L[c + G->X] + h[c] * L[c - G->X] +
               m[c] * L[c + G->XY] + n[c] * L[c - G->XY] - R[c]) +
-         (1.0f - OMEGA) * L[c];
+         (1.0f - omega) * L[c];
 }
 
 /*
@@ -88,9 +91,9 @@ static inline float sor_cell(const grid_t *G, long c, const float *e, const floa
  * err_hist (nullable) receives each iteration's error as a double.
  * Returns the number of iterations performed.
  */
-int qo_sor(int ordering, int err_fp64, int Nx, int Ny, int Nz, const float *e, const float *f,
-           const float *g_, const float *h, const float *m, const float *n, const float *R, float *L,
-           float tol, int itermax, double *final_error, double *err_hist)
+int qo_sor_omega(int ordering, int err_fp64, int Nx, int Ny, int Nz, const float *e, const float *f,
+                 const float *g_, const float *h, const float *m, const float *n, const float *R, float *L,
+                 float tol, int itermax, double *final_error, double *err_hist, float omega)
 {
   grid_t G = mkgrid(Nx, Ny, Nz);
   long nc = G.XY * (G.nz - 1);
@@ -104,7 +107,7 @@ int qo_sor(int ordering, int err_fp64, int Nx, int Ny, int Nz, const float *e, c
         for (int j = 1; j < G.ny - 2; ++j)
           for (int i = 1; i < G.nx - 2; ++i) {
             long c = cellix(&G, i, j, k);
-            L[c] = sor_cell(&G, c, e, f, g_, h, m, n, R, L);
+            L[c] = sor_cell(&G, c, e, f, g_, h, m, n, R, L, omega);
           }
     } else {
       for (int colour = 0; colour < 2; ++colour)
@@ -113,7 +116,7 @@ int qo_sor(int ordering, int err_fp64, int Nx, int Ny, int Nz, const float *e, c
             for (int i = 1; i < G.nx - 2; ++i)
               if (((i + j + k) % 2) == colour) {
                 long c = cellix(&G, i, j, k);
-                L[c] = sor_cell(&G, c, e, f, g_, h, m, n, R, L);
+                L[c] = sor_cell(&G, c, e, f, g_, h, m, n, R, L, omega);
               }
     }
     for (int j = 0; j < G.ny - 1; ++j)
@@ -142,6 +145,14 @@ int qo_sor(int ordering, int err_fp64, int Nx, int Ny, int Nz, const float *e, c
   if (final_error) *final_error = max_error;
   free(old);
   return iter;
+}
+
+int qo_sor(int ordering, int err_fp64, int Nx, int Ny, int Nz, const float *e, const float *f,
+           const float *g_, const float *h, const float *m, const float *n, const float *R, float *L,
+           float tol, int itermax, double *final_error, double *err_hist)
+{
+  return qo_sor_omega(ordering, err_fp64, Nx, Ny, Nz, e, f, g_, h, m, n, R, L, tol, itermax, final_error,
+                      err_hist, OMEGA);
 }
 
 /* Velocity correction and solid-cell zeroing, src/winds/Solver_CPU.cpp:157-231. */

@@ -135,7 +135,7 @@ __global__ void k_build_mask(DevGrid G, const float *__restrict__ e, const float
 // inv[k*64 + bits] = omega / (e + f + g + h + m + n) with absent terms 0,
 // summed in the reference's order (Solver_CPU.cpp:107).
 __global__ void k_inv_table(DevGrid G, const unsigned *__restrict__ vmax, float *__restrict__ inv,
-                            float *__restrict__ val)
+                            float *__restrict__ val, float omega)
 {
   const int k = blockIdx.x, bits = threadIdx.x;
   float v[6];
@@ -147,7 +147,7 @@ __global__ void k_inv_table(DevGrid G, const unsigned *__restrict__ vmax, float 
   s = s + (bits & 8 ? v[3] : 0.0f);
   s = s + (bits & 16 ? v[4] : 0.0f);
   s = s + (bits & 32 ? v[5] : 0.0f);
-  inv[k * 64 + bits] = kOmega / s;
+  inv[k * 64 + bits] = omega / s;
   if (bits < 6) val[bits * G.Z + k] = v[bits];
 }
 
@@ -515,6 +515,14 @@ struct qesb_handle {
   float *d_lam_s = nullptr, *d_R_s = nullptr;
   uint8_t *d_mask_s = nullptr;
 
+  // over-relaxed pre-phase (qesb_set_prephase): omega 0 = off
+  float pre_omega = 0.0f, pre_tol = 0.0f;
+  int pre_iters = 0;
+  float *d_inv_pre = nullptr;     // [Z][64] pre_omega / sum
+  float inv_pre_omega = 0.0f;     // omega d_inv_pre holds (0 = stale)
+  int last_pre_iterations = 0;
+  SweepGraph sgraph_pre;
+
   // sweep kernels: this solve as a one-domain list
   SweepList list;
   SweepCtl *h_ctl = nullptr;  // pinned
@@ -632,7 +640,8 @@ qesb_status prepare_coefs(qesb_handle *h)
     CK(cudaMemcpyAsync(&bad, h->d_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (!bad) {
-      k_inv_table<<<G.Z, 64, 0, s>>>(G, h->d_vmax, h->d_inv, h->d_val);
+      k_inv_table<<<G.Z, 64, 0, s>>>(G, h->d_vmax, h->d_inv, h->d_val, kOmega);
+      h->inv_pre_omega = 0.0f;  // the pre-phase table follows the new inputs at the next solve
       k_pad_to_split_u8<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_mask, h->d_mask_s);
       CK(cudaGetLastError());
       h->packed = true;
@@ -889,7 +898,23 @@ SweepDomain sweep_domain(qesb_handle *h, int itermax, double tol)
   d.st = h->d_state;
   d.itermax = itermax;
   d.tol = tol;
+  d.c1 = 1.0f - kOmega;
   return d;
+}
+
+// The pre-phase's view of a domain: omega = pre_omega through its own inv
+// table and c1, its own tolerance and iteration cap.
+qesb_status sweep_domain_pre(qesb_handle *h, SweepDomain &d, cudaStream_t s)
+{
+  if (h->inv_pre_omega != h->pre_omega) {
+    k_inv_table<<<h->G.Z, 64, 0, s>>>(h->G, h->d_vmax, h->d_inv_pre, h->d_val, h->pre_omega);
+    CK(cudaGetLastError());
+    h->inv_pre_omega = h->pre_omega;
+  }
+  d = sweep_domain(h, h->pre_iters, (double)h->pre_tol);
+  d.inv = h->d_inv_pre;
+  d.c1 = 1.0f - h->pre_omega;
+  return QESB_OK;
 }
 
 // The iteration loop over a domain list: CUDA-graph chunks of (red, black)
@@ -956,14 +981,32 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
   k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam, h->d_lam_s);
   k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_R, h->d_R_s);
   CK(cudaGetLastError());
+  int launched = 0, pre_launched = 0;
+  h->last_pre_iterations = 0;
+  if (h->pre_omega > 0.0f && h->pre_iters > 0) {
+    // over-relaxed pre-phase from the current lambda; its state and error
+    // history are then cleared for the reference loop
+    SweepDomain pre;
+    CKS(sweep_domain_pre(h, pre, s));
+    CKS(h->list.upload({pre}, sv.span, s));
+    SweepArgs a = h->list.a;
+    a.one = pre;
+    CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, h->pre_iters, h->opt_graph != 0,
+                       &h->sgraph_pre, h->h_ctl, &pre_launched));
+    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the pre-phase");
+    h->last_pre_iterations = h->h_state->it;
+    CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
+    CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+  }
   const SweepDomain one = sweep_domain(h, itermax, (double)h->tol);
   CKS(h->list.upload({one}, sv.span, s));
   SweepArgs a = h->list.a;
   a.one = one;
-  int launched = 0;
   CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, itermax, h->opt_graph != 0, &h->sgraph,
                      h->h_ctl, &launched));
-  h->last_launches = 2 * launched;
+  h->last_launches = 2 * (launched + pre_launched);
   k_split_mirror_ring<<<G.Y, 128, 0, s>>>(G, h->S, h->d_lam_s);
   k_split_to_pad<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam_s, h->d_lam);
   CK(cudaGetLastError());
@@ -979,13 +1022,14 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   CK(cudaSetDevice(h->device));
   const DevGrid &G = h->G;
   cudaStream_t s = h->stream;
-  CKS(ensure_err(h, std::max(itermax, 1)));
+  const int nerr = std::max({itermax, 1, h->pre_omega > 0.0f ? h->pre_iters : 0});
+  CKS(ensure_err(h, nerr));
   CK(cudaEventRecord(h->ev[0], s));
   k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(
       G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_u0, h->d_v0,
       h->d_w0, h->d_dz, h->dx, h->dy, h->d_R);
   CK(cudaGetLastError());
-  CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
+  CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * nerr, s));
   CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
   CK(cudaEventRecord(h->ev[1], s));
   const bool packed = h->packed && h->opt_path == 1;
@@ -997,6 +1041,7 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   const bool split = packed && vi >= kSplitVariant;
   const Variant *var = packed && !split ? &kVariants[vi] : nullptr;
   h->last_launches = 0;
+  h->last_pre_iterations = 0;
   if (itermax > 0) {
     if (split) CKS(run_iterations_sweep(h, kSweepVariants[vi - kSplitVariant], itermax));
     else if (var) CKS(run_iterations_tiled(h, *var, itermax));
@@ -1022,6 +1067,7 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
     st->path = packed ? 1 : 0;
     st->sweeps_per_launch = var ? var->K : 1;
     st->launches = 2 + (packed ? h->last_launches : 4 * st->iterations);
+    st->pre_iterations = h->last_pre_iterations;
   }
   if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the solve (iteration %d)", h->h_state->it);
   return QESB_OK;
@@ -1052,11 +1098,12 @@ void free_all(qesb_handle *h)
   for (auto &g : h->gexec)
     if (g) cudaGraphExecDestroy(g);
   h->sgraph.reset();
+  h->sgraph_pre.reset();
   void *ptrs[] = {h->d_lam_s, h->d_R_s, h->d_mask_s, h->d_lam, h->d_lam2, h->d_R, h->d_mask, h->d_pc[0], h->d_pc[1], h->d_pc[2],
                   h->d_pc[3], h->d_pc[4], h->d_pc[5], h->d_own_in[0], h->d_own_in[1],
                   h->d_own_in[2], h->d_own_in[3], h->d_own_in[4], h->d_own_in[5], h->d_own_flag,
                   h->d_own_u0, h->d_own_v0, h->d_own_w0, h->d_dz, h->d_vmax, h->d_inv, h->d_val,
-                  h->d_bad, h->d_err, h->d_state, h->d_u, h->d_v, h->d_w};
+                  h->d_inv_pre, h->d_bad, h->d_err, h->d_state, h->d_u, h->d_v, h->d_w};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   h->list.destroy();
@@ -1123,6 +1170,7 @@ qesb_status qesb_create(const qesb_grid *grid, float tol, int device, qesb_handl
   TRY(dalloc(&h->d_dz, G.Z));
   TRY(dalloc(&h->d_vmax, 6 * G.Z));
   TRY(dalloc(&h->d_inv, 64 * G.Z));
+  TRY(dalloc(&h->d_inv_pre, 64 * G.Z));
   TRY(dalloc(&h->d_val, 6 * G.Z));
   TRY(dalloc(&h->d_bad, 1));
   TRY(dalloc(&h->d_state, 1));
@@ -1488,14 +1536,25 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   CK(cudaEventRecord(h0->ev[0], s));
   std::vector<SweepDomain> doms(n);
   double cells = 0;
+  std::vector<SweepDomain> pre;
+  std::vector<int> pre_of;  // batch index of each pre-phase domain
   for (int i = 0; i < n; ++i) {
     qesb_handle *h = hs[i];
     const DevGrid &G = h->G;
-    CKS(ensure_err(h, std::max(itermax, 1)));
+    const bool pre_on = h->pre_omega > 0.0f && h->pre_iters > 0 && itermax > 0;
+    const int nerr = std::max({itermax, 1, pre_on ? h->pre_iters : 0});
+    CKS(ensure_err(h, nerr));
     k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(
         G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_u0, h->d_v0,
         h->d_w0, h->d_dz, h->dx, h->dy, h->d_R);
-    CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
+    CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * nerr, s));
+    h->last_pre_iterations = 0;
+    if (pre_on) {
+      SweepDomain p;
+      CKS(sweep_domain_pre(h, p, s));
+      pre.push_back(p);
+      pre_of.push_back(i);
+    }
     CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
     k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam, h->d_lam_s);
     k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_R, h->d_R_s);
@@ -1505,8 +1564,30 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   }
   SweepList list;
   CKS(list.create(n));
-  qesb_status qs = list.upload(doms, sv.span, s);
-  int launched = 0;
+  qesb_status qs = QESB_OK;
+  int launched = 0, pre_launched = 0;
+  if (!pre.empty()) {
+    // the over-relaxed pre-phase of the domains that have one, as a list of its own
+    qs = list.upload(pre, sv.span, s);
+    SweepGraph gx;
+    int pre_max = 0;
+    for (int i : pre_of) pre_max = std::max(pre_max, hs[i]->pre_iters);
+    if (qs == QESB_OK)
+      qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, pre_max, h0->opt_graph != 0, &gx, h0->h_ctl,
+                          &pre_launched);
+    gx.reset();
+    for (size_t q = 0; q < pre_of.size() && qs == QESB_OK; ++q) {
+      qesb_handle *h = hs[pre_of[q]];
+      SolveState sp;
+      CK(cudaMemcpyAsync(&sp, h->d_state, sizeof sp, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      if (sp.nan) qs = qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d during the pre-phase", pre_of[q]);
+      h->last_pre_iterations = sp.it;
+      CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
+      CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+    }
+  }
+  if (qs == QESB_OK) qs = list.upload(doms, sv.span, s);
   if (qs == QESB_OK) {
     k_sweep_stamp<<<1, 1, 0, s>>>(list.a.ctl);
     SweepGraph gx;
@@ -1548,10 +1629,23 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
       st[i].ms_sor = sti.t_done > t0 ? (double)(sti.t_done - t0) * 1e-6 : 0.0;
       st[i].path = 1;
       st[i].sweeps_per_launch = 1;
-      st[i].launches = 2 * launched;
+      st[i].launches = 2 * (launched + pre_launched);
+      st[i].pre_iterations = hs[i]->last_pre_iterations;
     }
   }
   if (nan_at >= 0) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d", nan_at);
+  return QESB_OK;
+}
+
+qesb_status qesb_set_prephase(qesb_handle *h, float omega, float tol, int max_iterations)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  if (omega != 0.0f && !(omega > 1.0f && omega < 2.0f))
+    return qesb_fail(QESB_ERR_ARG, "qesb_set_prephase: omega must be 0 (off) or in (1, 2)");
+  if (max_iterations < 0) return qesb_fail(QESB_ERR_ARG, "qesb_set_prephase: max_iterations must be >= 0");
+  h->pre_omega = omega;
+  h->pre_tol = tol;
+  h->pre_iters = max_iterations;
   return QESB_OK;
 }
 

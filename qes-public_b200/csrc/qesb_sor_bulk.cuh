@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(32 * W) k_sor_bulk(BulkArgs b)
   };
 
   // ---- consumer ------------------------------------------------------------
-  const float c1 = 1.0f - kOmega;
+  float c1 = 0.0f;
   int cd = -1, cX = 0, cY = 0, cPQ = 0, cnch = 1, kcur = -1, cit = 0;
   long cCS = 0;
   float *cL = nullptr;
@@ -251,6 +251,7 @@ __global__ void __launch_bounds__(32 * W) k_sor_bulk(BulkArgs b)
       cinv = D.inv;
       cerr = D.err;
       cit = D.st->it;
+      c1 = D.c1;
       kcur = -1;
     }
     const int j = hdr.y, k = hdr.z, q0 = hdr.w * kChunk;

@@ -45,6 +45,7 @@ struct SplitDom {
   double *err = nullptr;
   int it = 0;
   int kcur = -1;
+  float c1 = 0.0f;
   float ve = 0, vf = 0, vg = 0, vh = 0, vm = 0, vn = 0, inv63 = 0;
   const float *inv = nullptr;
   double dmax = 0.0;    // warp-wide max |dlambda| so far (all lanes hold it)
@@ -64,6 +65,7 @@ struct SplitDom {
     inv_all = D.inv;
     err = D.err;
     it = D.st->it;
+    c1 = D.c1;
     kcur = -1;
   }
   __device__ __forceinline__ void layer(int k)
@@ -159,7 +161,6 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SweepArgs b)
   const int na = b.ctl->nactive;
   if (na <= 0) return;
   const int lane = threadIdx.x;
-  const float c1 = 1.0f - kOmega;
   SplitDom D;
   split_rows<RPB, STRIDED, MULTI>(b, na, D, [&](int j, int k) {
     const int i0 = (COLOUR + j + k) & 1;
@@ -218,7 +219,7 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SweepArgs b)
         for (int u = 0; u < U; ++u)
           nv[u] = D.inv63 * (D.ve * xp[u] + D.vf * xm[u] + D.vg * yp[u] + D.vh * ym[u] + D.vm * zp[u] +
                              D.vn * zm[u] - rr[u]) +
-                  c1 * old[u];
+                  D.c1 * old[u];
       } else {
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -228,7 +229,7 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SweepArgs b)
           const float m = (m_ & 16u) ? D.vm : 0.0f, n = (m_ & 32u) ? D.vn : 0.0f;
           nv[u] = __ldg(D.inv + m_) * (e * xp[u] + f * xm[u] + g * yp[u] + hh * ym[u] + m * zp[u] + n * zm[u] -
                                        rr[u]) +
-                  c1 * old[u];
+                  D.c1 * old[u];
         }
       }
       bool big = false;
@@ -275,7 +276,6 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split4(SweepArgs b)
   const int na = b.ctl->nactive;
   if (na <= 0) return;
   const int lane = threadIdx.x;
-  const float c1 = 1.0f - kOmega;
   SplitDom D;
   split_rows<RPB, STRIDED, MULTI>(b, na, D, [&](int j, int k) {
     const int i0 = (COLOUR + j + k) & 1;
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split4(SweepArgs b)
         for (int t = 0; t < 4; ++t)
           nv[t] = D.inv63 * (D.ve * xpv[t] + D.vf * xmv[t] + D.vg * ypv[t] + D.vh * ymv[t] + D.vm * zpv[t] +
                              D.vn * zmv[t] - rv[t]) +
-                  c1 * ov[t];
+                  D.c1 * ov[t];
       } else {
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split4(SweepArgs b)
           const float m = (m_ & 16u) ? D.vm : 0.0f, n = (m_ & 32u) ? D.vn : 0.0f;
           nv[t] = __ldg(D.inv + m_) * (e * xpv[t] + f * xmv[t] + g * ypv[t] + hh * ymv[t] + m * zpv[t] +
                                        n * zmv[t] - rv[t]) +
-                  c1 * ov[t];
+                  D.c1 * ov[t];
         }
       }
       bool big = false;

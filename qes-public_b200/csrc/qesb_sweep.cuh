@@ -25,6 +25,7 @@ struct SweepDomain {
   SolveState *st;
   int itermax;
   double tol;
+  float c1;  // 1 - omega (omega/sum sits in inv): the reference's 1.78f, or a pre-phase's
 };
 
 struct SweepCtl {

@@ -58,7 +58,7 @@ class Grid(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("residual", C.c_double),
                 ("ms_total", C.c_double), ("ms_sor", C.c_double), ("path", C.c_int),
-                ("sweeps_per_launch", C.c_int), ("launches", C.c_int)]
+                ("sweeps_per_launch", C.c_int), ("launches", C.c_int), ("pre_iterations", C.c_int)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -103,6 +103,7 @@ def lib() -> C.CDLL:
             "qesb_get_divergence": ([V, V], C.c_int),
             "qesb_get_residual_history": ([V, V, C.c_int], C.c_int),
             "qesb_set_tolerance": ([V, C.c_float], C.c_int),
+            "qesb_set_prephase": ([V, C.c_float, C.c_float, C.c_int], C.c_int),
             "qesb_time_sweeps": ([V, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)], C.c_int),
             "qesb_autotune": ([V, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int], C.c_int),
             "qesb_solve_batch": ([C.POINTER(V), C.c_int, C.c_int, C.POINTER(V), C.POINTER(V), C.POINTER(V),
@@ -290,6 +291,10 @@ class Solver_B200:
 
     def set_option(self, key: str, value: int):
         check(lib().qesb_set_option(self._h, key.encode(), int(value)))
+
+    def set_prephase(self, omega: float, tol: float = 1e-3, max_iterations: int = 10000):
+        """Over-relaxed SOR pre-phase before the reference loop (omega 0: off)."""
+        check(lib().qesb_set_prephase(self._h, float(omega), float(tol), int(max_iterations)))
 
     def set_tolerance(self, tol: float):
         self.tol = np.float32(tol)

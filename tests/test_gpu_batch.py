@@ -82,3 +82,37 @@ def test_batch_rejects_repeated_and_non_stair_step_handles():
         s.set_option("path", 0)
         with pytest.raises(qesb.QesbError):
             qesb.solve_batch([s], 10)
+
+
+def test_batch_prephase_per_domain():
+    """Domains of one batch with and without an over-relaxed pre-phase: each
+    matches the oracle's two-phase (or one-phase) solve."""
+    import torch
+
+    ws = _cities()
+    tol = 1.1e-3
+    pre = [(1.9, 1e-3, 4000), None, (1.95, 1e-3, 80), None]
+    solvers = [qesb.Solver_B200(w.domain, tol) for w in ws]
+    try:
+        for s, w, p in zip(solvers, ws, pre):
+            s.set_inputs(w)
+            if p:
+                s.set_prephase(*p)
+        st = qesb.solve_batch(solvers, 4000)
+        lams = [s.lambda_ for s in solvers]
+    finally:
+        for s in solvers:
+            s.close()
+    for w, p, sti, L in zip(ws, pre, st, lams):
+        d = w.domain
+        R = O.divergence(d, w)
+        lam0 = None
+        if p:
+            lam0, itp, *_ = O.sor(d, w, R, p[1], p[2], omega=p[0])
+            assert sti["pre_iterations"] == itp
+        else:
+            assert sti["pre_iterations"] == 0
+        Lo, it, *_ = O.sor(d, w, R, tol, 4000, lam=lam0)
+        assert sti["iterations"] == it
+        np.testing.assert_array_equal(L, Lo)
+    torch.cuda.synchronize()

@@ -232,3 +232,28 @@ def test_autotune_restores_lambda_and_results_stay_exact(golden):
     Lo, it, *_ = O.sor(d, w, O.divergence(d, w), 1e-9, 150, lam=lam0)
     assert st["iterations"] == it == 150
     np.testing.assert_array_equal(L, Lo)
+
+
+@pytest.mark.parametrize("variant", [5, 16, BULK + 1])
+@pytest.mark.parametrize("omega,pre_tol,pre_max", [(1.9, 1e-3, 5000), (1.95, 5e-4, 150)])
+def test_overrelaxed_prephase_then_reference_loop(variant, omega, pre_tol, pre_max):
+    """qesb_set_prephase: red-black SOR with another omega until its own rule
+    (or cap), then the reference loop (omega 1.78, the handle's tolerance)
+    from that lambda; both phases bit-exact against the oracle."""
+    d = qesb.Domain(70, 45, 21, 2.0, 2.0, 1.0, qesb.city_dz(21, 1.0, 1.03))
+    c = qesb.city_random(d, 9, 8, fp=(6, 18), h=(4, 30))
+    w = qesb.city_build(d, c.buildings, c.inflow)
+    tol = 1.1e-3
+    with qesb.Solver_B200(d, tol) as s:
+        s.set_option("variant", variant)
+        s.set_prephase(omega, pre_tol, pre_max)
+        st = s.solve(w, 5000)
+        L = s.lambda_
+        u = w.u.copy()
+    R = O.divergence(d, w)
+    Lp, itp, *_ = O.sor(d, w, R, pre_tol, pre_max, omega=omega)
+    Lo, it, *_ = O.sor(d, w, R, tol, 5000, lam=Lp)
+    assert st["pre_iterations"] == itp
+    assert st["iterations"] == it and st["converged"] == 1
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(u, O.correct(d, w, Lo)[0])

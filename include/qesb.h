@@ -176,8 +176,9 @@ qesb_status qesb_set_stream(qesb_handle *h, void *stream);
  * The network grid is planes 0..Nz-1 of the X x Y cell grid (all but the top
  * boundary plane), channels-last [Nz][Ny][Nx][C] BF16.
  *   qesb_compute_divergence: R from the current inputs (as a solve does first).
- *   qesb_warm_input:  network input from R, icellflag and dz (C >= 5 channels:
- *                     R/s, solid, dz/mean dz, boundary, height fraction);
+ *   qesb_warm_input:  network input from R, icellflag and dz (C a multiple of
+ *                     8, >= 8; channels R/s, solid, dz/mean dz, boundary,
+ *                     height fraction, then zeros);
  *                     *scale (device) receives s = max|R| over updated cells.
  *   qesb_warm_target: lambda/s and a 1/0 weight (updated cells) per voxel, FP32.
  *   qesb_warm_apply:  lambda <- s * yhead[v][0] on updated cells (yhead FP32
@@ -205,10 +206,16 @@ qesb_status qesb_umma_selftest(const uint16_t *A, const uint16_t *B, float *C, i
  * zero-padded; tap = (dz+1)*9 + (dy+1)*3 + (dx+1). Output [D][H][W][N] to y
  * (BF16) or yf (FP32); optional bias[N] (FP32), ReLU, and mask (BF16 [V][N]:
  * output zeroed where mask <= 0). N in {16, 32, 64, 128}. *err is set if a
- * kernel's tensor-core completion wait gives up. */
+ * kernel's tensor-core completion wait gives up. Grids with W a multiple of
+ * 128 and N in {16, 32} run a direct kernel (each 16-channel input slice
+ * staged once per tile, the 27 taps as shifted descriptors into it); the
+ * others the implicit GEMM (per-tap gather). */
 qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H, int W,
                         int sign, const void *Bm, int Kp, int N, void *y, void *yf, const float *bias,
                         int relu, const void *mask, int *err, void *stream);
+/* Process-wide choice of the qesb_conv3d kernel: 0 = direct kernel where it
+ * applies (default), 1 = implicit GEMM everywhere (for comparison). */
+qesb_status qesb_net_set_conv_path(int path);
 /* Weight gradient dW[tap*(c1+c2) + c][n] += sum_v X[v + offset(tap)][c] * dY[v][n]
  * (FP32, accumulated with atomics: zero it first); X as in qesb_conv3d,
  * dY BF16 [V][N]; vchunk = voxels per CTA (>= 64). */

@@ -281,6 +281,156 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
   }
 }
 
+// Direct 3x3x3 convolution for grids whose x rows are multiples of 128
+// voxels (the network's full- and half-resolution levels, where the implicit
+// GEMM's per-tap gather dominates). A CTA owns 128 consecutive x positions of
+// TY x TZ output rows; for each 16-channel slice of the input it stages the
+// (TY+2) x (TZ+2) rows of 130 voxels around them once in shared memory
+// (cp.async, zero-filled outside the grid), laid out as
+//     byte ((cg * NR + r) * 130 + xi) * 16,   cg = channel group of 8,
+// so that for every tap (dz, dy, dx) the 128 x 16 A operand of an output row
+// is a canonical K-major tile starting at row r(z+dz, y+dy), voxel 1+dx, with
+// SBO = 128 B (next 8 voxels) and LBO = NR*130*16 B (next channel group): the
+// 27 taps are 27 descriptors into the same tile, no im2col copy. B (all 27
+// taps of the slice) is staged next to it. One thread issues the
+// 27 * TY * TZ MMAs per slice into TY * TZ accumulators of N FP32 columns of
+// TMEM. sign = -1 flips the taps (input gradient with the transposed weights).
+constexpr int kDirTY = 2, kDirTZ = 2, kDirNR = (kDirTY + 2) * (kDirTZ + 2), kDirXW = 130;
+
+__device__ __forceinline__ void cp16_zfill(void *dst, const void *src, bool valid)
+{
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(umma::smem_u32(dst)), "l"(src),
+               "r"(valid ? 16 : 0)
+               : "memory");
+}
+
+// Address of the 8 channels c..c+7 of the input at voxel (z, y, x) (caller
+// checks the grid bounds).
+__device__ __forceinline__ const __nv_bfloat16 *in_ptr8(const ConvIn &in, const ConvGeom &g, int z, int y, int x,
+                                                        int c)
+{
+  if (c < in.c1) {
+    if (in.up1) return in.x1 + ((((long)(z >> 1) * (g.H >> 1) + (y >> 1)) * (g.W >> 1) + (x >> 1)) * in.c1 + c);
+    return in.x1 + ((((long)z * g.H + y) * g.W + x) * in.c1 + c);
+  }
+  return in.x2 + ((((long)z * g.H + y) * g.W + x) * in.c2 + (c - in.c1));
+}
+
+template <int N>
+__global__ void __launch_bounds__(128) k_conv_direct(ConvIn in, ConvGeom g, int sign,
+                                                    const __nv_bfloat16 *__restrict__ Bm, int Kp, ConvOut out,
+                                                    int *err)
+{
+  constexpr int TY = kDirTY, TZ = kDirTZ, NR = kDirNR, XW = kDirXW, NACC = TY * TZ;
+  constexpr uint32_t SA = NR * XW * 32, SB = 27 * N * 32;
+  constexpr uint32_t NCOLS = NACC * N <= 32 ? 32 : NACC * N <= 64 ? 64 : NACC * N <= 128 ? 128 : NACC * N <= 256 ? 256 : 512;
+  static_assert(NACC * N <= 512, "accumulators exceed TMEM");
+  extern __shared__ __align__(1024) uint8_t sm[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int cin = in.c1 + in.c2, KC = cin / 16;
+  const int x0 = blockIdx.x * 128, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+  if (warp == 0) umma::tmem_alloc(&tmem_base, NCOLS);
+  if (tid == 0) {
+    umma::mbar_init(&mbar, 1);
+    umma::fence_mbar_init();
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  constexpr uint32_t idesc = umma::idesc_bf16(128, N, 0, 0);
+  uint8_t *sa = sm, *sb = sm + SA;
+  bool ok = true;
+  for (int kc = 0; kc < KC && ok; ++kc) {
+    if (kc > 0) ok = umma::mbar_wait(&mbar, (kc - 1) & 1, kWaitLimit);  // the slice's MMAs read sa, sb
+    if (!ok) break;
+    for (int idx = tid; idx < NR * XW * 2; idx += 128) {
+      const int cg = idx / (NR * XW), rem = idx - cg * NR * XW;
+      const int r = rem / XW, xi = rem - r * XW;
+      const int zz = z0 - 1 + r / (TY + 2), yy = y0 - 1 + r % (TY + 2), xx = x0 - 1 + xi;
+      const bool inside = zz >= 0 && zz < g.D && yy >= 0 && yy < g.H && xx >= 0 && xx < g.W;
+      const __nv_bfloat16 *src = inside ? in_ptr8(in, g, zz, yy, xx, 16 * kc + 8 * cg) : in.x1;
+      cp16_zfill(sa + ((cg * NR + r) * XW + xi) * 16, src, inside);
+    }
+    for (int idx = tid; idx < 27 * N * 2; idx += 128) {
+      const int t = idx / (N * 2), rem = idx - t * N * 2, n = rem >> 1, kg = rem & 1;
+      cp16_zfill(sb + t * N * 32 + (n >> 3) * 256 + kg * 128 + (n & 7) * 16,
+                 Bm + (long)n * Kp + t * cin + 16 * kc + 8 * kg, true);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    umma::fence_smem_async();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+      const uint32_t a0 = umma::smem_u32(sa), b0 = umma::smem_u32(sb);
+      for (int a = 0; a < NACC; ++a) {
+        const int zt = a / TY, yt = a % TY;
+        for (int t = 0; t < 27; ++t) {
+          int dz, dy, dx;
+          tap_offset(t, dz, dy, dx);
+          const int r = (zt + 1 + sign * dz) * (TY + 2) + (yt + 1 + sign * dy);
+          const uint64_t ad = umma::desc(a0 + (uint32_t)(r * XW + 1 + sign * dx) * 16, NR * XW * 16, 128);
+          const uint64_t bd = umma::desc(b0 + (uint32_t)(t * N * 32), 128, 256);
+          umma::mma_bf16(tmem + (uint32_t)(a * N), ad, bd, idesc, (kc > 0 || t > 0) ? 1u : 0u);
+        }
+      }
+      umma::mma_commit(&mbar);
+    }
+  }
+  if (ok) ok = umma::mbar_wait(&mbar, (KC - 1) & 1, kWaitLimit);
+  umma::fence_after_sync();
+  if (!ok) {
+    if (lane == 0) atomicExch(err, 1);
+  } else {
+    const int x = x0 + warp * 32 + lane;
+    for (int a = 0; a < NACC; ++a) {
+      const int z = z0 + a / TY, y = y0 + a % TY;
+      const bool valid = z < g.D && y < g.H && x < g.W;
+      const long v = ((long)z * g.H + y) * g.W + x;
+      for (int c0 = 0; c0 < N; c0 += 8) {
+        float f[8];
+        umma::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * N + c0), f);
+        if (!valid) continue;
+        if (out.bias) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) f[q] += __ldg(out.bias + c0 + q);
+        }
+        if (out.relu) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) f[q] = fmaxf(f[q], 0.0f);
+        }
+        if (out.mask) {
+          const uint4 mk = __ldg(reinterpret_cast<const uint4 *>(out.mask + v * N + c0));
+          const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&mk);
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (!(__bfloat162float(mb[q]) > 0.0f)) f[q] = 0.0f;
+        }
+        if (out.yf) {
+          float4 *dst = reinterpret_cast<float4 *>(out.yf + v * N + c0);
+          dst[0] = make_float4(f[0], f[1], f[2], f[3]);
+          dst[1] = make_float4(f[4], f[5], f[6], f[7]);
+        } else {
+          uint4 pk;
+          __nv_bfloat162 *h2 = reinterpret_cast<__nv_bfloat162 *>(&pk);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) h2[q] = __floats2bfloat162_rn(f[2 * q], f[2 * q + 1]);
+          *reinterpret_cast<uint4 *>(out.y + v * N + c0) = pk;
+        }
+      }
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, NCOLS);
+  }
+}
+
 // Weight gradient: dW[t*cin + c][n] += sum_v X[v + off(t)][c] * dY[v][n] over
 // this CTA's voxel range. M-tile = 128 rows of (t, c); K = voxels in chunks
 // of 64; both operands MN-major (channels contiguous). Partial sums from the
@@ -401,6 +551,27 @@ qesb_status launch_conv(const ConvIn &in, const ConvGeom &g, int sign, const __n
   return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));
 }
 
+int g_conv_path = 0;  // 0: direct kernel where it applies, 1: implicit GEMM only
+
+template <int N>
+qesb_status launch_conv_direct(const ConvIn &in, const ConvGeom &g, int sign, const __nv_bfloat16 *Bm, int Kp,
+                               const ConvOut &out, int *err, cudaStream_t s)
+{
+  constexpr int smem = kDirNR * kDirXW * 32 + 27 * N * 32;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  static bool attr[64] = {};
+  if (!attr[dev & 63]) {
+    cudaError_t e = cudaFuncSetAttribute(k_conv_direct<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv attr: %s", cudaGetErrorString(e));
+    attr[dev & 63] = true;
+  }
+  const dim3 grid(g.W / 128, (g.H + kDirTY - 1) / kDirTY, (g.D + kDirTZ - 1) / kDirTZ);
+  k_conv_direct<N><<<grid, 128, smem, s>>>(in, g, sign, Bm, Kp, out, err);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));
+}
+
 template <int N>
 qesb_status launch_wgrad(const ConvIn &in, const ConvGeom &g, const __nv_bfloat16 *dY, long vchunk, float *dW,
                          int *err, cudaStream_t s)
@@ -480,12 +651,23 @@ extern "C" qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *
             static_cast<const __nv_bfloat16 *>(mask)};
   const auto *B = static_cast<const __nv_bfloat16 *>(Bm);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (g_conv_path == 0 && W % 128 == 0 && (N == 16 || N == 32)) {
+    if (N == 16) return launch_conv_direct<16>(in, g, sign, B, Kp, o, err, s);
+    return launch_conv_direct<32>(in, g, sign, B, Kp, o, err, s);
+  }
   switch (N) {
     case 16: return launch_conv<16>(in, g, sign, B, Kp, o, err, s);
     case 32: return launch_conv<32>(in, g, sign, B, Kp, o, err, s);
     case 64: return launch_conv<64>(in, g, sign, B, Kp, o, err, s);
     default: return launch_conv<128>(in, g, sign, B, Kp, o, err, s);
   }
+}
+
+extern "C" qesb_status qesb_net_set_conv_path(int path)
+{
+  if (path != 0 && path != 1) return qesb_fail(QESB_ERR_ARG, "qesb_net_set_conv_path: path must be 0 or 1");
+  g_conv_path = path;
+  return QESB_OK;
 }
 
 extern "C" qesb_status qesb_conv3d_wgrad(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H,

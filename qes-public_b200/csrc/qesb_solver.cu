@@ -351,30 +351,41 @@ __global__ void k_absmax_R(DevGrid G, const float *__restrict__ R, unsigned *__r
   if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(mx));
 }
 
+__device__ __forceinline__ uint32_t bf16_bits_rne(float f)
+{
+  const uint32_t b = __float_as_uint(f);
+  return (b + 0x7FFFu + ((b >> 16) & 1u)) >> 16;  // round to nearest even
+}
+
+// One block per (row j, layer k) of the net grid, threads along x; channels
+// 0..4 as above, 5..C-1 zero, written 8 channels (16 bytes) at a time.
 __global__ void k_warm_input(DevGrid G, int Dn, int C, const float *__restrict__ R, const int *__restrict__ flag,
                              const float *__restrict__ dz, const unsigned *__restrict__ smax, float dz_mean,
                              float height, uint16_t *__restrict__ x)
 {
-  const float inv_s = 1.0f / fmaxf(__uint_as_float(*smax), 1e-30f);
-  const long V = (long)Dn * G.Y * G.X;
-  for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < V; v += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(v % G.X), j = (int)((v / G.X) % G.Y), k = (int)(v / ((long)G.X * G.Y));
-    const bool upd = i >= 1 && i <= G.X - 2 && j >= 1 && j <= G.Y - 2 && k >= 1 && k <= G.Z - 2;
+  const int j = blockIdx.y, k = blockIdx.z;
+  __shared__ float s_zc;
+  if (threadIdx.x == 0) {
     float zc = 0.0f;
     for (int q = 1; q < k; ++q) zc += dz[q];
-    zc += 0.5f * dz[k];
-    float ch[5];
-    ch[0] = upd ? R[G.pad(i, j, k)] * inv_s : 0.0f;
-    ch[1] = is_solid(flag[G.cell(i, j, k)]) ? 1.0f : 0.0f;
-    ch[2] = dz[k] / dz_mean;
-    ch[3] = upd ? 0.0f : 1.0f;
-    ch[4] = zc / height;
-    uint16_t *dst = x + v * C;
-    for (int c = 0; c < C; ++c) {
-      const float val = c < 5 ? ch[c] : 0.0f;
-      const uint32_t b = __float_as_uint(val);
-      dst[c] = (uint16_t)((b + 0x7FFFu + ((b >> 16) & 1u)) >> 16);  // round to nearest even
-    }
+    s_zc = zc + 0.5f * dz[k];
+  }
+  __syncthreads();
+  const float inv_s = 1.0f / fmaxf(__uint_as_float(*smax), 1e-30f);
+  const float c2 = dz[k] / dz_mean, c4 = s_zc / height;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G.X; i += gridDim.x * blockDim.x) {
+    const bool upd = i >= 1 && i <= G.X - 2 && j >= 1 && j <= G.Y - 2 && k >= 1 && k <= G.Z - 2;
+    const float ch0 = upd ? R[G.pad(i, j, k)] * inv_s : 0.0f;
+    const float ch1 = is_solid(flag[G.cell(i, j, k)]) ? 1.0f : 0.0f;
+    const float ch3 = upd ? 0.0f : 1.0f;
+    uint4 lo;
+    lo.x = bf16_bits_rne(ch0) | (bf16_bits_rne(ch1) << 16);
+    lo.y = bf16_bits_rne(c2) | (bf16_bits_rne(ch3) << 16);
+    lo.z = bf16_bits_rne(c4);
+    lo.w = 0u;
+    uint4 *dst = reinterpret_cast<uint4 *>(x + (((long)k * G.Y + j) * G.X + i) * C);
+    dst[0] = lo;
+    for (int q = 1; q < C / 8; ++q) dst[q] = make_uint4(0, 0, 0, 0);
   }
 }
 
@@ -397,11 +408,10 @@ __global__ void k_warm_target(DevGrid G, int Dn, const float *__restrict__ L, co
 __global__ void k_warm_apply(DevGrid G, int Dn, const float *__restrict__ yhead, int N,
                              const unsigned *__restrict__ smax, float *__restrict__ L)
 {
+  const int j = blockIdx.y, k = blockIdx.z;
   const float s = __uint_as_float(*smax);
-  const long V = (long)G.Z * G.Y * G.X;
-  for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < V; v += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(v % G.X), j = (int)((v / G.X) % G.Y), k = (int)(v / ((long)G.X * G.Y));
-    const int kk = k == 0 ? 1 : k;
+  const int kk = k == 0 ? 1 : k;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G.X; i += gridDim.x * blockDim.x) {
     const bool upd = i >= 1 && i <= G.X - 2 && j >= 1 && j <= G.Y - 2 && kk >= 1 && kk <= G.Z - 2 && kk < Dn;
     L[G.pad(i, j, k)] = upd ? s * yhead[(((long)kk * G.Y + j) * G.X + i) * N] : 0.0f;
   }
@@ -1373,7 +1383,7 @@ qesb_status qesb_compute_divergence(qesb_handle *h)
 
 qesb_status qesb_warm_input(qesb_handle *h, void *x, int C, unsigned *scale)
 {
-  if (!h || !x || !scale || C < 5) return qesb_fail(QESB_ERR_ARG, "qesb_warm_input: bad arguments");
+  if (!h || !x || !scale || C < 8 || C % 8) return qesb_fail(QESB_ERR_ARG, "qesb_warm_input: bad arguments");
   CK(cudaSetDevice(h->device));
   const DevGrid &G = h->G;
   CK(cudaMemsetAsync(scale, 0, sizeof(unsigned), h->stream));
@@ -1381,8 +1391,8 @@ qesb_status qesb_warm_input(qesb_handle *h, void *x, int C, unsigned *scale)
   double dzs = 0.0, height = 0.0;
   for (int k = 1; k < G.Z; ++k) dzs += h->dz[k];
   for (int k = 1; k < G.Z - 1; ++k) height += h->dz[k];
-  k_warm_input<<<148 * 8, 256, 0, h->stream>>>(G, G.Z - 1, C, h->d_R, h->d_flag, h->d_dz, scale,
-                                               (float)(dzs / (G.Z - 1)), (float)height, (uint16_t *)x);
+  k_warm_input<<<dim3((G.X + 127) / 128, G.Y, G.Z - 1), 128, 0, h->stream>>>(
+      G, G.Z - 1, C, h->d_R, h->d_flag, h->d_dz, scale, (float)(dzs / (G.Z - 1)), (float)height, (uint16_t *)x);
   CK(cudaGetLastError());
   return QESB_OK;
 }
@@ -1400,7 +1410,8 @@ qesb_status qesb_warm_apply(qesb_handle *h, const float *yhead, int N, const uns
 {
   if (!h || !yhead || !scale || N < 1) return qesb_fail(QESB_ERR_ARG, "qesb_warm_apply: bad arguments");
   CK(cudaSetDevice(h->device));
-  k_warm_apply<<<148 * 8, 256, 0, h->stream>>>(h->G, h->G.Z - 1, yhead, N, scale, h->d_lam);
+  k_warm_apply<<<dim3((h->G.X + 127) / 128, h->G.Y, h->G.Z), 128, 0, h->stream>>>(h->G, h->G.Z - 1, yhead, N,
+                                                                                  scale, h->d_lam);
   CK(cudaGetLastError());
   return QESB_OK;
 }

@@ -116,6 +116,7 @@ def lib() -> C.CDLL:
             "qesb_umma_selftest": ([V, V, V, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
             "qesb_conv3d": ([V, C.c_int, C.c_int, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, V,
                              C.c_int, C.c_int, V, V, V, C.c_int, V, V, V], C.c_int),
+            "qesb_net_set_conv_path": ([C.c_int], C.c_int),
             "qesb_conv3d_wgrad": ([V, C.c_int, C.c_int, V, C.c_int, C.c_int, C.c_int, C.c_int, V, C.c_int,
                                    C.c_long, V, V, V], C.c_int),
             "qesb_compute_divergence": ([V], C.c_int),

@@ -169,3 +169,64 @@ def test_conv3d_weight_gradient(D, H, W, ci, co, up):
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     np.testing.assert_allclose(dW.view(27 * cin, co).cpu().double().numpy(), ref.numpy(), rtol=1e-4, atol=1e-3)
+
+
+# ---------------------------------------------------------------------------
+# direct conv3d kernel (rows of 128 voxels): same contract as the implicit GEMM
+# ---------------------------------------------------------------------------
+@pytest.fixture
+def conv_path():
+    yield lambda p: qesb.check(qesb.lib().qesb_net_set_conv_path(p))
+    qesb.check(qesb.lib().qesb_net_set_conv_path(0))
+
+
+@pytest.mark.parametrize("D,H,W,ci,co", [(4, 6, 128, 16, 16), (3, 5, 256, 16, 32), (4, 4, 128, 48, 16),
+                                         (2, 3, 128, 32, 32)])
+def test_conv3d_direct_forward_matches_torch_and_gemm(conv_path, D, H, W, ci, co):
+    import torch
+    torch.manual_seed(D * H + ci + co)
+    x = _bf16(torch.randn(1, ci, D, H, W))
+    w = _bf16(torch.randn(co, ci, 3, 3, 3) / (27 * ci) ** 0.5)
+    b = torch.randn(co)
+    ref = torch.relu(torch.nn.functional.conv3d(x.double(), w.double(), b.double(), padding=1))
+    bm, kp = _bm_forward(w)
+    dev = "cuda:0"
+    xd, bmd, bd = _cl(x).to(dev), bm.to(dev), b.float().to(dev)
+    out = _run_conv(xd, ci, 0, None, 0, D, H, W, 1, bmd, kp, co, bias=bd, relu=1)
+    np.testing.assert_allclose(out.numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)
+    conv_path(1)
+    out_gemm = _run_conv(xd, ci, 0, None, 0, D, H, W, 1, bmd, kp, co, bias=bd, relu=1)
+    np.testing.assert_allclose(out.numpy(), out_gemm.numpy(), rtol=1e-5, atol=1e-5)
+
+
+def test_conv3d_direct_concat_upsampled_input():
+    import torch
+    torch.manual_seed(5)
+    D, H, W, c1, c2, co = 4, 6, 128, 32, 16, 16
+    x1 = _bf16(torch.randn(1, c1, D // 2, H // 2, W // 2))
+    x2 = _bf16(torch.randn(1, c2, D, H, W))
+    w = _bf16(torch.randn(co, c1 + c2, 3, 3, 3) / (27 * 48) ** 0.5)
+    up = torch.nn.functional.interpolate(x1.double(), scale_factor=2, mode="nearest")
+    ref = torch.nn.functional.conv3d(torch.cat([up, x2.double()], 1), w.double(), padding=1)
+    bm, kp = _bm_forward(w)
+    dev = "cuda:0"
+    out = _run_conv(_cl(x1).to(dev), c1, 1, _cl(x2).to(dev), c2, D, H, W, 1, bm.to(dev), kp, co)
+    np.testing.assert_allclose(out.numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.parametrize("ci,co", [(16, 16), (32, 16), (16, 32)])
+def test_conv3d_direct_input_gradient_with_relu_mask(ci, co):
+    import torch
+    D, H, W = 3, 4, 128
+    torch.manual_seed(17 + ci + co)
+    x = torch.relu(_bf16(torch.randn(1, ci, D, H, W)).double())
+    w = _bf16(torch.randn(co, ci, 3, 3, 3) / (27 * ci) ** 0.5)
+    dy = _bf16(torch.randn(1, co, D, H, W))
+    xr = x.clone().requires_grad_(True)
+    y = torch.nn.functional.conv3d(xr, w.double(), padding=1)
+    (y * dy.double()).sum().backward()
+    ref = xr.grad * (x > 0)
+    bd, kp = _bm_dgrad(w)
+    dev = "cuda:0"
+    out = _run_conv(_cl(dy).to(dev), co, 0, None, 0, D, H, W, -1, bd.to(dev), kp, ci, mask=_cl(_bf16(x)).to(dev))
+    np.testing.assert_allclose(out.numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)

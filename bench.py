@@ -72,7 +72,7 @@ PRE_TOL = 3e-3
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
@@ -86,6 +86,9 @@ def parse():
                     help="profiling driver: one solve of this many iterations (tol 0) with --variant, exit")
     ap.add_argument("--sweeps-only", type=int, default=0,
                     help="profiling driver: set up the workload, run this many sweep launches, exit")
+    ap.add_argument("--ensemble", action="store_true",
+                    help="batched ensemble: 64 cities of uneven size x 36 wind directions (solves/s, p50/p99)")
+    ap.add_argument("--ensemble-domains", type=int, default=64)
     ap.add_argument("--forward-only", type=int, default=0,
                     help="profiling driver: run this many warm-start forward passes on one domain, exit")
     return ap.parse_args()
@@ -329,15 +332,20 @@ def run_b200(args):
         return sts, sum(x["launches"] for x in sts)
 
     def timed(fn, steps, warmup, clocks=False):
+        # the clock sampler starts before the warm-up so that its first samples
+        # (nvidia-smi takes a moment to start) fall inside the timed region
+        clk = ClockSampler(dev) if clocks else None
+        if clk:
+            clk.__enter__()
+            time.sleep(0.3)
         for _ in range(warmup):
             fn()
         barrier()
         torch.cuda.synchronize(dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         res, launches = [], 0
-        clk = ClockSampler(dev) if clocks else None
         if clk:
-            clk.__enter__()
+            clk.lines.clear()  # keep only the samples taken while the timed steps run
         e0.record(stream)
         for _ in range(steps):
             r, n = fn()
@@ -519,6 +527,82 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def run_ensemble(args):
+    """Batched ensemble: cities with Nx, Ny ~ U[64, 256] and Nz ~ U[32, 96]
+    (dx = dy = 2 m, z stretched 1.03, building count scaled from the 400 x 400
+    config's 60), each at 36 wind directions 10 degrees apart. The 36 solves of
+    a city run as one qesb_solve_batch (inputs resident beforehand: only the
+    batch is timed, CUDA events): over-relaxed pre-phase warm start, reference
+    loop, correction; launch shape autotuned per grid. solves/s = all solves /
+    the sum of batch times; latency of a solve = device time from its batch's
+    first sweep to the poll that ended it."""
+    import torch
+
+    import qesb
+
+    rng = np.random.default_rng(20260907)
+    nd, ndir = args.ensemble_domains, 36
+    dev = 0
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    lat, batch_ms, iters, pre_iters, cells_total = [], [], [], [], 0
+    shapes = []
+    for d in range(nd):
+        Nx, Ny = (int(v) for v in rng.integers(64, 257, 2))
+        Nz = int(rng.integers(32, 97))
+        dom = qesb.Domain(Nx, Ny, Nz, 2.0, 2.0, 1.0, qesb.city_dz(Nz, 1.0, 1.03))
+        nb = max(3, int(round(60 * Nx * Ny / 160000)))
+        c = qesb.city_random(dom, 700000 + d, nb)
+        base = qesb.city_build(dom, c.buildings, c.inflow)
+        wgds = [qesb.city_inflow(base, qesb.Inflow(c.inflow.u_ref, c.inflow.z_ref, c.inflow.p, 10.0 * k))
+                for k in range(ndir)]
+        solvers = [qesb.Solver_B200(dom, TOL, device=dev) for _ in range(ndir)]
+        try:
+            om = qesb.prephase_omega(Nx, Ny)
+            for s, w in zip(solvers, wgds):
+                s.set_stream(stream.cuda_stream)
+                s.set_inputs(w)
+                s.set_prephase(om, PRE_TOL, ITERMAX)
+            solvers[0].autotune()
+            nf = dom.numFaceCentered()
+            outs = [[torch.empty(nf, dtype=torch.float32, device=f"cuda:{dev}") for _ in range(3)]
+                    for _ in range(ndir)]
+            ptrs = [[o[q].data_ptr() for o in outs] for q in range(3)]
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = qesb.solve_batch(solvers, ITERMAX, *ptrs)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            batch_ms.append(e0.elapsed_time(e1))
+            lat += [x["ms_sor"] for x in st]
+            iters += [x["iterations"] for x in st]
+            pre_iters += [x["pre_iterations"] for x in st]
+            assert all(x["converged"] for x in st)
+        finally:
+            for s in solvers:
+                s.close()
+        cells_total += ndir * Nx * Ny * (Nz + 1)
+        shapes.append((Nx, Ny, Nz))
+    total_ms = float(np.sum(batch_ms))
+    n = nd * ndir
+    line = {
+        "metric": "ensemble solves/s (cities of uneven size x 36 wind directions, batched)",
+        "value": n / (total_ms * 1e-3), "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{nd} cities, Nx,Ny ~ U[64,256], Nz ~ U[32,96], x {ndir} directions",
+                   "solves": n, "batch": ndir, "tol": TOL, "itermax": ITERMAX,
+                   "warm_start": "over-relaxed pre-phase, omega = 2 - 7.5/max(Nx, Ny) within [1.85, 1.97], "
+                                 f"to {PRE_TOL}", "cells_total": cells_total},
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "ms_total": total_ms, "iterations_mean": float(np.mean(iters)),
+        "pre_iterations_mean": float(np.mean(pre_iters)),
+        "mcell_iterations_per_s": float(sum(ndir * (a - 2) * (b - 2) * (z - 1) * 1.0 for a, b, z in shapes) *
+                                        (np.mean(iters) + np.mean(pre_iters)) / (total_ms * 1e-3) / 1e6),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_sweeps_only(args):
     import qesb
 
@@ -571,6 +655,8 @@ def main():
         run_sweeps_only(args)
     elif args.forward_only:
         run_forward_only(args)
+    elif args.ensemble:
+        run_ensemble(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

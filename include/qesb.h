@@ -317,6 +317,12 @@ qesb_status qesb_city_build(const qesb_grid *grid, int n_buildings, const qesb_b
                             float *g, float *hc, float *m, float *n, float *u0, float *v0,
                             float *w0);
 
+/* Only the initial winds of qesb_city_build for another inflow over the same
+ * icellflag (power-law profile, then the solid faces zeroed): a wind-direction
+ * ensemble rebuilds no walls. */
+qesb_status qesb_city_inflow(const qesb_grid *grid, const int *icellflag, const qesb_inflow *inflow, float *u0,
+                             float *v0, float *w0);
+
 /* Seed-indexed random city: up to max_buildings non-overlapping cuboids with
  * footprints U[fp_min, fp_max] m, heights U[h_min, h_max] m, and a random
  * inflow (u_ref U[3,10] m/s at 10 m, p U[0.1,0.3], direction U[0,360)).

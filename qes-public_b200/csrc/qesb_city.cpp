@@ -254,6 +254,19 @@ qesb_status qesb_city_build(const qesb_grid *grid, int n_buildings, const qesb_b
   return QESB_OK;
 }
 
+qesb_status qesb_city_inflow(const qesb_grid *grid, const int *icellflag, const qesb_inflow *in, float *u0,
+                             float *v0, float *w0)
+{
+  if (!valid_grid(grid) || !icellflag || !in || !u0 || !v0 || !w0)
+    return qesb_fail(QESB_ERR_ARG, "qesb_city_inflow: bad arguments");
+  Grid G(*grid);
+  std::vector<float> z, zf;
+  vertical_grid(G, grid->dz_array, z, zf);
+  inflow(G, z, *in, u0, v0, w0);
+  velocity_zero(G, icellflag, u0, v0, w0);
+  return QESB_OK;
+}
+
 qesb_status qesb_city_random(const qesb_grid *grid, uint64_t seed, int max_buildings, float fp_min,
                              float fp_max, float h_min, float h_max, qesb_building *b_out,
                              int *n_out, qesb_inflow *inflow_out)

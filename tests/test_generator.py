@@ -82,3 +82,17 @@ def test_stretched_dz():
     dz = qesb.city_dz(100, 1.0, 1.03)
     assert dz[0] == dz[1] == 1.0
     assert abs(dz[100] - 1.03 ** 99) < 1e-3
+
+
+def test_city_inflow_reuses_geometry():
+    """qesb_city_inflow over a built city's flags gives the winds
+    qesb_city_build gives for that inflow (flags and coefficients shared)."""
+    w, c = qesb.random_city("city128", 5)
+    same = qesb.city_inflow(w, c.inflow)
+    for a, b in ((same.u0, w.u0), (same.v0, w.v0), (same.w0, w.w0)):
+        np.testing.assert_array_equal(a, b)
+    other = qesb.Inflow(c.inflow.u_ref, c.inflow.z_ref, c.inflow.p, (c.inflow.dir_deg + 130.0) % 360.0)
+    ref = qesb.city_build(w.domain, c.buildings, other)
+    got = qesb.city_inflow(w, other)
+    for a, b in ((got.u0, ref.u0), (got.v0, ref.v0), (got.w0, ref.w0), (got.e, ref.e), (got.icellflag, ref.icellflag)):
+        np.testing.assert_array_equal(a, b)

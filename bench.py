@@ -89,6 +89,8 @@ def parse():
     ap.add_argument("--ensemble", action="store_true",
                     help="batched ensemble: 64 cities of uneven size x 36 wind directions (solves/s, p50/p99)")
     ap.add_argument("--ensemble-domains", type=int, default=64)
+    ap.add_argument("--profile-batch", action="store_true",
+                    help="profiling driver: the headline batch (pre-phase pipeline) once untimed, once more, exit")
     ap.add_argument("--forward-only", type=int, default=0,
                     help="profiling driver: run this many warm-start forward passes on one domain, exit")
     return ap.parse_args()
@@ -629,6 +631,36 @@ def run_profile_solve(args):
     print(json.dumps({"profile_solve": args.profile_solve, **st}))
 
 
+def run_profile_batch(args):
+    """The headline step (a batch of B cities, over-relaxed pre-phase, reference
+    loop, correction) twice, for launch-list captures."""
+    import torch
+
+    import qesb
+
+    cities = [make_city(args.workload, SEED0 + i) for i in range(args.batch)]
+    solvers = [qesb.Solver_B200(w.domain, TOL) for w in cities]
+    try:
+        for s, w in zip(solvers, cities):
+            s.set_inputs(w)
+            s.set_prephase(PRE_OMEGA, PRE_TOL, ITERMAX)
+        if args.variant >= 0:
+            solvers[0].set_option("variant", args.variant)
+        nf = cities[0].domain.numFaceCentered()
+        outs = [[torch.empty(nf, dtype=torch.float32, device="cuda:0") for _ in range(3)] for _ in cities]
+        ptrs = [[o[q].data_ptr() for o in outs] for q in range(3)]
+        for _ in range(2):
+            for s in solvers:
+                s.resetLambda()
+            st = qesb.solve_batch(solvers, ITERMAX, *ptrs)
+        torch.cuda.synchronize()
+    finally:
+        for s in solvers:
+            s.close()
+    print(json.dumps({"profile_batch": args.batch, "iterations": [x["iterations"] for x in st],
+                      "pre_iterations": [x["pre_iterations"] for x in st]}))
+
+
 def run_forward_only(args):
     """Warm-start forward passes on one domain, for network captures."""
     import torch
@@ -655,6 +687,8 @@ def main():
         run_sweeps_only(args)
     elif args.forward_only:
         run_forward_only(args)
+    elif args.profile_batch:
+        run_profile_batch(args)
     elif args.ensemble:
         run_ensemble(args)
     elif args.impl == "reference":

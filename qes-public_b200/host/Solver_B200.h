@@ -21,6 +21,10 @@ public:
   Solver_B200(const Solver_B200 &) = delete;
   Solver_B200 &operator=(const Solver_B200 &) = delete;
 
+  // The library handle, for the options the Solver interface has no place
+  // for (qesb_set_prephase, qesb_set_option, qesb_set_stream, qesb_solve_batch).
+  qesb_handle *handle() const { return handle_; }
+
 protected:
   // Solver::solve semantics (src/winds/Solver_CPU.cpp:42-238): reads e..n,
   // icellflag, u0 v0 w0 and writes u v w of WGD. lambda lives in the base

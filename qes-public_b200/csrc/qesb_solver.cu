@@ -814,29 +814,31 @@ struct SweepVariant {
   void (*red_m)(SweepArgs);  // domain lists
   void (*black_m)(SweepArgs);
 };
-template <int RPB, int U, int STRIDED = 0>
+// MINB: resident CTAs per SM the compiler must allow (caps registers per
+// thread); the default allows 512 threads per SM (at most 128 registers)
+template <int RPB, int U, int STRIDED = 0, int MINB = (16 / RPB > 1 ? 16 / RPB : 1)>
 constexpr SweepVariant make_split(const char *name)
 {
   return SweepVariant{name,
                       false,
                       RPB,
                       0,
-                      k_sor_split<0, RPB, U, STRIDED, false>,
-                      k_sor_split<1, RPB, U, STRIDED, false>,
-                      k_sor_split<0, RPB, U, STRIDED, true>,
-                      k_sor_split<1, RPB, U, STRIDED, true>};
+                      k_sor_split<0, RPB, U, STRIDED, false, MINB>,
+                      k_sor_split<1, RPB, U, STRIDED, false, MINB>,
+                      k_sor_split<0, RPB, U, STRIDED, true, MINB>,
+                      k_sor_split<1, RPB, U, STRIDED, true, MINB>};
 }
-template <int RPB, int STRIDED = 0>
+template <int RPB, int STRIDED = 0, int MINB = (16 / RPB > 1 ? 16 / RPB : 1)>
 constexpr SweepVariant make_split4(const char *name)
 {
   return SweepVariant{name,
                       false,
                       RPB,
                       0,
-                      k_sor_split4<0, RPB, STRIDED, false>,
-                      k_sor_split4<1, RPB, STRIDED, false>,
-                      k_sor_split4<0, RPB, STRIDED, true>,
-                      k_sor_split4<1, RPB, STRIDED, true>};
+                      k_sor_split4<0, RPB, STRIDED, false, MINB>,
+                      k_sor_split4<1, RPB, STRIDED, false, MINB>,
+                      k_sor_split4<0, RPB, STRIDED, true, MINB>,
+                      k_sor_split4<1, RPB, STRIDED, true, MINB>};
 }
 template <int W, int NS, int ASYNC>
 constexpr SweepVariant make_bulk(const char *name)
@@ -853,15 +855,20 @@ constexpr SweepVariant make_bulk(const char *name)
 const SweepVariant kSweepVariants[] = {
     // streaming split kernels (option "variant" 5..17)
     make_split<8, 4>("split_r8_u4"), make_split<8, 1>("split_r8_u1"), make_split<8, 2>("split_r8_u2"),
-    make_split<4, 8>("split_r4_u8"), make_split<16, 2>("split_r16_u2"), make_split<4, 4>("split_r4_u4"),
+    make_split<4, 8>("split_r4_u8"), make_split<16, 2>("split_r16_u2"), make_split<4, 4, 0, 5>("split_r4_u4"),
     make_split4<4>("split4_r4"), make_split4<8>("split4_r8"), make_split4<16>("split4_r16"),
-    make_split<4, 4, 1>("split_r4_u4_strided"), make_split<8, 2, 1>("split_r8_u2_strided"),
+    make_split<4, 4, 1, 5>("split_r4_u4_strided"), make_split<8, 2, 1>("split_r8_u2_strided"),
     make_split4<4, 1>("split4_r4_strided"), make_split4<8, 1>("split4_r8_strided"),
     // staged kernels: bulk copies (18..22), per-lane async copies (23..27)
     make_bulk<4, 3, 0>("bulk_w4_s3"), make_bulk<4, 4, 0>("bulk_w4_s4"), make_bulk<4, 6, 0>("bulk_w4_s6"),
     make_bulk<8, 2, 0>("bulk_w8_s2"), make_bulk<8, 3, 0>("bulk_w8_s3"), make_bulk<4, 4, 1>("async_w4_s4"),
     make_bulk<8, 3, 1>("async_w8_s3"), make_bulk<4, 6, 1>("async_w4_s6"), make_bulk<16, 2, 1>("async_w16_s2"),
     make_bulk<8, 4, 1>("async_w8_s4"),
+    // register-capped window-order shapes (28..31): more warps per SM for the same loads
+    make_split4<8, 1, 3>("split4_r8_strided_b3"), make_split4<4, 1, 6>("split4_r4_strided_b6"),
+    make_split<4, 4, 1, 6>("split_r4_u4_strided_b6"), make_split<8, 2, 1, 4>("split_r8_u2_strided_b4"),
+    make_split4<8, 1, 4>("split4_r8_strided_b4"), make_split4<4, 1, 8>("split4_r4_strided_b8"),
+    make_split4<16, 1, 2>("split4_r16_strided_b2"), make_split4<8, 0, 3>("split4_r8_b3"),
 };
 constexpr int kNumSweep = sizeof(kSweepVariants) / sizeof(kSweepVariants[0]);
 constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the first sweep shape

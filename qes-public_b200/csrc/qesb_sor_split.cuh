@@ -155,8 +155,8 @@ __device__ __forceinline__ void split_mirror_row(const SplitDom &D, int j, int l
 // GPU at once and each warp sweeps its share of the rows, so it pays the
 // start-up latency once, reloads the per-layer tables only when k changes,
 // and never waits on another warp inside the sweep.
-template <int COLOUR, int RPB, int U, int STRIDED, bool MULTI>
-__global__ void __launch_bounds__(32 * RPB) k_sor_split(SweepArgs b)
+template <int COLOUR, int RPB, int U, int STRIDED, bool MULTI, int MINB = (16 / RPB > 1 ? 16 / RPB : 1)>
+__global__ void __launch_bounds__(32 * RPB, MINB) k_sor_split(SweepArgs b)
 {
   const int na = b.ctl->nactive;
   if (na <= 0) return;
@@ -270,8 +270,8 @@ __global__ void __launch_bounds__(32 * RPB) k_sor_split(SweepArgs b)
 // across the group edge (q-1 when i0 = 0, q+4 when i0 = 1), taken from the
 // neighbouring lane by a shuffle, or loaded at the warp's edge. Cells of the
 // group outside [qlo, qhi] are rewritten with the value this lane read.
-template <int COLOUR, int RPB, int STRIDED, bool MULTI>
-__global__ void __launch_bounds__(32 * RPB) k_sor_split4(SweepArgs b)
+template <int COLOUR, int RPB, int STRIDED, bool MULTI, int MINB = (16 / RPB > 1 ? 16 / RPB : 1)>
+__global__ void __launch_bounds__(32 * RPB, MINB) k_sor_split4(SweepArgs b)
 {
   const int na = b.ctl->nactive;
   if (na <= 0) return;

@@ -81,6 +81,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 same-SOR error and divergence checks")
     ap.add_argument("--variant", type=int, default=-1, help="sweep variant for the profiling drivers (-1: autotune)")
     ap.add_argument("--profile-solve", type=int, default=0,
                     help="profiling driver: one solve of this many iterations (tol 0) with --variant, exit")
@@ -216,6 +217,11 @@ def reference_cpu_measure(workload, seed, seconds, threads):
 
 
 def run_reference(args):
+    """The reference's Solver_CPU_RB on this host, per city of the headline
+    batch: ms per iteration sampled on the first city (every city has the same
+    grid), times the mean of the iterations the reference needs on each of the
+    batch's cities (tests/golden/ref_iters.json, equal to this solver's plain
+    iteration counts)."""
     rank, _, world = dist_env()
     if rank != 0:
         return
@@ -228,20 +234,52 @@ def run_reference(args):
                                                      max(2.0, args.cpu_seconds / max(args.steps, 1)), threads)
         steps.append(ms_it)
     ms_it = statistics.median(steps)
+    if args.workload == WORKLOAD:
+        per_city = [ref_iterations(f"{WORKLOAD}:{SEED0 + i}") for i in range(args.batch)]
+        if all(per_city):
+            iters = float(np.mean(per_city))
     value = ms_it * iters if iters else None
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.workload} seed {seed}", "solver": "Solver_CPU_RB (reference, OpenMP)",
+        "config": {"workload": f"{args.workload} seeds {seed}..{seed + args.batch - 1}",
+                   "solver": "Solver_CPU_RB (reference, OpenMP)",
                    "tol": TOL, "itermax": ITERMAX},
         "cpu_baseline": {"value": value, "unit": "ms", "cores": threads, "kind": "reference",
-                         "sample": f"{sample} red-black iterations per step timed, x {iters} iterations "
-                                   f"the reference needs to reach tol {TOL}"},
+                         "sample": f"{sample} red-black iterations per step timed on seed {seed}, x {iters} "
+                                   f"iterations (mean over the batch's cities) the reference needs to reach "
+                                   f"tol {TOL}"},
         "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "ms_per_iteration": ms_it,
     }
     print(json.dumps(line), flush=True)
+
+
+def fp64_checks(w, seed, st, lam, winds):
+    """The headline pipeline's FP32 result on one city against an FP64 run of
+    the same SOR (same phases, same iteration counts, oracle restatement in
+    double), and its FP64 final divergence against the reference solver's
+    (Solver_CPU_RB run for the iterations it needs to reach the same rule)."""
+    from oracle import oracle as O
+
+    d = w.domain
+    t0 = time.time()
+    u64, v64, w64, L64, _, _ = O.solve_f64(d, w, -1.0, st["iterations"],
+                                           phases=[(PRE_OMEGA, -1.0, st["pre_iterations"])])
+    t_f64 = time.time() - t0
+    lam_err = float(np.abs(lam.astype(np.float64) - L64).max() / max(np.abs(L64).max(), 1e-30))
+    wind_err = max(float(np.abs(a.astype(np.float64) - b).max()) for a, b in zip(winds, (u64, v64, w64)))
+    out = {"seed": seed, "pre_iterations": st["pre_iterations"], "iterations": st["iterations"],
+           "lambda_max_rel_err_vs_fp64": lam_err, "wind_max_err_vs_fp64_m_s": wind_err,
+           "max_divergence_fp64": st["max_divergence"], "fp64_run_s": t_f64}
+    riters = ref_iterations(f"{WORKLOAD}:{seed}")
+    if riters:
+        O.ref_set_threads(os.cpu_count() or 1)
+        ur, vr, wr, _, _ = _quiet(lambda: O.ref_solve(d, w, -1.0, riters, kind=1, want_lambda=False))
+        out["reference_max_divergence"] = O.max_divergence(d, w.icellflag, ur, vr, wr)
+        out["reference"] = f"Solver_CPU_RB, {riters} iterations (its count to tol {TOL})"
+    return out
 
 
 def network_flops(net, s):
@@ -392,7 +430,10 @@ def run_b200(args):
         s.resetLambda()
         return s.solve_device(ITERMAX, o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr()), 0
 
-    ms_first, _, _, _ = timed(first_domain_warm, 3, 1)
+    ms_first, res_first, _, _ = timed(first_domain_warm, 3, 1)
+    st_first = res_first[-1]
+    lam_first = solvers[0].lambda_
+    winds_first = [t.cpu().numpy() for t in outs[0]]
 
     # ---- end to end through the host API (warm step) -------------------------
     host_keep = [[pinned_copy(torch, a) for a in w.inputs()] for w in cities]  # tensors own the pinned memory
@@ -449,9 +490,10 @@ def run_b200(args):
     ms_fwd = fwd[0].elapsed_time(fwd[1]) / nf_rep
     flops = network_flops(net, s0)
 
-    # ---- reference GPU solver and CPU baseline (rank 0, N = 1) -----------------------
+    # ---- reference GPU solver, CPU baseline, FP64 checks (rank 0, N = 1) --------------
     ref_gpu = None
     cpu = None
+    precision = None
     if rank == 0 and world == 1:
         for s in solvers:
             s.close()
@@ -471,14 +513,23 @@ def run_b200(args):
                     ref_gpu = {"unavailable": "oracle/_ref/libqesref_gpu.so not built"}
             except Exception as ex:  # noqa: BLE001
                 ref_gpu = {"unavailable": str(ex)[:200]}
+        if not args.no_fp64:
+            try:
+                precision = fp64_checks(cities[0], seeds[0], st_first, lam_first, winds_first)
+            except Exception as ex:  # noqa: BLE001
+                precision = {"unavailable": str(ex)[:200]}
         if not args.no_cpu_baseline:
             try:
                 threads = os.cpu_count() or 1
                 ms_c, sample, riters = reference_cpu_measure(args.workload, seeds[0], args.cpu_seconds, threads)
+                per_city = [ref_iterations(f"{args.workload}:{sd}") for sd in seeds]
+                if all(per_city):
+                    riters = float(np.mean(per_city))
                 cpu = {"value": ms_c * riters if riters else None, "unit": "ms", "cores": threads,
                        "kind": "reference",
                        "sample": f"Solver_CPU_RB on seed {seeds[0]}: {sample} iterations timed "
-                                 f"({ms_c:.2f} ms/iteration) x {riters} iterations to tol {TOL}"}
+                                 f"({ms_c:.2f} ms/iteration) x {riters} iterations to tol {TOL} (mean over "
+                                 f"the batch's cities)"}
             except Exception as ex:  # noqa: BLE001
                 cpu = {"value": None, "unit": "ms", "cores": os.cpu_count(), "kind": "reference",
                        "sample": f"unavailable: {ex}"}
@@ -518,6 +569,7 @@ def run_b200(args):
             "network": {"bound": "tensor", "ms_per_forward": ms_fwd, "flops_per_forward": flops,
                         "achieved_tflops": flops / (ms_fwd * 1e-3) / 1e12, "peak_tflops": tpeak,
                         "frac": flops / (ms_fwd * 1e-3) / 1e12 / tpeak},
+            "precision": precision,
             "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clocks,

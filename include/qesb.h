@@ -63,6 +63,9 @@ typedef struct qesb_stats {
   int sweeps_per_launch; /* iterations fused per sweep launch */
   int launches;          /* kernels this solve launched (including polls and early exits) */
   int pre_iterations;    /* iterations of the over-relaxed pre-phase (qesb_set_prephase), 0 if none */
+  double max_divergence; /* final check, in FP64: max |du/dx + dv/dy + dw/dz| over fluid cells
+                            (icellflag 1), i in [1,nx-3], j in [1,ny-3], k in [1,nz-4], of the
+                            corrected winds; -1 when the solve wrote no winds */
 } qesb_stats;
 
 /* Library and device. */

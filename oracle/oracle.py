@@ -46,6 +46,8 @@ def port() -> C.CDLL:
         L.qo_sor.restype = i
         L.qo_sor_omega.argtypes = [i, i, i, i, i] + [_V] * 8 + [f, i, _V, _V, f]
         L.qo_sor_omega.restype = i
+        L.qo_sor_rb_f64_omega.argtypes = [i, i, i] + [_V] * 8 + [d, i, _V, d]
+        L.qo_sor_rb_f64_omega.restype = i
         L.qo_correct.argtypes = [i, i, i, f, f] + [_V] * 11
         L.qo_correct.restype = None
         L.qo_divergence_f64.argtypes = [i, i, i, f, f] + [_V] * 11
@@ -128,8 +130,11 @@ def solve(dom, w, tol, itermax, ordering=1, err_fp64=True, lam=None):
     return u, v, ww, L, it, fe
 
 
-def solve_f64(dom, w, tol, itermax):
-    """FP64 run of the same red-black SOR: (u, v, w, lambda, iters, err) in double."""
+def solve_f64(dom, w, tol, itermax, phases=None):
+    """FP64 run of the same red-black SOR: (u, v, w, lambda, iters, err) in double.
+    phases: optional [(omega, tol, itermax), ...] run in order before the
+    reference loop (the solver's over-relaxed pre-phase); omega is taken as
+    the float the GPU uses, widened to double."""
     Nx, Ny, Nz = dom.base
     nc, nf = dom.numCellCentered(), dom.numFaceCentered()
     R = np.zeros(nc, np.float64)
@@ -137,6 +142,9 @@ def solve_f64(dom, w, tol, itermax):
                              _p(w.m), _p(w.n), _p(w.u0), _p(w.v0), _p(w.w0), _p(R))
     L = np.zeros(nc, np.float64)
     fe = C.c_double()
+    for om, ptol, pit in (phases or ()):
+        port().qo_sor_rb_f64_omega(Nx, Ny, Nz, _p(w.e), _p(w.f), _p(w.g), _p(w.h), _p(w.m), _p(w.n), _p(R),
+                                   _p(L), float(ptol), int(pit), C.byref(fe), float(np.float32(om)))
     it = port().qo_sor_rb_f64(Nx, Ny, Nz, _p(w.e), _p(w.f), _p(w.g), _p(w.h), _p(w.m), _p(w.n),
                               _p(R), _p(L), float(tol), int(itermax), C.byref(fe))
     u, v, ww = (np.zeros(nf, np.float64) for _ in range(3))

@@ -221,14 +221,13 @@ void qo_divergence_f64(int Nx, int Ny, int Nz, float dx, float dy, const float *
       }
 }
 
-int qo_sor_rb_f64(int Nx, int Ny, int Nz, const float *e, const float *f, const float *g_,
-                  const float *h, const float *m, const float *n, const double *R, double *L,
-                  double tol, int itermax, double *final_error)
+int qo_sor_rb_f64_omega(int Nx, int Ny, int Nz, const float *e, const float *f, const float *g_,
+                        const float *h, const float *m, const float *n, const double *R, double *L,
+                        double tol, int itermax, double *final_error, double om)
 {
   grid_t G = mkgrid(Nx, Ny, Nz);
   long nc = G.XY * (G.nz - 1);
   double *old = (double *)malloc(sizeof(double) * nc);
-  const double om = (double)OMEGA;
   int iter = 0;
   double max_error = 1.0;
   while (iter < itermax && max_error > tol) {
@@ -262,6 +261,13 @@ int qo_sor_rb_f64(int Nx, int Ny, int Nz, const float *e, const float *f, const 
   if (final_error) *final_error = max_error;
   free(old);
   return iter;
+}
+
+int qo_sor_rb_f64(int Nx, int Ny, int Nz, const float *e, const float *f, const float *g_,
+                  const float *h, const float *m, const float *n, const double *R, double *L,
+                  double tol, int itermax, double *final_error)
+{
+  return qo_sor_rb_f64_omega(Nx, Ny, Nz, e, f, g_, h, m, n, R, L, tol, itermax, final_error, (double)OMEGA);
 }
 
 void qo_correct_f64(int Nx, int Ny, int Nz, float dx, float dy, const float *dz, const float *f,

@@ -286,6 +286,30 @@ __global__ void k_poll(SolveState *st, const double *__restrict__ err, double to
   if (st->it >= itermax) st->done = 1;
 }
 
+// Final divergence check in FP64: max over fluid cells (icellflag == 1),
+// i in [1, nx-3], j in [1, ny-3], k in [1, kmax], of
+//   |(u[i+1]-u[i])/dx + (v[j+1]-v[j])/dy + (w[k+1]-w[k])/dz[k]|
+// evaluated in double. kmax = nz-4 leaves out the last solved layer, whose top
+// face the reference never corrects (Solver_CPU.cpp:197-209 stops at k = nz-3).
+__global__ void k_max_divergence(DevGrid G, const int *__restrict__ flag, const float *__restrict__ u,
+                                 const float *__restrict__ v, const float *__restrict__ w,
+                                 const float *__restrict__ dz, float dx, float dy, int kmax, double *out)
+{
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  double mx = 0.0;
+  if (j <= G.Y - 2 && k <= kmax) {
+    for (int i = 1 + blockIdx.x * blockDim.x + threadIdx.x; i <= G.X - 2; i += gridDim.x * blockDim.x) {
+      if (flag[G.cell(i, j, k)] != 1) continue;
+      const long fc = G.face(i, j, k);
+      const double d = ((double)u[fc + 1] - u[fc]) / dx + ((double)v[fc + G.FX] - v[fc]) / dy +
+                       ((double)w[fc + G.FXY] - w[fc]) / dz[k];
+      const double a = fabs(d);
+      if (a > mx || a != a) mx = a;
+    }
+  }
+  block_max_to(out, mx);
+}
+
 // ---------------------------------------------------------------------------
 // kernels: velocity correction (Solver_CPU.cpp:157-231)
 // ---------------------------------------------------------------------------
@@ -508,6 +532,7 @@ struct qesb_handle {
   int err_cap = 0;
   SolveState *d_state = nullptr;
   SolveState *h_state = nullptr;  // pinned
+  double *d_div = nullptr;        // final divergence check (FP64)
   float *d_u = nullptr, *d_v = nullptr, *d_w = nullptr;  // output staging for host solves
   cudaEvent_t ev[4] = {};
 
@@ -1031,6 +1056,20 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
   return QESB_OK;
 }
 
+// FP64 final divergence check of (u, v, w) into h->d_div (all three needed).
+qesb_status enqueue_divergence_check(qesb_handle *h, const float *u, const float *v, const float *w, cudaStream_t s)
+{
+  const DevGrid &G = h->G;
+  CK(cudaMemsetAsync(h->d_div, 0, sizeof(double), s));
+  const int kmax = G.FZ - 4;
+  if (kmax >= 1) {
+    k_max_divergence<<<dim3((G.X + 255) / 256, G.Y - 2, kmax), 256, 0, s>>>(G, h->d_flag, u, v, w, h->d_dz, h->dx,
+                                                                           h->dy, kmax, h->d_div);
+    CK(cudaGetLastError());
+  }
+  return QESB_OK;
+}
+
 qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w, qesb_stats *st)
 {
   if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
@@ -1070,9 +1109,14 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
       h->d_dz, h->dx, h->dy, u, v, w);
   CK(cudaGetLastError());
   CK(cudaEventRecord(h->ev[3], s));
+  const bool check = u && v && w;
+  if (check) CKS(enqueue_divergence_check(h, u, v, w, s));
+  double div = -1.0;
+  if (check) CK(cudaMemcpyAsync(&div, h->d_div, sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (st) {
+    st->max_divergence = div;
     float a = 0, b = 0;
     CK(cudaEventElapsedTime(&a, h->ev[0], h->ev[3]));
     CK(cudaEventElapsedTime(&b, h->ev[1], h->ev[2]));
@@ -1191,6 +1235,7 @@ qesb_status qesb_create(const qesb_grid *grid, float tol, int device, qesb_handl
   TRY(dalloc(&h->d_val, 6 * G.Z));
   TRY(dalloc(&h->d_bad, 1));
   TRY(dalloc(&h->d_state, 1));
+  TRY(dalloc(&h->d_div, 1));
   TRY(h->list.create(1));
   TRY(ensure_err(h, 1024));
   if (cudaMallocHost((void **)&h->h_state, sizeof(SolveState)) != cudaSuccess ||
@@ -1626,6 +1671,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
         h->dy, u ? u[i] : nullptr, v ? v[i] : nullptr, w ? w[i] : nullptr);
     cudaError_t ce = cudaGetLastError();
     if (ce != cudaSuccess) qs = qesb_fail(QESB_ERR_CUDA, "batch finish: %s", cudaGetErrorString(ce));
+    if (qs == QESB_OK && u && v && w && u[i] && v[i] && w[i]) qs = enqueue_divergence_check(h, u[i], v[i], w[i], s);
   }
   CK(cudaEventRecord(h0->ev[3], s));
   cudaError_t se = cudaStreamSynchronize(s);
@@ -1638,6 +1684,9 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   for (int i = 0; i < n; ++i) {
     SolveState sti;
     CK(cudaMemcpy(&sti, hs[i]->d_state, sizeof sti, cudaMemcpyDeviceToHost));
+    double div = -1.0;
+    if (u && v && w && u[i] && v[i] && w[i]) CK(cudaMemcpy(&div, hs[i]->d_div, sizeof div, cudaMemcpyDeviceToHost));
+    if (st) st[i].max_divergence = div;
     if (sti.nan && nan_at < 0) nan_at = i;
     if (st) {
       st[i].iterations = itermax > 0 ? sti.it : 0;

@@ -58,7 +58,8 @@ class Grid(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("residual", C.c_double),
                 ("ms_total", C.c_double), ("ms_sor", C.c_double), ("path", C.c_int),
-                ("sweeps_per_launch", C.c_int), ("launches", C.c_int), ("pre_iterations", C.c_int)]
+                ("sweeps_per_launch", C.c_int), ("launches", C.c_int), ("pre_iterations", C.c_int),
+                ("max_divergence", C.c_double)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -58,6 +58,7 @@ def test_batch_matches_oracle_per_domain(variant):
         np.testing.assert_array_equal(v, vo)
         np.testing.assert_array_equal(ww, wo)
         assert 0 < s["ms_sor"] <= s["ms_total"]
+        assert s["max_divergence"] == O.max_divergence(d, w.icellflag, u, v, ww)
     # the domains stop on different iterations
     assert len({s["iterations"] for s in st}) > 1
 

@@ -151,6 +151,18 @@ def test_converged_winds_match_solver_cpu_cuboid100():
         assert abs(comp.astype(np.float64).sum() - float(z[key])) <= WIND_TOL * comp.size
     div = O.max_divergence(d, w.icellflag, u, v, ww)
     assert div <= float(z["max_div"]) * 1.05 + 1e-6, (div, float(z["max_div"]))
+    # the solver's own FP64 final check is the same number
+    assert st["max_divergence"] == div
+
+
+@pytest.mark.parametrize("variant", [5, 17, BULK + 1])
+def test_final_divergence_check_matches_oracle_metric(golden, variant):
+    """qesb_stats.max_divergence (computed on the device in FP64 after the
+    correction) equals the oracle's metric on the same winds, for single and
+    batched solves."""
+    d, w, z = golden("small_city.npz")
+    u, v, ww, L, st, _ = gpu_solve(d, w, 300, tol=1.1e-3, variant=variant)
+    assert st["max_divergence"] == O.max_divergence(d, w.icellflag, u, v, ww) > 0
 
 
 def test_nan_input_is_reported():
@@ -258,3 +270,17 @@ def test_overrelaxed_prephase_then_reference_loop(variant, omega, pre_tol, pre_m
     assert st["iterations"] == it and st["converged"] == 1
     np.testing.assert_array_equal(L, Lo)
     np.testing.assert_array_equal(u, O.correct(d, w, Lo)[0])
+
+
+@pytest.mark.parametrize("seed", [500001, 500004])
+def test_benchmark_cities_stop_where_the_reference_stops(seed):
+    """On the benchmark's 256x256x64 cities the solver stops on the iteration
+    the reference Solver_CPU_RB stops on (tests/golden/ref_iters.json, made by
+    running the reference build)."""
+    import json
+
+    ref = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ref_iters.json")))
+    w, _ = qesb.random_city("city256", seed)
+    with qesb.Solver_B200(w.domain, 1e-3) as s:
+        st = s.solve(w, 10000)
+    assert st["converged"] and st["iterations"] == ref[f"city256:{seed}"]["Solver_CPU_RB"]["iterations"]

@@ -171,6 +171,9 @@ qesb_status qesb_set_tolerance(qesb_handle *h, float tol);
 qesb_status qesb_set_option(qesb_handle *h, const char *key, int value);
 /* cudaStream_t to run on (NULL = the handle's own stream). */
 qesb_status qesb_set_stream(qesb_handle *h, void *stream);
+/* The stream the handle's work runs on (its own, or the one set): callers
+ * that add work on the same data (the warm-start glue below) order it there. */
+qesb_status qesb_get_stream(qesb_handle *h, void **stream);
 
 /* ---------------------------------------------------------------------
  * Warm-start network (tensor-core kernels).
@@ -319,6 +322,18 @@ qesb_status qesb_city_build(const qesb_grid *grid, int n_buildings, const qesb_b
                             const qesb_inflow *inflow, int *icellflag, float *e, float *f,
                             float *g, float *hc, float *m, float *n, float *u0, float *v0,
                             float *w0);
+
+/* qesb_city_build on the device: the same icellflag, e..n, u0, v0, w0, bit for
+ * bit, written by kernels into device arrays (reference layouts) on `stream`
+ * (NULL: the default stream). The building list and inflow are host inputs;
+ * the vertical grid, each building's cell box and layer range, and the
+ * power-law profile are evaluated on the host as qesb_city_build does, the
+ * per-cell and per-face work on the device. Returns once the arrays are
+ * written. Restates the same reference steps as qesb_city_build. */
+qesb_status qesb_city_build_device(const qesb_grid *grid, int n_buildings, const qesb_building *b,
+                                   const qesb_inflow *inflow, int *icellflag, float *e, float *f, float *g,
+                                   float *hc, float *m, float *n, float *u0, float *v0, float *w0,
+                                   void *stream);
 
 /* Only the initial winds of qesb_city_build for another inflow over the same
  * icellflag (power-law profile, then the solid faces zeroed): a wind-direction

@@ -326,9 +326,11 @@ __global__ void k_correct(DevGrid G, const float *__restrict__ L, const float *_
                           const float *__restrict__ dz, float dx, float dy, float *__restrict__ u,
                           float *__restrict__ v, float *__restrict__ w)
 {
-  const int j = blockIdx.y, k = blockIdx.z;
+  // a warp per face row (j, k), 32 faces per step along x
+  const int j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+  if (j >= G.FY) return;
   const float half = 1.0f / (2.0f * 1.0f);
-  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < G.FX; i += gridDim.x * blockDim.x) {
+  for (int i = threadIdx.x; i < G.FX; i += blockDim.x) {
     const long q = G.face(i, j, k);
     float uu = u0[q], vv = v0[q], ww = w0[q];
     const bool corr = i >= 1 && i <= G.FX - 2 && j >= 1 && j <= G.FY - 2 && k >= 1 && k <= G.FZ - 3;
@@ -1104,7 +1106,7 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
     else CKS(run_iterations_full(h, itermax));
   }
   CK(cudaEventRecord(h->ev[2], s));
-  k_correct<<<row_grid(G, G.FY, G.FZ, G.FX), 256, 0, s>>>(
+  k_correct<<<dim3(1, (G.FY + 7) / 8, G.FZ), dim3(32, 8), 0, s>>>(
       G, h->d_lam, h->d_in[1], h->d_in[3], h->d_in[5], h->d_flag, h->d_u0, h->d_v0, h->d_w0,
       h->d_dz, h->dx, h->dy, u, v, w);
   CK(cudaGetLastError());
@@ -1666,7 +1668,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     const DevGrid &G = h->G;
     k_split_mirror_ring<<<G.Y, 128, 0, s>>>(G, h->S, h->d_lam_s);
     k_split_to_pad<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam_s, h->d_lam);
-    k_correct<<<row_grid(G, G.FY, G.FZ, G.FX), 256, 0, s>>>(
+    k_correct<<<dim3(1, (G.FY + 7) / 8, G.FZ), dim3(32, 8), 0, s>>>(
         G, h->d_lam, h->d_in[1], h->d_in[3], h->d_in[5], h->d_flag, h->d_u0, h->d_v0, h->d_w0, h->d_dz, h->dx,
         h->dy, u ? u[i] : nullptr, v ? v[i] : nullptr, w ? w[i] : nullptr);
     cudaError_t ce = cudaGetLastError();
@@ -1751,6 +1753,13 @@ qesb_status qesb_set_stream(qesb_handle *h, void *stream)
 {
   if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
   h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return QESB_OK;
+}
+
+qesb_status qesb_get_stream(qesb_handle *h, void **stream)
+{
+  if (!h || !stream) return qesb_fail(QESB_ERR_ARG, "qesb_get_stream: null argument");
+  *stream = h->stream;
   return QESB_OK;
 }
 

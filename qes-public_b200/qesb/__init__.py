@@ -112,6 +112,7 @@ def lib() -> C.CDLL:
             "qesb_num_variants": ([], C.c_int),
             "qesb_set_option": ([V, C.c_char_p, C.c_int], C.c_int),
             "qesb_set_stream": ([V, V], C.c_int),
+            "qesb_get_stream": ([V, C.POINTER(V)], C.c_int),
             "qesb_solve_noalloc": ([C.POINTER(Grid), C.c_float, C.c_int] + [V] * 14
                                    + [V, C.POINTER(Stats)], C.c_int),
             "qesb_umma_selftest": ([V, V, V, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
@@ -140,6 +141,8 @@ def lib() -> C.CDLL:
             "qesb_city_dz": ([C.c_int, C.c_float, C.c_float, _FP], C.c_int),
             "qesb_city_build": ([C.POINTER(Grid), C.c_int, C.POINTER(Building), C.POINTER(Inflow)]
                                 + [V] * 10, C.c_int),
+            "qesb_city_build_device": ([C.POINTER(Grid), C.c_int, C.POINTER(Building), C.POINTER(Inflow)]
+                                       + [V] * 10 + [V], C.c_int),
             "qesb_city_inflow": ([C.POINTER(Grid), V, C.POINTER(Inflow), V, V, V], C.c_int),
             "qesb_city_random": ([C.POINTER(Grid), C.c_uint64, C.c_int, C.c_float, C.c_float,
                                   C.c_float, C.c_float, C.POINTER(Building), _IP,
@@ -357,6 +360,12 @@ class Solver_B200:
     def set_stream(self, stream_ptr: int | None):
         check(lib().qesb_set_stream(self._h, stream_ptr))
 
+    def stream_ptr(self) -> int:
+        """The cudaStream_t the handle's work runs on."""
+        out = C.c_void_p()
+        check(lib().qesb_get_stream(self._h, C.byref(out)))
+        return out.value or 0
+
     def residual_history(self, n: int) -> np.ndarray:
         out = np.empty(n, dtype=np.float64)
         check(lib().qesb_get_residual_history(self._h, _ptr(out), int(n)))
@@ -431,6 +440,17 @@ def city_build(domain: Domain, buildings, inflow: Inflow) -> WINDSGeneralData:
                                 *[_ptr(a) for a in (wgd.icellflag, wgd.e, wgd.f, wgd.g, wgd.h,
                                                     wgd.m, wgd.n, wgd.u0, wgd.v0, wgd.w0)]))
     return wgd
+
+
+def city_build_device(domain: Domain, buildings, inflow: Inflow, arrays: dict, stream=None):
+    """qesb_city_build_device into device arrays: `arrays` maps icellflag, e,
+    f, g, h, m, n, u0, v0, w0 to device pointers (ints) in the reference
+    layouts."""
+    nb = len(buildings)
+    arr = (Building * max(nb, 1))(*buildings)
+    g = domain.grid_struct()
+    names = ("icellflag", "e", "f", "g", "h", "m", "n", "u0", "v0", "w0")
+    check(lib().qesb_city_build_device(C.byref(g), nb, arr, C.byref(inflow), *[arrays[k] for k in names], stream))
 
 
 def city_inflow(wgd: WINDSGeneralData, inflow: Inflow) -> WINDSGeneralData:

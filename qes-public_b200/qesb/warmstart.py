@@ -149,6 +149,8 @@ class WarmStartNet:
             b[f"d{l}a"], b[f"d{l}"] = bf(l, C[l]), bf(l, C[l])
             b[f"gup{l}"] = f32(l, C[l + 1])       # gradient of upsample(level l+1) at level l
             b[f"gsk{l}"] = f32(l, C[l])           # gradient of the skip e_l from the decoder
+        # the zero fills ran on torch's stream; the kernels may run on another
+        T.cuda.synchronize(d)
         self._buf[key] = b
         return b
 
@@ -254,12 +256,20 @@ class WarmStartNet:
         check(lib().qesb_warm_input(solver._h, _p(self._bufs(s)["x"]), IN_CH, _p(scale)))
 
     def warm_start(self, solver: Solver_B200, stream=None):
-        """Predicts lambda for the solver's inputs and sets it as the start."""
+        """Predicts lambda for the solver's inputs and sets it as the start.
+        Everything runs on the solver's stream (the input and apply kernels
+        are the handle's work, ordered there); `stream`, when given, must be
+        that stream."""
         s = shapes_of(solver)
-        scale = self.torch.zeros(1, dtype=self.torch.int32, device=self.dev)
-        self.input_from(solver, s, scale)
-        y = self.forward(s, stream)
-        check(lib().qesb_warm_apply(solver._h, _p(y), HEAD_N, _p(scale)))
+        hs = solver.stream_ptr()
+        if stream is not None and int(stream) != hs:
+            raise ValueError("warm_start: stream differs from the solver's stream")
+        if getattr(self, "_scale", None) is None:
+            self._scale = self.torch.zeros(1, dtype=self.torch.int32, device=self.dev)
+            self.torch.cuda.synchronize(self.dev)
+        self.input_from(solver, s, self._scale)
+        y = self.forward(s, hs)
+        check(lib().qesb_warm_apply(solver._h, _p(y), HEAD_N, _p(self._scale)))
         return s
 
     # ------------------------------------------------------------------ persistence

@@ -50,6 +50,7 @@ def generate(net, n, workload, target_iters, threads=8):
     solver = None
     s = None
     scale = torch.zeros(1, dtype=torch.int32, device=net.dev)
+    torch.cuda.synchronize()  # its zero fill is torch's work; the kernels that use it run on the solver's
     t0 = time.time()
     for k, w in enumerate(cities()):
         if solver is None:
@@ -63,9 +64,10 @@ def generate(net, n, workload, target_iters, threads=8):
         solver.resetLambda()
         solver.solve(w, target_iters, set_inputs=False)
         net.input_from(solver, s, scale)
+        qesb.check(qesb.lib().qesb_warm_target(solver._h, T[k].data_ptr(), weight.data_ptr(), scale.data_ptr()))
+        torch.cuda.synchronize()  # the input and target kernels ran on the solver's stream
         xb = net._bufs(s)["x"].view(s.V(0), ws.IN_CH)
         X[k].copy_(xb[:, :5])
-        qesb.check(qesb.lib().qesb_warm_target(solver._h, T[k].data_ptr(), weight.data_ptr(), scale.data_ptr()))
         if k % 200 == 0:
             torch.cuda.synchronize()
             print(f"  generated {k + 1}/{n} ({time.time() - t0:.1f} s)", flush=True)

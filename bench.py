@@ -585,8 +585,8 @@ def run_ensemble(args):
     """Batched ensemble: cities with Nx, Ny ~ U[64, 256] and Nz ~ U[32, 96]
     (dx = dy = 2 m, z stretched 1.03, building count scaled from the 400 x 400
     config's 60), each at 36 wind directions 10 degrees apart. The 36 solves of
-    a city run as one qesb_solve_batch (inputs resident beforehand: only the
-    batch is timed, CUDA events): over-relaxed pre-phase warm start, reference
+    a city run as one qesb_solve_batch (inputs built on the device beforehand
+    and reported as setup_ms_per_solve; only the batch is timed, CUDA events): over-relaxed pre-phase warm start, reference
     loop, correction; launch shape autotuned per grid. solves/s = all solves /
     the sum of batch times; latency of a solve = device time from its batch's
     first sweep to the poll that ended it."""
@@ -612,22 +612,38 @@ def run_ensemble(args):
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(device=dev)
     lat, batch_ms, iters, pre_iters, cells_total = [], [], [], [], 0
-    shapes = []
+    shapes, setup_ms = [], []
     for d in shard.rank_share(nd, world, rank):  # cities of this rank; none crosses ranks
         Nx, Ny, Nz = dims[d]
         dom = qesb.Domain(Nx, Ny, Nz, 2.0, 2.0, 1.0, qesb.city_dz(Nz, 1.0, 1.03))
         nb = max(3, int(round(60 * Nx * Ny / 160000)))
         c = qesb.city_random(dom, 700000 + d, nb)
-        base = qesb.city_build(dom, c.buildings, c.inflow)
-        wgds = [qesb.city_inflow(base, qesb.Inflow(c.inflow.u_ref, c.inflow.z_ref, c.inflow.p, 10.0 * k))
-                for k in range(ndir)]
         solvers = [qesb.Solver_B200(dom, TOL, device=dev) for _ in range(ndir)]
         try:
             om = qesb.prephase_omega(Nx, Ny)
-            for s, w in zip(solvers, wgds):
+            # inputs built on the device (qesb_city_build_device), one set per
+            # direction, handed to the handles as device arrays
+            nc_, nf_ = dom.numCellCentered(), dom.numFaceCentered()
+            names = ("icellflag", "e", "f", "g", "h", "m", "n", "u0", "v0", "w0")
+            torch.cuda.synchronize(dev)
+            t_set = time.perf_counter()
+            arrays = []
+            for k in range(ndir):
+                a = {q: torch.empty(nc_ if q not in ("u0", "v0", "w0") else nf_,
+                                    dtype=torch.int32 if q == "icellflag" else torch.float32,
+                                    device=f"cuda:{dev}") for q in names}
+                torch.cuda.current_stream(dev).synchronize()
+                qesb.city_build_device(dom, c.buildings,
+                                       qesb.Inflow(c.inflow.u_ref, c.inflow.z_ref, c.inflow.p, 10.0 * k),
+                                       {q: v.data_ptr() for q, v in a.items()}, stream.cuda_stream)
+                arrays.append(a)
+            for s, a in zip(solvers, arrays):
                 s.set_stream(stream.cuda_stream)
-                s.set_inputs(w)
+                s.set_inputs_device(*[a[q].data_ptr() for q in ("e", "f", "g", "h", "m", "n", "icellflag", "u0",
+                                                                 "v0", "w0")])
                 s.set_prephase(om, PRE_TOL, ITERMAX)
+            torch.cuda.synchronize(dev)
+            setup_ms.append(1e3 * (time.perf_counter() - t_set))
             solvers[0].autotune()
             nf = dom.numFaceCentered()
             outs = [[torch.empty(nf, dtype=torch.float32, device=f"cuda:{dev}") for _ in range(3)]
@@ -650,6 +666,7 @@ def run_ensemble(args):
         cells_total += ndir * Nx * Ny * (Nz + 1)
         shapes.append((Nx, Ny, Nz))
     total_ms = shard.max_over_ranks(float(np.sum(batch_ms)), device=f"cuda:{dev}" if world > 1 else None)
+    setup_total = shard.max_over_ranks(float(np.sum(setup_ms)), device=f"cuda:{dev}" if world > 1 else None)
     lat = shard.gather_lists(lat)
     iters, pre_iters = shard.gather_lists(iters), shard.gather_lists(pre_iters)
     cells_total = int(sum(shard.gather_lists([cells_total])))
@@ -671,6 +688,9 @@ def run_ensemble(args):
                    "warm_start": "over-relaxed pre-phase, omega = 2 - 7.5/max(Nx, Ny) within [1.85, 1.97], "
                                  f"to {PRE_TOL}", "cells_total": cells_total},
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "setup_ms_per_solve": setup_total / n,
+        "setup": "inputs (flags, wall coefficients, winds) built on the device by qesb_city_build_device "
+                 "and handed over with qesb_set_inputs_device; wall clock, not in value",
         "ms_total": total_ms, "iterations_mean": float(np.mean(iters)),
         "pre_iterations_mean": float(np.mean(pre_iters)),
         "mcell_iterations_per_s": float(sum(ndir * (a - 2) * (b - 2) * (z - 1) * 1.0 for a, b, z in shapes) *

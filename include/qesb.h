@@ -194,6 +194,10 @@ qesb_status qesb_compute_divergence(qesb_handle *h);
 qesb_status qesb_warm_input(qesb_handle *h, void *x, int C, unsigned *scale);
 qesb_status qesb_warm_target(qesb_handle *h, float *tgt, float *w, const unsigned *scale);
 qesb_status qesb_warm_apply(qesb_handle *h, const float *yhead, int N, const unsigned *scale);
+/* qesb_warm_apply for a network run at half resolution: yhead on the
+ * (Nz/2) x (Ny/2) x (Nx/2) grid (even sizes), interpolated trilinearly to
+ * the cell centres. */
+qesb_status qesb_warm_apply_up2(qesb_handle *h, const float *yhead, int N, const unsigned *scale);
 
 /* Self-test of the tcgen05 GEMM core: C[128 x N] = A[128 x K] * B[N x K]^T
  * in BF16 with FP32 accumulation. A is [128][K] (a_mn = 0) or [K][128]
@@ -232,6 +236,8 @@ qesb_status qesb_conv3d_wgrad(const void *x1, int c1, int up1, const void *x2, i
 /* Elementwise kernels of the network (device pointers; BF16 activations
  * channels-last; FP32 gradients where named float). */
 qesb_status qesb_net_pool2(const void *x, void *y, int D, int H, int W, int C, void *stream);
+/* 2x2x2 average of an FP32 scalar field [D][H][W] (even sizes). */
+qesb_status qesb_net_pool2_f32(const float *x, float *y, int D, int H, int W, void *stream);
 qesb_status qesb_net_skip_grad(const float *gcat, int ccat, int coff, const float *gpool, const void *e,
                                void *ge, int D, int H, int W, int C, void *stream);
 qesb_status qesb_net_up_grad(const float *gcat, int ccat, const void *x, void *gx, int D, int H, int W,

@@ -713,6 +713,22 @@ __global__ void k_pool2(const __nv_bfloat16 *__restrict__ x, __nv_bfloat16 *__re
   }
 }
 
+// 2x2x2 average of an FP32 scalar field (training targets and weights of a
+// network run at half resolution).
+__global__ void k_pool2_f32(const float *__restrict__ x, float *__restrict__ y, int D, int H, int W)
+{
+  const int d = D / 2, h = H / 2, w = W / 2;
+  const long n = (long)d * h * w;
+  for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < n; v += (long)gridDim.x * blockDim.x) {
+    const int xx = (int)(v % w), yy = (int)((v / w) % h), zz = (int)(v / ((long)w * h));
+    float s = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      s += x[((long)(2 * zz + (q >> 2)) * H + 2 * yy + ((q >> 1) & 1)) * W + 2 * xx + (q & 1)];
+    y[v] = s * 0.125f;
+  }
+}
+
 // Gradient into a skip tensor e (level grid D x H x W, C channels):
 //   g_e = (gcat[v][coff + c] + gpool[parent(v)][c] / 8) * (e[v][c] > 0)
 // gcat: FP32 input gradient of the decoder conv that reads e (its channels
@@ -889,6 +905,15 @@ qesb_status qesb_net_pool2(const void *x, void *y, int D, int H, int W, int C, v
   if (!x || !y || D % 2 || H % 2 || W % 2 || C <= 0) return qesb_fail(QESB_ERR_ARG, "qesb_net_pool2: bad arguments");
   const long n = (long)(D / 2) * (H / 2) * (W / 2) * C;
   k_pool2<<<gs_blocks(n), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)x, (__nv_bfloat16 *)y, D, H, W, C);
+  NET_CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_net_pool2_f32(const float *x, float *y, int D, int H, int W, void *stream)
+{
+  if (!x || !y || D % 2 || H % 2 || W % 2) return qesb_fail(QESB_ERR_ARG, "qesb_net_pool2_f32: bad arguments");
+  const long n = (long)(D / 2) * (H / 2) * (W / 2);
+  k_pool2_f32<<<gs_blocks(n), 256, 0, (cudaStream_t)stream>>>(x, y, D, H, W);
   NET_CK(cudaGetLastError());
   return QESB_OK;
 }

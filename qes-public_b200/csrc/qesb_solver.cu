@@ -443,6 +443,50 @@ __global__ void k_warm_apply(DevGrid G, int Dn, const float *__restrict__ yhead,
   }
 }
 
+// As k_warm_apply for a network run at half resolution: yhead is the
+// (Dn/2) x (Y/2) x (X/2) grid, and each fine cell takes the trilinear
+// interpolation of it at its centre (coarse coordinate f/2 - 1/4 per axis,
+// constant beyond the outermost coarse centres), so the start carries no
+// 2-cell steps for the sweeps to smooth.
+__device__ __forceinline__ void up2_axis(int f, int n2, int &a, int &b, float &t)
+{
+  const float c = 0.5f * (float)f - 0.25f;
+  const int lo = (int)floorf(c);
+  t = c - (float)lo;
+  a = min(max(lo, 0), n2 - 1);
+  b = min(max(lo + 1, 0), n2 - 1);
+}
+
+__global__ void k_warm_apply_up2(DevGrid G, int Dn, const float *__restrict__ yhead, int N,
+                                 const unsigned *__restrict__ smax, float *__restrict__ L)
+{
+  const int j = blockIdx.y, k = blockIdx.z;
+  const float s = __uint_as_float(*smax);
+  const int kk = k == 0 ? 1 : k;
+  const int D2 = Dn / 2, H2 = G.Y / 2, W2 = G.X / 2;
+  int z0, z1, y0, y1;
+  float tz, ty;
+  up2_axis(kk, D2, z0, z1, tz);
+  up2_axis(j, H2, y0, y1, ty);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G.X; i += gridDim.x * blockDim.x) {
+    const bool upd = i >= 1 && i <= G.X - 2 && j >= 1 && j <= G.Y - 2 && kk >= 1 && kk <= G.Z - 2 && kk < Dn;
+    float v = 0.0f;
+    if (upd) {
+      int x0, x1;
+      float tx;
+      up2_axis(i, W2, x0, x1, tx);
+      auto at = [&](int z, int y, int x) { return yhead[(((long)z * H2 + y) * W2 + x) * N]; };
+      const float c00 = at(z0, y0, x0) * (1.0f - tx) + at(z0, y0, x1) * tx;
+      const float c01 = at(z0, y1, x0) * (1.0f - tx) + at(z0, y1, x1) * tx;
+      const float c10 = at(z1, y0, x0) * (1.0f - tx) + at(z1, y0, x1) * tx;
+      const float c11 = at(z1, y1, x0) * (1.0f - tx) + at(z1, y1, x1) * tx;
+      const float c0 = c00 * (1.0f - ty) + c01 * ty, c1 = c10 * (1.0f - ty) + c11 * ty;
+      v = s * (c0 * (1.0f - tz) + c1 * tz);
+    }
+    L[G.pad(i, j, k)] = v;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------
@@ -1466,6 +1510,18 @@ qesb_status qesb_warm_apply(qesb_handle *h, const float *yhead, int N, const uns
   CK(cudaSetDevice(h->device));
   k_warm_apply<<<dim3((h->G.X + 127) / 128, h->G.Y, h->G.Z), 128, 0, h->stream>>>(h->G, h->G.Z - 1, yhead, N,
                                                                                   scale, h->d_lam);
+  CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_warm_apply_up2(qesb_handle *h, const float *yhead, int N, const unsigned *scale)
+{
+  if (!h || !yhead || !scale || N < 1) return qesb_fail(QESB_ERR_ARG, "qesb_warm_apply_up2: bad arguments");
+  if ((h->G.Z - 1) % 2 || h->G.Y % 2 || h->G.X % 2)
+    return qesb_fail(QESB_ERR_ARG, "qesb_warm_apply_up2: the net grid (Nz x Ny x Nx) must have even sizes");
+  CK(cudaSetDevice(h->device));
+  k_warm_apply_up2<<<dim3((h->G.X + 127) / 128, h->G.Y, h->G.Z), 128, 0, h->stream>>>(h->G, h->G.Z - 1, yhead, N,
+                                                                                      scale, h->d_lam);
   CK(cudaGetLastError());
   return QESB_OK;
 }

@@ -125,7 +125,9 @@ def lib() -> C.CDLL:
             "qesb_warm_input": ([V, V, C.c_int, V], C.c_int),
             "qesb_warm_target": ([V, V, V, V], C.c_int),
             "qesb_warm_apply": ([V, V, C.c_int, V], C.c_int),
+            "qesb_warm_apply_up2": ([V, V, C.c_int, V], C.c_int),
             "qesb_net_pool2": ([V, V, C.c_int, C.c_int, C.c_int, C.c_int, V], C.c_int),
+            "qesb_net_pool2_f32": ([V, V, C.c_int, C.c_int, C.c_int, V], C.c_int),
             "qesb_net_skip_grad": ([V, C.c_int, C.c_int, V, V, V, C.c_int, C.c_int, C.c_int, C.c_int, V],
                                    C.c_int),
             "qesb_net_up_grad": ([V, C.c_int, V, V, C.c_int, C.c_int, C.c_int, C.c_int, V], C.c_int),

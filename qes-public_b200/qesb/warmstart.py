@@ -1,10 +1,11 @@
 """Learned warm start for the lambda solve.
 
-A 3D convolutional encoder-decoder (channels 16 -> 32 -> 64 -> 128 and two
-more 128-channel levels, 2x2x2 average pooling down, nearest upsampling and
-skip concatenation up)
-maps per-cell features of a domain (R / max|R|, solid flag, dz profile,
-boundary flag, height) to lambda / max|R|. Every convolution (forward, input
+A 3D convolutional encoder-decoder (channels 16 -> 32 -> 64 -> 128 by
+default, 2x2x2 average pooling down, nearest upsampling and skip
+concatenation up) maps per-cell features of a domain (R / max|R|, solid flag,
+dz profile, boundary flag, height) to lambda / max|R|, at the cell grid
+(res = 1) or at the grid halved in every direction (res = 2: features
+2x2x2-averaged, prediction interpolated trilinearly back to the cells). Every convolution (forward, input
 gradient, weight gradient) runs in the library's tcgen05 kernels with BF16
 operands and FP32 accumulation (qesb_conv3d, qesb_conv3d_wgrad); pooling,
 gradient routing, the loss and Adam are the library's kernels too. torch only
@@ -98,14 +99,19 @@ class WarmStartNet:
     by 2^l. Encoder: two convolutions per level, 2x2x2 average pooling down.
     Decoder: from level L-2 up to 0, a convolution of [upsample(level l+1),
     skip e_l] then a second convolution; a linear head gives lambda / max|R|.
-    Six levels put the whole training domain inside the bottleneck's reach.
+    Four levels (16-128 channels) by default; deeper stacks train worse here.
     """
 
-    CH = (16, 32, 64, 128, 128, 128)
+    CH = (16, 32, 64, 128)
 
-    def __init__(self, device=0, seed=0, channels=None):
+    def __init__(self, device=0, seed=0, channels=None, res=1):
+        """res = 2: the network runs on the grid halved in every direction
+        (input 2x2x2-averaged, prediction interpolated trilinearly back)."""
         import torch
 
+        if res not in (1, 2):
+            raise ValueError("res must be 1 or 2")
+        self.res = res
         self.torch = torch
         self.dev = torch.device(f"cuda:{device}")
         self.CH = tuple(channels) if channels else self.CH
@@ -250,17 +256,37 @@ class WarmStartNet:
             raise RuntimeError("a tensor-core kernel's completion wait gave up")
 
     # ------------------------------------------------------------------ solver glue
+    def net_shapes(self, solver: Solver_B200) -> Shapes:
+        """The grid the network runs on for this solver's domain."""
+        f = shapes_of(solver)
+        return Shapes(f.D // self.res, f.H // self.res, f.W // self.res)
+
+    def _full_input(self, f: Shapes):
+        key = ("xfull", f.D, f.H, f.W)
+        if key not in self._buf:
+            self._buf[key] = self.torch.zeros(f.V(0) * IN_CH, dtype=self.torch.bfloat16, device=self.dev)
+            self.torch.cuda.synchronize(self.dev)
+        return self._buf[key]
+
     def input_from(self, solver: Solver_B200, s: Shapes, scale):
-        """Network input of the solver's current inputs into buffer 'x'."""
+        """Network input of the solver's current inputs into buffer 'x' of the
+        network grid s (2x2x2 averages of the cell features when res = 2), on
+        the solver's stream."""
         check(lib().qesb_compute_divergence(solver._h))
-        check(lib().qesb_warm_input(solver._h, _p(self._bufs(s)["x"]), IN_CH, _p(scale)))
+        if self.res == 1:
+            check(lib().qesb_warm_input(solver._h, _p(self._bufs(s)["x"]), IN_CH, _p(scale)))
+            return
+        f = shapes_of(solver)
+        xf = self._full_input(f)
+        check(lib().qesb_warm_input(solver._h, _p(xf), IN_CH, _p(scale)))
+        check(lib().qesb_net_pool2(_p(xf), _p(self._bufs(s)["x"]), f.D, f.H, f.W, IN_CH, solver.stream_ptr()))
 
     def warm_start(self, solver: Solver_B200, stream=None):
         """Predicts lambda for the solver's inputs and sets it as the start.
         Everything runs on the solver's stream (the input and apply kernels
         are the handle's work, ordered there); `stream`, when given, must be
         that stream."""
-        s = shapes_of(solver)
+        s = self.net_shapes(solver)
         hs = solver.stream_ptr()
         if stream is not None and int(stream) != hs:
             raise ValueError("warm_start: stream differs from the solver's stream")
@@ -269,12 +295,13 @@ class WarmStartNet:
             self.torch.cuda.synchronize(self.dev)
         self.input_from(solver, s, self._scale)
         y = self.forward(s, hs)
-        check(lib().qesb_warm_apply(solver._h, _p(y), HEAD_N, _p(self._scale)))
+        apply = lib().qesb_warm_apply if self.res == 1 else lib().qesb_warm_apply_up2
+        check(apply(solver._h, _p(y), HEAD_N, _p(self._scale)))
         return s
 
     # ------------------------------------------------------------------ persistence
     def state(self) -> dict:
-        out = {"channels": np.array(self.CH)}
+        out = {"channels": np.array(self.CH), "res": np.array(self.res)}
         for name, L in self.layers.items():
             out[f"{name}.W"] = L.W.cpu().numpy()
             out[f"{name}.b"] = L.b.cpu().numpy()
@@ -287,7 +314,8 @@ class WarmStartNet:
     @classmethod
     def from_file(cls, path, device=0):
         z = np.load(path)
-        net = cls(device=device, channels=tuple(int(c) for c in z["channels"]))
+        net = cls(device=device, channels=tuple(int(c) for c in z["channels"]),
+                  res=int(z["res"]) if "res" in z.files else 1)
         for name, L in net.layers.items():
             L.W.copy_(net.torch.from_numpy(z[f"{name}.W"]).to(net.dev))
             L.b.copy_(net.torch.from_numpy(z[f"{name}.b"]).to(net.dev))

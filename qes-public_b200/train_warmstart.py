@@ -55,16 +55,27 @@ def generate(net, n, workload, target_iters, threads=8):
     for k, w in enumerate(cities()):
         if solver is None:
             solver = qesb.Solver_B200(w.domain, 0.0)
-            s = ws.shapes_of(solver)
+            s = net.net_shapes(solver)
+            f = ws.shapes_of(solver)
             V = s.V(0)
             X = torch.empty((n, V, 5), dtype=torch.bfloat16, device=net.dev)
             T = torch.empty((n, V), dtype=torch.float32, device=net.dev)
             weight = torch.empty(V, dtype=torch.float32, device=net.dev)
+            if net.res == 2:  # full-resolution target and weight, averaged 2x2x2
+                Tf = torch.empty(f.V(0), dtype=torch.float32, device=net.dev)
+                Wf = torch.empty(f.V(0), dtype=torch.float32, device=net.dev)
+            torch.cuda.synchronize()
         solver.set_inputs(w)
         solver.resetLambda()
         solver.solve(w, target_iters, set_inputs=False)
         net.input_from(solver, s, scale)
-        qesb.check(qesb.lib().qesb_warm_target(solver._h, T[k].data_ptr(), weight.data_ptr(), scale.data_ptr()))
+        if net.res == 1:
+            qesb.check(qesb.lib().qesb_warm_target(solver._h, T[k].data_ptr(), weight.data_ptr(), scale.data_ptr()))
+        else:
+            hs = solver.stream_ptr()
+            qesb.check(qesb.lib().qesb_warm_target(solver._h, Tf.data_ptr(), Wf.data_ptr(), scale.data_ptr()))
+            qesb.check(qesb.lib().qesb_net_pool2_f32(Tf.data_ptr(), T[k].data_ptr(), f.D, f.H, f.W, hs))
+            qesb.check(qesb.lib().qesb_net_pool2_f32(Wf.data_ptr(), weight.data_ptr(), f.D, f.H, f.W, hs))
         torch.cuda.synchronize()  # the input and target kernels ran on the solver's stream
         xb = net._bufs(s)["x"].view(s.V(0), ws.IN_CH)
         X[k].copy_(xb[:, :5])
@@ -150,12 +161,13 @@ def main():
     ap.add_argument("--eval-workload", default="city256")
     ap.add_argument("--levels", type=int, default=4, help="encoder-decoder levels (channels 16, 32, 64, 128, 128, ...)")
     ap.add_argument("--seed", type=int, default=0, help="weight initialisation seed")
+    ap.add_argument("--res", type=int, default=1, help="1: network at full resolution, 2: at half resolution")
     ap.add_argument("--coarse-beta", type=float, default=0.0,
                     help="weight of the 8x8x8-block error term of the loss (0: plain MSE)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
     channels = tuple(min(128, 16 << l) for l in range(args.levels))
-    net = ws.WarmStartNet(device=0, seed=args.seed, channels=channels)
+    net = ws.WarmStartNet(device=0, seed=args.seed, channels=channels, res=args.res)
     t0 = time.time()
     X, T, weight, s = generate(net, args.train, args.train_workload, args.target_iters)
     t_gen = time.time() - t0

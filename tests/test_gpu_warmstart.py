@@ -49,12 +49,17 @@ def _ref_network(net, x, tgt, w, inv_count):
     return y[0, 0].detach().numpy(), float(loss), grads
 
 
-def test_network_forward_and_gradients_match_cpu_oracle():
+@pytest.mark.parametrize("channels,cos_min,rel_max", [((16, 32, 64, 128), 0.99, 0.15),
+                                                     ((16, 32, 64, 128, 128, 128), 0.97, 0.25)])
+def test_network_forward_and_gradients_match_cpu_oracle(channels, cos_min, rel_max):
+    """The shipped 4-level network, and a 6-level one whose deepest weight
+    gradients, carried in BF16 through twelve layers and summed with FP32
+    atomics in any order, sit furthest from the float64 ones."""
     import torch
 
     from qesb import warmstart as ws
 
-    net = ws.WarmStartNet(device=0, seed=1)
+    net = ws.WarmStartNet(device=0, seed=1, channels=channels)
     # larger-than-init head weights so every layer carries a visible gradient
     for L in net.layers.values():
         L.W.mul_(1.5)
@@ -90,26 +95,26 @@ def test_network_forward_and_gradients_match_cpu_oracle():
         rW, rb = gref[name][0], gref[name][1][: L.cout_real]
         cos = float((gW * rW).sum() / (np.linalg.norm(gW) * np.linalg.norm(rW) + 1e-30))
         # gradients are carried in BF16 between layers: the error grows with
-        # depth (the deepest layer of six sees ~10 %), the direction does not
-        assert cos > 0.99, (name, cos)
-        assert np.linalg.norm(gW - rW) <= 0.15 * np.linalg.norm(rW), name
-        assert np.linalg.norm(gb - rb) <= 0.15 * np.linalg.norm(rb) + 1e-6, name
+        # depth, the direction holds
+        assert cos > cos_min, (name, cos)
+        assert np.linalg.norm(gW - rW) <= rel_max * np.linalg.norm(rW), name
+        assert np.linalg.norm(gb - rb) <= rel_max * np.linalg.norm(rb) + 1e-6, name
 
 
 def test_trained_network_gain_on_held_out_cities():
     """The committed trained network on held-out 256x256x64 cities (seeds the
-    training never saw): the reference loop started from its prediction
-    stops after fewer iterations than from lambda = 0 on every seed, and the
-    winds agree with plain SOR's within the stopping rule's accuracy. The
-    gain is small (about 1.02x measured): the prediction's error is mostly
-    smooth (~20 % of lambda), the part of the error plain SOR removes slowest."""
+    training never saw): on average the reference loop started from its
+    prediction stops after fewer iterations than from lambda = 0 (about 1.2x
+    measured on 40 cities; single cities range from a little worse to 1.5x
+    better), and the winds agree with plain SOR's within the stopping rule's
+    accuracy."""
     from qesb import warmstart as ws
 
     if not os.path.exists(ws.DEFAULT_WEIGHTS):
         pytest.skip("no trained weights committed")
     net = ws.WarmStartNet.from_file(ws.DEFAULT_WEIGHTS, device=0)
     gains = []
-    for seed in (900001, 900002):
+    for seed in (900001, 900002, 900003, 900004, 900005, 900006):
         w, _ = qesb.random_city("city256", seed)
         with qesb.Solver_B200(w.domain, 1e-3) as s:
             s.set_inputs(w)
@@ -122,7 +127,7 @@ def test_trained_network_gain_on_held_out_cities():
         assert warm["converged"] and plain["converged"]
         gains.append(plain["iterations"] / warm["iterations"])
         assert np.abs(uw - up).max() < 0.02
-    assert min(gains) > 1.0, gains
+    assert np.mean(gains) > 1.05 and min(gains) > 0.8, gains
 
 
 def test_overrelaxed_prephase_gain_and_accuracy():
@@ -148,3 +153,32 @@ def test_overrelaxed_prephase_gain_and_accuracy():
         assert pre["converged"] and plain["converged"]
         assert 3 * (pre["pre_iterations"] + pre["iterations"]) < plain["iterations"], (pre, plain)
         assert ew < ep, (ew, ep)
+
+
+def test_half_resolution_apply_interpolates_trilinearly():
+    """qesb_warm_apply_up2: a prediction linear in the coarse cell coordinates
+    comes back exactly linear at the fine cell centres (away from the outer
+    half cell, where it is held constant); boundary cells get 0."""
+    import torch
+
+    d = qesb.Domain(20, 16, 12, 1.0, 1.0, 1.0)
+    w = qesb.city_build(d, [], qesb.Inflow(5.0, 10.0, 0.15, 270.0))
+    X, Y, Dn = 20, 16, 12
+    zc, yc, xc = np.meshgrid(np.arange(Dn // 2), np.arange(Y // 2), np.arange(X // 2), indexing="ij")
+    a, bx, by, bz = 0.5, 0.25, -0.125, 0.375
+    yh = (a + bx * (2 * xc + 0.5) + by * (2 * yc + 0.5) + bz * (2 * zc + 0.5)).astype(np.float32)
+    yhd = torch.from_numpy(np.repeat(yh.reshape(-1, 1), 16, axis=1).copy()).cuda()
+    scale = torch.tensor([np.float32(2.0).view(np.int32)], dtype=torch.int32, device="cuda")
+    with qesb.Solver_B200(d, 1e-3) as s:
+        s.set_inputs(w)
+        torch.cuda.synchronize()
+        qesb.check(qesb.lib().qesb_warm_apply_up2(s._h, yhd.data_ptr(), 16, scale.data_ptr()))
+        torch.cuda.synchronize()
+        L = s.lambda_.reshape(Dn + 1, Y, X)
+    for k in range(2, Dn - 1):
+        for j in range(2, Y - 2):
+            for i in range(2, X - 2):
+                want = 2.0 * (a + bx * i + by * j + bz * k)
+                assert abs(L[k, j, i] - want) < 1e-4, (k, j, i, L[k, j, i], want)
+    assert not L[:, 0, :].any() and not L[:, :, 0].any() and not L[Dn].any()
+    np.testing.assert_array_equal(L[0], L[1])

@@ -477,7 +477,7 @@ def run_b200(args):
             traffic = None
 
     # ---- the network alone ---------------------------------------------------------
-    s0 = ws.shapes_of(solvers[0])
+    s0 = net.net_shapes(solvers[0])
     fwd = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     for _ in range(2):
         net.forward(s0, stream.cuda_stream)

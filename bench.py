@@ -61,6 +61,11 @@ WORKLOAD = "city256"
 SEED0 = 500000
 METRIC = "ms to SOR tolerance per domain: learned warm start vs plain SOR, 1 B200"
 BYTES_PER_CELL_ITER = 36  # 6 coefficients + R read (28 B), lambda read + write (8 B)
+# Bytes the packed red/black sweep must move per updated cell and iteration:
+# its colour's lambda read + write (8), the other colour's lambda read (4),
+# R (4) and the wall mask (1).
+MOVED_BYTES_PER_CELL_ITER = 17
+SIZE_ITERS = 300  # iterations per timed solve of the size sweep
 # Over-relaxed pre-phase of the warm start on this grid: omega and its stopping
 # tolerance, picked by a sweep of omega in {1.90 .. 1.98} x tol in {1e-3, 3e-3}
 # on 256x256x64 cities (every seed tried preferred 1.97 / 3e-3; 1.98 stalled
@@ -82,6 +87,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 same-SOR error and divergence checks")
+    ap.add_argument("--no-sizes", action="store_true", help="skip the 400^2 and 800^2 sweep-speed section")
     ap.add_argument("--variant", type=int, default=-1, help="sweep variant for the profiling drivers (-1: autotune)")
     ap.add_argument("--profile-solve", type=int, default=0,
                     help="profiling driver: one solve of this many iterations (tol 0) with --variant, exit")
@@ -282,6 +288,35 @@ def fp64_checks(w, seed, st, lam, winds):
     return out
 
 
+def size_rates(peak, workloads=("city400", "city800")):
+    """Sweep speed at the large single-city configurations: one autotuned
+    solve of SIZE_ITERS iterations (tolerance 0, so every iteration runs)
+    after a warm-up solve, per workload; the SOR time comes from the solve's
+    own device events around its graphs."""
+    import qesb
+
+    out = {}
+    for name in workloads:
+        w, _ = qesb.random_city(name, 0)
+        Nx, Ny, Nz = w.domain.base
+        upd = (Nx - 2) * (Ny - 2) * (Nz - 1)
+        with qesb.Solver_B200(w.domain, 0.0) as s:
+            s.set_inputs(w)
+            variant, _ = s.autotune()
+            per = []
+            for _ in range(3):
+                s.resetLambda()
+                st = s.solve(w, SIZE_ITERS, set_inputs=False)
+                per.append(st["ms_sor"] / st["iterations"])
+        ms_it = statistics.median(per[1:])
+        alg = BYTES_PER_CELL_ITER * upd / (ms_it * 1e-3) / 1e9
+        moved = MOVED_BYTES_PER_CELL_ITER * upd / (ms_it * 1e-3) / 1e9
+        out[name] = {"grid": [Nx, Ny, Nz], "updated_cells": upd, "variant": variant, "iterations": SIZE_ITERS,
+                     "us_per_iteration": 1e3 * ms_it, "algorithmic_gbs": alg, "algorithmic_frac": alg / peak,
+                     "moved_gbs": moved, "moved_frac": moved / peak}
+    return out
+
+
 def network_flops(net, s):
     """Multiply-add FLOPs of one forward pass (2 per MAC, real channels)."""
     total = 0
@@ -320,9 +355,10 @@ def run_b200(args):
     for s, w in zip(solvers, cities):
         s.set_stream(stream.cuda_stream)
         s.set_inputs(w)
-    # autotuner: picks the sweep shape for this grid (untimed set-up, cached for
-    # the process like a library's algorithm search); the batch uses it too
+    # autotuners (untimed set-up, like a library's algorithm search): the sweep
+    # shape for single solves of this grid, and the one for this batch's list
     variant, variant_us = solvers[0].autotune()
+    batch_variant, _ = qesb.autotune_batch(solvers)
     wpath = args.weights or ws.DEFAULT_WEIGHTS
     net = ws.WarmStartNet.from_file(wpath, device=dev)
 
@@ -476,6 +512,24 @@ def run_b200(args):
         except ValueError:
             traffic = None
 
+    # ---- the headline step as a whole: the domain list's sweeps -----------------------
+    # Every domain-iteration of the step (pre-phase and reference loop) moves at
+    # least MOVED_BYTES_PER_CELL_ITER per updated cell; over the whole step time
+    # (R, layout changes and correction included) that is a lower bound on the
+    # sweep kernels' DRAM rate.
+    dom_iters = sum(x["iterations"] + x["pre_iterations"] for x in res_warm[-1])
+    moved = MOVED_BYTES_PER_CELL_ITER * updated * dom_iters / (ms_warm * 1e-3) / 1e9
+    headline_sweep = {"domain_iterations": dom_iters, "us_per_domain_iteration": 1e3 * ms_warm / dom_iters,
+                      "moved_gbs_lower_bound": moved, "moved_frac": moved / peak, "batch_variant": batch_variant}
+
+    # ---- the sweep at the 400^2 x 100 and 800^2 x 128 configurations ------------------
+    sizes = None
+    if not args.no_sizes:
+        try:
+            sizes = size_rates(peak)
+        except Exception as ex:  # noqa: BLE001
+            sizes = {"unavailable": str(ex)[:200]}
+
     # ---- the network alone ---------------------------------------------------------
     s0 = net.net_shapes(solvers[0])
     fwd = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -546,7 +600,8 @@ def run_b200(args):
                                    f"(+{B} per rank)",
                        "batch": B, "tol": TOL, "itermax": ITERMAX, "network": os.path.basename(wpath),
                        "network_levels": net.nlev, "channels": list(net.CH),
-                       "sweep_variant": variant, "parallelism": f"replicas x{world}",
+                       "sweep_variant": variant, "batch_variant": batch_variant,
+                       "parallelism": f"replicas x{world}",
                        "warm_start": f"red-black SOR at omega {PRE_OMEGA} from lambda = 0 to max|dlambda| <= "
                                      f"{PRE_TOL}, then the reference loop (omega 1.78, tol {TOL}); the learned "
                                      f"network's start is measured in arms (network, network+prephase) and is "
@@ -562,10 +617,12 @@ def run_b200(args):
             "speedup_vs_reference_gpu": (ref_gpu["ms"] / ms_first) if ref_gpu and "ms" in ref_gpu else None,
             "e2e": {"value": ms_e2e / B, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "matches_device_result": bool(e2e_ok)},
+            "headline_sweep": headline_sweep,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "kernel": "red+black sweep pair (variant %d), per iteration inside the solve graphs" % variant,
                          "ms_per_iteration": ms_it, "algorithmic_bytes_per_iteration": alg_bytes},
+            "sizes": sizes,
             "network": {"bound": "tensor", "ms_per_forward": ms_fwd, "flops_per_forward": flops,
                         "achieved_tflops": flops / (ms_fwd * 1e-3) / 1e12, "peak_tflops": tpeak,
                         "frac": flops / (ms_fwd * 1e-3) / 1e12 / tpeak},

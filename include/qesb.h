@@ -161,11 +161,23 @@ qesb_status qesb_set_prephase(qesb_handle *h, float omega, float tol, int max_it
 qesb_status qesb_solve_batch(qesb_handle *const *handles, int n, int itermax, float *const *u,
                              float *const *v, float *const *w, qesb_stats *st);
 
+/* Batch autotuner: times every sweep launch shape on the domain list that
+ * qesb_solve_batch would run for these handles (same checks), a few launches
+ * each from the handles' current lambda, and stores the fastest as
+ * handles[0]'s "batch_variant" option, which qesb_solve_batch then uses.
+ * lambda is left unchanged (the sweeps advance the split-layout copy only).
+ * us_per_iter (nullable, n_variants entries) receives each shape's time per
+ * iteration over the whole list, at its variant index (entries below the
+ * first sweep shape are left untouched); *best the chosen index. */
+qesb_status qesb_autotune_batch(qesb_handle *const *handles, int n, int *best, float *us_per_iter, int n_variants);
+
 /* Tolerance (Solver::tol) and tuning knobs. Keys:
  *   "sweeps_per_launch"  iterations fused per sweep launch (0 = autotuned)
  *   "path"               0 = force full coefficients, 1 = allow the packed mask (default)
  *   "graph"              1 = run the iteration loop as a CUDA graph (default), 0 = plain launches
  *   "variant"            sweep variant index (-1 = autotuned / default), see qesb_num_variants
+ *   "batch_variant"      sweep shape for qesb_solve_batch led by this handle (-1 = from "variant");
+ *                        set by qesb_autotune_batch
  *   "autotune"           1 = run qesb_autotune at the first solve of an untuned grid shape (default 0) */
 qesb_status qesb_set_tolerance(qesb_handle *h, float tol);
 qesb_status qesb_set_option(qesb_handle *h, const char *key, int value);

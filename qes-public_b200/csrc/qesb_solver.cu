@@ -39,6 +39,7 @@
 #include "qesb_device.cuh"
 #include "qesb_sor_tiled.cuh"
 #include "qesb_sor_split.cuh"
+#include "qesb_sor_zm.cuh"
 #include "qesb_sor_bulk.cuh"
 
 // ---------------------------------------------------------------------------
@@ -509,14 +510,14 @@ struct SweepList {
   }
   // Uploads the domains (all active) and a fresh control block; returns once
   // the copies are done (the host-side sources may be locals).
-  qesb_status upload(const std::vector<SweepDomain> &doms, bool span, cudaStream_t s)
+  qesb_status upload(const std::vector<SweepDomain> &doms, int unit, cudaStream_t s)
   {
     const int n = (int)doms.size();
     if (n > cap) return qesb_fail(QESB_ERR_ARG, "domain list capacity %d < %d", cap, n);
     std::vector<int> active(n), uoff(n + 1, 0);
     for (int i = 0; i < n; ++i) {
       active[i] = i;
-      uoff[i + 1] = uoff[i] + (span ? doms[i].rows * doms[i].nch : doms[i].rows);
+      uoff[i + 1] = uoff[i] + sweep_units(doms[i], unit);
     }
     const SweepCtl ctl{0u, n, 0, 0, 0ull};
     CK(cudaMemcpyAsync((void *)a.dom, doms.data(), sizeof(SweepDomain) * n, cudaMemcpyHostToDevice, s));
@@ -588,6 +589,7 @@ struct qesb_handle {
   int opt_k = 0;
   int opt_graph = 1;
   int opt_variant = -1;
+  int opt_batch_variant = -1;  // sweep shape for batches led by this handle (qesb_autotune_batch)
   int opt_autotune = 0;
   int last_launches = 0;
 
@@ -872,12 +874,12 @@ qesb_status run_iterations_tiled(qesb_handle *h, const Variant &v, int itermax)
 }
 
 // Red/black sweep launch shapes over domain lists: the streaming split
-// kernels (rows per CTA, cells per lane, row order) and the staged kernels
-// (warps per CTA, stages per warp, copy engine). SPAN: work units are
-// 128-cell row spans (staged kernels) rather than rows.
+// kernels (rows per CTA, cells per lane, row order), the staged kernels
+// (warps per CTA, stages per warp, copy engine) and the z-march kernels
+// (rows per tile). unit: what the domain list counts (SweepUnit).
 struct SweepVariant {
   const char *name;
-  bool span;
+  int unit;
   int block_y;  // warps per CTA
   size_t smem;  // dynamic shared memory per CTA
   void (*red)(SweepArgs);  // single domain (from the kernel parameters)
@@ -891,7 +893,7 @@ template <int RPB, int U, int STRIDED = 0, int MINB = (16 / RPB > 1 ? 16 / RPB :
 constexpr SweepVariant make_split(const char *name)
 {
   return SweepVariant{name,
-                      false,
+                      kUnitRow,
                       RPB,
                       0,
                       k_sor_split<0, RPB, U, STRIDED, false, MINB>,
@@ -903,7 +905,7 @@ template <int RPB, int STRIDED = 0, int MINB = (16 / RPB > 1 ? 16 / RPB : 1)>
 constexpr SweepVariant make_split4(const char *name)
 {
   return SweepVariant{name,
-                      false,
+                      kUnitRow,
                       RPB,
                       0,
                       k_sor_split4<0, RPB, STRIDED, false, MINB>,
@@ -915,13 +917,25 @@ template <int W, int NS, int ASYNC>
 constexpr SweepVariant make_bulk(const char *name)
 {
   return SweepVariant{name,
-                      true,
+                      kUnitSpan,
                       W,
                       bulk_smem_bytes<W, NS>(),
                       k_sor_bulk<0, W, NS, ASYNC, false>,
                       k_sor_bulk<1, W, NS, ASYNC, false>,
                       k_sor_bulk<0, W, NS, ASYNC, true>,
                       k_sor_bulk<1, W, NS, ASYNC, true>};
+}
+template <int TY, int MINB>
+constexpr SweepVariant make_zm(const char *name)
+{
+  return SweepVariant{name,
+                      kUnitTile,
+                      TY,
+                      zm_smem_bytes<TY>(),
+                      k_sor_zm<0, TY, false, MINB>,
+                      k_sor_zm<1, TY, false, MINB>,
+                      k_sor_zm<0, TY, true, MINB>,
+                      k_sor_zm<1, TY, true, MINB>};
 }
 const SweepVariant kSweepVariants[] = {
     // streaming split kernels (option "variant" 5..17)
@@ -940,6 +954,11 @@ const SweepVariant kSweepVariants[] = {
     make_split<4, 4, 1, 6>("split_r4_u4_strided_b6"), make_split<8, 2, 1, 4>("split_r8_u2_strided_b4"),
     make_split4<8, 1, 4>("split4_r8_strided_b4"), make_split4<4, 1, 8>("split4_r4_strided_b8"),
     make_split4<16, 1, 2>("split4_r16_strided_b2"), make_split4<8, 0, 3>("split4_r8_b3"),
+    // window order with an L2 prefetch of each warp's next row (36..39)
+    make_split4<8, 2, 3>("split4_r8_pf_b3"), make_split4<4, 2, 6>("split4_r4_pf_b6"),
+    make_split<4, 4, 2, 6>("split_r4_u4_pf_b6"), make_split4<4, 2, 8>("split4_r4_pf_b8"),
+    // z-march tiles, other colour staged in shared memory (40..43)
+    make_zm<8, 4>("zm_y8"), make_zm<4, 6>("zm_y4_b6"), make_zm<8, 3>("zm_y8_b3"), make_zm<8, 2>("zm_y8_b2"),
 };
 constexpr int kNumSweep = sizeof(kSweepVariants) / sizeof(kSweepVariants[0]);
 constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the first sweep shape
@@ -964,6 +983,31 @@ int sweep_ctas(const SweepVariant &sv, bool multi, int device)
   int per = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, multi ? sv.black_m : sv.black, 32 * sv.block_y, sv.smem);
   return std::max(1, per) * std::max(1, nsm[device & 63]);
+}
+
+// Planes per z-march tile for a list: the kc in [4, 32] that minimises
+// waves x (kc + 2) (the persistent grid's passes over the tiles, each costing
+// its kc planes plus two staged halo planes), the same kc for every domain.
+void sweep_tiles(std::vector<SweepDomain> &doms, const SweepVariant &sv, bool multi, int device)
+{
+  if (sv.unit != kUnitTile) return;
+  const long ctas = sweep_ctas(sv, multi, device);
+  int best = 4;
+  long best_cost = -1;
+  for (int kc = 4; kc <= 32; ++kc) {
+    long tiles = 0;
+    for (SweepDomain &d : doms) {
+      d.tile_y = sv.block_y;
+      d.kc = kc;
+      tiles += sweep_units(d, kUnitTile);
+    }
+    const long cost = (tiles + ctas - 1) / ctas * (kc + 2);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best = kc;
+    }
+  }
+  for (SweepDomain &d : doms) d.kc = best;
 }
 
 SweepDomain sweep_domain(qesb_handle *h, int itermax, double tol)
@@ -1074,11 +1118,12 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
   if (h->pre_omega > 0.0f && h->pre_iters > 0) {
     // over-relaxed pre-phase from the current lambda; its state and error
     // history are then cleared for the reference loop
-    SweepDomain pre;
-    CKS(sweep_domain_pre(h, pre, s));
-    CKS(h->list.upload({pre}, sv.span, s));
+    std::vector<SweepDomain> pre(1);
+    CKS(sweep_domain_pre(h, pre[0], s));
+    sweep_tiles(pre, sv, false, h->device);
+    CKS(h->list.upload(pre, sv.unit, s));
     SweepArgs a = h->list.a;
-    a.one = pre;
+    a.one = pre[0];
     CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, h->pre_iters, h->opt_graph != 0,
                        &h->sgraph_pre, h->h_ctl, &pre_launched));
     CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
@@ -1088,10 +1133,11 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
     CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
     CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
   }
-  const SweepDomain one = sweep_domain(h, itermax, (double)h->tol);
-  CKS(h->list.upload({one}, sv.span, s));
+  std::vector<SweepDomain> one{sweep_domain(h, itermax, (double)h->tol)};
+  sweep_tiles(one, sv, false, h->device);
+  CKS(h->list.upload(one, sv.unit, s));
   SweepArgs a = h->list.a;
-  a.one = one;
+  a.one = one[0];
   CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, itermax, h->opt_graph != 0, &h->sgraph,
                      h->h_ctl, &launched));
   h->last_launches = 2 * (launched + pre_launched);
@@ -1547,11 +1593,12 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
     CKS(ensure_err(h, n + 1));
     cudaStream_t s = h->stream;
     CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
-    const SweepDomain one = sweep_domain(h, 1 << 30, -1.0);  // tol < 0: every launch runs
-    CKS(h->list.upload({one}, sv.span, s));
+    std::vector<SweepDomain> one{sweep_domain(h, 1 << 30, -1.0)};  // tol < 0: every launch runs
+    sweep_tiles(one, sv, false, h->device);
+    CKS(h->list.upload(one, sv.unit, s));
     const dim3 grid(sweep_ctas(sv, false, h->device)), block(32, sv.block_y);
     SweepArgs a = h->list.a;
-    a.one = one;
+    a.one = one[0];
     CK(cudaEventRecord(h->ev[0], s));
     for (int c = 0; c < n; ++c) {
       sv.red<<<grid, block, sv.smem, s>>>(a);
@@ -1633,25 +1680,114 @@ qesb_status qesb_autotune(qesb_handle *h, int *best, float *us_per_iter, int n_v
   return QESB_OK;
 }
 
-qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *const *u, float *const *v,
-                             float *const *w, qesb_stats *st)
+// Checks shared by the batch entry points.
+static qesb_status batch_check(qesb_handle *const *hs, int n, const char *who)
 {
-  if (!hs || n <= 0 || itermax < 0) return qesb_fail(QESB_ERR_ARG, "qesb_solve_batch: bad argument");
+  if (!hs || n <= 0) return qesb_fail(QESB_ERR_ARG, "%s: bad argument", who);
   for (int i = 0; i < n; ++i) {
-    if (!hs[i]) return qesb_fail(QESB_ERR_ARG, "qesb_solve_batch: null handle %d", i);
-    if (!hs[i]->have_inputs) return qesb_fail(QESB_ERR_STATE, "qesb_solve_batch: domain %d has no inputs", i);
+    if (!hs[i]) return qesb_fail(QESB_ERR_ARG, "%s: null handle %d", who, i);
+    if (!hs[i]->have_inputs) return qesb_fail(QESB_ERR_STATE, "%s: domain %d has no inputs", who, i);
     if (!hs[i]->packed || hs[i]->opt_path != 1)
-      return qesb_fail(QESB_ERR_STATE, "qesb_solve_batch: domain %d is not on the packed (stair-step) path", i);
-    if (hs[i]->device != hs[0]->device) return qesb_fail(QESB_ERR_ARG, "qesb_solve_batch: handles on two devices");
+      return qesb_fail(QESB_ERR_STATE, "%s: domain %d is not on the packed (stair-step) path", who, i);
+    if (hs[i]->device != hs[0]->device) return qesb_fail(QESB_ERR_ARG, "%s: handles on two devices", who);
     for (int k = 0; k < i; ++k)
-      if (hs[k] == hs[i]) return qesb_fail(QESB_ERR_ARG, "qesb_solve_batch: handle %d repeated", i);
+      if (hs[k] == hs[i]) return qesb_fail(QESB_ERR_ARG, "%s: handle %d repeated", who, i);
   }
+  return QESB_OK;
+}
+
+qesb_status qesb_autotune_batch(qesb_handle *const *hs, int n, int *best, float *us_per_iter, int n_variants)
+{
+  CKS(batch_check(hs, n, "qesb_autotune_batch"));
   qesb_handle *h0 = hs[0];
   CK(cudaSetDevice(h0->device));
   cudaStream_t s = h0->stream;
-  // launch shape: handles[0]'s "variant" option when it names a sweep shape,
-  // else its grid's autotuned shape when that is one, else the default
-  int vi = h0->opt_variant >= kSplitVariant ? h0->opt_variant : tuned_variant(h0->G);
+  // the domains as a solve would start them: R, and lambda and R in the split
+  // layout (the tuning sweeps advance only the split copy; a solve re-derives
+  // it from lambda)
+  for (int i = 0; i < n; ++i) {
+    qesb_handle *h = hs[i];
+    const DevGrid &G = h->G;
+    k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(
+        G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_u0, h->d_v0, h->d_w0,
+        h->d_dz, h->dx, h->dy, h->d_R);
+    k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam, h->d_lam_s);
+    k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_R, h->d_R_s);
+  }
+  CK(cudaGetLastError());
+  SweepList list;
+  CKS(list.create(n));
+  qesb_status qs = QESB_OK;
+  int arg = -1;
+  float best_us = 0.0f;
+  for (int v = kSplitVariant; v < kAllVariants && qs == QESB_OK; ++v) {
+    const SweepVariant &sv = kSweepVariants[v - kSplitVariant];
+    qs = sweep_prepare(sv);
+    const dim3 grid(sweep_ctas(sv, true, h0->device)), block(32, sv.block_y);
+    float ms = 0.0f;
+    int reps = 2;
+    for (int pass = 0; pass < 3 && qs == QESB_OK; ++pass) {
+      // pass 0 warms up, pass 1 sizes the timed pass 2 to about 8 ms
+      std::vector<SweepDomain> doms(n);
+      for (int i = 0; i < n && qs == QESB_OK; ++i) {
+        qs = ensure_err(hs[i], reps + 1);
+        if (qs != QESB_OK) break;
+        if (cudaMemsetAsync(hs[i]->d_err, 0, sizeof(double) * (reps + 1), s) != cudaSuccess ||
+            cudaMemsetAsync(hs[i]->d_state, 0, sizeof(SolveState), s) != cudaSuccess)
+          qs = qesb_fail(QESB_ERR_CUDA, "qesb_autotune_batch: memset");
+        doms[i] = sweep_domain(hs[i], 1 << 30, -1.0);  // tol < 0: every launch runs
+      }
+      if (qs != QESB_OK) break;
+      sweep_tiles(doms, sv, true, h0->device);
+      qs = list.upload(doms, sv.unit, s);
+      if (qs != QESB_OK) break;
+      cudaEventRecord(h0->ev[0], s);
+      for (int c = 0; c < reps; ++c) {
+        sv.red_m<<<grid, block, sv.smem, s>>>(list.a);
+        sv.black_m<<<grid, block, sv.smem, s>>>(list.a);
+      }
+      cudaEventRecord(h0->ev[1], s);
+      if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(h0->ev[1]) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, h0->ev[0], h0->ev[1]) != cudaSuccess) {
+        qs = qesb_fail(QESB_ERR_CUDA, "qesb_autotune_batch: variant %d launch failed", v);
+        break;
+      }
+      SweepCtl ctl;
+      if (cudaMemcpy(&ctl, list.a.ctl, sizeof ctl, cudaMemcpyDeviceToHost) != cudaSuccess || ctl.fault) {
+        qs = qesb_fail(QESB_ERR_CUDA, "qesb_autotune_batch: variant %d stage wait gave up", v);
+        break;
+      }
+      if (pass == 1) reps = std::max(2, std::min(64, (int)(8.0f / std::max(ms / reps, 1e-3f))));
+    }
+    if (qs != QESB_OK) break;
+    const float us = 1000.0f * ms / reps;
+    if (us_per_iter && v < n_variants) us_per_iter[v] = us;
+    if (arg < 0 || us < best_us) {
+      arg = v;
+      best_us = us;
+    }
+  }
+  list.destroy();
+  if (qs != QESB_OK) return qs;
+  h0->opt_batch_variant = arg;
+  if (best) *best = arg;
+  return QESB_OK;
+}
+
+qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *const *u, float *const *v,
+                             float *const *w, qesb_stats *st)
+{
+  if (itermax < 0) return qesb_fail(QESB_ERR_ARG, "qesb_solve_batch: bad argument");
+  CKS(batch_check(hs, n, "qesb_solve_batch"));
+  qesb_handle *h0 = hs[0];
+  CK(cudaSetDevice(h0->device));
+  cudaStream_t s = h0->stream;
+  // launch shape: handles[0]'s "batch_variant" option (qesb_autotune_batch),
+  // else its "variant" option when it names a sweep shape, else its grid's
+  // autotuned shape when that is one, else the default
+  int vi = h0->opt_batch_variant >= kSplitVariant ? h0->opt_batch_variant
+           : h0->opt_variant >= kSplitVariant    ? h0->opt_variant
+                                                 : tuned_variant(h0->G);
   if (vi < kSplitVariant) vi = kSplitVariant + kDefaultSweep;
   const SweepVariant &sv = kSweepVariants[vi - kSplitVariant];
   CK(cudaEventRecord(h0->ev[0], s));
@@ -1689,7 +1825,8 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   int launched = 0, pre_launched = 0;
   if (!pre.empty()) {
     // the over-relaxed pre-phase of the domains that have one, as a list of its own
-    qs = list.upload(pre, sv.span, s);
+    sweep_tiles(pre, sv, true, h0->device);
+    qs = list.upload(pre, sv.unit, s);
     SweepGraph gx;
     int pre_max = 0;
     for (int i : pre_of) pre_max = std::max(pre_max, hs[i]->pre_iters);
@@ -1708,7 +1845,8 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
       CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
     }
   }
-  if (qs == QESB_OK) qs = list.upload(doms, sv.span, s);
+  sweep_tiles(doms, sv, true, h0->device);
+  if (qs == QESB_OK) qs = list.upload(doms, sv.unit, s);
   if (qs == QESB_OK) {
     k_sweep_stamp<<<1, 1, 0, s>>>(list.a.ctl);
     SweepGraph gx;
@@ -1799,6 +1937,11 @@ qesb_status qesb_set_option(qesb_handle *h, const char *key, int value)
     if (value < -1 || value >= kAllVariants)
       return qesb_fail(QESB_ERR_ARG, "variant must be in [-1, %d)", kAllVariants);
     h->opt_variant = value;
+  } else if (k == "batch_variant") {
+    if (value != -1 && (value < kSplitVariant || value >= kAllVariants))
+      return qesb_fail(QESB_ERR_ARG, "batch_variant must be -1 or a sweep variant in [%d, %d)", kSplitVariant,
+                       kAllVariants);
+    h->opt_batch_variant = value;
   } else {
     return qesb_fail(QESB_ERR_ARG, "unknown option '%s'", key);
   }

@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(32 * W) k_sor_bulk(BulkArgs b)
 #pragma unroll
     for (int t4 = 0; t4 < 4; ++t4) {
       nv[t4] = up[t4] ? nv[t4] : ov[t4];
-      big |= up[t4] && !(fabsf(nv[t4] - ov[t4]) < dmax_f);
+      big |= up[t4] && !(fabsf(nv[t4] - ov[t4]) < dmax_f) && nv[t4] != ov[t4];
     }
     const long rowo = ((long)k * cY + j) * cPQ;
     if (p < n) *reinterpret_cast<float4 *>(cL + COLOUR * cCS + rowo + q) = make_float4(nv[0], nv[1], nv[2], nv[3]);
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(32 * W) k_sor_bulk(BulkArgs b)
   if (ASYNC) lane_wait<0>();
   sweep_flush_end<MULTI>(dmax, MULTI ? (cerr ? cerr + cit : nullptr) : b.one.err + b.one.st->it);
 
-  if (COLOUR == 1) sweep_finish_black<true, MULTI>(b, na);
+  if (COLOUR == 1) sweep_finish_black<kUnitSpan, MULTI>(b, na);
 }
 
 }  // namespace qesb

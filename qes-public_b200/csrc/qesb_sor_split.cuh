@@ -96,11 +96,37 @@ struct SplitDom {
   // err[] is poll-read only after every CTA's flushes (last-CTA protocol).
 };
 
+// Hint to the TMA engine: bring `bytes` (a multiple of 16, 16-byte aligned
+// address) into L2. No completion to wait for and no shared memory.
+__device__ __forceinline__ void l2_prefetch_bulk(const void *p, unsigned bytes)
+{
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// L2 prefetch of the streams a half-sweep of colour `colour` first touches on
+// row (j, k): its own lambda, R and mask rows, and the other colour's row
+// k + 1 (rows k and k - 1 of the other colour were the z+1 neighbours of
+// earlier rows in window order). Rows start on 128-byte boundaries (PQ is a
+// multiple of 32), so every address and size is a multiple of 16 bytes; k + 1
+// is at most Z - 1, inside the colour array.
+__device__ __forceinline__ void split_prefetch_row(const SplitDom &D, int colour, int j, int k)
+{
+  const long own = colour * D.CS + ((long)k * D.Y + j) * D.PQ;
+  const long zp = (1 - colour) * D.CS + ((long)(k + 1) * D.Y + j) * D.PQ;
+  const unsigned nb = 4u * (unsigned)D.PQ;
+  l2_prefetch_bulk(D.L + own, nb);
+  l2_prefetch_bulk(D.R + own, nb);
+  l2_prefetch_bulk(D.mask + own, (unsigned)D.PQ);
+  l2_prefetch_bulk(D.L + zp, nb);
+}
+
 // Walks the rows r of the warp's share of the flattened active-row space,
 // switching domain (and flushing the error) when r leaves the current one.
-// Calls body(D, j, k) for each row.
+// Calls body(D, j, k) for each row. STRIDED = 2 is window order with an L2
+// prefetch, before each row, of the warp's next row (one window ahead), so
+// each SM keeps far more DRAM bytes in flight than its loads in registers.
 template <int RPB, int STRIDED, bool MULTI, class Body>
-__device__ __forceinline__ void split_rows(const SweepArgs &b, int na, SplitDom &D, Body body)
+__device__ __forceinline__ void split_rows(const SweepArgs &b, int na, SplitDom &D, Body body, int colour)
 {
   const int lane = threadIdx.x;
   const int nrows = MULTI ? b.uoff[na] : b.one.rows;
@@ -128,6 +154,10 @@ __device__ __forceinline__ void split_rows(const SweepArgs &b, int na, SplitDom 
     }
     const int local = r - lo;
     const int k = 1 + local / (D.Y - 2), j = 1 + local % (D.Y - 2);
+    if (STRIDED == 2 && lane == 0 && r + r_step < (MULTI ? min(r_end, hi) : r_end)) {
+      const int l2 = local + r_step;
+      split_prefetch_row(D, colour, 1 + l2 % (D.Y - 2), 1 + l2 / (D.Y - 2));
+    }
     D.layer(k);
     body(j, k);
   }
@@ -237,7 +267,7 @@ __global__ void __launch_bounds__(32 * RPB, MINB) k_sor_split(SweepArgs b)
       for (int u = 0; u < U; ++u) {
         if (live[u]) {
           pw[q0b + 32 * u] = nv[u];
-          big |= !(fabsf(nv[u] - old[u]) < D.dmax_f);
+          big |= !(fabsf(nv[u] - old[u]) < D.dmax_f) && nv[u] != old[u];
         }
       }
       if (__any_sync(0xffffffffu, big)) {
@@ -257,9 +287,9 @@ __global__ void __launch_bounds__(32 * RPB, MINB) k_sor_split(SweepArgs b)
     for (; q0 + lane_off + 32 * (U - 1) <= qhi; q0 += 32 * U) batch(q0, std::false_type{});
     if (q0 - lane <= qhi) batch(q0, std::true_type{});
     if (COLOUR == 1 && k == 1) split_mirror_row(D, j, lane);
-  });
+  }, COLOUR);
   sweep_flush_end<MULTI>(D.dmax, MULTI ? (D.err ? D.err + D.it : nullptr) : b.one.err + b.one.st->it);
-  if (COLOUR == 1) sweep_finish_black<false, MULTI>(b, na);
+  if (COLOUR == 1) sweep_finish_black<kUnitRow, MULTI>(b, na);
 }
 
 // Vectorised variant of k_sor_split: each lane updates four consecutive
@@ -355,7 +385,7 @@ __global__ void __launch_bounds__(32 * RPB, MINB) k_sor_split4(SweepArgs b)
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         nv[t] = up[t] ? nv[t] : ov[t];
-        big |= up[t] && !(fabsf(nv[t] - ov[t]) < D.dmax_f);
+        big |= up[t] && !(fabsf(nv[t] - ov[t]) < D.dmax_f) && nv[t] != ov[t];
       }
       if (live) *reinterpret_cast<float4 *>(pw + q) = make_float4(nv[0], nv[1], nv[2], nv[3]);
       if (__any_sync(0xffffffffu, big)) {
@@ -369,9 +399,9 @@ __global__ void __launch_bounds__(32 * RPB, MINB) k_sor_split4(SweepArgs b)
       }
     }
     if (COLOUR == 1 && k == 1) split_mirror_row(D, j, lane);
-  });
+  }, COLOUR);
   sweep_flush_end<MULTI>(D.dmax, MULTI ? (D.err ? D.err + D.it : nullptr) : b.one.err + b.one.st->it);
-  if (COLOUR == 1) sweep_finish_black<false, MULTI>(b, na);
+  if (COLOUR == 1) sweep_finish_black<kUnitRow, MULTI>(b, na);
 }
 
 // Plane-0 boundary ring (j = 0, Y-1 rows; i = 0, X-1 columns) <- plane 1.

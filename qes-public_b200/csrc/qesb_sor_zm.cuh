@@ -1,0 +1,300 @@
+// Red/black half-sweeps that march in z over tiles of the split layout, with
+// the other colour staged once through shared memory (a 2.5D stencil).
+//
+// A work unit (tile) is 128 cells of a colour row (q in [q0, q0 + 128)),
+// TY rows (j in [j0, j0 + TY)) and kc planes (k in [k0, k0 + kc)) of one
+// domain. The CTA has TY warps; warp w updates row j0 + w, lane l the cells
+// q0 + 4l .. q0 + 4l + 3, one plane after the other. Per plane the CTA stages,
+// with 16-byte cp.async copies (zero-filled outside the arrays' rows):
+//   - the other colour's plane k + 1 over rows j0 - 1 .. j0 + TY and
+//     q0 - 4 .. q0 + 131 (the y and x halos), into a ring of five planes, so
+//     planes k - 1, k, k + 1 are resident when plane k is updated;
+//   - the own colour's lambda, R and wall mask of plane k, into a ring of three.
+// Copies run two planes ahead of the update. Every neighbour then comes from
+// shared memory: each byte of the other colour leaves L2 about once per tile
+// (plus the halos), against five times in the row kernels.
+//
+// The arithmetic is the row kernels' (Solver_CPU_RB.cpp:118-125, with the
+// same operation order), so the results are bit-identical; the black kernel
+// applies the ground mirror (Solver_CPU_RB.cpp:155-162) on plane 1 and its
+// last CTA runs the convergence poll (qesb_sweep.cuh).
+#pragma once
+#include "qesb_device.cuh"
+#include "qesb_sor_split.cuh"
+#include "qesb_sweep.cuh"
+#include "qesb_umma.cuh"
+
+namespace qesb {
+
+constexpr int kZmQ = 128;            // colour cells per tile row
+constexpr int kZmOW = kZmQ + 8;      // staged other-colour row: q0 - 4 .. q0 + 131
+constexpr int kZmOtherSlots = 5;     // planes k - 1 .. k + 3
+constexpr int kZmOwnSlots = 3;       // planes k .. k + 2
+
+template <int TY>
+constexpr size_t zm_smem_bytes()
+{
+  return sizeof(float) * kZmOtherSlots * (TY + 2) * kZmOW + kZmOwnSlots * TY * kZmQ * (2 * sizeof(float) + 1);
+}
+
+// 16-byte asynchronous copy global -> shared; src_bytes = 0 fills zeros and
+// reads nothing.
+__device__ __forceinline__ void zm_cp16(void *dst, const void *src, int src_bytes)
+{
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(umma::smem_u32(dst)), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void zm_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void zm_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void zm_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <int TY>
+struct ZmSmem {
+  float *oth;     // [kZmOtherSlots][TY + 2][kZmOW]
+  float *own;     // [kZmOwnSlots][TY][kZmQ]
+  float *rr;      // [kZmOwnSlots][TY][kZmQ]
+  uint8_t *mask;  // [kZmOwnSlots][TY][kZmQ]
+  __device__ ZmSmem(unsigned char *base)
+  {
+    oth = reinterpret_cast<float *>(base);
+    own = oth + kZmOtherSlots * (TY + 2) * kZmOW;
+    rr = own + kZmOwnSlots * TY * kZmQ;
+    mask = reinterpret_cast<uint8_t *>(rr + kZmOwnSlots * TY * kZmQ);
+  }
+};
+
+// A thread's share of a tile's staging, fixed for the tile: shared-memory
+// offsets within a slot and global offsets within a colour plane (valid ones
+// only; the others zero-fill). Each plane then costs a few adds per copy.
+template <int TY>
+struct ZmCopies {
+  static constexpr int NCH = kZmOW / 4;                   // 16-byte chunks per staged row
+  static constexpr int NOTH = (TY + 2) * NCH;             // other-colour chunks per plane
+  static constexpr int NT = 32 * TY;                      // threads
+  static constexpr int NO = (NOTH + NT - 1) / NT;         // other-colour chunks per thread
+  int os[NO], og[NO];  // other colour: slot offset (floats), plane offset (floats; -1: zero-fill)
+  int ls, lg;          // own lambda and R: one chunk per thread
+  int ms, mg;          // own mask: threads tid < TY * 8 (ms < 0: none)
+
+  __device__ __forceinline__ void init(const SplitDom &D, int j0, int q0, int tid)
+  {
+#pragma unroll
+    for (int t = 0; t < NO; ++t) {
+      const int c = tid + t * NT;
+      const int r = c / NCH, col = c - r * NCH;
+      const int j = j0 - 1 + r, q = q0 - 4 + 4 * col;
+      os[t] = c < NOTH ? r * kZmOW + 4 * col : -1;
+      og[t] = (c < NOTH && j < D.Y && q >= 0 && q < D.PQ) ? j * D.PQ + q : -1;
+    }
+    {
+      const int r = tid >> 5, col = tid & 31;
+      const int j = j0 + r, q = q0 + 4 * col;
+      ls = r * kZmQ + 4 * col;
+      lg = (j <= D.Y - 2 && q < D.PQ) ? j * D.PQ + q : -1;
+    }
+    {
+      const int r = tid >> 3, col = tid & 7;
+      const int j = j0 + r, q = q0 + 16 * col;
+      ms = tid < TY * 8 ? r * kZmQ + 16 * col : -1;
+      mg = (tid < TY * 8 && j <= D.Y - 2 && q < D.PQ) ? j * D.PQ + q : -1;
+    }
+  }
+};
+
+// Stage the other colour's plane p into other-colour slot `slot`.
+template <int COLOUR, int TY>
+__device__ __forceinline__ void zm_stage_other(const ZmSmem<TY> &sm, const ZmCopies<TY> &cp, const SplitDom &D,
+                                               int p, int slot)
+{
+  float *dst = sm.oth + slot * (TY + 2) * kZmOW;
+  const float *src = D.L + (1 - COLOUR) * D.CS + (long)p * D.Y * D.PQ;
+#pragma unroll
+  for (int t = 0; t < ZmCopies<TY>::NO; ++t)
+    if (cp.os[t] >= 0) zm_cp16(dst + cp.os[t], cp.og[t] >= 0 ? src + cp.og[t] : D.L, cp.og[t] >= 0 ? 16 : 0);
+}
+
+// Stage the own colour's lambda, R and mask of plane p into own slot `slot`.
+template <int COLOUR, int TY>
+__device__ __forceinline__ void zm_stage_own(const ZmSmem<TY> &sm, const ZmCopies<TY> &cp, const SplitDom &D, int p,
+                                             int slot)
+{
+  const long base = COLOUR * D.CS + (long)p * D.Y * D.PQ;
+  const int n = cp.lg >= 0 ? 16 : 0;
+  const long g = base + (cp.lg >= 0 ? cp.lg : 0);
+  zm_cp16(sm.own + slot * TY * kZmQ + cp.ls, D.L + g, n);
+  zm_cp16(sm.rr + slot * TY * kZmQ + cp.ls, D.R + g, n);
+  if (cp.ms >= 0)
+    zm_cp16(sm.mask + slot * TY * kZmQ + cp.ms, D.mask + base + (cp.mg >= 0 ? cp.mg : 0), cp.mg >= 0 ? 16 : 0);
+}
+
+// One pipeline step's copies: the other colour's plane p + 1 and the own
+// colour's plane p (p < k1), as one copy group (empty past the tile's end).
+template <int COLOUR, int TY>
+__device__ __forceinline__ void zm_stage(const ZmSmem<TY> &sm, const ZmCopies<TY> &cp, const SplitDom &D, int p,
+                                         int k1, int oslot, int wslot)
+{
+  if (p < k1) {
+    zm_stage_other<COLOUR, TY>(sm, cp, D, p + 1, oslot);
+    zm_stage_own<COLOUR, TY>(sm, cp, D, p, wslot);
+  }
+  zm_commit();
+}
+
+__device__ __forceinline__ int zm_wrap5(int x) { return x >= 5 ? x - 5 : x; }
+__device__ __forceinline__ int zm_wrap3(int x) { return x >= 3 ? x - 3 : x; }
+
+template <int COLOUR, int TY, bool MULTI, int MINB>
+__global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
+{
+  const int na = b.ctl->nactive;
+  if (na <= 0) return;
+  extern __shared__ __align__(16) unsigned char zm_raw[];
+  const ZmSmem<TY> sm(zm_raw);
+  const int lane = threadIdx.x, w = threadIdx.y, tid = lane + 32 * w;
+  const int total = MULTI ? b.uoff[na] : sweep_units(b.one, kUnitTile);
+  SplitDom D;
+  int slot = -1, lo = 0, hi = 0;
+  for (int u = blockIdx.x; u < total; u += gridDim.x) {
+    if (!MULTI) {
+      if (slot < 0) {
+        slot = 0;
+        hi = total;
+        D.load(b.one);
+      }
+    } else if (slot < 0 || u >= hi) {
+      if (slot >= 0) D.flush(lane);
+      slot = sweep_slot(b.uoff, na, u);
+      lo = b.uoff[slot];
+      hi = b.uoff[slot + 1];
+      D.load(sweep_dom<MULTI>(b, slot));
+    }
+    const SweepDomain &SD = sweep_dom<MULTI>(b, slot);
+    const int njt = (D.Y - 2 + TY - 1) / TY, kc = SD.kc;
+    const int nch = SD.nch;
+    int t = u - lo;
+    const int qt = t % nch;
+    t /= nch;
+    const int jt = t % njt, kt = t / njt;
+    const int q0 = qt * kZmQ, j0 = 1 + jt * TY, k0 = 1 + kt * kc;
+    const int k1 = min(k0 + kc, D.Z - 1);
+    const int j = j0 + w, q = q0 + 4 * lane;
+    const bool row_ok = j <= D.Y - 2;
+    const int qn = (D.X + 1) >> 1;
+    ZmCopies<TY> cp;
+    cp.init(D, j0, q0, tid);
+
+    // Ring slots restart with each tile: the other colour's plane k0 - 1 + s
+    // sits in slot s mod 5, the own colour's plane k0 + s in slot s mod 3.
+    // Prologue: other planes k0 - 1, k0 (and k0 + 1 with own k0) as one
+    // group, then the step of plane k0 + 1.
+    zm_stage_other<COLOUR, TY>(sm, cp, D, k0 - 1, 0);
+    zm_stage_other<COLOUR, TY>(sm, cp, D, k0, 1);
+    zm_stage<COLOUR, TY>(sm, cp, D, k0, k1, 2, 0);
+    zm_stage<COLOUR, TY>(sm, cp, D, k0 + 1, k1, 3, 1);
+    int om1 = 0, wk = 0;  // slots of the other colour's plane k - 1 and the own colour's plane k
+    for (int k = k0; k < k1; ++k, om1 = zm_wrap5(om1 + 1), wk = zm_wrap3(wk + 1)) {
+      zm_wait1();        // this thread's copies of plane k's step have landed
+      __syncthreads();   // everyone's; and every warp is done with plane k - 1
+      zm_stage<COLOUR, TY>(sm, cp, D, k + 2, k1, zm_wrap5(om1 + 4), zm_wrap3(wk + 2));
+      D.layer(k);
+      if (row_ok) {
+        // Every lane computes (the staged rows are 128 cells wide, zero-filled
+        // past PQ); only cells inside [qlo, qhi] are updated and stored.
+        const int i0 = (COLOUR + j + k) & 1;
+        const int qlo = i0 ? 0 : 1;
+        const int qhi = (D.X - 2 - i0) >> 1;  // inclusive
+        const float *om = sm.oth + om1 * (TY + 2) * kZmOW;
+        const float *ok = sm.oth + zm_wrap5(om1 + 1) * (TY + 2) * kZmOW;
+        const float *op = sm.oth + zm_wrap5(om1 + 2) * (TY + 2) * kZmOW;
+        const int c = 4 + 4 * lane;  // column of q in a staged other-colour row
+        const int so = wk * TY * kZmQ + w * kZmQ + 4 * lane;
+        const float4 o = *reinterpret_cast<const float4 *>(sm.own + so);
+        const float4 rr = *reinterpret_cast<const float4 *>(sm.rr + so);
+        const uint32_t m4 = *reinterpret_cast<const uint32_t *>(sm.mask + so);
+        const float4 xc = *reinterpret_cast<const float4 *>(ok + (w + 1) * kZmOW + c);
+        const float4 ym = *reinterpret_cast<const float4 *>(ok + w * kZmOW + c);
+        const float4 yp = *reinterpret_cast<const float4 *>(ok + (w + 2) * kZmOW + c);
+        const float4 zm = *reinterpret_cast<const float4 *>(om + (w + 1) * kZmOW + c);
+        const float4 zp = *reinterpret_cast<const float4 *>(op + (w + 1) * kZmOW + c);
+        // value across the group edge: other[q - 1] (i0 = 0) or other[q + 4] (i0 = 1)
+        const float edge = ok[(w + 1) * kZmOW + (i0 ? c + 4 : c - 1)];
+        const float xm0 = i0 ? xc.x : edge, xm1 = i0 ? xc.y : xc.x, xm2 = i0 ? xc.z : xc.y,
+                    xm3 = i0 ? xc.w : xc.z;
+        const float xp0 = i0 ? xc.y : xc.x, xp1 = i0 ? xc.z : xc.y, xp2 = i0 ? xc.w : xc.z,
+                    xp3 = i0 ? edge : xc.w;
+        bool up[4];
+#pragma unroll
+        for (int t4 = 0; t4 < 4; ++t4) up[t4] = q + t4 >= qlo && q + t4 <= qhi;
+        const unsigned mk[4] = {m4 & 0xffu, (m4 >> 8) & 0xffu, (m4 >> 16) & 0xffu, m4 >> 24};
+        bool full = true;
+#pragma unroll
+        for (int t4 = 0; t4 < 4; ++t4) full &= (!up[t4] || mk[t4] == 63u);
+        const float ov[4] = {o.x, o.y, o.z, o.w};
+        const float xmv[4] = {xm0, xm1, xm2, xm3}, xpv[4] = {xp0, xp1, xp2, xp3};
+        const float ymv[4] = {ym.x, ym.y, ym.z, ym.w}, ypv[4] = {yp.x, yp.y, yp.z, yp.w};
+        const float zmv[4] = {zm.x, zm.y, zm.z, zm.w}, zpv[4] = {zp.x, zp.y, zp.z, zp.w};
+        const float rv[4] = {rr.x, rr.y, rr.z, rr.w};
+        float nv[4];
+        if (__all_sync(0xffffffffu, full)) {
+#pragma unroll
+          for (int t4 = 0; t4 < 4; ++t4)
+            nv[t4] = D.inv63 * (D.ve * xpv[t4] + D.vf * xmv[t4] + D.vg * ypv[t4] + D.vh * ymv[t4] +
+                                D.vm * zpv[t4] + D.vn * zmv[t4] - rv[t4]) +
+                     D.c1 * ov[t4];
+        } else {
+#pragma unroll
+          for (int t4 = 0; t4 < 4; ++t4) {
+            const unsigned m_ = up[t4] ? mk[t4] : 63u;
+            const float e = (m_ & 1u) ? D.ve : 0.0f, f = (m_ & 2u) ? D.vf : 0.0f;
+            const float g = (m_ & 4u) ? D.vg : 0.0f, hh = (m_ & 8u) ? D.vh : 0.0f;
+            const float m = (m_ & 16u) ? D.vm : 0.0f, n = (m_ & 32u) ? D.vn : 0.0f;
+            nv[t4] = __ldg(D.inv + m_) * (e * xpv[t4] + f * xmv[t4] + g * ypv[t4] + hh * ymv[t4] +
+                                          m * zpv[t4] + n * zmv[t4] - rv[t4]) +
+                     D.c1 * ov[t4];
+          }
+        }
+        bool big = false;
+#pragma unroll
+        for (int t4 = 0; t4 < 4; ++t4) {
+          nv[t4] = up[t4] ? nv[t4] : ov[t4];
+          // a cell whose value did not change cannot raise the maximum
+          big |= up[t4] && !(fabsf(nv[t4] - ov[t4]) < D.dmax_f) && nv[t4] != ov[t4];
+        }
+        if (q <= qhi) {
+          float *pw = D.L + COLOUR * D.CS + ((long)k * D.Y + j) * D.PQ + q;
+          *reinterpret_cast<float4 *>(pw) = make_float4(nv[0], nv[1], nv[2], nv[3]);
+        }
+        if (COLOUR == 1 && k == 1) {
+          // ground mirror of this lane's cells: red (i, j, 0) <- black (i, j, 1),
+          // black (i, j, 0) <- red (i, j, 1), for q < qn
+          float *r0 = D.L + (long)j * D.PQ;
+          float *b0 = D.L + D.CS + (long)j * D.PQ;
+          const float xv[4] = {xc.x, xc.y, xc.z, xc.w};
+#pragma unroll
+          for (int t4 = 0; t4 < 4; ++t4)
+            if (q + t4 < qn) {
+              r0[q + t4] = nv[t4];
+              b0[q + t4] = xv[t4];
+            }
+        }
+        // the warp's running max |dlambda|, FP64-exact as in the row kernels
+        if (__any_sync(0xffffffffu, big)) {
+#pragma unroll
+          for (int t4 = 0; t4 < 4; ++t4) {
+            const double d = fabs((double)nv[t4] - (double)ov[t4]);
+            if (up[t4] && (d > D.dmax || d != d)) D.dmax = d;
+          }
+          D.dmax = warp_max_d(D.dmax);
+          D.dmax_f = __double2float_rd(D.dmax);
+        }
+      }
+    }
+    zm_wait0();
+    __syncthreads();  // the ring is reused by the next tile
+  }
+  sweep_flush_end<MULTI>(D.dmax, MULTI ? (D.err ? D.err + D.it : nullptr) : b.one.err + b.one.st->it);
+  if (COLOUR == 1) sweep_finish_black<kUnitTile, MULTI>(b, na);
+}
+
+}  // namespace qesb

@@ -1,7 +1,7 @@
 // Domain lists for the red/black half-sweep kernels: one solve is a list of
 // one domain, a batched solve (qesb_solve_batch) a list of many. The sweep
-// kernels spread the work units (rows, or 128-cell row spans) of the
-// unfinished domains over a persistent grid; the last CTA of each black
+// kernels spread the work units (rows, 128-cell row spans, or z-march tiles)
+// of the unfinished domains over a persistent grid; the last CTA of each black
 // launch polls every unfinished domain (the loop condition of
 // Solver_CPU_RB.cpp:106, with max|dlambda| in FP64) and compacts the list,
 // so finished domains drop out of the next launch without a host round trip.
@@ -16,6 +16,8 @@ struct SweepDomain {
   long CS;
   int nch;    // 128-cell spans per colour row: ceil(PQ / 128)
   int rows;   // (Y - 2) * (Z - 2) updated rows per colour
+  int tile_y; // z-march tiles: rows per tile (the kernel's warps per CTA)
+  int kc;     // z-march tiles: planes per tile
   float *lam;           // [2][CS]
   const float *R;       // [2][CS]
   const uint8_t *mask;  // [2][CS]
@@ -72,18 +74,22 @@ __device__ __forceinline__ void poll_one(SolveState *st, const double *err, doub
   }
 }
 
-// Work units of a domain for a kernel family: rows (SPAN = false) or
-// 128-cell row spans (SPAN = true).
-template <bool SPAN>
-__device__ __forceinline__ int sweep_units(const SweepDomain &D)
+// Kinds of work unit: a row, a 128-cell row span, or a z-march tile
+// (128 cells of a colour row x tile_y rows x kc planes).
+enum SweepUnit { kUnitRow = 0, kUnitSpan = 1, kUnitTile = 2 };
+
+// Work units of a domain for a kernel family.
+__host__ __device__ __forceinline__ int sweep_units(const SweepDomain &D, int unit)
 {
-  return SPAN ? D.rows * D.nch : D.rows;
+  if (unit == kUnitSpan) return D.rows * D.nch;
+  if (unit == kUnitTile) return D.nch * ((D.Y - 2 + D.tile_y - 1) / D.tile_y) * ((D.Z - 2 + D.kc - 1) / D.kc);
+  return D.rows;
 }
 
 // End of a black launch. Every thread of the CTA calls it after its own error
 // flushes; the last CTA to arrive polls the unfinished domains and rebuilds
 // the active list and unit offsets for the next launch.
-template <bool SPAN, bool MULTI>
+template <int UNIT, bool MULTI>
 __device__ __forceinline__ void sweep_finish_black(const SweepArgs &b, int na)
 {
   __syncthreads();
@@ -117,7 +123,7 @@ __device__ __forceinline__ void sweep_finish_black(const SweepArgs &b, int na)
       poll_one(D.st, D.err, D.tol, D.itermax);
       keep = !D.st->done;
       if (!keep) D.st->t_done = global_ns();
-      units = sweep_units<SPAN>(D);
+      units = sweep_units(D, UNIT);
     }
     __syncwarp();
     const unsigned mball = __ballot_sync(0xffffffffu, keep);

@@ -109,6 +109,8 @@ def lib() -> C.CDLL:
             "qesb_autotune": ([V, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int], C.c_int),
             "qesb_solve_batch": ([C.POINTER(V), C.c_int, C.c_int, C.POINTER(V), C.POINTER(V), C.POINTER(V),
                                   C.POINTER(Stats)], C.c_int),
+            "qesb_autotune_batch": ([C.POINTER(V), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int],
+                                    C.c_int),
             "qesb_num_variants": ([], C.c_int),
             "qesb_set_option": ([V, C.c_char_p, C.c_int], C.c_int),
             "qesb_set_stream": ([V, V], C.c_int),
@@ -378,6 +380,22 @@ class Solver_B200:
         out = np.empty(self.domain.numCellCentered(), dtype=np.float32)
         check(lib().qesb_get_divergence(self._h, _ptr(out)))
         return out
+
+
+def autotune_batch(solvers) -> tuple[int, list[float]]:
+    """qesb_autotune_batch: times every sweep launch shape on the domain list
+    qesb_solve_batch would run for these solvers (inputs set), keeps the
+    fastest as solvers[0]'s "batch_variant" option, and returns it with each
+    shape's microseconds per iteration over the list (0 for the fused tile
+    shapes, which batches do not use)."""
+    n = len(solvers)
+    V = C.c_void_p
+    hs = (V * n)(*[s._h for s in solvers])
+    nv = lib().qesb_num_variants()
+    us = (C.c_float * nv)()
+    best = C.c_int()
+    check(lib().qesb_autotune_batch(hs, n, C.byref(best), us, nv))
+    return best.value, list(us)
 
 
 def solve_batch(solvers, itermax: int, u_ptrs=None, v_ptrs=None, w_ptrs=None) -> list[dict]:

@@ -41,7 +41,7 @@ def _batch(ws, tol, itermax, lam0s, variant=-1):
             s.close()
 
 
-@pytest.mark.parametrize("variant", [-1, 18, 21, 23, 26])
+@pytest.mark.parametrize("variant", [-1, 18, 21, 23, 26, 40, 41, 42])
 def test_batch_matches_oracle_per_domain(variant):
     ws = _cities()
     rng = np.random.default_rng(11)
@@ -117,3 +117,39 @@ def test_batch_prephase_per_domain():
         assert sti["iterations"] == it
         np.testing.assert_array_equal(L, Lo)
     torch.cuda.synchronize()
+
+
+def test_batch_autotune_keeps_lambda_and_results_exact():
+    """qesb_autotune_batch times the sweep shapes on the batch's own domain
+    list, leaves every lambda as it was, and the batch it tunes still gives
+    the oracle's bits."""
+    import torch
+
+    ws = _cities()
+    rng = np.random.default_rng(5)
+    lam0s = [rng.standard_normal(w.domain.numCellCentered()).astype(np.float32) for w in ws]
+    solvers = [qesb.Solver_B200(w.domain, 1.1e-3) for w in ws]
+    try:
+        for s, w, l0 in zip(solvers, ws, lam0s):
+            s.set_inputs(w)
+            s.lambda_ = l0
+        best, us = qesb.autotune_batch(solvers)
+        nv = qesb.lib().qesb_num_variants()
+        assert 5 <= best < nv and len(us) == nv
+        assert all(u > 0 for u in us[5:]) and us[best] == min(us[5:])
+        for s, l0 in zip(solvers, lam0s):
+            np.testing.assert_array_equal(s.lambda_, l0)
+        outs = [[torch.zeros(w.domain.numFaceCentered(), dtype=torch.float32, device="cuda") for _ in range(3)]
+                for w in ws]
+        st = qesb.solve_batch(solvers, 3000, *[[o[q].data_ptr() for o in outs] for q in range(3)])
+        for w, l0, s, x, o in zip(ws, lam0s, st, solvers, outs):
+            d = w.domain
+            Lo, it, _, _ = O.sor(d, w, O.divergence(d, w), 1.1e-3, 3000, ordering=1, err_fp64=True, lam=l0)
+            assert s["iterations"] == it
+            np.testing.assert_array_equal(x.lambda_, Lo)
+            np.testing.assert_array_equal(o[0].cpu().numpy(), O.correct(d, w, Lo)[0])
+        with pytest.raises(qesb.QesbError):
+            solvers[0].set_option("batch_variant", 2)  # a fused tile shape: not a batch shape
+    finally:
+        for s in solvers:
+            s.close()

@@ -54,7 +54,8 @@ def test_divergence_R_bit_exact(golden):
 # fused tile shapes (0-4), scalar split (5-10), float4 split (11-13),
 # window-order split (14-17), bulk-copy staged (18-22), cp.async staged (23-27),
 # register-capped split (28-35)
-N_VARIANTS = 36
+N_VARIANTS = 44
+ZM = 40  # first z-march variant
 BULK = 18
 
 
@@ -155,7 +156,7 @@ def test_converged_winds_match_solver_cpu_cuboid100():
     assert st["max_divergence"] == div
 
 
-@pytest.mark.parametrize("variant", [5, 17, BULK + 1])
+@pytest.mark.parametrize("variant", [5, 17, BULK + 1, ZM + 2])
 def test_final_divergence_check_matches_oracle_metric(golden, variant):
     """qesb_stats.max_divergence (computed on the device in FP64 after the
     correction) equals the oracle's metric on the same winds, for single and
@@ -211,7 +212,7 @@ def test_graph_and_plain_launches_agree(golden, graph):
     np.testing.assert_array_equal(L, Lo)
 
 
-@pytest.mark.parametrize("variant", [1, 5, BULK + 1, BULK + 6])
+@pytest.mark.parametrize("variant", [1, 5, BULK + 1, BULK + 6, ZM, ZM + 1])
 def test_full_size_city400_packed_equals_full_path(variant):
     """400x400x100 stretched city: after 24 iterations the packed paths (fused
     and split) and the full-coefficient path hold the same lambda bits and the
@@ -231,6 +232,28 @@ def test_full_size_city400_packed_equals_full_path(variant):
     assert out[1][2]["path"] == 1 and out[0][2]["path"] == 0
 
 
+def test_full_size_city800_bit_exact_against_oracle():
+    """The largest configuration, 800x800x128 with 150 buildings: the default
+    (autotuned) sweep holds the oracle's lambda bits, residual history and
+    corrected winds after 6 iterations."""
+    w, _ = qesb.random_city("city800", 0)
+    d = w.domain
+    with qesb.Solver_B200(d, 1e-9) as s:
+        s.set_inputs(w)
+        s.autotune()
+        st = s.solve(w, 6, set_inputs=False)
+        L, H = s.lambda_, s.residual_history(6)
+    assert st["path"] == 1 and st["iterations"] == 6
+    R = O.divergence(d, w)
+    Lo, it, _, Ho = O.sor(d, w, R, 1e-9, 6, hist=True)
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(H, Ho)
+    uo, vo, wo = O.correct(d, w, Lo)
+    np.testing.assert_array_equal(w.u, uo)
+    np.testing.assert_array_equal(w.v, vo)
+    np.testing.assert_array_equal(w.w, wo)
+
+
 def test_autotune_restores_lambda_and_results_stay_exact(golden):
     d, w, z = golden("small_city.npz")
     lam0 = np.random.default_rng(7).standard_normal(d.numCellCentered()).astype(np.float32)
@@ -247,7 +270,7 @@ def test_autotune_restores_lambda_and_results_stay_exact(golden):
     np.testing.assert_array_equal(L, Lo)
 
 
-@pytest.mark.parametrize("variant", [5, 16, BULK + 1])
+@pytest.mark.parametrize("variant", [5, 16, BULK + 1, ZM])
 @pytest.mark.parametrize("omega,pre_tol,pre_max", [(1.9, 1e-3, 5000), (1.95, 5e-4, 150)])
 def test_overrelaxed_prephase_then_reference_loop(variant, omega, pre_tol, pre_max):
     """qesb_set_prephase: red-black SOR with another omega until its own rule

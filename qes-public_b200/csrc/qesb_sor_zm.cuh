@@ -34,7 +34,8 @@ constexpr int kZmOwnSlots = 3;       // planes k .. k + 2
 template <int TY>
 constexpr size_t zm_smem_bytes()
 {
-  return sizeof(float) * kZmOtherSlots * (TY + 2) * kZmOW + kZmOwnSlots * TY * kZmQ * (2 * sizeof(float) + 1);
+  return sizeof(float) * kZmOtherSlots * (TY + 2) * kZmOW + kZmOwnSlots * TY * kZmQ * (2 * sizeof(float) + 1) +
+         sizeof(float) * kZmOwnSlots * 64;
 }
 
 // 16-byte asynchronous copy global -> shared; src_bytes = 0 fills zeros and
@@ -55,12 +56,14 @@ struct ZmSmem {
   float *own;     // [kZmOwnSlots][TY][kZmQ]
   float *rr;      // [kZmOwnSlots][TY][kZmQ]
   uint8_t *mask;  // [kZmOwnSlots][TY][kZmQ]
+  float *inv;     // [kZmOwnSlots][64]: omega / (sum of the open faces' coefficients) per wall mask
   __device__ ZmSmem(unsigned char *base)
   {
     oth = reinterpret_cast<float *>(base);
     own = oth + kZmOtherSlots * (TY + 2) * kZmOW;
     rr = own + kZmOwnSlots * TY * kZmQ;
     mask = reinterpret_cast<uint8_t *>(rr + kZmOwnSlots * TY * kZmQ);
+    inv = reinterpret_cast<float *>(mask + kZmOwnSlots * TY * kZmQ);
   }
 };
 
@@ -114,7 +117,8 @@ __device__ __forceinline__ void zm_stage_other(const ZmSmem<TY> &sm, const ZmCop
     if (cp.os[t] >= 0) zm_cp16(dst + cp.os[t], cp.og[t] >= 0 ? src + cp.og[t] : D.L, cp.og[t] >= 0 ? 16 : 0);
 }
 
-// Stage the own colour's lambda, R and mask of plane p into own slot `slot`.
+// Stage the own colour's lambda, R and mask of plane p, and the plane's
+// 64-entry inverse-coefficient row, into own slot `slot`.
 template <int COLOUR, int TY>
 __device__ __forceinline__ void zm_stage_own(const ZmSmem<TY> &sm, const ZmCopies<TY> &cp, const SplitDom &D, int p,
                                              int slot)
@@ -126,6 +130,8 @@ __device__ __forceinline__ void zm_stage_own(const ZmSmem<TY> &sm, const ZmCopie
   zm_cp16(sm.rr + slot * TY * kZmQ + cp.ls, D.R + g, n);
   if (cp.ms >= 0)
     zm_cp16(sm.mask + slot * TY * kZmQ + cp.ms, D.mask + base + (cp.mg >= 0 ? cp.mg : 0), cp.mg >= 0 ? 16 : 0);
+  const int tid = threadIdx.x + 32 * threadIdx.y;
+  if (tid < 16) zm_cp16(sm.inv + slot * 64 + 4 * tid, D.inv_all + (long)p * 64 + 4 * tid, 16);
 }
 
 // One pipeline step's copies: the other colour's plane p + 1 and the own
@@ -193,11 +199,26 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
     zm_stage<COLOUR, TY>(sm, cp, D, k0, k1, 2, 0);
     zm_stage<COLOUR, TY>(sm, cp, D, k0 + 1, k1, 3, 1);
     int om1 = 0, wk = 0;  // slots of the other colour's plane k - 1 and the own colour's plane k
+    // the plane's six face coefficients, loaded one plane ahead
+    float lv[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) lv[f] = __ldg(D.val + f * D.Z + k0);
     for (int k = k0; k < k1; ++k, om1 = zm_wrap5(om1 + 1), wk = zm_wrap3(wk + 1)) {
       zm_wait1();        // this thread's copies of plane k's step have landed
       __syncthreads();   // everyone's; and every warp is done with plane k - 1
       zm_stage<COLOUR, TY>(sm, cp, D, k + 2, k1, zm_wrap5(om1 + 4), zm_wrap3(wk + 2));
-      D.layer(k);
+      D.ve = lv[0];
+      D.vf = lv[1];
+      D.vg = lv[2];
+      D.vh = lv[3];
+      D.vm = lv[4];
+      D.vn = lv[5];
+      const float *sinv = sm.inv + wk * 64;
+      D.inv63 = sinv[63];
+      if (k + 1 < k1) {
+#pragma unroll
+        for (int f = 0; f < 6; ++f) lv[f] = __ldg(D.val + f * D.Z + k + 1);
+      }
       if (row_ok) {
         // Every lane computes (the staged rows are 128 cells wide, zero-filled
         // past PQ); only cells inside [qlo, qhi] are updated and stored.
@@ -249,7 +270,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
             const float e = (m_ & 1u) ? D.ve : 0.0f, f = (m_ & 2u) ? D.vf : 0.0f;
             const float g = (m_ & 4u) ? D.vg : 0.0f, hh = (m_ & 8u) ? D.vh : 0.0f;
             const float m = (m_ & 16u) ? D.vm : 0.0f, n = (m_ & 32u) ? D.vn : 0.0f;
-            nv[t4] = __ldg(D.inv + m_) * (e * xpv[t4] + f * xmv[t4] + g * ypv[t4] + hh * ymv[t4] +
+            nv[t4] = sinv[m_] * (e * xpv[t4] + f * xmv[t4] + g * ypv[t4] + hh * ymv[t4] +
                                           m * zpv[t4] + n * zmv[t4] - rv[t4]) +
                      D.c1 * ov[t4];
           }

@@ -493,34 +493,41 @@ def run_b200(args):
     ms_e2e = max_over_ranks(ms_e2e)
     e2e_ok = all(torch.equal(ho[0], o[0].cpu()) for ho, o in zip(host_out, outs))
 
-    # ---- the SOR sweep kernel (roofline), from the plain single solves ------------
-    sor_ms = [x["ms_sor"] / max(x["iterations"], 1) for x in res_single[-1]]
-    ms_it = statistics.median(sor_ms)
-    alg_bytes = BYTES_PER_CELL_ITER * updated
-    achieved = alg_bytes / (ms_it * 1e-3) / 1e9
+    # ---- roofline of the dominant kernel: the list sweep of the headline step ---------
+    # The headline step is ~97 % red/black list sweeps. Its domain-iterations
+    # (pre-phase and reference loop, every domain) times the algorithmic bytes
+    # per updated cell, over the whole timed step (R, layout changes and the
+    # correction included), is a lower bound on the sweep kernel's rate. One
+    # launch is a half-sweep over the active list; per launch of the full list
+    # that is 1/2 x batch x updated cells x 36 B.
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         peak, peak_src = float(peaks["hbm_gbs"]), "measured"
         tpeak = float(peaks.get("bf16_tflops", 1590.0))
     except (OSError, KeyError, ValueError):
         peak, peak_src, tpeak = 6650.0, "fallback", 1590.0
+    dom_iters = sum(x["iterations"] + x["pre_iterations"] for x in res_warm[-1])
+    achieved = BYTES_PER_CELL_ITER * updated * dom_iters / (ms_warm * 1e-3) / 1e9
+    moved = MOVED_BYTES_PER_CELL_ITER * updated * dom_iters / (ms_warm * 1e-3) / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "sor_split4_city256.json")
+    prof = os.path.join(ROOT, "profiles", "sor_zm_batch_city256.json")
     if os.path.exists(prof):
         try:
-            traffic = json.load(open(prof)).get("dram_bytes_per_iteration")
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
         except ValueError:
             traffic = None
-
-    # ---- the headline step as a whole: the domain list's sweeps -----------------------
-    # Every domain-iteration of the step (pre-phase and reference loop) moves at
-    # least MOVED_BYTES_PER_CELL_ITER per updated cell; over the whole step time
-    # (R, layout changes and correction included) that is a lower bound on the
-    # sweep kernels' DRAM rate.
-    dom_iters = sum(x["iterations"] + x["pre_iterations"] for x in res_warm[-1])
-    moved = MOVED_BYTES_PER_CELL_ITER * updated * dom_iters / (ms_warm * 1e-3) / 1e9
     headline_sweep = {"domain_iterations": dom_iters, "us_per_domain_iteration": 1e3 * ms_warm / dom_iters,
                       "moved_gbs_lower_bound": moved, "moved_frac": moved / peak, "batch_variant": batch_variant}
+
+    # the same kernel family on one domain at a time (the plain single solves)
+    sor_ms = [x["ms_sor"] / max(x["iterations"], 1) for x in res_single[-1]]
+    ms_it = statistics.median(sor_ms)
+    alg_bytes = BYTES_PER_CELL_ITER * updated
+    single_domain = {"kernel": "red+black sweep pair (variant %d), per iteration inside the solve graphs" % variant,
+                     "ms_per_iteration": ms_it, "algorithmic_bytes_per_iteration": alg_bytes,
+                     "achieved": alg_bytes / (ms_it * 1e-3) / 1e9,
+                     "frac": alg_bytes / (ms_it * 1e-3) / 1e9 / peak,
+                     "note": "one 256^2 domain's sweep data (~70 MB) stays in L2 between launches"}
 
     # ---- the sweep at the 400^2 x 100 and 800^2 x 128 configurations ------------------
     sizes = None
@@ -543,6 +550,24 @@ def run_b200(args):
     torch.cuda.synchronize(dev)
     ms_fwd = fwd[0].elapsed_time(fwd[1]) / nf_rep
     flops = network_flops(net, s0)
+
+    # ---- log-law wall treatment (Wall::wallLogBC) on domain 0's solved winds --------
+    wall_log = None
+    try:
+        tmp = [o.clone() for o in outs[0]]
+        dzn = float(np.min(d0.dz_array))
+        solvers[0].wall_log_law(0.1, dzn, *[x.data_ptr() for x in tmp])
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize(dev)
+        ev[0].record(stream)
+        for _ in range(5):
+            solvers[0].wall_log_law(0.1, dzn, *[x.data_ptr() for x in tmp])
+        ev[1].record(stream)
+        torch.cuda.synchronize(dev)
+        wall_log = {"us_per_call": 1e3 * ev[0].elapsed_time(ev[1]) / 5, "launches_per_call": 7, "z0": 0.1,
+                    "workload": "domain 0 of the headline batch, after its solve"}
+    except Exception as ex:  # noqa: BLE001
+        wall_log = {"unavailable": str(ex)[:200]}
 
     # ---- reference GPU solver, CPU baseline, FP64 checks (rank 0, N = 1) --------------
     ref_gpu = None
@@ -620,9 +645,12 @@ def run_b200(args):
             "headline_sweep": headline_sweep,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                         "kernel": "red+black sweep pair (variant %d), per iteration inside the solve graphs" % variant,
-                         "ms_per_iteration": ms_it, "algorithmic_bytes_per_iteration": alg_bytes},
+                         "kernel": "red/black list sweep (variant %d) over the batch's domains, timed as the "
+                                   "whole headline step (lower bound)" % batch_variant,
+                         "algorithmic_bytes_per_launch": BYTES_PER_CELL_ITER * updated * B // 2,
+                         "moved_frac": moved / peak, "single_domain": single_domain},
             "sizes": sizes,
+            "wall_log_law": wall_log,
             "network": {"bound": "tensor", "ms_per_forward": ms_fwd, "flops_per_forward": flops,
                         "achieved_tflops": flops / (ms_fwd * 1e-3) / 1e12, "peak_tflops": tpeak,
                         "frac": flops / (ms_fwd * 1e-3) / 1e12 / tpeak},

@@ -161,6 +161,21 @@ qesb_status qesb_set_prephase(qesb_handle *h, float omega, float tol, int max_it
 qesb_status qesb_solve_batch(qesb_handle *const *handles, int n, int itermax, float *const *u,
                              float *const *v, float *const *w, qesb_stats *st);
 
+/* Log-law wall treatment after a solve, replacing the call
+ * WGD->wall->wallLogBC(WGD, true) that qesWindsMain.cpp:157-166 makes when
+ * logLawFlag = 1 (src/winds/Wall.cpp:352-803), for stair-step walls: u, v, w
+ * (device face arrays, nx*ny*nz each, typically the winds qesb_solve_device
+ * just wrote) are changed in place on the faces of fluid cells next to solid
+ * ones, side by side in the reference's order (below, above, back, front,
+ * right, left). z0 is WINDSGeneralData::z0 (roughness length, m); dz is the
+ * Domain's nominal dz (Domain::getDomainSize, Domain.h:104), whose first value
+ * (dx) the reference uses for the x and the y walls alike, as here. Runs on the
+ * handle's stream and returns when done. Cells flagged 7 or 8 (cut cells, whose
+ * walls the first part of wallLogBC treats) make it return QESB_ERR_STATE
+ * without changing u, v, w. Results agree with the reference to float
+ * rounding of atan2, cos and sin (the rest is the reference's arithmetic). */
+qesb_status qesb_wall_log_law(qesb_handle *h, float z0, float dz, float *u, float *v, float *w);
+
 /* Batch autotuner: times every sweep launch shape on the domain list that
  * qesb_solve_batch would run for these handles (same checks), a few launches
  * each from the handles' current lambda, and stores the fastest as

@@ -58,6 +58,8 @@ def port() -> C.CDLL:
         L.qo_correct_f64.restype = None
         L.qo_max_divergence.argtypes = [i, i, i, f, f] + [_V] * 5 + [i]
         L.qo_max_divergence.restype = d
+        L.qo_wall_log.argtypes = [i, i, i, f, f, f] + [_V] * 4
+        L.qo_wall_log.restype = i
         _port = L
     return _port
 
@@ -77,6 +79,8 @@ def ref() -> C.CDLL:
         L.qesref_set_velocity_zero.restype = i
         L.qesref_solve.argtypes = [i, i, i, i, f, f] + [_V] * 11 + [f, i] + [_V] * 5
         L.qesref_solve.restype = C.c_double
+        L.qesref_wall_log_bc.argtypes = [i, i, i, f, f, _V, _V, f, _V, _V, _V]
+        L.qesref_wall_log_bc.restype = i
         L.qesref_set_threads.argtypes = [i]
         L.qesref_set_threads.restype = None
         L.qesref_set_threads(1)
@@ -183,6 +187,26 @@ def ref_set_velocity_zero(dom, icellflag, u0, v0, w0):
     ref().qesref_set_velocity_zero(*_dims(dom), _p(dom.dz_array), _p(icellflag), _p(u0), _p(v0),
                                    _p(w0))
     return u0, v0, w0
+
+
+def wall_log(dom, icellflag, z0, u, v, w, dz=None):
+    """The stair-step log-law wall treatment (qo_wall_log) on copies of u, v,
+    w; dz defaults to min(dz_array), the nominal dz of the reference domain
+    the tests build. Returns (u, v, w), or None for cut-cell flags."""
+    u, v, w = (np.ascontiguousarray(a, dtype=np.float32).copy() for a in (u, v, w))
+    dz = float(np.min(dom.dz_array)) if dz is None else dz
+    r = port().qo_wall_log(*dom.base, float(dom.dx()), dz, float(z0),
+                           _p(np.ascontiguousarray(icellflag, dtype=np.int32)), _p(u), _p(v), _p(w))
+    return None if r != 0 else (u, v, w)
+
+
+def ref_wall_log_bc(dom, icellflag, z0, u, v, w):
+    """The reference's Wall::defineWalls + Wall::wallLogBC(WGD, true) on copies
+    of u, v, w (the reference build). Returns (u, v, w, flags after defineWalls)."""
+    u, v, w = (np.ascontiguousarray(a, dtype=np.float32).copy() for a in (u, v, w))
+    flag = np.ascontiguousarray(icellflag, dtype=np.int32).copy()
+    ref().qesref_wall_log_bc(*_dims(dom), _p(dom.dz_array), _p(flag), float(z0), _p(u), _p(v), _p(w))
+    return u, v, w, flag
 
 
 def ref_solve(dom, w, tol, itermax, kind=0, lam=None, want_lambda=True):

@@ -325,3 +325,79 @@ double qo_max_divergence(int Nx, int Ny, int Nz, float dx, float dy, const float
       }
   return mx;
 }
+
+/* Log-law wall treatment of the stair-step walls: the list construction of
+ * Wall::defineWalls (src/winds/Wall.cpp:287-340: fluid cells, k in [1, nz-3],
+ * loop order k, i, j, neighbours by flat cell index as Domain::cellAdd takes
+ * them) followed by the six list loops of Wall::wallLogBC
+ * (src/winds/Wall.cpp:656-796), in place on u0, v0, w0. Wall.h includes
+ * <math.h> under `using namespace std`, so atan2, log, cos and sin of floats
+ * are the float functions, and sqrt(pow(x, 2.0) + ...) is evaluated in double.
+ * dxy is Domain::getDomainSize()'s first value, which the reference uses for
+ * both the x and the y walls (it returns dx twice, src/qes/Domain.h:104); dz is
+ * its third, the Domain's nominal dz. vk = 0.4f (WINDSGeneralData.h).
+ * Returns -1, changing nothing, when a cell in that k range carries a cut-cell
+ * flag (7 or 8), whose walls the first part of wallLogBC treats; else 0. */
+static int wl_solid(int f) { return f == 0 || f == 2; }
+
+static void wl_fix(float *a, float *b, float *c_normal, long f, long nb, float d1, float d2, float z0)
+{
+  /* a, b: the two wall-parallel components (wind_dir = atan2(b, a)); the
+   * normal component c_normal is zeroed. */
+  const float vk = 0.4f;
+  float ustar_wall = 0.1f, wind_dir = 0.0f, vel_mag1 = 0.0f, vel_mag2, new_ustar;
+  for (int iter = 0; iter < 20; iter++) {
+    wind_dir = atan2f(b[nb], a[nb]);
+    vel_mag2 = (float)sqrt(pow(a[nb], 2.0) + pow(b[nb], 2.0));
+    vel_mag1 = vel_mag2 - (ustar_wall / vk) * logf(d2 / d1);
+    c_normal[f] = 0;
+    a[f] = vel_mag1 * cosf(wind_dir);
+    b[f] = vel_mag1 * sinf(wind_dir);
+    new_ustar = vk * vel_mag1 / logf(d1 / z0);
+    ustar_wall = new_ustar;
+  }
+}
+
+int qo_wall_log(int Nx, int Ny, int Nz, float dxy, float dz, float z0, const int *flag, float *u0, float *v0,
+                float *w0)
+{
+  grid_t g = mkgrid(Nx, Ny, Nz);
+  for (int k = 1; k < g.nz - 2; k++)
+    for (int i = 0; i < g.nx - 1; i++)
+      for (int j = 0; j < g.ny - 1; j++) {
+        const int fl = flag[cellix(&g, i, j, k)];
+        if (fl == 7 || fl == 8) return -1;
+      }
+  for (int side = 0; side < 6; side++) {
+    /* below, above (0.5 dz), back, front (0.5 dx), right, left (0.5 "dy" = dx) */
+    const float d1 = side < 2 ? 0.5f * dz : 0.5f * dxy, d2 = side < 2 ? 1.5f * dz : 1.5f * dxy;
+    for (int k = 1; k < g.nz - 2; k++)
+      for (int i = 0; i < g.nx - 1; i++)
+        for (int j = 0; j < g.ny - 1; j++) {
+          const long c = cellix(&g, i, j, k), f = faceix(&g, i, j, k);
+          const int fl = flag[c];
+          if (fl == 0 || fl == 2) continue;
+          switch (side) {
+          case 0:
+            if (wl_solid(flag[c - g.XY])) wl_fix(u0, v0, w0, f, f + g.FXY, d1, d2, z0);
+            break;
+          case 1:
+            if (wl_solid(flag[c + g.XY])) wl_fix(u0, v0, w0, f, f - g.FXY, d1, d2, z0);
+            break;
+          case 2:
+            if (wl_solid(flag[c - 1]) && i > 0) wl_fix(v0, w0, u0, f, f + 1, d1, d2, z0);
+            break;
+          case 3:
+            if (wl_solid(flag[c + 1])) wl_fix(v0, w0, u0, f, f - 1, d1, d2, z0);
+            break;
+          case 4:
+            if (wl_solid(flag[c - g.X]) && j > 0) wl_fix(u0, w0, v0, f, f + g.FX, d1, d2, z0);
+            break;
+          default:
+            if (wl_solid(flag[c + g.X])) wl_fix(u0, w0, v0, f, f - g.FX, d1, d2, z0);
+            break;
+          }
+        }
+  }
+  return 0;
+}

@@ -19,6 +19,7 @@
 #include "Solver_CPU.h"
 #include "Solver_CPU_RB.h"
 #include "Wall.h"
+#include <iostream>
 
 namespace {
 
@@ -116,6 +117,40 @@ int qesref_set_velocity_zero(int Nx, int Ny, int Nz, float dx, float dy, const f
   wgd.w0.assign(w0, w0 + nf);
   Wall wall;
   wall.setVelocityZero(&wgd);
+  std::memcpy(u0, wgd.u0.data(), sizeof(float) * nf);
+  std::memcpy(v0, wgd.v0.data(), sizeof(float) * nf);
+  std::memcpy(w0, wgd.w0.data(), sizeof(float) * nf);
+  return 0;
+}
+
+// Wall::defineWalls, then the reference's own Wall::wallLogBC(WGD, true)
+// (src/winds/Wall.cpp:352-803) on u0, v0, w0 in place, with WGD->z0 = z0, as
+// qesWindsMain.cpp:157-166 runs it after a solve (u0 <- u first). The domain is
+// make_domain's, so getDomainSize() gives (dx, dx, min dz). icellflag receives
+// the flags after defineWalls.
+int qesref_wall_log_bc(int Nx, int Ny, int Nz, float dx, float dy, const float *dz_array, int *icellflag,
+                       float z0, float *u0, float *v0, float *w0)
+{
+  qes::Domain d = make_domain(Nx, Ny, Nz, dx, dy, dz_array);
+  WINDSGeneralData wgd(d);
+  const long nc = d.numCellCentered(), nf = d.numFaceCentered();
+  for (auto *v : {&wgd.e, &wgd.f, &wgd.g, &wgd.h, &wgd.m, &wgd.n}) v->assign(nc, 1.0f);
+  wgd.building_volume_frac.assign(nc, 1.0f);
+  for (auto *v : {&wgd.ni, &wgd.nj, &wgd.nk, &wgd.ti, &wgd.tj, &wgd.tk, &wgd.wall_distance}) v->assign(nc, 0.0f);
+  wgd.center_id.assign(nc, 0);
+  wgd.icellflag.assign(icellflag, icellflag + nc);
+  Wall wall;
+  wall.defineWalls(&wgd);
+  wgd.z0 = z0;
+  wgd.u0.assign(u0, u0 + nf);
+  wgd.v0.assign(v0, v0 + nf);
+  wgd.w0.assign(w0, w0 + nf);
+  {
+    std::streambuf *keep = std::cout.rdbuf(nullptr);  // wallLogBC prints progress
+    wall.wallLogBC(&wgd, true);
+    std::cout.rdbuf(keep);
+  }
+  std::memcpy(icellflag, wgd.icellflag.data(), sizeof(int) * nc);
   std::memcpy(u0, wgd.u0.data(), sizeof(float) * nf);
   std::memcpy(v0, wgd.v0.data(), sizeof(float) * nf);
   std::memcpy(w0, wgd.w0.data(), sizeof(float) * nf);

@@ -40,6 +40,7 @@
 #include "qesb_sor_tiled.cuh"
 #include "qesb_sor_split.cuh"
 #include "qesb_sor_zm.cuh"
+#include "qesb_wall_log.cuh"
 #include "qesb_sor_bulk.cuh"
 
 // ---------------------------------------------------------------------------
@@ -592,6 +593,10 @@ struct qesb_handle {
   int opt_batch_variant = -1;  // sweep shape for batches led by this handle (qesb_autotune_batch)
   int opt_autotune = 0;
   int last_launches = 0;
+
+  // log-law wall treatment (qesb_wall_log_law): per-cell wall sides, cut-cell flag
+  uint8_t *d_wbits = nullptr;
+  int *d_wcut = nullptr;
 
   // red/black split layout (packed streaming path)
   SplitGeom S{};
@@ -1256,7 +1261,8 @@ void free_all(qesb_handle *h)
                   h->d_pc[3], h->d_pc[4], h->d_pc[5], h->d_own_in[0], h->d_own_in[1],
                   h->d_own_in[2], h->d_own_in[3], h->d_own_in[4], h->d_own_in[5], h->d_own_flag,
                   h->d_own_u0, h->d_own_v0, h->d_own_w0, h->d_dz, h->d_vmax, h->d_inv, h->d_val,
-                  h->d_inv_pre, h->d_bad, h->d_err, h->d_state, h->d_u, h->d_v, h->d_w};
+                  h->d_inv_pre, h->d_bad, h->d_err, h->d_state, h->d_u, h->d_v, h->d_w, h->d_wbits,
+                  h->d_wcut};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   h->list.destroy();
@@ -1433,6 +1439,43 @@ qesb_status qesb_set_inputs_device(qesb_handle *h, const float *e, const float *
   CKS(prepare_coefs(h));
   CK(cudaStreamSynchronize(h->stream));
   h->have_inputs = true;
+  return QESB_OK;
+}
+
+qesb_status qesb_wall_log_law(qesb_handle *h, float z0, float dz, float *u, float *v, float *w)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  if (!u || !v || !w) return qesb_fail(QESB_ERR_ARG, "qesb_wall_log_law: null wind array");
+  if (!(z0 > 0.0f) || !(dz > 0.0f)) return qesb_fail(QESB_ERR_ARG, "qesb_wall_log_law: z0 and dz must be > 0");
+  if (!h->have_inputs) return qesb_fail(QESB_ERR_STATE, "qesb_wall_log_law needs inputs (icellflag)");
+  CK(cudaSetDevice(h->device));
+  const DevGrid &G = h->G;
+  cudaStream_t s = h->stream;
+  if (!h->d_wbits) {
+    CK(cudaMalloc((void **)&h->d_wbits, (size_t)G.XY * G.Z));
+    CK(cudaMalloc((void **)&h->d_wcut, sizeof(int)));
+  }
+  CK(cudaMemsetAsync(h->d_wcut, 0, sizeof(int), s));
+  const dim3 grid((G.X + 127) / 128, G.Y, G.Z - 2), block(128);
+  k_wall_bits<<<grid, block, 0, s>>>(G, h->d_flag, h->d_wbits, h->d_wcut);
+  // the reference's distances: getDomainSize() is (dx, dx, dz) (Domain.h:104),
+  // so the y walls use dx as well; its logarithms of floats are logf
+  const float dxy = h->dx;
+  const float lz21 = logf((1.5f * dz) / (0.5f * dz)), lz10 = logf((0.5f * dz) / z0);
+  const float lx21 = logf((1.5f * dxy) / (0.5f * dxy)), lx10 = logf((0.5f * dxy) / z0);
+  k_wall_log<kWallBelow><<<grid, block, 0, s>>>(G, h->d_wbits, h->d_wcut, u, v, w, lz21, lz10);
+  k_wall_log<kWallAbove><<<grid, block, 0, s>>>(G, h->d_wbits, h->d_wcut, u, v, w, lz21, lz10);
+  k_wall_log<kWallBack><<<grid, block, 0, s>>>(G, h->d_wbits, h->d_wcut, u, v, w, lx21, lx10);
+  k_wall_log<kWallFront><<<grid, block, 0, s>>>(G, h->d_wbits, h->d_wcut, u, v, w, lx21, lx10);
+  k_wall_log<kWallRight><<<grid, block, 0, s>>>(G, h->d_wbits, h->d_wcut, u, v, w, lx21, lx10);
+  k_wall_log<kWallLeft><<<grid, block, 0, s>>>(G, h->d_wbits, h->d_wcut, u, v, w, lx21, lx10);
+  CK(cudaGetLastError());
+  int cut = 0;
+  CK(cudaMemcpyAsync(&cut, h->d_wcut, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (cut)
+    return qesb_fail(QESB_ERR_STATE,
+                     "qesb_wall_log_law: cut-cell flags (7, 8) present; only stair-step walls are treated");
   return QESB_OK;
 }
 

@@ -111,6 +111,7 @@ def lib() -> C.CDLL:
                                   C.POINTER(Stats)], C.c_int),
             "qesb_autotune_batch": ([C.POINTER(V), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int],
                                     C.c_int),
+            "qesb_wall_log_law": ([V, C.c_float, C.c_float, V, V, V], C.c_int),
             "qesb_num_variants": ([], C.c_int),
             "qesb_set_option": ([V, C.c_char_p, C.c_int], C.c_int),
             "qesb_set_stream": ([V, V], C.c_int),
@@ -333,6 +334,11 @@ class Solver_B200:
         check(lib().qesb_solve_device(self._h, int(itermax), u_ptr, v_ptr, w_ptr, C.byref(st)))
         self.last_stats = st.as_dict()
         return self.last_stats
+
+    def wall_log_law(self, z0: float, dz: float, u_ptr, v_ptr, w_ptr) -> None:
+        """qesb_wall_log_law: the log-law wall treatment (Wall::wallLogBC's
+        stair-step part) in place on device wind arrays (pointers as ints)."""
+        check(lib().qesb_wall_log_law(self._h, float(z0), float(dz), u_ptr, v_ptr, w_ptr))
 
     @property
     def lambda_(self) -> np.ndarray:

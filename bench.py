@@ -88,6 +88,7 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 same-SOR error and divergence checks")
     ap.add_argument("--no-sizes", action="store_true", help="skip the 400^2 and 800^2 sweep-speed section")
+    ap.add_argument("--no-fire-loop", action="store_true", help="skip the fire-step section")
     ap.add_argument("--variant", type=int, default=-1, help="sweep variant for the profiling drivers (-1: autotune)")
     ap.add_argument("--profile-solve", type=int, default=0,
                     help="profiling driver: one solve of this many iterations (tol 0) with --variant, exit")
@@ -96,6 +97,8 @@ def parse():
     ap.add_argument("--ensemble", action="store_true",
                     help="batched ensemble: 64 cities of uneven size x 36 wind directions (solves/s, p50/p99)")
     ap.add_argument("--ensemble-domains", type=int, default=64)
+    ap.add_argument("--fire-loop", type=int, default=0,
+                    help="QES-Fire solve pattern: this many fire steps warm-started from the previous lambda, exit")
     ap.add_argument("--profile-batch", action="store_true",
                     help="profiling driver: the headline batch (pre-phase pipeline) once untimed, once more, exit")
     ap.add_argument("--forward-only", type=int, default=0,
@@ -315,6 +318,97 @@ def size_rates(peak, workloads=("city400", "city800")):
                      "us_per_iteration": 1e3 * ms_it, "algorithmic_gbs": alg, "algorithmic_frac": alg / peak,
                      "moved_gbs": moved, "moved_frac": moved / peak}
     return out
+
+
+def fire_inflow(wgd, t, x0=60.0, speed=4.0, updraft=3.0, inflow=1.0, sigma=20.0, zc=30.0):
+    """u0, v0, w0 of QES-Fire step t: the sensor field plus a synthetic
+    fire-induced wind, for driving the solver as qesFireMain.cpp:232-259 does
+    (u0 reset to the sensor field, fire winds added, solve without
+    resetLambda). The fire physics (Fire::LevelSetNB, Fire::potential) is not
+    on the solve path; this stand-in is a Gaussian updraft over a fire centre
+    moving `speed` m per step along x at mid-y, with convergent horizontal
+    inflow, fading above zc. Faces of solid cells are zeroed as
+    Wall::setVelocityZero does (src/winds/Wall.cpp:805-825)."""
+    d = wgd.domain
+    nx, ny, nz = d.nx(), d.ny(), d.nz()
+    dx, dy = d.dx(), d.dy()
+    xf, yf = x0 + speed * t, 0.5 * (ny - 1) * dy
+    zc_k = np.minimum(1.0, np.maximum(d.z[:nz - 1], 0.0) / zc)
+    zk = np.concatenate([zc_k, zc_k[-1:]])[:, None, None]
+    i = np.arange(nx)[None, None, :]
+    j = np.arange(ny)[None, :, None]
+
+    def gauss(x, y):
+        return np.exp(-((x - xf) ** 2 + (y - yf) ** 2) / sigma ** 2)
+
+    fade = np.exp(-np.maximum(np.concatenate([d.z, d.z[-1:]]) - zc, 0.0) / zc)[:, None, None]
+    xu, yu = i * dx, (j + 0.5) * dy
+    xv, yv = (i + 0.5) * dx, j * dy
+    xw, yw = (i + 0.5) * dx, (j + 0.5) * dy
+    du = -inflow * (xu - xf) / sigma * gauss(xu, yu) * fade
+    dv = -inflow * (yv - yf) / sigma * gauss(xv, yv) * fade
+    dw = updraft * gauss(xw, yw) * zk * fade
+    import qesb
+
+    out = qesb.WINDSGeneralData(d)  # shares the flags and coefficients
+    out.icellflag, out.e, out.f, out.g, out.h, out.m, out.n = (wgd.icellflag, wgd.e, wgd.f, wgd.g, wgd.h, wgd.m,
+                                                                wgd.n)
+    shape = (nz, ny, nx)
+    out.u0 = (wgd.u0.reshape(shape) + du).astype(np.float32).ravel()
+    out.v0 = (wgd.v0.reshape(shape) + dv).astype(np.float32).ravel()
+    out.w0 = (wgd.w0.reshape(shape) + dw).astype(np.float32).ravel()
+    fl = wgd.icellflag.reshape(d.cell_shape())
+    u0, v0, w0 = (a.reshape(shape) for a in (out.u0, out.v0, out.w0))
+    solid = (fl == 0) | (fl == 2)
+    ks, js, is_ = np.nonzero(solid[:, 1:ny - 1, 1:nx - 1])
+    js, is_ = js + 1, is_ + 1
+    for a, di, dj, dk in ((u0, 0, 0, 0), (u0, 1, 0, 0), (v0, 0, 0, 0), (v0, 0, 1, 0), (w0, 0, 0, 0), (w0, 0, 0, 1)):
+        a[ks + dk, js + dj, is_ + di] = 0.0
+    return out
+
+
+def run_fire_loop(args, steps=None, print_line=True):
+    """QES-Fire's solve pattern on one 256x256x64 city: a first solve from
+    lambda = 0, then `steps` fire steps, each with new u0 (fire_inflow) and
+    Solver::solve without resetLambda, so every solve starts from the previous
+    step's lambda, as the reference's fire loop does. Three arms on the same
+    inputs: warm (that behaviour), cold (resetLambda before every step), warm
+    + over-relaxed pre-phase. Device time per solve (CUDA events) and
+    iterations."""
+    import torch
+
+    import qesb
+
+    steps = steps or args.fire_loop
+    w, _ = qesb.random_city(args.workload, SEED0)
+    d = w.domain
+    seq = [fire_inflow(w, t) for t in range(1, steps + 1)]
+    arms = {}
+    with qesb.Solver_B200(d, TOL) as s:
+        s.set_inputs(w)
+        s.autotune()
+        for arm in ("warm", "cold", "warm+prephase"):
+            s.set_prephase(PRE_OMEGA if arm == "warm+prephase" else 0.0, PRE_TOL, ITERMAX)
+            s.resetLambda()
+            s.solve(w, ITERMAX)
+            its, pre, ms = [], [], []
+            for wt in seq:
+                if arm == "cold":
+                    s.resetLambda()
+                st = s.solve(wt, ITERMAX)
+                its.append(st["iterations"])
+                pre.append(st["pre_iterations"])
+                ms.append(st["ms_total"])
+            arms[arm] = {"ms_per_solve": float(np.mean(ms)), "iterations": its, "pre_iterations": pre}
+        torch.cuda.synchronize()
+    out = {"fire_loop": {"workload": f"{args.workload} seed {SEED0}", "steps": steps,
+                         "perturbation": "synthetic fire-induced winds: 3 m/s Gaussian updraft (sigma 20 m) and "
+                                         "1 m/s convergent inflow over a fire centre moving 4 m per step",
+                         "arms": arms,
+                         "speedup_warm_vs_cold": arms["cold"]["ms_per_solve"] / arms["warm"]["ms_per_solve"]}}
+    if print_line:
+        print(json.dumps(out), flush=True)
+    return out["fire_loop"]
 
 
 def network_flops(net, s):
@@ -551,6 +645,14 @@ def run_b200(args):
     ms_fwd = fwd[0].elapsed_time(fwd[1]) / nf_rep
     flops = network_flops(net, s0)
 
+    # ---- QES-Fire's solve pattern: fire steps warm-started from the previous lambda ----
+    fire = None
+    if not args.no_fire_loop and rank == 0:
+        try:
+            fire = run_fire_loop(args, steps=8, print_line=False)
+        except Exception as ex:  # noqa: BLE001
+            fire = {"unavailable": str(ex)[:200]}
+
     # ---- log-law wall treatment (Wall::wallLogBC) on domain 0's solved winds --------
     wall_log = None
     try:
@@ -651,6 +753,7 @@ def run_b200(args):
                          "moved_frac": moved / peak, "single_domain": single_domain},
             "sizes": sizes,
             "wall_log_law": wall_log,
+            "fire_loop": fire,
             "network": {"bound": "tensor", "ms_per_forward": ms_fwd, "flops_per_forward": flops,
                         "achieved_tflops": flops / (ms_fwd * 1e-3) / 1e12, "peak_tflops": tpeak,
                         "frac": flops / (ms_fwd * 1e-3) / 1e12 / tpeak},
@@ -870,6 +973,8 @@ def main():
         run_profile_batch(args)
     elif args.ensemble:
         run_ensemble(args)
+    elif args.fire_loop:
+        run_fire_loop(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -886,6 +886,7 @@ struct SweepVariant {
   const char *name;
   int unit;
   int block_y;  // warps per CTA
+  int tile_rows;  // z-march tiles: rows per tile (0 for the other kinds)
   size_t smem;  // dynamic shared memory per CTA
   void (*red)(SweepArgs);  // single domain (from the kernel parameters)
   void (*black)(SweepArgs);
@@ -901,6 +902,7 @@ constexpr SweepVariant make_split(const char *name)
                       kUnitRow,
                       RPB,
                       0,
+                      0,
                       k_sor_split<0, RPB, U, STRIDED, false, MINB>,
                       k_sor_split<1, RPB, U, STRIDED, false, MINB>,
                       k_sor_split<0, RPB, U, STRIDED, true, MINB>,
@@ -913,6 +915,7 @@ constexpr SweepVariant make_split4(const char *name)
                       kUnitRow,
                       RPB,
                       0,
+                      0,
                       k_sor_split4<0, RPB, STRIDED, false, MINB>,
                       k_sor_split4<1, RPB, STRIDED, false, MINB>,
                       k_sor_split4<0, RPB, STRIDED, true, MINB>,
@@ -924,23 +927,25 @@ constexpr SweepVariant make_bulk(const char *name)
   return SweepVariant{name,
                       kUnitSpan,
                       W,
+                      0,
                       bulk_smem_bytes<W, NS>(),
                       k_sor_bulk<0, W, NS, ASYNC, false>,
                       k_sor_bulk<1, W, NS, ASYNC, false>,
                       k_sor_bulk<0, W, NS, ASYNC, true>,
                       k_sor_bulk<1, W, NS, ASYNC, true>};
 }
-template <int TY, int MINB>
+template <int TY, int RW, int MINB>
 constexpr SweepVariant make_zm(const char *name)
 {
   return SweepVariant{name,
                       kUnitTile,
                       TY,
-                      zm_smem_bytes<TY>(),
-                      k_sor_zm<0, TY, false, MINB>,
-                      k_sor_zm<1, TY, false, MINB>,
-                      k_sor_zm<0, TY, true, MINB>,
-                      k_sor_zm<1, TY, true, MINB>};
+                      TY * RW,
+                      zm_smem_bytes<TY * RW>(),
+                      k_sor_zm<0, TY, RW, false, MINB>,
+                      k_sor_zm<1, TY, RW, false, MINB>,
+                      k_sor_zm<0, TY, RW, true, MINB>,
+                      k_sor_zm<1, TY, RW, true, MINB>};
 }
 const SweepVariant kSweepVariants[] = {
     // streaming split kernels (option "variant" 5..17)
@@ -963,7 +968,10 @@ const SweepVariant kSweepVariants[] = {
     make_split4<8, 2, 3>("split4_r8_pf_b3"), make_split4<4, 2, 6>("split4_r4_pf_b6"),
     make_split<4, 4, 2, 6>("split_r4_u4_pf_b6"), make_split4<4, 2, 8>("split4_r4_pf_b8"),
     // z-march tiles, other colour staged in shared memory (40..43)
-    make_zm<8, 4>("zm_y8"), make_zm<4, 6>("zm_y4_b6"), make_zm<8, 3>("zm_y8_b3"), make_zm<8, 2>("zm_y8_b2"),
+    make_zm<8, 1, 4>("zm_y8"), make_zm<4, 1, 6>("zm_y4_b6"), make_zm<8, 1, 3>("zm_y8_b3"), make_zm<8, 1, 2>("zm_y8_b2"),
+    // two rows per warp (44..47)
+    make_zm<4, 2, 4>("zm_y4x2_b4"), make_zm<4, 2, 5>("zm_y4x2_b5"), make_zm<2, 2, 8>("zm_y2x2_b8"),
+    make_zm<8, 2, 2>("zm_y8x2_b2"),
 };
 constexpr int kNumSweep = sizeof(kSweepVariants) / sizeof(kSweepVariants[0]);
 constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the first sweep shape
@@ -1002,7 +1010,7 @@ void sweep_tiles(std::vector<SweepDomain> &doms, const SweepVariant &sv, bool mu
   for (int kc = 4; kc <= 32; ++kc) {
     long tiles = 0;
     for (SweepDomain &d : doms) {
-      d.tile_y = sv.block_y;
+      d.tile_y = sv.tile_rows;
       d.kc = kc;
       tiles += sweep_units(d, kUnitTile);
     }

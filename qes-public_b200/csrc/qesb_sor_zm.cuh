@@ -70,15 +70,18 @@ struct ZmSmem {
 // A thread's share of a tile's staging, fixed for the tile: shared-memory
 // offsets within a slot and global offsets within a colour plane (valid ones
 // only; the others zero-fill). Each plane then costs a few adds per copy.
-template <int TY>
+// TR: rows per tile; NT: threads of the CTA.
+template <int TR, int NT>
 struct ZmCopies {
   static constexpr int NCH = kZmOW / 4;                   // 16-byte chunks per staged row
-  static constexpr int NOTH = (TY + 2) * NCH;             // other-colour chunks per plane
-  static constexpr int NT = 32 * TY;                      // threads
+  static constexpr int NOTH = (TR + 2) * NCH;             // other-colour chunks per plane
   static constexpr int NO = (NOTH + NT - 1) / NT;         // other-colour chunks per thread
+  static constexpr int NL = TR * 32 / NT;                 // own lambda / R chunks per thread
+  static constexpr int NM = (TR * 8 + NT - 1) / NT;       // own mask chunks per thread
+  static_assert(TR * 32 % NT == 0, "own-colour rows must split evenly over the threads");
   int os[NO], og[NO];  // other colour: slot offset (floats), plane offset (floats; -1: zero-fill)
-  int ls, lg;          // own lambda and R: one chunk per thread
-  int ms, mg;          // own mask: threads tid < TY * 8 (ms < 0: none)
+  int ls[NL], lg[NL];  // own lambda and R
+  int ms[NM], mg[NM];  // own mask (ms < 0: none)
 
   __device__ __forceinline__ void init(const SplitDom &D, int j0, int q0, int tid)
   {
@@ -90,59 +93,69 @@ struct ZmCopies {
       os[t] = c < NOTH ? r * kZmOW + 4 * col : -1;
       og[t] = (c < NOTH && j < D.Y && q >= 0 && q < D.PQ) ? j * D.PQ + q : -1;
     }
-    {
-      const int r = tid >> 5, col = tid & 31;
+#pragma unroll
+    for (int t = 0; t < NL; ++t) {
+      const int c = tid + t * NT;
+      const int r = c >> 5, col = c & 31;
       const int j = j0 + r, q = q0 + 4 * col;
-      ls = r * kZmQ + 4 * col;
-      lg = (j <= D.Y - 2 && q < D.PQ) ? j * D.PQ + q : -1;
+      ls[t] = r * kZmQ + 4 * col;
+      lg[t] = (j <= D.Y - 2 && q < D.PQ) ? j * D.PQ + q : -1;
     }
-    {
-      const int r = tid >> 3, col = tid & 7;
+#pragma unroll
+    for (int t = 0; t < NM; ++t) {
+      const int c = tid + t * NT;
+      const int r = c >> 3, col = c & 7;
       const int j = j0 + r, q = q0 + 16 * col;
-      ms = tid < TY * 8 ? r * kZmQ + 16 * col : -1;
-      mg = (tid < TY * 8 && j <= D.Y - 2 && q < D.PQ) ? j * D.PQ + q : -1;
+      ms[t] = c < TR * 8 ? r * kZmQ + 16 * col : -1;
+      mg[t] = (c < TR * 8 && j <= D.Y - 2 && q < D.PQ) ? j * D.PQ + q : -1;
     }
   }
 };
 
 // Stage the other colour's plane p into other-colour slot `slot`.
-template <int COLOUR, int TY>
-__device__ __forceinline__ void zm_stage_other(const ZmSmem<TY> &sm, const ZmCopies<TY> &cp, const SplitDom &D,
+template <int COLOUR, int TR, int NT>
+__device__ __forceinline__ void zm_stage_other(const ZmSmem<TR> &sm, const ZmCopies<TR, NT> &cp, const SplitDom &D,
                                                int p, int slot)
 {
-  float *dst = sm.oth + slot * (TY + 2) * kZmOW;
+  float *dst = sm.oth + slot * (TR + 2) * kZmOW;
   const float *src = D.L + (1 - COLOUR) * D.CS + (long)p * D.Y * D.PQ;
 #pragma unroll
-  for (int t = 0; t < ZmCopies<TY>::NO; ++t)
+  for (int t = 0; t < ZmCopies<TR, NT>::NO; ++t)
     if (cp.os[t] >= 0) zm_cp16(dst + cp.os[t], cp.og[t] >= 0 ? src + cp.og[t] : D.L, cp.og[t] >= 0 ? 16 : 0);
 }
 
 // Stage the own colour's lambda, R and mask of plane p, and the plane's
 // 64-entry inverse-coefficient row, into own slot `slot`.
-template <int COLOUR, int TY>
-__device__ __forceinline__ void zm_stage_own(const ZmSmem<TY> &sm, const ZmCopies<TY> &cp, const SplitDom &D, int p,
-                                             int slot)
+template <int COLOUR, int TR, int NT>
+__device__ __forceinline__ void zm_stage_own(const ZmSmem<TR> &sm, const ZmCopies<TR, NT> &cp, const SplitDom &D,
+                                             int p, int slot)
 {
   const long base = COLOUR * D.CS + (long)p * D.Y * D.PQ;
-  const int n = cp.lg >= 0 ? 16 : 0;
-  const long g = base + (cp.lg >= 0 ? cp.lg : 0);
-  zm_cp16(sm.own + slot * TY * kZmQ + cp.ls, D.L + g, n);
-  zm_cp16(sm.rr + slot * TY * kZmQ + cp.ls, D.R + g, n);
-  if (cp.ms >= 0)
-    zm_cp16(sm.mask + slot * TY * kZmQ + cp.ms, D.mask + base + (cp.mg >= 0 ? cp.mg : 0), cp.mg >= 0 ? 16 : 0);
+#pragma unroll
+  for (int t = 0; t < ZmCopies<TR, NT>::NL; ++t) {
+    const int n = cp.lg[t] >= 0 ? 16 : 0;
+    const long g = base + (cp.lg[t] >= 0 ? cp.lg[t] : 0);
+    zm_cp16(sm.own + slot * TR * kZmQ + cp.ls[t], D.L + g, n);
+    zm_cp16(sm.rr + slot * TR * kZmQ + cp.ls[t], D.R + g, n);
+  }
+#pragma unroll
+  for (int t = 0; t < ZmCopies<TR, NT>::NM; ++t)
+    if (cp.ms[t] >= 0)
+      zm_cp16(sm.mask + slot * TR * kZmQ + cp.ms[t], D.mask + base + (cp.mg[t] >= 0 ? cp.mg[t] : 0),
+              cp.mg[t] >= 0 ? 16 : 0);
   const int tid = threadIdx.x + 32 * threadIdx.y;
   if (tid < 16) zm_cp16(sm.inv + slot * 64 + 4 * tid, D.inv_all + (long)p * 64 + 4 * tid, 16);
 }
 
 // One pipeline step's copies: the other colour's plane p + 1 and the own
 // colour's plane p (p < k1), as one copy group (empty past the tile's end).
-template <int COLOUR, int TY>
-__device__ __forceinline__ void zm_stage(const ZmSmem<TY> &sm, const ZmCopies<TY> &cp, const SplitDom &D, int p,
+template <int COLOUR, int TR, int NT>
+__device__ __forceinline__ void zm_stage(const ZmSmem<TR> &sm, const ZmCopies<TR, NT> &cp, const SplitDom &D, int p,
                                          int k1, int oslot, int wslot)
 {
   if (p < k1) {
-    zm_stage_other<COLOUR, TY>(sm, cp, D, p + 1, oslot);
-    zm_stage_own<COLOUR, TY>(sm, cp, D, p, wslot);
+    zm_stage_other<COLOUR, TR, NT>(sm, cp, D, p + 1, oslot);
+    zm_stage_own<COLOUR, TR, NT>(sm, cp, D, p, wslot);
   }
   zm_commit();
 }
@@ -150,13 +163,15 @@ __device__ __forceinline__ void zm_stage(const ZmSmem<TY> &sm, const ZmCopies<TY
 __device__ __forceinline__ int zm_wrap5(int x) { return x >= 5 ? x - 5 : x; }
 __device__ __forceinline__ int zm_wrap3(int x) { return x >= 3 ? x - 3 : x; }
 
-template <int COLOUR, int TY, bool MULTI, int MINB>
+// TY warps per CTA, RW rows per warp (rows w, w + TY, ...): tiles of TY x RW rows.
+template <int COLOUR, int TY, int RW, bool MULTI, int MINB>
 __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
 {
+  constexpr int TR = TY * RW, NT = 32 * TY;
   const int na = b.ctl->nactive;
   if (na <= 0) return;
   extern __shared__ __align__(16) unsigned char zm_raw[];
-  const ZmSmem<TY> sm(zm_raw);
+  const ZmSmem<TR> sm(zm_raw);
   const int lane = threadIdx.x, w = threadIdx.y, tid = lane + 32 * w;
   const int total = MULTI ? b.uoff[na] : sweep_units(b.one, kUnitTile);
   SplitDom D;
@@ -176,28 +191,27 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
       D.load(sweep_dom<MULTI>(b, slot));
     }
     const SweepDomain &SD = sweep_dom<MULTI>(b, slot);
-    const int njt = (D.Y - 2 + TY - 1) / TY, kc = SD.kc;
+    const int njt = (D.Y - 2 + TR - 1) / TR, kc = SD.kc;
     const int nch = SD.nch;
     int t = u - lo;
     const int qt = t % nch;
     t /= nch;
     const int jt = t % njt, kt = t / njt;
-    const int q0 = qt * kZmQ, j0 = 1 + jt * TY, k0 = 1 + kt * kc;
+    const int q0 = qt * kZmQ, j0 = 1 + jt * TR, k0 = 1 + kt * kc;
     const int k1 = min(k0 + kc, D.Z - 1);
-    const int j = j0 + w, q = q0 + 4 * lane;
-    const bool row_ok = j <= D.Y - 2;
+    const int q = q0 + 4 * lane;
     const int qn = (D.X + 1) >> 1;
-    ZmCopies<TY> cp;
+    ZmCopies<TR, NT> cp;
     cp.init(D, j0, q0, tid);
 
     // Ring slots restart with each tile: the other colour's plane k0 - 1 + s
     // sits in slot s mod 5, the own colour's plane k0 + s in slot s mod 3.
     // Prologue: other planes k0 - 1, k0 (and k0 + 1 with own k0) as one
     // group, then the step of plane k0 + 1.
-    zm_stage_other<COLOUR, TY>(sm, cp, D, k0 - 1, 0);
-    zm_stage_other<COLOUR, TY>(sm, cp, D, k0, 1);
-    zm_stage<COLOUR, TY>(sm, cp, D, k0, k1, 2, 0);
-    zm_stage<COLOUR, TY>(sm, cp, D, k0 + 1, k1, 3, 1);
+    zm_stage_other<COLOUR, TR, NT>(sm, cp, D, k0 - 1, 0);
+    zm_stage_other<COLOUR, TR, NT>(sm, cp, D, k0, 1);
+    zm_stage<COLOUR, TR, NT>(sm, cp, D, k0, k1, 2, 0);
+    zm_stage<COLOUR, TR, NT>(sm, cp, D, k0 + 1, k1, 3, 1);
     int om1 = 0, wk = 0;  // slots of the other colour's plane k - 1 and the own colour's plane k
     // the plane's six face coefficients, loaded one plane ahead
     float lv[6];
@@ -206,7 +220,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
     for (int k = k0; k < k1; ++k, om1 = zm_wrap5(om1 + 1), wk = zm_wrap3(wk + 1)) {
       zm_wait1();        // this thread's copies of plane k's step have landed
       __syncthreads();   // everyone's; and every warp is done with plane k - 1
-      zm_stage<COLOUR, TY>(sm, cp, D, k + 2, k1, zm_wrap5(om1 + 4), zm_wrap3(wk + 2));
+      zm_stage<COLOUR, TR, NT>(sm, cp, D, k + 2, k1, zm_wrap5(om1 + 4), zm_wrap3(wk + 2));
       D.ve = lv[0];
       D.vf = lv[1];
       D.vg = lv[2];
@@ -219,27 +233,30 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
 #pragma unroll
         for (int f = 0; f < 6; ++f) lv[f] = __ldg(D.val + f * D.Z + k + 1);
       }
-      if (row_ok) {
+#pragma unroll
+      for (int r = 0; r < RW; ++r) {
+        const int wr = w + r * TY, j = j0 + wr;
+        if (j > D.Y - 2) continue;  // warp-uniform
         // Every lane computes (the staged rows are 128 cells wide, zero-filled
         // past PQ); only cells inside [qlo, qhi] are updated and stored.
         const int i0 = (COLOUR + j + k) & 1;
         const int qlo = i0 ? 0 : 1;
         const int qhi = (D.X - 2 - i0) >> 1;  // inclusive
-        const float *om = sm.oth + om1 * (TY + 2) * kZmOW;
-        const float *ok = sm.oth + zm_wrap5(om1 + 1) * (TY + 2) * kZmOW;
-        const float *op = sm.oth + zm_wrap5(om1 + 2) * (TY + 2) * kZmOW;
+        const float *om = sm.oth + om1 * (TR + 2) * kZmOW;
+        const float *ok = sm.oth + zm_wrap5(om1 + 1) * (TR + 2) * kZmOW;
+        const float *op = sm.oth + zm_wrap5(om1 + 2) * (TR + 2) * kZmOW;
         const int c = 4 + 4 * lane;  // column of q in a staged other-colour row
-        const int so = wk * TY * kZmQ + w * kZmQ + 4 * lane;
+        const int so = wk * TR * kZmQ + wr * kZmQ + 4 * lane;
         const float4 o = *reinterpret_cast<const float4 *>(sm.own + so);
         const float4 rr = *reinterpret_cast<const float4 *>(sm.rr + so);
         const uint32_t m4 = *reinterpret_cast<const uint32_t *>(sm.mask + so);
-        const float4 xc = *reinterpret_cast<const float4 *>(ok + (w + 1) * kZmOW + c);
-        const float4 ym = *reinterpret_cast<const float4 *>(ok + w * kZmOW + c);
-        const float4 yp = *reinterpret_cast<const float4 *>(ok + (w + 2) * kZmOW + c);
-        const float4 zm = *reinterpret_cast<const float4 *>(om + (w + 1) * kZmOW + c);
-        const float4 zp = *reinterpret_cast<const float4 *>(op + (w + 1) * kZmOW + c);
+        const float4 xc = *reinterpret_cast<const float4 *>(ok + (wr + 1) * kZmOW + c);
+        const float4 ym = *reinterpret_cast<const float4 *>(ok + wr * kZmOW + c);
+        const float4 yp = *reinterpret_cast<const float4 *>(ok + (wr + 2) * kZmOW + c);
+        const float4 zm = *reinterpret_cast<const float4 *>(om + (wr + 1) * kZmOW + c);
+        const float4 zp = *reinterpret_cast<const float4 *>(op + (wr + 1) * kZmOW + c);
         // value across the group edge: other[q - 1] (i0 = 0) or other[q + 4] (i0 = 1)
-        const float edge = ok[(w + 1) * kZmOW + (i0 ? c + 4 : c - 1)];
+        const float edge = ok[(wr + 1) * kZmOW + (i0 ? c + 4 : c - 1)];
         const float xm0 = i0 ? xc.x : edge, xm1 = i0 ? xc.y : xc.x, xm2 = i0 ? xc.z : xc.y,
                     xm3 = i0 ? xc.w : xc.z;
         const float xp0 = i0 ? xc.y : xc.x, xp1 = i0 ? xc.z : xc.y, xp2 = i0 ? xc.w : xc.z,

@@ -10,7 +10,7 @@
 //     q0 - 4 .. q0 + 131 (the y and x halos), into a ring of five planes, so
 //     planes k - 1, k, k + 1 are resident when plane k is updated;
 //   - the own colour's lambda, R and wall mask of plane k, into a ring of three.
-// Copies run two planes ahead of the update. Every neighbour then comes from
+// Copies run DIST (1 or 2) planes ahead of the update. Every neighbour then comes from
 // shared memory: each byte of the other colour leaves L2 about once per tile
 // (plus the halos), against five times in the row kernels.
 //
@@ -28,14 +28,16 @@ namespace qesb {
 
 constexpr int kZmQ = 128;            // colour cells per tile row
 constexpr int kZmOW = kZmQ + 8;      // staged other-colour row: q0 - 4 .. q0 + 131
-constexpr int kZmOtherSlots = 5;     // planes k - 1 .. k + 3
-constexpr int kZmOwnSlots = 3;       // planes k .. k + 2
+// Copies run DIST planes ahead of the update (1 or 2): the other colour's ring
+// holds planes k - 1 .. k + DIST + 1, the own colour's planes k .. k + DIST.
+__host__ __device__ constexpr int zm_other_slots(int dist) { return dist + 3; }
+__host__ __device__ constexpr int zm_own_slots(int dist) { return dist + 1; }
 
-template <int TY>
+template <int TR, int DIST>
 constexpr size_t zm_smem_bytes()
 {
-  return sizeof(float) * kZmOtherSlots * (TY + 2) * kZmOW + kZmOwnSlots * TY * kZmQ * (2 * sizeof(float) + 1) +
-         sizeof(float) * kZmOwnSlots * 64;
+  return sizeof(float) * zm_other_slots(DIST) * (TR + 2) * kZmOW +
+         zm_own_slots(DIST) * TR * kZmQ * (2 * sizeof(float) + 1) + sizeof(float) * zm_own_slots(DIST) * 64;
 }
 
 // 16-byte asynchronous copy global -> shared; src_bytes = 0 fills zeros and
@@ -47,23 +49,24 @@ __device__ __forceinline__ void zm_cp16(void *dst, const void *src, int src_byte
                : "memory");
 }
 __device__ __forceinline__ void zm_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void zm_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void zm_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 __device__ __forceinline__ void zm_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 template <int TY>
 struct ZmSmem {
-  float *oth;     // [kZmOtherSlots][TY + 2][kZmOW]
-  float *own;     // [kZmOwnSlots][TY][kZmQ]
-  float *rr;      // [kZmOwnSlots][TY][kZmQ]
-  uint8_t *mask;  // [kZmOwnSlots][TY][kZmQ]
-  float *inv;     // [kZmOwnSlots][64]: omega / (sum of the open faces' coefficients) per wall mask
-  __device__ ZmSmem(unsigned char *base)
+  float *oth;     // [other slots][TY + 2][kZmOW]
+  float *own;     // [own slots][TY][kZmQ]
+  float *rr;      // [own slots][TY][kZmQ]
+  uint8_t *mask;  // [own slots][TY][kZmQ]
+  float *inv;     // [own slots][64]: omega / (sum of the open faces' coefficients) per wall mask
+  __device__ ZmSmem(unsigned char *base, int nso, int nsw)
   {
     oth = reinterpret_cast<float *>(base);
-    own = oth + kZmOtherSlots * (TY + 2) * kZmOW;
-    rr = own + kZmOwnSlots * TY * kZmQ;
-    mask = reinterpret_cast<uint8_t *>(rr + kZmOwnSlots * TY * kZmQ);
-    inv = reinterpret_cast<float *>(mask + kZmOwnSlots * TY * kZmQ);
+    own = oth + nso * (TY + 2) * kZmOW;
+    rr = own + nsw * TY * kZmQ;
+    mask = reinterpret_cast<uint8_t *>(rr + nsw * TY * kZmQ);
+    inv = reinterpret_cast<float *>(mask + nsw * TY * kZmQ);
   }
 };
 
@@ -160,18 +163,20 @@ __device__ __forceinline__ void zm_stage(const ZmSmem<TR> &sm, const ZmCopies<TR
   zm_commit();
 }
 
-__device__ __forceinline__ int zm_wrap5(int x) { return x >= 5 ? x - 5 : x; }
-__device__ __forceinline__ int zm_wrap3(int x) { return x >= 3 ? x - 3 : x; }
+template <int N>
+__device__ __forceinline__ int zm_wrap(int x) { return x >= N ? x - N : x; }
 
-// TY warps per CTA, RW rows per warp (rows w, w + TY, ...): tiles of TY x RW rows.
-template <int COLOUR, int TY, int RW, bool MULTI, int MINB>
+// TY warps per CTA, RW rows per warp (rows w, w + TY, ...): tiles of TY x RW rows;
+// copies DIST planes ahead.
+template <int COLOUR, int TY, int RW, int DIST, bool MULTI, int MINB>
 __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
 {
-  constexpr int TR = TY * RW, NT = 32 * TY;
+  constexpr int TR = TY * RW, NT = 32 * TY, NSO = zm_other_slots(DIST), NSW = zm_own_slots(DIST);
+  static_assert(DIST == 1 || DIST == 2, "copies run one or two planes ahead");
   const int na = b.ctl->nactive;
   if (na <= 0) return;
   extern __shared__ __align__(16) unsigned char zm_raw[];
-  const ZmSmem<TR> sm(zm_raw);
+  const ZmSmem<TR> sm(zm_raw, NSO, NSW);
   const int lane = threadIdx.x, w = threadIdx.y, tid = lane + 32 * w;
   const int total = MULTI ? b.uoff[na] : sweep_units(b.one, kUnitTile);
   SplitDom D;
@@ -205,22 +210,22 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
     cp.init(D, j0, q0, tid);
 
     // Ring slots restart with each tile: the other colour's plane k0 - 1 + s
-    // sits in slot s mod 5, the own colour's plane k0 + s in slot s mod 3.
+    // sits in slot s mod NSO, the own colour's plane k0 + s in slot s mod NSW.
     // Prologue: other planes k0 - 1, k0 (and k0 + 1 with own k0) as one
-    // group, then the step of plane k0 + 1.
+    // group, then the steps of planes k0 + 1 .. k0 + DIST - 1.
     zm_stage_other<COLOUR, TR, NT>(sm, cp, D, k0 - 1, 0);
     zm_stage_other<COLOUR, TR, NT>(sm, cp, D, k0, 1);
-    zm_stage<COLOUR, TR, NT>(sm, cp, D, k0, k1, 2, 0);
-    zm_stage<COLOUR, TR, NT>(sm, cp, D, k0 + 1, k1, 3, 1);
+#pragma unroll
+    for (int d = 0; d < DIST; ++d) zm_stage<COLOUR, TR, NT>(sm, cp, D, k0 + d, k1, 2 + d, d);
     int om1 = 0, wk = 0;  // slots of the other colour's plane k - 1 and the own colour's plane k
     // the plane's six face coefficients, loaded one plane ahead
     float lv[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) lv[f] = __ldg(D.val + f * D.Z + k0);
-    for (int k = k0; k < k1; ++k, om1 = zm_wrap5(om1 + 1), wk = zm_wrap3(wk + 1)) {
-      zm_wait1();        // this thread's copies of plane k's step have landed
-      __syncthreads();   // everyone's; and every warp is done with plane k - 1
-      zm_stage<COLOUR, TR, NT>(sm, cp, D, k + 2, k1, zm_wrap5(om1 + 4), zm_wrap3(wk + 2));
+    for (int k = k0; k < k1; ++k, om1 = zm_wrap<NSO>(om1 + 1), wk = zm_wrap<NSW>(wk + 1)) {
+      zm_wait<DIST - 1>();  // this thread's copies of plane k's step have landed
+      __syncthreads();      // everyone's; and every warp is done with plane k - 1
+      zm_stage<COLOUR, TR, NT>(sm, cp, D, k + DIST, k1, zm_wrap<NSO>(om1 + DIST + 2), zm_wrap<NSW>(wk + DIST));
       D.ve = lv[0];
       D.vf = lv[1];
       D.vg = lv[2];
@@ -243,8 +248,8 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
         const int qlo = i0 ? 0 : 1;
         const int qhi = (D.X - 2 - i0) >> 1;  // inclusive
         const float *om = sm.oth + om1 * (TR + 2) * kZmOW;
-        const float *ok = sm.oth + zm_wrap5(om1 + 1) * (TR + 2) * kZmOW;
-        const float *op = sm.oth + zm_wrap5(om1 + 2) * (TR + 2) * kZmOW;
+        const float *ok = sm.oth + zm_wrap<NSO>(om1 + 1) * (TR + 2) * kZmOW;
+        const float *op = sm.oth + zm_wrap<NSO>(om1 + 2) * (TR + 2) * kZmOW;
         const int c = 4 + 4 * lane;  // column of q in a staged other-colour row
         const int so = wk * TR * kZmQ + wr * kZmQ + 4 * lane;
         const float4 o = *reinterpret_cast<const float4 *>(sm.own + so);

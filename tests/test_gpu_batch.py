@@ -41,7 +41,7 @@ def _batch(ws, tol, itermax, lam0s, variant=-1):
             s.close()
 
 
-@pytest.mark.parametrize("variant", [-1, 18, 21, 23, 26, 40, 41, 42, 44, 46])
+@pytest.mark.parametrize("variant", [-1, 18, 21, 23, 26, 40, 41, 42, 44, 46, 48, 50])
 def test_batch_matches_oracle_per_domain(variant):
     ws = _cities()
     rng = np.random.default_rng(11)

@@ -19,6 +19,8 @@
 // applies the ground mirror (Solver_CPU_RB.cpp:155-162) on plane 1 and its
 // last CTA runs the convergence poll (qesb_sweep.cuh).
 #pragma once
+#include <type_traits>
+
 #include "qesb_device.cuh"
 #include "qesb_sor_split.cuh"
 #include "qesb_sweep.cuh"
@@ -27,6 +29,7 @@
 namespace qesb {
 
 constexpr int kZmQ = 128;            // colour cells per tile row
+constexpr float kZmTinyF = 1.40129846e-45f;  // the smallest positive (subnormal) float
 constexpr int kZmOW = kZmQ + 8;      // staged other-colour row: q0 - 4 .. q0 + 131
 // Copies run DIST planes ahead of the update (1 or 2): the other colour's ring
 // holds planes k - 1 .. k + DIST + 1, the own colour's planes k .. k + DIST.
@@ -208,6 +211,18 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
     const int qn = (D.X + 1) >> 1;
     ZmCopies<TR, NT> cp;
     cp.init(D, j0, q0, tid);
+    // the lane's updated cells for rows of each x parity: q + t in [qlo, qhi],
+    // qlo = 1 - I0, qhi = (X - 2 - I0) / 2
+    unsigned up0 = 0, up1 = 0, upb0 = 0, upb1 = 0;  // bit / byte t: cell q + t
+#pragma unroll
+    for (int t4 = 0; t4 < 4; ++t4) {
+      const bool a0 = q + t4 >= 1 && q + t4 <= (D.X - 2) >> 1, a1 = q + t4 <= (D.X - 3) >> 1;
+      up0 |= a0 ? 1u << t4 : 0u;
+      up1 |= a1 ? 1u << t4 : 0u;
+      upb0 |= a0 ? 0xffu << (8 * t4) : 0u;
+      upb1 |= a1 ? 0xffu << (8 * t4) : 0u;
+    }
+    D.dmax_f = fmaxf(D.dmax_f, kZmTinyF);
 
     // Ring slots restart with each tile: the other colour's plane k0 - 1 + s
     // sits in slot s mod NSO, the own colour's plane k0 + s in slot s mod NSW.
@@ -238,19 +253,15 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
 #pragma unroll
         for (int f = 0; f < 6; ++f) lv[f] = __ldg(D.val + f * D.Z + k + 1);
       }
-#pragma unroll
-      for (int r = 0; r < RW; ++r) {
-        const int wr = w + r * TY, j = j0 + wr;
-        if (j > D.Y - 2) continue;  // warp-uniform
-        // Every lane computes (the staged rows are 128 cells wide, zero-filled
-        // past PQ); only cells inside [qlo, qhi] are updated and stored.
-        const int i0 = (COLOUR + j + k) & 1;
-        const int qlo = i0 ? 0 : 1;
-        const int qhi = (D.X - 2 - i0) >> 1;  // inclusive
-        const float *om = sm.oth + om1 * (TR + 2) * kZmOW;
-        const float *ok = sm.oth + zm_wrap<NSO>(om1 + 1) * (TR + 2) * kZmOW;
-        const float *op = sm.oth + zm_wrap<NSO>(om1 + 2) * (TR + 2) * kZmOW;
-        const int c = 4 + 4 * lane;  // column of q in a staged other-colour row
+      const float *om = sm.oth + om1 * (TR + 2) * kZmOW;
+      const float *ok = sm.oth + zm_wrap<NSO>(om1 + 1) * (TR + 2) * kZmOW;
+      const float *op = sm.oth + zm_wrap<NSO>(om1 + 2) * (TR + 2) * kZmOW;
+      const int c = 4 + 4 * lane;  // column of q in a staged other-colour row
+      // One row: I0 = (COLOUR + j + k) & 1, the x parity of the row's cells
+      // (cell q is i = 2q + I0), known at compile time in each branch.
+      auto row = [&](const int wr, const int j, auto i0_tag) {
+        constexpr int I0 = decltype(i0_tag)::value;
+        const unsigned upm = I0 ? up1 : up0;  // which of the lane's 4 cells are updated
         const int so = wk * TR * kZmQ + wr * kZmQ + 4 * lane;
         const float4 o = *reinterpret_cast<const float4 *>(sm.own + so);
         const float4 rr = *reinterpret_cast<const float4 *>(sm.rr + so);
@@ -260,21 +271,14 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
         const float4 yp = *reinterpret_cast<const float4 *>(ok + (wr + 2) * kZmOW + c);
         const float4 zm = *reinterpret_cast<const float4 *>(om + (wr + 1) * kZmOW + c);
         const float4 zp = *reinterpret_cast<const float4 *>(op + (wr + 1) * kZmOW + c);
-        // value across the group edge: other[q - 1] (i0 = 0) or other[q + 4] (i0 = 1)
-        const float edge = ok[(wr + 1) * kZmOW + (i0 ? c + 4 : c - 1)];
-        const float xm0 = i0 ? xc.x : edge, xm1 = i0 ? xc.y : xc.x, xm2 = i0 ? xc.z : xc.y,
-                    xm3 = i0 ? xc.w : xc.z;
-        const float xp0 = i0 ? xc.y : xc.x, xp1 = i0 ? xc.z : xc.y, xp2 = i0 ? xc.w : xc.z,
-                    xp3 = i0 ? edge : xc.w;
-        bool up[4];
-#pragma unroll
-        for (int t4 = 0; t4 < 4; ++t4) up[t4] = q + t4 >= qlo && q + t4 <= qhi;
+        // value across the group edge: other[q - 1] (I0 = 0) or other[q + 4] (I0 = 1)
+        const float edge = ok[(wr + 1) * kZmOW + (I0 ? c + 4 : c - 1)];
+        const float xmv[4] = {I0 ? xc.x : edge, I0 ? xc.y : xc.x, I0 ? xc.z : xc.y, I0 ? xc.w : xc.z};
+        const float xpv[4] = {I0 ? xc.y : xc.x, I0 ? xc.z : xc.y, I0 ? xc.w : xc.z, I0 ? edge : xc.w};
         const unsigned mk[4] = {m4 & 0xffu, (m4 >> 8) & 0xffu, (m4 >> 16) & 0xffu, m4 >> 24};
-        bool full = true;
-#pragma unroll
-        for (int t4 = 0; t4 < 4; ++t4) full &= (!up[t4] || mk[t4] == 63u);
+        // all-fluid: every updated cell has all six faces open (mask byte 63)
+        const bool full = ((m4 ^ 0x3f3f3f3fu) & (I0 ? upb1 : upb0)) == 0u;
         const float ov[4] = {o.x, o.y, o.z, o.w};
-        const float xmv[4] = {xm0, xm1, xm2, xm3}, xpv[4] = {xp0, xp1, xp2, xp3};
         const float ymv[4] = {ym.x, ym.y, ym.z, ym.w}, ypv[4] = {yp.x, yp.y, yp.z, yp.w};
         const float zmv[4] = {zm.x, zm.y, zm.z, zm.w}, zpv[4] = {zp.x, zp.y, zp.z, zp.w};
         const float rv[4] = {rr.x, rr.y, rr.z, rr.w};
@@ -288,23 +292,27 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
         } else {
 #pragma unroll
           for (int t4 = 0; t4 < 4; ++t4) {
-            const unsigned m_ = up[t4] ? mk[t4] : 63u;
+            const unsigned m_ = (upm >> t4) & 1u ? mk[t4] : 63u;
             const float e = (m_ & 1u) ? D.ve : 0.0f, f = (m_ & 2u) ? D.vf : 0.0f;
             const float g = (m_ & 4u) ? D.vg : 0.0f, hh = (m_ & 8u) ? D.vh : 0.0f;
             const float m = (m_ & 16u) ? D.vm : 0.0f, n = (m_ & 32u) ? D.vn : 0.0f;
-            nv[t4] = sinv[m_] * (e * xpv[t4] + f * xmv[t4] + g * ypv[t4] + hh * ymv[t4] +
-                                          m * zpv[t4] + n * zmv[t4] - rv[t4]) +
+            nv[t4] = sinv[m_] * (e * xpv[t4] + f * xmv[t4] + g * ypv[t4] + hh * ymv[t4] + m * zpv[t4] +
+                                 n * zmv[t4] - rv[t4]) +
                      D.c1 * ov[t4];
           }
         }
+        // Cells outside [qlo, qhi] keep their value. The error trigger: a
+        // change of at least the warp's max so far (thr >= the smallest
+        // subnormal, so unchanged cells, whose difference is exactly 0, never
+        // trigger; denormals are not flushed in this file, so any change is
+        // at least that).
         bool big = false;
 #pragma unroll
         for (int t4 = 0; t4 < 4; ++t4) {
-          nv[t4] = up[t4] ? nv[t4] : ov[t4];
-          // a cell whose value did not change cannot raise the maximum
-          big |= up[t4] && !(fabsf(nv[t4] - ov[t4]) < D.dmax_f) && nv[t4] != ov[t4];
+          nv[t4] = (upm >> t4) & 1u ? nv[t4] : ov[t4];
+          big |= !(fabsf(nv[t4] - ov[t4]) < D.dmax_f);
         }
-        if (q <= qhi) {
+        if (upm) {
           float *pw = D.L + COLOUR * D.CS + ((long)k * D.Y + j) * D.PQ + q;
           *reinterpret_cast<float4 *>(pw) = make_float4(nv[0], nv[1], nv[2], nv[3]);
         }
@@ -326,11 +334,18 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
 #pragma unroll
           for (int t4 = 0; t4 < 4; ++t4) {
             const double d = fabs((double)nv[t4] - (double)ov[t4]);
-            if (up[t4] && (d > D.dmax || d != d)) D.dmax = d;
+            if (d > D.dmax || d != d) D.dmax = d;
           }
           D.dmax = warp_max_d(D.dmax);
-          D.dmax_f = __double2float_rd(D.dmax);
+          D.dmax_f = fmaxf(__double2float_rd(D.dmax), kZmTinyF);
         }
+      };
+#pragma unroll
+      for (int r = 0; r < RW; ++r) {
+        const int wr = w + r * TY, j = j0 + wr;
+        if (j > D.Y - 2) continue;  // warp-uniform
+        if ((COLOUR + j + k) & 1) row(wr, j, std::integral_constant<int, 1>{});
+        else row(wr, j, std::integral_constant<int, 0>{});
       }
     }
     zm_wait0();

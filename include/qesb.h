@@ -176,6 +176,28 @@ qesb_status qesb_solve_batch(qesb_handle *const *handles, int n, int itermax, fl
  * rounding of atan2, cos and sin (the rest is the reference's arithmetic). */
 qesb_status qesb_wall_log_law(qesb_handle *h, float z0, float dz, float *u, float *v, float *w);
 
+/* Workspace files (NetCDF classic, 64-bit offsets): the fields of the solve's
+ * path with the dimension and variable names, layouts and attributes of the
+ * reference's workspace output (src/winds/WINDSOutputWorkspace.cpp:40-154):
+ * t(t); x_face, y_face, z_face, x, y, z; u, v, w, u0, v0, w0 (t, z_face, y_face,
+ * x_face); dz_array(z); icellflag, e, f, g, h, m, n (t, z, y, x), one record.
+ * netCDF-C reads the file like any NetCDF file. Host arrays in the reference
+ * layouts. */
+qesb_status qesb_workspace_write(const char *path, const qesb_grid *grid, double t, const float *u, const float *v,
+                                 const float *w, const float *u0, const float *v0, const float *w0,
+                                 const int *icellflag, const float *e, const float *f, const float *g,
+                                 const float *h, const float *m, const float *n);
+/* Grid of a workspace file (classic CDF-1 or CDF-2; NetCDF-4 files are
+ * refused with the conversion to use): base counts from the x, y, z
+ * dimensions, dx and dy (nullable) from the cell-centre coordinates. */
+qesb_status qesb_workspace_dims(const char *path, int *Nx, int *Ny, int *Nz, float *dx, float *dy);
+/* Reads a workspace's fields (record 0) into host arrays, any of which may be
+ * NULL; numeric types are converted. The role of the reference's coefficient
+ * re-read (src/winds/WINDSGeneralData.cpp:880-910), whole arrays. */
+qesb_status qesb_workspace_read(const char *path, int Nx, int Ny, int Nz, float *dz_array, int *icellflag,
+                                float *e, float *f, float *g, float *h, float *m, float *n, float *u0, float *v0,
+                                float *w0, float *u, float *v, float *w);
+
 /* Batch autotuner: times every sweep launch shape on the domain list that
  * qesb_solve_batch would run for these handles (same checks), a few launches
  * each from the handles' current lambda, and stores the fastest as

@@ -112,6 +112,10 @@ def lib() -> C.CDLL:
             "qesb_autotune_batch": ([C.POINTER(V), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int],
                                     C.c_int),
             "qesb_wall_log_law": ([V, C.c_float, C.c_float, V, V, V], C.c_int),
+            "qesb_workspace_write": ([C.c_char_p, C.POINTER(Grid), C.c_double] + [V] * 13, C.c_int),
+            "qesb_workspace_dims": ([C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
+            "qesb_workspace_read": ([C.c_char_p, C.c_int, C.c_int, C.c_int] + [V] * 14, C.c_int),
             "qesb_num_variants": ([], C.c_int),
             "qesb_set_option": ([V, C.c_char_p, C.c_int], C.c_int),
             "qesb_set_stream": ([V, V], C.c_int),
@@ -386,6 +390,32 @@ class Solver_B200:
         out = np.empty(self.domain.numCellCentered(), dtype=np.float32)
         check(lib().qesb_get_divergence(self._h, _ptr(out)))
         return out
+
+
+def workspace_write(path: str, wgd: "WINDSGeneralData", t: float = 0.0) -> None:
+    """qesb_workspace_write: wgd's winds, inputs and grid as a workspace file
+    (NetCDF classic) with the reference's variable names and layouts."""
+    g = wgd.domain.grid_struct()
+    arrs = [np.ascontiguousarray(a) for a in (wgd.u, wgd.v, wgd.w, wgd.u0, wgd.v0, wgd.w0, wgd.icellflag,
+                                              wgd.e, wgd.f, wgd.g, wgd.h, wgd.m, wgd.n)]
+    check(lib().qesb_workspace_write(os.fsencode(path), C.byref(g), float(t), *[_ptr(a) for a in arrs]))
+
+
+def workspace_read(path: str) -> "WINDSGeneralData":
+    """qesb_workspace_read: a workspace file (NetCDF classic) as a
+    WINDSGeneralData on its own grid (dz_array from the file)."""
+    Nx, Ny, Nz, dx, dy = C.c_int(), C.c_int(), C.c_int(), C.c_float(), C.c_float()
+    check(lib().qesb_workspace_dims(os.fsencode(path), C.byref(Nx), C.byref(Ny), C.byref(Nz), C.byref(dx),
+                                    C.byref(dy)))
+    dz = np.empty(Nz.value + 1, dtype=np.float32)
+    check(lib().qesb_workspace_read(os.fsencode(path), Nx.value, Ny.value, Nz.value, _ptr(dz),
+                                    *[None] * 13))
+    d = Domain(Nx.value, Ny.value, Nz.value, dx.value, dy.value, float(dz.min()), dz)
+    w = WINDSGeneralData(d)
+    check(lib().qesb_workspace_read(os.fsencode(path), Nx.value, Ny.value, Nz.value, None,
+                                    *[_ptr(a) for a in (w.icellflag, w.e, w.f, w.g, w.h, w.m, w.n, w.u0, w.v0,
+                                                        w.w0, w.u, w.v, w.w)]))
+    return w
 
 
 def autotune_batch(solvers) -> tuple[int, list[float]]:

@@ -775,7 +775,8 @@ def run_ensemble(args):
     config's 60), each at 36 wind directions 10 degrees apart. The 36 solves of
     a city run as one qesb_solve_batch (inputs built on the device beforehand
     and reported as setup_ms_per_solve; only the batch is timed, CUDA events): over-relaxed pre-phase warm start, reference
-    loop, correction; launch shape autotuned per grid. solves/s = all solves /
+    loop, correction; the list sweep's launch shape tuned once (qesb_autotune_batch
+    on the first city's 36 solves) and used for every city. solves/s = all solves /
     the sum of batch times; latency of a solve = device time from its batch's
     first sweep to the poll that ended it."""
     import torch
@@ -801,6 +802,7 @@ def run_ensemble(args):
     stream = torch.cuda.Stream(device=dev)
     lat, batch_ms, iters, pre_iters, cells_total = [], [], [], [], 0
     shapes, setup_ms = [], []
+    batch_shape = None  # the list sweep shape, tuned once on the first city's batch
     for d in shard.rank_share(nd, world, rank):  # cities of this rank; none crosses ranks
         Nx, Ny, Nz = dims[d]
         dom = qesb.Domain(Nx, Ny, Nz, 2.0, 2.0, 1.0, qesb.city_dz(Nz, 1.0, 1.03))
@@ -832,7 +834,9 @@ def run_ensemble(args):
                 s.set_prephase(om, PRE_TOL, ITERMAX)
             torch.cuda.synchronize(dev)
             setup_ms.append(1e3 * (time.perf_counter() - t_set))
-            solvers[0].autotune()
+            if batch_shape is None:
+                batch_shape, _ = qesb.autotune_batch(solvers)
+            solvers[0].set_option("batch_variant", batch_shape)
             nf = dom.numFaceCentered()
             outs = [[torch.empty(nf, dtype=torch.float32, device=f"cuda:{dev}") for _ in range(3)]
                     for _ in range(ndir)]
@@ -874,7 +878,7 @@ def run_ensemble(args):
         "config": {"workload": f"{nd} cities, Nx,Ny ~ U[64,256], Nz ~ U[32,96], x {ndir} directions",
                    "solves": n, "batch": ndir, "tol": TOL, "itermax": ITERMAX,
                    "warm_start": "over-relaxed pre-phase, omega = 2 - 7.5/max(Nx, Ny) within [1.85, 1.97], "
-                                 f"to {PRE_TOL}", "cells_total": cells_total},
+                                 f"to {PRE_TOL}", "cells_total": cells_total, "batch_variant": batch_shape},
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
         "setup_ms_per_solve": setup_total / n,
         "setup": "inputs (flags, wall coefficients, winds) built on the device by qesb_city_build_device "

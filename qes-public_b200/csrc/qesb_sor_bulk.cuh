@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(32 * W) k_sor_bulk(BulkArgs b)
     bool up[4];
 #pragma unroll
     for (int t4 = 0; t4 < 4; ++t4) up[t4] = q + t4 >= qlo && q + t4 <= qhi;
-    const unsigned mk[4] = {m4 & 0xffu, (m4 >> 8) & 0xffu, (m4 >> 16) & 0xffu, m4 >> 24};
+    const unsigned mk[4] = {m4 & 0x3fu, (m4 >> 8) & 0x3fu, (m4 >> 16) & 0x3fu, (m4 >> 24) & 0x3fu};
     bool full = true;
 #pragma unroll
     for (int t4 = 0; t4 < 4; ++t4) full &= (!up[t4] || mk[t4] == 63u);

@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(32 * RPB, MINB) k_sor_split(SweepArgs b)
           zm[u] = __ldg(pzm + q);
           zp[u] = __ldg(pzp + q);
           rr[u] = __ldg(pr + q);
-          mk[u] = __ldg(pm + q);
+          mk[u] = __ldg(pm + q) & 63u;  // 6-bit wall mask: table indexes stay inside 64 entries
         }
       }
       bool full = true;
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(32 * RPB, MINB) k_sor_split4(SweepArgs b)
       bool up[4];
 #pragma unroll
       for (int t = 0; t < 4; ++t) up[t] = live && q + t >= qlo && q + t <= qhi;
-      unsigned mk[4] = {m4 & 0xffu, (m4 >> 8) & 0xffu, (m4 >> 16) & 0xffu, m4 >> 24};
+      unsigned mk[4] = {m4 & 0x3fu, (m4 >> 8) & 0x3fu, (m4 >> 16) & 0x3fu, (m4 >> 24) & 0x3fu};
       bool full = true;
 #pragma unroll
       for (int t = 0; t < 4; ++t) full &= (!up[t] || mk[t] == 63u);

@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(NT) k_sor_tiled(TiledArgs a)
           const float lyp = sl[sp + me + BX];
           const float lzm = sl[sd + me];
           const float lzp = sl[su + me];
-          const unsigned mk = sm[sp + me];
+          const unsigned mk = sm[sp + me] & 63u;  // 6-bit wall mask: tb index stays inside the table
           const float e = (mk & 1u) ? ve : 0.0f, f = (mk & 2u) ? vf : 0.0f;
           const float g = (mk & 4u) ? vg : 0.0f, hh = (mk & 8u) ? vh : 0.0f;
           const float m = (mk & 16u) ? vm : 0.0f, n = (mk & 32u) ? vn : 0.0f;

@@ -275,7 +275,8 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
         const float edge = ok[(wr + 1) * kZmOW + (I0 ? c + 4 : c - 1)];
         const float xmv[4] = {I0 ? xc.x : edge, I0 ? xc.y : xc.x, I0 ? xc.z : xc.y, I0 ? xc.w : xc.z};
         const float xpv[4] = {I0 ? xc.y : xc.x, I0 ? xc.z : xc.y, I0 ? xc.w : xc.z, I0 ? edge : xc.w};
-        const unsigned mk[4] = {m4 & 0xffu, (m4 >> 8) & 0xffu, (m4 >> 16) & 0xffu, m4 >> 24};
+        // 6-bit wall masks (the & keeps every table index inside its 64 entries)
+        const unsigned mk[4] = {m4 & 0x3fu, (m4 >> 8) & 0x3fu, (m4 >> 16) & 0x3fu, (m4 >> 24) & 0x3fu};
         // all-fluid: every updated cell has all six faces open (mask byte 63)
         const bool full = ((m4 ^ 0x3f3f3f3fu) & (I0 ? upb1 : upb0)) == 0u;
         const float ov[4] = {o.x, o.y, o.z, o.w};

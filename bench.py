@@ -582,10 +582,74 @@ def run_b200(args):
                     ho[q].copy_(o[q], non_blocking=True)
         return st, n
 
-    ms_e2e, _, _, _ = timed(e2e_step, max(1, args.steps // 2), 1)
+    ms_e2e_serial, _, _, _ = timed(e2e_step, max(1, args.steps // 2), 1)
     torch.cuda.synchronize(dev)
-    ms_e2e = max_over_ranks(ms_e2e)
-    e2e_ok = all(torch.equal(ho[0], o[0].cpu()) for ho, o in zip(host_out, outs))
+    ms_e2e_serial = max_over_ranks(ms_e2e_serial)
+
+    # Pipelined, as a stream of batches runs: two solver sets on two streams.
+    # While one batch solves and its winds are read back, a second host thread
+    # loads the next batch's inputs through the same public call
+    # (qesb_set_inputs, host -> device, blocking that thread only). Every
+    # step's copies still run inside the timed region, the first batch's
+    # upload before any overlap; only their order against the other batch's
+    # solve changes.
+    import threading
+
+    stream2 = torch.cuda.Stream(device=dev)
+    solvers2 = [qesb.Solver_B200(w.domain, TOL, device=dev) for w in cities]
+    for s2 in solvers2:
+        s2.set_stream(stream2.cuda_stream)
+        s2.set_prephase(PRE_OMEGA, PRE_TOL, ITERMAX)
+    solvers2[0].set_option("batch_variant", batch_variant)
+    sets, streams = [solvers, solvers2], [stream, stream2]
+    outs2 = [[torch.empty(nf, dtype=torch.float32, device=f"cuda:{dev}") for _ in range(3)] for _ in range(B)]
+    set_outs = [outs, outs2]
+    set_uvw = [uvw, [[o[q].data_ptr() for o in outs2] for q in range(3)]]
+    host_out2 = [[torch.empty(nf, dtype=torch.float32, pin_memory=True) for _ in range(3)] for _ in range(B)]
+    set_host_out = [host_out, host_out2]
+
+    def load(k):
+        for s_, ins in zip(sets[k], host_in):
+            qesb.check(qesb.lib().qesb_set_inputs(s_._h, *[a.ctypes.data for a in ins]))
+
+    def solve_read(k):
+        for s_ in sets[k]:
+            s_.set_prephase(PRE_OMEGA, PRE_TOL, ITERMAX)
+            s_.resetLambda()
+        st_ = qesb.solve_batch(sets[k], ITERMAX, *set_uvw[k])
+        with torch.cuda.stream(streams[k]):
+            for o, ho in zip(set_outs[k], set_host_out[k]):
+                for q in range(3):
+                    ho[q].copy_(o[q], non_blocking=True)
+        return st_
+
+    def pipelined(nsteps):
+        load(0)
+        for i in range(nsteps):
+            cur = i % 2
+            th = threading.Thread(target=load, args=(1 - cur,)) if i + 1 < nsteps else None
+            if th:
+                th.start()
+            solve_read(cur)
+            if th:
+                th.join()
+        torch.cuda.synchronize(dev)
+
+    pipelined(2)  # warm-up
+    k_e2e = max(2, args.steps // 2)
+    barrier()
+    torch.cuda.synchronize(dev)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    pipelined(k_e2e)
+    p1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = max_over_ranks(p0.elapsed_time(p1) / k_e2e)
+    last = (k_e2e - 1) % 2
+    e2e_ok = all(torch.equal(ho[0], o[0].cpu()) for ho, o in zip(set_host_out[last], set_outs[last]))
+    e2e_ok = e2e_ok and all(torch.equal(a[0], b[0]) for a, b in zip(set_outs[last], outs if last else outs2))
+    for s2 in solvers2:
+        s2.close()
 
     # ---- roofline of the dominant kernel: the list sweep of the headline step ---------
     # The headline step is ~97 % red/black list sweeps. Its domain-iterations
@@ -743,7 +807,11 @@ def run_b200(args):
             "first_domain_ms": ms_first,
             "speedup_vs_reference_gpu": (ref_gpu["ms"] / ms_first) if ref_gpu and "ms" in ref_gpu else None,
             "e2e": {"value": ms_e2e / B, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "matches_device_result": bool(e2e_ok)},
+                    "matches_device_result": bool(e2e_ok),
+                    "how": "public API (qesb_set_inputs from pinned host arrays, qesb_solve_batch, winds read "
+                           "back to pinned host memory) on two solver sets: the next batch's inputs load on a "
+                           "second host thread while the current batch solves; device-timed over the steps",
+                    "serial_value": ms_e2e_serial / B},
             "headline_sweep": headline_sweep,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,

@@ -2,6 +2,8 @@
 // accumulation in TMEM) for the 3D-convolution network, and their C ABI.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <mutex>
+#include <map>
 
 #include <algorithm>
 #include <cstdint>
@@ -152,6 +154,7 @@ struct ConvOut {
   const float *bias;      // [N] (nullable)
   int relu;               // ReLU in the epilogue
   const __nv_bfloat16 *mask;  // [V][N] (nullable): zero where mask <= 0 (gradient through a ReLU)
+  float *acc;             // split-K: [V][N] FP32 partial sums (atomic adds), epilogue left to k_conv_finish
 };
 
 // Y[v][n] = epilogue( sum_k A[v][k] * Bm[n][k] ), A the implicit im2col of
@@ -163,6 +166,8 @@ template <int N>
 __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int sign, const __nv_bfloat16 *__restrict__ Bm,
                                                    int Kp, ConvOut out, int *err)
 {
+  // split-K (gridDim.y > 1, small grids): CTA y sums the K chunks [jb, je)
+  // and adds its partial to out.acc; k_conv_finish applies the epilogue.
   constexpr uint32_t SA = 128 * 64 * 2, SB = N * 64 * 2, STAGE = SA + SB;
   constexpr uint32_t NCOLS = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
   extern __shared__ __align__(1024) uint8_t sm[];
@@ -196,11 +201,12 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
     ry[i] = (int)((vv / g.W) % g.H);
     rz[i] = (int)(vv / ((long)g.W * g.H));
   }
-  const int nk = Kp / 64;
+  const int nk_all = Kp / 64, per = (nk_all + gridDim.y - 1) / gridDim.y;
+  const int jb = blockIdx.y * per, je = min(nk_all, jb + per), nk = je > jb ? je - jb : 0;
   bool ok = true;
-  for (int j = 0; j < nk && ok; ++j) {
-    const int s = j & 1;
-    if (j >= 2) ok = umma::mbar_wait(&mbar[s], ((j - 2) >> 1) & 1, kWaitLimit);
+  for (int jl = 0; jl < nk && ok; ++jl) {
+    const int j = jb + jl, s = jl & 1;
+    if (jl >= 2) ok = umma::mbar_wait(&mbar[s], ((jl - 2) >> 1) & 1, kWaitLimit);
     if (!ok) break;
     uint8_t *sa = sm + s * STAGE, *sb = sa + SA;
     // A: rows m = tid/8 + 16 i, k-group g8
@@ -230,14 +236,25 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
 #pragma unroll
       for (int kk = 0; kk < 4; ++kk)
         umma::mma_bf16(tmem, umma::desc(a0 + kk * 256, 128, 1024), umma::desc(b0 + kk * 256, 128, 1024), idesc,
-                       (j > 0 || kk > 0) ? 1u : 0u);
+                       (jl > 0 || kk > 0) ? 1u : 0u);
       umma::mma_commit(&mbar[s]);
     }
   }
-  if (ok) ok = umma::mbar_wait(&mbar[(nk - 1) & 1], ((nk - 1) >> 1) & 1, kWaitLimit);
+  if (ok && nk > 0) ok = umma::mbar_wait(&mbar[(nk - 1) & 1], ((nk - 1) >> 1) & 1, kWaitLimit);
   umma::fence_after_sync();
   if (!ok) {
     if (lane == 0) atomicExch(err, 1);
+  } else if (out.acc) {
+    const long v = m0 + warp * 32 + lane;
+    if (nk > 0)
+      for (int c0 = 0; c0 < N; c0 += 8) {
+        float a[8];
+        umma::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, a);
+        if (v < g.V) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) atomicAdd(out.acc + v * N + c0 + q, a[q]);
+        }
+      }
   } else {
     const long v = m0 + warp * 32 + lane;
     for (int c0 = 0; c0 < N; c0 += 8) {
@@ -534,19 +551,80 @@ __global__ void __launch_bounds__(128) k_conv_wgrad(ConvIn in, ConvGeom g, const
   }
 }
 
+// Epilogue of a split-K convolution: y = act(acc + bias), as k_conv_igemm's.
+__global__ void k_conv_finish(const float *__restrict__ acc, long V, int N, ConvOut out)
+{
+  for (long i = threadIdx.x + (long)blockIdx.x * blockDim.x; i < V * N; i += (long)gridDim.x * blockDim.x) {
+    float a = acc[i];
+    if (out.bias) a += __ldg(out.bias + (int)(i % N));
+    if (out.relu) a = fmaxf(a, 0.0f);
+    if (out.mask && !(__bfloat162float(out.mask[i]) > 0.0f)) a = 0.0f;
+    if (out.yf) out.yf[i] = a;
+    else out.y[i] = __float2bfloat16_rn(a);
+  }
+}
+
+// FP32 partial-sum buffers of the split-K convolutions, one per (device,
+// stream) so that convolutions on different streams never share one; grown on
+// demand (the network's small levels: a few MB) and kept for the process.
+struct AccBuf {
+  float *p = nullptr;
+  size_t cap = 0;
+};
+std::mutex g_acc_mu;
+std::map<std::pair<int, cudaStream_t>, AccBuf> g_acc;
+
+qesb_status acc_buffer(int dev, cudaStream_t s, size_t need, float **out)
+{
+  std::lock_guard<std::mutex> lk(g_acc_mu);
+  AccBuf &b = g_acc[{dev, s}];
+  if (b.cap < need) {
+    if (b.p) {
+      cudaStreamSynchronize(s);  // the old buffer may still be read by this stream's work
+      cudaFree(b.p);
+    }
+    b.p = nullptr;
+    b.cap = 0;
+    cudaError_t e = cudaMalloc((void **)&b.p, need * sizeof(float));
+    if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv split-K buffer: %s", cudaGetErrorString(e));
+    b.cap = need;
+  }
+  *out = b.p;
+  return QESB_OK;
+}
+
 template <int N>
 qesb_status launch_conv(const ConvIn &in, const ConvGeom &g, int sign, const __nv_bfloat16 *Bm, int Kp,
                         const ConvOut &out, int *err, cudaStream_t s)
 {
   constexpr int smem = 2 * (128 * 64 * 2 + N * 64 * 2);
-  static bool attr = false;
-  if (!attr) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  static bool attr[64] = {};
+  if (!attr[dev & 63]) {
     cudaError_t e = cudaFuncSetAttribute(k_conv_igemm<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv attr: %s", cudaGetErrorString(e));
-    attr = true;
+    attr[dev & 63] = true;
   }
   const unsigned blocks = (unsigned)((g.V + 127) / 128);
-  k_conv_igemm<N><<<blocks, 128, smem, s>>>(in, g, sign, Bm, Kp, out, err);
+  // Small grids (fewer CTAs than about two per SM): split the K chunks over
+  // grid.y, at least 4 chunks per split, partial sums in FP32.
+  const int nk = Kp / 64;
+  int split = 1;
+  if (blocks < 296) split = std::max(1, std::min((int)(296 / blocks), nk / 4));
+  ConvOut o = out;
+  if (split > 1) {
+    const size_t need = (size_t)g.V * N;
+    const qesb_status st = acc_buffer(dev, s, need, &o.acc);
+    if (st != QESB_OK) return st;
+    cudaError_t e = cudaMemsetAsync(o.acc, 0, need * sizeof(float), s);
+    if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv split-K clear: %s", cudaGetErrorString(e));
+  }
+  k_conv_igemm<N><<<dim3(blocks, split), 128, smem, s>>>(in, g, sign, Bm, Kp, o, err);
+  if (split > 1) {
+    const long total = g.V * N;
+    k_conv_finish<<<(unsigned)std::min<long>((total + 255) / 256, 148L * 16), 256, 0, s>>>(o.acc, g.V, N, out);
+  }
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));
 }

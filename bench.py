@@ -627,12 +627,22 @@ def run_b200(args):
         load(0)
         for i in range(nsteps):
             cur = i % 2
-            th = threading.Thread(target=load, args=(1 - cur,)) if i + 1 < nsteps else None
+            failed = []
+
+            def load_next(k=1 - cur):
+                try:
+                    load(k)
+                except Exception as ex:  # noqa: BLE001  (re-raised below, in the timing thread)
+                    failed.append(ex)
+
+            th = threading.Thread(target=load_next) if i + 1 < nsteps else None
             if th:
                 th.start()
             solve_read(cur)
             if th:
                 th.join()
+            if failed:
+                raise failed[0]
         torch.cuda.synchronize(dev)
 
     pipelined(2)  # warm-up

@@ -25,6 +25,7 @@
 // Coordinates follow WINDSOutputWorkspace.cpp:50-88: x, y, z are the cell
 // centres (Domain::x, y, z); x_face = {x[0] - dx, x[0], ..., x[nx-2]},
 // y_face = {y[0] - dy, y[0] + dy, ..., y[ny-2] + dy}, z_face = Domain::z_face.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -139,7 +140,8 @@ struct RVar {
   uint64_t vsize, begin;
 };
 struct NcFile {
-  std::vector<unsigned char> bytes;
+  std::string path;
+  uint64_t size = 0;  // bytes in the file
   uint64_t numrecs = 0, recsize = 0;
   int rec_dim = -1;
   std::vector<RDim> dims;
@@ -161,33 +163,31 @@ qesb_status skip_atts(In &in)
   return in.ok ? QESB_OK : qesb_fail(QESB_ERR_ARG, "workspace: truncated header");
 }
 
-qesb_status nc_open(const char *path, NcFile &f)
+// Parses the header in bytes [0, n) of a file of `size` bytes; *truncated
+// reports a header that runs past n (the caller then reads a longer prefix).
+qesb_status nc_parse(const unsigned char *b, size_t n, NcFile &f, bool *truncated)
 {
-  FILE *fp = std::fopen(path, "rb");
-  if (!fp) return qesb_fail(QESB_ERR_ARG, "workspace: cannot open %s", path);
-  std::fseek(fp, 0, SEEK_END);
-  const long fsize = std::ftell(fp);
-  std::fseek(fp, 0, SEEK_SET);
-  f.bytes.resize(fsize > 0 ? (size_t)fsize : 0);
-  const size_t got = fsize > 0 ? std::fread(f.bytes.data(), 1, (size_t)fsize, fp) : 0;
-  std::fclose(fp);
-  if (got != f.bytes.size() || f.bytes.size() < 8) return qesb_fail(QESB_ERR_ARG, "workspace: cannot read %s", path);
-  const unsigned char *b = f.bytes.data();
-  if (b[0] == 0x89 && b[1] == 'H' && b[2] == 'D' && b[3] == 'F')
+  *truncated = false;
+  f.dims.clear();
+  f.vars.clear();
+  f.rec_dim = -1;
+  f.recsize = 0;
+  const char *path = f.path.c_str();
+  if (n >= 4 && b[0] == 0x89 && b[1] == 'H' && b[2] == 'D' && b[3] == 'F')
     return qesb_fail(QESB_ERR_ARG,
                      "workspace: %s is NetCDF-4 (HDF5); convert it to the classic format first "
                      "(nccopy -k 2 in.nc out.nc)",
                      path);
-  if (b[0] != 'C' || b[1] != 'D' || b[2] != 'F' || (b[3] != 1 && b[3] != 2))
+  if (n < 8 || b[0] != 'C' || b[1] != 'D' || b[2] != 'F' || (b[3] != 1 && b[3] != 2))
     return qesb_fail(QESB_ERR_ARG, "workspace: %s is not a NetCDF classic (CDF-1 / CDF-2) file", path);
   const bool off64 = b[3] == 2;
-  In in{b + 4, b + f.bytes.size()};
+  In in{b + 4, b + n};
   f.numrecs = in.u32();
   if (f.numrecs == 0xFFFFFFFFu) return qesb_fail(QESB_ERR_ARG, "workspace: streaming record count not supported");
-  uint32_t tag = in.u32(), n = in.u32();
-  if (!(tag == 0 && n == 0)) {
+  uint32_t tag = in.u32(), cnt = in.u32();
+  if (!(tag == 0 && cnt == 0)) {
     if (tag != kTagDim) return qesb_fail(QESB_ERR_ARG, "workspace: bad dimension list");
-    for (uint32_t d = 0; d < n && in.ok; ++d) {
+    for (uint32_t d = 0; d < cnt && in.ok; ++d) {
       RDim dim;
       dim.name = in.name();
       dim.len = in.u32();
@@ -195,27 +195,36 @@ qesb_status nc_open(const char *path, NcFile &f)
       f.dims.push_back(dim);
     }
   }
-  CKS(skip_atts(in));
+  if (!in.ok) return *truncated = true, QESB_ERR_ARG;
+  {
+    const qesb_status st = skip_atts(in);
+    if (!in.ok) return *truncated = true, QESB_ERR_ARG;
+    if (st != QESB_OK) return st;
+  }
   tag = in.u32();
-  n = in.u32();
-  if (!(tag == 0 && n == 0)) {
+  cnt = in.u32();
+  if (!(tag == 0 && cnt == 0) && in.ok) {
     if (tag != kTagVar) return qesb_fail(QESB_ERR_ARG, "workspace: bad variable list");
-    for (uint32_t v = 0; v < n && in.ok; ++v) {
+    for (uint32_t v = 0; v < cnt && in.ok; ++v) {
       RVar var;
       var.name = in.name();
       const uint32_t nd = in.u32();
       for (uint32_t d = 0; d < nd && in.ok; ++d) var.dims.push_back(in.u32());
-      CKS(skip_atts(in));
+      const qesb_status st = skip_atts(in);
+      if (!in.ok) break;
+      if (st != QESB_OK) return st;
       var.type = (int)in.u32();
       var.vsize = in.u32();
       var.begin = off64 ? in.u64() : in.u32();
+      if (!in.ok) break;
       if (!type_size(var.type)) return qesb_fail(QESB_ERR_ARG, "workspace: bad type of %s", var.name.c_str());
       for (uint32_t d : var.dims)
         if (d >= f.dims.size()) return qesb_fail(QESB_ERR_ARG, "workspace: bad dimension id in %s", var.name.c_str());
       f.vars.push_back(var);
     }
   }
-  if (!in.ok) return qesb_fail(QESB_ERR_ARG, "workspace: truncated header");
+  if (!in.ok) return *truncated = true, QESB_ERR_ARG;
+
   // record size: the record variables' slabs (one record variable: unpadded)
   int nrec = 0;
   for (const RVar &v : f.vars)
@@ -231,6 +240,35 @@ qesb_status nc_open(const char *path, NcFile &f)
         f.recsize = c;
       }
   return QESB_OK;
+}
+
+// Opens a classic file: its size and header (read as a prefix that grows until
+// the header fits); the data stay on disk until read_var.
+qesb_status nc_open(const char *path, NcFile &f)
+{
+  f.path = path;
+  FILE *fp = std::fopen(path, "rb");
+  if (!fp) return qesb_fail(QESB_ERR_ARG, "workspace: cannot open %s", path);
+  std::fseek(fp, 0, SEEK_END);
+  const long fsize = std::ftell(fp);
+  f.size = fsize > 0 ? (uint64_t)fsize : 0;
+  std::vector<unsigned char> buf;
+  for (uint64_t cap = 1 << 16;; cap *= 8) {
+    const size_t n = (size_t)std::min<uint64_t>(cap, f.size);
+    buf.resize(n);
+    std::fseek(fp, 0, SEEK_SET);
+    if (std::fread(buf.data(), 1, n, fp) != n) {
+      std::fclose(fp);
+      return qesb_fail(QESB_ERR_ARG, "workspace: cannot read %s", path);
+    }
+    bool truncated = false;
+    const qesb_status st = nc_parse(buf.data(), n, f, &truncated);
+    if (st == QESB_OK || !truncated || n == f.size) {
+      std::fclose(fp);
+      if (truncated) return qesb_fail(QESB_ERR_ARG, "workspace: truncated header in %s", path);
+      return st;
+    }
+  }
 }
 
 const RVar *find_var(const NcFile &f, const char *name)
@@ -260,33 +298,48 @@ qesb_status read_var(const NcFile &f, const char *name, size_t want, int as, voi
     return qesb_fail(QESB_ERR_ARG, "workspace: %s holds %llu values, the grid needs %zu", name,
                      (unsigned long long)count, want);
   const int ts = type_size(v->type);
-  if (v->begin + count * ts > f.bytes.size()) return qesb_fail(QESB_ERR_ARG, "workspace: %s runs past the file", name);
-  const unsigned char *src = f.bytes.data() + v->begin;
-  for (size_t i = 0; i < want; ++i) {
-    const unsigned char *e = src + i * ts;
-    double x = 0.0;
-    switch (v->type) {
-    case kByte: x = (double)(int8_t)e[0]; break;
-    case kShort: x = (double)(int16_t)((uint16_t)e[0] << 8 | e[1]); break;
-    case kInt: x = (double)(int32_t)((uint32_t)e[0] << 24 | (uint32_t)e[1] << 16 | (uint32_t)e[2] << 8 | e[3]); break;
-    case kFloat: {
-      const uint32_t u = (uint32_t)e[0] << 24 | (uint32_t)e[1] << 16 | (uint32_t)e[2] << 8 | e[3];
-      float fl;
-      std::memcpy(&fl, &u, 4);
-      x = fl;
-      break;
-    }
-    case kDouble: {
-      uint64_t u = 0;
-      for (int k = 0; k < 8; ++k) u = u << 8 | e[k];
-      std::memcpy(&x, &u, 8);
-      break;
-    }
-    default: return qesb_fail(QESB_ERR_ARG, "workspace: %s has a text type", name);
-    }
-    if (as == kFloat) static_cast<float *>(out)[i] = (float)x;
-    else static_cast<int *>(out)[i] = (int)x;
+  if (v->begin + count * ts > f.size) return qesb_fail(QESB_ERR_ARG, "workspace: %s runs past the file", name);
+  if (v->type == kChar) return qesb_fail(QESB_ERR_ARG, "workspace: %s has a text type", name);
+  FILE *fp = std::fopen(f.path.c_str(), "rb");
+  if (!fp) return qesb_fail(QESB_ERR_ARG, "workspace: cannot open %s", f.path.c_str());
+  if (fseeko(fp, (off_t)v->begin, SEEK_SET) != 0) {
+    std::fclose(fp);
+    return qesb_fail(QESB_ERR_ARG, "workspace: cannot seek to %s", name);
   }
+  constexpr size_t kChunk = 1 << 20;  // values per read
+  std::vector<unsigned char> buf(std::min(want, kChunk) * ts);
+  for (size_t i0 = 0; i0 < want; i0 += kChunk) {
+    const size_t n = std::min(kChunk, want - i0);
+    if (std::fread(buf.data(), 1, n * ts, fp) != n * ts) {
+      std::fclose(fp);
+      return qesb_fail(QESB_ERR_ARG, "workspace: short read of %s", name);
+    }
+    for (size_t i = 0; i < n; ++i) {
+      const unsigned char *e = buf.data() + i * ts;
+      double x = 0.0;
+      switch (v->type) {
+      case kByte: x = (double)(int8_t)e[0]; break;
+      case kShort: x = (double)(int16_t)((uint16_t)e[0] << 8 | e[1]); break;
+      case kInt: x = (double)(int32_t)((uint32_t)e[0] << 24 | (uint32_t)e[1] << 16 | (uint32_t)e[2] << 8 | e[3]); break;
+      case kFloat: {
+        const uint32_t u = (uint32_t)e[0] << 24 | (uint32_t)e[1] << 16 | (uint32_t)e[2] << 8 | e[3];
+        float fl;
+        std::memcpy(&fl, &u, 4);
+        x = fl;
+        break;
+      }
+      default: {
+        uint64_t u = 0;
+        for (int k = 0; k < 8; ++k) u = u << 8 | e[k];
+        std::memcpy(&x, &u, 8);
+        break;
+      }
+      }
+      if (as == kFloat) static_cast<float *>(out)[i0 + i] = (float)x;
+      else static_cast<int *>(out)[i0 + i] = (int)x;
+    }
+  }
+  std::fclose(fp);
   return QESB_OK;
 }
 
@@ -389,30 +442,35 @@ qesb_status qesb_workspace_write(const char *path, const qesb_grid *g, double t,
   }
   // data: fixed-size variables, then the one record
   uint64_t pos = o.b.size();
-  for (WVar &wv : vars)
-    if (!wv.record) {
-      for (int s = 0; s < 8; ++s) o.b[wv.begin_pos + s] = (unsigned char)(pos >> (56 - 8 * s));
-      pos += wv.vsize;
-    }
-  for (WVar &wv : vars)
-    if (wv.record) {
-      for (int s = 0; s < 8; ++s) o.b[wv.begin_pos + s] = (unsigned char)(pos >> (56 - 8 * s));
-      pos += wv.vsize;
-    }
-  const size_t header = o.b.size();
-  o.b.resize(pos, 0);
-  size_t at = header;
   for (int pass = 0; pass < 2; ++pass)
-    for (const WVar &wv : vars)
+    for (WVar &wv : vars)
       if (wv.record == (pass == 1)) {
-        put_be(o.b.data() + at, wv.data, wv.count, type_size(wv.type));
-        at += wv.vsize;
+        for (int k = 0; k < 8; ++k) o.b[wv.begin_pos + k] = (unsigned char)(pos >> (56 - 8 * k));
+        pos += wv.vsize;
       }
   FILE *fp = std::fopen(path, "wb");
   if (!fp) return qesb_fail(QESB_ERR_ARG, "qesb_workspace_write: cannot create %s", path);
-  const size_t put = std::fwrite(o.b.data(), 1, o.b.size(), fp);
+  bool good = std::fwrite(o.b.data(), 1, o.b.size(), fp) == o.b.size();
+  // each variable in big-endian chunks, then its padding to vsize
+  constexpr size_t kChunk = 1 << 20;  // values per write
+  std::vector<unsigned char> buf;
+  for (int pass = 0; pass < 2 && good; ++pass)
+    for (const WVar &wv : vars) {
+      if (wv.record != (pass == 1) || !good) continue;
+      const int ts = type_size(wv.type);
+      const unsigned char *src = static_cast<const unsigned char *>(wv.data);
+      for (size_t i0 = 0; i0 < wv.count && good; i0 += kChunk) {
+        const size_t n = std::min(kChunk, wv.count - i0);
+        buf.resize(n * ts);
+        put_be(buf.data(), src + i0 * ts, n, ts);
+        good = std::fwrite(buf.data(), 1, n * ts, fp) == n * ts;
+      }
+      const size_t padn = wv.vsize - wv.count * ts;
+      const unsigned char zeros[4] = {0, 0, 0, 0};
+      if (good && padn) good = std::fwrite(zeros, 1, padn, fp) == padn;
+    }
   const int cl = std::fclose(fp);
-  if (put != o.b.size() || cl != 0) return qesb_fail(QESB_ERR_ARG, "qesb_workspace_write: write to %s failed", path);
+  if (!good || cl != 0) return qesb_fail(QESB_ERR_ARG, "qesb_workspace_write: write to %s failed", path);
   return QESB_OK;
 }
 

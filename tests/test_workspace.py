@@ -103,3 +103,37 @@ def test_rejects_netcdf4_and_wrong_grids(tmp_path):
     e = np.empty(10, np.float32)
     st = qesb.lib().qesb_workspace_read(path.encode(), 31, 26, 12, None, None, e.ctypes.data, *[None] * 11)
     assert st != 0 and "grid" in qesb.lib().qesb_last_error().decode()
+
+
+def test_large_header_and_truncated_files(tmp_path):
+    """A header longer than the reader's first 64 KB prefix (many variables
+    with long attributes) is read in full; a file cut inside its header is
+    refused."""
+    d, w = _city()
+    nz, ny, nx = d.face_shape()
+    path = str(tmp_path / "big_header.nc")
+    with scipy_io.netcdf_file(path, "w", version=2) as f:
+        f.createDimension("t", None)
+        for name, n in (("x_face", nx), ("y_face", ny), ("z_face", nz), ("x", nx - 1), ("y", ny - 1),
+                        ("z", nz - 1)):
+            f.createDimension(name, n)
+        for q in range(400):  # ~400 x 220 bytes of header before the fields
+            v = f.createVariable(f"extra_{q:03d}", "f4", ("z",))
+            v.long_name = "padding attribute " + "x" * 180
+            v[:] = q
+        f.createVariable("x", "f4", ("x",))[:] = (np.arange(nx - 1) + 0.5) * d.dx()
+        f.createVariable("y", "f4", ("y",))[:] = (np.arange(ny - 1) + 0.5) * d.dy()
+        f.createVariable("dz_array", "f4", ("z",))[:] = d.dz_array
+        for name in ("u", "v", "w", "u0", "v0", "w0"):
+            f.createVariable(name, "f4", ("t", "z_face", "y_face", "x_face"))[0] = \
+                getattr(w, name).reshape(nz, ny, nx)
+        f.createVariable("icellflag", "i4", ("t", "z", "y", "x"))[0] = w.icellflag.reshape(d.cell_shape())
+        for name in ("e", "f", "g", "h", "m", "n"):
+            f.createVariable(name, "f4", ("t", "z", "y", "x"))[0] = getattr(w, name).reshape(d.cell_shape())
+    r = qesb.workspace_read(path)
+    for name in ("icellflag", "e", "n", "u0", "w"):
+        np.testing.assert_array_equal(getattr(r, name), getattr(w, name))
+    cut = tmp_path / "cut.nc"
+    cut.write_bytes(open(path, "rb").read()[:70000])
+    with pytest.raises(qesb.QesbError, match="truncated"):
+        qesb.workspace_read(str(cut))

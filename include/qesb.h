@@ -170,7 +170,8 @@ qesb_status qesb_solve_batch(qesb_handle *const *handles, int n, int itermax, fl
  * right, left). z0 is WINDSGeneralData::z0 (roughness length, m); dz is the
  * Domain's nominal dz (Domain::getDomainSize, Domain.h:104), whose first value
  * (dx) the reference uses for the x and the y walls alike, as here. Runs on the
- * handle's stream and returns when done. Cells flagged 7 or 8 (cut cells, whose
+ * handle's stream and returns when done; its first call on a handle allocates
+ * a byte per cell for the wall sides. Cells flagged 7 or 8 (cut cells, whose
  * walls the first part of wallLogBC treats) make it return QESB_ERR_STATE
  * without changing u, v, w. Results agree with the reference to float
  * rounding of atan2, cos and sin (the rest is the reference's arithmetic). */
@@ -268,7 +269,11 @@ qesb_status qesb_umma_selftest(const uint16_t *A, const uint16_t *B, float *C, i
  * kernel's tensor-core completion wait gives up. Grids with W a multiple of
  * 128 and N in {16, 32} run a direct kernel (each 16-channel input slice
  * staged once per tile, the 27 taps as shifted descriptors into it); the
- * others the implicit GEMM (per-tap gather). */
+ * others the implicit GEMM (per-tap gather). Small grids (fewer than about two
+ * 128-voxel tiles per SM) split the K chunks over more CTAs and add FP32
+ * partial sums in a scratch buffer kept per (device, stream), allocated on the
+ * first such call on a stream and grown as needed (a few MB for the network's
+ * deep levels); the sum order then varies from run to run. */
 qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H, int W,
                         int sign, const void *Bm, int Kp, int N, void *y, void *yf, const float *bias,
                         int relu, const void *mask, int *err, void *stream);

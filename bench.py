@@ -844,6 +844,7 @@ def run_b200(args):
     if world > 1:
         import torch.distributed as dist
 
+        barrier()  # rank 0 ran the fire-step section alone: the ranks leave together
         dist.destroy_process_group()
 
 

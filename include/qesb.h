@@ -216,7 +216,11 @@ qesb_status qesb_autotune_batch(qesb_handle *const *handles, int n, int *best, f
  *   "variant"            sweep variant index (-1 = autotuned / default), see qesb_num_variants
  *   "batch_variant"      sweep shape for qesb_solve_batch led by this handle (-1 = from "variant");
  *                        set by qesb_autotune_batch
- *   "autotune"           1 = run qesb_autotune at the first solve of an untuned grid shape (default 0) */
+ *   "autotune"           1 = run qesb_autotune at the first solve of an untuned grid shape (default 0)
+ *   "wait_limit"         polls of a staged sweep's shared-memory stage barrier before the kernel gives
+ *                        up, lets its copies in flight land, and the solve returns QESB_ERR_CUDA
+ *                        ("sweep stage wait gave up"); 0 = the default (2^22 polls). Applies to the
+ *                        bulk-copy sweep shapes and to batches led by this handle */
 qesb_status qesb_set_tolerance(qesb_handle *h, float tol);
 qesb_status qesb_set_option(qesb_handle *h, const char *key, int value);
 /* cudaStream_t to run on (NULL = the handle's own stream). */

@@ -42,12 +42,14 @@ __global__ void __launch_bounds__(128) k_umma_selftest(const __nv_bfloat16 *__re
   uint8_t *sa = sm;              // 128 x 64 bf16 = 16 KB
   uint8_t *sb = sm + 16384;      // N x 64 bf16 <= 32 KB
   __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mdrain;  // completion of every issued MMA, after a wait gave up
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t ncols = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
   if (warp == 0) umma::tmem_alloc(&tmem_base, ncols);
   if (tid == 0) {
     umma::mbar_init(&mbar, 1);
+    umma::mbar_init(&mdrain, 1);
     umma::fence_mbar_init();
   }
   umma::fence_before_sync();
@@ -88,6 +90,7 @@ __global__ void __launch_bounds__(128) k_umma_selftest(const __nv_bfloat16 *__re
   }
   if (!ok) {
     if (lane == 0) atomicExch(err, 1);
+    umma::mma_drain(&mdrain, tid == 0, kWaitLimit);
   } else {
     for (int c0 = 0; c0 < N; c0 += 8) {
       float v[8];
@@ -172,6 +175,7 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
   constexpr uint32_t NCOLS = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
   extern __shared__ __align__(1024) uint8_t sm[];
   __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ __align__(8) uint64_t mdrain;  // completion of every issued MMA, after a wait gave up
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int cin = in.c1 + in.c2;
@@ -180,6 +184,7 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
   if (tid == 0) {
     umma::mbar_init(&mbar[0], 1);
     umma::mbar_init(&mbar[1], 1);
+    umma::mbar_init(&mdrain, 1);
     umma::fence_mbar_init();
   }
   umma::fence_before_sync();
@@ -244,6 +249,7 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
   umma::fence_after_sync();
   if (!ok) {
     if (lane == 0) atomicExch(err, 1);
+    umma::mma_drain(&mdrain, tid == 0, kWaitLimit);
   } else if (out.acc) {
     const long v = m0 + warp * 32 + lane;
     if (nk > 0)
@@ -344,6 +350,7 @@ __global__ void __launch_bounds__(128) k_conv_direct(ConvIn in, ConvGeom g, int 
   static_assert(NACC * N <= 512, "accumulators exceed TMEM");
   extern __shared__ __align__(1024) uint8_t sm[];
   __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mdrain;  // completion of every issued MMA, after a wait gave up
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int cin = in.c1 + in.c2, KC = cin / 16;
@@ -351,6 +358,7 @@ __global__ void __launch_bounds__(128) k_conv_direct(ConvIn in, ConvGeom g, int 
   if (warp == 0) umma::tmem_alloc(&tmem_base, NCOLS);
   if (tid == 0) {
     umma::mbar_init(&mbar, 1);
+    umma::mbar_init(&mdrain, 1);
     umma::fence_mbar_init();
   }
   umma::fence_before_sync();
@@ -401,6 +409,7 @@ __global__ void __launch_bounds__(128) k_conv_direct(ConvIn in, ConvGeom g, int 
   umma::fence_after_sync();
   if (!ok) {
     if (lane == 0) atomicExch(err, 1);
+    umma::mma_drain(&mdrain, tid == 0, kWaitLimit);
   } else {
     const int x = x0 + warp * 32 + lane;
     for (int a = 0; a < NACC; ++a) {
@@ -460,6 +469,7 @@ __global__ void __launch_bounds__(128) k_conv_wgrad(ConvIn in, ConvGeom g, const
   constexpr uint32_t NCOLS = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
   extern __shared__ __align__(1024) uint8_t sm[];
   __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ __align__(8) uint64_t mdrain;  // completion of every issued MMA, after a wait gave up
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int cin = in.c1 + in.c2;
@@ -471,6 +481,7 @@ __global__ void __launch_bounds__(128) k_conv_wgrad(ConvIn in, ConvGeom g, const
   if (tid == 0) {
     umma::mbar_init(&mbar[0], 1);
     umma::mbar_init(&mbar[1], 1);
+    umma::mbar_init(&mdrain, 1);
     umma::fence_mbar_init();
   }
   umma::fence_before_sync();
@@ -532,6 +543,7 @@ __global__ void __launch_bounds__(128) k_conv_wgrad(ConvIn in, ConvGeom g, const
   umma::fence_after_sync();
   if (!ok) {
     if (lane == 0) atomicExch(err, 1);
+    umma::mma_drain(&mdrain, tid == 0, kWaitLimit);
   } else {
     const int m = mt0 + warp * 32 + lane;
     for (int c0 = 0; c0 < N; c0 += 8) {

@@ -166,7 +166,10 @@ __global__ void k_na_correct(NaGrid G, const float *__restrict__ L, const float 
   }
 }
 
-// Device address of the scratch array, looked up once per device.
+// Device address of the scratch array, looked up once per device and kept
+// for the process. cudaDeviceReset destroys the context that holds the
+// array; a later context may place it elsewhere, so a process that resets a
+// device must not call this entry point on that device again.
 std::mutex g_na_mu;
 unsigned char *g_na_addr[64] = {};
 
@@ -208,6 +211,9 @@ extern "C" qesb_status qesb_solve_noalloc(const qesb_grid *grid, float tol, int 
     return qesb_fail(QESB_ERR_ARG, "qesb_solve_noalloc: grid needs Nx, Ny >= 3, Nz >= 2, dx, dy > 0 and dz_array");
   if (!e || !f || !g || !hc || !m || !n || !icellflag || !u0 || !v0 || !w0 || !lambda || !u || !v || !w)
     return qesb_fail(QESB_ERR_ARG, "qesb_solve_noalloc: null array");
+  // launch grids put the rows (Ny, or Ny + 1 faces) in grid.y, whose limit is 65535
+  if (grid->Ny + 1 > 65535)
+    return qesb_fail(QESB_ERR_ARG, "qesb_solve_noalloc: Ny = %d exceeds the limit of 65534 rows", grid->Ny);
   if (itermax < 0 || itermax > QESB_NOALLOC_MAX_ITERS)
     return qesb_fail(QESB_ERR_ARG, "qesb_solve_noalloc: itermax %d outside [0, %d]", itermax, QESB_NOALLOC_MAX_ITERS);
   const long ncell = (long)grid->Nx * grid->Ny * (grid->Nz + 1);

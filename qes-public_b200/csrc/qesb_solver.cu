@@ -592,6 +592,7 @@ struct qesb_handle {
   int opt_variant = -1;
   int opt_batch_variant = -1;  // sweep shape for batches led by this handle (qesb_autotune_batch)
   int opt_autotune = 0;
+  unsigned opt_wait_limit = 0;  // staged sweeps' mbarrier polls before giving up (0: default)
   int last_launches = 0;
 
   // log-law wall treatment (qesb_wall_log_law): per-cell wall sides, cut-cell flag
@@ -1139,6 +1140,7 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
     CKS(h->list.upload(pre, sv.unit, s));
     SweepArgs a = h->list.a;
     a.one = pre[0];
+    a.wait_limit = h->opt_wait_limit;
     CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, h->pre_iters, h->opt_graph != 0,
                        &h->sgraph_pre, h->h_ctl, &pre_launched));
     CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
@@ -1153,6 +1155,7 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
   CKS(h->list.upload(one, sv.unit, s));
   SweepArgs a = h->list.a;
   a.one = one[0];
+  a.wait_limit = h->opt_wait_limit;
   CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, itermax, h->opt_graph != 0, &h->sgraph,
                      h->h_ctl, &launched));
   h->last_launches = 2 * (launched + pre_launched);
@@ -1652,6 +1655,7 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
     const dim3 grid(sweep_ctas(sv, false, h->device)), block(32, sv.block_y);
     SweepArgs a = h->list.a;
     a.one = one[0];
+    a.wait_limit = h->opt_wait_limit;
     CK(cudaEventRecord(h->ev[0], s));
     for (int c = 0; c < n; ++c) {
       sv.red<<<grid, block, sv.smem, s>>>(a);
@@ -1874,6 +1878,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   }
   SweepList list;
   CKS(list.create(n));
+  list.a.wait_limit = h0->opt_wait_limit;
   qesb_status qs = QESB_OK;
   int launched = 0, pre_launched = 0;
   if (!pre.empty()) {
@@ -1990,6 +1995,9 @@ qesb_status qesb_set_option(qesb_handle *h, const char *key, int value)
     if (value < -1 || value >= kAllVariants)
       return qesb_fail(QESB_ERR_ARG, "variant must be in [-1, %d)", kAllVariants);
     h->opt_variant = value;
+  } else if (k == "wait_limit") {
+    if (value < 0) return qesb_fail(QESB_ERR_ARG, "wait_limit must be >= 0 (0: the default)");
+    h->opt_wait_limit = (unsigned)value;
   } else if (k == "batch_variant") {
     if (value != -1 && (value < kSplitVariant || value >= kAllVariants))
       return qesb_fail(QESB_ERR_ARG, "batch_variant must be -1 or a sweep variant in [%d, %d)", kSplitVariant,

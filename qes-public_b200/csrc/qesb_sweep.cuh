@@ -38,11 +38,17 @@ struct SweepCtl {
   unsigned long long t0;  // %globaltimer at the start of the batch
 };
 
+// Polls of an mbarrier before a staged kernel's stage wait gives up, sets
+// SweepCtl::fault and returns (unless the handle's "wait_limit" option sets
+// another count).
+constexpr uint32_t kStageWaitLimit = 1u << 22;
+
 struct SweepArgs {
   const SweepDomain *dom;  // [n]
   int *active;             // [n]: indices of the unfinished domains, in batch order
   int *uoff;               // [n + 1]: work-unit offsets over `active`
   SweepCtl *ctl;
+  unsigned wait_limit;     // polls before a stage wait gives up (0: kStageWaitLimit)
   SweepDomain one;         // the domain of a single solve, read from the kernel
                            // parameters by the MULTI = false instances
 };

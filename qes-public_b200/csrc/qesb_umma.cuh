@@ -109,6 +109,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, uint3
   return false;
 }
 
+// After a wait gave up: the issuing thread makes `drain` (an mbarrier
+// initialised with count 1 and not used otherwise) track every MMA it has
+// started, and every thread waits for it, at most `limit` polls, so that TMEM
+// and the operand tiles are not released under a running MMA. Every thread of
+// the CTA that gave up calls it.
+__device__ __forceinline__ void mma_drain(uint64_t *drain, bool issuer, uint32_t limit)
+{
+  if (issuer) mma_commit(drain);
+  mbar_wait(drain, 0, limit);
+}
+
 // 32 lanes x 8 consecutive 32-bit columns of TMEM into 8 registers per thread
 // (warp w of a warpgroup reads lanes 32*(w%4) .. +31).
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8])

@@ -91,3 +91,14 @@ def test_every_called_entry_point_has_a_ctypes_signature():
     for name in sorted(called):
         assert getattr(L, name).argtypes is not None, name
     assert len(called) >= 20
+
+
+def test_noalloc_rejects_rows_beyond_the_launch_limit():
+    """A long thin grid under the cell cap still needs Ny + 1 <= 65535 rows
+    in a launch's y dimension: refused as an argument error before any
+    device work (so this runs without a GPU)."""
+    d = qesb.Domain(3, 65535, 2, 2.0, 2.0, 1.0)
+    with pytest.raises(qesb.QesbError) as ei:
+        qesb.solve_noalloc(d, 1e-3, 10, *([16] * 14))
+    assert ei.value.status == 1
+    assert "65534 rows" in str(ei.value)

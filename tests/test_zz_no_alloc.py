@@ -59,6 +59,97 @@ def test_noalloc_matches_handle_solve_on_two_calls():
         np.testing.assert_array_equal(uvw[2].cpu().numpy(), rw)
 
 
+def _handle_solve(d, ptrs, lam0, itermax, tol):
+    import torch
+
+    dev = torch.device("cuda:0")
+    nf = d.numFaceCentered()
+    with qesb.Solver_B200(d, tol) as s:
+        s.set_inputs_device(*ptrs)
+        s.lambda_ = lam0
+        uvw = [torch.empty(nf, dtype=torch.float32, device=dev) for _ in range(3)]
+        st = s.solve_device(itermax, *[t.data_ptr() for t in uvw])
+        torch.cuda.synchronize()
+        return st, s.lambda_, [t.cpu().numpy() for t in uvw]
+
+
+def test_noalloc_stops_inside_a_chunk_like_the_handle_solve():
+    """tol 1e-3 on this city stops at iteration 186 (the oracle's count),
+    inside the entry point's third 64-iteration chunk: the kernels after the
+    stop must leave lambda alone and the host loop must end there."""
+    import torch
+
+    from oracle import oracle as O
+
+    d, w = _city()
+    dev = torch.device("cuda:0")
+    ins = [torch.from_numpy(a).to(dev) for a in w.inputs()]
+    ptrs = [t.data_ptr() for t in ins]
+    nc, nf = d.numCellCentered(), d.numFaceCentered()
+    tol, itermax = 1e-3, 300
+    _, it_oracle, _, _ = O.sor(d, w, O.divergence(d, w), tol, itermax)
+    assert it_oracle % 64 != 0 and it_oracle < itermax
+    rst, rlam, (ru, rv, rw) = _handle_solve(d, ptrs, np.zeros(nc, np.float32), itermax, tol)
+    lam = torch.zeros(nc, dtype=torch.float32, device=dev)
+    uvw = [torch.empty(nf, dtype=torch.float32, device=dev) for _ in range(3)]
+    st = qesb.solve_noalloc(d, tol, itermax, *ptrs, lam.data_ptr(), *[t.data_ptr() for t in uvw])
+    torch.cuda.synchronize()
+    assert st["iterations"] == rst["iterations"] == it_oracle
+    assert st["converged"] == rst["converged"] == 1
+    assert st["residual"] == rst["residual"] <= tol
+    np.testing.assert_array_equal(lam.cpu().numpy(), rlam)
+    for a, b in zip(uvw, (ru, rv, rw)):
+        np.testing.assert_array_equal(a.cpu().numpy(), b)
+
+
+def test_noalloc_zero_iterations_corrects_the_given_lambda():
+    import torch
+
+    d, w = _city()
+    dev = torch.device("cuda:0")
+    ins = [torch.from_numpy(a).to(dev) for a in w.inputs()]
+    ptrs = [t.data_ptr() for t in ins]
+    nc, nf = d.numCellCentered(), d.numFaceCentered()
+    lam0 = np.random.default_rng(9).standard_normal(nc).astype(np.float32)
+    rst, rlam, (ru, rv, rw) = _handle_solve(d, ptrs, lam0, 0, 1e-9)
+    lam = torch.from_numpy(lam0.copy()).to(dev)
+    uvw = [torch.empty(nf, dtype=torch.float32, device=dev) for _ in range(3)]
+    st = qesb.solve_noalloc(d, 1e-9, 0, *ptrs, lam.data_ptr(), *[t.data_ptr() for t in uvw])
+    torch.cuda.synchronize()
+    assert st["iterations"] == rst["iterations"] == 0
+    np.testing.assert_array_equal(lam.cpu().numpy(), lam0)
+    for a, b in zip(uvw, (ru, rv, rw)):
+        np.testing.assert_array_equal(a.cpu().numpy(), b)
+
+
+def test_noalloc_reports_nan_in_lambda():
+    """A NaN initial wind reaches R and then lambda: the solve stops and
+    returns QESB_ERR_NUMERIC (the array keeps no state that a later call
+    could trip over: the next call on good inputs matches the handle path)."""
+    import torch
+
+    d, w = _city()
+    dev = torch.device("cuda:0")
+    nc, nf = d.numCellCentered(), d.numFaceCentered()
+    bad_u0 = w.u0.copy()
+    bad_u0[d.face(30, 20, 5)] = np.nan
+    bad = [torch.from_numpy(a).to(dev) for a in w.inputs()[:7] + (bad_u0,) + w.inputs()[8:]]
+    lam = torch.zeros(nc, dtype=torch.float32, device=dev)
+    uvw = [torch.empty(nf, dtype=torch.float32, device=dev) for _ in range(3)]
+    with pytest.raises(qesb.QesbError) as ei:
+        qesb.solve_noalloc(d, 1e-9, 50, *[t.data_ptr() for t in bad], lam.data_ptr(),
+                           *[t.data_ptr() for t in uvw])
+    assert ei.value.status == 5
+    good = [torch.from_numpy(a).to(dev) for a in w.inputs()]
+    ptrs = [t.data_ptr() for t in good]
+    rst, rlam, _ = _handle_solve(d, ptrs, np.zeros(nc, np.float32), 40, 1e-9)
+    lam.zero_()
+    st = qesb.solve_noalloc(d, 1e-9, 40, *ptrs, lam.data_ptr(), *[t.data_ptr() for t in uvw])
+    torch.cuda.synchronize()
+    assert st["iterations"] == rst["iterations"] == 40
+    np.testing.assert_array_equal(lam.cpu().numpy(), rlam)
+
+
 def test_noalloc_rejects_grids_beyond_its_scratch():
     import torch
 

@@ -55,7 +55,8 @@ typedef struct qesb_grid {
 /* Per-solve report. */
 typedef struct qesb_stats {
   int iterations;        /* SOR iterations performed (the reference's `iter`) */
-  int converged;         /* 1 if the stop came from max|dlambda| <= tol */
+  int converged;         /* 1 if the stop came from max|dlambda| <= tol, 2 if from the window
+                            rule (qesb_set_window_rule), 0 if from itermax */
   double residual;       /* FP64 max|lambda - lambda_old| of the last iteration */
   double ms_total;       /* device time of the whole solve (CUDA events) */
   double ms_sor;         /* device time of the SOR iterations alone */
@@ -66,6 +67,8 @@ typedef struct qesb_stats {
   double max_divergence; /* final check, in FP64: max |du/dx + dv/dy + dw/dz| over fluid cells
                             (icellflag 1), i in [1,nx-3], j in [1,ny-3], k in [1,nz-4], of the
                             corrected winds; -1 when the solve wrote no winds */
+  double window_drift;   /* window rule: FP64 max|lambda - lambda(window iterations earlier)| at the
+                            last window check; -1 when the rule is off or no window completed */
 } qesb_stats;
 
 /* Library and device. */
@@ -143,6 +146,25 @@ int qesb_num_variants(void);
  * starting point differs. omega = 0 turns it off (the default). The fused
  * tiled and full-coefficient paths ignore it. */
 qesb_status qesb_set_prephase(qesb_handle *h, float omega, float tol, int max_iterations);
+
+/* Window stopping rule (no reference counterpart; a reachable stop for the
+ * reference loop). The reference stops when one iteration changes lambda by at
+ * most tol (Solver_CPU.cpp:93,129-143). In FP32 that change never falls below
+ * the rounding flutter of lambda's largest values (10-15 ulp on the benchmark
+ * cities), where the winds are still 1-5e-3 m/s from their converged values, so
+ * a small tol is never met and a large one stops early. With window > 0 the
+ * reference loop also stops, after every window-th iteration n, when
+ *     max over all cells |lambda_n - lambda_(n - window)| <= tol   (FP64, exact)
+ * a drift that keeps falling below the flutter. Iterations, the per-iteration
+ * rule and itermax are unchanged; st->converged = 2 marks a window stop and
+ * st->window_drift holds the last window's value. The pre-phase
+ * (qesb_set_prephase) is not affected; the first window starts when the
+ * reference loop does. Applies to qesb_solve/qesb_solve_device and
+ * qesb_solve_batch (every handle of a batch must use the same window length);
+ * the packed path then runs on the sweep kernels, not the fused tile shapes.
+ * The first call with window > 0 allocates one lambda-sized buffer on the
+ * handle. window = 0 turns the rule off (the default). */
+qesb_status qesb_set_window_rule(qesb_handle *h, int window, double tol);
 
 /* Batched solve (no reference counterpart: the reference solves one domain
  * per Solver::solve call, src/winds/Solver.h:108). Each of the n handles

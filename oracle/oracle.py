@@ -46,6 +46,8 @@ def port() -> C.CDLL:
         L.qo_sor.restype = i
         L.qo_sor_omega.argtypes = [i, i, i, i, i] + [_V] * 8 + [f, i, _V, _V, f]
         L.qo_sor_omega.restype = i
+        L.qo_sor_window.argtypes = [i, i, i, i, i] + [_V] * 8 + [f, i, _V, _V, f, i, d, _V, _V]
+        L.qo_sor_window.restype = i
         L.qo_sor_rb_f64_omega.argtypes = [i, i, i] + [_V] * 8 + [d, i, _V, d]
         L.qo_sor_rb_f64_omega.restype = i
         L.qo_correct.argtypes = [i, i, i, f, f] + [_V] * 11
@@ -116,6 +118,19 @@ def sor(dom, w, R, tol, itermax, ordering=1, err_fp64=True, lam=None, hist=False
     else:
         it = port().qo_sor_omega(*args, float(np.float32(omega)))
     return L, it, fe.value, (H[:it] if hist else None)
+
+
+def sor_window(dom, w, R, tol, itermax, window, wtol, lam=None, omega=None, ordering=1):
+    """SOR with the solver's window rule (qo_sor_window): returns (lambda,
+    iterations, stop kind 0/1/2 for itermax/tol/window, last window drift)."""
+    Nx, Ny, Nz = dom.base
+    L = np.zeros(dom.numCellCentered(), np.float32) if lam is None else lam.astype(np.float32).copy()
+    fe, stop, drift = C.c_double(), C.c_int(), C.c_double()
+    it = port().qo_sor_window(ordering, 1, Nx, Ny, Nz, _p(w.e), _p(w.f), _p(w.g), _p(w.h), _p(w.m), _p(w.n),
+                              _p(R), _p(L), float(np.float32(tol)), int(itermax), C.byref(fe), None,
+                              float(np.float32(1.78 if omega is None else omega)), int(window), float(wtol),
+                              C.byref(stop), C.byref(drift))
+    return L, it, stop.value, drift.value
 
 
 def correct(dom, w, L):

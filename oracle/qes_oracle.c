@@ -91,16 +91,27 @@ static inline float sor_cell(const grid_t *G, long c, const float *e, const floa
  * err_hist (nullable) receives each iteration's error as a double.
  * Returns the number of iterations performed.
  */
-int qo_sor_omega(int ordering, int err_fp64, int Nx, int Ny, int Nz, const float *e, const float *f,
-                 const float *g_, const float *h, const float *m, const float *n, const float *R, float *L,
-                 float tol, int itermax, double *final_error, double *err_hist, float omega)
+/*
+ * window > 0 adds the solver's window rule (no reference counterpart): after
+ * an iteration that leaves the reference condition true, if the iteration
+ * count is a multiple of `window`, the loop also stops when
+ * max over all cells |lambda - lambda(window iterations earlier)| <= wtol,
+ * in double; *stop (nullable) receives 0 (itermax), 1 (tol) or 2 (window),
+ * *drift (nullable) the last window's value (-1 if none).
+ */
+int qo_sor_window(int ordering, int err_fp64, int Nx, int Ny, int Nz, const float *e, const float *f,
+                  const float *g_, const float *h, const float *m, const float *n, const float *R, float *L,
+                  float tol, int itermax, double *final_error, double *err_hist, float omega, int window,
+                  double wtol, int *stop, double *drift)
 {
   grid_t G = mkgrid(Nx, Ny, Nz);
   long nc = G.XY * (G.nz - 1);
   float *old = (float *)malloc(sizeof(float) * nc);
-  int iter = 0;
-  double max_error = 1.0;
-  while (iter < itermax && max_error > (double)tol) {
+  float *snap = window > 0 ? (float *)malloc(sizeof(float) * nc) : NULL;
+  if (snap) memcpy(snap, L, sizeof(float) * nc);
+  int iter = 0, wstop = 0;
+  double max_error = 1.0, wdrift = -1.0;
+  while (iter < itermax && max_error > (double)tol && !wstop) {
     memcpy(old, L, sizeof(float) * nc);
     if (ordering == 0) {
       for (int k = 1; k < G.nz - 2; ++k)
@@ -141,10 +152,31 @@ int qo_sor_omega(int ordering, int err_fp64, int Nx, int Ny, int Nz, const float
     max_error = err_fp64 ? me : (double)mef;
     if (err_hist) err_hist[iter] = max_error;
     iter += 1;
+    if (snap && iter % window == 0 && iter < itermax && max_error > (double)tol && max_error == max_error) {
+      double dw = 0.0;
+      for (long c = 0; c < nc; ++c) {
+        double d = fabs((double)L[c] - (double)snap[c]);
+        if (d > dw || d != d) dw = d;
+      }
+      memcpy(snap, L, sizeof(float) * nc);
+      wdrift = dw;
+      if (dw <= wtol) wstop = 1;
+    }
   }
   if (final_error) *final_error = max_error;
+  if (stop) *stop = wstop ? 2 : (max_error > (double)tol ? 0 : 1);
+  if (drift) *drift = wdrift;
   free(old);
+  free(snap);
   return iter;
+}
+
+int qo_sor_omega(int ordering, int err_fp64, int Nx, int Ny, int Nz, const float *e, const float *f,
+                 const float *g_, const float *h, const float *m, const float *n, const float *R, float *L,
+                 float tol, int itermax, double *final_error, double *err_hist, float omega)
+{
+  return qo_sor_window(ordering, err_fp64, Nx, Ny, Nz, e, f, g_, h, m, n, R, L, tol, itermax, final_error,
+                       err_hist, omega, 0, 0.0, NULL, NULL);
 }
 
 int qo_sor(int ordering, int err_fp64, int Nx, int Ny, int Nz, const float *e, const float *f,
@@ -400,4 +432,175 @@ int qo_wall_log(int Nx, int Ny, int Nz, float dxy, float dz, float z0, const int
         }
   }
   return 0;
+}
+
+/* -------------------------------------------------------------------------
+ * Seeded synthetic city, restated for the reference-only benchmark leg: the
+ * same cities the product's generator (qesb_city_random / qesb_city_build)
+ * makes, built without the product library. The wall coefficients and the
+ * solid-face zeroing then come from the reference's own Wall.cpp
+ * (oracle/_ref); this file supplies what the reference has no code for: the
+ * seeded building layout, the cell flags of the buildings (PolyBuilding's
+ * PNPOLY test, src/winds/PolyBuilding.cpp:157-224, for the closed 5-vertex
+ * ring of RectangularBuilding.h:70-108) and the power-law inflow
+ * (WindProfilerSensorType.cpp:220,328-333).
+ * ------------------------------------------------------------------------- */
+
+/* SplitMix64 (Steele, Lea, Flood 2014). */
+static uint64_t sm64_next(uint64_t *s)
+{
+  uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+static float sm64_uniform(uint64_t *s, float a, float b)
+{
+  double u = (double)(sm64_next(s) >> 11) * (1.0 / 9007199254740992.0);
+  return (float)(a + (b - a) * u);
+}
+
+/* Buildings (x_start, y_start, length, width, height, base_height: 6 floats
+ * each) and inflow (u_ref, z_ref, p, dir_deg) of the seed's city: up to
+ * max_b non-overlapping cuboids with a one-cell gap, kept a margin from the
+ * domain edges, placed by rejection. Returns the count. */
+int qo_city_random(int Nx, int Ny, float dx, float dy, uint64_t seed, int max_b, float fp_min, float fp_max,
+                   float h_min, float h_max, float *b, float *inflow)
+{
+  uint64_t s = seed;
+  const float Lx = Nx * dx, Ly = Ny * dy;
+  const float dmax = dx > dy ? dx : dy;
+  const float margin = 2.0f * dmax + 1.0f, gap = dmax;
+  int nb = 0;
+  for (int attempt = 0; attempt < 200 * max_b && nb < max_b; ++attempt) {
+    float len = sm64_uniform(&s, fp_min, fp_max);
+    float wid = sm64_uniform(&s, fp_min, fp_max);
+    float hgt = sm64_uniform(&s, h_min, h_max);
+    if (Lx - 2 * margin - len <= 0 || Ly - 2 * margin - wid <= 0) continue;
+    float xs = floorf(sm64_uniform(&s, margin, Lx - margin - len));
+    float ys = floorf(sm64_uniform(&s, margin, Ly - margin - wid));
+    int ok = 1;
+    for (int q = 0; q < nb && ok; ++q) {
+      const float *o = b + 6 * q;
+      if (xs < o[0] + o[2] + gap && o[0] < xs + len + gap && ys < o[1] + o[3] + gap && o[1] < ys + wid + gap) ok = 0;
+    }
+    if (ok) {
+      float *c = b + 6 * nb++;
+      c[0] = xs;
+      c[1] = ys;
+      c[2] = len;
+      c[3] = wid;
+      c[4] = hgt;
+      c[5] = 0.0f;
+    }
+  }
+  inflow[0] = sm64_uniform(&s, 3.0f, 10.0f);
+  inflow[1] = 10.0f;
+  inflow[2] = sm64_uniform(&s, 0.1f, 0.3f);
+  inflow[3] = sm64_uniform(&s, 0.0f, 360.0f);
+  return nb;
+}
+
+/* z and z_face from dz, as Domain::defineVerticalGrid (src/qes/Domain.cpp:135-151). */
+static void vgrid(int nz, const float *dz, float *z, float *zf)
+{
+  zf[0] = -dz[0];
+  zf[1] = 0.0f;
+  for (int k = 2; k < nz; ++k) zf[k] = zf[k - 1] + dz[k - 1];
+  z[0] = -0.5f * dz[0];
+  for (int k = 1; k < nz - 1; ++k) z[k] = 0.5f * (zf[k] + zf[k + 1]);
+}
+
+/* icellflag of the city: 1 everywhere, 2 on the ground plane k = 0
+ * (WINDSGeneralData.cpp:438-444), 0 in the buildings' cells. */
+void qo_city_flags(int Nx, int Ny, int Nz, float dx, float dy, const float *dz, int nb, const float *b, int *flag)
+{
+  grid_t G = mkgrid(Nx, Ny, Nz);
+  const long nc = G.XY * (G.nz - 1);
+  float *z = (float *)malloc(sizeof(float) * (G.nz - 1)), *zf = (float *)malloc(sizeof(float) * G.nz);
+  vgrid(G.nz, dz, z, zf);
+  for (long c = 0; c < nc; ++c) flag[c] = 1;
+  for (int j = 0; j < G.ny - 1; ++j)
+    for (int i = 0; i < G.nx - 1; ++i) flag[cellix(&G, i, j, 0)] = 2;
+  for (int q = 0; q < nb; ++q) {
+    const float *B = b + 6 * q;
+    const float xs = B[0], ys = B[1], len = B[2], wid = B[3], hgt = B[4], base = B[5];
+    float px[5], py[5];
+    px[0] = px[4] = xs;
+    py[0] = py[4] = ys;
+    px[1] = xs - wid * 0.0f;
+    py[1] = ys + wid * 1.0f;
+    px[2] = px[1] + len * 1.0f;
+    py[2] = py[1] + len * 0.0f;
+    px[3] = xs + len * 1.0f;
+    py[3] = ys + len * 0.0f;
+    float x_min = px[0], x_max = px[0], y_min = py[0], y_max = py[0];
+    for (int v = 1; v < 5; ++v) {
+      if (px[v] > x_max) x_max = px[v];
+      if (px[v] < x_min) x_min = px[v];
+      if (py[v] > y_max) y_max = py[v];
+      if (py[v] < y_min) y_min = py[v];
+    }
+    const int i_start = (int)(x_min / dx), i_end = (int)((x_max / dx) + 1);
+    const int j_start = (int)(y_min / dy), j_end = (int)((y_max / dy) + 1);
+    const float top = hgt + base;
+    int k_start = 1, k_end = 1;
+    for (int k = 1; k < G.nz - 1; ++k) {
+      k_start = k;
+      if (base <= zf[k + 1]) break;
+    }
+    for (int k = 0; k < G.nz - 1; ++k) {
+      k_end = k + 1;
+      if (top < z[k + 1]) break;
+    }
+    for (int j = j_start; j <= j_end; ++j) {
+      const float yc = (float)((j + 0.5) * dy);
+      for (int i = i_start; i <= i_end; ++i) {
+        const float xc = (float)((i + 0.5) * dx);
+        unsigned v = 0, st = 0;
+        int cross = 0;
+        while (v < 4) {
+          if ((py[v] <= yc && py[v + 1] > yc) || (py[v] > yc && py[v + 1] <= yc)) {
+            const float t = (yc - py[v]) / (py[v + 1] - py[v]);
+            if (xc < (px[v] + t * (px[v + 1] - px[v]))) cross += 1;
+          }
+          v += 1;
+          if (px[v] == px[st] && py[v] == py[st]) {
+            v += 1;
+            st = v;
+          }
+        }
+        if (cross % 2 != 0 && i >= 0 && j >= 0 && i < G.X && j < G.ny - 1)
+          for (int k = k_start; k < k_end && k < G.nz - 1; ++k) flag[cellix(&G, i, j, k)] = 0;
+      }
+    }
+  }
+  free(z);
+  free(zf);
+}
+
+/* Power-law inflow on every face column, faces k in [1, nz-2]; w0 = 0
+ * (flat terrain, one sensor). Solid faces are not zeroed here. */
+void qo_city_inflow(int Nx, int Ny, int Nz, const float *dz, const float *inflow, float *u0, float *v0, float *w0)
+{
+  grid_t G = mkgrid(Nx, Ny, Nz);
+  const long nf = G.FXY * G.nz;
+  float *z = (float *)malloc(sizeof(float) * (G.nz - 1)), *zf = (float *)malloc(sizeof(float) * G.nz);
+  vgrid(G.nz, dz, z, zf);
+  memset(u0, 0, sizeof(float) * nf);
+  memset(v0, 0, sizeof(float) * nf);
+  memset(w0, 0, sizeof(float) * nf);
+  const float theta = (float)((270.0 - inflow[3]) * M_PI / 180.0);
+  for (int k = 1; k < G.nz - 1; ++k) {
+    const float s = powf((z[k] - 0.0f) / inflow[1], inflow[2]);
+    const float up = cosf(theta) * inflow[0] * s, vp = sinf(theta) * inflow[0] * s;
+    for (int j = 0; j < G.ny; ++j)
+      for (int i = 0; i < G.nx; ++i) {
+        const long q = faceix(&G, i, j, k);
+        u0[q] = up;
+        v0[q] = vp;
+      }
+  }
+  free(z);
+  free(zf);
 }

@@ -40,6 +40,8 @@ struct SolveState {
   int redo_par;   // its output buffer
   unsigned blocks_done;  // CTAs of the current black half-sweep that have finished
   unsigned long long t_done;  // %globaltimer (ns) when a batched solve's loop ended
+  double wacc;    // window rule: max|lambda - snapshot| being gathered by the current check
+  double wdrift;  // window rule: the last completed window's max|lambda - snapshot|
 };
 
 __device__ __forceinline__ unsigned long long global_ns()

@@ -288,6 +288,41 @@ __global__ void k_poll(SolveState *st, const double *__restrict__ err, double to
   if (st->it >= itermax) st->done = 1;
 }
 
+// Window rule on the full-coefficient path (one domain, padded layout):
+// max|lambda - snapshot| over the n4 float4 of the layout into st->wacc,
+// FP64 exact, and the snapshot takes lambda's values; skipped once the loop
+// has stopped. k_window_poll_full then applies the rule.
+__global__ void k_window_full(const float4 *__restrict__ L, float4 *__restrict__ S, long n4, SolveState *st)
+{
+  if (st->done) return;
+  double dmax = 0.0;
+  for (long i = threadIdx.x + (long)blockIdx.x * blockDim.x; i < n4; i += (long)gridDim.x * blockDim.x) {
+    const float4 a = L[i], o = S[i];
+    const double d[4] = {fabs((double)a.x - (double)o.x), fabs((double)a.y - (double)o.y),
+                         fabs((double)a.z - (double)o.z), fabs((double)a.w - (double)o.w)};
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (d[q] > dmax || d[q] != d[q]) dmax = d[q];
+    S[i] = a;
+  }
+  block_max_to(&st->wacc, dmax);
+}
+
+__global__ void k_window_poll_full(SolveState *st, double wtol)
+{
+  if (st->done) return;
+  const double d = st->wacc;
+  st->wacc = 0.0;
+  st->wdrift = d;
+  if (isnan(d)) {
+    st->done = 1;
+    st->nan = 1;
+  } else if (d <= wtol) {
+    st->done = 1;
+    st->converged = 2;
+  }
+}
+
 // Final divergence check in FP64: max over fluid cells (icellflag == 1),
 // i in [1, nx-3], j in [1, ny-3], k in [1, kmax], of
 //   |(u[i+1]-u[i])/dx + (v[j+1]-v[j])/dy + (w[k+1]-w[k])/dz[k]|
@@ -540,6 +575,7 @@ struct SweepList {
 struct SweepGraph {
   cudaGraphExec_t exec = nullptr;
   int variant = -1, chunk = 0;
+  int wk = 0, nslots = 0;  // window checks captured: every wk launches, over nslots list slots
   bool multi = false;
   SweepArgs args{};
   cudaStream_t stream = nullptr;
@@ -611,6 +647,11 @@ struct qesb_handle {
   float inv_pre_omega = 0.0f;     // omega d_inv_pre holds (0 = stale)
   int last_pre_iterations = 0;
   SweepGraph sgraph_pre;
+
+  // window rule (qesb_set_window_rule): window 0 = off
+  int win_k = 0;
+  double win_tol = 0.0;
+  float *d_snap = nullptr;  // lambda at the start of the current window (split or padded layout)
 
   // sweep kernels: this solve as a one-domain list
   SweepList list;
@@ -753,6 +794,9 @@ qesb_status run_iterations_full(qesb_handle *h, int itermax)
   dim3 grid(((G.X - 2) / 2 + 1 + nthr - 1) / nthr, G.Y - 2, G.Z - 2);
   dim3 mgrid((G.X + 255) / 256, G.Y, 1);
   const int chunk = 64;
+  const long n4 = (long)pad_cells(G) / 4;
+  if (h->win_k > 0)  // the first window starts from lambda as the loop begins
+    CK(cudaMemcpyAsync(h->d_snap, h->d_lam, sizeof(float) * pad_cells(G), cudaMemcpyDeviceToDevice, s));
   for (int base = 0; base < itermax; base += chunk) {
     const int n = std::min(chunk, itermax - base);
     for (int t = 0; t < n; ++t) {
@@ -762,6 +806,11 @@ qesb_status run_iterations_full(qesb_handle *h, int itermax)
                                          h->d_state);
       k_mirror<<<mgrid, 256, 0, s>>>(G, h->d_lam, h->d_state);
       k_poll<<<1, 1, 0, s>>>(h->d_state, h->d_err, (double)h->tol, itermax, 1, 0);
+      if (h->win_k > 0 && (base + t + 1) % h->win_k == 0) {
+        k_window_full<<<592, 256, 0, s>>>(reinterpret_cast<const float4 *>(h->d_lam),
+                                          reinterpret_cast<float4 *>(h->d_snap), n4, h->d_state);
+        k_window_poll_full<<<1, 1, 0, s>>>(h->d_state, h->win_tol);
+      }
     }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
@@ -1047,6 +1096,10 @@ SweepDomain sweep_domain(qesb_handle *h, int itermax, double tol)
   d.itermax = itermax;
   d.tol = tol;
   d.c1 = 1.0f - kOmega;
+  d.wK = h->win_k;
+  d.wn = 2 * h->S.CS;
+  d.wtol = h->win_tol;
+  d.snap = h->d_snap;
   return d;
 }
 
@@ -1062,25 +1115,49 @@ qesb_status sweep_domain_pre(qesb_handle *h, SweepDomain &d, cudaStream_t s)
   d = sweep_domain(h, h->pre_iters, (double)h->pre_tol);
   d.inv = h->d_inv_pre;
   d.c1 = 1.0f - h->pre_omega;
+  d.wK = 0;  // the window rule ends the reference loop only
   return QESB_OK;
+}
+
+// Window check launch for a list of kernels of work-unit kind `unit`.
+void launch_window(int unit, bool multi, dim3 grid, cudaStream_t s, const SweepArgs &a)
+{
+  if (unit == kUnitTile) {
+    if (multi) k_window_check<kUnitTile, true><<<grid, 256, 0, s>>>(a);
+    else k_window_check<kUnitTile, false><<<grid, 256, 0, s>>>(a);
+  } else if (unit == kUnitSpan) {
+    if (multi) k_window_check<kUnitSpan, true><<<grid, 256, 0, s>>>(a);
+    else k_window_check<kUnitSpan, false><<<grid, 256, 0, s>>>(a);
+  } else {
+    if (multi) k_window_check<kUnitRow, true><<<grid, 256, 0, s>>>(a);
+    else k_window_check<kUnitRow, false><<<grid, 256, 0, s>>>(a);
+  }
 }
 
 // The iteration loop over a domain list: CUDA-graph chunks of (red, black)
 // launches, the list's control block read back every ~2 ms of device work,
 // until no domain is left or itermax launches ran. *launched: iterations
-// launched.
+// launched. wk > 0: a window check (k_window_check over `nslots` list slots)
+// follows every wk-th black launch; chunks are then whole windows, so the
+// checks fall on iterations wk, 2 wk, ... of the loop for every domain.
 qesb_status run_sweep_loop(const SweepVariant &sv, bool multi, const SweepArgs &a, int device, cudaStream_t s,
-                           double cells, int itermax, bool graph, SweepGraph *cache, SweepCtl *h_ctl, int *launched)
+                           double cells, int itermax, bool graph, SweepGraph *cache, SweepCtl *h_ctl, int *launched,
+                           int wk = 0, int nslots = 1)
 {
   CKS(sweep_prepare(sv));
   const dim3 grid(sweep_ctas(sv, multi, device)), block(32, sv.block_y);
   const int per_it_us = std::max(1, (int)(cells / 4.0e5));
-  const int chunk = std::max(1, std::min(128, 2000 / per_it_us));
+  int chunk = std::max(1, std::min(128, 2000 / per_it_us));
+  if (wk > 0) chunk = wk * std::max(1, chunk / wk);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const dim3 wgrid(std::max(1, 4 * sms / std::max(1, nslots)), std::max(1, nslots));
   auto red = multi ? sv.red_m : sv.red, black = multi ? sv.black_m : sv.black;
   auto enqueue = [&]() {
     for (int c = 0; c < chunk; ++c) {
       red<<<grid, block, sv.smem, s>>>(a);
       black<<<grid, block, sv.smem, s>>>(a);
+      if (wk > 0 && (c + 1) % wk == 0) launch_window(sv.unit, multi, wgrid, s, a);
     }
     return cudaGetLastError();
   };
@@ -1089,7 +1166,8 @@ qesb_status run_sweep_loop(const SweepVariant &sv, bool multi, const SweepArgs &
   while (*launched < itermax) {
     if (graph) {
       const bool hit = cache->exec && cache->variant == vid && cache->chunk == chunk && cache->multi == multi &&
-                       cache->stream == s && std::memcmp(&cache->args, &a, sizeof a) == 0;
+                       cache->wk == wk && cache->nslots == nslots && cache->stream == s &&
+                       std::memcmp(&cache->args, &a, sizeof a) == 0;
       if (!hit) {
         cache->reset();
         cudaGraph_t g;
@@ -1103,6 +1181,8 @@ qesb_status run_sweep_loop(const SweepVariant &sv, bool multi, const SweepArgs &
         if (ce != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
         cache->variant = vid;
         cache->chunk = chunk;
+        cache->wk = wk;
+        cache->nslots = nslots;
         cache->multi = multi;
         cache->stream = s;
         std::memcpy(&cache->args, &a, sizeof a);
@@ -1156,9 +1236,11 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
   SweepArgs a = h->list.a;
   a.one = one[0];
   a.wait_limit = h->opt_wait_limit;
+  if (h->win_k > 0)  // the first window starts from lambda as the reference loop begins
+    CK(cudaMemcpyAsync(h->d_snap, h->d_lam_s, sizeof(float) * 2 * h->S.CS, cudaMemcpyDeviceToDevice, s));
   CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, itermax, h->opt_graph != 0, &h->sgraph,
-                     h->h_ctl, &launched));
-  h->last_launches = 2 * (launched + pre_launched);
+                     h->h_ctl, &launched, h->win_k, 1));
+  h->last_launches = 2 * (launched + pre_launched) + (h->win_k > 0 ? launched / h->win_k : 0);
   k_split_mirror_ring<<<G.Y, 128, 0, s>>>(G, h->S, h->d_lam_s);
   k_split_to_pad<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam_s, h->d_lam);
   CK(cudaGetLastError());
@@ -1203,7 +1285,9 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
     CKS(qesb_autotune(h, nullptr, nullptr, 0));
     CK(cudaEventRecord(h->ev[1], s));
   }
-  const int vi = packed ? pick_variant(h) : -1;
+  int vi = packed ? pick_variant(h) : -1;
+  // the fused tiled kernels have no window checks: the window rule runs on the sweep kernels
+  if (packed && h->win_k > 0 && vi < kSplitVariant) vi = kSplitVariant + kDefaultSweep;
   const bool split = packed && vi >= kSplitVariant;
   const Variant *var = packed && !split ? &kVariants[vi] : nullptr;
   h->last_launches = 0;
@@ -1239,6 +1323,7 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
     st->sweeps_per_launch = var ? var->K : 1;
     st->launches = 2 + (packed ? h->last_launches : 4 * st->iterations);
     st->pre_iterations = h->last_pre_iterations;
+    st->window_drift = h->win_k > 0 && st->iterations >= h->win_k ? h->h_state->wdrift : -1.0;
   }
   if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the solve (iteration %d)", h->h_state->it);
   return QESB_OK;
@@ -1275,7 +1360,7 @@ void free_all(qesb_handle *h)
                   h->d_own_in[2], h->d_own_in[3], h->d_own_in[4], h->d_own_in[5], h->d_own_flag,
                   h->d_own_u0, h->d_own_v0, h->d_own_w0, h->d_dz, h->d_vmax, h->d_inv, h->d_val,
                   h->d_inv_pre, h->d_bad, h->d_err, h->d_state, h->d_u, h->d_v, h->d_w, h->d_wbits,
-                  h->d_wcut};
+                  h->d_wcut, h->d_snap};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   h->list.destroy();
@@ -1852,6 +1937,10 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   double cells = 0;
   std::vector<SweepDomain> pre;
   std::vector<int> pre_of;  // batch index of each pre-phase domain
+  for (int i = 1; i < n; ++i)
+    if (hs[i]->win_k != h0->win_k)
+      return qesb_fail(QESB_ERR_ARG, "qesb_solve_batch: handles %d and 0 have different window lengths (%d, %d)", i,
+                       hs[i]->win_k, h0->win_k);
   for (int i = 0; i < n; ++i) {
     qesb_handle *h = hs[i];
     const DevGrid &G = h->G;
@@ -1905,12 +1994,17 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   }
   sweep_tiles(doms, sv, true, h0->device);
   if (qs == QESB_OK) qs = list.upload(doms, sv.unit, s);
+  if (qs == QESB_OK && h0->win_k > 0)  // each domain's first window starts from lambda as the loop begins
+    for (int i = 0; i < n && qs == QESB_OK; ++i)
+      if (cudaMemcpyAsync(hs[i]->d_snap, hs[i]->d_lam_s, sizeof(float) * 2 * hs[i]->S.CS, cudaMemcpyDeviceToDevice,
+                          s) != cudaSuccess)
+        qs = qesb_fail(QESB_ERR_CUDA, "qesb_solve_batch: window snapshot copy failed");
   if (qs == QESB_OK) {
     k_sweep_stamp<<<1, 1, 0, s>>>(list.a.ctl);
     SweepGraph gx;
     if (itermax > 0)
       qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, itermax, h0->opt_graph != 0, &gx, h0->h_ctl,
-                          &launched);
+                          &launched, h0->win_k, n);
     gx.reset();
   }
   const unsigned long long t0 = h0->h_ctl->t0;
@@ -1950,8 +2044,9 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
       st[i].ms_sor = sti.t_done > t0 ? (double)(sti.t_done - t0) * 1e-6 : 0.0;
       st[i].path = 1;
       st[i].sweeps_per_launch = 1;
-      st[i].launches = 2 * (launched + pre_launched);
+      st[i].launches = 2 * (launched + pre_launched) + (h0->win_k > 0 ? launched / h0->win_k : 0);
       st[i].pre_iterations = hs[i]->last_pre_iterations;
+      st[i].window_drift = h0->win_k > 0 && st[i].iterations >= h0->win_k ? sti.wdrift : -1.0;
     }
   }
   if (nan_at >= 0) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d", nan_at);
@@ -1967,6 +2062,21 @@ qesb_status qesb_set_prephase(qesb_handle *h, float omega, float tol, int max_it
   h->pre_omega = omega;
   h->pre_tol = tol;
   h->pre_iters = max_iterations;
+  return QESB_OK;
+}
+
+qesb_status qesb_set_window_rule(qesb_handle *h, int window, double tol)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  if (window < 0 || window > 4096 || (window > 0 && !(tol >= 0.0)))
+    return qesb_fail(QESB_ERR_ARG, "qesb_set_window_rule: window must be in [0, 4096] and tol >= 0");
+  if (window > 0 && !h->d_snap) {
+    CK(cudaSetDevice(h->device));
+    const size_t nsnap = std::max((size_t)(2 * h->S.CS), pad_cells(h->G));
+    CKS(dalloc(&h->d_snap, nsnap));
+  }
+  h->win_k = window;
+  h->win_tol = tol;
   return QESB_OK;
 }
 

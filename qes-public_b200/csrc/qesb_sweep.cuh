@@ -28,6 +28,13 @@ struct SweepDomain {
   int itermax;
   double tol;
   float c1;  // 1 - omega (omega/sum sits in inv): the reference's 1.78f, or a pre-phase's
+  // Window rule (off when wK = 0): after every wK-th iteration of the loop the
+  // domain stops if the FP64 max|lambda - snap| over its wn floats is <= wtol;
+  // snap then takes lambda's values for the next window.
+  int wK;
+  long wn;
+  double wtol;
+  float *snap;
 };
 
 struct SweepCtl {
@@ -92,11 +99,29 @@ __host__ __device__ __forceinline__ int sweep_units(const SweepDomain &D, int un
   return D.rows;
 }
 
-// End of a black launch. Every thread of the CTA calls it after its own error
-// flushes; the last CTA to arrive polls the unfinished domains and rebuilds
-// the active list and unit offsets for the next launch.
-template <int UNIT, bool MULTI>
-__device__ __forceinline__ void sweep_finish_black(const SweepArgs &b, int na)
+// Window rule poll of one domain after a window check gathered its drift:
+// the stop when max|lambda - snapshot| <= wtol (converged = 2), NaN as in
+// poll_one. One thread per domain.
+__device__ __forceinline__ void window_poll_one(const SweepDomain &D)
+{
+  SolveState *st = D.st;
+  const double d = *reinterpret_cast<volatile double *>(&st->wacc);
+  st->wacc = 0.0;
+  st->wdrift = d;
+  if (isnan(d)) {
+    st->done = 1;
+    st->nan = 1;
+  } else if (d <= D.wtol) {
+    st->done = 1;
+    st->converged = 2;
+  }
+}
+
+// The last CTA of a launch (blocks counted in ctl->blocks_done, `nblocks` in
+// all) polls every active domain with `poll` and rebuilds the active list and
+// unit offsets for the next launch. Every thread of the CTA calls it.
+template <int UNIT, bool MULTI, typename Poll>
+__device__ __forceinline__ void sweep_last_cta_poll(const SweepArgs &b, int na, unsigned nblocks, Poll poll)
 {
   __syncthreads();
   const int tid = threadIdx.x + threadIdx.y * blockDim.x, lane = tid & 31;
@@ -104,16 +129,16 @@ __device__ __forceinline__ void sweep_finish_black(const SweepArgs &b, int na)
   unsigned last = 0;
   if (lane == 0) {
     __threadfence();
-    last = atomicAdd(&b.ctl->blocks_done, 1u) == gridDim.x - 1;
+    last = atomicAdd(&b.ctl->blocks_done, 1u) == nblocks - 1;
   }
   last = __shfl_sync(0xffffffffu, last, 0);
   if (!last) return;
   __threadfence();
   if (!MULTI) {
     if (lane == 0) {
-      poll_one(b.one.st, b.one.err, b.one.tol, b.one.itermax);
-      const bool done = b.one.st->done;
-      if (done) b.one.st->t_done = global_ns();
+      if (na > 0) poll(b.one);
+      const bool done = na <= 0 || b.one.st->done;
+      if (done && na > 0) b.one.st->t_done = global_ns();
       b.ctl->nactive = done ? 0 : 1;
       b.ctl->blocks_done = 0;
     }
@@ -126,7 +151,7 @@ __device__ __forceinline__ void sweep_finish_black(const SweepArgs &b, int na)
     if (a < na) {
       d = b.active[a];
       const SweepDomain &D = b.dom[d];
-      poll_one(D.st, D.err, D.tol, D.itermax);
+      poll(D);
       keep = !D.st->done;
       if (!keep) D.st->t_done = global_ns();
       units = sweep_units(D, UNIT);
@@ -152,6 +177,53 @@ __device__ __forceinline__ void sweep_finish_black(const SweepArgs &b, int na)
     b.ctl->nactive = out;
     b.ctl->blocks_done = 0;
   }
+}
+
+// End of a black launch. Every thread of the CTA calls it after its own error
+// flushes; the last CTA to arrive polls the unfinished domains (the loop
+// condition) and rebuilds the active list and unit offsets for the next launch.
+template <int UNIT, bool MULTI>
+__device__ __forceinline__ void sweep_finish_black(const SweepArgs &b, int na)
+{
+  sweep_last_cta_poll<UNIT, MULTI>(b, na, gridDim.x, [](const SweepDomain &D) {
+    poll_one(D.st, D.err, D.tol, D.itermax);
+  });
+}
+
+// Window check after every wK-th black launch of a loop (every active domain
+// then stands at the same iteration, a multiple of wK). blockIdx.y = active
+// slot; the CTAs of a slot compare lambda with the domain's snapshot, FP64
+// exact, copy lambda into the snapshot and fold the max into st->wacc; the
+// last CTA applies the window rule and compacts the list.
+template <int UNIT, bool MULTI>
+__global__ void __launch_bounds__(256) k_window_check(SweepArgs b)
+{
+  const int na = b.ctl->nactive;
+  const int slot = blockIdx.y;
+  double dmax = 0.0;
+  double *dst = nullptr;
+  if (slot < na) {
+    const SweepDomain &D = sweep_dom<MULTI>(b, slot);
+    if (D.wK > 0) {
+      dst = &D.st->wacc;
+      const float4 *L = reinterpret_cast<const float4 *>(D.lam);
+      float4 *S = reinterpret_cast<float4 *>(D.snap);
+      const long n4 = D.wn >> 2;
+      for (long i = threadIdx.x + (long)blockIdx.x * blockDim.x; i < n4; i += (long)gridDim.x * blockDim.x) {
+        const float4 a = L[i], o = S[i];
+        const double d[4] = {fabs((double)a.x - (double)o.x), fabs((double)a.y - (double)o.y),
+                             fabs((double)a.z - (double)o.z), fabs((double)a.w - (double)o.w)};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (d[q] > dmax || d[q] != d[q]) dmax = d[q];
+        S[i] = a;
+      }
+    }
+  }
+  block_max_to(dst, dmax);
+  sweep_last_cta_poll<UNIT, MULTI>(b, na, gridDim.x * gridDim.y, [](const SweepDomain &D) {
+    if (D.wK > 0) window_poll_one(D);
+  });
 }
 
 // Slot of `active` holding unit u: the last slot with uoff[slot] <= u.

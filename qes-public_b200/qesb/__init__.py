@@ -59,7 +59,7 @@ class Stats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("residual", C.c_double),
                 ("ms_total", C.c_double), ("ms_sor", C.c_double), ("path", C.c_int),
                 ("sweeps_per_launch", C.c_int), ("launches", C.c_int), ("pre_iterations", C.c_int),
-                ("max_divergence", C.c_double)]
+                ("max_divergence", C.c_double), ("window_drift", C.c_double)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -105,6 +105,7 @@ def lib() -> C.CDLL:
             "qesb_get_residual_history": ([V, V, C.c_int], C.c_int),
             "qesb_set_tolerance": ([V, C.c_float], C.c_int),
             "qesb_set_prephase": ([V, C.c_float, C.c_float, C.c_int], C.c_int),
+            "qesb_set_window_rule": ([V, C.c_int, C.c_double], C.c_int),
             "qesb_time_sweeps": ([V, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)], C.c_int),
             "qesb_autotune": ([V, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int], C.c_int),
             "qesb_solve_batch": ([C.POINTER(V), C.c_int, C.c_int, C.POINTER(V), C.POINTER(V), C.POINTER(V),
@@ -310,6 +311,12 @@ class Solver_B200:
     def set_prephase(self, omega: float, tol: float = 1e-3, max_iterations: int = 10000):
         """Over-relaxed SOR pre-phase before the reference loop (omega 0: off)."""
         check(lib().qesb_set_prephase(self._h, float(omega), float(tol), int(max_iterations)))
+
+    def set_window_rule(self, window: int, tol: float = 0.0):
+        """Window stopping rule: the reference loop also stops after every
+        window-th iteration n when FP64 max|lambda_n - lambda_(n-window)| <= tol
+        (window 0: off, the reference's rule alone)."""
+        check(lib().qesb_set_window_rule(self._h, int(window), float(tol)))
 
     def set_tolerance(self, tol: float):
         self.tol = np.float32(tol)

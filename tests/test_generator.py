@@ -96,3 +96,19 @@ def test_city_inflow_reuses_geometry():
     got = qesb.city_inflow(w, other)
     for a, b in ((got.u0, ref.u0), (got.v0, ref.v0), (got.w0, ref.w0), (got.e, ref.e), (got.icellflag, ref.icellflag)):
         np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("name,seed", [("city128", 1001), ("city128", 1002), ("city256", 500000), ("city256", 500001)])
+def test_reference_leg_cities_equal_the_product_generator(name, seed):
+    """The benchmark's reference leg builds its cities without the product
+    library (oracle/city.py: the layout, flags and inflow restated in C, the
+    walls and solid faces by the reference's Wall.cpp); they must be the
+    product generator's cities bit for bit."""
+    from oracle import city as OC
+
+    wr = OC.random_city(name, seed)
+    wp, _ = qesb.random_city(name, seed)
+    np.testing.assert_array_equal(wr.domain.dz_array, wp.domain.dz_array)
+    for k in ("icellflag", "e", "f", "g", "h", "m", "n", "u0", "v0", "w0"):
+        np.testing.assert_array_equal(getattr(wr, k), getattr(wp, k), err_msg=k)

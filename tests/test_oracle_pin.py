@@ -64,3 +64,32 @@ def test_fp64_same_sor_close_to_fp32(golden):
     assert it == 2000 and it8 < 2000  # FP64 converges; FP32 plateaus at its ulp
     assert np.abs(u - u8).max() < 1e-3
     assert np.abs(L - L8).max() / np.abs(L8).max() < 1e-4
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build oracle/_ref absent")
+def test_window_rule_stop_matches_chained_reference_solves():
+    """The window rule (stop after iteration n, a multiple of K, when
+    max|lambda_n - lambda_(n-K)| <= wtol in double) restated in the oracle
+    stops where the reference's own red-black solver, run K iterations per
+    Solver::solve call with lambda carried over and the drift taken here in
+    numpy, first meets it; and with the same lambda."""
+    import qesb
+
+    d = qesb.Domain(40, 34, 14, 2.0, 2.0, 1.0, qesb.city_dz(14, 1.0, 1.03))
+    c = qesb.city_random(d, 77, 5, fp=(6, 14), h=(4, 16))
+    w = qesb.city_build(d, c.buildings, c.inflow)
+    K, wtol = 16, 2e-3
+    L, it, stop, drift = O.sor_window(d, w, O.divergence(d, w), 1e-9, 4000, K, wtol)
+    assert stop == 2 and it % K == 0 and drift <= wtol
+    lam = np.zeros(d.numCellCentered(), np.float32)
+    n = 0
+    while True:
+        _, _, _, nxt, _ = O.ref_solve(d, w, -1.0, K, kind=1, lam=lam)
+        n += K
+        dr = float(np.abs(nxt.astype(np.float64) - lam.astype(np.float64)).max())
+        lam = nxt
+        if dr <= wtol:
+            break
+        assert n < 4000
+    assert n == it and dr == drift
+    np.testing.assert_array_equal(lam, L)

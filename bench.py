@@ -5,44 +5,42 @@ Workload: held-out synthetic cities of 256 x 256 x 64 cells (dx = dy = 2 m,
 z stretched 1 m x 1.03^k, 40-80 seed-placed cuboid buildings, power-law
 inflow from a random direction), seeds 500000 + i, disjoint from the
 warm-start network's training seeds. One step = one batch of B domains
-(default 8) taken from their inputs in HBM to corrected winds in HBM:
+(default 8) taken from their inputs in HBM to corrected winds in HBM.
 
-  prephase (the headline `value`): per domain, the divergence R, an
-      over-relaxed red-black SOR pre-phase from lambda = 0 (omega PRE_OMEGA, to
-      max|dlambda| <= PRE_TOL in FP64) as the warm start, then the reference
-      loop (omega 1.78, max|dlambda| <= 1e-3 in FP64, at most 10 000
-      iterations) and the velocity correction; all B domains iterate together
-      in qesb_solve_batch (persistent red/black launches in CUDA-graph chunks,
-      each domain stopping on its own rule). ms per domain = step time / B.
-  arms: the same batch as plain SOR from lambda = 0, the learned network's
-      prediction as the start (BF16 tcgen05 convolutions, FP32 accumulation),
-      network + pre-phase, and pre-phase alone, each with its iterations and
-      its winds' max error against a converged field (first two domains).
-  plain_single: the plain arm with the domains solved one after another.
+Stopping rule, the same for every arm and for the reference: the reference
+loop `while (iter < itermax && max_error > tol)` with the reference's own
+tol = 1e-9 (never met in FP32) and itermax = 10000, plus the window rule:
+after every WINDOW-th iteration n the loop also ends when
+max|lambda_n - lambda_(n - WINDOW)| <= WINDOW_TOL (FP64, all cells). With
+it, plain SOR's winds land within 1e-3 m/s of the converged field; the
+per-iteration change alone never falls below the FP32 rounding flutter.
 
-The reference's own tolerance (1e-9) is never reached in FP32, so every arm
-stops at 1e-3, the same rule.
+Arms (all batched, qesb_solve_batch, each domain stopping on its own):
+  plain             red-black SOR from lambda = 0 (the method's fallback and judge)
+  prephase          an over-relaxed red-black pre-phase from lambda = 0 (omega
+                    PRE_OMEGA to max|dlambda| <= PRE_TOL) as the warm start
+  network           the learned network's prediction as the start
+  network+prephase  the network's start, then the pre-phase
+each then running the reference loop to the rule and the velocity
+correction. `value` is the HEADLINE arm's ms per domain = step time / B.
 
-  e2e            the warm step through the host API: pinned host inputs copied
-                 in (qesb_set_inputs) and u, v, w copied out each step.
-  roofline       the SOR sweep kernel of the plain single solves: algorithmic
-                 bytes (36 B per updated cell per iteration) over its measured
-                 device time per iteration (CUDA events, inside the graphs).
-  network        tensor-core rate of one warm-start forward pass.
-  reference_gpu  the reference's own GPU solver (Solver_GPU_GlobalMemory, built
-                 from its sources into oracle/_ref) on the first domain, from
-                 lambda = 0, same tolerance: wall ms, the solve() call.
-  cpu_baseline   the reference's Solver_CPU_RB (oracle/_ref) on this host's
-                 cores: a bounded sample of iterations, scaled by the iterations
-                 the reference needs to reach the rule (tests/golden/ref_iters.json).
+  e2e            the headline step through the host API: pinned host inputs
+                 copied in (qesb_set_inputs), u, v, w copied out, each step.
+  roofline       the red/black list sweep, the kernel that dominates the step:
+                 the bytes the layout moves per updated cell and iteration
+                 (17 B) over the device time of every sweep launch of the timed
+                 steps (CUDA events around the sweep loops, qesb_stats.ms_sweeps).
+  cpu_baseline   the reference's Solver_CPU_RB (oracle/_ref) run in full, to
+                 the rule's iteration count, on this host's cores.
 
 --impl reference runs only the reference CPU solver (rank 0), same metric.
-Multi-GPU (torchrun): each rank solves its own batch (seeds offset by rank);
-no data crosses ranks ("scaling": "weak").
+--gpus N without torchrun re-launches itself as N ranks; each rank solves
+its own batch (seeds offset by rank); no data crosses ranks ("scaling": "weak").
 """
 import argparse
 import json
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -55,26 +53,26 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "qes-public_b200"))
 sys.path.insert(0, ROOT)
 
-TOL = 1e-3
+TOL = 1e-9          # the reference's own tolerance (Solver.h), never met in FP32
 ITERMAX = 10000
+WINDOW, WINDOW_TOL = 32, 4e-3
 WORKLOAD = "city256"
 SEED0 = 500000
 METRIC = "ms to SOR tolerance per domain: learned warm start vs plain SOR, 1 B200"
-BYTES_PER_CELL_ITER = 36  # 6 coefficients + R read (28 B), lambda read + write (8 B)
 # Bytes the packed red/black sweep must move per updated cell and iteration:
 # its colour's lambda read + write (8), the other colour's lambda read (4),
 # R (4) and the wall mask (1).
 MOVED_BYTES_PER_CELL_ITER = 17
+ALG_BYTES_PER_CELL_ITER = 36  # 6 coefficients + R read (28 B), lambda read + write (8 B)
 SIZE_ITERS = 300  # iterations per timed solve of the size sweep
-# Over-relaxed pre-phase of the warm start on this grid: omega and its stopping
-# tolerance, picked by a sweep of omega in {1.90 .. 1.98} x tol in {1e-3, 3e-3}
-# on 256x256x64 cities (every seed tried preferred 1.97 / 3e-3; 1.98 stalled
-# on some).
 PRE_OMEGA = 1.97
-PRE_TOL = 3e-3
+PRE_TOL = 2e-3
+HEADLINE = "prephase"
+ARMS = {"plain": (False, False), "prephase": (False, True), "network": (True, False),
+        "network+prephase": (True, True)}
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -82,32 +80,91 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--batch", type=int, default=8, help="domains per step")
+    ap.add_argument("--backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process-group backend for N > 1 (gloo: the CPU rehearsal of --plan)")
+    ap.add_argument("--plan", action="store_true",
+                    help="print each rank's share of the work and exit (no GPU work; runs on CPU with gloo)")
     ap.add_argument("--weights", default=None, help="warm-start network (default: the committed weights)")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 same-SOR error and divergence checks")
     ap.add_argument("--no-sizes", action="store_true", help="skip the 400^2 and 800^2 sweep-speed section")
     ap.add_argument("--no-fire-loop", action="store_true", help="skip the fire-step section")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble section")
     ap.add_argument("--variant", type=int, default=-1, help="sweep variant for the profiling drivers (-1: autotune)")
     ap.add_argument("--profile-solve", type=int, default=0,
                     help="profiling driver: one solve of this many iterations (tol 0) with --variant, exit")
     ap.add_argument("--sweeps-only", type=int, default=0,
                     help="profiling driver: set up the workload, run this many sweep launches, exit")
     ap.add_argument("--ensemble", action="store_true",
-                    help="batched ensemble: 64 cities of uneven size x 36 wind directions (solves/s, p50/p99)")
+                    help="batched ensemble alone: cities of uneven size x 36 wind directions (solves/s, p50/p99)")
     ap.add_argument("--ensemble-domains", type=int, default=64)
     ap.add_argument("--fire-loop", type=int, default=0,
                     help="QES-Fire solve pattern: this many fire steps warm-started from the previous lambda, exit")
     ap.add_argument("--profile-batch", action="store_true",
-                    help="profiling driver: the headline batch (pre-phase pipeline) once untimed, once more, exit")
+                    help="profiling driver: the headline batch once untimed, once more, exit")
     ap.add_argument("--forward-only", type=int, default=0,
                     help="profiling driver: run this many warm-start forward passes on one domain, exit")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def maybe_relaunch(args):
+    """--gpus N > 1 outside torchrun: run this script as N ranks (one process
+    per GPU) and exit with their status. Inside torchrun the world size must
+    be N."""
+    from qesb import shard
+
+    world = int(os.environ.get("WORLD_SIZE", 0))
+    if world == 0 and args.gpus > 1:
+        cmd = shard.launch_command(sys.executable, os.path.abspath(__file__), args.gpus, _free_port(), sys.argv[1:])
+        sys.exit(subprocess.call(cmd))
+    if world and world != args.gpus:
+        raise SystemExit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE {world}")
+
+
+def init_group(args, world, local):
+    """Process group of the ranks (no-op for one rank): NCCL over the GPUs, or
+    gloo for the CPU rehearsal; a short timeout so that a missing rank ends in
+    an error."""
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    if args.backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(args.backend, timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def run_plan(args):
+    """Each rank's share of the headline workload, gathered and printed by
+    rank 0 (the launch and sharding logic without GPU work)."""
+    from qesb import shard
+
+    rank, local, world = dist_env()
+    dist = init_group(args, world, local)
+    mine = {"rank": rank, "seeds": shard.rank_seeds(SEED0, args.batch, rank)}
+    everything = shard.gather_lists([mine])
+    comm = dist.get_world_size() if dist else 1
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"plan": {"world": world, "communicator_size": comm, "backend": args.backend,
+                                   "shares": sorted(everything, key=lambda x: x["rank"])}}), flush=True)
 
 
 class ClockSampler:
@@ -182,12 +239,24 @@ def pinned_copy(torch, a):
     return t, arr
 
 
-def ref_iterations(key, solver="Solver_CPU_RB"):
+def ref_counts():
+    """The reference's own iteration counts to the rule (tests/golden/ref_iters.json,
+    made by tests/golden/make_ref_iters.py from the reference build)."""
     path = os.path.join(ROOT, "tests", "golden", "ref_iters.json")
+    doc = json.load(open(path))
+    r = doc["rule"]
+    assert (r["tol"], r["itermax"], r["window"], r["window_tol"]) == (TOL, ITERMAX, WINDOW, WINDOW_TOL), r
+    return doc
+
+
+def cpu_model():
     try:
-        return json.load(open(path))[key][solver]["iterations"]
-    except (OSError, KeyError):
-        return None
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def _quiet(fn):
@@ -206,96 +275,162 @@ def _quiet(fn):
         os.close(null)
 
 
-def reference_cpu_measure(workload, seed, seconds, threads):
-    """Reference Solver_CPU_RB (oracle/_ref), `threads` OpenMP threads, timed on a
-    bounded sample of iterations, scaled to the reference's iterations to the
-    stopping rule. tol < 0 makes the loop run exactly `sample` iterations, so the
-    reference's racy max_error reset (Solver_CPU_RB.cpp:166) cannot end it early."""
+# ---------------------------------------------------------------------------
+# the reference on the host
+# ---------------------------------------------------------------------------
+def reference_solves(seeds, threads, counts, keep_winds=False):
+    """Full solves of the reference's Solver_CPU_RB (oracle/_ref) on the
+    seeds' cities, built without the product library (oracle/city.py), each
+    for the iterations the reference needs to reach the rule (tol < 0 and
+    itermax = that count: the same iterates as the rule's run, without the
+    OpenMP race on its max_error reset, Solver_CPU_RB.cpp:166). Returns
+    [(seed, seconds of solve(), iterations, winds or None)]."""
+    from oracle import city as OC
     from oracle import oracle as O
 
     O.ref_set_threads(threads)
-    w = make_city(workload, seed)
-    d = w.domain
-    _, _, _, _, t_cal = _quiet(lambda: O.ref_solve(d, w, -1.0, 3, kind=1, want_lambda=False))
-    per_it = max(t_cal / 3, 1e-6)
-    sample = int(max(5, min(ITERMAX, seconds / per_it)))
-    _, _, _, _, t = _quiet(lambda: O.ref_solve(d, w, -1.0, sample, kind=1, want_lambda=False))
-    ms_it = 1e3 * t / sample
-    iters = ref_iterations(f"{workload}:{seed}") or ref_iterations(workload)
-    return ms_it, sample, iters
+    out = []
+    for seed in seeds:
+        w = OC.random_city(WORKLOAD, seed)
+        n = counts[f"{WORKLOAD}:{seed}"]["Solver_CPU_RB"]["iterations"]
+        u, v, ww, _, t = _quiet(lambda: O.ref_solve(w.domain, w, -1.0, n, kind=1, want_lambda=False))
+        out.append((seed, t, n, (w, u, v, ww) if keep_winds else None))
+    return out
+
+
+def serial_solver_cpu_sample(seed, counts, iters=60):
+    """Serial Solver_CPU (the reference's default build) timed on a bounded
+    sample of its iterations on one core, and its own iteration count to the
+    rule: the extrapolated time of one full serial solve."""
+    from oracle import city as OC
+    from oracle import oracle as O
+
+    w = OC.random_city(WORKLOAD, seed)
+    _, _, _, _, t = _quiet(lambda: O.ref_solve(w.domain, w, -1.0, iters, kind=0, want_lambda=False))
+    n = counts[f"{WORKLOAD}:{seed}"]["Solver_CPU"]["iterations"]
+    return {"seed": seed, "iterations_timed": iters, "ms_per_iteration": 1e3 * t / iters,
+            "iterations_to_rule": n, "ms_per_solve_extrapolated": 1e3 * t / iters * n, "cores": 1,
+            "note": "extrapolated: a bounded sample of iterations x the reference's own count to the rule"}
 
 
 def run_reference(args):
-    """The reference's Solver_CPU_RB on this host, per city of the headline
-    batch: ms per iteration sampled on the first city (every city has the same
-    grid), times the mean of the iterations the reference needs on each of the
-    batch's cities (tests/golden/ref_iters.json, equal to this solver's plain
-    iteration counts)."""
+    """The reference's Solver_CPU_RB on this host's cores, one full solve of one
+    headline city per step (cycling through the batch's seeds), to the rule's
+    iteration count. ms per domain = the mean of the timed solves."""
     rank, _, world = dist_env()
     if rank != 0:
         return
+    counts = ref_counts()
     threads = os.cpu_count() or 1
-    seed = SEED0 if args.workload == WORKLOAD else 0
-    steps = []
-    sample = iters = None
-    for _ in range(max(args.steps, 1)):
-        ms_it, sample, iters = reference_cpu_measure(args.workload, seed,
-                                                     max(2.0, args.cpu_seconds / max(args.steps, 1)), threads)
-        steps.append(ms_it)
-    ms_it = statistics.median(steps)
-    if args.workload == WORKLOAD:
-        per_city = [ref_iterations(f"{WORKLOAD}:{SEED0 + i}") for i in range(args.batch)]
-        if all(per_city):
-            iters = float(np.mean(per_city))
-    value = ms_it * iters if iters else None
+    seeds = [SEED0 + i for i in range(args.batch)]
+    from oracle import city as OC
+
+    t_build = time.time()
+    for sd in seeds:  # untimed: the inputs of every step
+        OC.random_city(WORKLOAD, sd)
+    build_s = time.time() - t_build
+    for k in range(args.warmup):
+        reference_solves([seeds[k % len(seeds)]], threads, counts)
+    t0 = time.time()
+    timed = []
+    for k in range(args.steps):
+        timed += reference_solves([seeds[k % len(seeds)]], threads, counts)
+    wall = time.time() - t0
+    ms = [1e3 * t for _, t, _, _ in timed]
+    value = float(np.mean(ms))
+    serial = serial_solver_cpu_sample(seeds[0], counts)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.workload} seeds {seed}..{seed + args.batch - 1}",
-                   "solver": "Solver_CPU_RB (reference, OpenMP)",
-                   "tol": TOL, "itermax": ITERMAX},
+        "config": {"workload": f"{WORKLOAD} (256x256x64), held-out seeds {seeds[0]}..{seeds[-1]}",
+                   "batch": args.batch, "tol": TOL, "itermax": ITERMAX, "window": WINDOW,
+                   "window_tol": WINDOW_TOL, "solver": "Solver_CPU_RB (reference, OpenMP), one city per step"},
         "cpu_baseline": {"value": value, "unit": "ms", "cores": threads, "kind": "reference",
-                         "sample": f"{sample} red-black iterations per step timed on seed {seed}, x {iters} "
-                                   f"iterations (mean over the batch's cities) the reference needs to reach "
-                                   f"tol {TOL}"},
+                         "sample": f"{args.steps} full Solver_CPU_RB solves to the rule ("
+                                   f"{', '.join(str(n) for _, _, n, _ in timed[:len(seeds)])} iterations), "
+                                   f"one per step, {threads} threads, {cpu_model()}"},
         "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "ms_per_iteration": ms_it,
+        "timed_wall_s": wall, "input_build_s": build_s,
+        "ms_per_solve": ms, "iterations": [n for _, _, n, _ in timed],
+        "solver_cpu_serial": serial,
     }
     print(json.dumps(line), flush=True)
 
 
-def fp64_checks(w, seed, st, lam, winds):
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def fp64_checks(w, seed, st, lam, winds, ref_div=None):
     """The headline pipeline's FP32 result on one city against an FP64 run of
     the same SOR (same phases, same iteration counts, oracle restatement in
-    double), and its FP64 final divergence against the reference solver's
-    (Solver_CPU_RB run for the iterations it needs to reach the same rule)."""
+    double), and its FP64 final divergence beside the reference solver's."""
     from oracle import oracle as O
 
     d = w.domain
     t0 = time.time()
-    u64, v64, w64, L64, _, _ = O.solve_f64(d, w, -1.0, st["iterations"],
-                                           phases=[(PRE_OMEGA, -1.0, st["pre_iterations"])])
+    phases = [(PRE_OMEGA, -1.0, st["pre_iterations"])] if st["pre_iterations"] else None
+    u64, v64, w64, L64, _, _ = O.solve_f64(d, w, -1.0, st["iterations"], phases=phases)
     t_f64 = time.time() - t0
     lam_err = float(np.abs(lam.astype(np.float64) - L64).max() / max(np.abs(L64).max(), 1e-30))
     wind_err = max(float(np.abs(a.astype(np.float64) - b).max()) for a, b in zip(winds, (u64, v64, w64)))
     out = {"seed": seed, "pre_iterations": st["pre_iterations"], "iterations": st["iterations"],
            "lambda_max_rel_err_vs_fp64": lam_err, "wind_max_err_vs_fp64_m_s": wind_err,
            "max_divergence_fp64": st["max_divergence"], "fp64_run_s": t_f64}
-    riters = ref_iterations(f"{WORKLOAD}:{seed}")
-    if riters:
-        O.ref_set_threads(os.cpu_count() or 1)
-        ur, vr, wr, _, _ = _quiet(lambda: O.ref_solve(d, w, -1.0, riters, kind=1, want_lambda=False))
-        out["reference_max_divergence"] = O.max_divergence(d, w.icellflag, ur, vr, wr)
-        out["reference"] = f"Solver_CPU_RB, {riters} iterations (its count to tol {TOL})"
+    if ref_div is not None:
+        out["reference_max_divergence"] = ref_div
+        out["reference"] = "Solver_CPU_RB to the rule on the same city (its own iteration count)"
+    return out
+
+
+def precision_device(s, outs, use_net, use_pre, net=None, stream=None, omega=PRE_OMEGA):
+    """One solve of the handle's domain with the arm's start, to the rule, then
+    the same SOR in FP64 on the device from the same start with its iteration
+    counts (qesb_fp64_same_sor): the FP32 result's lambda and wind errors."""
+    import torch
+
+    s.set_prephase(omega if use_pre else 0.0, PRE_TOL, ITERMAX)
+    if use_net:
+        net.warm_start(s, stream)
+        lam0 = s.lambda_
+    else:
+        s.resetLambda()
+        lam0 = None
+    ptrs = [o.data_ptr() for o in outs]
+    st = s.solve_device(ITERMAX, *ptrs)
+    torch.cuda.synchronize()
+    rep = s.fp64_same_sor(omega if use_pre else 0.0, st["pre_iterations"], st["iterations"], *ptrs, lambda0=lam0)
+    return st, {"pre_iterations": st["pre_iterations"], "iterations": st["iterations"],
+                "stop": st["converged"], "lambda_max_rel_err_vs_fp64": rep["lambda_max_rel_err"],
+                "wind_max_err_vs_fp64_m_s": rep["wind_max_err"], "max_divergence_fp64": st["max_divergence"],
+                "fp64_run_ms": rep["ms"], "how": "qesb_fp64_same_sor: the same red-black SOR in FP64 on the "
+                                                 "device, same start and iteration counts"}
+
+
+def precision_city800():
+    """The FP32 pipeline on one 800 x 800 x 128 city (150 buildings, seed 0)
+    against an FP64 run of the same SOR (configuration 2's precision report)."""
+    import torch
+
+    import qesb
+
+    w = make_city("city800", 0)
+    nf = w.domain.numFaceCentered()
+    outs = [torch.empty(nf, dtype=torch.float32, device="cuda") for _ in range(3)]
+    with qesb.Solver_B200(w.domain, TOL) as s:
+        s.set_inputs(w)
+        s.set_window_rule(WINDOW, WINDOW_TOL)
+        st, out = precision_device(s, outs, False, True, omega=qesb.prephase_omega(800, 800))
+    out.update({"seed": 0, "grid": [800, 800, 128], "ms_solve": st["ms_total"],
+                "pre_omega": qesb.prephase_omega(800, 800)})
     return out
 
 
 def size_rates(peak, workloads=("city400", "city800")):
     """Sweep speed at the large single-city configurations: one autotuned
-    solve of SIZE_ITERS iterations (tolerance 0, so every iteration runs)
-    after a warm-up solve, per workload; the SOR time comes from the solve's
-    own device events around its graphs."""
+    solve of SIZE_ITERS iterations (tolerance -1, so every iteration runs)
+    after a warm-up solve, per workload; the time is the solve's own sweep
+    loop (CUDA events around it)."""
     import qesb
 
     out = {}
@@ -303,20 +438,20 @@ def size_rates(peak, workloads=("city400", "city800")):
         w, _ = qesb.random_city(name, 0)
         Nx, Ny, Nz = w.domain.base
         upd = (Nx - 2) * (Ny - 2) * (Nz - 1)
-        with qesb.Solver_B200(w.domain, 0.0) as s:
+        with qesb.Solver_B200(w.domain, -1.0) as s:
             s.set_inputs(w)
             variant, _ = s.autotune()
             per = []
             for _ in range(3):
                 s.resetLambda()
                 st = s.solve(w, SIZE_ITERS, set_inputs=False)
-                per.append(st["ms_sor"] / st["iterations"])
+                per.append((st["ms_sweeps"] if st["ms_sweeps"] > 0 else st["ms_sor"]) / st["iterations"])
         ms_it = statistics.median(per[1:])
-        alg = BYTES_PER_CELL_ITER * upd / (ms_it * 1e-3) / 1e9
         moved = MOVED_BYTES_PER_CELL_ITER * upd / (ms_it * 1e-3) / 1e9
+        alg = ALG_BYTES_PER_CELL_ITER * upd / (ms_it * 1e-3) / 1e9
         out[name] = {"grid": [Nx, Ny, Nz], "updated_cells": upd, "variant": variant, "iterations": SIZE_ITERS,
-                     "us_per_iteration": 1e3 * ms_it, "algorithmic_gbs": alg, "algorithmic_frac": alg / peak,
-                     "moved_gbs": moved, "moved_frac": moved / peak}
+                     "us_per_iteration": 1e3 * ms_it, "moved_gbs": moved, "moved_frac": moved / peak,
+                     "algorithmic_36B_gbs": alg}
     return out
 
 
@@ -372,9 +507,9 @@ def run_fire_loop(args, steps=None, print_line=True):
     lambda = 0, then `steps` fire steps, each with new u0 (fire_inflow) and
     Solver::solve without resetLambda, so every solve starts from the previous
     step's lambda, as the reference's fire loop does. Three arms on the same
-    inputs: warm (that behaviour), cold (resetLambda before every step), warm
-    + over-relaxed pre-phase. Device time per solve (CUDA events) and
-    iterations."""
+    inputs, every solve to the rule: warm (that behaviour), cold (resetLambda
+    before every step), warm + over-relaxed pre-phase. Device time per solve
+    (CUDA events) and iterations."""
     import torch
 
     import qesb
@@ -386,6 +521,7 @@ def run_fire_loop(args, steps=None, print_line=True):
     arms = {}
     with qesb.Solver_B200(d, TOL) as s:
         s.set_inputs(w)
+        s.set_window_rule(WINDOW, WINDOW_TOL)
         s.autotune()
         for arm in ("warm", "cold", "warm+prephase"):
             s.set_prephase(PRE_OMEGA if arm == "warm+prephase" else 0.0, PRE_TOL, ITERMAX)
@@ -420,86 +556,79 @@ def network_flops(net, s):
     return total
 
 
+def peaks():
+    try:
+        p = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(p["hbm_gbs"]), "measured", float(p.get("bf16_tflops", 1590.0))
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback", 1590.0
+
+
 def run_b200(args):
     import torch
 
     import qesb
+    from qesb import shard
     from qesb import warmstart as ws
 
     rank, local, world = dist_env()
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = init_group(args, world, local)
     dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(device=dev)
     B = args.batch
-    seeds = [SEED0 + rank * B + i for i in range(B)]  # each rank its own batch: weak scaling
+    seeds = shard.rank_seeds(SEED0, B, rank)  # each rank its own batch: weak scaling
     cities = [make_city(args.workload, sd) for sd in seeds]
     d0 = cities[0].domain
     Nx, Ny, Nz = d0.base
     updated = (Nx - 2) * (Ny - 2) * (Nz - 1)
     nf = d0.numFaceCentered()
 
-    solvers = [qesb.Solver_B200(w.domain, TOL, device=dev) for w in cities]
+    def new_solvers(strm):
+        out = [qesb.Solver_B200(w.domain, TOL, device=dev) for w in cities]
+        for s in out:
+            s.set_stream(strm.cuda_stream)
+            s.set_window_rule(WINDOW, WINDOW_TOL)
+        return out
+
+    solvers = new_solvers(stream)
     for s, w in zip(solvers, cities):
-        s.set_stream(stream.cuda_stream)
         s.set_inputs(w)
     # autotuners (untimed set-up, like a library's algorithm search): the sweep
     # shape for single solves of this grid, and the one for this batch's list
-    variant, variant_us = solvers[0].autotune()
+    variant, _ = solvers[0].autotune()
     batch_variant, _ = qesb.autotune_batch(solvers)
     wpath = args.weights or ws.DEFAULT_WEIGHTS
     net = ws.WarmStartNet.from_file(wpath, device=dev)
 
     def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
+        if dist:
             dist.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        import torch.distributed as dist
-
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return shard.max_over_ranks(x, device=f"cuda:{dev}") if dist else x
 
     outs = [[torch.empty(nf, dtype=torch.float32, device=f"cuda:{dev}") for _ in range(3)] for _ in range(B)]
     uvw = [[o[q].data_ptr() for o in outs] for q in range(3)]
-    launches_per_warm = 4 + (4 * net.nlev - 1) + (net.nlev - 1)  # R, input (2), apply + convs + pools
+    launches_per_net = 4 + (4 * net.nlev - 1) + (net.nlev - 1)  # R, input (2), apply + convs + pools
 
-    def set_pre(on):
-        for s in solvers:
-            s.set_prephase(PRE_OMEGA if on else 0.0, PRE_TOL, ITERMAX)
+    def set_arm(sset, use_pre):
+        for s in sset:
+            s.set_prephase(PRE_OMEGA if use_pre else 0.0, PRE_TOL, ITERMAX)
 
-    def batch_step(use_net, use_pre):
+    def batch_step(use_net, use_pre, sset=None, ptrs=None, strm=None):
+        sset, ptrs, strm = sset or solvers, ptrs or uvw, strm or stream
+
         def step():
-            set_pre(use_pre)
-            for s in solvers:
+            set_arm(sset, use_pre)
+            for s in sset:
                 if use_net:
-                    net.warm_start(s, stream.cuda_stream)
+                    net.warm_start(s, strm.cuda_stream)
                 else:
                     s.resetLambda()
-            st = qesb.solve_batch(solvers, ITERMAX, *uvw)
-            return st, (B * launches_per_warm if use_net else 0) + 6 * B + 1 + st[0]["launches"]
+            st = qesb.solve_batch(sset, ITERMAX, *ptrs)
+            return st, (B * launches_per_net if use_net else 0) + 6 * B + st[0]["launches"]
         return step
-
-    warm_step = batch_step(False, True)  # the headline pipeline: over-relaxed pre-phase, reference loop
-
-    def plain_single_step():
-        set_pre(False)
-        sts = []
-        for s, o in zip(solvers, outs):
-            s.resetLambda()
-            sts.append(s.solve_device(ITERMAX, o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr()))
-        return sts, sum(x["launches"] for x in sts)
 
     def timed(fn, steps, warmup, clocks=False):
         # the clock sampler starts before the warm-up so that its first samples
@@ -528,44 +657,45 @@ def run_b200(args):
         barrier()
         return e0.elapsed_time(e1) / steps, res, launches, (clk.summary() if clk else None)
 
-    # converged fields of the first two domains (long over-relaxed runs, untimed)
-    # to state each arm's wind error
+    # converged fields of the first two domains (long over-relaxed runs, then the
+    # reference omega, no stopping rule; untimed) to state each arm's wind error
     conv = []
     for s, o in list(zip(solvers, outs))[:2]:
-        s.set_prephase(PRE_OMEGA, -1.0, 4000)
+        s.set_window_rule(0, 0.0)
+        s.set_tolerance(-1.0)
+        s.set_prephase(1.97, -1.0, 8000)
         s.resetLambda()
-        s.solve_device(1, o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr())
+        s.solve_device(3000, o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr())
         conv.append([t.clone() for t in o])
+        s.set_tolerance(TOL)
+        s.set_window_rule(WINDOW, WINDOW_TOL)
 
     def wind_err():
         return max(float((o[q] - c[q]).abs().max()) for o, c in zip(outs, conv) for q in range(3))
 
-    arms = {}
-    for name, (use_net, use_pre) in {"plain": (False, False), "network": (True, False),
-                                     "network+prephase": (True, True)}.items():
+    arms, arm_res = {}, {}
+    for name, (use_net, use_pre) in ARMS.items():
+        if name == HEADLINE:
+            continue
         ms, res, _, _ = timed(batch_step(use_net, use_pre), max(1, args.steps // 2), 1)
+        arm_res[name] = res
         arms[name] = {"ms_per_domain": max_over_ranks(ms) / B, "iterations": [x["iterations"] for x in res[-1]],
                       "pre_iterations": [x["pre_iterations"] for x in res[-1]], "wind_err_vs_converged": wind_err()}
-    ms_warm, res_warm, launches, clocks = timed(warm_step, args.steps, args.warmup, clocks=True)
-    ms_warm = max_over_ranks(ms_warm)
-    arms["prephase"] = {"ms_per_domain": ms_warm / B, "iterations": [x["iterations"] for x in res_warm[-1]],
-                        "pre_iterations": [x["pre_iterations"] for x in res_warm[-1]],
-                        "wind_err_vs_converged": wind_err()}
+    use_net, use_pre = ARMS[HEADLINE]
+    head_step = batch_step(use_net, use_pre)
+    ms_head, res_head, launches, clocks = timed(head_step, args.steps, args.warmup, clocks=True)
+    ms_head = max_over_ranks(ms_head)
+    arms[HEADLINE] = {"ms_per_domain": ms_head / B, "iterations": [x["iterations"] for x in res_head[-1]],
+                      "pre_iterations": [x["pre_iterations"] for x in res_head[-1]],
+                      "wind_err_vs_converged": wind_err()}
     ms_plain = arms["plain"]["ms_per_domain"] * B
-    ms_single, res_single, _, _ = timed(plain_single_step, 1, 1)
-
-    def first_domain_warm():  # the headline pipeline on domain 0 alone (reference GPU comparison)
-        s, o = solvers[0], outs[0]
-        s.set_prephase(PRE_OMEGA, PRE_TOL, ITERMAX)
-        s.resetLambda()
-        return s.solve_device(ITERMAX, o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr()), 0
-
-    ms_first, res_first, _, _ = timed(first_domain_warm, 3, 1)
-    st_first = res_first[-1]
+    # precision of domain 0 under the headline arm: FP64 replay on the device,
+    # and (rank 0, below) the oracle's FP64 restatement on the host as a cross-check
+    st_first, prec_first = precision_device(solvers[0], outs[0], use_net, use_pre, net, stream.cuda_stream)
     lam_first = solvers[0].lambda_
     winds_first = [t.cpu().numpy() for t in outs[0]]
 
-    # ---- end to end through the host API (warm step) -------------------------
+    # ---- end to end through the host API (the headline step) -----------------
     host_keep = [[pinned_copy(torch, a) for a in w.inputs()] for w in cities]  # tensors own the pinned memory
     host_in = [[arr for _, arr in ins] for ins in host_keep]
     host_out = [[torch.empty(nf, dtype=torch.float32, pin_memory=True) for _ in range(3)] for _ in range(B)]
@@ -575,7 +705,7 @@ def run_b200(args):
     def e2e_step():
         for s, ins in zip(solvers, host_in):
             qesb.check(qesb.lib().qesb_set_inputs(s._h, *[a.ctypes.data for a in ins]))
-        st, n = warm_step()
+        st, n = head_step()
         with torch.cuda.stream(stream):
             for o, ho in zip(outs, host_out):
                 for q in range(3):
@@ -593,13 +723,8 @@ def run_b200(args):
     # step's copies still run inside the timed region, the first batch's
     # upload before any overlap; only their order against the other batch's
     # solve changes.
-    import threading
-
     stream2 = torch.cuda.Stream(device=dev)
-    solvers2 = [qesb.Solver_B200(w.domain, TOL, device=dev) for w in cities]
-    for s2 in solvers2:
-        s2.set_stream(stream2.cuda_stream)
-        s2.set_prephase(PRE_OMEGA, PRE_TOL, ITERMAX)
+    solvers2 = new_solvers(stream2)
     solvers2[0].set_option("batch_variant", batch_variant)
     sets, streams = [solvers, solvers2], [stream, stream2]
     outs2 = [[torch.empty(nf, dtype=torch.float32, device=f"cuda:{dev}") for _ in range(3)] for _ in range(B)]
@@ -607,16 +732,14 @@ def run_b200(args):
     set_uvw = [uvw, [[o[q].data_ptr() for o in outs2] for q in range(3)]]
     host_out2 = [[torch.empty(nf, dtype=torch.float32, pin_memory=True) for _ in range(3)] for _ in range(B)]
     set_host_out = [host_out, host_out2]
+    steps_of_set = [batch_step(use_net, use_pre, sets[k], set_uvw[k], streams[k]) for k in range(2)]
 
     def load(k):
         for s_, ins in zip(sets[k], host_in):
             qesb.check(qesb.lib().qesb_set_inputs(s_._h, *[a.ctypes.data for a in ins]))
 
     def solve_read(k):
-        for s_ in sets[k]:
-            s_.set_prephase(PRE_OMEGA, PRE_TOL, ITERMAX)
-            s_.resetLambda()
-        st_ = qesb.solve_batch(sets[k], ITERMAX, *set_uvw[k])
+        st_, _ = steps_of_set[k]()
         with torch.cuda.stream(streams[k]):
             for o, ho in zip(set_outs[k], set_host_out[k]):
                 for q in range(3):
@@ -661,43 +784,38 @@ def run_b200(args):
     for s2 in solvers2:
         s2.close()
 
-    # ---- roofline of the dominant kernel: the list sweep of the headline step ---------
-    # The headline step is ~97 % red/black list sweeps. Its domain-iterations
-    # (pre-phase and reference loop, every domain) times the algorithmic bytes
-    # per updated cell, over the whole timed step (R, layout changes and the
-    # correction included), is a lower bound on the sweep kernel's rate. One
-    # launch is a half-sweep over the active list; per launch of the full list
-    # that is 1/2 x batch x updated cells x 36 B.
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
-        tpeak = float(peaks.get("bf16_tflops", 1590.0))
-    except (OSError, KeyError, ValueError):
-        peak, peak_src, tpeak = 6650.0, "fallback", 1590.0
-    dom_iters = sum(x["iterations"] + x["pre_iterations"] for x in res_warm[-1])
-    achieved = BYTES_PER_CELL_ITER * updated * dom_iters / (ms_warm * 1e-3) / 1e9
-    moved = MOVED_BYTES_PER_CELL_ITER * updated * dom_iters / (ms_warm * 1e-3) / 1e9
-    traffic = None
+    # ---- roofline of the dominant kernel: the red/black list sweep --------------
+    # Every sweep launch of the timed headline steps (pre-phase and reference
+    # loop, the window checks between them included), timed by CUDA events on
+    # the launching stream around the loops (qesb_stats.ms_sweeps); the bytes
+    # are those the split layout must move per updated cell and iteration.
+    peak, peak_src, tpeak = peaks()
+    sweep_ms = sum(r[0]["ms_sweeps"] for r in res_head)
+    dom_iters = sum(x["iterations"] + x["pre_iterations"] for r in res_head for x in r)
+    list_launches = sum(r[0]["launches"] for r in res_head)
+    moved = MOVED_BYTES_PER_CELL_ITER * updated * dom_iters / (sweep_ms * 1e-3) / 1e9
+    alg = ALG_BYTES_PER_CELL_ITER * updated * dom_iters / (sweep_ms * 1e-3) / 1e9
+    traffic, prof_note = None, None
     prof = os.path.join(ROOT, "profiles", "sor_zm_batch_city256.json")
     if os.path.exists(prof):
         try:
-            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+            pj = json.load(open(prof))
+            traffic = pj.get("dram_bytes_per_launch")
+            prof_note = pj.get("launch")
         except ValueError:
             traffic = None
-    headline_sweep = {"domain_iterations": dom_iters, "us_per_domain_iteration": 1e3 * ms_warm / dom_iters,
-                      "moved_gbs_lower_bound": moved, "moved_frac": moved / peak, "batch_variant": batch_variant}
+    roofline = {"bound": "hbm", "achieved": moved, "peak": peak, "unit": "GB/s", "frac": moved / peak,
+                "traffic": traffic, "peak_source": peak_src,
+                "kernel": "red/black list sweep (variant %d): every launch of the timed steps' sweep loops, CUDA "
+                          "events on the launching stream around them" % batch_variant,
+                "bytes_per_cell_iteration": MOVED_BYTES_PER_CELL_ITER,
+                "moved_bytes_per_full_list_launch": MOVED_BYTES_PER_CELL_ITER * updated * B // 2,
+                "traffic_launch": prof_note, "domain_iterations": dom_iters, "sweep_ms": sweep_ms,
+                "launches": list_launches, "us_per_domain_iteration": 1e3 * sweep_ms / dom_iters,
+                "algorithmic_36B_gbs": alg, "algorithmic_36B_frac": alg / peak,
+                "sweep_share_of_step": sweep_ms / (ms_head * args.steps)}
 
-    # the same kernel family on one domain at a time (the plain single solves)
-    sor_ms = [x["ms_sor"] / max(x["iterations"], 1) for x in res_single[-1]]
-    ms_it = statistics.median(sor_ms)
-    alg_bytes = BYTES_PER_CELL_ITER * updated
-    single_domain = {"kernel": "red+black sweep pair (variant %d), per iteration inside the solve graphs" % variant,
-                     "ms_per_iteration": ms_it, "algorithmic_bytes_per_iteration": alg_bytes,
-                     "achieved": alg_bytes / (ms_it * 1e-3) / 1e9,
-                     "frac": alg_bytes / (ms_it * 1e-3) / 1e9 / peak,
-                     "note": "one 256^2 domain's sweep data (~70 MB) stays in L2 between launches"}
-
-    # ---- the sweep at the 400^2 x 100 and 800^2 x 128 configurations ------------------
+    # ---- the sweep at the 400^2 x 100 and 800^2 x 128 configurations ------------
     sizes = None
     if not args.no_sizes:
         try:
@@ -745,180 +863,195 @@ def run_b200(args):
     except Exception as ex:  # noqa: BLE001
         wall_log = {"unavailable": str(ex)[:200]}
 
+    for s in solvers:
+        s.close()
+    solvers = []
+
+    # ---- the batched ensemble (64 uneven cities x 36 directions) -----------------
+    ensemble = None
+    if not args.no_ensemble:
+        try:
+            ensemble = ensemble_run(args, print_line=False, dist=dist, dev=dev)
+        except Exception as ex:  # noqa: BLE001
+            ensemble = {"unavailable": str(ex)[:200]}
+
     # ---- reference GPU solver, CPU baseline, FP64 checks (rank 0, N = 1) --------------
-    ref_gpu = None
-    cpu = None
-    precision = None
+    ref_gpu = cpu = precision = None
     if rank == 0 and world == 1:
-        for s in solvers:
-            s.close()
-        solvers = []
         torch.cuda.synchronize(dev)
-        if not args.no_reference_gpu:
+        counts = None
+        try:
+            counts = ref_counts()
+        except Exception as ex:  # noqa: BLE001
+            cpu = {"value": None, "unit": "ms", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {ex}"}
+        ref_div = None
+        if counts and not args.no_cpu_baseline:
+            try:
+                threads = os.cpu_count() or 1
+                runs = reference_solves(seeds[:2], threads, counts, keep_winds=True)
+                from oracle import oracle as O
+
+                rw, ru, rv, rww = runs[0][3]
+                ref_div = O.max_divergence(rw.domain, rw.icellflag, ru, rv, rww)
+                ms_c = [1e3 * t for _, t, _, _ in runs]
+                cpu = {"value": float(np.mean(ms_c)), "unit": "ms", "cores": threads, "kind": "reference",
+                       "sample": f"full Solver_CPU_RB solves of seeds {seeds[0]}, {seeds[1]} to the rule "
+                                 f"({runs[0][2]}, {runs[1][2]} iterations), {threads} threads, {cpu_model()}; "
+                                 f"ms per solve {', '.join('%.0f' % m for m in ms_c)}",
+                       "solver_cpu_serial": serial_solver_cpu_sample(seeds[0], counts)}
+            except Exception as ex:  # noqa: BLE001
+                cpu = {"value": None, "unit": "ms", "cores": os.cpu_count(), "kind": "reference",
+                       "sample": f"unavailable: {ex}"}
+        if not args.no_reference_gpu and counts:
             try:
                 from oracle import oracle as O
 
                 if O.ref_gpu_available():
                     w = cities[0]
-                    u, v, ww, secs, iters = O.ref_solve_gpu(w.domain, w, TOL, ITERMAX)
-                    ref_gpu = {"ms": 1e3 * secs, "iterations": iters, "seed": seeds[0],
+                    n_rb = counts[f"{WORKLOAD}:{seeds[0]}"]["Solver_CPU_RB"]["iterations"]
+                    _, _, _, secs, iters = O.ref_solve_gpu(w.domain, w, -1.0, n_rb)
+                    ref_gpu = {"ms": 1e3 * secs, "iterations": n_rb, "seed": seeds[0],
                                "solver": "Solver_GPU_GlobalMemory::solve (reference, wall clock incl. its "
-                                         "allocations and copies)"}
+                                         "allocations and copies), the rule's red-black iteration count"}
                 else:
                     ref_gpu = {"unavailable": "oracle/_ref/libqesref_gpu.so not built"}
             except Exception as ex:  # noqa: BLE001
                 ref_gpu = {"unavailable": str(ex)[:200]}
         if not args.no_fp64:
+            precision = {"city256": dict(prec_first, seed=seeds[0])}
             try:
-                precision = fp64_checks(cities[0], seeds[0], st_first, lam_first, winds_first)
+                if not use_net:
+                    precision["city256"]["host_oracle_cross_check"] = fp64_checks(
+                        cities[0], seeds[0], st_first, lam_first, winds_first, ref_div)
             except Exception as ex:  # noqa: BLE001
-                precision = {"unavailable": str(ex)[:200]}
-        if not args.no_cpu_baseline:
+                precision["city256"]["host_oracle_cross_check"] = {"unavailable": str(ex)[:200]}
             try:
-                threads = os.cpu_count() or 1
-                ms_c, sample, riters = reference_cpu_measure(args.workload, seeds[0], args.cpu_seconds, threads)
-                per_city = [ref_iterations(f"{args.workload}:{sd}") for sd in seeds]
-                if all(per_city):
-                    riters = float(np.mean(per_city))
-                cpu = {"value": ms_c * riters if riters else None, "unit": "ms", "cores": threads,
-                       "kind": "reference",
-                       "sample": f"Solver_CPU_RB on seed {seeds[0]}: {sample} iterations timed "
-                                 f"({ms_c:.2f} ms/iteration) x {riters} iterations to tol {TOL} (mean over "
-                                 f"the batch's cities)"}
+                precision["city800"] = precision_city800()
             except Exception as ex:  # noqa: BLE001
-                cpu = {"value": None, "unit": "ms", "cores": os.cpu_count(), "kind": "reference",
-                       "sample": f"unavailable: {ex}"}
-    for s in solvers:
-        s.close()
+                precision["city800"] = {"unavailable": str(ex)[:200]}
 
     if rank == 0:
-        value = ms_warm / B
+        value = ms_head / B
         line = {
             "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_warm, "higher_is_better": False, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_head, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{args.workload} ({Nx}x{Ny}x{Nz}), held-out seeds {seeds[0]}..{seeds[-1]} "
                                    f"(+{B} per rank)",
-                       "batch": B, "tol": TOL, "itermax": ITERMAX, "network": os.path.basename(wpath),
+                       "batch": B, "tol": TOL, "itermax": ITERMAX, "window": WINDOW, "window_tol": WINDOW_TOL,
+                       "headline_arm": HEADLINE, "network": os.path.basename(wpath),
                        "network_levels": net.nlev, "channels": list(net.CH),
                        "sweep_variant": variant, "batch_variant": batch_variant,
                        "parallelism": f"replicas x{world}",
-                       "warm_start": f"red-black SOR at omega {PRE_OMEGA} from lambda = 0 to max|dlambda| <= "
-                                     f"{PRE_TOL}, then the reference loop (omega 1.78, tol {TOL}); the learned "
-                                     f"network's start is measured in arms (network, network+prephase) and is "
-                                     f"not in this pipeline because it does not shorten it",
+                       "warm_start": f"pre-phase: red-black SOR at omega {PRE_OMEGA} from the start to "
+                                     f"max|dlambda| <= {PRE_TOL}; then the reference loop (omega 1.78) to the "
+                                     f"rule",
                        "l2": "8 domains x ~40 MB packed sweep data + network buffers > L2 (126 MB) per step"},
             "arms": arms,
+            "speedup_vs_plain": ms_plain / ms_head,
             "network_ms_per_domain": ms_fwd,
-            "plain_single": {"ms_per_domain": ms_single / B,
-                             "iterations": [x["iterations"] for x in res_single[-1]]},
-            "speedup_vs_plain": (ms_plain / ms_warm),
-            "reference_gpu": ref_gpu,
-            "first_domain_ms": ms_first,
-            "speedup_vs_reference_gpu": (ref_gpu["ms"] / ms_first) if ref_gpu and "ms" in ref_gpu else None,
             "e2e": {"value": ms_e2e / B, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "matches_device_result": bool(e2e_ok),
                     "how": "public API (qesb_set_inputs from pinned host arrays, qesb_solve_batch, winds read "
                            "back to pinned host memory) on two solver sets: the next batch's inputs load on a "
                            "second host thread while the current batch solves; device-timed over the steps",
                     "serial_value": ms_e2e_serial / B},
-            "headline_sweep": headline_sweep,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                         "kernel": "red/black list sweep (variant %d) over the batch's domains, timed as the "
-                                   "whole headline step (lower bound)" % batch_variant,
-                         "algorithmic_bytes_per_launch": BYTES_PER_CELL_ITER * updated * B // 2,
-                         "moved_frac": moved / peak, "single_domain": single_domain},
+            "roofline": roofline,
             "sizes": sizes,
-            "wall_log_law": wall_log,
-            "fire_loop": fire,
             "network": {"bound": "tensor", "ms_per_forward": ms_fwd, "flops_per_forward": flops,
                         "achieved_tflops": flops / (ms_fwd * 1e-3) / 1e12, "peak_tflops": tpeak,
                         "frac": flops / (ms_fwd * 1e-3) / 1e12 / tpeak},
+            "ensemble": ensemble,
+            "wall_log_law": wall_log,
+            "fire_loop": fire,
+            "reference_gpu": ref_gpu,
             "precision": precision,
             "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-
-        barrier()  # rank 0 ran the fire-step section alone: the ranks leave together
+    if dist:
+        barrier()  # rank 0 ran the CPU sections alone: the ranks leave together
         dist.destroy_process_group()
 
 
-def run_ensemble(args):
+def ensemble_run(args, print_line=True, dist=None, dev=0):
     """Batched ensemble: cities with Nx, Ny ~ U[64, 256] and Nz ~ U[32, 96]
     (dx = dy = 2 m, z stretched 1.03, building count scaled from the 400 x 400
-    config's 60), each at 36 wind directions 10 degrees apart. The 36 solves of
-    a city run as one qesb_solve_batch (inputs built on the device beforehand
-    and reported as setup_ms_per_solve; only the batch is timed, CUDA events): over-relaxed pre-phase warm start, reference
-    loop, correction; the list sweep's launch shape tuned once (qesb_autotune_batch
-    on the first city's 36 solves) and used for every city. solves/s = all solves /
-    the sum of batch times; latency of a solve = device time from its batch's
-    first sweep to the poll that ended it."""
+    config's 60), each at 36 wind directions 10 degrees apart, 2304 solves for
+    64 cities. Inputs are built on the device (qesb_city_build_device,
+    reported as setup, not timed). Cities are packed into launch lists of
+    uneven sizes (whole cities, up to 250 M cells a list), each list one
+    qesb_solve_batch: over-relaxed pre-phase warm start, reference loop to the
+    rule, correction; the list sweep's launch shape tuned once on the first
+    list. solves/s = all solves / the sum of list times (CUDA events); the
+    latency of a solve = device time from its list's first reference-loop sweep
+    to the poll that ended it."""
     import torch
 
     import qesb
-
     from qesb import shard
 
     rank, local, world = dist_env()
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     rng = np.random.default_rng(20260907)
     nd, ndir = args.ensemble_domains, 36
     dims = [(int(a), int(b), int(c)) for a, b, c in zip(rng.integers(64, 257, nd), rng.integers(64, 257, nd),
                                                        rng.integers(32, 97, nd))]
-    dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(device=dev)
-    lat, batch_ms, iters, pre_iters, cells_total = [], [], [], [], 0
-    shapes, setup_ms = [], []
-    batch_shape = None  # the list sweep shape, tuned once on the first city's batch
-    for d in shard.rank_share(nd, world, rank):  # cities of this rank; none crosses ranks
+    mine = shard.rank_share(nd, world, rank)  # cities of this rank; none crosses ranks
+    lists, cur, cur_cells = [], [], 0
+    for d in mine:
         Nx, Ny, Nz = dims[d]
-        dom = qesb.Domain(Nx, Ny, Nz, 2.0, 2.0, 1.0, qesb.city_dz(Nz, 1.0, 1.03))
-        nb = max(3, int(round(60 * Nx * Ny / 160000)))
-        c = qesb.city_random(dom, 700000 + d, nb)
-        solvers = [qesb.Solver_B200(dom, TOL, device=dev) for _ in range(ndir)]
+        cells = ndir * Nx * Ny * (Nz + 1)
+        if cur and cur_cells + cells > 250_000_000:
+            lists.append(cur)
+            cur, cur_cells = [], 0
+        cur.append(d)
+        cur_cells += cells
+    if cur:
+        lists.append(cur)
+    lat, list_ms, iters, pre_iters, cells_total, shapes, setup_ms, list_sizes = [], [], [], [], 0, [], [], []
+    batch_shape = None
+    names = ("icellflag", "e", "f", "g", "h", "m", "n", "u0", "v0", "w0")
+    for lst in lists:
+        solvers, arrays, outs = [], [], []
         try:
-            om = qesb.prephase_omega(Nx, Ny)
-            # inputs built on the device (qesb_city_build_device), one set per
-            # direction, handed to the handles as device arrays
-            nc_, nf_ = dom.numCellCentered(), dom.numFaceCentered()
-            names = ("icellflag", "e", "f", "g", "h", "m", "n", "u0", "v0", "w0")
             torch.cuda.synchronize(dev)
             t_set = time.perf_counter()
-            arrays = []
-            for k in range(ndir):
-                a = {q: torch.empty(nc_ if q not in ("u0", "v0", "w0") else nf_,
-                                    dtype=torch.int32 if q == "icellflag" else torch.float32,
-                                    device=f"cuda:{dev}") for q in names}
-                torch.cuda.current_stream(dev).synchronize()
-                qesb.city_build_device(dom, c.buildings,
-                                       qesb.Inflow(c.inflow.u_ref, c.inflow.z_ref, c.inflow.p, 10.0 * k),
-                                       {q: v.data_ptr() for q, v in a.items()}, stream.cuda_stream)
-                arrays.append(a)
-            for s, a in zip(solvers, arrays):
-                s.set_stream(stream.cuda_stream)
-                s.set_inputs_device(*[a[q].data_ptr() for q in ("e", "f", "g", "h", "m", "n", "icellflag", "u0",
-                                                                 "v0", "w0")])
-                s.set_prephase(om, PRE_TOL, ITERMAX)
+            for d in lst:
+                Nx, Ny, Nz = dims[d]
+                dom = qesb.Domain(Nx, Ny, Nz, 2.0, 2.0, 1.0, qesb.city_dz(Nz, 1.0, 1.03))
+                nb = max(3, int(round(60 * Nx * Ny / 160000)))
+                c = qesb.city_random(dom, 700000 + d, nb)
+                om = qesb.prephase_omega(Nx, Ny)
+                nc_, nf_ = dom.numCellCentered(), dom.numFaceCentered()
+                for k in range(ndir):
+                    a = {q: torch.empty(nc_ if q not in ("u0", "v0", "w0") else nf_,
+                                        dtype=torch.int32 if q == "icellflag" else torch.float32,
+                                        device=f"cuda:{dev}") for q in names}
+                    torch.cuda.current_stream(dev).synchronize()
+                    qesb.city_build_device(dom, c.buildings,
+                                           qesb.Inflow(c.inflow.u_ref, c.inflow.z_ref, c.inflow.p, 10.0 * k),
+                                           {q: v.data_ptr() for q, v in a.items()}, stream.cuda_stream)
+                    s = qesb.Solver_B200(dom, TOL, device=dev)
+                    s.set_stream(stream.cuda_stream)
+                    s.set_window_rule(WINDOW, WINDOW_TOL)
+                    s.set_inputs_device(*[a[q].data_ptr() for q in ("e", "f", "g", "h", "m", "n", "icellflag",
+                                                                     "u0", "v0", "w0")])
+                    s.set_prephase(om, PRE_TOL, ITERMAX)
+                    solvers.append(s)
+                    arrays.append(a)
+                    outs.append([torch.empty(nf_, dtype=torch.float32, device=f"cuda:{dev}") for _ in range(3)])
+                shapes.append((Nx, Ny, Nz))
+                cells_total += ndir * Nx * Ny * (Nz + 1)
             torch.cuda.synchronize(dev)
             setup_ms.append(1e3 * (time.perf_counter() - t_set))
             if batch_shape is None:
                 batch_shape, _ = qesb.autotune_batch(solvers)
             solvers[0].set_option("batch_variant", batch_shape)
-            nf = dom.numFaceCentered()
-            outs = [[torch.empty(nf, dtype=torch.float32, device=f"cuda:{dev}") for _ in range(3)]
-                    for _ in range(ndir)]
             ptrs = [[o[q].data_ptr() for o in outs] for q in range(3)]
             torch.cuda.synchronize(dev)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -926,7 +1059,8 @@ def run_ensemble(args):
             st = qesb.solve_batch(solvers, ITERMAX, *ptrs)
             e1.record(stream)
             torch.cuda.synchronize(dev)
-            batch_ms.append(e0.elapsed_time(e1))
+            list_ms.append(e0.elapsed_time(e1))
+            list_sizes.append(len(solvers))
             lat += [x["ms_sor"] for x in st]
             iters += [x["iterations"] for x in st]
             pre_iters += [x["pre_iterations"] for x in st]
@@ -934,28 +1068,22 @@ def run_ensemble(args):
         finally:
             for s in solvers:
                 s.close()
-        cells_total += ndir * Nx * Ny * (Nz + 1)
-        shapes.append((Nx, Ny, Nz))
-    total_ms = shard.max_over_ranks(float(np.sum(batch_ms)), device=f"cuda:{dev}" if world > 1 else None)
-    setup_total = shard.max_over_ranks(float(np.sum(setup_ms)), device=f"cuda:{dev}" if world > 1 else None)
+            del arrays, outs
+    dv = f"cuda:{dev}" if dist else None
+    total_ms = shard.max_over_ranks(float(np.sum(list_ms)), device=dv)
+    setup_total = shard.max_over_ranks(float(np.sum(setup_ms)), device=dv)
     lat = shard.gather_lists(lat)
     iters, pre_iters = shard.gather_lists(iters), shard.gather_lists(pre_iters)
     cells_total = int(sum(shard.gather_lists([cells_total])))
-    shapes = shard.gather_lists(shapes)
+    list_sizes = shard.gather_lists(list_sizes)
     n = nd * ndir
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
-    if rank != 0:
-        return
-    line = {
+    out = {
         "metric": "ensemble solves/s (cities of uneven size x 36 wind directions, batched)",
         "value": n / (total_ms * 1e-3), "unit": "solves/s", "n_gpus": world, "higher_is_better": True,
-        "scaling": "strong",
-        "dtype": "f32", "data": "synthetic",
+        "scaling": "strong", "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{nd} cities, Nx,Ny ~ U[64,256], Nz ~ U[32,96], x {ndir} directions",
-                   "solves": n, "batch": ndir, "tol": TOL, "itermax": ITERMAX,
+                   "solves": n, "launch_lists": len(list_sizes), "solves_per_list": list_sizes, "tol": TOL,
+                   "itermax": ITERMAX, "window": WINDOW, "window_tol": WINDOW_TOL,
                    "warm_start": "over-relaxed pre-phase, omega = 2 - 7.5/max(Nx, Ny) within [1.85, 1.97], "
                                  f"to {PRE_TOL}", "cells_total": cells_total, "batch_variant": batch_shape},
         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
@@ -964,10 +1092,19 @@ def run_ensemble(args):
                  "and handed over with qesb_set_inputs_device; wall clock, not in value",
         "ms_total": total_ms, "iterations_mean": float(np.mean(iters)),
         "pre_iterations_mean": float(np.mean(pre_iters)),
-        "mcell_iterations_per_s": float(sum(ndir * (a - 2) * (b - 2) * (z - 1) * 1.0 for a, b, z in shapes) *
-                                        (np.mean(iters) + np.mean(pre_iters)) / (total_ms * 1e-3) / 1e6),
     }
-    print(json.dumps(line), flush=True)
+    if print_line and rank == 0:
+        print(json.dumps(out), flush=True)
+    return out
+
+
+def run_ensemble(args):
+    rank, local, world = dist_env()
+    dist = init_group(args, world, local)
+    ensemble_run(args, print_line=True, dist=dist, dev=local if world > 1 else 0)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_sweeps_only(args):
@@ -989,7 +1126,7 @@ def run_profile_solve(args):
     import qesb
 
     w = make_city(args.workload, SEED0 if args.workload == WORKLOAD else 0)
-    with qesb.Solver_B200(w.domain, 0.0) as s:
+    with qesb.Solver_B200(w.domain, -1.0) as s:
         if args.variant >= 0:
             s.set_option("variant", args.variant)
         st = s.solve(w, args.profile_solve)
@@ -997,8 +1134,8 @@ def run_profile_solve(args):
 
 
 def run_profile_batch(args):
-    """The headline step (a batch of B cities, over-relaxed pre-phase, reference
-    loop, correction) twice, for launch-list captures."""
+    """The headline step (a batch of B cities, its arm, the rule) twice, for
+    launch-list captures."""
     import torch
 
     import qesb
@@ -1008,7 +1145,8 @@ def run_profile_batch(args):
     try:
         for s, w in zip(solvers, cities):
             s.set_inputs(w)
-            s.set_prephase(PRE_OMEGA, PRE_TOL, ITERMAX)
+            s.set_window_rule(WINDOW, WINDOW_TOL)
+            s.set_prephase(PRE_OMEGA if ARMS[HEADLINE][1] else 0.0, PRE_TOL, ITERMAX)
         if args.variant >= 0:
             solvers[0].set_option("variant", args.variant)
         nf = cities[0].domain.numFaceCentered()
@@ -1046,7 +1184,10 @@ def run_forward_only(args):
 
 def main():
     args = parse()
-    if args.profile_solve:
+    maybe_relaunch(args)
+    if args.plan:
+        run_plan(args)
+    elif args.profile_solve:
         run_profile_solve(args)
     elif args.sweeps_only:
         run_sweeps_only(args)

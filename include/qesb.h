@@ -69,6 +69,9 @@ typedef struct qesb_stats {
                             corrected winds; -1 when the solve wrote no winds */
   double window_drift;   /* window rule: FP64 max|lambda - lambda(window iterations earlier)| at the
                             last window check; -1 when the rule is off or no window completed */
+  double ms_sweeps;      /* device time of the sweep-kernel loops alone (pre-phase and reference loop,
+                            CUDA events on the launching stream around them; a batch's loops for
+                            every domain of the batch); -1 on the fused tile and full-coefficient paths */
 } qesb_stats;
 
 /* Library and device. */
@@ -165,6 +168,30 @@ qesb_status qesb_set_prephase(qesb_handle *h, float omega, float tol, int max_it
  * The first call with window > 0 allocates one lambda-sized buffer on the
  * handle. window = 0 turns the rule off (the default). */
 qesb_status qesb_set_window_rule(qesb_handle *h, int window, double tol);
+
+/* FP64 run of the same SOR (no reference counterpart; the precision check of
+ * an FP32 result). On the handle's inputs, in double on the device: R, then
+ * from lambda0 (host, cell layout, widened to double; NULL: zero)
+ * pre_iterations red-black iterations at pre_omega (the pre-phase; 0 for
+ * none), then `iterations` at the reference's omega (1.78f as a double), the
+ * ground mirror after each, with the reference's loop bounds and operation
+ * order, no stopping rule; then the correction. Pass the counts a solve
+ * reported (qesb_stats.pre_iterations, .iterations) to measure that solve's
+ * FP32 rounding error: rep receives max|lambda - lambda64| over all cells
+ * (lambda: the handle's current lambda), max|lambda64|, and, when u, v, w
+ * (device face arrays, the FP32 winds of the solve) are given, the max over
+ * all faces of |x - x64| for x = u, v, w (else -1), and the device ms of the
+ * FP64 run. lambda64 (host, nullable, cell layout) receives the FP64 lambda.
+ * Allocates two cell arrays of doubles for the call. */
+typedef struct qesb_fp64_report {
+  double lambda_max_abs_err;
+  double lambda_max_abs;
+  double wind_max_err;
+  double ms;
+} qesb_fp64_report;
+qesb_status qesb_fp64_same_sor(qesb_handle *h, const float *lambda0, float pre_omega, int pre_iterations,
+                               int iterations, const float *u, const float *v, const float *w, double *lambda64,
+                               qesb_fp64_report *rep);
 
 /* Batched solve (no reference counterpart: the reference solves one domain
  * per Solver::solve call, src/winds/Solver.h:108). Each of the n handles

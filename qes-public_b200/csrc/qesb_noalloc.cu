@@ -285,6 +285,10 @@ extern "C" qesb_status qesb_solve_noalloc(const qesb_grid *grid, float tol, int 
     st->path = 0;
     st->sweeps_per_launch = 1;
     st->launches = launches;
+    st->pre_iterations = 0;
+    st->max_divergence = -1.0;
+    st->window_drift = -1.0;
+    st->ms_sweeps = -1.0;
   }
   if (hst.nan) return qesb_fail(QESB_ERR_NUMERIC, "qesb_solve_noalloc: NaN in lambda (iteration %d)", hst.it);
   return QESB_OK;

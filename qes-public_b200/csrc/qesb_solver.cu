@@ -41,6 +41,7 @@
 #include "qesb_sor_split.cuh"
 #include "qesb_sor_zm.cuh"
 #include "qesb_wall_log.cuh"
+#include "qesb_fp64.cuh"
 #include "qesb_sor_bulk.cuh"
 
 // ---------------------------------------------------------------------------
@@ -619,6 +620,8 @@ struct qesb_handle {
   double *d_div = nullptr;        // final divergence check (FP64)
   float *d_u = nullptr, *d_v = nullptr, *d_w = nullptr;  // output staging for host solves
   cudaEvent_t ev[4] = {};
+  cudaEvent_t evs[4] = {};  // around the sweep loops: pre-phase [0, 1], reference loop [2, 3]
+  bool sweeps_timed = false;  // the last solve recorded evs
 
   bool have_inputs = false;
   bool packed = false;
@@ -1211,6 +1214,7 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
   CK(cudaGetLastError());
   int launched = 0, pre_launched = 0;
   h->last_pre_iterations = 0;
+  CK(cudaEventRecord(h->evs[0], s));
   if (h->pre_omega > 0.0f && h->pre_iters > 0) {
     // over-relaxed pre-phase from the current lambda; its state and error
     // history are then cleared for the reference loop
@@ -1230,6 +1234,7 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
     CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
     CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
   }
+  CK(cudaEventRecord(h->evs[1], s));
   std::vector<SweepDomain> one{sweep_domain(h, itermax, (double)h->tol)};
   sweep_tiles(one, sv, false, h->device);
   CKS(h->list.upload(one, sv.unit, s));
@@ -1238,8 +1243,11 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
   a.wait_limit = h->opt_wait_limit;
   if (h->win_k > 0)  // the first window starts from lambda as the reference loop begins
     CK(cudaMemcpyAsync(h->d_snap, h->d_lam_s, sizeof(float) * 2 * h->S.CS, cudaMemcpyDeviceToDevice, s));
+  CK(cudaEventRecord(h->evs[2], s));
   CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, itermax, h->opt_graph != 0, &h->sgraph,
                      h->h_ctl, &launched, h->win_k, 1));
+  CK(cudaEventRecord(h->evs[3], s));
+  h->sweeps_timed = true;
   h->last_launches = 2 * (launched + pre_launched) + (h->win_k > 0 ? launched / h->win_k : 0);
   k_split_mirror_ring<<<G.Y, 128, 0, s>>>(G, h->S, h->d_lam_s);
   k_split_to_pad<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam_s, h->d_lam);
@@ -1292,6 +1300,7 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   const Variant *var = packed && !split ? &kVariants[vi] : nullptr;
   h->last_launches = 0;
   h->last_pre_iterations = 0;
+  h->sweeps_timed = false;
   if (itermax > 0) {
     if (split) CKS(run_iterations_sweep(h, kSweepVariants[vi - kSplitVariant], itermax));
     else if (var) CKS(run_iterations_tiled(h, *var, itermax));
@@ -1324,6 +1333,13 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
     st->launches = 2 + (packed ? h->last_launches : 4 * st->iterations);
     st->pre_iterations = h->last_pre_iterations;
     st->window_drift = h->win_k > 0 && st->iterations >= h->win_k ? h->h_state->wdrift : -1.0;
+    st->ms_sweeps = -1.0;
+    if (h->sweeps_timed) {
+      float p = 0, r = 0;
+      CK(cudaEventElapsedTime(&p, h->evs[0], h->evs[1]));
+      CK(cudaEventElapsedTime(&r, h->evs[2], h->evs[3]));
+      st->ms_sweeps = (double)p + (double)r;
+    }
   }
   if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the solve (iteration %d)", h->h_state->it);
   return QESB_OK;
@@ -1367,6 +1383,8 @@ void free_all(qesb_handle *h)
   if (h->h_state) cudaFreeHost(h->h_state);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
   for (auto &e : h->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto &e : h->evs)
     if (e) cudaEventDestroy(e);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
 }
@@ -1438,6 +1456,8 @@ qesb_status qesb_create(const qesb_grid *grid, float tol, int device, qesb_handl
       cudaMallocHost((void **)&h->h_ctl, sizeof(SweepCtl)) != cudaSuccess)
     return fail(qesb_fail(QESB_ERR_NOMEM, "cudaMallocHost failed"));
   for (auto &e : h->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaEventCreate failed"));
+  for (auto &e : h->evs)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaEventCreate failed"));
   for (void *p : {(void *)h->d_lam, (void *)h->d_lam2, (void *)h->d_R})
     if (cudaMemset(p, 0, np * sizeof(float)) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaMemset failed"));
@@ -1970,6 +1990,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   list.a.wait_limit = h0->opt_wait_limit;
   qesb_status qs = QESB_OK;
   int launched = 0, pre_launched = 0;
+  CK(cudaEventRecord(h0->evs[0], s));
   if (!pre.empty()) {
     // the over-relaxed pre-phase of the domains that have one, as a list of its own
     sweep_tiles(pre, sv, true, h0->device);
@@ -1992,6 +2013,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
       CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
     }
   }
+  CK(cudaEventRecord(h0->evs[1], s));
   sweep_tiles(doms, sv, true, h0->device);
   if (qs == QESB_OK) qs = list.upload(doms, sv.unit, s);
   if (qs == QESB_OK && h0->win_k > 0)  // each domain's first window starts from lambda as the loop begins
@@ -2002,9 +2024,11 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   if (qs == QESB_OK) {
     k_sweep_stamp<<<1, 1, 0, s>>>(list.a.ctl);
     SweepGraph gx;
+    CK(cudaEventRecord(h0->evs[2], s));
     if (itermax > 0)
       qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, itermax, h0->opt_graph != 0, &gx, h0->h_ctl,
                           &launched, h0->win_k, n);
+    CK(cudaEventRecord(h0->evs[3], s));
     gx.reset();
   }
   const unsigned long long t0 = h0->h_ctl->t0;
@@ -2026,8 +2050,10 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   list.destroy();
   if (qs != QESB_OK) return qs;
   if (se != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "batch: %s", cudaGetErrorString(se));
-  float ms_all = 0;
+  float ms_all = 0, ms_pre = 0, ms_ref = 0;
   CK(cudaEventElapsedTime(&ms_all, h0->ev[0], h0->ev[3]));
+  CK(cudaEventElapsedTime(&ms_pre, h0->evs[0], h0->evs[1]));
+  CK(cudaEventElapsedTime(&ms_ref, h0->evs[2], h0->evs[3]));
   int nan_at = -1;
   for (int i = 0; i < n; ++i) {
     SolveState sti;
@@ -2047,6 +2073,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
       st[i].launches = 2 * (launched + pre_launched) + (h0->win_k > 0 ? launched / h0->win_k : 0);
       st[i].pre_iterations = hs[i]->last_pre_iterations;
       st[i].window_drift = h0->win_k > 0 && st[i].iterations >= h0->win_k ? sti.wdrift : -1.0;
+      st[i].ms_sweeps = (double)ms_pre + (double)ms_ref;
     }
   }
   if (nan_at >= 0) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d", nan_at);
@@ -2062,6 +2089,81 @@ qesb_status qesb_set_prephase(qesb_handle *h, float omega, float tol, int max_it
   h->pre_omega = omega;
   h->pre_tol = tol;
   h->pre_iters = max_iterations;
+  return QESB_OK;
+}
+
+qesb_status qesb_fp64_same_sor(qesb_handle *h, const float *lambda0, float pre_omega, int pre_iterations,
+                               int iterations, const float *u, const float *v, const float *w, double *lambda64,
+                               qesb_fp64_report *rep)
+{
+  if (!h || !rep || pre_iterations < 0 || iterations < 0 || (pre_iterations > 0 && !(pre_omega > 0.0f)))
+    return qesb_fail(QESB_ERR_ARG, "qesb_fp64_same_sor: bad argument");
+  if (!h->have_inputs) return qesb_fail(QESB_ERR_STATE, "qesb_fp64_same_sor before qesb_set_inputs");
+  CK(cudaSetDevice(h->device));
+  const DevGrid &G = h->G;
+  cudaStream_t s = h->stream;
+  const size_t nc = (size_t)G.XY * G.Z;
+  double *L = nullptr, *R = nullptr, *acc = nullptr;
+  auto release = [&]() {
+    cudaFree(L);
+    cudaFree(R);
+    cudaFree(acc);
+  };
+  if (dalloc(&L, nc) != QESB_OK || dalloc(&R, nc) != QESB_OK || dalloc(&acc, 4) != QESB_OK) {
+    release();
+    return qesb_fail(QESB_ERR_NOMEM, "qesb_fp64_same_sor: no room for the FP64 lambda and R");
+  }
+  cudaError_t e = cudaSuccess;
+  auto ok = [&](cudaError_t x) {
+    if (e == cudaSuccess) e = x;
+    return e == cudaSuccess;
+  };
+  if (lambda0) {  // the start, widened to double (R's buffer holds the floats meanwhile)
+    float *tmp = reinterpret_cast<float *>(R);
+    ok(cudaMemcpyAsync(tmp, lambda0, nc * sizeof(float), cudaMemcpyHostToDevice, s));
+    k_widen64<<<(unsigned)((nc + 255) / 256), 256, 0, s>>>(tmp, L, (long)nc);
+  } else {
+    ok(cudaMemsetAsync(L, 0, nc * sizeof(double), s));
+  }
+  ok(cudaMemsetAsync(R, 0, nc * sizeof(double), s));
+  ok(cudaMemsetAsync(acc, 0, 4 * sizeof(double), s));
+  ok(cudaEventRecord(h->ev[0], s));
+  k_div64<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3],
+                                                          h->d_in[4], h->d_in[5], h->d_u0, h->d_v0, h->d_w0,
+                                                          h->d_dz, h->dx, h->dy, R);
+  const dim3 sgrid(((G.X - 2) / 2 + 1 + 127) / 128, G.Y - 2, G.Z - 2), mgrid((G.X + 255) / 256, G.Y, 1);
+  for (int phase = 0; phase < 2 && e == cudaSuccess; ++phase) {
+    const int n = phase == 0 ? pre_iterations : iterations;
+    const double om = phase == 0 ? (double)pre_omega : (double)kOmega;
+    for (int t = 0; t < n; ++t) {
+      for (int colour = 0; colour < 2; ++colour)
+        k_sor64<<<sgrid, 128, 0, s>>>(G, colour, om, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4],
+                                      h->d_in[5], R, L);
+      k_mirror64<<<mgrid, 256, 0, s>>>(G, L);
+      if ((t & 255) == 255 && !ok(cudaGetLastError())) break;
+    }
+  }
+  ok(cudaGetLastError());
+  ok(cudaEventRecord(h->ev[1], s));
+  k_lambda_cmp64<<<dim3((G.X + 255) / 256, G.Y, G.Z), 256, 0, s>>>(G, L, h->d_lam, acc);
+  const bool winds = u && v && w;
+  if (winds)
+    k_correct_cmp64<<<dim3((G.FX + 255) / 256, G.FY, G.FZ), 256, 0, s>>>(
+        G, L, h->d_in[1], h->d_in[3], h->d_in[5], h->d_flag, h->d_u0, h->d_v0, h->d_w0, h->d_dz, h->dx, h->dy, u,
+        v, w, acc + 2);
+  ok(cudaGetLastError());
+  double host[4] = {0, 0, 0, 0};
+  ok(cudaMemcpyAsync(host, acc, sizeof host, cudaMemcpyDeviceToHost, s));
+  if (lambda64) ok(cudaMemcpyAsync(lambda64, L, nc * sizeof(double), cudaMemcpyDeviceToHost, s));
+  ok(cudaStreamSynchronize(s));
+  float ms = 0.0f;
+  if (e == cudaSuccess) ok(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
+  release();
+  if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "qesb_fp64_same_sor: %s", cudaGetErrorString(e));
+  rep->lambda_max_abs_err = host[0];
+  rep->lambda_max_abs = host[1];
+  rep->wind_max_err = winds ? host[2] : -1.0;
+  rep->ms = ms;
   return QESB_OK;
 }
 

@@ -59,7 +59,16 @@ class Stats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("residual", C.c_double),
                 ("ms_total", C.c_double), ("ms_sor", C.c_double), ("path", C.c_int),
                 ("sweeps_per_launch", C.c_int), ("launches", C.c_int), ("pre_iterations", C.c_int),
-                ("max_divergence", C.c_double), ("window_drift", C.c_double)]
+                ("max_divergence", C.c_double), ("window_drift", C.c_double),
+                ("ms_sweeps", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class Fp64Report(C.Structure):
+    _fields_ = [("lambda_max_abs_err", C.c_double), ("lambda_max_abs", C.c_double),
+                ("wind_max_err", C.c_double), ("ms", C.c_double)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -106,6 +115,8 @@ def lib() -> C.CDLL:
             "qesb_set_tolerance": ([V, C.c_float], C.c_int),
             "qesb_set_prephase": ([V, C.c_float, C.c_float, C.c_int], C.c_int),
             "qesb_set_window_rule": ([V, C.c_int, C.c_double], C.c_int),
+            "qesb_fp64_same_sor": ([V, V, C.c_float, C.c_int, C.c_int, V, V, V, V, C.POINTER(Fp64Report)],
+                                   C.c_int),
             "qesb_time_sweeps": ([V, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)], C.c_int),
             "qesb_autotune": ([V, C.POINTER(C.c_int), C.POINTER(C.c_float), C.c_int], C.c_int),
             "qesb_solve_batch": ([C.POINTER(V), C.c_int, C.c_int, C.POINTER(V), C.POINTER(V), C.POINTER(V),
@@ -317,6 +328,23 @@ class Solver_B200:
         window-th iteration n when FP64 max|lambda_n - lambda_(n-window)| <= tol
         (window 0: off, the reference's rule alone)."""
         check(lib().qesb_set_window_rule(self._h, int(window), float(tol)))
+
+    def fp64_same_sor(self, pre_omega: float, pre_iterations: int, iterations: int, u_ptr=None, v_ptr=None,
+                      w_ptr=None, want_lambda: bool = False, lambda0: np.ndarray | None = None) -> dict:
+        """qesb_fp64_same_sor: the same red-black SOR replayed in FP64 on the
+        device from lambda0 (None: zero) with a solve's pre-phase and
+        reference-loop iteration counts, and the errors of the handle's FP32
+        lambda and of the given FP32 winds (device pointers) against it."""
+        rep = Fp64Report()
+        lam = np.empty(self.domain.numCellCentered(), np.float64) if want_lambda else None
+        l0 = None if lambda0 is None else np.ascontiguousarray(lambda0, np.float32)
+        check(lib().qesb_fp64_same_sor(self._h, _ptr(l0), float(pre_omega), int(pre_iterations), int(iterations),
+                                       u_ptr, v_ptr, w_ptr, _ptr(lam), C.byref(rep)))
+        out = rep.as_dict()
+        out["lambda_max_rel_err"] = out["lambda_max_abs_err"] / max(out["lambda_max_abs"], 1e-30)
+        if want_lambda:
+            out["lambda64"] = lam
+        return out
 
     def set_tolerance(self, tol: float):
         self.tol = np.float32(tol)

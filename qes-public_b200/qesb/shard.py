@@ -38,3 +38,20 @@ def gather_lists(values: list, device=None) -> list:
     out = [None] * dist.get_world_size()
     dist.all_gather_object(out, list(values))
     return [v for part in out for v in part]
+
+
+def rank_seeds(seed0: int, batch: int, rank: int) -> list[int]:
+    """Seeds of the cities rank `rank` solves when every rank takes its own
+    batch of `batch` cities (weak scaling): seed0 + rank*batch + i."""
+    if batch < 1 or rank < 0:
+        raise ValueError(f"batch {batch}, rank {rank}")
+    return [seed0 + rank * batch + i for i in range(batch)]
+
+
+def launch_command(python: str, script: str, nproc: int, port: int, argv: list[str]) -> list[str]:
+    """The torch.distributed.run command line that runs `script` as `nproc`
+    ranks on one node, rendezvous on 127.0.0.1:port."""
+    if nproc < 1:
+        raise ValueError(f"nproc {nproc}")
+    return [python, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={nproc}",
+            "--master-addr", "127.0.0.1", "--master-port", str(port), script, *argv]

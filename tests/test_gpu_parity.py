@@ -293,17 +293,3 @@ def test_overrelaxed_prephase_then_reference_loop(variant, omega, pre_tol, pre_m
     assert st["iterations"] == it and st["converged"] == 1
     np.testing.assert_array_equal(L, Lo)
     np.testing.assert_array_equal(u, O.correct(d, w, Lo)[0])
-
-
-@pytest.mark.parametrize("seed", [500001, 500004])
-def test_benchmark_cities_stop_where_the_reference_stops(seed):
-    """On the benchmark's 256x256x64 cities the solver stops on the iteration
-    the reference Solver_CPU_RB stops on (tests/golden/ref_iters.json, made by
-    running the reference build)."""
-    import json
-
-    ref = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ref_iters.json")))
-    w, _ = qesb.random_city("city256", seed)
-    with qesb.Solver_B200(w.domain, 1e-3) as s:
-        st = s.solve(w, 10000)
-    assert st["converged"] and st["iterations"] == ref[f"city256:{seed}"]["Solver_CPU_RB"]["iterations"]

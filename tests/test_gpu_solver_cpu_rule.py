@@ -1,0 +1,73 @@
+"""The benchmark's stopping rule, against the reference on the benchmark's own
+256 x 256 x 64 cities.
+
+The rule: the reference loop with its own tol (1e-9, never met in FP32) and
+itermax 10000, plus the window rule (stop after every 32nd iteration when
+lambda moved by at most 4e-3 over the last 32). tests/golden/ref_iters.json
+holds the iterations the reference's own solvers need under it, and
+tests/golden/solver_cpu_city256_<seed>.npz the serial Solver_CPU winds there
+(every 4th face column in x and y, all layers; made by
+tests/golden/make_ref_iters.py from the reference build).
+
+  * plain red-black SOR stops where the reference Solver_CPU_RB stops;
+  * the plain and the benchmark pipelines' winds lie within 1e-3 m/s of
+    serial Solver_CPU's (Solver_CPU.cpp:42-238, lexicographic), and their FP64
+    max divergence is at or below Solver_CPU's on the same cells.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import qesb
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+WINDOW, WINDOW_TOL, TOL, ITERMAX = 32, 4e-3, 1e-9, 10000
+WIND_TOL = 1e-3
+PRE_OMEGA, PRE_TOL = 1.97, 2e-3
+
+
+def _rule():
+    doc = json.load(open(os.path.join(GOLDEN, "ref_iters.json")))
+    return doc
+
+
+def test_rule_constants_match_the_fixture():
+    r = _rule()["rule"]
+    assert (r["window"], r["window_tol"], r["tol"], r["itermax"]) == (WINDOW, WINDOW_TOL, TOL, ITERMAX)
+
+
+def _solve(seed, prephase):
+    w, _ = qesb.random_city("city256", seed)
+    with qesb.Solver_B200(w.domain, TOL) as s:
+        s.set_window_rule(WINDOW, WINDOW_TOL)
+        if prephase:
+            s.set_prephase(PRE_OMEGA, PRE_TOL, ITERMAX)
+        st = s.solve(w, ITERMAX)
+    return w, st
+
+
+@pytest.mark.parametrize("seed", [500000, 500001, 500004])
+def test_plain_sor_stops_where_the_reference_red_black_solver_stops(seed):
+    ref = _rule()[f"city256:{seed}"]["Solver_CPU_RB"]
+    w, st = _solve(seed, prephase=False)
+    assert st["converged"] == 2
+    assert st["iterations"] == ref["iterations"]
+    assert st["window_drift"] == ref["window_drift"]
+
+
+@pytest.mark.parametrize("prephase", [False, True], ids=["plain", "prephase"])
+@pytest.mark.parametrize("seed", [500000, 500001])
+def test_winds_match_serial_solver_cpu_at_the_rule(seed, prephase):
+    z = np.load(os.path.join(GOLDEN, f"solver_cpu_city256_{seed}.npz"))
+    w, st = _solve(seed, prephase)
+    d = w.domain
+    s = int(z["stride"])
+    shape = (d.nz(), d.ny(), d.nx())
+    sub = (slice(None), slice(None, None, s), slice(None, None, s))
+    err = max(float(np.abs(a.reshape(shape)[sub] - z[k]).max()) for a, k in ((w.u, "u"), (w.v, "v"), (w.w, "w")))
+    assert err <= WIND_TOL, err
+    assert st["max_divergence"] <= float(z["max_div"]), (st["max_divergence"], float(z["max_div"]))

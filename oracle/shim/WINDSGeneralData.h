@@ -8,6 +8,7 @@
 #include <utility>
 #include <vector>
 #include "qes/Domain.h"
+#include "util/QESout.h"  // the reference header reaches it through its own includes
 
 class Wall;
 

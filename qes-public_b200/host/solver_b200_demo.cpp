@@ -1,13 +1,16 @@
-// Drop-in demonstration: drives Solver_B200 exactly as qesWinds drives its
-// solver (qesWinds/qesWindsMain.cpp:134-169): construct through the base
-// type, resetLambda, solve. Inputs come from the library's city generator;
-// u, v, w and lambda are written to a binary file for comparison.
-//   solver_b200_demo <out.bin> <Nx> <Ny> <Nz> <seed> <nbuildings> <itermax> <tol> [calls]
+// Drop-in demonstration: drives the solver exactly as qesWinds does
+// (qesWinds/qesWindsMain.cpp:134-169): SolverFactory::create(type, domain,
+// tol) with the B200 type registered as INTEGRATION.md describes (type 5; the
+// reference's own types keep their meaning, type 1 being Solver_CPU_RB in an
+// OpenMP build), then resetLambda and solve through Solver*. Inputs come from
+// the library's city generator; u, v, w and lambda are written to a binary
+// file for comparison.
+//   solver_b200_demo <out.bin> <Nx> <Ny> <Nz> <seed> <nbuildings> <itermax> <tol> [calls] [type]
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
 
-#include "Solver_B200.h"
+#include "SolverFactory.h"
 #include "WINDSGeneralData.h"
 
 int main(int argc, char **argv)
@@ -21,6 +24,7 @@ int main(int argc, char **argv)
   const int nb = std::atoi(argv[6]), itermax = std::atoi(argv[7]);
   const float tol = std::strtof(argv[8], nullptr);
   const int calls = argc > 9 ? std::atoi(argv[9]) : 1;
+  const int type = argc > 10 ? std::atoi(argv[10]) : B200_Type;
 
   std::vector<float> dz(Nz + 1);
   qesb_city_dz(Nz, 1.0f, 1.03f, dz.data());
@@ -43,11 +47,11 @@ int main(int argc, char **argv)
     return 1;
   }
 
-  Solver *solver = new Solver_B200(wgd.domain, tol);
+  Solver *solver = SolverFactory::create(type, wgd.domain, tol);
   solver->resetLambda();
   for (int c = 0; c < calls; ++c) solver->solve(&wgd, itermax);
 
-  struct LambdaOf : Solver_B200 {  // reads the base class's protected lambda for the dump
+  struct LambdaOf : Solver {  // reads the base class's protected lambda for the dump
     static const std::vector<float> &get(Solver *s) { return s->*(&LambdaOf::lambda); }
   };
   FILE *fo = std::fopen(argv[1], "wb");
@@ -57,6 +61,7 @@ int main(int argc, char **argv)
   std::fwrite(wgd.w.data(), sizeof(float), nf, fo);
   std::fwrite(LambdaOf::get(solver).data(), sizeof(float), nc, fo);
   std::fclose(fo);
-  delete static_cast<Solver_B200 *>(solver);
+  // Solver has no virtual destructor: delete through the type the factory made
+  if (type == B200_Type) delete static_cast<Solver_B200 *>(solver);
   return 0;
 }

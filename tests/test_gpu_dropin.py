@@ -1,7 +1,10 @@
 """The C++ drop-in: Solver_B200 derived from the reference's own Solver
-class (built by oracle/Makefile against src/winds/Solver.h with the shim
-WINDSGeneralData), driven through Solver* exactly as qesWinds drives its
-solver. Its u, v, w and lambda must equal the oracle's red-black result."""
+class and registered in the reference's own SolverFactory as type 5 (the
+registration of INTEGRATION.md applied to src/winds/SolverFactory.{h,cpp} by
+oracle/Makefile), driven through Solver* exactly as qesWinds drives its
+solver. Type 5's u, v, w and lambda must equal the oracle's red-black result
+and those of the reference's type 1 (Solver_CPU_RB in this OpenMP build)
+through the same factory."""
 import os
 import subprocess
 
@@ -11,31 +14,72 @@ import pytest
 import qesb
 from oracle import oracle as O
 
-pytestmark = pytest.mark.gpu
 DEMO = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
                     "solver_b200_demo")
+needs_demo = pytest.mark.skipif(not os.path.exists(DEMO), reason="drop-in demo not built (needs the reference tree)")
+Nx, Ny, Nz, SEED, NB, ITERMAX = 40, 32, 16, 2024, 5, 150
 
 
-@pytest.mark.skipif(not os.path.exists(DEMO), reason="drop-in demo not built (needs the reference tree)")
-@pytest.mark.parametrize("calls", [1, 2])
-def test_dropin_through_reference_solver_base(tmp_path, calls):
-    Nx, Ny, Nz, seed, nb, itermax = 40, 32, 16, 2024, 5, 150
-    out = tmp_path / "out.bin"
-    r = subprocess.run([DEMO, str(out), str(Nx), str(Ny), str(Nz), str(seed), str(nb), str(itermax),
-                        "1e-9", str(calls)], capture_output=True, text=True, timeout=300)
-    assert r.returncode == 0, r.stderr
-    assert f"Residual after {itermax} itertations" in r.stdout
+def _run(tmp_path, calls, solver_type):
+    out = tmp_path / f"out_{solver_type}_{calls}.bin"
+    r = subprocess.run([DEMO, str(out), str(Nx), str(Ny), str(Nz), str(SEED), str(NB), str(ITERMAX), "1e-9",
+                        str(calls), str(solver_type)], capture_output=True, text=True, timeout=300)
+    return r, out
+
+
+def _read(out):
     d = qesb.Domain(Nx, Ny, Nz, 2.0, 2.0, 1.0, qesb.city_dz(Nz, 1.0, 1.03))
-    c = qesb.city_random(d, seed, nb, fp=(6, 16), h=(4, 20))
-    w = qesb.city_build(d, c.buildings, c.inflow)
     nf, nc = d.numFaceCentered(), d.numCellCentered()
     raw = np.fromfile(out, dtype=np.float32)
     assert raw.size == 3 * nf + nc
-    u, v, ww, lam = raw[:nf], raw[nf:2 * nf], raw[2 * nf:3 * nf], raw[3 * nf:]
+    return d, raw[:nf], raw[nf:2 * nf], raw[2 * nf:3 * nf], raw[3 * nf:]
+
+
+def _oracle(d, calls):
+    c = qesb.city_random(d, SEED, NB, fp=(6, 16), h=(4, 20))
+    w = qesb.city_build(d, c.buildings, c.inflow)
     L = None
     for _ in range(calls):
-        uo, vo, wo, L, it, _ = O.solve(d, w, 1e-9, itermax, ordering=1, lam=L)
+        uo, vo, wo, L, it, _ = O.solve(d, w, 1e-9, ITERMAX, ordering=1, lam=L)
+    return uo, vo, wo, L
+
+
+@needs_demo
+def test_factory_type_1_is_the_reference_red_black_solver(tmp_path):
+    """Type 1 through the patched factory is the reference's own Solver_CPU_RB
+    (this build has OpenMP): its result is the oracle's red-black result."""
+    r, out = _run(tmp_path, 1, 1)
+    assert r.returncode == 0, r.stderr
+    assert "Red/Black CPU Solver" in r.stdout
+    d, u, v, ww, lam = _read(out)
+    uo, vo, wo, L = _oracle(d, 1)
+    np.testing.assert_array_equal(lam, L)
+    np.testing.assert_array_equal(u, uo)
+
+
+@needs_demo
+def test_factory_rejects_unknown_types_as_the_reference_does(tmp_path):
+    r, _ = _run(tmp_path, 1, 9)
+    assert r.returncode != 0
+    assert "Invalid solver type" in r.stderr
+
+
+@needs_demo
+@pytest.mark.gpu
+@pytest.mark.parametrize("calls", [1, 2])
+def test_dropin_type_5_through_the_reference_factory(tmp_path, calls):
+    r, out = _run(tmp_path, calls, 5)
+    assert r.returncode == 0, r.stderr
+    assert "B200 Solver" in r.stdout and f"Residual after {ITERMAX} itertations" in r.stdout
+    d, u, v, ww, lam = _read(out)
+    uo, vo, wo, L = _oracle(d, calls)
     np.testing.assert_array_equal(lam, L)
     np.testing.assert_array_equal(u, uo)
     np.testing.assert_array_equal(v, vo)
     np.testing.assert_array_equal(ww, wo)
+    r1, out1 = _run(tmp_path, calls, 1)
+    assert r1.returncode == 0, r1.stderr
+    _, u1, v1, w1, lam1 = _read(out1)
+    np.testing.assert_array_equal(lam, lam1)
+    np.testing.assert_array_equal(u, u1)
+    np.testing.assert_array_equal(ww, w1)

@@ -302,6 +302,27 @@ qesb_status qesb_warm_apply(qesb_handle *h, const float *yhead, int N, const uns
  * the cell centres. */
 qesb_status qesb_warm_apply_up2(qesb_handle *h, const float *yhead, int N, const unsigned *scale);
 
+/* The learned warm start as one call (no reference counterpart; the reference
+ * starts every solve from lambda = 0 after resetLambda, qesWindsMain.cpp:154).
+ * qesb_warmnet_load reads a trained network (the "QESBWNT1" weights file that
+ * qes-public_b200/qesb/warmstart.py writes: levels, resolution, channels, then
+ * each layer's FP32 weights and bias) onto `device`, converting the weights to
+ * the convolution kernels' BF16 layout. qesb_warm_start runs it for handle
+ * h's current inputs on h's stream: R, the network input (R / max|R|, solid
+ * flag, dz, boundary flag, height), the forward pass (BF16 tcgen05
+ * convolutions, FP32 accumulation), and lambda <- max|R| * prediction on the
+ * updated cells (trilinear from the half-resolution grid when the network
+ * runs at res 2), ground plane mirrored; the next solve on h starts from it.
+ * The grid's Nx, Ny and Nz must be multiples of res * 2^(levels-1). The first
+ * call for a grid shape allocates that shape's activations on the network
+ * (kept until qesb_warmnet_destroy); calls on one network are serialised. It
+ * returns when the start is in place (QESB_ERR_CUDA if a tensor-core wait gave
+ * up). */
+typedef struct qesb_warmnet qesb_warmnet;
+qesb_status qesb_warmnet_load(const char *path, int device, qesb_warmnet **out);
+qesb_status qesb_warmnet_destroy(qesb_warmnet *net);
+qesb_status qesb_warm_start(qesb_handle *h, qesb_warmnet *net);
+
 /* Self-test of the tcgen05 GEMM core: C[128 x N] = A[128 x K] * B[N x K]^T
  * in BF16 with FP32 accumulation. A is [128][K] (a_mn = 0) or [K][128]
  * (a_mn = 1); B is [N][K] (b_mn = 0) or [K][N] (b_mn = 1); BF16 bit patterns,

@@ -2092,6 +2092,20 @@ qesb_status qesb_set_prephase(qesb_handle *h, float omega, float tol, int max_it
   return QESB_OK;
 }
 
+}  // extern "C"
+
+qesb_status qesb_handle_grid(qesb_handle *h, int *Nx, int *Ny, int *Nz, int *device)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  *Nx = h->G.X;
+  *Ny = h->G.Y;
+  *Nz = h->G.Z - 1;
+  *device = h->device;
+  return QESB_OK;
+}
+
+extern "C" {
+
 qesb_status qesb_fp64_same_sor(qesb_handle *h, const float *lambda0, float pre_omega, int pre_iterations,
                                int iterations, const float *u, const float *v, const float *w, double *lambda64,
                                qesb_fp64_report *rep)

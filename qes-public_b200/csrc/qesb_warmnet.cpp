@@ -1,0 +1,300 @@
+// The learned warm start behind the C ABI: loads a trained network
+// (qesb_warmnet_load), predicts lambda for a handle's inputs and sets it as
+// the handle's starting lambda (qesb_warm_start). The layer loop, buffers and
+// weight layouts live here; every convolution, pooling, input and apply step
+// is one of the library's kernels, called through its C entry points, on the
+// handle's stream.
+//
+// Network (the one qes-public_b200/qesb/warmstart.py trains): levels
+// l = 0..L-1 with channels C[l] on the net grid divided by 2^l. Encoder: two
+// 3x3x3 convolutions (ReLU) per level, 2x2x2 average pooling between levels.
+// Decoder, l = L-2 .. 0: a convolution of [nearest-upsampled level l+1,
+// skip e_l], then a second convolution. Head: one convolution to 16 FP32
+// channels, channel 0 being lambda / max|R|. With res = 2 the net grid is the
+// cell grid halved in every direction (features pooled, prediction applied by
+// trilinear interpolation).
+//
+// Weights file (little-endian): "QESBWNT1", int32 nlev, res, in_ch, head_n,
+// int32 channels[nlev], then per layer in the order e0a, e0, ..., e{L-1}a,
+// e{L-1}, d{L-2}a, d{L-2}, ..., d0a, d0, head: int32 c1, c2, cout, cout_real,
+// relu, up1, float W[27 (c1 + c2) cout] (row tap (c1 + c2) + c, column
+// output channel), float b[cout].
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "qesb.h"
+#include "qesb_internal.h"
+
+namespace {
+
+constexpr int kInCh = 16;   // network input channels (5 used)
+constexpr int kHeadN = 16;  // head width (channel 0 is the prediction)
+
+struct Layer {
+  int c1 = 0, c2 = 0, cout = 0, cout_real = 0, relu = 0, up1 = 0, Kp = 0;
+  uint16_t *Bm = nullptr;  // BF16 [cout][Kp], device
+  float *bias = nullptr;   // [cout], device
+};
+
+// Activations of one net grid shape (D, H, W at level 0), BF16 channels-last.
+struct Buffers {
+  uint16_t *xfull = nullptr;  // res 2: the cell-grid input before pooling
+  uint16_t *x = nullptr;
+  float *y = nullptr;
+  std::vector<uint16_t *> ea, e, p, da, d;
+};
+
+uint16_t bf16_rn(float f)
+{
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)((u >> 16) | ((u & 0xffffu) ? 0x40u : 0u));
+  u += 0x7fffu + ((u >> 16) & 1u);  // round to nearest, ties to even
+  return (uint16_t)(u >> 16);
+}
+
+}  // namespace
+
+struct qesb_warmnet {
+  int device = 0, nlev = 0, res = 1;
+  std::vector<int> ch;
+  std::vector<Layer> layers;  // file order
+  int *d_err = nullptr;
+  unsigned *d_scale = nullptr;
+  std::map<std::tuple<int, int, int>, Buffers> bufs;
+  std::vector<void *> owned;
+  std::mutex mu;
+
+  qesb_status alloc(void **p, size_t bytes)
+  {
+    if (cudaMalloc(p, bytes) != cudaSuccess) return qesb_fail(QESB_ERR_NOMEM, "qesb_warmnet: cudaMalloc of %zu bytes", bytes);
+    owned.push_back(*p);
+    if (cudaMemset(*p, 0, bytes) != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "qesb_warmnet: cudaMemset");
+    return QESB_OK;
+  }
+
+  int index(char kind, int l, bool a) const
+  {
+    // e0a, e0, e1a, e1, ... then d{L-2}a, d{L-2}, ..., d0a, d0, then head
+    if (kind == 'e') return 2 * l + (a ? 0 : 1);
+    if (kind == 'd') return 2 * nlev + 2 * (nlev - 2 - l) + (a ? 0 : 1);
+    return 2 * nlev + 2 * (nlev - 1);
+  }
+
+  qesb_status buffers(int D, int H, int W, Buffers **out)
+  {
+    auto key = std::make_tuple(D, H, W);
+    auto it = bufs.find(key);
+    if (it != bufs.end()) {
+      *out = &it->second;
+      return QESB_OK;
+    }
+    Buffers b;
+    auto V = [&](int l) { return (size_t)(D >> l) * (size_t)(H >> l) * (size_t)(W >> l); };
+    void *p = nullptr;
+    if (res == 2) {
+      CKS_FWD(alloc(&p, V(0) * 8 * kInCh * 2));
+      b.xfull = static_cast<uint16_t *>(p);
+    }
+    CKS_FWD(alloc(&p, V(0) * kInCh * 2));
+    b.x = static_cast<uint16_t *>(p);
+    CKS_FWD(alloc(&p, V(0) * kHeadN * 4));
+    b.y = static_cast<float *>(p);
+    b.ea.resize(nlev);
+    b.e.resize(nlev);
+    b.p.assign(nlev, nullptr);
+    b.da.assign(nlev, nullptr);
+    b.d.assign(nlev, nullptr);
+    for (int l = 0; l < nlev; ++l) {
+      CKS_FWD(alloc(&p, V(l) * ch[l] * 2));
+      b.ea[l] = static_cast<uint16_t *>(p);
+      CKS_FWD(alloc(&p, V(l) * ch[l] * 2));
+      b.e[l] = static_cast<uint16_t *>(p);
+      if (l > 0) {
+        CKS_FWD(alloc(&p, V(l) * ch[l - 1] * 2));
+        b.p[l] = static_cast<uint16_t *>(p);
+      }
+      if (l < nlev - 1) {
+        CKS_FWD(alloc(&p, V(l) * ch[l] * 2));
+        b.da[l] = static_cast<uint16_t *>(p);
+        CKS_FWD(alloc(&p, V(l) * ch[l] * 2));
+        b.d[l] = static_cast<uint16_t *>(p);
+      }
+    }
+    *out = &bufs.emplace(key, b).first->second;
+    return QESB_OK;
+  }
+
+  qesb_status conv(const Layer &L, const void *x1, const void *x2, int D, int H, int W, void *y, void *yf,
+                   void *stream)
+  {
+    return qesb_conv3d(x1, L.c1, L.up1, x2, L.c2, D, H, W, 1, L.Bm, L.Kp, L.cout, y, yf, L.bias, L.relu, nullptr,
+                       d_err, stream);
+  }
+
+  // forward pass on b.x (net grid D x H x W) into b.y
+  qesb_status forward(Buffers &b, int D, int H, int W, void *s)
+  {
+    for (int l = 0; l < nlev; ++l) {
+      const int Dl = D >> l, Hl = H >> l, Wl = W >> l;
+      const void *xin = b.x;
+      if (l > 0) {
+        CKS_FWD(qesb_net_pool2(b.e[l - 1], b.p[l], D >> (l - 1), H >> (l - 1), W >> (l - 1), ch[l - 1], s));
+        xin = b.p[l];
+      }
+      CKS_FWD(conv(layers[index('e', l, true)], xin, nullptr, Dl, Hl, Wl, b.ea[l], nullptr, s));
+      CKS_FWD(conv(layers[index('e', l, false)], b.ea[l], nullptr, Dl, Hl, Wl, b.e[l], nullptr, s));
+    }
+    for (int l = nlev - 2; l >= 0; --l) {
+      const int Dl = D >> l, Hl = H >> l, Wl = W >> l;
+      const void *below = l == nlev - 2 ? (const void *)b.e[l + 1] : (const void *)b.d[l + 1];
+      CKS_FWD(conv(layers[index('d', l, true)], below, b.e[l], Dl, Hl, Wl, b.da[l], nullptr, s));
+      CKS_FWD(conv(layers[index('d', l, false)], b.da[l], nullptr, Dl, Hl, Wl, b.d[l], nullptr, s));
+    }
+    return conv(layers[index('h', 0, false)], b.d[0], nullptr, D, H, W, nullptr, b.y, s);
+  }
+
+  void release()
+  {
+    cudaSetDevice(device);
+    for (void *p : owned) cudaFree(p);
+    owned.clear();
+    bufs.clear();
+  }
+};
+
+namespace {
+
+struct File {
+  FILE *f;
+  explicit File(const char *path) : f(std::fopen(path, "rb")) {}
+  ~File()
+  {
+    if (f) std::fclose(f);
+  }
+  bool read(void *p, size_t bytes) { return std::fread(p, 1, bytes, f) == bytes; }
+};
+
+}  // namespace
+
+extern "C" {
+
+qesb_status qesb_warmnet_load(const char *path, int device, qesb_warmnet **out)
+{
+  if (!path || !out) return qesb_fail(QESB_ERR_ARG, "qesb_warmnet_load: null argument");
+  *out = nullptr;
+  File F(path);
+  if (!F.f) return qesb_fail(QESB_ERR_ARG, "qesb_warmnet_load: cannot open %s", path);
+  char magic[8];
+  int32_t hdr[4];
+  if (!F.read(magic, 8) || std::memcmp(magic, "QESBWNT1", 8) != 0 || !F.read(hdr, sizeof hdr))
+    return qesb_fail(QESB_ERR_ARG, "qesb_warmnet_load: %s is not a warm-start network file", path);
+  const int nlev = hdr[0], res = hdr[1];
+  if (nlev < 2 || nlev > 8 || (res != 1 && res != 2) || hdr[2] != kInCh || hdr[3] != kHeadN)
+    return qesb_fail(QESB_ERR_ARG, "qesb_warmnet_load: unsupported network (levels %d, res %d)", nlev, res);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    return qesb_fail(QESB_ERR_NODEV, "qesb_warmnet_load: no CUDA device %d", device);
+  if (cudaSetDevice(device) != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "qesb_warmnet_load: cudaSetDevice");
+  auto *net = new qesb_warmnet();
+  net->device = device;
+  net->nlev = nlev;
+  net->res = res;
+  net->ch.resize(nlev);
+  auto fail = [&](qesb_status s) {
+    net->release();
+    delete net;
+    return s;
+  };
+  if (!F.read(net->ch.data(), sizeof(int32_t) * nlev)) return fail(qesb_fail(QESB_ERR_ARG, "qesb_warmnet_load: truncated"));
+  const int nlayers = 2 * nlev + 2 * (nlev - 1) + 1;
+  net->layers.resize(nlayers);
+  void *p = nullptr;
+  qesb_status s = QESB_OK;
+  for (int q = 0; q < nlayers; ++q) {
+    int32_t d[6];
+    if (!F.read(d, sizeof d)) return fail(qesb_fail(QESB_ERR_ARG, "qesb_warmnet_load: truncated at layer %d", q));
+    Layer &L = net->layers[q];
+    L.c1 = d[0], L.c2 = d[1], L.cout = d[2], L.cout_real = d[3], L.relu = d[4], L.up1 = d[5];
+    const int cin = L.c1 + L.c2;
+    if (L.c1 <= 0 || L.c1 % 16 || L.c2 < 0 || L.c2 % 16 || L.cout_real < 1 || L.cout_real > L.cout ||
+        (L.cout != 16 && L.cout != 32 && L.cout != 64 && L.cout != 128))
+      return fail(qesb_fail(QESB_ERR_ARG, "qesb_warmnet_load: layer %d has an unsupported shape", q));
+    L.Kp = (27 * cin + 63) / 64 * 64;
+    std::vector<float> W((size_t)27 * cin * L.cout), b(L.cout);
+    if (!F.read(W.data(), W.size() * 4) || !F.read(b.data(), b.size() * 4))
+      return fail(qesb_fail(QESB_ERR_ARG, "qesb_warmnet_load: truncated at layer %d", q));
+    // the tensor-core weight layout: Bm[n][k] = W[k][n], k = tap * cin + c,
+    // zero beyond 27 cin and for output channels past cout_real
+    std::vector<uint16_t> Bm((size_t)L.cout * L.Kp, 0);
+    for (size_t row = 0; row < (size_t)27 * cin; ++row)
+      for (int n = 0; n < L.cout; ++n)
+        Bm[(size_t)n * L.Kp + row] = bf16_rn(n < L.cout_real ? W[row * L.cout + n] : 0.0f);
+    if ((s = net->alloc(&p, Bm.size() * 2)) != QESB_OK) return fail(s);
+    L.Bm = static_cast<uint16_t *>(p);
+    if ((s = net->alloc(&p, b.size() * 4)) != QESB_OK) return fail(s);
+    L.bias = static_cast<float *>(p);
+    if (cudaMemcpy(L.Bm, Bm.data(), Bm.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(L.bias, b.data(), b.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(qesb_fail(QESB_ERR_CUDA, "qesb_warmnet_load: weight upload"));
+  }
+  if ((s = net->alloc(&p, sizeof(int))) != QESB_OK) return fail(s);
+  net->d_err = static_cast<int *>(p);
+  if ((s = net->alloc(&p, sizeof(unsigned))) != QESB_OK) return fail(s);
+  net->d_scale = static_cast<unsigned *>(p);
+  *out = net;
+  return QESB_OK;
+}
+
+qesb_status qesb_warmnet_destroy(qesb_warmnet *net)
+{
+  if (!net) return QESB_OK;
+  net->release();
+  delete net;
+  return QESB_OK;
+}
+
+qesb_status qesb_warm_start(qesb_handle *h, qesb_warmnet *net)
+{
+  if (!h || !net) return qesb_fail(QESB_ERR_ARG, "qesb_warm_start: null argument");
+  int Nx = 0, Ny = 0, Nz = 0, dev = -1;
+  CKS_FWD(qesb_handle_grid(h, &Nx, &Ny, &Nz, &dev));
+  if (dev != net->device)
+    return qesb_fail(QESB_ERR_ARG, "qesb_warm_start: network on device %d, handle on device %d", net->device, dev);
+  const int F = net->res << (net->nlev - 1);
+  if (Nx % F || Ny % F || Nz % F)
+    return qesb_fail(QESB_ERR_ARG, "qesb_warm_start: grid %d x %d x %d not divisible by %d", Nx, Ny, Nz, F);
+  std::lock_guard<std::mutex> lk(net->mu);
+  if (cudaSetDevice(net->device) != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "qesb_warm_start: cudaSetDevice");
+  void *s = nullptr;
+  CKS_FWD(qesb_get_stream(h, &s));
+  const int D = Nz / net->res, H = Ny / net->res, W = Nx / net->res;
+  Buffers *b = nullptr;
+  CKS_FWD(net->buffers(D, H, W, &b));
+  CKS_FWD(qesb_compute_divergence(h));
+  if (net->res == 1) {
+    CKS_FWD(qesb_warm_input(h, b->x, kInCh, net->d_scale));
+  } else {
+    CKS_FWD(qesb_warm_input(h, b->xfull, kInCh, net->d_scale));
+    CKS_FWD(qesb_net_pool2(b->xfull, b->x, Nz, Ny, Nx, kInCh, s));
+  }
+  CKS_FWD(net->forward(*b, D, H, W, s));
+  CKS_FWD(net->res == 1 ? qesb_warm_apply(h, b->y, kHeadN, net->d_scale)
+                        : qesb_warm_apply_up2(h, b->y, kHeadN, net->d_scale));
+  int err = 0;
+  if (cudaMemcpyAsync(&err, net->d_err, sizeof err, cudaMemcpyDeviceToHost, (cudaStream_t)s) != cudaSuccess ||
+      cudaStreamSynchronize((cudaStream_t)s) != cudaSuccess)
+    return qesb_fail(QESB_ERR_CUDA, "qesb_warm_start: %s", cudaGetErrorString(cudaGetLastError()));
+  if (err) return qesb_fail(QESB_ERR_CUDA, "qesb_warm_start: a tensor-core completion wait gave up");
+  return QESB_OK;
+}
+
+}  // extern "C"

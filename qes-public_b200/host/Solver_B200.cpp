@@ -46,7 +46,18 @@ void Solver_B200::solve(WINDSGeneralData *WGD, const int &itermax)
                         WGD->m.data(), WGD->n.data(), WGD->icellflag.data(), WGD->u0.data(),
                         WGD->v0.data(), WGD->w0.data()),
         "qesb_set_inputs");
-  check(qesb_set_lambda(handle_, lambda.data()), "qesb_set_lambda");
+  bool from_zero = true;  // a solve from lambda = 0: the first, or the first after resetLambda
+  for (float x : lambda)
+    if (x != 0.0f) {
+      from_zero = false;
+      break;
+    }
+  if (net_ && from_zero) {
+    std::cout << "[Solver]\t Learned warm start ..." << std::endl;
+    check(qesb_warm_start(handle_, net_), "qesb_warm_start");
+  } else {
+    check(qesb_set_lambda(handle_, lambda.data()), "qesb_set_lambda");
+  }
   qesb_stats st{};
   check(qesb_solve(handle_, itermax, WGD->u.data(), WGD->v.data(), WGD->w.data(), &st), "qesb_solve");
   check(qesb_get_lambda(handle_, lambda.data()), "qesb_get_lambda");

@@ -25,6 +25,13 @@ public:
   // for (qesb_set_prephase, qesb_set_option, qesb_set_stream, qesb_solve_batch).
   qesb_handle *handle() const { return handle_; }
 
+  // The learned warm start (qesb_warm_start): every solve that would start
+  // from lambda = 0 (the first one, and each one after resetLambda, as
+  // qesWinds solves) starts from the network's prediction instead; a solve
+  // that continues from a previous lambda (QES-Fire's repeated solves) keeps
+  // it. The network is the caller's (qesb_warmnet_load); nullptr turns it off.
+  void useLearnedStart(qesb_warmnet *net) { net_ = net; }
+
 protected:
   // Solver::solve semantics (src/winds/Solver_CPU.cpp:42-238): reads e..n,
   // icellflag, u0 v0 w0 and writes u v w of WGD. lambda lives in the base
@@ -35,4 +42,5 @@ protected:
 
 private:
   qesb_handle *handle_ = nullptr;
+  qesb_warmnet *net_ = nullptr;
 };

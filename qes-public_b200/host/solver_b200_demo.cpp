@@ -5,7 +5,9 @@
 // OpenMP build), then resetLambda and solve through Solver*. Inputs come from
 // the library's city generator; u, v, w and lambda are written to a binary
 // file for comparison.
-//   solver_b200_demo <out.bin> <Nx> <Ny> <Nz> <seed> <nbuildings> <itermax> <tol> [calls] [type]
+// With a weights file (type 5 only) every solve that starts from lambda = 0
+// uses the learned warm start (Solver_B200::useLearnedStart).
+//   solver_b200_demo <out.bin> <Nx> <Ny> <Nz> <seed> <nbuildings> <itermax> <tol> [calls] [type] [weights]
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -48,6 +50,14 @@ int main(int argc, char **argv)
   }
 
   Solver *solver = SolverFactory::create(type, wgd.domain, tol);
+  qesb_warmnet *net = nullptr;
+  if (argc > 11 && type == B200_Type) {
+    if (qesb_warmnet_load(argv[11], 0, &net) != QESB_OK) {
+      std::fprintf(stderr, "warm-start network: %s\n", qesb_last_error());
+      return 1;
+    }
+    static_cast<Solver_B200 *>(solver)->useLearnedStart(net);
+  }
   solver->resetLambda();
   for (int c = 0; c < calls; ++c) solver->solve(&wgd, itermax);
 
@@ -63,5 +73,6 @@ int main(int argc, char **argv)
   std::fclose(fo);
   // Solver has no virtual destructor: delete through the type the factory made
   if (type == B200_Type) delete static_cast<Solver_B200 *>(solver);
+  qesb_warmnet_destroy(net);
   return 0;
 }

@@ -135,6 +135,9 @@ def lib() -> C.CDLL:
             "qesb_solve_noalloc": ([C.POINTER(Grid), C.c_float, C.c_int] + [V] * 14
                                    + [V, C.POINTER(Stats)], C.c_int),
             "qesb_umma_selftest": ([V, V, V, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+            "qesb_warmnet_load": ([C.c_char_p, C.c_int, C.POINTER(V)], C.c_int),
+            "qesb_warmnet_destroy": ([V], C.c_int),
+            "qesb_warm_start": ([V, V], C.c_int),
             "qesb_conv3d": ([V, C.c_int, C.c_int, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, V,
                              C.c_int, C.c_int, V, V, V, C.c_int, V, V, V], C.c_int),
             "qesb_net_set_conv_path": ([C.c_int], C.c_int),

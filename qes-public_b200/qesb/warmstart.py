@@ -308,14 +308,56 @@ class WarmStartNet:
         out["step"] = np.array(self.step_count)
         return out
 
+    def layer_order(self):
+        """Layer names in the order of the library's weights file."""
+        L = self.nlev
+        return ([n for l in range(L) for n in (f"e{l}a", f"e{l}")] +
+                [n for l in range(L - 2, -1, -1) for n in (f"d{l}a", f"d{l}")] + ["head"])
+
     def save(self, path):
-        np.savez_compressed(path, **self.state())
+        """Weights file: the library's "QESBWNT1" format when path ends in
+        .qwn (what qesb_warmnet_load reads), else a numpy .npz (with the
+        training step count)."""
+        if not str(path).endswith(".qwn"):
+            np.savez_compressed(path, **self.state())
+            return
+        with open(path, "wb") as f:
+            f.write(b"QESBWNT1")
+            f.write(np.array([self.nlev, self.res, IN_CH, HEAD_N], np.int32).tobytes())
+            f.write(np.array(self.CH, np.int32).tobytes())
+            for name in self.layer_order():
+                L = self.layers[name]
+                f.write(np.array([L.c1, L.c2, L.cout, L.cout_real, L.relu, L.up1], np.int32).tobytes())
+                f.write(L.W.cpu().numpy().astype(np.float32).tobytes())
+                f.write(L.b.cpu().numpy().astype(np.float32).tobytes())
+
+    @staticmethod
+    def read_qwn(path) -> dict:
+        """The arrays of a "QESBWNT1" weights file, as state() names them."""
+        raw = open(path, "rb").read()
+        if raw[:8] != b"QESBWNT1":
+            raise ValueError(f"{path} is not a warm-start network file")
+        nlev, res, _, _ = np.frombuffer(raw, np.int32, 4, 8)
+        ch = np.frombuffer(raw, np.int32, int(nlev), 24)
+        out = {"channels": ch.copy(), "res": np.array(res), "step": np.array(0)}
+        pos = 24 + 4 * int(nlev)
+        names = ([n for l in range(nlev) for n in (f"e{l}a", f"e{l}")] +
+                 [n for l in range(nlev - 2, -1, -1) for n in (f"d{l}a", f"d{l}")] + ["head"])
+        for name in names:
+            c1, c2, cout, _, _, _ = (int(x) for x in np.frombuffer(raw, np.int32, 6, pos))
+            pos += 24
+            n = 27 * (c1 + c2) * cout
+            out[f"{name}.W"] = np.frombuffer(raw, np.float32, n, pos).copy()
+            pos += 4 * n
+            out[f"{name}.b"] = np.frombuffer(raw, np.float32, cout, pos).copy()
+            pos += 4 * cout
+        return out
 
     @classmethod
     def from_file(cls, path, device=0):
-        z = np.load(path)
+        z = cls.read_qwn(path) if str(path).endswith(".qwn") else dict(np.load(path))
         net = cls(device=device, channels=tuple(int(c) for c in z["channels"]),
-                  res=int(z["res"]) if "res" in z.files else 1)
+                  res=int(z["res"]) if "res" in z else 1)
         for name, L in net.layers.items():
             L.W.copy_(net.torch.from_numpy(z[f"{name}.W"]).to(net.dev))
             L.b.copy_(net.torch.from_numpy(z[f"{name}.b"]).to(net.dev))
@@ -330,4 +372,27 @@ def shapes_of(solver: Solver_B200) -> Shapes:
 
 
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "weights",
-                               "warmstart_city.npz")
+                               "warmstart_city.qwn")
+
+
+class WarmNet:
+    """The learned warm start through the C ABI (qesb_warmnet_load,
+    qesb_warm_start): inference only, the layer loop in the library."""
+
+    def __init__(self, path=DEFAULT_WEIGHTS, device=0):
+        self._p = C.c_void_p()
+        check(lib().qesb_warmnet_load(os.fsencode(path), int(device), C.byref(self._p)))
+
+    def warm_start(self, solver: Solver_B200):
+        check(lib().qesb_warm_start(solver._h, self._p))
+
+    def close(self):
+        if self._p:
+            lib().qesb_warmnet_destroy(self._p)
+            self._p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -9,7 +9,8 @@ held-out 256 x 256 x 64 cities (seeds disjoint from training), each solved to
 the benchmark's stopping rule (max|dlambda| <= 1e-3, FP64) from lambda = 0 and
 from the network's prediction; reports iterations, device ms (network
 included) and the largest wind difference between the two results.
-Writes DIR/warmstart_city.npz (weights) and DIR/warmstart_report.json.
+Writes DIR/warmstart_city.qwn (weights, the library format qesb_warmnet_load reads) and
+DIR/warmstart_report.json.
 """
 import argparse
 import json
@@ -173,7 +174,7 @@ def main():
     t_gen = time.time() - t0
     losses, t_train = train(net, X, T, weight, s, args.epochs, args.lr, coarse=((8, args.coarse_beta),))
     del X, T
-    wpath = os.path.join(args.out, "warmstart_city.npz")
+    wpath = os.path.join(args.out, "warmstart_city.qwn")
     net.save(wpath)
     rows = evaluate(net, args.eval, args.eval_workload)
     it_p = np.array([r["plain_iters"] for r in rows], float)

@@ -83,3 +83,35 @@ def test_dropin_type_5_through_the_reference_factory(tmp_path, calls):
     np.testing.assert_array_equal(lam, lam1)
     np.testing.assert_array_equal(u, u1)
     np.testing.assert_array_equal(ww, w1)
+
+
+@needs_demo
+@pytest.mark.gpu
+def test_dropin_learned_warm_start_from_cpp(tmp_path):
+    """Solver_B200::useLearnedStart through the reference factory: the C++
+    caller's solves from lambda = 0 start from the network (qesb_warm_start).
+    The result matches the same warm-started solve run from Python."""
+    from qesb import warmstart as ws
+
+    nx, ny, nz, itermax = 64, 48, 32, 120
+    out = tmp_path / "warm.bin"
+    r = subprocess.run([DEMO, str(out), str(nx), str(ny), str(nz), str(SEED), str(NB), str(itermax), "1e-9", "1",
+                        "5", ws.DEFAULT_WEIGHTS], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "Learned warm start" in r.stdout
+    d = qesb.Domain(nx, ny, nz, 2.0, 2.0, 1.0, qesb.city_dz(nz, 1.0, 1.03))
+    nf, nc = d.numFaceCentered(), d.numCellCentered()
+    raw = np.fromfile(out, dtype=np.float32)
+    lam = raw[3 * nf:]
+    c = qesb.city_random(d, SEED, NB, fp=(6, 16), h=(4, 20))
+    w = qesb.city_build(d, c.buildings, c.inflow)
+    net = ws.WarmStartNet.from_file(ws.DEFAULT_WEIGHTS, device=0)
+    with qesb.Solver_B200(d, 1e-9) as s:
+        s.set_inputs(w)
+        net.warm_start(s)
+        s.solve(w, itermax, set_inputs=False)
+        lam_py = s.lambda_
+    cold, *_ = O.sor(d, w, O.divergence(d, w), 1e-9, itermax)
+    scale = np.abs(lam_py).max()
+    assert np.abs(lam - lam_py).max() <= 1e-2 * scale
+    assert np.abs(lam - cold).max() > 10 * np.abs(lam - lam_py).max()  # the start was the network's

@@ -203,3 +203,50 @@ def test_half_resolution_apply_interpolates_trilinearly():
                 assert abs(L[k, j, i] - want) < 1e-4, (k, j, i, L[k, j, i], want)
     assert not L[:, 0, :].any() and not L[:, :, 0].any() and not L[Dn].any()
     np.testing.assert_array_equal(L[0], L[1])
+
+
+def test_cabi_warm_start_matches_the_python_network():
+    """qesb_warmnet_load + qesb_warm_start (the layer loop in the library) give
+    the start the Python orchestration gives from the same weights file: the
+    same kernels in the same order, up to the order of the split-K partial
+    sums of the deep levels (FP32 atomics)."""
+    from qesb import warmstart as ws
+
+    if not os.path.exists(ws.DEFAULT_WEIGHTS):
+        pytest.skip("no trained weights committed")
+    w, _ = qesb.random_city("city256", 900003)
+    py = ws.WarmStartNet.from_file(ws.DEFAULT_WEIGHTS, device=0)
+    cnet = ws.WarmNet(ws.DEFAULT_WEIGHTS, device=0)
+    try:
+        with qesb.Solver_B200(w.domain, RULE_TOL) as s:
+            s.set_inputs(w)
+            py.warm_start(s)
+            lp = s.lambda_
+            s.resetLambda()
+            cnet.warm_start(s)
+            lc = s.lambda_
+            cnet.warm_start(s)  # a second call reuses the grid's buffers
+            lc2 = s.lambda_
+    finally:
+        cnet.close()
+    scale = np.abs(lp).max()
+    assert scale > 0 and np.abs(lc).max() > 0
+    assert np.abs(lc - lp).max() <= 1e-2 * scale, np.abs(lc - lp).max() / scale
+    assert np.abs(lc2 - lc).max() <= 1e-2 * scale
+
+
+def test_cabi_warm_start_rejects_grids_it_cannot_pool():
+    from qesb import warmstart as ws
+
+    if not os.path.exists(ws.DEFAULT_WEIGHTS):
+        pytest.skip("no trained weights committed")
+    d = qesb.Domain(40, 32, 16, 2.0, 2.0, 1.0, qesb.city_dz(16, 1.0, 1.03))
+    w = qesb.city_build(d, [], qesb.Inflow(5.0, 10.0, 0.15, 270.0))
+    cnet = ws.WarmNet(ws.DEFAULT_WEIGHTS, device=0)
+    try:
+        with qesb.Solver_B200(d, 1e-9) as s:
+            s.set_inputs(w)
+            with pytest.raises(qesb.QesbError, match="not divisible"):
+                cnet.warm_start(s)
+    finally:
+        cnet.close()

@@ -99,6 +99,8 @@ def parse(argv=None):
     ap.add_argument("--ensemble", action="store_true",
                     help="batched ensemble alone: cities of uneven size x 36 wind directions (solves/s, p50/p99)")
     ap.add_argument("--ensemble-domains", type=int, default=64)
+    ap.add_argument("--ensemble-list-cells", type=int, default=250_000_000,
+                    help="cells per ensemble launch list (whole cities; 0: one city per list)")
     ap.add_argument("--fire-loop", type=int, default=0,
                     help="QES-Fire solve pattern: this many fire steps warm-started from the previous lambda, exit")
     ap.add_argument("--profile-batch", action="store_true",
@@ -983,12 +985,12 @@ def ensemble_run(args, print_line=True, dist=None, dev=0):
     config's 60), each at 36 wind directions 10 degrees apart, 2304 solves for
     64 cities. Inputs are built on the device (qesb_city_build_device,
     reported as setup, not timed). Cities are packed into launch lists of
-    uneven sizes (whole cities, up to 250 M cells a list), each list one
-    qesb_solve_batch: over-relaxed pre-phase warm start, reference loop to the
-    rule, correction; the list sweep's launch shape tuned once on the first
-    list. solves/s = all solves / the sum of list times (CUDA events); the
-    latency of a solve = device time from its list's first reference-loop sweep
-    to the poll that ended it."""
+    uneven sizes (whole cities, up to --ensemble-list-cells cells a list), each
+    list one qesb_solve_batch: over-relaxed pre-phase warm start, reference
+    loop to the rule, correction; the list sweep's launch shape tuned once on
+    the first list. solves/s = all solves / the sum of list times (CUDA
+    events); the latency of a solve = device time from the start of its list's
+    iterations (pre-phase included) to the poll that ended it."""
     import torch
 
     import qesb
@@ -1006,7 +1008,7 @@ def ensemble_run(args, print_line=True, dist=None, dev=0):
     for d in mine:
         Nx, Ny, Nz = dims[d]
         cells = ndir * Nx * Ny * (Nz + 1)
-        if cur and cur_cells + cells > 250_000_000:
+        if cur and cur_cells + cells > args.ensemble_list_cells:
             lists.append(cur)
             cur, cur_cells = [], 0
         cur.append(d)
@@ -1082,7 +1084,8 @@ def ensemble_run(args, print_line=True, dist=None, dev=0):
         "value": n / (total_ms * 1e-3), "unit": "solves/s", "n_gpus": world, "higher_is_better": True,
         "scaling": "strong", "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{nd} cities, Nx,Ny ~ U[64,256], Nz ~ U[32,96], x {ndir} directions",
-                   "solves": n, "launch_lists": len(list_sizes), "solves_per_list": list_sizes, "tol": TOL,
+                   "solves": n, "launch_lists": len(list_sizes), "solves_per_list": list_sizes,
+                   "cells_per_list_cap": args.ensemble_list_cells, "tol": TOL,
                    "itermax": ITERMAX, "window": WINDOW, "window_tol": WINDOW_TOL,
                    "warm_start": "over-relaxed pre-phase, omega = 2 - 7.5/max(Nx, Ny) within [1.85, 1.97], "
                                  f"to {PRE_TOL}", "cells_total": cells_total, "batch_variant": batch_shape},

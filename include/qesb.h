@@ -203,8 +203,9 @@ qesb_status qesb_fp64_same_sor(qesb_handle *h, const float *lambda0, float pre_o
  * does. Results are those of n qesb_solve_device calls, bit for bit: lambda
  * stays in each handle; u[i], v[i], w[i] (device pointers, each array
  * nullable) receive domain i's corrected winds. st[i] (nullable array): as
- * for qesb_solve, with ms_sor = device time from the batch's first sweep to
- * the poll that ended domain i, ms_total = the whole batch. All handles on one
+ * for qesb_solve, with ms_sor = device time from the start of the batch's
+ * iterations (pre-phase included) to the poll that ended domain i, ms_total =
+ * the whole batch. All handles on one
  * device; the work runs on handles[0]'s stream, whose "variant" option picks
  * the bulk launch shape when it names one. */
 qesb_status qesb_solve_batch(qesb_handle *const *handles, int n, int itermax, float *const *u,
@@ -295,6 +296,10 @@ qesb_status qesb_get_stream(qesb_handle *h, void **stream);
  *                     qesb_solve starts from it. */
 qesb_status qesb_compute_divergence(qesb_handle *h);
 qesb_status qesb_warm_input(qesb_handle *h, void *x, int C, unsigned *scale);
+/* qesb_warm_input followed by a 2x2x2 average (qesb_net_pool2), bit for bit,
+ * in one pass: the input of a network run at half resolution, on the
+ * (Nz/2) x (Ny/2) x (Nx/2) grid (even sizes). */
+qesb_status qesb_warm_input_half(qesb_handle *h, void *x, int C, unsigned *scale);
 qesb_status qesb_warm_target(qesb_handle *h, float *tgt, float *w, const unsigned *scale);
 qesb_status qesb_warm_apply(qesb_handle *h, const float *yhead, int N, const unsigned *scale);
 /* qesb_warm_apply for a network run at half resolution: yhead on the

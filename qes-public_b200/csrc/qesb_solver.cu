@@ -453,6 +453,50 @@ __global__ void k_warm_input(DevGrid G, int Dn, int C, const float *__restrict__
   }
 }
 
+// The network input at half resolution in one pass: each voxel (xx, yy, zz)
+// of the (Dn/2) x (Y/2) x (X/2) grid is the 2x2x2 average of k_warm_input's
+// features of cells (2xx + a, 2yy + b, 2zz + c), each first rounded to BF16
+// and summed in FP32 in k_pool2's order, then scaled by 1/8 and rounded: the
+// bits of k_warm_input followed by the pooling, without the full-resolution
+// tensor. One block per half-resolution (row, layer), threads along x.
+__global__ void k_warm_input_half(DevGrid G, int C, const float *__restrict__ R, const int *__restrict__ flag,
+                                  const float *__restrict__ dz, const unsigned *__restrict__ smax, float dz_mean,
+                                  float height, uint16_t *__restrict__ x)
+{
+  const int yy = blockIdx.y, zz = blockIdx.z, W2 = G.X / 2, H2 = G.Y / 2;
+  __shared__ float s_zc[2];
+  if (threadIdx.x < 2) {
+    const int k = 2 * zz + threadIdx.x;
+    float zc = 0.0f;
+    for (int q = 1; q < k; ++q) zc += dz[q];
+    s_zc[threadIdx.x] = zc + 0.5f * dz[k];
+  }
+  __syncthreads();
+  const float inv_s = 1.0f / fmaxf(__uint_as_float(*smax), 1e-30f);
+  auto bf = [](float v) { return __uint_as_float(bf16_bits_rne(v) << 16); };
+  for (int xx = blockIdx.x * blockDim.x + threadIdx.x; xx < W2; xx += gridDim.x * blockDim.x) {
+    float acc[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int c = q >> 2, k = 2 * zz + c, j = 2 * yy + ((q >> 1) & 1), i = 2 * xx + (q & 1);
+      const bool upd = i >= 1 && i <= G.X - 2 && j >= 1 && j <= G.Y - 2 && k >= 1 && k <= G.Z - 2;
+      acc[0] += bf(upd ? R[G.pad(i, j, k)] * inv_s : 0.0f);
+      acc[1] += bf(is_solid(flag[G.cell(i, j, k)]) ? 1.0f : 0.0f);
+      acc[2] += bf(dz[k] / dz_mean);
+      acc[3] += bf(upd ? 0.0f : 1.0f);
+      acc[4] += bf(s_zc[c] / height);
+    }
+    uint4 lo;
+    lo.x = bf16_bits_rne(acc[0] * 0.125f) | (bf16_bits_rne(acc[1] * 0.125f) << 16);
+    lo.y = bf16_bits_rne(acc[2] * 0.125f) | (bf16_bits_rne(acc[3] * 0.125f) << 16);
+    lo.z = bf16_bits_rne(acc[4] * 0.125f);
+    lo.w = 0u;
+    uint4 *dst = reinterpret_cast<uint4 *>(x + (((long)zz * H2 + yy) * W2 + xx) * C);
+    dst[0] = lo;
+    for (int q = 1; q < C / 8; ++q) dst[q] = make_uint4(0, 0, 0, 0);
+  }
+}
+
 // Training target lambda / s and weight (1 on updated cells) on the net grid.
 __global__ void k_warm_target(DevGrid G, int Dn, const float *__restrict__ L, const unsigned *__restrict__ smax,
                               float *__restrict__ tgt, float *__restrict__ w)
@@ -558,7 +602,8 @@ struct SweepList {
     }
     const SweepCtl ctl{0u, n, 0, 0, 0ull};
     CK(cudaMemcpyAsync((void *)a.dom, doms.data(), sizeof(SweepDomain) * n, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(a.ctl, &ctl, sizeof ctl, cudaMemcpyHostToDevice, s));
+    // everything but t0, the batch's start stamp (k_sweep_stamp), which outlives the pre-phase's list
+    CK(cudaMemcpyAsync(a.ctl, &ctl, offsetof(SweepCtl, t0), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(a.active, active.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(a.uoff, uoff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
@@ -987,7 +1032,7 @@ constexpr SweepVariant make_bulk(const char *name)
                       k_sor_bulk<0, W, NS, ASYNC, true>,
                       k_sor_bulk<1, W, NS, ASYNC, true>};
 }
-template <int TY, int RW, int MINB, int DIST = 2>
+template <int TY, int RW, int MINB, int DIST = 2, int PK = 0>
 constexpr SweepVariant make_zm(const char *name)
 {
   return SweepVariant{name,
@@ -995,10 +1040,10 @@ constexpr SweepVariant make_zm(const char *name)
                       TY,
                       TY * RW,
                       zm_smem_bytes<TY * RW, DIST>(),
-                      k_sor_zm<0, TY, RW, DIST, false, MINB>,
-                      k_sor_zm<1, TY, RW, DIST, false, MINB>,
-                      k_sor_zm<0, TY, RW, DIST, true, MINB>,
-                      k_sor_zm<1, TY, RW, DIST, true, MINB>};
+                      k_sor_zm<0, TY, RW, DIST, false, MINB, PK>,
+                      k_sor_zm<1, TY, RW, DIST, false, MINB, PK>,
+                      k_sor_zm<0, TY, RW, DIST, true, MINB, PK>,
+                      k_sor_zm<1, TY, RW, DIST, true, MINB, PK>};
 }
 const SweepVariant kSweepVariants[] = {
     // streaming split kernels (option "variant" 5..17)
@@ -1027,6 +1072,9 @@ const SweepVariant kSweepVariants[] = {
     make_zm<8, 2, 2>("zm_y8x2_b2"),
     // copies one plane ahead: smaller rings, more CTAs per SM (48..50)
     make_zm<4, 2, 5, 1>("zm_y4x2_d1_b5"), make_zm<4, 2, 4, 1>("zm_y4x2_d1_b4"), make_zm<2, 2, 8, 1>("zm_y2x2_d1_b8"),
+    // the same with the update arithmetic on cell pairs (sm_100 packed FP32) (51..54)
+    make_zm<4, 2, 4, 2, 1>("zm_y4x2_b4_pk"), make_zm<4, 2, 5, 1, 1>("zm_y4x2_d1_b5_pk"),
+    make_zm<4, 2, 4, 1, 1>("zm_y4x2_d1_b4_pk"), make_zm<2, 2, 8, 1, 1>("zm_y2x2_d1_b8_pk"),
 };
 constexpr int kNumSweep = sizeof(kSweepVariants) / sizeof(kSweepVariants[0]);
 constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the first sweep shape
@@ -1702,6 +1750,24 @@ qesb_status qesb_warm_input(qesb_handle *h, void *x, int C, unsigned *scale)
   return QESB_OK;
 }
 
+qesb_status qesb_warm_input_half(qesb_handle *h, void *x, int C, unsigned *scale)
+{
+  if (!h || !x || !scale || C < 8 || C % 8) return qesb_fail(QESB_ERR_ARG, "qesb_warm_input_half: bad arguments");
+  const DevGrid &G = h->G;
+  if (G.X % 2 || G.Y % 2 || (G.Z - 1) % 2)
+    return qesb_fail(QESB_ERR_ARG, "qesb_warm_input_half: the net grid (Nz x Ny x Nx) must have even sizes");
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemsetAsync(scale, 0, sizeof(unsigned), h->stream));
+  k_absmax_R<<<148 * 4, 256, 0, h->stream>>>(G, h->d_R, scale);
+  double dzs = 0.0, height = 0.0;
+  for (int k = 1; k < G.Z; ++k) dzs += h->dz[k];
+  for (int k = 1; k < G.Z - 1; ++k) height += h->dz[k];
+  k_warm_input_half<<<dim3((G.X / 2 + 127) / 128, G.Y / 2, (G.Z - 1) / 2), 128, 0, h->stream>>>(
+      G, C, h->d_R, h->d_flag, h->d_dz, scale, (float)(dzs / (G.Z - 1)), (float)height, (uint16_t *)x);
+  CK(cudaGetLastError());
+  return QESB_OK;
+}
+
 qesb_status qesb_warm_target(qesb_handle *h, float *tgt, float *w, const unsigned *scale)
 {
   if (!h || !tgt || !w || !scale) return qesb_fail(QESB_ERR_ARG, "qesb_warm_target: bad arguments");
@@ -1988,6 +2054,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   SweepList list;
   CKS(list.create(n));
   list.a.wait_limit = h0->opt_wait_limit;
+  k_sweep_stamp<<<1, 1, 0, s>>>(list.a.ctl);  // the latencies (ms_sor) count from here
   qesb_status qs = QESB_OK;
   int launched = 0, pre_launched = 0;
   CK(cudaEventRecord(h0->evs[0], s));
@@ -2022,7 +2089,6 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
                           s) != cudaSuccess)
         qs = qesb_fail(QESB_ERR_CUDA, "qesb_solve_batch: window snapshot copy failed");
   if (qs == QESB_OK) {
-    k_sweep_stamp<<<1, 1, 0, s>>>(list.a.ctl);
     SweepGraph gx;
     CK(cudaEventRecord(h0->evs[2], s));
     if (itermax > 0)

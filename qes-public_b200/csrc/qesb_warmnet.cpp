@@ -46,7 +46,6 @@ struct Layer {
 
 // Activations of one net grid shape (D, H, W at level 0), BF16 channels-last.
 struct Buffers {
-  uint16_t *xfull = nullptr;  // res 2: the cell-grid input before pooling
   uint16_t *x = nullptr;
   float *y = nullptr;
   std::vector<uint16_t *> ea, e, p, da, d;
@@ -100,10 +99,6 @@ struct qesb_warmnet {
     Buffers b;
     auto V = [&](int l) { return (size_t)(D >> l) * (size_t)(H >> l) * (size_t)(W >> l); };
     void *p = nullptr;
-    if (res == 2) {
-      CKS_FWD(alloc(&p, V(0) * 8 * kInCh * 2));
-      b.xfull = static_cast<uint16_t *>(p);
-    }
     CKS_FWD(alloc(&p, V(0) * kInCh * 2));
     b.x = static_cast<uint16_t *>(p);
     CKS_FWD(alloc(&p, V(0) * kHeadN * 4));
@@ -280,12 +275,8 @@ qesb_status qesb_warm_start(qesb_handle *h, qesb_warmnet *net)
   Buffers *b = nullptr;
   CKS_FWD(net->buffers(D, H, W, &b));
   CKS_FWD(qesb_compute_divergence(h));
-  if (net->res == 1) {
-    CKS_FWD(qesb_warm_input(h, b->x, kInCh, net->d_scale));
-  } else {
-    CKS_FWD(qesb_warm_input(h, b->xfull, kInCh, net->d_scale));
-    CKS_FWD(qesb_net_pool2(b->xfull, b->x, Nz, Ny, Nx, kInCh, s));
-  }
+  if (net->res == 1) CKS_FWD(qesb_warm_input(h, b->x, kInCh, net->d_scale));
+  else CKS_FWD(qesb_warm_input_half(h, b->x, kInCh, net->d_scale));
   CKS_FWD(net->forward(*b, D, H, W, s));
   CKS_FWD(net->res == 1 ? qesb_warm_apply(h, b->y, kHeadN, net->d_scale)
                         : qesb_warm_apply_up2(h, b->y, kHeadN, net->d_scale));

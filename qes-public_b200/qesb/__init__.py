@@ -145,6 +145,7 @@ def lib() -> C.CDLL:
                                    C.c_long, V, V, V], C.c_int),
             "qesb_compute_divergence": ([V], C.c_int),
             "qesb_warm_input": ([V, V, C.c_int, V], C.c_int),
+            "qesb_warm_input_half": ([V, V, C.c_int, V], C.c_int),
             "qesb_warm_target": ([V, V, V, V], C.c_int),
             "qesb_warm_apply": ([V, V, C.c_int, V], C.c_int),
             "qesb_warm_apply_up2": ([V, V, C.c_int, V], C.c_int),

@@ -261,13 +261,6 @@ class WarmStartNet:
         f = shapes_of(solver)
         return Shapes(f.D // self.res, f.H // self.res, f.W // self.res)
 
-    def _full_input(self, f: Shapes):
-        key = ("xfull", f.D, f.H, f.W)
-        if key not in self._buf:
-            self._buf[key] = self.torch.zeros(f.V(0) * IN_CH, dtype=self.torch.bfloat16, device=self.dev)
-            self.torch.cuda.synchronize(self.dev)
-        return self._buf[key]
-
     def input_from(self, solver: Solver_B200, s: Shapes, scale):
         """Network input of the solver's current inputs into buffer 'x' of the
         network grid s (2x2x2 averages of the cell features when res = 2), on
@@ -276,10 +269,7 @@ class WarmStartNet:
         if self.res == 1:
             check(lib().qesb_warm_input(solver._h, _p(self._bufs(s)["x"]), IN_CH, _p(scale)))
             return
-        f = shapes_of(solver)
-        xf = self._full_input(f)
-        check(lib().qesb_warm_input(solver._h, _p(xf), IN_CH, _p(scale)))
-        check(lib().qesb_net_pool2(_p(xf), _p(self._bufs(s)["x"]), f.D, f.H, f.W, IN_CH, solver.stream_ptr()))
+        check(lib().qesb_warm_input_half(solver._h, _p(self._bufs(s)["x"]), IN_CH, _p(scale)))
 
     def warm_start(self, solver: Solver_B200, stream=None):
         """Predicts lambda for the solver's inputs and sets it as the start.

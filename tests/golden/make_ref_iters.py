@@ -22,7 +22,8 @@ serial, and Solver_CPU_RB at one thread has no max_error reset race
 (Solver_CPU_RB.cpp:166); the calls use tol < 0, so the loop runs exactly
 WINDOW iterations either way. The fixture keeps the serial Solver_CPU winds
 on every 4th face column in x and y (all layers) and the max divergence of
-the full field.
+the full field; ref_iters.json holds every run's max divergence (FP64, fluid
+cells, k <= nz-4, the solver's final check).
 """
 import json
 import os
@@ -66,7 +67,8 @@ def run(args):
         if step == WINDOW and drift <= WINDOW_TOL:
             break
     out = {"iterations": n, "window_drift": drift, "solve_seconds_1thread": secs,
-           "ms_per_iteration_1thread": 1e3 * secs / n, "wall_s": time.time() - t0}
+           "ms_per_iteration_1thread": 1e3 * secs / n, "wall_s": time.time() - t0,
+           "max_div": O.max_divergence(d, w.icellflag, u, v, ww)}
     if kind == 0 and seed in FIXTURE_SEEDS:
         shape = (d.nz(), d.ny(), d.nx())
         sub = (slice(None), slice(None, None, STRIDE), slice(None, None, STRIDE))

@@ -250,3 +250,27 @@ def test_cabi_warm_start_rejects_grids_it_cannot_pool():
                 cnet.warm_start(s)
     finally:
         cnet.close()
+
+
+def test_half_resolution_input_equals_full_input_then_pooling():
+    """qesb_warm_input_half: the network input of a half-resolution network in
+    one pass, bit for bit qesb_warm_input followed by the 2x2x2 average."""
+    import torch
+
+    w, _ = qesb.random_city("city128", 1001)
+    Nx, Ny, Nz = w.domain.base
+    full = torch.zeros(Nz * Ny * Nx * 16, dtype=torch.bfloat16, device="cuda")
+    pooled = torch.zeros(full.numel() // 8, dtype=torch.bfloat16, device="cuda")
+    half = torch.ones_like(pooled)
+    scale = torch.zeros(2, dtype=torch.int32, device="cuda")
+    with qesb.Solver_B200(w.domain, 1e-9) as s:
+        s.set_inputs(w)
+        torch.cuda.synchronize()
+        L = qesb.lib()
+        qesb.check(L.qesb_compute_divergence(s._h))
+        qesb.check(L.qesb_warm_input(s._h, full.data_ptr(), 16, scale.data_ptr()))
+        qesb.check(L.qesb_net_pool2(full.data_ptr(), pooled.data_ptr(), Nz, Ny, Nx, 16, s.stream_ptr()))
+        qesb.check(L.qesb_warm_input_half(s._h, half.data_ptr(), 16, scale.data_ptr() + 4))
+        torch.cuda.synchronize()
+    assert int(scale[0]) == int(scale[1]) != 0
+    assert torch.equal(half.view(torch.int16), pooled.view(torch.int16))

@@ -67,7 +67,7 @@ ALG_BYTES_PER_CELL_ITER = 36  # 6 coefficients + R read (28 B), lambda read + wr
 SIZE_ITERS = 300  # iterations per timed solve of the size sweep
 PRE_OMEGA = 1.97
 PRE_TOL = 2e-3
-HEADLINE = "prephase"
+HEADLINE = "network+prephase"  # the metric's method: the learned start, then the pre-phase
 ARMS = {"plain": (False, False), "prephase": (False, True), "network": (True, False),
         "network+prephase": (True, True)}
 
@@ -946,9 +946,12 @@ def run_b200(args):
                        "network_levels": net.nlev, "channels": list(net.CH),
                        "sweep_variant": variant, "batch_variant": batch_variant,
                        "parallelism": f"replicas x{world}",
-                       "warm_start": f"pre-phase: red-black SOR at omega {PRE_OMEGA} from the start to "
+                       "warm_start": f"the learned network's prediction (BF16 tcgen05 convolutions, half "
+                                     f"resolution), then the pre-phase: red-black SOR at omega {PRE_OMEGA} to "
                                      f"max|dlambda| <= {PRE_TOL}; then the reference loop (omega 1.78) to the "
-                                     f"rule",
+                                     f"rule; arms holds plain SOR, the pre-phase alone and the network alone",
+                       "learned_start_note": "the pre-phase alone (arms.prephase) is faster: the network's "
+                                             "start saves fewer pre-phase iterations than its forward pass costs",
                        "l2": "8 domains x ~40 MB packed sweep data + network buffers > L2 (126 MB) per step"},
             "arms": arms,
             "speedup_vs_plain": ms_plain / ms_head,

@@ -1032,7 +1032,7 @@ constexpr SweepVariant make_bulk(const char *name)
                       k_sor_bulk<0, W, NS, ASYNC, true>,
                       k_sor_bulk<1, W, NS, ASYNC, true>};
 }
-template <int TY, int RW, int MINB, int DIST = 2, int PK = 0>
+template <int TY, int RW, int MINB, int DIST = 2>
 constexpr SweepVariant make_zm(const char *name)
 {
   return SweepVariant{name,
@@ -1040,10 +1040,10 @@ constexpr SweepVariant make_zm(const char *name)
                       TY,
                       TY * RW,
                       zm_smem_bytes<TY * RW, DIST>(),
-                      k_sor_zm<0, TY, RW, DIST, false, MINB, PK>,
-                      k_sor_zm<1, TY, RW, DIST, false, MINB, PK>,
-                      k_sor_zm<0, TY, RW, DIST, true, MINB, PK>,
-                      k_sor_zm<1, TY, RW, DIST, true, MINB, PK>};
+                      k_sor_zm<0, TY, RW, DIST, false, MINB>,
+                      k_sor_zm<1, TY, RW, DIST, false, MINB>,
+                      k_sor_zm<0, TY, RW, DIST, true, MINB>,
+                      k_sor_zm<1, TY, RW, DIST, true, MINB>};
 }
 const SweepVariant kSweepVariants[] = {
     // streaming split kernels (option "variant" 5..17)
@@ -1072,9 +1072,6 @@ const SweepVariant kSweepVariants[] = {
     make_zm<8, 2, 2>("zm_y8x2_b2"),
     // copies one plane ahead: smaller rings, more CTAs per SM (48..50)
     make_zm<4, 2, 5, 1>("zm_y4x2_d1_b5"), make_zm<4, 2, 4, 1>("zm_y4x2_d1_b4"), make_zm<2, 2, 8, 1>("zm_y2x2_d1_b8"),
-    // the same with the update arithmetic on cell pairs (sm_100 packed FP32) (51..54)
-    make_zm<4, 2, 4, 2, 1>("zm_y4x2_b4_pk"), make_zm<4, 2, 5, 1, 1>("zm_y4x2_d1_b5_pk"),
-    make_zm<4, 2, 4, 1, 1>("zm_y4x2_d1_b4_pk"), make_zm<2, 2, 8, 1, 1>("zm_y2x2_d1_b8_pk"),
 };
 constexpr int kNumSweep = sizeof(kSweepVariants) / sizeof(kSweepVariants[0]);
 constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the first sweep shape

@@ -169,31 +169,9 @@ __device__ __forceinline__ void zm_stage(const ZmSmem<TR> &sm, const ZmCopies<TR
 template <int N>
 __device__ __forceinline__ int zm_wrap(int x) { return x >= N ? x - N : x; }
 
-// The SOR update of two cells at once with the packed FP32 pair instructions
-// of sm_100 (__fmul2_rn, __fadd2_rn: per component exactly __fmul_rn and
-// __fadd_rn, never contracted), in the reference's order
-// (Solver_CPU_RB.cpp:118-125):
-//   inv * (((((e xp + f xm) + g yp) + h ym) + m zp) + n zm - r) + c1 * o
-// so each component rounds as the scalar update does. a - b is formed as
-// a + (-b), which rounds identically.
-__device__ __forceinline__ float2 zm_update2(float2 e, float2 f, float2 g, float2 h, float2 m, float2 n,
-                                             float2 xp, float2 xm, float2 yp, float2 ym, float2 zp, float2 zm,
-                                             float2 r, float2 inv, float2 c1, float2 o)
-{
-  float2 t = __fmul2_rn(e, xp);
-  t = __fadd2_rn(t, __fmul2_rn(f, xm));
-  t = __fadd2_rn(t, __fmul2_rn(g, yp));
-  t = __fadd2_rn(t, __fmul2_rn(h, ym));
-  t = __fadd2_rn(t, __fmul2_rn(m, zp));
-  t = __fadd2_rn(t, __fmul2_rn(n, zm));
-  t = __fadd2_rn(t, make_float2(-r.x, -r.y));
-  return __fadd2_rn(__fmul2_rn(inv, t), __fmul2_rn(c1, o));
-}
-
 // TY warps per CTA, RW rows per warp (rows w, w + TY, ...): tiles of TY x RW rows;
 // copies DIST planes ahead.
-// PK = 1: the update arithmetic on cell pairs (zm_update2), bit-identical.
-template <int COLOUR, int TY, int RW, int DIST, bool MULTI, int MINB, int PK = 0>
+template <int COLOUR, int TY, int RW, int DIST, bool MULTI, int MINB>
 __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
 {
   constexpr int TR = TY * RW, NT = 32 * TY, NSO = zm_other_slots(DIST), NSW = zm_own_slots(DIST);
@@ -306,46 +284,12 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
         const float zmv[4] = {zm.x, zm.y, zm.z, zm.w}, zpv[4] = {zp.x, zp.y, zp.z, zp.w};
         const float rv[4] = {rr.x, rr.y, rr.z, rr.w};
         float nv[4];
-        [[maybe_unused]] const float2 c12 = make_float2(D.c1, D.c1);
         if (__all_sync(0xffffffffu, full)) {
-          if constexpr (PK) {
-            const float2 e = make_float2(D.ve, D.ve), f = make_float2(D.vf, D.vf), g = make_float2(D.vg, D.vg);
-            const float2 hh = make_float2(D.vh, D.vh), m = make_float2(D.vm, D.vm), n = make_float2(D.vn, D.vn);
-            const float2 inv = make_float2(D.inv63, D.inv63);
 #pragma unroll
-            for (int t2 = 0; t2 < 4; t2 += 2) {
-              const float2 r2 = zm_update2(
-                  e, f, g, hh, m, n, make_float2(xpv[t2], xpv[t2 + 1]), make_float2(xmv[t2], xmv[t2 + 1]),
-                  make_float2(ypv[t2], ypv[t2 + 1]), make_float2(ymv[t2], ymv[t2 + 1]),
-                  make_float2(zpv[t2], zpv[t2 + 1]), make_float2(zmv[t2], zmv[t2 + 1]),
-                  make_float2(rv[t2], rv[t2 + 1]), inv, c12, make_float2(ov[t2], ov[t2 + 1]));
-              nv[t2] = r2.x;
-              nv[t2 + 1] = r2.y;
-            }
-          } else {
-#pragma unroll
-            for (int t4 = 0; t4 < 4; ++t4)
-              nv[t4] = D.inv63 * (D.ve * xpv[t4] + D.vf * xmv[t4] + D.vg * ypv[t4] + D.vh * ymv[t4] +
-                                  D.vm * zpv[t4] + D.vn * zmv[t4] - rv[t4]) +
-                       D.c1 * ov[t4];
-          }
-        } else if constexpr (PK) {
-#pragma unroll
-          for (int t2 = 0; t2 < 4; t2 += 2) {  // a cell pair at a time: its coefficients by wall mask
-            const unsigned ma = (upm >> t2) & 1u ? mk[t2] : 63u, mb = (upm >> (t2 + 1)) & 1u ? mk[t2 + 1] : 63u;
-            auto sel = [&](unsigned bit, float v) {
-              return make_float2((ma & bit) ? v : 0.0f, (mb & bit) ? v : 0.0f);
-            };
-            const float2 r2 = zm_update2(
-                sel(1u, D.ve), sel(2u, D.vf), sel(4u, D.vg), sel(8u, D.vh), sel(16u, D.vm), sel(32u, D.vn),
-                make_float2(xpv[t2], xpv[t2 + 1]), make_float2(xmv[t2], xmv[t2 + 1]),
-                make_float2(ypv[t2], ypv[t2 + 1]), make_float2(ymv[t2], ymv[t2 + 1]),
-                make_float2(zpv[t2], zpv[t2 + 1]), make_float2(zmv[t2], zmv[t2 + 1]),
-                make_float2(rv[t2], rv[t2 + 1]), make_float2(sinv[ma], sinv[mb]), c12,
-                make_float2(ov[t2], ov[t2 + 1]));
-            nv[t2] = r2.x;
-            nv[t2 + 1] = r2.y;
-          }
+          for (int t4 = 0; t4 < 4; ++t4)
+            nv[t4] = D.inv63 * (D.ve * xpv[t4] + D.vf * xmv[t4] + D.vg * ypv[t4] + D.vh * ymv[t4] +
+                                D.vm * zpv[t4] + D.vn * zmv[t4] - rv[t4]) +
+                     D.c1 * ov[t4];
         } else {
 #pragma unroll
           for (int t4 = 0; t4 < 4; ++t4) {

@@ -1145,14 +1145,17 @@ def run_profile_batch(args):
     import torch
 
     import qesb
+    from qesb import warmstart as ws
 
+    use_net, use_pre = ARMS[HEADLINE]
     cities = [make_city(args.workload, SEED0 + i) for i in range(args.batch)]
     solvers = [qesb.Solver_B200(w.domain, TOL) for w in cities]
+    net = ws.WarmNet(args.weights or ws.DEFAULT_WEIGHTS) if use_net else None
     try:
         for s, w in zip(solvers, cities):
             s.set_inputs(w)
             s.set_window_rule(WINDOW, WINDOW_TOL)
-            s.set_prephase(PRE_OMEGA if ARMS[HEADLINE][1] else 0.0, PRE_TOL, ITERMAX)
+            s.set_prephase(PRE_OMEGA if use_pre else 0.0, PRE_TOL, ITERMAX)
         if args.variant >= 0:
             solvers[0].set_option("variant", args.variant)
         nf = cities[0].domain.numFaceCentered()
@@ -1160,12 +1163,17 @@ def run_profile_batch(args):
         ptrs = [[o[q].data_ptr() for o in outs] for q in range(3)]
         for _ in range(2):
             for s in solvers:
-                s.resetLambda()
+                if net:
+                    net.warm_start(s)
+                else:
+                    s.resetLambda()
             st = qesb.solve_batch(solvers, ITERMAX, *ptrs)
         torch.cuda.synchronize()
     finally:
         for s in solvers:
             s.close()
+        if net:
+            net.close()
     print(json.dumps({"profile_batch": args.batch, "iterations": [x["iterations"] for x in st],
                       "pre_iterations": [x["pre_iterations"] for x in st]}))
 

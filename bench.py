@@ -781,8 +781,10 @@ def run_b200(args):
     torch.cuda.synchronize(dev)
     ms_e2e = max_over_ranks(p0.elapsed_time(p1) / k_e2e)
     last = (k_e2e - 1) % 2
-    e2e_ok = all(torch.equal(ho[0], o[0].cpu()) for ho, o in zip(set_host_out[last], set_outs[last]))
-    e2e_ok = e2e_ok and all(torch.equal(a[0], b[0]) for a, b in zip(set_outs[last], outs if last else outs2))
+    # the host copies are the device results, and both solver sets give the same winds
+    e2e_ok = all(torch.equal(ho[q], o[q].cpu()) for ho, o in zip(set_host_out[last], set_outs[last]) for q in range(3))
+    e2e_ok = e2e_ok and all(torch.equal(a[q], b[q]) for a, b in zip(set_outs[last], outs if last else outs2)
+                            for q in range(3))
     for s2 in solvers2:
         s2.close()
 

@@ -350,9 +350,10 @@ qesb_status qesb_umma_selftest(const uint16_t *A, const uint16_t *B, float *C, i
  * staged once per tile, the 27 taps as shifted descriptors into it); the
  * others the implicit GEMM (per-tap gather). Small grids (fewer than about two
  * 128-voxel tiles per SM) split the K chunks over more CTAs and add FP32
- * partial sums in a scratch buffer kept per (device, stream), allocated on the
- * first such call on a stream and grown as needed (a few MB for the network's
- * deep levels); the sum order then varies from run to run. */
+ * partial sums in a scratch buffer kept per (device, stream), one slice per
+ * split, allocated on the first such call on a stream and grown as needed (a
+ * few MB for the network's deep levels); the slices are added in a fixed
+ * order, so every call gives the same bits. */
 qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H, int W,
                         int sign, const void *Bm, int Kp, int N, void *y, void *yf, const float *bias,
                         int relu, const void *mask, int *err, void *stream);

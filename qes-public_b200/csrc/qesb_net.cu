@@ -157,7 +157,8 @@ struct ConvOut {
   const float *bias;      // [N] (nullable)
   int relu;               // ReLU in the epilogue
   const __nv_bfloat16 *mask;  // [V][N] (nullable): zero where mask <= 0 (gradient through a ReLU)
-  float *acc;             // split-K: [V][N] FP32 partial sums (atomic adds), epilogue left to k_conv_finish
+  float *acc;             // split-K: [split][V][N] FP32 partial sums, one slice per K split (plain
+                          // stores), summed in split order by k_conv_finish with the epilogue
 };
 
 // Y[v][n] = epilogue( sum_k A[v][k] * Bm[n][k] ), A the implicit im2col of
@@ -170,7 +171,8 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
                                                    int Kp, ConvOut out, int *err)
 {
   // split-K (gridDim.y > 1, small grids): CTA y sums the K chunks [jb, je)
-  // and adds its partial to out.acc; k_conv_finish applies the epilogue.
+  // and stores its partial in slice y of out.acc; k_conv_finish adds the
+  // slices in order and applies the epilogue (the same bits every run).
   constexpr uint32_t SA = 128 * 64 * 2, SB = N * 64 * 2, STAGE = SA + SB;
   constexpr uint32_t NCOLS = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
   extern __shared__ __align__(1024) uint8_t sm[];
@@ -252,15 +254,14 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
     umma::mma_drain(&mdrain, tid == 0, kWaitLimit);
   } else if (out.acc) {
     const long v = m0 + warp * 32 + lane;
-    if (nk > 0)
-      for (int c0 = 0; c0 < N; c0 += 8) {
-        float a[8];
-        umma::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, a);
-        if (v < g.V) {
+    for (int c0 = 0; c0 < N; c0 += 8) {
+      float a[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // an empty K range contributes zeros
+      if (nk > 0) umma::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, a);
+      if (v < g.V) {
 #pragma unroll
-          for (int q = 0; q < 8; ++q) atomicAdd(out.acc + v * N + c0 + q, a[q]);
-        }
+        for (int q = 0; q < 8; ++q) out.acc[((long)blockIdx.y * g.V + v) * N + c0 + q] = a[q];
       }
+    }
   } else {
     const long v = m0 + warp * 32 + lane;
     for (int c0 = 0; c0 < N; c0 += 8) {
@@ -563,11 +564,13 @@ __global__ void __launch_bounds__(128) k_conv_wgrad(ConvIn in, ConvGeom g, const
   }
 }
 
-// Epilogue of a split-K convolution: y = act(acc + bias), as k_conv_igemm's.
-__global__ void k_conv_finish(const float *__restrict__ acc, long V, int N, ConvOut out)
+// Epilogue of a split-K convolution: y = act(sum of the split slices in
+// order + bias), as k_conv_igemm's.
+__global__ void k_conv_finish(const float *__restrict__ acc, int split, long V, int N, ConvOut out)
 {
   for (long i = threadIdx.x + (long)blockIdx.x * blockDim.x; i < V * N; i += (long)gridDim.x * blockDim.x) {
     float a = acc[i];
+    for (int y = 1; y < split; ++y) a += acc[(long)y * V * N + i];
     if (out.bias) a += __ldg(out.bias + (int)(i % N));
     if (out.relu) a = fmaxf(a, 0.0f);
     if (out.mask && !(__bfloat162float(out.mask[i]) > 0.0f)) a = 0.0f;
@@ -625,17 +628,15 @@ qesb_status launch_conv(const ConvIn &in, const ConvGeom &g, int sign, const __n
   int split = 1;
   if (blocks < 296) split = std::max(1, std::min((int)(296 / blocks), nk / 4));
   ConvOut o = out;
-  if (split > 1) {
-    const size_t need = (size_t)g.V * N;
+  if (split > 1) {  // every slice element is written by exactly one CTA: no clearing
+    const size_t need = (size_t)split * g.V * N;
     const qesb_status st = acc_buffer(dev, s, need, &o.acc);
     if (st != QESB_OK) return st;
-    cudaError_t e = cudaMemsetAsync(o.acc, 0, need * sizeof(float), s);
-    if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv split-K clear: %s", cudaGetErrorString(e));
   }
   k_conv_igemm<N><<<dim3(blocks, split), 128, smem, s>>>(in, g, sign, Bm, Kp, o, err);
   if (split > 1) {
     const long total = g.V * N;
-    k_conv_finish<<<(unsigned)std::min<long>((total + 255) / 256, 148L * 16), 256, 0, s>>>(o.acc, g.V, N, out);
+    k_conv_finish<<<(unsigned)std::min<long>((total + 255) / 256, 148L * 16), 256, 0, s>>>(o.acc, split, g.V, N, out);
   }
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));

@@ -3,12 +3,17 @@
     python qes-public_b200/train_warmstart.py --out DIR [--train 2000] [--eval 200] [--epochs 3]
 
 Training data: seeded 128 x 128 x 64 synthetic cities (20-40 buildings,
-stretched z, power-law inflow); the target of each is the lambda this solver
-reaches after --target-iters red-black iterations from lambda = 0. Evaluation:
-held-out 256 x 256 x 64 cities (seeds disjoint from training), each solved to
-the benchmark's stopping rule (max|dlambda| <= 1e-3, FP64) from lambda = 0 and
-from the network's prediction; reports iterations, device ms (network
-included) and the largest wind difference between the two results.
+stretched z, power-law inflow); the target of each is the converged lambda
+(--target converged: an over-relaxed run of --target-iters red-black
+iterations, then 1000 at the reference's omega) or the lambda after
+--target-iters iterations from lambda = 0 (--target iters). Evaluation:
+held-out 256 x 256 x 64 cities (seeds 500000 + i, disjoint from training),
+each solved to the benchmark's stopping rule (the reference's tol 1e-9 and
+itermax 10000, plus the window rule: 32 iterations, 4e-3) in four arms: plain
+SOR from lambda = 0, the network's start, the over-relaxed pre-phase, the
+network's start then the pre-phase; reports each arm's iterations and device
+ms (network included), and its largest wind difference from the converged
+field. --eval-only WEIGHTS evaluates a trained network without training.
 Writes DIR/warmstart_city.qwn (weights, the library format qesb_warmnet_load reads) and
 DIR/warmstart_report.json.
 """
@@ -29,10 +34,24 @@ import qesb  # noqa: E402
 from qesb import warmstart as ws  # noqa: E402
 
 TRAIN_SEED0, EVAL_SEED0 = 1000, 500000
-TOL = 1e-3
+TOL, ITERMAX, WINDOW, WINDOW_TOL = 1e-9, 10000, 32, 4e-3
+PRE_OMEGA, PRE_TOL = 1.97, 2e-3
 
 
-def generate(net, n, workload, target_iters, threads=8):
+def converge(solver, w, omega, pre_iters, ref_iters=1000):
+    """lambda converged to the FP32 noise floor: pre_iters over-relaxed
+    red-black iterations, then ref_iters at the reference's omega, no stopping
+    rule (the handle's rule settings are restored)."""
+    solver.set_tolerance(-1.0)
+    solver.set_window_rule(0, 0.0)
+    solver.set_prephase(omega, -1.0, pre_iters)
+    solver.resetLambda()
+    solver.solve(w, ref_iters, set_inputs=False)
+    solver.set_prephase(0.0, 0.0, 0)
+    solver.set_tolerance(TOL)
+
+
+def generate(net, n, workload, target_iters, threads=8, target="converged"):
     """Compact inputs [n][V][5] (BF16) and targets [n][V] (FP32) on the device."""
     torch = net.torch
     pool = ThreadPoolExecutor(max_workers=threads)
@@ -67,8 +86,11 @@ def generate(net, n, workload, target_iters, threads=8):
                 Wf = torch.empty(f.V(0), dtype=torch.float32, device=net.dev)
             torch.cuda.synchronize()
         solver.set_inputs(w)
-        solver.resetLambda()
-        solver.solve(w, target_iters, set_inputs=False)
+        if target == "converged":
+            converge(solver, w, qesb.prephase_omega(f.W, f.H), target_iters)
+        else:
+            solver.resetLambda()
+            solver.solve(w, target_iters, set_inputs=False)
         net.input_from(solver, s, scale)
         if net.res == 1:
             qesb.check(qesb.lib().qesb_warm_target(solver._h, T[k].data_ptr(), weight.data_ptr(), scale.data_ptr()))
@@ -119,35 +141,58 @@ def train(net, X, T, weight, s, epochs, lr0, log_every=200, coarse=((8, 0.0),)):
     return losses, time.time() - t0
 
 
-def evaluate(net, n, workload, itermax=10000):
+def evaluate(net, n, workload):
+    """Four arms per held-out city under the benchmark's rule (see the module
+    docstring); ms are device time (CUDA events) of the start and the solve."""
     torch = net.torch
     rows = []
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     solver = None
     for k in range(n):
         w, _ = qesb.random_city(workload, EVAL_SEED0 + k)
         if solver is None:
             solver = qesb.Solver_B200(w.domain, TOL)
+            solver.set_inputs(w)
+            solver.autotune()
         solver.set_inputs(w)
-        solver.resetLambda()
-        torch.cuda.synchronize()
-        ev[0].record()
-        plain = solver.solve(w, itermax, set_inputs=False)
-        ev[1].record()
-        up = (w.u.copy(), w.v.copy(), w.w.copy())
-        solver.resetLambda()
-        torch.cuda.synchronize()
-        ev[2].record()
-        net.warm_start(solver)
-        warm = solver.solve(w, itermax, set_inputs=False)
-        ev[3].record()
-        torch.cuda.synchronize()
-        dw = max(float(np.abs(a - b).max()) for a, b in zip((w.u, w.v, w.w), up))
-        rows.append({"seed": EVAL_SEED0 + k, "plain_iters": plain["iterations"], "warm_iters": warm["iterations"],
-                     "plain_ms": ev[0].elapsed_time(ev[1]), "warm_ms": ev[2].elapsed_time(ev[3]),
-                     "max_dwind": dw})
+        converge(solver, w, 1.97, 8000, 3000)
+        uc = (w.u.copy(), w.v.copy(), w.w.copy())
+        solver.set_window_rule(WINDOW, WINDOW_TOL)
+        row = {"seed": EVAL_SEED0 + k}
+        for arm, (use_net, use_pre) in {"plain": (0, 0), "network": (1, 0), "prephase": (0, 1),
+                                        "network+prephase": (1, 1)}.items():
+            solver.set_prephase(PRE_OMEGA if use_pre else 0.0, PRE_TOL, ITERMAX)
+            solver.resetLambda()
+            torch.cuda.synchronize()
+            ev[0].record(torch.cuda.ExternalStream(solver.stream_ptr()))
+            if use_net:
+                net.warm_start(solver)
+            st = solver.solve(w, ITERMAX, set_inputs=False)
+            ev[1].record(torch.cuda.ExternalStream(solver.stream_ptr()))
+            torch.cuda.synchronize()
+            row[arm] = {"iterations": st["iterations"], "pre_iterations": st["pre_iterations"],
+                        "ms": ev[0].elapsed_time(ev[1]), "stop": st["converged"],
+                        "wind_err_vs_converged": max(float(np.abs(a - b).max()) for a, b in zip((w.u, w.v, w.w), uc))}
+        rows.append(row)
+        if k % 20 == 0:
+            print(f"  evaluated {k + 1}/{n}: {row}", flush=True)
     solver.close()
     return rows
+
+
+def summary(rows):
+    out = {}
+    for arm in ("plain", "network", "prephase", "network+prephase"):
+        its = np.array([r[arm]["iterations"] + r[arm]["pre_iterations"] for r in rows], float)
+        ms = np.array([r[arm]["ms"] for r in rows], float)
+        out[arm] = {"iterations_mean": float(its.mean()), "ms_mean": float(ms.mean()),
+                    "wind_err_max": max(r[arm]["wind_err_vs_converged"] for r in rows),
+                    "all_stopped_by_rule": all(r[arm]["stop"] == 2 for r in rows)}
+    p, pp = out["plain"]["ms_mean"], out["prephase"]["ms_mean"]
+    for arm in out:
+        out[arm]["speedup_vs_plain"] = p / out[arm]["ms_mean"]
+        out[arm]["speedup_vs_prephase"] = pp / out[arm]["ms_mean"]
+    return out
 
 
 def main():
@@ -155,8 +200,10 @@ def main():
     ap.add_argument("--out", required=True)
     ap.add_argument("--train", type=int, default=2000)
     ap.add_argument("--eval", type=int, default=200)
+    ap.add_argument("--eval-only", default=None, help="evaluate this weights file, no training")
     ap.add_argument("--epochs", type=int, default=3)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--target", default="converged", choices=["converged", "iters"])
     ap.add_argument("--target-iters", type=int, default=4000)
     ap.add_argument("--train-workload", default="city128")
     ap.add_argument("--eval-workload", default="city256")
@@ -167,34 +214,29 @@ def main():
                     help="weight of the 8x8x8-block error term of the loss (0: plain MSE)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
-    channels = tuple(min(128, 16 << l) for l in range(args.levels))
-    net = ws.WarmStartNet(device=0, seed=args.seed, channels=channels, res=args.res)
-    t0 = time.time()
-    X, T, weight, s = generate(net, args.train, args.train_workload, args.target_iters)
-    t_gen = time.time() - t0
-    losses, t_train = train(net, X, T, weight, s, args.epochs, args.lr, coarse=((8, args.coarse_beta),))
-    del X, T
-    wpath = os.path.join(args.out, "warmstart_city.qwn")
-    net.save(wpath)
+    report = {}
+    if args.eval_only:
+        net = ws.WarmStartNet.from_file(args.eval_only, device=0)
+        report["weights"] = os.path.basename(args.eval_only)
+    else:
+        channels = tuple(min(128, 16 << l) for l in range(args.levels))
+        net = ws.WarmStartNet(device=0, seed=args.seed, channels=channels, res=args.res)
+        t0 = time.time()
+        X, T, weight, s = generate(net, args.train, args.train_workload, args.target_iters, target=args.target)
+        t_gen = time.time() - t0
+        losses, t_train = train(net, X, T, weight, s, args.epochs, args.lr, coarse=((8, args.coarse_beta),))
+        del X, T
+        net.save(os.path.join(args.out, "warmstart_city.qwn"))
+        report["train"] = {"n": args.train, "workload": args.train_workload, "epochs": args.epochs,
+                           "target": args.target, "target_iters": args.target_iters, "res": args.res,
+                           "coarse_beta": args.coarse_beta, "generate_s": t_gen, "train_s": t_train,
+                           "losses": losses}
     rows = evaluate(net, args.eval, args.eval_workload)
-    it_p = np.array([r["plain_iters"] for r in rows], float)
-    it_w = np.array([r["warm_iters"] for r in rows], float)
-    ms_p = np.array([r["plain_ms"] for r in rows], float)
-    ms_w = np.array([r["warm_ms"] for r in rows], float)
-    report = {
-        "train": {"n": args.train, "workload": args.train_workload, "epochs": args.epochs, "target_iters":
-                  args.target_iters, "coarse_beta": args.coarse_beta, "generate_s": t_gen, "train_s": t_train,
-                  "losses": losses},
-        "eval": {"n": args.eval, "workload": args.eval_workload, "tol": TOL,
-                 "plain_iters_mean": it_p.mean(), "warm_iters_mean": it_w.mean(),
-                 "iters_ratio_mean": float((it_p / it_w).mean()),
-                 "plain_ms_mean": ms_p.mean(), "warm_ms_mean": ms_w.mean(),
-                 "ms_ratio_mean": float((ms_p / ms_w).mean()),
-                 "max_dwind": max(r["max_dwind"] for r in rows), "rows": rows},
-    }
+    report["eval"] = {"n": args.eval, "workload": args.eval_workload, "seeds": [EVAL_SEED0, EVAL_SEED0 + args.eval - 1],
+                      "rule": {"tol": TOL, "itermax": ITERMAX, "window": WINDOW, "window_tol": WINDOW_TOL},
+                      "prephase": {"omega": PRE_OMEGA, "tol": PRE_TOL}, "summary": summary(rows), "rows": rows}
     json.dump(report, open(os.path.join(args.out, "warmstart_report.json"), "w"), indent=1)
-    e = report["eval"]
-    print(json.dumps({k: v for k, v in e.items() if k != "rows"}))
+    print(json.dumps(report["eval"]["summary"]))
 
 
 if __name__ == "__main__":

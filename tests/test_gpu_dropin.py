@@ -90,7 +90,7 @@ def test_dropin_type_5_through_the_reference_factory(tmp_path, calls):
 def test_dropin_learned_warm_start_from_cpp(tmp_path):
     """Solver_B200::useLearnedStart through the reference factory: the C++
     caller's solves from lambda = 0 start from the network (qesb_warm_start).
-    The result matches the same warm-started solve run from Python."""
+    The result is the same warm-started solve run from Python, bit for bit."""
     from qesb import warmstart as ws
 
     nx, ny, nz, itermax = 64, 48, 32, 120
@@ -111,7 +111,6 @@ def test_dropin_learned_warm_start_from_cpp(tmp_path):
         net.warm_start(s)
         s.solve(w, itermax, set_inputs=False)
         lam_py = s.lambda_
+    np.testing.assert_array_equal(lam, lam_py)
     cold, *_ = O.sor(d, w, O.divergence(d, w), 1e-9, itermax)
-    scale = np.abs(lam_py).max()
-    assert np.abs(lam - lam_py).max() <= 1e-2 * scale
-    assert np.abs(lam - cold).max() > 10 * np.abs(lam - lam_py).max()  # the start was the network's
+    assert np.abs(lam - cold).max() > 0  # the start was the network's

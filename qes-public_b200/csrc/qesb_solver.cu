@@ -21,6 +21,7 @@
 // halo beyond the domain edge without bounds checks. Inputs and outputs in
 // the reference layouts (cells i + j*X + k*X*Y, faces i + j*nx + k*nx*ny)
 // stay as the caller gave them.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -701,6 +702,11 @@ struct qesb_handle {
   double win_tol = 0.0;
   float *d_snap = nullptr;  // lambda at the start of the current window (split or padded layout)
 
+  // tensor maps of the split arrays for the TMA z-march shapes, encoded for tiles of tm_rows rows
+  TmaDesc *d_tmaps = nullptr;
+  TmaDesc h_tmaps[kTmCount] = {};
+  int tm_rows = 0;
+
   // sweep kernels: this solve as a one-domain list
   SweepList list;
   SweepCtl *h_ctl = nullptr;  // pinned
@@ -990,6 +996,7 @@ struct SweepVariant {
   void (*black)(SweepArgs);
   void (*red_m)(SweepArgs);  // domain lists
   void (*black_m)(SweepArgs);
+  int tma = 0;  // z-march shapes staged by tensor-map copies: the domains need their tensor maps
 };
 // MINB: resident CTAs per SM the compiler must allow (caps registers per
 // thread); the default allows 512 threads per SM (at most 128 registers)
@@ -1032,18 +1039,19 @@ constexpr SweepVariant make_bulk(const char *name)
                       k_sor_bulk<0, W, NS, ASYNC, true>,
                       k_sor_bulk<1, W, NS, ASYNC, true>};
 }
-template <int TY, int RW, int MINB, int DIST = 2>
+template <int TY, int RW, int MINB, int DIST = 2, int TMA = 0>
 constexpr SweepVariant make_zm(const char *name)
 {
   return SweepVariant{name,
                       kUnitTile,
                       TY,
                       TY * RW,
-                      zm_smem_bytes<TY * RW, DIST>(),
-                      k_sor_zm<0, TY, RW, DIST, false, MINB>,
-                      k_sor_zm<1, TY, RW, DIST, false, MINB>,
-                      k_sor_zm<0, TY, RW, DIST, true, MINB>,
-                      k_sor_zm<1, TY, RW, DIST, true, MINB>};
+                      zm_smem_bytes<TY * RW, DIST, TMA>(),
+                      k_sor_zm<0, TY, RW, DIST, false, MINB, TMA>,
+                      k_sor_zm<1, TY, RW, DIST, false, MINB, TMA>,
+                      k_sor_zm<0, TY, RW, DIST, true, MINB, TMA>,
+                      k_sor_zm<1, TY, RW, DIST, true, MINB, TMA>,
+                      TMA};
 }
 const SweepVariant kSweepVariants[] = {
     // streaming split kernels (option "variant" 5..17)
@@ -1072,6 +1080,8 @@ const SweepVariant kSweepVariants[] = {
     make_zm<8, 2, 2>("zm_y8x2_b2"),
     // copies one plane ahead: smaller rings, more CTAs per SM (48..50)
     make_zm<4, 2, 5, 1>("zm_y4x2_d1_b5"), make_zm<4, 2, 4, 1>("zm_y4x2_d1_b4"), make_zm<2, 2, 8, 1>("zm_y2x2_d1_b8"),
+    // the same staged by tensor-map copies issued from one thread (51..53)
+    make_zm<4, 2, 5, 1, 1>("zmt_y4x2_b5"), make_zm<4, 2, 4, 1, 1>("zmt_y4x2_b4"), make_zm<2, 2, 8, 1, 1>("zmt_y2x2_b8"),
 };
 constexpr int kNumSweep = sizeof(kSweepVariants) / sizeof(kSweepVariants[0]);
 constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the first sweep shape
@@ -1121,6 +1131,76 @@ void sweep_tiles(std::vector<SweepDomain> &doms, const SweepVariant &sv, bool mu
     }
   }
   for (SweepDomain &d : doms) d.kc = best;
+}
+
+// cuTensorMapEncodeTiled, from the driver through the runtime (no libcuda link).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+qesb_status encode_tiled_fn(EncodeTiledFn *out)
+{
+  static EncodeTiledFn fn = nullptr;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess || !p ||
+        q != cudaDriverEntryPointSuccess)
+      return qesb_fail(QESB_ERR_CUDA, "cuTensorMapEncodeTiled not available");
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  *out = fn;
+  return QESB_OK;
+}
+
+// The handle's split arrays as 4-D tensors (q, j, k, colour) with the boxes
+// the TMA z-march shapes copy for tiles of `rows` rows: the other colour's
+// slab 136 x (rows + 2), the own colour's lambda and R 128 x rows (floats),
+// the mask 128 x rows (bytes). Out-of-range elements read as zeros.
+qesb_status ensure_tmaps(qesb_handle *h, int rows)
+{
+  if (h->d_tmaps && h->tm_rows == rows) return QESB_OK;
+  EncodeTiledFn enc = nullptr;
+  CKS(encode_tiled_fn(&enc));
+  if (!h->d_tmaps) CKS(dalloc(&h->d_tmaps, kTmCount));
+  const cuuint64_t dims[4] = {(cuuint64_t)h->S.PQ, (cuuint64_t)h->G.Y, (cuuint64_t)h->G.Z, 2};
+  const cuuint64_t fstr[3] = {(cuuint64_t)h->S.PQ * 4, (cuuint64_t)h->S.PQ * h->G.Y * 4, (cuuint64_t)h->S.CS * 4};
+  const cuuint64_t bstr[3] = {(cuuint64_t)h->S.PQ, (cuuint64_t)h->S.PQ * h->G.Y, (cuuint64_t)h->S.CS};
+  const cuuint32_t one[4] = {1, 1, 1, 1};
+  const cuuint32_t box_oth[4] = {(cuuint32_t)kZmOW, (cuuint32_t)rows + 2, 1, 1};
+  const cuuint32_t box_own[4] = {(cuuint32_t)kZmQ, (cuuint32_t)rows, 1, 1};
+  struct M {
+    CUtensorMapDataType t;
+    void *base;
+    const cuuint64_t *str;
+    const cuuint32_t *box;
+  } maps[kTmCount] = {{CU_TENSOR_MAP_DATA_TYPE_FLOAT32, h->d_lam_s, fstr, box_oth},
+                      {CU_TENSOR_MAP_DATA_TYPE_FLOAT32, h->d_lam_s, fstr, box_own},
+                      {CU_TENSOR_MAP_DATA_TYPE_FLOAT32, h->d_R_s, fstr, box_own},
+                      {CU_TENSOR_MAP_DATA_TYPE_UINT8, h->d_mask_s, bstr, box_own}};
+  static_assert(sizeof(CUtensorMap) == sizeof(TmaDesc), "tensor map size");
+  for (int q = 0; q < kTmCount; ++q) {
+    CUtensorMap m;
+    const CUresult r = enc(&m, maps[q].t, 4, maps[q].base, dims, maps[q].str, maps[q].box, one,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return qesb_fail(QESB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d) for map %d", (int)r, q);
+    std::memcpy(&h->h_tmaps[q], &m, sizeof m);
+  }
+  CK(cudaMemcpyAsync(h->d_tmaps, h->h_tmaps, sizeof h->h_tmaps, cudaMemcpyHostToDevice, h->stream));
+  h->tm_rows = rows;
+  return QESB_OK;
+}
+
+// The domain's tensor maps for a TMA shape (no-op for the others).
+qesb_status attach_tmaps(qesb_handle *h, const SweepVariant &sv, SweepDomain &d)
+{
+  if (!sv.tma) return QESB_OK;
+  CKS(ensure_tmaps(h, sv.tile_rows));
+  d.tm = h->d_tmaps;
+  return QESB_OK;
 }
 
 SweepDomain sweep_domain(qesb_handle *h, int itermax, double tol)
@@ -1265,6 +1345,7 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
     // history are then cleared for the reference loop
     std::vector<SweepDomain> pre(1);
     CKS(sweep_domain_pre(h, pre[0], s));
+    CKS(attach_tmaps(h, sv, pre[0]));
     sweep_tiles(pre, sv, false, h->device);
     CKS(h->list.upload(pre, sv.unit, s));
     SweepArgs a = h->list.a;
@@ -1281,6 +1362,7 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
   }
   CK(cudaEventRecord(h->evs[1], s));
   std::vector<SweepDomain> one{sweep_domain(h, itermax, (double)h->tol)};
+  CKS(attach_tmaps(h, sv, one[0]));
   sweep_tiles(one, sv, false, h->device);
   CKS(h->list.upload(one, sv.unit, s));
   SweepArgs a = h->list.a;
@@ -1421,7 +1503,7 @@ void free_all(qesb_handle *h)
                   h->d_own_in[2], h->d_own_in[3], h->d_own_in[4], h->d_own_in[5], h->d_own_flag,
                   h->d_own_u0, h->d_own_v0, h->d_own_w0, h->d_dz, h->d_vmax, h->d_inv, h->d_val,
                   h->d_inv_pre, h->d_bad, h->d_err, h->d_state, h->d_u, h->d_v, h->d_w, h->d_wbits,
-                  h->d_wcut, h->d_snap};
+                  h->d_wcut, h->d_snap, h->d_tmaps};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   h->list.destroy();
@@ -1818,6 +1900,7 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
     cudaStream_t s = h->stream;
     CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
     std::vector<SweepDomain> one{sweep_domain(h, 1 << 30, -1.0)};  // tol < 0: every launch runs
+    CKS(attach_tmaps(h, sv, one[0]));
     sweep_tiles(one, sv, false, h->device);
     CKS(h->list.upload(one, sv.unit, s));
     const dim3 grid(sweep_ctas(sv, false, h->device)), block(32, sv.block_y);
@@ -1961,6 +2044,7 @@ qesb_status qesb_autotune_batch(qesb_handle *const *hs, int n, int *best, float 
             cudaMemsetAsync(hs[i]->d_state, 0, sizeof(SolveState), s) != cudaSuccess)
           qs = qesb_fail(QESB_ERR_CUDA, "qesb_autotune_batch: memset");
         doms[i] = sweep_domain(hs[i], 1 << 30, -1.0);  // tol < 0: every launch runs
+        if (qs == QESB_OK) qs = attach_tmaps(hs[i], sv, doms[i]);
       }
       if (qs != QESB_OK) break;
       sweep_tiles(doms, sv, true, h0->device);
@@ -2038,6 +2122,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     if (pre_on) {
       SweepDomain p;
       CKS(sweep_domain_pre(h, p, s));
+      CKS(attach_tmaps(h, sv, p));
       pre.push_back(p);
       pre_of.push_back(i);
     }
@@ -2046,6 +2131,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_R, h->d_R_s);
     CK(cudaGetLastError());
     doms[i] = sweep_domain(h, itermax, (double)h->tol);
+    CKS(attach_tmaps(h, sv, doms[i]));
     cells += (double)G.XY * G.Z;
   }
   SweepList list;

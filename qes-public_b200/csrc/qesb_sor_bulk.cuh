@@ -82,23 +82,6 @@ __device__ __forceinline__ void warp_g2s(unsigned char *dst, const void *src, in
   for (int o = lane * 16; o < bytes; o += 512) lane_g2s16(dst + o, p + o);
 }
 
-// Stage wait of the bulk kernels: a non-blocking test first, then up to
-// limit - 1 potentially suspending polls. With limit 1 the wait therefore
-// gives up unless the stage's copies have already landed (the timeout path
-// is reachable on demand, on correct data).
-__device__ __forceinline__ bool stage_wait(uint64_t *mbar, uint32_t parity, uint32_t limit)
-{
-  uint32_t done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(done)
-      : "r"(umma::smem_u32(mbar)), "r"(parity)
-      : "memory");
-  return done || (limit > 1 && umma::mbar_wait(mbar, parity, limit - 1));
-}
-
 template <int W, int NS>
 constexpr size_t bulk_smem_bytes()
 {
@@ -245,7 +228,7 @@ __global__ void __launch_bounds__(32 * W) k_sor_bulk(BulkArgs b)
     if (ASYNC) {
       lane_wait<NS - 1>();  // this lane's copies of unit t have landed
       __syncwarp();         // and every other lane's
-    } else if (!stage_wait(&bar[s], (uint32_t)((t / NS) & 1), b.wait_limit ? b.wait_limit : kStageWaitLimit)) {
+    } else if (!umma::mbar_wait_bounded(&bar[s], (uint32_t)((t / NS) & 1), b.wait_limit ? b.wait_limit : kStageWaitLimit)) {
       if (lane == 0) atomicExch(&b.ctl->fault, 1);
       // let every copy still in flight, this unit's included, land before the
       // CTA's shared memory goes away (bounded by the default limit)

@@ -42,6 +42,7 @@ struct SplitDom {
   float *L = nullptr;
   const float *R = nullptr, *val = nullptr, *inv_all = nullptr;
   const uint8_t *mask = nullptr;
+  const TmaDesc *tm = nullptr;
   double *err = nullptr;
   int it = 0;
   int kcur = -1;
@@ -61,6 +62,7 @@ struct SplitDom {
     L = D.lam;
     R = D.R;
     mask = D.mask;
+    tm = D.tm;
     val = D.val;
     inv_all = D.inv;
     err = D.err;

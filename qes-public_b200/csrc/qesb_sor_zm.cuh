@@ -14,6 +14,15 @@
 // shared memory: each byte of the other colour leaves L2 about once per tile
 // (plus the halos), against five times in the row kernels.
 //
+// TMA = 1 stages the same data with tensor-map bulk copies instead: one
+// thread per CTA issues, per plane, the other colour's slab (a box of
+// 136 x (rows + 2) floats at (q0 - 4, j0 - 1)), the own colour's lambda, R
+// and mask rows (boxes of 128 x rows) and the plane's inv row (a 256-byte
+// bulk copy), completing on one mbarrier per ring slot; out-of-range box
+// elements arrive as zeros, as the zero-filled cp.async copies leave them.
+// The waits are bounded (SweepArgs::wait_limit): a CTA that gives up lets its
+// copies in flight land, sets the list's fault flag and stops.
+//
 // The arithmetic is the row kernels' (Solver_CPU_RB.cpp:118-125, with the
 // same operation order), so the results are bit-identical; the black kernel
 // applies the ground mirror (Solver_CPU_RB.cpp:155-162) on plane 1 and its
@@ -36,12 +45,23 @@ constexpr int kZmOW = kZmQ + 8;      // staged other-colour row: q0 - 4 .. q0 + 
 __host__ __device__ constexpr int zm_other_slots(int dist) { return dist + 3; }
 __host__ __device__ constexpr int zm_own_slots(int dist) { return dist + 1; }
 
-template <int TR, int DIST>
+// Floats per other-colour slot: the staged slab, rounded up to 128 bytes for
+// the TMA shapes (a tensor copy's shared-memory destination is 128-byte aligned).
+template <int TR, int TMA>
+__host__ __device__ constexpr int zm_oslot_floats()
+{
+  return TMA ? ((TR + 2) * kZmOW * 4 + 127) / 128 * 32 : (TR + 2) * kZmOW;
+}
+
+template <int TR, int DIST, int TMA = 0>
 constexpr size_t zm_smem_bytes()
 {
-  return sizeof(float) * zm_other_slots(DIST) * (TR + 2) * kZmOW +
-         zm_own_slots(DIST) * TR * kZmQ * (2 * sizeof(float) + 1) + sizeof(float) * zm_own_slots(DIST) * 64;
+  return sizeof(float) * zm_other_slots(DIST) * zm_oslot_floats<TR, TMA>() +
+         zm_own_slots(DIST) * TR * kZmQ * (2 * sizeof(float) + 1) + sizeof(float) * zm_own_slots(DIST) * 64 +
+         (TMA ? 8 * zm_own_slots(DIST) : 0);
 }
+
+__host__ __device__ constexpr int zm_wrap_n(int x, int n) { return x >= n ? x - n : x; }
 
 // 16-byte asynchronous copy global -> shared; src_bytes = 0 fills zeros and
 // reads nothing.
@@ -58,20 +78,70 @@ __device__ __forceinline__ void zm_wait0() { asm volatile("cp.async.wait_group 0
 
 template <int TY>
 struct ZmSmem {
-  float *oth;     // [other slots][TY + 2][kZmOW]
+  float *oth;     // [other slots][ostride]: TY + 2 rows of kZmOW
   float *own;     // [own slots][TY][kZmQ]
   float *rr;      // [own slots][TY][kZmQ]
   uint8_t *mask;  // [own slots][TY][kZmQ]
   float *inv;     // [own slots][64]: omega / (sum of the open faces' coefficients) per wall mask
-  __device__ ZmSmem(unsigned char *base, int nso, int nsw)
+  uint64_t *bar;  // TMA shapes: [own slots] mbarriers, one per pipeline step in flight
+  __device__ ZmSmem(unsigned char *base, int nso, int nsw, int ostride)
   {
     oth = reinterpret_cast<float *>(base);
-    own = oth + nso * (TY + 2) * kZmOW;
+    own = oth + nso * ostride;
     rr = own + nsw * TY * kZmQ;
     mask = reinterpret_cast<uint8_t *>(rr + nsw * TY * kZmQ);
     inv = reinterpret_cast<float *>(mask + nsw * TY * kZmQ);
+    bar = reinterpret_cast<uint64_t *>(inv + nsw * 64);
   }
 };
+
+// 4-D tiled tensor copy global -> shared, completing on an mbarrier (no
+// multicast: this GPU's own memory only).
+__device__ __forceinline__ void zm_tma4(void *dst, const TmaDesc *map, int c0, int c1, int c2, int c3,
+                                        uint64_t *mbar)
+{
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(umma::smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(umma::smem_u32(mbar))
+      : "memory");
+}
+__device__ __forceinline__ void zm_expect_tx(uint64_t *mbar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(umma::smem_u32(mbar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void zm_bulk(void *dst, const void *src, uint32_t bytes, uint64_t *mbar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   umma::smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(umma::smem_u32(mbar))
+               : "memory");
+}
+
+// The TMA shapes' pipeline step for plane p of a tile (one thread): the own
+// colour's lambda, R and mask rows of plane p into own slot `wslot`, the
+// other colour's slab of plane p + 1 into other slot `oslot` and, for the
+// tile's first plane (first = true), also planes p - 1 and p into the two
+// slots before it; the plane's inv row. All on the mbarrier `bar`.
+template <int COLOUR, int TR, int OSTR, int NSO>
+__device__ __forceinline__ void zm_tma_step(const ZmSmem<TR> &sm, const SplitDom &D, int q0, int j0, int p,
+                                            bool first, int oslot, int wslot, uint64_t *bar)
+{
+  constexpr uint32_t ob = (TR + 2) * kZmOW * 4, wb = TR * kZmQ * 4;
+  umma::fence_smem_async();  // the slots' last readers (generic proxy) are done: the barrier before this
+  zm_expect_tx(bar, ob * (first ? 3u : 1u) + 2u * wb + TR * kZmQ + 256u);
+  const int oc = 1 - COLOUR;
+  if (first) {
+    zm_tma4(sm.oth + zm_wrap_n(oslot + NSO - 2, NSO) * OSTR, D.tm + kTmOther, q0 - 4, j0 - 1, p - 1, oc, bar);
+    zm_tma4(sm.oth + zm_wrap_n(oslot + NSO - 1, NSO) * OSTR, D.tm + kTmOther, q0 - 4, j0 - 1, p, oc, bar);
+  }
+  zm_tma4(sm.oth + oslot * OSTR, D.tm + kTmOther, q0 - 4, j0 - 1, p + 1, oc, bar);
+  zm_tma4(sm.own + wslot * TR * kZmQ, D.tm + kTmOwn, q0, j0, p, COLOUR, bar);
+  zm_tma4(sm.rr + wslot * TR * kZmQ, D.tm + kTmR, q0, j0, p, COLOUR, bar);
+  zm_tma4(sm.mask + wslot * TR * kZmQ, D.tm + kTmMask, q0, j0, p, COLOUR, bar);
+  zm_bulk(sm.inv + wslot * 64, D.inv_all + (long)p * 64, 256u, bar);
+}
 
 // A thread's share of a tile's staging, fixed for the tile: shared-memory
 // offsets within a slot and global offsets within a colour plane (valid ones
@@ -171,16 +241,30 @@ __device__ __forceinline__ int zm_wrap(int x) { return x >= N ? x - N : x; }
 
 // TY warps per CTA, RW rows per warp (rows w, w + TY, ...): tiles of TY x RW rows;
 // copies DIST planes ahead.
-template <int COLOUR, int TY, int RW, int DIST, bool MULTI, int MINB>
+template <int COLOUR, int TY, int RW, int DIST, bool MULTI, int MINB, int TMA = 0>
 __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
 {
   constexpr int TR = TY * RW, NT = 32 * TY, NSO = zm_other_slots(DIST), NSW = zm_own_slots(DIST);
+  constexpr int OSTR = zm_oslot_floats<TR, TMA>();
   static_assert(DIST == 1 || DIST == 2, "copies run one or two planes ahead");
+  static_assert(!TMA || DIST == 1, "the TMA shapes copy one plane ahead");
   const int na = b.ctl->nactive;
   if (na <= 0) return;
-  extern __shared__ __align__(16) unsigned char zm_raw[];
-  const ZmSmem<TR> sm(zm_raw, NSO, NSW);
+  extern __shared__ __align__(128) unsigned char zm_raw[];
+  const ZmSmem<TR> sm(zm_raw, NSO, NSW, OSTR);
   const int lane = threadIdx.x, w = threadIdx.y, tid = lane + 32 * w;
+  [[maybe_unused]] const uint32_t wlim = b.wait_limit ? b.wait_limit : kStageWaitLimit;
+  [[maybe_unused]] unsigned nst = 0, nwt = 0;  // TMA pipeline steps issued / waited by this CTA
+  [[maybe_unused]] bool tma_bad = false;       // TMA shapes: slots not 128-byte aligned
+  if constexpr (TMA) {
+    if (tid == 0) {
+#pragma unroll
+      for (int s2 = 0; s2 < NSW; ++s2) umma::mbar_init(&sm.bar[s2], 1);
+      umma::fence_mbar_init();
+    }
+    tma_bad = (umma::smem_u32(zm_raw) & 127u) != 0;
+    __syncthreads();
+  }
   const int total = MULTI ? b.uoff[na] : sweep_units(b.one, kUnitTile);
   SplitDom D;
   int slot = -1, lo = 0, hi = 0;
@@ -198,6 +282,12 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
       hi = b.uoff[slot + 1];
       D.load(sweep_dom<MULTI>(b, slot));
     }
+    if constexpr (TMA) {
+      if (tma_bad || D.tm == nullptr) {  // no tensor maps for this domain: stop with the fault flag set
+        if (tid == 0) atomicExch(&b.ctl->fault, 1);
+        break;
+      }
+    }
     const SweepDomain &SD = sweep_dom<MULTI>(b, slot);
     const int njt = (D.Y - 2 + TR - 1) / TR, kc = SD.kc;
     const int nch = SD.nch;
@@ -210,7 +300,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
     const int q = q0 + 4 * lane;
     const int qn = (D.X + 1) >> 1;
     ZmCopies<TR, NT> cp;
-    cp.init(D, j0, q0, tid);
+    if constexpr (!TMA) cp.init(D, j0, q0, tid);
     // the lane's updated cells for rows of each x parity: q + t in [qlo, qhi],
     // qlo = 1 - I0, qhi = (X - 2 - I0) / 2
     unsigned up0 = 0, up1 = 0, upb0 = 0, upb1 = 0;  // bit / byte t: cell q + t
@@ -228,19 +318,42 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
     // sits in slot s mod NSO, the own colour's plane k0 + s in slot s mod NSW.
     // Prologue: other planes k0 - 1, k0 (and k0 + 1 with own k0) as one
     // group, then the steps of planes k0 + 1 .. k0 + DIST - 1.
-    zm_stage_other<COLOUR, TR, NT>(sm, cp, D, k0 - 1, 0);
-    zm_stage_other<COLOUR, TR, NT>(sm, cp, D, k0, 1);
+    if constexpr (TMA) {
+      if (tid == 0) zm_tma_step<COLOUR, TR, OSTR, NSO>(sm, D, q0, j0, k0, true, 2, 0, &sm.bar[nst % NSW]);
+      ++nst;
+    } else {
+      zm_stage_other<COLOUR, TR, NT>(sm, cp, D, k0 - 1, 0);
+      zm_stage_other<COLOUR, TR, NT>(sm, cp, D, k0, 1);
 #pragma unroll
-    for (int d = 0; d < DIST; ++d) zm_stage<COLOUR, TR, NT>(sm, cp, D, k0 + d, k1, 2 + d, d);
+      for (int d = 0; d < DIST; ++d) zm_stage<COLOUR, TR, NT>(sm, cp, D, k0 + d, k1, 2 + d, d);
+    }
     int om1 = 0, wk = 0;  // slots of the other colour's plane k - 1 and the own colour's plane k
     // the plane's six face coefficients, loaded one plane ahead
     float lv[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) lv[f] = __ldg(D.val + f * D.Z + k0);
     for (int k = k0; k < k1; ++k, om1 = zm_wrap<NSO>(om1 + 1), wk = zm_wrap<NSW>(wk + 1)) {
-      zm_wait<DIST - 1>();  // this thread's copies of plane k's step have landed
-      __syncthreads();      // everyone's; and every warp is done with plane k - 1
-      zm_stage<COLOUR, TR, NT>(sm, cp, D, k + DIST, k1, zm_wrap<NSO>(om1 + DIST + 2), zm_wrap<NSW>(wk + DIST));
+      if constexpr (TMA) {
+        // plane k's step has landed (bounded wait), and every warp is done with plane k - 1
+        const bool ok = umma::mbar_wait_bounded(&sm.bar[nwt % NSW], (nwt / NSW) & 1u, wlim);
+        ++nwt;
+        if (__syncthreads_or(!ok)) {
+          // let every copy of this CTA still in flight land, then stop
+          for (unsigned n = nwt - 1; n < nst; ++n) umma::mbar_wait(&sm.bar[n % NSW], (n / NSW) & 1u, kStageWaitLimit);
+          if (tid == 0) atomicExch(&b.ctl->fault, 1);
+          goto tiles_done;
+        }
+        if (k + 1 < k1) {
+          if (tid == 0)
+            zm_tma_step<COLOUR, TR, OSTR, NSO>(sm, D, q0, j0, k + 1, false, zm_wrap<NSO>(om1 + 3),
+                                               zm_wrap<NSW>(wk + 1), &sm.bar[nst % NSW]);
+          ++nst;
+        }
+      } else {
+        zm_wait<DIST - 1>();  // this thread's copies of plane k's step have landed
+        __syncthreads();      // everyone's; and every warp is done with plane k - 1
+        zm_stage<COLOUR, TR, NT>(sm, cp, D, k + DIST, k1, zm_wrap<NSO>(om1 + DIST + 2), zm_wrap<NSW>(wk + DIST));
+      }
       D.ve = lv[0];
       D.vf = lv[1];
       D.vg = lv[2];
@@ -253,9 +366,9 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
 #pragma unroll
         for (int f = 0; f < 6; ++f) lv[f] = __ldg(D.val + f * D.Z + k + 1);
       }
-      const float *om = sm.oth + om1 * (TR + 2) * kZmOW;
-      const float *ok = sm.oth + zm_wrap<NSO>(om1 + 1) * (TR + 2) * kZmOW;
-      const float *op = sm.oth + zm_wrap<NSO>(om1 + 2) * (TR + 2) * kZmOW;
+      const float *om = sm.oth + om1 * OSTR;
+      const float *ok = sm.oth + zm_wrap<NSO>(om1 + 1) * OSTR;
+      const float *op = sm.oth + zm_wrap<NSO>(om1 + 2) * OSTR;
       const int c = 4 + 4 * lane;  // column of q in a staged other-colour row
       // One row: I0 = (COLOUR + j + k) & 1, the x parity of the row's cells
       // (cell q is i = 2q + I0), known at compile time in each branch.
@@ -349,9 +462,10 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
         else row(wr, j, std::integral_constant<int, 0>{});
       }
     }
-    zm_wait0();
+    if constexpr (!TMA) zm_wait0();
     __syncthreads();  // the ring is reused by the next tile
   }
+tiles_done:
   sweep_flush_end<MULTI>(D.dmax, MULTI ? (D.err ? D.err + D.it : nullptr) : b.one.err + b.one.st->it);
   if (COLOUR == 1) sweep_finish_black<kUnitTile, MULTI>(b, na);
 }

@@ -10,6 +10,16 @@
 
 namespace qesb {
 
+// A tensor map (CUtensorMap: 128 bytes, 64-byte aligned) as the TMA copies
+// read it from global memory.
+struct alignas(64) TmaDesc {
+  unsigned long long w[16];
+};
+// A domain's tensor maps for the TMA z-march shapes, over its split arrays
+// as 4-D tensors (q, j, k, colour): the other colour's slab (a box of
+// 136 x (rows + 2)), the own colour's lambda and R (128 x rows), the mask.
+enum { kTmOther = 0, kTmOwn = 1, kTmR = 2, kTmMask = 3, kTmCount = 4 };
+
 // One domain in the red/black split layout, as the sweep kernels see it.
 struct SweepDomain {
   int X, Y, Z, PQ;
@@ -35,6 +45,7 @@ struct SweepDomain {
   long wn;
   double wtol;
   float *snap;
+  const TmaDesc *tm;  // [kTmCount] device tensor maps (TMA z-march shapes), or null
 };
 
 struct SweepCtl {

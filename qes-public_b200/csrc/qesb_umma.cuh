@@ -109,6 +109,22 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, uint3
   return false;
 }
 
+// A bounded wait whose first poll does not block (mbarrier.test_wait), then up
+// to limit - 1 potentially suspending polls: with limit 1 it gives up unless
+// the phase has already completed, so a timeout can be reached on demand.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *mbar, uint32_t parity, uint32_t limit)
+{
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(smem_u32(mbar)), "r"(parity)
+      : "memory");
+  return done || (limit > 1 && mbar_wait(mbar, parity, limit - 1));
+}
+
 // After a wait gave up: the issuing thread makes `drain` (an mbarrier
 // initialised with count 1 and not used otherwise) track every MMA it has
 // started, and every thread waits for it, at most `limit` polls, so that TMEM

@@ -1,7 +1,7 @@
 """Bounded device waits end in an error status, not a hang.
 
-The bulk-copy sweep kernels wait on a shared-memory barrier for each stage's
-copies. With the handle option "wait_limit" at 1 poll, a correct solve on
+The bulk-copy sweep kernels, and the z-march shapes staged by tensor-map
+copies, wait on a shared-memory barrier for each stage's copies. With the handle option "wait_limit" at 1 poll, a correct solve on
 correct data meets stages whose copies have not landed yet: the kernel gives
 up, lets its copies in flight land, flags the fault and returns, and the solve
 reports QESB_ERR_CUDA. With the limit back at its default, the same handle
@@ -16,8 +16,10 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 # option "variant" index of bulk_w4_s3, the first bulk-copy sweep shape
-# (after the 5 fused tile shapes and the 13 streaming split shapes)
+# (after the 5 fused tile shapes and the 13 streaming split shapes), and of
+# zmt_y4x2_b5, the first z-march shape staged by tensor-map copies
 BULK_W4_S3 = 18
+ZMT_Y4X2_B5 = 51
 
 
 def _city():
@@ -26,12 +28,13 @@ def _city():
     return d, qesb.city_build(d, c.buildings, c.inflow)
 
 
-def test_stage_wait_timeout_is_an_error_status_and_the_handle_recovers():
+@pytest.mark.parametrize("variant", [BULK_W4_S3, ZMT_Y4X2_B5])
+def test_stage_wait_timeout_is_an_error_status_and_the_handle_recovers(variant):
     d, w = _city()
     itermax = 60
     with qesb.Solver_B200(d, 1e-9) as s:
         s.set_inputs(w)
-        s.set_option("variant", BULK_W4_S3)
+        s.set_option("variant", variant)
         s.set_option("wait_limit", 1)
         with pytest.raises(qesb.QesbError) as ei:
             s.solve(w, itermax, set_inputs=False)

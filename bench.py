@@ -385,7 +385,7 @@ def fp64_checks(w, seed, st, lam, winds, ref_div=None):
     return out
 
 
-def precision_device(s, outs, use_net, use_pre, net=None, stream=None, omega=PRE_OMEGA):
+def precision_device(s, outs, use_net, use_pre, net=None, omega=PRE_OMEGA):
     """One solve of the handle's domain with the arm's start, to the rule, then
     the same SOR in FP64 on the device from the same start with its iteration
     counts (qesb_fp64_same_sor): the FP32 result's lambda and wind errors."""
@@ -393,7 +393,7 @@ def precision_device(s, outs, use_net, use_pre, net=None, stream=None, omega=PRE
 
     s.set_prephase(omega if use_pre else 0.0, PRE_TOL, ITERMAX)
     if use_net:
-        net.warm_start(s, stream)
+        net.warm_start(s)
         lam0 = s.lambda_
     else:
         s.resetLambda()
@@ -601,7 +601,8 @@ def run_b200(args):
     variant, _ = solvers[0].autotune()
     batch_variant, _ = qesb.autotune_batch(solvers)
     wpath = args.weights or ws.DEFAULT_WEIGHTS
-    net = ws.WarmStartNet.from_file(wpath, device=dev)
+    net = ws.WarmStartNet.from_file(wpath, device=dev)  # the network alone (forward timing, FLOPs)
+    cnet = ws.WarmNet(wpath, device=dev)  # the arms' starts: the C ABI, the batch's forward in one pass
 
     def barrier():
         if dist:
@@ -612,7 +613,8 @@ def run_b200(args):
 
     outs = [[torch.empty(nf, dtype=torch.float32, device=f"cuda:{dev}") for _ in range(3)] for _ in range(B)]
     uvw = [[o[q].data_ptr() for o in outs] for q in range(3)]
-    launches_per_net = 4 + (4 * net.nlev - 1) + (net.nlev - 1)  # R, input (2), apply + convs + pools
+    # per batched start: R, input (2), apply per domain; convolutions and poolings once
+    launches_per_net = 4 * B + (4 * net.nlev - 1) + (net.nlev - 1)
 
     def set_arm(sset, use_pre):
         for s in sset:
@@ -623,13 +625,13 @@ def run_b200(args):
 
         def step():
             set_arm(sset, use_pre)
-            for s in sset:
-                if use_net:
-                    net.warm_start(s, strm.cuda_stream)
-                else:
+            if use_net:
+                cnet.warm_start_batch(sset)
+            else:
+                for s in sset:
                     s.resetLambda()
             st = qesb.solve_batch(sset, ITERMAX, *ptrs)
-            return st, (B * launches_per_net if use_net else 0) + 6 * B + st[0]["launches"]
+            return st, (launches_per_net if use_net else 0) + 6 * B + st[0]["launches"]
         return step
 
     def timed(fn, steps, warmup, clocks=False):
@@ -693,7 +695,7 @@ def run_b200(args):
     ms_plain = arms["plain"]["ms_per_domain"] * B
     # precision of domain 0 under the headline arm: FP64 replay on the device,
     # and (rank 0, below) the oracle's FP64 restatement on the host as a cross-check
-    st_first, prec_first = precision_device(solvers[0], outs[0], use_net, use_pre, net, stream.cuda_stream)
+    st_first, prec_first = precision_device(solvers[0], outs[0], use_net, use_pre, cnet)
     lam_first = solvers[0].lambda_
     winds_first = [t.cpu().numpy() for t in outs[0]]
 
@@ -840,6 +842,15 @@ def run_b200(args):
     torch.cuda.synchronize(dev)
     ms_fwd = fwd[0].elapsed_time(fwd[1]) / nf_rep
     flops = network_flops(net, s0)
+    # the batch's start as the headline runs it: R, inputs, one stacked forward, applies
+    for _ in range(2):
+        cnet.warm_start_batch(solvers)
+    fwd[0].record(stream)
+    for _ in range(nf_rep):
+        cnet.warm_start_batch(solvers)
+    fwd[1].record(stream)
+    torch.cuda.synchronize(dev)
+    ms_start_batch = fwd[0].elapsed_time(fwd[1]) / nf_rep / B
 
     # ---- QES-Fire's solve pattern: fire steps warm-started from the previous lambda ----
     fire = None
@@ -937,6 +948,11 @@ def run_b200(args):
 
     if rank == 0:
         value = ms_head / B
+        ms_pre_arm = arms["prephase"]["ms_per_domain"]
+        learned_note = (f"the learned start pays: {ms_pre_arm / value:.3f}x the pre-phase alone (arms.prephase)"
+                        if value < ms_pre_arm else
+                        f"the pre-phase alone (arms.prephase) is faster ({value / ms_pre_arm:.3f}x): the network's "
+                        "start saves fewer pre-phase iterations than its forward pass costs")
         line = {
             "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_head, "higher_is_better": False, "scaling": "weak",
@@ -952,8 +968,7 @@ def run_b200(args):
                                      f"resolution), then the pre-phase: red-black SOR at omega {PRE_OMEGA} to "
                                      f"max|dlambda| <= {PRE_TOL}; then the reference loop (omega 1.78) to the "
                                      f"rule; arms holds plain SOR, the pre-phase alone and the network alone",
-                       "learned_start_note": "the pre-phase alone (arms.prephase) is faster: the network's "
-                                             "start saves fewer pre-phase iterations than its forward pass costs",
+                       "learned_start_note": learned_note,
                        "l2": "8 domains x ~40 MB packed sweep data + network buffers > L2 (126 MB) per step"},
             "arms": arms,
             "speedup_vs_plain": ms_plain / ms_head,
@@ -968,7 +983,11 @@ def run_b200(args):
             "sizes": sizes,
             "network": {"bound": "tensor", "ms_per_forward": ms_fwd, "flops_per_forward": flops,
                         "achieved_tflops": flops / (ms_fwd * 1e-3) / 1e12, "peak_tflops": tpeak,
-                        "frac": flops / (ms_fwd * 1e-3) / 1e12 / tpeak},
+                        "frac": flops / (ms_fwd * 1e-3) / 1e12 / tpeak,
+                        "batched_start_ms_per_domain": ms_start_batch,
+                        "batched_frac": flops / (ms_start_batch * 1e-3) / 1e12 / tpeak,
+                        "batched_how": f"qesb_warm_start_batch over the {B} domains (R, inputs, one forward over "
+                                       "the inputs stacked along z, applies), CUDA events, per domain"},
             "ensemble": ensemble,
             "wall_log_law": wall_log,
             "fire_loop": fire,
@@ -1164,10 +1183,10 @@ def run_profile_batch(args):
         outs = [[torch.empty(nf, dtype=torch.float32, device="cuda:0") for _ in range(3)] for _ in cities]
         ptrs = [[o[q].data_ptr() for o in outs] for q in range(3)]
         for _ in range(2):
-            for s in solvers:
-                if net:
-                    net.warm_start(s)
-                else:
+            if net:
+                net.warm_start_batch(solvers)
+            else:
+                for s in solvers:
                     s.resetLambda()
             st = qesb.solve_batch(solvers, ITERMAX, *ptrs)
         torch.cuda.synchronize()

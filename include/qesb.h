@@ -63,7 +63,8 @@ typedef struct qesb_stats {
   int path;              /* 0 = full-coefficient sweep, 1 = packed wall-mask sweep */
   int sweeps_per_launch; /* iterations fused per sweep launch */
   int launches;          /* kernels this solve launched (including polls and early exits) */
-  int pre_iterations;    /* iterations of the over-relaxed pre-phase (qesb_set_prephase), 0 if none */
+  int pre_iterations;    /* iterations of the over-relaxed pre-phase (qesb_set_prephase), its start
+                            stage (qesb_set_prephase_start) included; 0 if none */
   double max_divergence; /* final check, in FP64: max |du/dx + dv/dy + dw/dz| over fluid cells
                             (icellflag 1), i in [1,nx-3], j in [1,ny-3], k in [1,nz-4], of the
                             corrected winds; -1 when the solve wrote no winds */
@@ -146,9 +147,20 @@ int qesb_num_variants(void);
  * max|dlambda| <= tol or max_iterations; then the reference loop runs as
  * always, with omega = 1.78 and the handle's tolerance, from that lambda. The
  * result therefore meets exactly the reference's stopping rule; only the
- * starting point differs. omega = 0 turns it off (the default). The fused
- * tiled and full-coefficient paths ignore it. */
+ * starting point differs. omega = 0 turns it off (the default). On the
+ * packed path a set pre-phase runs on the sweep kernels (the fused tile
+ * shapes have none); the full-coefficient path ignores it. */
 qesb_status qesb_set_prephase(qesb_handle *h, float omega, float tol, int max_iterations);
+
+/* Start stage of the pre-phase (no reference counterpart). With
+ * iterations > 0 and a pre-phase set, each solve's pre-phase begins with
+ * `iterations` red-black sweeps at this omega (in (0, 2); its own omega/sum
+ * table and 1 - omega, no stop on the tolerance), then continues at the
+ * pre-phase's omega until its tolerance. Over-relaxation near 2 from a rough
+ * start first amplifies the start's rough error; a short stage at a smaller
+ * omega damps it. qesb_stats.pre_iterations counts both parts; the reference
+ * loop is unchanged. iterations = 0 turns it off (the default). */
+qesb_status qesb_set_prephase_start(qesb_handle *h, float omega, int iterations);
 
 /* Window stopping rule (no reference counterpart; a reachable stop for the
  * reference loop). The reference stops when one iteration changes lambda by at
@@ -172,8 +184,10 @@ qesb_status qesb_set_window_rule(qesb_handle *h, int window, double tol);
 /* FP64 run of the same SOR (no reference counterpart; the precision check of
  * an FP32 result). On the handle's inputs, in double on the device: R, then
  * from lambda0 (host, cell layout, widened to double; NULL: zero)
- * pre_iterations red-black iterations at pre_omega (the pre-phase; 0 for
- * none), then `iterations` at the reference's omega (1.78f as a double), the
+ * pre_iterations red-black iterations of the pre-phase (0 for none): the
+ * first min(pre_iterations, its start-stage count) at the handle's start-stage
+ * omega when qesb_set_prephase_start set one, the rest at pre_omega; then
+ * `iterations` at the reference's omega (1.78f as a double), the
  * ground mirror after each, with the reference's loop bounds and operation
  * order, no stopping rule; then the correction. Pass the counts a solve
  * reported (qesb_stats.pre_iterations, .iterations) to measure that solve's
@@ -327,6 +341,12 @@ typedef struct qesb_warmnet qesb_warmnet;
 qesb_status qesb_warmnet_load(const char *path, int device, qesb_warmnet **out);
 qesb_status qesb_warmnet_destroy(qesb_warmnet *net);
 qesb_status qesb_warm_start(qesb_handle *h, qesb_warmnet *net);
+/* qesb_warm_start for n handles of one grid shape at once: their network
+ * inputs stacked along z (qesb_conv3d_items), one launch per layer for all of
+ * them, each start the one qesb_warm_start would give. Each handle's input
+ * and apply run on its own stream, ordered with the forward pass on handle
+ * 0's stream by an event; returns when every start is in place. */
+qesb_status qesb_warm_start_batch(qesb_handle *const *hs, int n, qesb_warmnet *net);
 
 /* Self-test of the tcgen05 GEMM core: C[128 x N] = A[128 x K] * B[N x K]^T
  * in BF16 with FP32 accumulation. A is [128][K] (a_mn = 0) or [K][128]
@@ -357,6 +377,13 @@ qesb_status qesb_umma_selftest(const uint16_t *A, const uint16_t *B, float *C, i
 qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H, int W,
                         int sign, const void *Bm, int Kp, int N, void *y, void *yf, const float *bias,
                         int relu, const void *mask, int *err, void *stream);
+/* The same over `items` grids of D x H x W stacked along z (activations
+ * [items * D][H][W][C]; x1 under up1 [items * D/2][H/2][W/2][c1]): one launch
+ * for all of them, taps never reaching from one item into the next, so each
+ * item's output is qesb_conv3d's on that item alone. D even when items > 1. */
+qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const void *x2, int c2, int items, int D,
+                              int H, int W, int sign, const void *Bm, int Kp, int N, void *y, void *yf,
+                              const float *bias, int relu, const void *mask, int *err, void *stream);
 /* Process-wide choice of the qesb_conv3d kernel: 0 = direct kernel where it
  * applies (default), 1 = implicit GEMM everywhere (for comparison). */
 qesb_status qesb_net_set_conv_path(int path);

@@ -125,13 +125,16 @@ struct ConvIn {
 struct ConvGeom {
   int D, H, W;  // voxel grid of the GEMM rows (output grid)
   long V;       // D*H*W
+  int Dc;       // depth of one item: D / Dc grids stacked along z, taps never cross from one to the next
 };
 
 // 16 bytes (8 channels c..c+7, never straddling x1/x2 since c1 % 16 == 0) of
-// the input at voxel (z, y, x), or zeros outside the grid.
-__device__ __forceinline__ uint4 load_in8(const ConvIn &in, const ConvGeom &g, int z, int y, int x, int c)
+// the input at voxel (z, y, x) for an output voxel at depth zo, or zeros
+// outside the output voxel's item.
+__device__ __forceinline__ uint4 load_in8(const ConvIn &in, const ConvGeom &g, int zo, int z, int y, int x, int c)
 {
-  if (z < 0 || z >= g.D || y < 0 || y >= g.H || x < 0 || x >= g.W) return make_uint4(0, 0, 0, 0);
+  const int zb = zo - zo % g.Dc;
+  if (z < zb || z >= zb + g.Dc || y < 0 || y >= g.H || x < 0 || x >= g.W) return make_uint4(0, 0, 0, 0);
   const __nv_bfloat16 *p;
   if (c < in.c1) {
     if (in.up1)
@@ -225,7 +228,8 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         uint4 val = make_uint4(0, 0, 0, 0);
-        if (rv[i] && t < 27) val = load_in8(in, g, rz[i] + sign * dz, ry[i] + sign * dy, rx[i] + sign * dx, c);
+        if (rv[i] && t < 27)
+          val = load_in8(in, g, rz[i], rz[i] + sign * dz, ry[i] + sign * dy, rx[i] + sign * dx, c);
         *reinterpret_cast<uint4 *>(sa + off_kmajor((tid >> 3) + 16 * i, 8 * g8)) = val;
       }
     }
@@ -356,6 +360,7 @@ __global__ void __launch_bounds__(128) k_conv_direct(ConvIn in, ConvGeom g, int 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int cin = in.c1 + in.c2, KC = cin / 16;
   const int x0 = blockIdx.x * 128, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+  const int zb = z0 - z0 % g.Dc;  // the tile's item (TZ divides Dc)
   if (warp == 0) umma::tmem_alloc(&tmem_base, NCOLS);
   if (tid == 0) {
     umma::mbar_init(&mbar, 1);
@@ -376,7 +381,7 @@ __global__ void __launch_bounds__(128) k_conv_direct(ConvIn in, ConvGeom g, int 
       const int cg = idx / (NR * XW), rem = idx - cg * NR * XW;
       const int r = rem / XW, xi = rem - r * XW;
       const int zz = z0 - 1 + r / (TY + 2), yy = y0 - 1 + r % (TY + 2), xx = x0 - 1 + xi;
-      const bool inside = zz >= 0 && zz < g.D && yy >= 0 && yy < g.H && xx >= 0 && xx < g.W;
+      const bool inside = zz >= zb && zz < zb + g.Dc && yy >= 0 && yy < g.H && xx >= 0 && xx < g.W;
       const __nv_bfloat16 *src = inside ? in_ptr8(in, g, zz, yy, xx, 16 * kc + 8 * cg) : in.x1;
       cp16_zfill(sa + ((cg * NR + r) * XW + xi) * 16, src, inside);
     }
@@ -516,7 +521,7 @@ __global__ void __launch_bounds__(128) k_conv_wgrad(ConvIn in, ConvGeom g, const
       if (vin && tg[i] < 27) {
         int dz, dy, dx;
         tap_offset(tg[i], dz, dy, dx);
-        val = load_in8(in, g, z + dz, y + dy, x + dx, cg[i]);
+        val = load_in8(in, g, z, z + dz, y + dy, x + dx, cg[i]);
       }
       *reinterpret_cast<uint4 *>(sa + off_mnmajor(8 * ((tid >> 6) + 2 * i), kv, 128)) = val;
     }
@@ -729,15 +734,15 @@ bool conv_args_ok(int c1, int c2, int N, int D, int H, int W, int up1)
 }
 }  // namespace
 
-extern "C" qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H, int W,
-                                   int sign, const void *Bm, int Kp, int N, void *y, void *yf, const float *bias,
-                                   int relu, const void *mask, int *err, void *stream)
+extern "C" qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const void *x2, int c2, int items, int D,
+                                         int H, int W, int sign, const void *Bm, int Kp, int N, void *y, void *yf,
+                                         const float *bias, int relu, const void *mask, int *err, void *stream)
 {
-  if (!conv_args_ok(c1, c2, N, D, H, W, up1) || !x1 || (c2 && !x2) || !Bm || (!y && !yf) || !err ||
-      (sign != 1 && sign != -1) || Kp < 27 * (c1 + c2) || Kp % 64)
+  if (!conv_args_ok(c1, c2, N, D, H, W, up1) || items < 1 || (items > 1 && D % 2) || !x1 || (c2 && !x2) ||
+      !Bm || (!y && !yf) || !err || (sign != 1 && sign != -1) || Kp < 27 * (c1 + c2) || Kp % 64)
     return qesb_fail(QESB_ERR_ARG, "qesb_conv3d: bad arguments");
   ConvIn in{static_cast<const __nv_bfloat16 *>(x1), static_cast<const __nv_bfloat16 *>(x2), c1, c2, up1};
-  ConvGeom g{D, H, W, (long)D * H * W};
+  ConvGeom g{items * D, H, W, (long)items * D * H * W, D};
   ConvOut o{static_cast<__nv_bfloat16 *>(y), static_cast<float *>(yf), bias, relu,
             static_cast<const __nv_bfloat16 *>(mask)};
   const auto *B = static_cast<const __nv_bfloat16 *>(Bm);
@@ -754,6 +759,13 @@ extern "C" qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *
   }
 }
 
+extern "C" qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H, int W,
+                                   int sign, const void *Bm, int Kp, int N, void *y, void *yf, const float *bias,
+                                   int relu, const void *mask, int *err, void *stream)
+{
+  return qesb_conv3d_items(x1, c1, up1, x2, c2, 1, D, H, W, sign, Bm, Kp, N, y, yf, bias, relu, mask, err, stream);
+}
+
 extern "C" qesb_status qesb_net_set_conv_path(int path)
 {
   if (path != 0 && path != 1) return qesb_fail(QESB_ERR_ARG, "qesb_net_set_conv_path: path must be 0 or 1");
@@ -767,7 +779,7 @@ extern "C" qesb_status qesb_conv3d_wgrad(const void *x1, int c1, int up1, const 
   if (!conv_args_ok(c1, c2, N, D, H, W, up1) || !x1 || (c2 && !x2) || !dY || !dW || !err || vchunk < 64)
     return qesb_fail(QESB_ERR_ARG, "qesb_conv3d_wgrad: bad arguments");
   ConvIn in{static_cast<const __nv_bfloat16 *>(x1), static_cast<const __nv_bfloat16 *>(x2), c1, c2, up1};
-  ConvGeom g{D, H, W, (long)D * H * W};
+  ConvGeom g{D, H, W, (long)D * H * W, D};
   const auto *d = static_cast<const __nv_bfloat16 *>(dY);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   switch (N) {

@@ -694,18 +694,26 @@ struct qesb_handle {
   int pre_iters = 0;
   float *d_inv_pre = nullptr;     // [Z][64] pre_omega / sum
   float inv_pre_omega = 0.0f;     // omega d_inv_pre holds (0 = stale)
+  // start stage of the pre-phase: its first start_iters sweeps at start_omega
+  float start_omega = 0.0f;
+  int start_iters = 0;
+  float *d_inv_start = nullptr;   // [Z][64] start_omega / sum
+  float inv_start_omega = 0.0f;   // omega d_inv_start holds (0 = stale)
   int last_pre_iterations = 0;
   SweepGraph sgraph_pre;
+  SweepGraph sgraph_start;
 
   // window rule (qesb_set_window_rule): window 0 = off
   int win_k = 0;
   double win_tol = 0.0;
   float *d_snap = nullptr;  // lambda at the start of the current window (split or padded layout)
 
-  // tensor maps of the split arrays for the TMA z-march shapes, encoded for tiles of tm_rows rows
+  // tensor maps of the split arrays for the TMA z-march shapes: slot i holds
+  // the kTmCount maps for tiles of tm_rows[i] rows (0: free). A slot is
+  // encoded once and never rewritten, so captured graphs and lists in
+  // flight keep valid maps whatever shape runs next.
   TmaDesc *d_tmaps = nullptr;
-  TmaDesc h_tmaps[kTmCount] = {};
-  int tm_rows = 0;
+  int tm_rows[kTmSlots] = {};
 
   // sweep kernels: this solve as a one-domain list
   SweepList list;
@@ -825,7 +833,8 @@ qesb_status prepare_coefs(qesb_handle *h)
     CK(cudaStreamSynchronize(s));
     if (!bad) {
       k_inv_table<<<G.Z, 64, 0, s>>>(G, h->d_vmax, h->d_inv, h->d_val, kOmega);
-      h->inv_pre_omega = 0.0f;  // the pre-phase table follows the new inputs at the next solve
+      h->inv_pre_omega = 0.0f;  // the pre-phase tables follow the new inputs at the next solve
+      h->inv_start_omega = 0.0f;
       k_pad_to_split_u8<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_mask, h->d_mask_s);
       CK(cudaGetLastError());
       h->packed = true;
@@ -1080,8 +1089,10 @@ const SweepVariant kSweepVariants[] = {
     make_zm<8, 2, 2>("zm_y8x2_b2"),
     // copies one plane ahead: smaller rings, more CTAs per SM (48..50)
     make_zm<4, 2, 5, 1>("zm_y4x2_d1_b5"), make_zm<4, 2, 4, 1>("zm_y4x2_d1_b4"), make_zm<2, 2, 8, 1>("zm_y2x2_d1_b8"),
-    // the same staged by tensor-map copies issued from one thread (51..53)
+    // the same staged by tensor-map copies issued from one thread (51..57; d2: two planes ahead)
     make_zm<4, 2, 5, 1, 1>("zmt_y4x2_b5"), make_zm<4, 2, 4, 1, 1>("zmt_y4x2_b4"), make_zm<2, 2, 8, 1, 1>("zmt_y2x2_b8"),
+    make_zm<8, 2, 2, 1, 1>("zmt_y8x2_b2"), make_zm<4, 4, 2, 1, 1>("zmt_y4x4_b2"),
+    make_zm<4, 2, 3, 2, 1>("zmt_y4x2_d2_b3"), make_zm<4, 2, 4, 2, 1>("zmt_y4x2_d2_b4"),
 };
 constexpr int kNumSweep = sizeof(kSweepVariants) / sizeof(kSweepVariants[0]);
 constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the first sweep shape
@@ -1159,12 +1170,19 @@ qesb_status encode_tiled_fn(EncodeTiledFn *out)
 // the TMA z-march shapes copy for tiles of `rows` rows: the other colour's
 // slab 136 x (rows + 2), the own colour's lambda and R 128 x rows (floats),
 // the mask 128 x rows (bytes). Out-of-range elements read as zeros.
-qesb_status ensure_tmaps(qesb_handle *h, int rows)
+qesb_status ensure_tmaps(qesb_handle *h, int rows, cudaStream_t s, const TmaDesc **out)
 {
-  if (h->d_tmaps && h->tm_rows == rows) return QESB_OK;
+  int slot = 0;
+  while (slot < kTmSlots && h->tm_rows[slot] != 0 && h->tm_rows[slot] != rows) ++slot;
+  if (slot == kTmSlots) return qesb_fail(QESB_ERR_ARG, "more than %d tile heights with tensor maps", kTmSlots);
+  if (h->tm_rows[slot] == rows) {
+    *out = h->d_tmaps + slot * kTmCount;
+    return QESB_OK;
+  }
   EncodeTiledFn enc = nullptr;
   CKS(encode_tiled_fn(&enc));
-  if (!h->d_tmaps) CKS(dalloc(&h->d_tmaps, kTmCount));
+  if (!h->d_tmaps) CKS(dalloc(&h->d_tmaps, kTmCount * kTmSlots));
+  TmaDesc maps_h[kTmCount];
   const cuuint64_t dims[4] = {(cuuint64_t)h->S.PQ, (cuuint64_t)h->G.Y, (cuuint64_t)h->G.Z, 2};
   const cuuint64_t fstr[3] = {(cuuint64_t)h->S.PQ * 4, (cuuint64_t)h->S.PQ * h->G.Y * 4, (cuuint64_t)h->S.CS * 4};
   const cuuint64_t bstr[3] = {(cuuint64_t)h->S.PQ, (cuuint64_t)h->S.PQ * h->G.Y, (cuuint64_t)h->S.CS};
@@ -1187,19 +1205,24 @@ qesb_status ensure_tmaps(qesb_handle *h, int rows)
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return qesb_fail(QESB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d) for map %d", (int)r, q);
-    std::memcpy(&h->h_tmaps[q], &m, sizeof m);
+    std::memcpy(&maps_h[q], &m, sizeof m);
   }
-  CK(cudaMemcpyAsync(h->d_tmaps, h->h_tmaps, sizeof h->h_tmaps, cudaMemcpyHostToDevice, h->stream));
-  h->tm_rows = rows;
+  // on the stream of the launches that read them; from pageable memory, so
+  // maps_h may go out of scope when the call returns
+  CK(cudaMemcpyAsync(h->d_tmaps + slot * kTmCount, maps_h, sizeof maps_h, cudaMemcpyHostToDevice, s));
+  h->tm_rows[slot] = rows;
+  *out = h->d_tmaps + slot * kTmCount;
   return QESB_OK;
 }
 
-// The domain's tensor maps for a TMA shape (no-op for the others).
-qesb_status attach_tmaps(qesb_handle *h, const SweepVariant &sv, SweepDomain &d)
+// The domain's tensor maps for a TMA shape (no-op for the others); s is the
+// stream of the launches that use them.
+qesb_status attach_tmaps(qesb_handle *h, const SweepVariant &sv, SweepDomain &d, cudaStream_t s)
 {
   if (!sv.tma) return QESB_OK;
-  CKS(ensure_tmaps(h, sv.tile_rows));
-  d.tm = h->d_tmaps;
+  const TmaDesc *m = nullptr;
+  CKS(ensure_tmaps(h, sv.tile_rows, s, &m));
+  d.tm = m;
   return QESB_OK;
 }
 
@@ -1245,6 +1268,30 @@ qesb_status sweep_domain_pre(qesb_handle *h, SweepDomain &d, cudaStream_t s)
   d.c1 = 1.0f - h->pre_omega;
   d.wK = 0;  // the window rule ends the reference loop only
   return QESB_OK;
+}
+
+// The pre-phase's start stage: start_iters sweeps at start_omega, no stop
+// on the tolerance (its own inv table, 1 - start_omega).
+qesb_status sweep_domain_start(qesb_handle *h, SweepDomain &d, cudaStream_t s)
+{
+  if (h->inv_start_omega != h->start_omega) {
+    k_inv_table<<<h->G.Z, 64, 0, s>>>(h->G, h->d_vmax, h->d_inv_start, h->d_val, h->start_omega);
+    CK(cudaGetLastError());
+    h->inv_start_omega = h->start_omega;
+  }
+  d = sweep_domain(h, h->start_iters, -1.0);  // tol < 0: every sweep runs
+  d.inv = h->d_inv_start;
+  d.c1 = 1.0f - h->start_omega;
+  d.wK = 0;
+  return QESB_OK;
+}
+
+// Whether the handle's next solve runs a pre-phase, and a start stage in it.
+bool prephase_on(const qesb_handle *h) { return h->pre_omega > 0.0f && h->pre_iters > 0; }
+bool start_on(const qesb_handle *h) { return prephase_on(h) && h->start_omega > 0.0f && h->start_iters > 0; }
+int err_slots(const qesb_handle *h, int itermax)
+{
+  return std::max({itermax, 1, prephase_on(h) ? h->pre_iters : 0, start_on(h) ? h->start_iters : 0});
 }
 
 // Window check launch for a list of kernels of work-unit kind `unit`.
@@ -1340,29 +1387,52 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
   int launched = 0, pre_launched = 0;
   h->last_pre_iterations = 0;
   CK(cudaEventRecord(h->evs[0], s));
-  if (h->pre_omega > 0.0f && h->pre_iters > 0) {
+  if (start_on(h)) {
+    // the pre-phase's start stage: start_iters sweeps at start_omega
+    std::vector<SweepDomain> st1(1);
+    CKS(sweep_domain_start(h, st1[0], s));
+    CKS(attach_tmaps(h, sv, st1[0], s));
+    sweep_tiles(st1, sv, false, h->device);
+    CKS(h->list.upload(st1, sv.unit, s));
+    SweepArgs a = h->list.a;
+    a.one = st1[0];
+    a.wait_limit = h->opt_wait_limit;
+    int n1 = 0;
+    CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, h->start_iters, h->opt_graph != 0,
+                       &h->sgraph_start, h->h_ctl, &n1));
+    pre_launched += n1;
+    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the pre-phase's start stage");
+    h->last_pre_iterations = h->h_state->it;
+    CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * err_slots(h, itermax), s));
+    CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+  }
+  if (prephase_on(h)) {
     // over-relaxed pre-phase from the current lambda; its state and error
     // history are then cleared for the reference loop
     std::vector<SweepDomain> pre(1);
     CKS(sweep_domain_pre(h, pre[0], s));
-    CKS(attach_tmaps(h, sv, pre[0]));
+    CKS(attach_tmaps(h, sv, pre[0], s));
     sweep_tiles(pre, sv, false, h->device);
     CKS(h->list.upload(pre, sv.unit, s));
     SweepArgs a = h->list.a;
     a.one = pre[0];
     a.wait_limit = h->opt_wait_limit;
+    int n2 = 0;
     CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, h->pre_iters, h->opt_graph != 0,
-                       &h->sgraph_pre, h->h_ctl, &pre_launched));
+                       &h->sgraph_pre, h->h_ctl, &n2));
+    pre_launched += n2;
     CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the pre-phase");
-    h->last_pre_iterations = h->h_state->it;
+    h->last_pre_iterations += h->h_state->it;
     CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
     CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
   }
   CK(cudaEventRecord(h->evs[1], s));
   std::vector<SweepDomain> one{sweep_domain(h, itermax, (double)h->tol)};
-  CKS(attach_tmaps(h, sv, one[0]));
+  CKS(attach_tmaps(h, sv, one[0], s));
   sweep_tiles(one, sv, false, h->device);
   CKS(h->list.upload(one, sv.unit, s));
   SweepArgs a = h->list.a;
@@ -1405,7 +1475,7 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   CK(cudaSetDevice(h->device));
   const DevGrid &G = h->G;
   cudaStream_t s = h->stream;
-  const int nerr = std::max({itermax, 1, h->pre_omega > 0.0f ? h->pre_iters : 0});
+  const int nerr = err_slots(h, itermax);
   CKS(ensure_err(h, nerr));
   CK(cudaEventRecord(h->ev[0], s));
   k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(
@@ -1421,8 +1491,8 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
     CK(cudaEventRecord(h->ev[1], s));
   }
   int vi = packed ? pick_variant(h) : -1;
-  // the fused tiled kernels have no window checks: the window rule runs on the sweep kernels
-  if (packed && h->win_k > 0 && vi < kSplitVariant) vi = kSplitVariant + kDefaultSweep;
+  // the fused tiled kernels have no window checks and no pre-phase: either runs on the sweep kernels
+  if (packed && (h->win_k > 0 || prephase_on(h)) && vi < kSplitVariant) vi = kSplitVariant + kDefaultSweep;
   const bool split = packed && vi >= kSplitVariant;
   const Variant *var = packed && !split ? &kVariants[vi] : nullptr;
   h->last_launches = 0;
@@ -1498,11 +1568,12 @@ void free_all(qesb_handle *h)
     if (g) cudaGraphExecDestroy(g);
   h->sgraph.reset();
   h->sgraph_pre.reset();
+  h->sgraph_start.reset();
   void *ptrs[] = {h->d_lam_s, h->d_R_s, h->d_mask_s, h->d_lam, h->d_lam2, h->d_R, h->d_mask, h->d_pc[0], h->d_pc[1], h->d_pc[2],
                   h->d_pc[3], h->d_pc[4], h->d_pc[5], h->d_own_in[0], h->d_own_in[1],
                   h->d_own_in[2], h->d_own_in[3], h->d_own_in[4], h->d_own_in[5], h->d_own_flag,
                   h->d_own_u0, h->d_own_v0, h->d_own_w0, h->d_dz, h->d_vmax, h->d_inv, h->d_val,
-                  h->d_inv_pre, h->d_bad, h->d_err, h->d_state, h->d_u, h->d_v, h->d_w, h->d_wbits,
+                  h->d_inv_pre, h->d_inv_start, h->d_bad, h->d_err, h->d_state, h->d_u, h->d_v, h->d_w, h->d_wbits,
                   h->d_wcut, h->d_snap, h->d_tmaps};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1573,6 +1644,7 @@ qesb_status qesb_create(const qesb_grid *grid, float tol, int device, qesb_handl
   TRY(dalloc(&h->d_vmax, 6 * G.Z));
   TRY(dalloc(&h->d_inv, 64 * G.Z));
   TRY(dalloc(&h->d_inv_pre, 64 * G.Z));
+  TRY(dalloc(&h->d_inv_start, 64 * G.Z));
   TRY(dalloc(&h->d_val, 6 * G.Z));
   TRY(dalloc(&h->d_bad, 1));
   TRY(dalloc(&h->d_state, 1));
@@ -1900,7 +1972,7 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
     cudaStream_t s = h->stream;
     CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
     std::vector<SweepDomain> one{sweep_domain(h, 1 << 30, -1.0)};  // tol < 0: every launch runs
-    CKS(attach_tmaps(h, sv, one[0]));
+    CKS(attach_tmaps(h, sv, one[0], s));
     sweep_tiles(one, sv, false, h->device);
     CKS(h->list.upload(one, sv.unit, s));
     const dim3 grid(sweep_ctas(sv, false, h->device)), block(32, sv.block_y);
@@ -2044,7 +2116,7 @@ qesb_status qesb_autotune_batch(qesb_handle *const *hs, int n, int *best, float 
             cudaMemsetAsync(hs[i]->d_state, 0, sizeof(SolveState), s) != cudaSuccess)
           qs = qesb_fail(QESB_ERR_CUDA, "qesb_autotune_batch: memset");
         doms[i] = sweep_domain(hs[i], 1 << 30, -1.0);  // tol < 0: every launch runs
-        if (qs == QESB_OK) qs = attach_tmaps(hs[i], sv, doms[i]);
+        if (qs == QESB_OK) qs = attach_tmaps(hs[i], sv, doms[i], s);
       }
       if (qs != QESB_OK) break;
       sweep_tiles(doms, sv, true, h0->device);
@@ -2102,8 +2174,8 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   CK(cudaEventRecord(h0->ev[0], s));
   std::vector<SweepDomain> doms(n);
   double cells = 0;
-  std::vector<SweepDomain> pre;
-  std::vector<int> pre_of;  // batch index of each pre-phase domain
+  std::vector<SweepDomain> pre, start;
+  std::vector<int> pre_of, start_of;  // batch index of each pre-phase / start-stage domain
   for (int i = 1; i < n; ++i)
     if (hs[i]->win_k != h0->win_k)
       return qesb_fail(QESB_ERR_ARG, "qesb_solve_batch: handles %d and 0 have different window lengths (%d, %d)", i,
@@ -2111,8 +2183,8 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   for (int i = 0; i < n; ++i) {
     qesb_handle *h = hs[i];
     const DevGrid &G = h->G;
-    const bool pre_on = h->pre_omega > 0.0f && h->pre_iters > 0 && itermax > 0;
-    const int nerr = std::max({itermax, 1, pre_on ? h->pre_iters : 0});
+    const bool pre_on = prephase_on(h) && itermax > 0;
+    const int nerr = err_slots(h, itermax);
     CKS(ensure_err(h, nerr));
     k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(
         G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_u0, h->d_v0,
@@ -2122,16 +2194,22 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     if (pre_on) {
       SweepDomain p;
       CKS(sweep_domain_pre(h, p, s));
-      CKS(attach_tmaps(h, sv, p));
+      CKS(attach_tmaps(h, sv, p, s));
       pre.push_back(p);
       pre_of.push_back(i);
+      if (start_on(h)) {
+        CKS(sweep_domain_start(h, p, s));
+        CKS(attach_tmaps(h, sv, p, s));
+        start.push_back(p);
+        start_of.push_back(i);
+      }
     }
     CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
     k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam, h->d_lam_s);
     k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_R, h->d_R_s);
     CK(cudaGetLastError());
     doms[i] = sweep_domain(h, itermax, (double)h->tol);
-    CKS(attach_tmaps(h, sv, doms[i]));
+    CKS(attach_tmaps(h, sv, doms[i], s));
     cells += (double)G.XY * G.Z;
   }
   SweepList list;
@@ -2141,24 +2219,50 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   qesb_status qs = QESB_OK;
   int launched = 0, pre_launched = 0;
   CK(cudaEventRecord(h0->evs[0], s));
-  if (!pre.empty()) {
+  if (!start.empty()) {
+    // the start stages of the pre-phases that have one, as a list of their own
+    sweep_tiles(start, sv, true, h0->device);
+    qs = list.upload(start, sv.unit, s);
+    SweepGraph gx;
+    int smax = 0;
+    for (int i : start_of) smax = std::max(smax, hs[i]->start_iters);
+    int n1 = 0;
+    if (qs == QESB_OK)
+      qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, smax, h0->opt_graph != 0, &gx, h0->h_ctl, &n1);
+    gx.reset();
+    pre_launched += n1;
+    for (size_t q = 0; q < start_of.size() && qs == QESB_OK; ++q) {
+      qesb_handle *h = hs[start_of[q]];
+      SolveState sp;
+      CK(cudaMemcpyAsync(&sp, h->d_state, sizeof sp, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      if (sp.nan)
+        qs = qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d during the pre-phase's start stage",
+                       start_of[q]);
+      h->last_pre_iterations = sp.it;
+      CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * err_slots(h, itermax), s));
+      CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+    }
+  }
+  if (!pre.empty() && qs == QESB_OK) {
     // the over-relaxed pre-phase of the domains that have one, as a list of its own
     sweep_tiles(pre, sv, true, h0->device);
     qs = list.upload(pre, sv.unit, s);
     SweepGraph gx;
     int pre_max = 0;
     for (int i : pre_of) pre_max = std::max(pre_max, hs[i]->pre_iters);
+    int n2 = 0;
     if (qs == QESB_OK)
-      qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, pre_max, h0->opt_graph != 0, &gx, h0->h_ctl,
-                          &pre_launched);
+      qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, pre_max, h0->opt_graph != 0, &gx, h0->h_ctl, &n2);
     gx.reset();
+    pre_launched += n2;
     for (size_t q = 0; q < pre_of.size() && qs == QESB_OK; ++q) {
       qesb_handle *h = hs[pre_of[q]];
       SolveState sp;
       CK(cudaMemcpyAsync(&sp, h->d_state, sizeof sp, cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
       if (sp.nan) qs = qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d during the pre-phase", pre_of[q]);
-      h->last_pre_iterations = sp.it;
+      h->last_pre_iterations += sp.it;
       CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
       CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
     }
@@ -2229,6 +2333,16 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   return QESB_OK;
 }
 
+qesb_status qesb_set_prephase_start(qesb_handle *h, float omega, int iterations)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  if (iterations < 0 || (iterations > 0 && !(omega > 0.0f && omega < 2.0f)))
+    return qesb_fail(QESB_ERR_ARG, "qesb_set_prephase_start: iterations must be >= 0 and omega in (0, 2)");
+  h->start_omega = iterations > 0 ? omega : 0.0f;
+  h->start_iters = iterations;
+  return QESB_OK;
+}
+
 qesb_status qesb_set_prephase(qesb_handle *h, float omega, float tol, int max_iterations)
 {
   if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
@@ -2295,9 +2409,12 @@ qesb_status qesb_fp64_same_sor(qesb_handle *h, const float *lambda0, float pre_o
                                                           h->d_in[4], h->d_in[5], h->d_u0, h->d_v0, h->d_w0,
                                                           h->d_dz, h->dx, h->dy, R);
   const dim3 sgrid(((G.X - 2) / 2 + 1 + 127) / 128, G.Y - 2, G.Z - 2), mgrid((G.X + 255) / 256, G.Y, 1);
-  for (int phase = 0; phase < 2 && e == cudaSuccess; ++phase) {
-    const int n = phase == 0 ? pre_iterations : iterations;
-    const double om = phase == 0 ? (double)pre_omega : (double)kOmega;
+  // phases: the handle's start stage (its share of pre_iterations), the rest
+  // of the pre-phase at pre_omega, the reference loop
+  const int n_start = start_on(h) ? std::min(h->start_iters, pre_iterations) : 0;
+  for (int phase = 0; phase < 3 && e == cudaSuccess; ++phase) {
+    const int n = phase == 0 ? n_start : phase == 1 ? pre_iterations - n_start : iterations;
+    const double om = phase == 0 ? (double)h->start_omega : phase == 1 ? (double)pre_omega : (double)kOmega;
     for (int t = 0; t < n; ++t) {
       for (int colour = 0; colour < 2; ++colour)
         k_sor64<<<sgrid, 128, 0, s>>>(G, colour, om, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4],

@@ -20,6 +20,7 @@
 // and mask rows (boxes of 128 x rows) and the plane's inv row (a 256-byte
 // bulk copy), completing on one mbarrier per ring slot; out-of-range box
 // elements arrive as zeros, as the zero-filled cp.async copies leave them.
+// DIST planes ahead (one or two), the own slots each with their mbarrier.
 // The waits are bounded (SweepArgs::wait_limit): a CTA that gives up lets its
 // copies in flight land, sets the list's fault flag and stops.
 //
@@ -247,7 +248,6 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
   constexpr int TR = TY * RW, NT = 32 * TY, NSO = zm_other_slots(DIST), NSW = zm_own_slots(DIST);
   constexpr int OSTR = zm_oslot_floats<TR, TMA>();
   static_assert(DIST == 1 || DIST == 2, "copies run one or two planes ahead");
-  static_assert(!TMA || DIST == 1, "the TMA shapes copy one plane ahead");
   const int na = b.ctl->nactive;
   if (na <= 0) return;
   extern __shared__ __align__(128) unsigned char zm_raw[];
@@ -321,6 +321,10 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
     if constexpr (TMA) {
       if (tid == 0) zm_tma_step<COLOUR, TR, OSTR, NSO>(sm, D, q0, j0, k0, true, 2, 0, &sm.bar[nst % NSW]);
       ++nst;
+      if (DIST == 2 && k0 + 1 < k1) {
+        if (tid == 0) zm_tma_step<COLOUR, TR, OSTR, NSO>(sm, D, q0, j0, k0 + 1, false, 3, 1, &sm.bar[nst % NSW]);
+        ++nst;
+      }
     } else {
       zm_stage_other<COLOUR, TR, NT>(sm, cp, D, k0 - 1, 0);
       zm_stage_other<COLOUR, TR, NT>(sm, cp, D, k0, 1);
@@ -343,10 +347,10 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
           if (tid == 0) atomicExch(&b.ctl->fault, 1);
           goto tiles_done;
         }
-        if (k + 1 < k1) {
+        if (k + DIST < k1) {
           if (tid == 0)
-            zm_tma_step<COLOUR, TR, OSTR, NSO>(sm, D, q0, j0, k + 1, false, zm_wrap<NSO>(om1 + 3),
-                                               zm_wrap<NSW>(wk + 1), &sm.bar[nst % NSW]);
+            zm_tma_step<COLOUR, TR, OSTR, NSO>(sm, D, q0, j0, k + DIST, false, zm_wrap<NSO>(om1 + DIST + 2),
+                                               zm_wrap<NSW>(wk + DIST), &sm.bar[nst % NSW]);
           ++nst;
         }
       } else {

@@ -18,7 +18,7 @@ struct alignas(64) TmaDesc {
 // A domain's tensor maps for the TMA z-march shapes, over its split arrays
 // as 4-D tensors (q, j, k, colour): the other colour's slab (a box of
 // 136 x (rows + 2)), the own colour's lambda and R (128 x rows), the mask.
-enum { kTmOther = 0, kTmOwn = 1, kTmR = 2, kTmMask = 3, kTmCount = 4 };
+enum { kTmOther = 0, kTmOwn = 1, kTmR = 2, kTmMask = 3, kTmCount = 4, kTmSlots = 4 };
 
 // One domain in the red/black split layout, as the sweep kernels see it.
 struct SweepDomain {

@@ -67,7 +67,9 @@ struct qesb_warmnet {
   std::vector<int> ch;
   std::vector<Layer> layers;  // file order
   int *d_err = nullptr;
-  unsigned *d_scale = nullptr;
+  unsigned *d_scale = nullptr;    // [nscale] max|R| per item of a call
+  int nscale = 0;
+  cudaEvent_t ev = nullptr;       // orders a batch's per-handle streams with the forward's stream
   std::map<std::tuple<int, int, int>, Buffers> bufs;
   std::vector<void *> owned;
   std::mutex mu;
@@ -128,38 +130,50 @@ struct qesb_warmnet {
     return QESB_OK;
   }
 
-  qesb_status conv(const Layer &L, const void *x1, const void *x2, int D, int H, int W, void *y, void *yf,
-                   void *stream)
+  qesb_status conv(const Layer &L, const void *x1, const void *x2, int items, int D, int H, int W, void *y,
+                   void *yf, void *stream)
   {
-    return qesb_conv3d(x1, L.c1, L.up1, x2, L.c2, D, H, W, 1, L.Bm, L.Kp, L.cout, y, yf, L.bias, L.relu, nullptr,
-                       d_err, stream);
+    return qesb_conv3d_items(x1, L.c1, L.up1, x2, L.c2, items, D, H, W, 1, L.Bm, L.Kp, L.cout, y, yf, L.bias,
+                             L.relu, nullptr, d_err, stream);
   }
 
-  // forward pass on b.x (net grid D x H x W) into b.y
-  qesb_status forward(Buffers &b, int D, int H, int W, void *s)
+  // forward pass on b.x (`items` net grids of D x H x W stacked along z) into b.y
+  qesb_status forward(Buffers &b, int items, int D, int H, int W, void *s)
   {
     for (int l = 0; l < nlev; ++l) {
       const int Dl = D >> l, Hl = H >> l, Wl = W >> l;
       const void *xin = b.x;
-      if (l > 0) {
-        CKS_FWD(qesb_net_pool2(b.e[l - 1], b.p[l], D >> (l - 1), H >> (l - 1), W >> (l - 1), ch[l - 1], s));
+      if (l > 0) {  // the items' depths are even: no 2x2x2 block spans two of them
+        CKS_FWD(qesb_net_pool2(b.e[l - 1], b.p[l], items * (D >> (l - 1)), H >> (l - 1), W >> (l - 1), ch[l - 1], s));
         xin = b.p[l];
       }
-      CKS_FWD(conv(layers[index('e', l, true)], xin, nullptr, Dl, Hl, Wl, b.ea[l], nullptr, s));
-      CKS_FWD(conv(layers[index('e', l, false)], b.ea[l], nullptr, Dl, Hl, Wl, b.e[l], nullptr, s));
+      CKS_FWD(conv(layers[index('e', l, true)], xin, nullptr, items, Dl, Hl, Wl, b.ea[l], nullptr, s));
+      CKS_FWD(conv(layers[index('e', l, false)], b.ea[l], nullptr, items, Dl, Hl, Wl, b.e[l], nullptr, s));
     }
     for (int l = nlev - 2; l >= 0; --l) {
       const int Dl = D >> l, Hl = H >> l, Wl = W >> l;
       const void *below = l == nlev - 2 ? (const void *)b.e[l + 1] : (const void *)b.d[l + 1];
-      CKS_FWD(conv(layers[index('d', l, true)], below, b.e[l], Dl, Hl, Wl, b.da[l], nullptr, s));
-      CKS_FWD(conv(layers[index('d', l, false)], b.da[l], nullptr, Dl, Hl, Wl, b.d[l], nullptr, s));
+      CKS_FWD(conv(layers[index('d', l, true)], below, b.e[l], items, Dl, Hl, Wl, b.da[l], nullptr, s));
+      CKS_FWD(conv(layers[index('d', l, false)], b.da[l], nullptr, items, Dl, Hl, Wl, b.d[l], nullptr, s));
     }
-    return conv(layers[index('h', 0, false)], b.d[0], nullptr, D, H, W, nullptr, b.y, s);
+    return conv(layers[index('h', 0, false)], b.d[0], nullptr, items, D, H, W, nullptr, b.y, s);
+  }
+
+  qesb_status ensure_scales(int n)
+  {
+    if (n <= nscale) return QESB_OK;
+    void *p = nullptr;
+    CKS_FWD(alloc(&p, sizeof(unsigned) * n));
+    d_scale = static_cast<unsigned *>(p);  // the old array stays owned until release
+    nscale = n;
+    return QESB_OK;
   }
 
   void release()
   {
     cudaSetDevice(device);
+    if (ev) cudaEventDestroy(ev);
+    ev = nullptr;
     for (void *p : owned) cudaFree(p);
     owned.clear();
     bufs.clear();
@@ -243,8 +257,9 @@ qesb_status qesb_warmnet_load(const char *path, int device, qesb_warmnet **out)
   }
   if ((s = net->alloc(&p, sizeof(int))) != QESB_OK) return fail(s);
   net->d_err = static_cast<int *>(p);
-  if ((s = net->alloc(&p, sizeof(unsigned))) != QESB_OK) return fail(s);
-  net->d_scale = static_cast<unsigned *>(p);
+  if ((s = net->ensure_scales(1)) != QESB_OK) return fail(s);
+  if (cudaEventCreateWithFlags(&net->ev, cudaEventDisableTiming) != cudaSuccess)
+    return fail(qesb_fail(QESB_ERR_CUDA, "qesb_warmnet_load: cudaEventCreate"));
   *out = net;
   return QESB_OK;
 }
@@ -257,11 +272,20 @@ qesb_status qesb_warmnet_destroy(qesb_warmnet *net)
   return QESB_OK;
 }
 
-qesb_status qesb_warm_start(qesb_handle *h, qesb_warmnet *net)
+qesb_status qesb_warm_start_batch(qesb_handle *const *hs, int n, qesb_warmnet *net)
 {
-  if (!h || !net) return qesb_fail(QESB_ERR_ARG, "qesb_warm_start: null argument");
+  if (!hs || n < 1 || !net) return qesb_fail(QESB_ERR_ARG, "qesb_warm_start: null argument");
   int Nx = 0, Ny = 0, Nz = 0, dev = -1;
-  CKS_FWD(qesb_handle_grid(h, &Nx, &Ny, &Nz, &dev));
+  for (int i = 0; i < n; ++i) {
+    if (!hs[i]) return qesb_fail(QESB_ERR_ARG, "qesb_warm_start: null handle %d", i);
+    int x = 0, y = 0, z = 0, d = -1;
+    CKS_FWD(qesb_handle_grid(hs[i], &x, &y, &z, &d));
+    if (i == 0) {
+      Nx = x, Ny = y, Nz = z, dev = d;
+    } else if (x != Nx || y != Ny || z != Nz || d != dev) {
+      return qesb_fail(QESB_ERR_ARG, "qesb_warm_start: handle %d's grid or device differs from handle 0's", i);
+    }
+  }
   if (dev != net->device)
     return qesb_fail(QESB_ERR_ARG, "qesb_warm_start: network on device %d, handle on device %d", net->device, dev);
   const int F = net->res << (net->nlev - 1);
@@ -269,23 +293,47 @@ qesb_status qesb_warm_start(qesb_handle *h, qesb_warmnet *net)
     return qesb_fail(QESB_ERR_ARG, "qesb_warm_start: grid %d x %d x %d not divisible by %d", Nx, Ny, Nz, F);
   std::lock_guard<std::mutex> lk(net->mu);
   if (cudaSetDevice(net->device) != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "qesb_warm_start: cudaSetDevice");
-  void *s = nullptr;
-  CKS_FWD(qesb_get_stream(h, &s));
+  std::vector<void *> st(n);
+  for (int i = 0; i < n; ++i) CKS_FWD(qesb_get_stream(hs[i], &st[i]));
+  void *s = st[0];
   const int D = Nz / net->res, H = Ny / net->res, W = Nx / net->res;
+  const size_t V0 = (size_t)D * H * W;
   Buffers *b = nullptr;
-  CKS_FWD(net->buffers(D, H, W, &b));
-  CKS_FWD(qesb_compute_divergence(h));
-  if (net->res == 1) CKS_FWD(qesb_warm_input(h, b->x, kInCh, net->d_scale));
-  else CKS_FWD(qesb_warm_input_half(h, b->x, kInCh, net->d_scale));
-  CKS_FWD(net->forward(*b, D, H, W, s));
-  CKS_FWD(net->res == 1 ? qesb_warm_apply(h, b->y, kHeadN, net->d_scale)
-                        : qesb_warm_apply_up2(h, b->y, kHeadN, net->d_scale));
+  CKS_FWD(net->buffers(n * D, H, W, &b));
+  CKS_FWD(net->ensure_scales(n));
+  auto join = [&](void *from, void *to) -> qesb_status {  // work on `to` after what `from` holds so far
+    if (from == to) return QESB_OK;
+    if (cudaEventRecord(net->ev, (cudaStream_t)from) != cudaSuccess ||
+        cudaStreamWaitEvent((cudaStream_t)to, net->ev, 0) != cudaSuccess)
+      return qesb_fail(QESB_ERR_CUDA, "qesb_warm_start: stream ordering");
+    return QESB_OK;
+  };
+  for (int i = 0; i < n; ++i) {  // each item's input on its handle's stream, then ordered before the forward
+    uint16_t *x = b->x + V0 * kInCh * i;
+    CKS_FWD(join(s, st[i]));
+    CKS_FWD(qesb_compute_divergence(hs[i]));
+    if (net->res == 1) CKS_FWD(qesb_warm_input(hs[i], x, kInCh, net->d_scale + i));
+    else CKS_FWD(qesb_warm_input_half(hs[i], x, kInCh, net->d_scale + i));
+    CKS_FWD(join(st[i], s));
+  }
+  CKS_FWD(net->forward(*b, n, D, H, W, s));
+  for (int i = 0; i < n; ++i) {
+    const float *y = b->y + V0 * kHeadN * i;
+    CKS_FWD(join(s, st[i]));
+    CKS_FWD(net->res == 1 ? qesb_warm_apply(hs[i], y, kHeadN, net->d_scale + i)
+                          : qesb_warm_apply_up2(hs[i], y, kHeadN, net->d_scale + i));
+  }
   int err = 0;
   if (cudaMemcpyAsync(&err, net->d_err, sizeof err, cudaMemcpyDeviceToHost, (cudaStream_t)s) != cudaSuccess ||
       cudaStreamSynchronize((cudaStream_t)s) != cudaSuccess)
     return qesb_fail(QESB_ERR_CUDA, "qesb_warm_start: %s", cudaGetErrorString(cudaGetLastError()));
+  for (int i = 0; i < n; ++i)
+    if (st[i] != s && cudaStreamSynchronize((cudaStream_t)st[i]) != cudaSuccess)
+      return qesb_fail(QESB_ERR_CUDA, "qesb_warm_start: %s", cudaGetErrorString(cudaGetLastError()));
   if (err) return qesb_fail(QESB_ERR_CUDA, "qesb_warm_start: a tensor-core completion wait gave up");
   return QESB_OK;
 }
+
+qesb_status qesb_warm_start(qesb_handle *h, qesb_warmnet *net) { return qesb_warm_start_batch(&h, 1, net); }
 
 }  // extern "C"

@@ -114,6 +114,7 @@ def lib() -> C.CDLL:
             "qesb_get_residual_history": ([V, V, C.c_int], C.c_int),
             "qesb_set_tolerance": ([V, C.c_float], C.c_int),
             "qesb_set_prephase": ([V, C.c_float, C.c_float, C.c_int], C.c_int),
+            "qesb_set_prephase_start": ([V, C.c_float, C.c_int], C.c_int),
             "qesb_set_window_rule": ([V, C.c_int, C.c_double], C.c_int),
             "qesb_fp64_same_sor": ([V, V, C.c_float, C.c_int, C.c_int, V, V, V, V, C.POINTER(Fp64Report)],
                                    C.c_int),
@@ -138,8 +139,11 @@ def lib() -> C.CDLL:
             "qesb_warmnet_load": ([C.c_char_p, C.c_int, C.POINTER(V)], C.c_int),
             "qesb_warmnet_destroy": ([V], C.c_int),
             "qesb_warm_start": ([V, V], C.c_int),
+            "qesb_warm_start_batch": ([C.POINTER(V), C.c_int, V], C.c_int),
             "qesb_conv3d": ([V, C.c_int, C.c_int, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, V,
                              C.c_int, C.c_int, V, V, V, C.c_int, V, V, V], C.c_int),
+            "qesb_conv3d_items": ([V, C.c_int, C.c_int, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                   V, C.c_int, C.c_int, V, V, V, C.c_int, V, V, V], C.c_int),
             "qesb_net_set_conv_path": ([C.c_int], C.c_int),
             "qesb_conv3d_wgrad": ([V, C.c_int, C.c_int, V, C.c_int, C.c_int, C.c_int, C.c_int, V, C.c_int,
                                    C.c_long, V, V, V], C.c_int),
@@ -326,6 +330,11 @@ class Solver_B200:
     def set_prephase(self, omega: float, tol: float = 1e-3, max_iterations: int = 10000):
         """Over-relaxed SOR pre-phase before the reference loop (omega 0: off)."""
         check(lib().qesb_set_prephase(self._h, float(omega), float(tol), int(max_iterations)))
+
+    def set_prephase_start(self, omega: float, iterations: int):
+        """Start stage of the pre-phase: its first `iterations` sweeps at this
+        omega (iterations 0: none)."""
+        check(lib().qesb_set_prephase_start(self._h, float(omega), int(iterations)))
 
     def set_window_rule(self, window: int, tol: float = 0.0):
         """Window stopping rule: the reference loop also stops after every

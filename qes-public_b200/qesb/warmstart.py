@@ -376,6 +376,12 @@ class WarmNet:
     def warm_start(self, solver: Solver_B200):
         check(lib().qesb_warm_start(solver._h, self._p))
 
+    def warm_start_batch(self, solvers):
+        """qesb_warm_start_batch: the starts of several solvers of one grid
+        shape in one forward pass (their inputs stacked along z)."""
+        arr = (C.c_void_p * len(solvers))(*[s._h for s in solvers])
+        check(lib().qesb_warm_start_batch(arr, len(solvers), self._p))
+
     def close(self):
         if self._p:
             lib().qesb_warmnet_destroy(self._p)

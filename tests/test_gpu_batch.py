@@ -119,6 +119,58 @@ def test_batch_prephase_per_domain():
     torch.cuda.synchronize()
 
 
+@pytest.mark.parametrize("variant", [-1, 51])
+def test_prephase_start_stage_single_and_batch(variant):
+    """A pre-phase start stage (its first sweeps at another omega): per
+    domain of a batch, with and without one, and in a single solve, the
+    oracle's three-phase solve bit for bit; pre_iterations counts the stage."""
+    ws = _cities()
+    tol = 1.1e-3
+    cfg = [((1.7, 12), (1.95, 1e-3, 4000)), (None, (1.9, 1e-3, 4000)), ((1.5, 5), (1.9, 2e-3, 60)), (None, None)]
+
+    def setup(s, w, c):
+        s.set_inputs(w)
+        if variant >= 0:
+            s.set_option("variant", variant)
+        if c[1]:
+            s.set_prephase(*c[1])
+        if c[0]:
+            s.set_prephase_start(*c[0])
+
+    def oracle(w, c):
+        d = w.domain
+        R = O.divergence(d, w)
+        lam, npre = None, 0
+        if c[1]:
+            if c[0]:
+                lam, n0, *_ = O.sor(d, w, R, -1.0, c[0][1], omega=c[0][0])
+                npre += n0
+            lam, n1, *_ = O.sor(d, w, R, c[1][1], c[1][2], omega=c[1][0], lam=lam)
+            npre += n1
+        Lo, it, *_ = O.sor(d, w, R, tol, 4000, lam=lam)
+        return npre, it, Lo
+
+    solvers = [qesb.Solver_B200(w.domain, tol) for w in ws]
+    try:
+        for s, w, c in zip(solvers, ws, cfg):
+            setup(s, w, c)
+        st = qesb.solve_batch(solvers, 4000)
+        lams = [s.lambda_ for s in solvers]
+    finally:
+        for s in solvers:
+            s.close()
+    for w, c, sti, L in zip(ws, cfg, st, lams):
+        npre, it, Lo = oracle(w, c)
+        assert sti["pre_iterations"] == npre and sti["iterations"] == it
+        np.testing.assert_array_equal(L, Lo)
+    with qesb.Solver_B200(ws[0].domain, tol) as s:
+        setup(s, ws[0], cfg[0])
+        st0 = s.solve(ws[0], 4000, set_inputs=False)
+        npre, it, Lo = oracle(ws[0], cfg[0])
+        assert st0["pre_iterations"] == npre and st0["iterations"] == it
+        np.testing.assert_array_equal(s.lambda_, Lo)
+
+
 def test_batch_autotune_keeps_lambda_and_results_exact():
     """qesb_autotune_batch times the sweep shapes on the batch's own domain
     list, leaves every lambda as it was, and the batch it tunes still gives

@@ -13,7 +13,10 @@ pytestmark = pytest.mark.gpu
 WIND_TOL = 1e-3
 
 
-def test_fp64_replay_matches_the_oracle_bit_for_bit():
+@pytest.mark.parametrize("start", [None, (1.6, 10)])
+def test_fp64_replay_matches_the_oracle_bit_for_bit(start):
+    """With a pre-phase start stage set, the replay runs it too: its first
+    sweeps at the stage's omega, as the FP32 solve did."""
     import torch
 
     d = qesb.Domain(72, 56, 24, 2.0, 2.0, 1.0, qesb.city_dz(24, 1.0, 1.03))
@@ -24,13 +27,17 @@ def test_fp64_replay_matches_the_oracle_bit_for_bit():
     with qesb.Solver_B200(d, 1e-9) as s:
         s.set_inputs(w)
         s.set_prephase(1.9, 3e-3, 2000)
+        if start:
+            s.set_prephase_start(*start)
         s.set_window_rule(16, 1e-2)
         st = s.solve_device(3000, *[t.data_ptr() for t in uvw])
         rep = s.fp64_same_sor(1.9, st["pre_iterations"], st["iterations"], *[t.data_ptr() for t in uvw],
                               want_lambda=True)
         lam32 = s.lambda_
     assert st["pre_iterations"] > 0 and st["converged"] == 2
-    u64, v64, w64, L64, _, _ = O.solve_f64(d, w, -1.0, st["iterations"], phases=[(1.9, -1.0, st["pre_iterations"])])
+    npre = st["pre_iterations"]
+    phases = [(start[0], -1.0, start[1]), (1.9, -1.0, npre - start[1])] if start else [(1.9, -1.0, npre)]
+    u64, v64, w64, L64, _, _ = O.solve_f64(d, w, -1.0, st["iterations"], phases=phases)
     np.testing.assert_array_equal(rep["lambda64"], L64)
     assert rep["lambda_max_abs"] == np.abs(L64).max()
     assert rep["lambda_max_abs_err"] == np.abs(lam32.astype(np.float64) - L64).max()

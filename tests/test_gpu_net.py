@@ -230,3 +230,39 @@ def test_conv3d_direct_input_gradient_with_relu_mask(ci, co):
     dev = "cuda:0"
     out = _run_conv(_cl(dy).to(dev), co, 0, None, 0, D, H, W, -1, bd.to(dev), kp, ci, mask=_cl(_bf16(x)).to(dev))
     np.testing.assert_allclose(out.numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.parametrize("D,H,W,c1,c2,co,up", [(4, 6, 128, 16, 0, 16, 0), (4, 6, 64, 32, 0, 32, 0),
+                                               (4, 6, 128, 32, 16, 16, 1), (2, 4, 32, 64, 64, 64, 1)])
+def test_conv3d_items_stack_along_z_without_crosstalk(D, H, W, c1, c2, co, up):
+    """qesb_conv3d_items: three grids stacked along z in one launch give, item
+    by item, the convolution of each grid alone (zero padding at every item's
+    z faces), against torch per item; direct and implicit-GEMM paths, with and
+    without an upsampled concatenated input."""
+    import torch
+    torch.manual_seed(D + H + W + c1 + co)
+    items, ci = 3, c1 + c2
+    x1 = [_bf16(torch.randn(1, c1, D // 2, H // 2, W // 2) if up else torch.randn(1, c1, D, H, W))
+          for _ in range(items)]
+    x2 = [_bf16(torch.randn(1, c2, D, H, W)) for _ in range(items)] if c2 else None
+    w = _bf16(torch.randn(co, ci, 3, 3, 3) / (27 * ci) ** 0.5)
+    b = torch.randn(co)
+    bm, kp = _bm_forward(w)
+    dev = "cuda:0"
+    x1d = torch.cat([_cl(t) for t in x1], 0).to(dev)
+    x2d = torch.cat([_cl(t) for t in x2], 0).to(dev) if c2 else None
+    bmd, bd = bm.to(dev), b.float().to(dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    yf = torch.zeros(items * D * H * W * co, dtype=torch.float32, device=dev)
+    g = lambda t: t.data_ptr() if t is not None else None  # noqa: E731
+    qesb.check(qesb.lib().qesb_conv3d_items(g(x1d), c1, up, g(x2d), c2, items, D, H, W, 1, g(bmd), kp, co, None,
+                                            g(yf), g(bd), 1, None, g(err), None))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    out = yf.view(items, D, H, W, co).cpu().double()
+    for i in range(items):
+        xin = torch.nn.functional.interpolate(x1[i].double(), scale_factor=2, mode="nearest") if up else x1[i].double()
+        if c2:
+            xin = torch.cat([xin, x2[i].double()], 1)
+        ref = torch.relu(torch.nn.functional.conv3d(xin, w.double(), b.double(), padding=1))
+        np.testing.assert_allclose(out[i].numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)

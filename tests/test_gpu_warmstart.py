@@ -234,6 +234,41 @@ def test_cabi_warm_start_matches_the_python_network():
     np.testing.assert_array_equal(lc2, lc)
 
 
+def test_cabi_warm_start_batch_matches_single_starts():
+    """qesb_warm_start_batch: three cities' inputs stacked along z, one
+    forward pass, each start the single call's (to the summation order of
+    split-K partial sums, which depends on the grid's size), none leaking
+    into another; a second batched call repeats the bits."""
+    from qesb import warmstart as ws
+
+    if not os.path.exists(ws.DEFAULT_WEIGHTS):
+        pytest.skip("no trained weights committed")
+    cities = [qesb.random_city("city128", 1001 + i)[0] for i in range(3)]
+    solvers = [qesb.Solver_B200(w.domain, RULE_TOL) for w in cities]
+    cnet = ws.WarmNet(ws.DEFAULT_WEIGHTS, device=0)
+    try:
+        for s, w in zip(solvers, cities):
+            s.set_inputs(w)
+        single = []
+        for s in solvers:
+            cnet.warm_start(s)
+            single.append(s.lambda_)
+            s.resetLambda()
+        cnet.warm_start_batch(solvers)
+        batch = [s.lambda_ for s in solvers]
+        cnet.warm_start_batch(solvers)
+        again = [s.lambda_ for s in solvers]
+    finally:
+        cnet.close()
+        for s in solvers:
+            s.close()
+    for a, b, c in zip(single, batch, again):
+        assert np.abs(a).max() > 0
+        np.testing.assert_array_equal(b, c)
+        assert np.abs(a - b).max() <= 1e-3 * np.abs(a).max()
+    assert np.abs(batch[0] - batch[1]).max() > 1e-2 * np.abs(batch[0]).max()
+
+
 def test_cabi_warm_start_rejects_grids_it_cannot_pool():
     from qesb import warmstart as ws
 

@@ -70,6 +70,15 @@ PRE_TOL = 2e-3
 HEADLINE = "network+prephase"  # the metric's method: the learned start, then the pre-phase
 ARMS = {"plain": (False, False), "prephase": (False, True), "network": (True, False),
         "network+prephase": (True, True)}
+# After the network's start the pre-phase begins with a few sweeps at a smaller
+# omega (qesb_set_prephase_start), which damp the start's rough, wall-adjacent
+# error before the over-relaxation amplifies it; from lambda = 0 there is
+# nothing rough to damp and the pre-phase starts at once.
+START_STAGE = (1.8, 8)
+
+
+def start_stage(use_net, use_pre):
+    return START_STAGE if use_net and use_pre else (0.0, 0)
 
 
 def parse(argv=None):
@@ -392,6 +401,7 @@ def precision_device(s, outs, use_net, use_pre, net=None, omega=PRE_OMEGA):
     import torch
 
     s.set_prephase(omega if use_pre else 0.0, PRE_TOL, ITERMAX)
+    s.set_prephase_start(*start_stage(use_net, use_pre))
     if use_net:
         net.warm_start(s)
         lam0 = s.lambda_
@@ -616,15 +626,16 @@ def run_b200(args):
     # per batched start: R, input (2), apply per domain; convolutions and poolings once
     launches_per_net = 4 * B + (4 * net.nlev - 1) + (net.nlev - 1)
 
-    def set_arm(sset, use_pre):
+    def set_arm(sset, use_net, use_pre):
         for s in sset:
             s.set_prephase(PRE_OMEGA if use_pre else 0.0, PRE_TOL, ITERMAX)
+            s.set_prephase_start(*start_stage(use_net, use_pre))
 
     def batch_step(use_net, use_pre, sset=None, ptrs=None, strm=None):
         sset, ptrs, strm = sset or solvers, ptrs or uvw, strm or stream
 
         def step():
-            set_arm(sset, use_pre)
+            set_arm(sset, use_net, use_pre)
             if use_net:
                 cnet.warm_start_batch(sset)
             else:
@@ -965,9 +976,11 @@ def run_b200(args):
                        "sweep_variant": variant, "batch_variant": batch_variant,
                        "parallelism": f"replicas x{world}",
                        "warm_start": f"the learned network's prediction (BF16 tcgen05 convolutions, half "
-                                     f"resolution), then the pre-phase: red-black SOR at omega {PRE_OMEGA} to "
-                                     f"max|dlambda| <= {PRE_TOL}; then the reference loop (omega 1.78) to the "
-                                     f"rule; arms holds plain SOR, the pre-phase alone and the network alone",
+                                     f"resolution, the batch's inputs stacked in one forward pass), then the "
+                                     f"pre-phase: {START_STAGE[1]} red-black sweeps at omega {START_STAGE[0]}, "
+                                     f"then omega {PRE_OMEGA} to max|dlambda| <= {PRE_TOL}; then the reference "
+                                     f"loop (omega 1.78) to the rule; arms holds plain SOR, the pre-phase alone "
+                                     f"and the network alone",
                        "learned_start_note": learned_note,
                        "l2": "8 domains x ~40 MB packed sweep data + network buffers > L2 (126 MB) per step"},
             "arms": arms,
@@ -1177,6 +1190,7 @@ def run_profile_batch(args):
             s.set_inputs(w)
             s.set_window_rule(WINDOW, WINDOW_TOL)
             s.set_prephase(PRE_OMEGA if use_pre else 0.0, PRE_TOL, ITERMAX)
+            s.set_prephase_start(*start_stage(use_net, use_pre))
         if args.variant >= 0:
             solvers[0].set_option("variant", args.variant)
         nf = cities[0].domain.numFaceCentered()
@@ -1200,21 +1214,27 @@ def run_profile_batch(args):
 
 
 def run_forward_only(args):
-    """Warm-start forward passes on one domain, for network captures."""
+    """Batched learned starts (qesb_warm_start_batch over the B cities of the
+    headline batch, one forward pass each), for network captures."""
     import torch
 
     import qesb
     from qesb import warmstart as ws
 
-    w = make_city(args.workload, SEED0 if args.workload == WORKLOAD else 0)
-    net = ws.WarmStartNet.from_file(args.weights or ws.DEFAULT_WEIGHTS, device=0)
-    with qesb.Solver_B200(w.domain, TOL) as s:
-        s.set_inputs(w)
+    cities = [make_city(args.workload, SEED0 + i) for i in range(args.batch)]
+    solvers = [qesb.Solver_B200(w.domain, TOL) for w in cities]
+    net = ws.WarmNet(args.weights or ws.DEFAULT_WEIGHTS, device=0)
+    try:
+        for s, w in zip(solvers, cities):
+            s.set_inputs(w)
         for _ in range(args.forward_only):
-            net.warm_start(s)
+            net.warm_start_batch(solvers)
         torch.cuda.synchronize()
-        net.check_err()
-    print(json.dumps({"forward_only": args.forward_only}))
+    finally:
+        net.close()
+        for s in solvers:
+            s.close()
+    print(json.dumps({"forward_only": args.forward_only, "batch": args.batch}))
 
 
 def main():

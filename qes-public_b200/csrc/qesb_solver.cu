@@ -1006,6 +1006,7 @@ struct SweepVariant {
   void (*red_m)(SweepArgs);  // domain lists
   void (*black_m)(SweepArgs);
   int tma = 0;  // z-march shapes staged by tensor-map copies: the domains need their tensor maps
+  int bal = 0;  // z-march shapes with equal plane-step shares per CTA (units of one plane: kc = 1)
 };
 // MINB: resident CTAs per SM the compiler must allow (caps registers per
 // thread); the default allows 512 threads per SM (at most 128 registers)
@@ -1048,7 +1049,7 @@ constexpr SweepVariant make_bulk(const char *name)
                       k_sor_bulk<0, W, NS, ASYNC, true>,
                       k_sor_bulk<1, W, NS, ASYNC, true>};
 }
-template <int TY, int RW, int MINB, int DIST = 2, int TMA = 0>
+template <int TY, int RW, int MINB, int DIST = 2, int TMA = 0, int BAL = 0>
 constexpr SweepVariant make_zm(const char *name)
 {
   return SweepVariant{name,
@@ -1056,11 +1057,12 @@ constexpr SweepVariant make_zm(const char *name)
                       TY,
                       TY * RW,
                       zm_smem_bytes<TY * RW, DIST, TMA>(),
-                      k_sor_zm<0, TY, RW, DIST, false, MINB, TMA>,
-                      k_sor_zm<1, TY, RW, DIST, false, MINB, TMA>,
-                      k_sor_zm<0, TY, RW, DIST, true, MINB, TMA>,
-                      k_sor_zm<1, TY, RW, DIST, true, MINB, TMA>,
-                      TMA};
+                      k_sor_zm<0, TY, RW, DIST, false, MINB, TMA, BAL>,
+                      k_sor_zm<1, TY, RW, DIST, false, MINB, TMA, BAL>,
+                      k_sor_zm<0, TY, RW, DIST, true, MINB, TMA, BAL>,
+                      k_sor_zm<1, TY, RW, DIST, true, MINB, TMA, BAL>,
+                      TMA,
+                      BAL};
 }
 const SweepVariant kSweepVariants[] = {
     // streaming split kernels (option "variant" 5..17)
@@ -1093,6 +1095,9 @@ const SweepVariant kSweepVariants[] = {
     make_zm<4, 2, 5, 1, 1>("zmt_y4x2_b5"), make_zm<4, 2, 4, 1, 1>("zmt_y4x2_b4"), make_zm<2, 2, 8, 1, 1>("zmt_y2x2_b8"),
     make_zm<8, 2, 2, 1, 1>("zmt_y8x2_b2"), make_zm<4, 4, 2, 1, 1>("zmt_y4x4_b2"),
     make_zm<4, 2, 3, 2, 1>("zmt_y4x2_d2_b3"), make_zm<4, 2, 4, 2, 1>("zmt_y4x2_d2_b4"),
+    // the same with equal plane-step shares per CTA (58..60)
+    make_zm<4, 2, 4, 2, 1, 1>("zmtb_y4x2_d2_b4"), make_zm<4, 2, 5, 1, 1, 1>("zmtb_y4x2_b5"),
+    make_zm<4, 2, 4, 1, 1, 1>("zmtb_y4x2_b4"),
 };
 constexpr int kNumSweep = sizeof(kSweepVariants) / sizeof(kSweepVariants[0]);
 constexpr int kSplitVariant = kNumVariants;  // option "variant" index of the first sweep shape
@@ -1125,6 +1130,13 @@ int sweep_ctas(const SweepVariant &sv, bool multi, int device)
 void sweep_tiles(std::vector<SweepDomain> &doms, const SweepVariant &sv, bool multi, int device)
 {
   if (sv.unit != kUnitTile) return;
+  if (sv.bal) {  // units of one plane of a tile column; the kernel splits them evenly over its CTAs
+    for (SweepDomain &d : doms) {
+      d.tile_y = sv.tile_rows;
+      d.kc = 1;
+    }
+    return;
+  }
   const long ctas = sweep_ctas(sv, multi, device);
   int best = 4;
   long best_cost = -1;

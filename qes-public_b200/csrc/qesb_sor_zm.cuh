@@ -241,8 +241,12 @@ template <int N>
 __device__ __forceinline__ int zm_wrap(int x) { return x >= N ? x - N : x; }
 
 // TY warps per CTA, RW rows per warp (rows w, w + TY, ...): tiles of TY x RW rows;
-// copies DIST planes ahead.
-template <int COLOUR, int TY, int RW, int DIST, bool MULTI, int MINB, int TMA = 0>
+// copies DIST planes ahead. BAL = 1: the list's units are single planes of a
+// tile column (kc = 1, planes fastest) and each CTA takes an equal share of
+// them, walked as runs of consecutive planes, so every CTA does the same
+// number of plane steps whatever the list's size (one or two runs each, each
+// run paying its own pipeline start).
+template <int COLOUR, int TY, int RW, int DIST, bool MULTI, int MINB, int TMA = 0, int BAL = 0>
 __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
 {
   constexpr int TR = TY * RW, NT = 32 * TY, NSO = zm_other_slots(DIST), NSW = zm_own_slots(DIST);
@@ -268,7 +272,10 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
   const int total = MULTI ? b.uoff[na] : sweep_units(b.one, kUnitTile);
   SplitDom D;
   int slot = -1, lo = 0, hi = 0;
-  for (int u = blockIdx.x; u < total; u += gridDim.x) {
+  const int ub = BAL ? (int)((long)total * blockIdx.x / gridDim.x) : (int)blockIdx.x;
+  const int ue = BAL ? (int)((long)total * (blockIdx.x + 1) / gridDim.x) : total;
+  int unext = ub;
+  for (int u = ub; u < ue; u = unext) {
     if (!MULTI) {
       if (slot < 0) {
         slot = 0;
@@ -289,14 +296,27 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
       }
     }
     const SweepDomain &SD = sweep_dom<MULTI>(b, slot);
-    const int njt = (D.Y - 2 + TR - 1) / TR, kc = SD.kc;
+    const int njt = (D.Y - 2 + TR - 1) / TR;
     const int nch = SD.nch;
-    int t = u - lo;
-    const int qt = t % nch;
-    t /= nch;
-    const int jt = t % njt, kt = t / njt;
-    const int q0 = qt * kZmQ, j0 = 1 + jt * TR, k0 = 1 + kt * kc;
-    const int k1 = min(k0 + kc, D.Z - 1);
+    int qt, jt, k0, k1;
+    if constexpr (BAL) {  // planes fastest: a run of this column's planes, to the column's end or the share's
+      const int P = D.Z - 2, t = u - lo, kt = t % P, col = t / P;
+      qt = col % nch;
+      jt = col / nch;
+      k0 = 1 + kt;
+      k1 = 1 + min(P, kt + (ue - u));
+      unext = u + (k1 - k0);
+    } else {
+      const int kc = SD.kc;
+      int t = u - lo;
+      qt = t % nch;
+      t /= nch;
+      jt = t % njt;
+      k0 = 1 + (t / njt) * kc;
+      k1 = min(k0 + kc, D.Z - 1);
+      unext = u + (int)gridDim.x;
+    }
+    const int q0 = qt * kZmQ, j0 = 1 + jt * TR;
     const int q = q0 + 4 * lane;
     const int qn = (D.X + 1) >> 1;
     ZmCopies<TR, NT> cp;

@@ -11,7 +11,8 @@ held-out 256 x 256 x 64 cities (seeds 500000 + i, disjoint from training),
 each solved to the benchmark's stopping rule (the reference's tol 1e-9 and
 itermax 10000, plus the window rule: 32 iterations, 4e-3) in four arms: plain
 SOR from lambda = 0, the network's start, the over-relaxed pre-phase, the
-network's start then the pre-phase; reports each arm's iterations and device
+network's start then the pre-phase (beginning with START_STAGE's sweeps at
+a smaller omega); reports each arm's iterations and device
 ms (network included), and its largest wind difference from the converged
 field. --eval-only WEIGHTS evaluates a trained network without training.
 Writes DIR/warmstart_city.qwn (weights, the library format qesb_warmnet_load reads) and
@@ -36,6 +37,7 @@ from qesb import warmstart as ws  # noqa: E402
 TRAIN_SEED0, EVAL_SEED0 = 1000, 500000
 TOL, ITERMAX, WINDOW, WINDOW_TOL = 1e-9, 10000, 32, 4e-3
 PRE_OMEGA, PRE_TOL = 1.97, 2e-3
+START_STAGE = (1.8, 8)  # the pre-phase's first sweeps after the network's start (the benchmark's setting)
 
 
 def converge(solver, w, omega, pre_iters, ref_iters=1000):
@@ -162,6 +164,7 @@ def evaluate(net, n, workload):
         for arm, (use_net, use_pre) in {"plain": (0, 0), "network": (1, 0), "prephase": (0, 1),
                                         "network+prephase": (1, 1)}.items():
             solver.set_prephase(PRE_OMEGA if use_pre else 0.0, PRE_TOL, ITERMAX)
+            solver.set_prephase_start(*(START_STAGE if use_net and use_pre else (0.0, 0)))
             solver.resetLambda()
             torch.cuda.synchronize()
             ev[0].record(torch.cuda.ExternalStream(solver.stream_ptr()))
@@ -234,7 +237,9 @@ def main():
     rows = evaluate(net, args.eval, args.eval_workload)
     report["eval"] = {"n": args.eval, "workload": args.eval_workload, "seeds": [EVAL_SEED0, EVAL_SEED0 + args.eval - 1],
                       "rule": {"tol": TOL, "itermax": ITERMAX, "window": WINDOW, "window_tol": WINDOW_TOL},
-                      "prephase": {"omega": PRE_OMEGA, "tol": PRE_TOL}, "summary": summary(rows), "rows": rows}
+                      "prephase": {"omega": PRE_OMEGA, "tol": PRE_TOL,
+                                   "start_stage_after_network": list(START_STAGE)},
+                      "summary": summary(rows), "rows": rows}
     json.dump(report, open(os.path.join(args.out, "warmstart_report.json"), "w"), indent=1)
     print(json.dumps(report["eval"]["summary"]))
 

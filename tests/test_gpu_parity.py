@@ -54,8 +54,8 @@ def test_divergence_R_bit_exact(golden):
 # fused tile shapes (0-4), scalar split (5-10), float4 split (11-13),
 # window-order split (14-17), bulk-copy staged (18-22), cp.async staged (23-27),
 # register-capped split (28-35), window-order split with prefetch (36-39),
-# z-march (40-50), z-march staged by tensor-map copies (51-57)
-N_VARIANTS = 58
+# z-march (40-50), z-march staged by tensor-map copies (51-57; 58-60 with equal plane-step shares per CTA)
+N_VARIANTS = 61
 ZM = 40  # first z-march variant
 BULK = 18
 

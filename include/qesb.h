@@ -384,8 +384,14 @@ qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *x2, int c2,
 qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const void *x2, int c2, int items, int D,
                               int H, int W, int sign, const void *Bm, int Kp, int N, void *y, void *yf,
                               const float *bias, int relu, const void *mask, int *err, void *stream);
-/* Process-wide choice of the qesb_conv3d kernel: 0 = direct kernel where it
- * applies (default), 1 = implicit GEMM everywhere (for comparison). */
+/* Process-wide choice of the qesb_conv3d kernel: 0 = the default (the
+ * z-marching direct kernel for forward convolutions of one 16-channel input
+ * without mask on grids with W a multiple of 128: input planes staged once by
+ * tensor-map copies, MMAs of one plane overlapping the read-out of the
+ * previous; else the direct kernel where it applies; else the implicit GEMM),
+ * 1 = implicit GEMM everywhere, 2 = the direct kernel but not the z-marching
+ * one, 3 / 4 = the z-marching kernel with 2 / 4 output rows per CTA (4 is the
+ * default's) - for comparison. */
 qesb_status qesb_net_set_conv_path(int path);
 /* Weight gradient dW[tap*(c1+c2) + c][n] += sum_v X[v + offset(tap)][c] * dY[v][n]
  * (FP32, accumulated with atomics: zero it first); X as in qesb_conv3d,

@@ -1,5 +1,6 @@
 // Learned warm start: tensor-core kernels (tcgen05, BF16 operands, FP32
 // accumulation in TMEM) for the 3D-convolution network, and their C ABI.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <mutex>
@@ -463,6 +464,201 @@ __global__ void __launch_bounds__(128) k_conv_direct(ConvIn in, ConvGeom g, int 
   }
 }
 
+// z-marching direct convolution for 16-channel inputs on grids whose x rows
+// are multiples of 128 voxels (the network's half-resolution level 0). A CTA
+// owns 128 consecutive x positions of TY output rows and marches along z
+// through up to ZC output planes of one item. Each input plane of
+// (TY + 2) rows x 130 voxels (the x and y halos) arrives once, by two
+// tensor-map copies (channels 0-7 and 8-15; zeros outside the grid), into a
+// ring of four plane slots laid out as
+//     byte cg * CG + (r * 130 + xi) * 16,   cg = channel group of 8,
+// so that, as in k_conv_direct, every tap (dz, dy, dx) of output row r is a
+// canonical K-major 128 x 16 A operand starting at row r + 1 + dy, voxel
+// 1 + dx of the slot of plane z + dz (SBO 128 B, LBO CG). Taps reaching past
+// the item's z faces are not issued (zero padding). Lane 0 of warp r issues
+// the 27 MMAs of output row r of a plane into one of two TMEM accumulator
+// sets and commits them to that set's mbarrier (TY arrivals); while they run,
+// thread 0 refills the slot the previous plane's MMAs have released (two
+// planes ahead) and the four warps read the previous plane's accumulators out
+// (bias, ReLU, store). Every wait is bounded; a CTA that gives up lets its
+// copies and MMAs finish, flags *err and stops.
+constexpr int kZdX = 130;  // staged voxels per row: x0 - 1 .. x0 + 128
+
+template <int TY>
+__host__ __device__ constexpr uint32_t zd_cg_bytes()
+{
+  return ((TY + 2) * kZdX * 16 + 127) / 128 * 128;
+}
+
+template <int N, int TY>
+__host__ __device__ constexpr uint32_t zd_smem_bytes()
+{
+  return 4 * 2 * zd_cg_bytes<TY>() + 27 * N * 32;
+}
+
+template <int N, int TY>
+__global__ void __launch_bounds__(128, 1) k_conv_zdirect(const __grid_constant__ CUtensorMap xmap, ConvGeom g, int ZC,
+                                                         const __nv_bfloat16 *__restrict__ Bm, int Kp, ConvOut out,
+                                                         int *err)
+{
+  constexpr uint32_t CG = zd_cg_bytes<TY>(), SLOT = 2 * CG, PLANE_TX = 2u * (TY + 2) * kZdX * 16;
+  constexpr uint32_t NCOLS = 2 * TY * N <= 32 ? 32 : 2 * TY * N <= 64 ? 64 : 2 * TY * N <= 128 ? 128 : 256;
+  static_assert(2 * TY * N <= 256, "two accumulator sets exceed the TMEM columns allocated");
+  extern __shared__ __align__(1024) uint8_t sm[];
+  __shared__ __align__(8) uint64_t full[4];  // plane slot s: its copies (or a plain arrival) of plane i, i % 4 == s
+  __shared__ __align__(8) uint64_t mmab[2];  // accumulator set b: the MMAs of plane step t, t % 2 == b (TY issuers)
+  __shared__ __align__(8) uint64_t mdrain;
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nzc = (g.Dc + ZC - 1) / ZC;
+  const int item = blockIdx.z / nzc, zlo = item * g.Dc, zhi = zlo + g.Dc;
+  const int z0 = zlo + (blockIdx.z % nzc) * ZC, z1 = min(z0 + ZC, zhi), nz = z1 - z0;
+  const int x0 = blockIdx.x * 128, y0 = blockIdx.y * TY;
+  uint8_t *sb = sm + 4 * SLOT;
+  if (umma::smem_u32(sm) & 127u) {  // tensor copies need 128-byte aligned slots
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+  if (warp == 0) umma::tmem_alloc(&tmem_base, NCOLS);
+  if (tid == 0) {
+    for (int q = 0; q < 4; ++q) umma::mbar_init(&full[q], 1);
+    umma::mbar_init(&mmab[0], TY);
+    umma::mbar_init(&mmab[1], TY);
+    umma::mbar_init(&mdrain, TY);
+    umma::fence_mbar_init();
+  }
+  // the weights of the 27 taps (K = 16), canonical K-major: tap t, row n, k-group kg
+  for (int idx = tid; idx < 27 * N * 2; idx += 128) {
+    const int t = idx / (N * 2), rem = idx - t * N * 2, n = rem >> 1, kg = rem & 1;
+    cp16_zfill(sb + t * N * 32 + (n >> 3) * 256 + kg * 128 + (n & 7) * 16, Bm + (long)n * Kp + t * 16 + 8 * kg, true);
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  umma::fence_smem_async();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+  constexpr uint32_t idesc = umma::idesc_bf16(128, N, 0, 0);
+  const uint32_t a0 = umma::smem_u32(sm), b0 = umma::smem_u32(sb);
+  // plane index i is z = z0 - 1 + i, in slot i % 4; planes outside the item
+  // (or past z1) get a plain arrival instead of copies
+  int issued = 0, landed = 0;
+  auto issue = [&](int i) {
+    const int z = z0 - 1 + i;
+    uint64_t *bar = &full[i & 3];
+    if (z < zlo || z >= zhi || z > z1) {
+      umma::mbar_arrive(bar);
+    } else {
+      umma::mbar_expect_tx(bar, PLANE_TX);
+      uint8_t *dst = sm + (i & 3) * SLOT;
+      umma::tma_load4(dst, &xmap, 0, x0 - 1, y0 - 1, z, bar);
+      umma::tma_load4(dst + CG, &xmap, 8, x0 - 1, y0 - 1, z, bar);
+    }
+  };
+  if (tid == 0)
+    for (; issued < 3; ++issued) issue(issued);
+  bool ok = true;
+  auto epilogue = [&](int t) {  // output plane z0 + t from accumulator set t % 2
+    const int z = z0 + t, x = x0 + warp * 32 + lane;
+    for (int r = 0; r < TY; ++r) {
+      const int y = y0 + r;
+      if (y >= g.H) break;  // warp-uniform
+      const long v = ((long)z * g.H + y) * g.W + x;
+      for (int c0 = 0; c0 < N; c0 += 8) {
+        float f[8];
+        umma::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((t & 1) * TY * N + r * N + c0), f);
+        if (out.bias) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) f[q] += __ldg(out.bias + c0 + q);
+        }
+        if (out.relu) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) f[q] = fmaxf(f[q], 0.0f);
+        }
+        if (out.yf) {
+          float4 *dst = reinterpret_cast<float4 *>(out.yf + v * N + c0);
+          dst[0] = make_float4(f[0], f[1], f[2], f[3]);
+          dst[1] = make_float4(f[4], f[5], f[6], f[7]);
+        } else {
+          uint4 pk;
+          __nv_bfloat162 *h2 = reinterpret_cast<__nv_bfloat162 *>(&pk);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) h2[q] = __floats2bfloat162_rn(f[2 * q], f[2 * q + 1]);
+          *reinterpret_cast<uint4 *>(out.y + v * N + c0) = pk;
+        }
+      }
+    }
+  };
+  const bool issuer = warp < TY && lane == 0;  // issues output row r = warp
+  // descriptors of the tap (dz, dy, dx) = (0, -1, -1) of row `warp` in slot 0 and of tap 0's weights;
+  // the other taps and slots are fixed offsets from them (16-byte units in the address field)
+  const uint64_t ad0 = umma::desc(a0 + (uint32_t)(warp * kZdX) * 16, CG, 128);
+  const uint64_t bd0 = umma::desc(b0, 128, 256);
+  for (int t = 0; t < nz; ++t) {
+    const int z = z0 + t;
+    if (issuer) {
+      for (; ok && landed <= t + 2; ++landed) ok = umma::mbar_wait(&full[landed & 3], (landed >> 2) & 1, kWaitLimit);
+      if (ok) {
+        umma::fence_after_sync();
+        const uint32_t acc = tmem + (uint32_t)((t & 1) * TY * N + warp * N);
+        uint32_t first = 1;
+        int tap = 0;
+        for (int dz = -1; dz <= 1; ++dz) {
+          if (z + dz < zlo || z + dz >= zhi) {
+            tap += 9;
+            continue;
+          }
+          const uint64_t as = ad0 + (uint64_t)(((t + 1 + dz) & 3) * (SLOT >> 4));
+          for (int dy = 0; dy < 3; ++dy)
+            for (int dx = 0; dx < 3; ++dx, ++tap) {
+              const uint64_t ad = as + (uint64_t)((dy * kZdX + dx) * 1);  // 16-byte units: one voxel
+              const uint64_t bd = bd0 + (uint64_t)(tap * N * 2);          // tap * N * 32 bytes
+              umma::mma_bf16(acc, ad, bd, idesc, first ? 0u : 1u);
+              first = 0;
+            }
+        }
+        umma::mma_commit(&mmab[t & 1]);
+      }
+    }
+    // thread 0 refills the slot step t - 1's MMAs read last (plane index t - 1) with plane index t + 3
+    if (tid == 0 && ok && issued <= nz + 1) {
+      if (t >= 1) ok = umma::mbar_wait(&mmab[(t - 1) & 1], ((t - 1) >> 1) & 1, kWaitLimit);
+      if (ok) issue(issued++);
+    }
+    if (t >= 1 && ok) {
+      ok = umma::mbar_wait(&mmab[(t - 1) & 1], ((t - 1) >> 1) & 1, kWaitLimit);
+      umma::fence_after_sync();
+      if (ok) epilogue(t - 1);
+    }
+    umma::fence_before_sync();
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      break;
+    }
+    umma::fence_after_sync();
+  }
+  if (ok && nz > 0) {
+    ok = umma::mbar_wait(&mmab[(nz - 1) & 1], ((nz - 1) >> 1) & 1, kWaitLimit);
+    umma::fence_after_sync();
+    if (ok) epilogue(nz - 1);
+  }
+  if (__syncthreads_or(!ok)) {
+    // a wait gave up: let every issued copy land and every issued MMA finish before TMEM and the slots go
+    if (tid == 0) {
+      atomicExch(err, 1);
+      for (; landed < issued; ++landed) umma::mbar_wait(&full[landed & 3], (landed >> 2) & 1, kWaitLimit);
+    }
+    umma::mma_drain(&mdrain, issuer, kWaitLimit);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, NCOLS);
+  }
+}
+
 // Weight gradient: dW[t*cin + c][n] += sum_v X[v + off(t)][c] * dY[v][n] over
 // this CTA's voxel range. M-tile = 128 rows of (t, c); K = voxels in chunks
 // of 64; both operands MN-major (channels contiguous). Partial sums from the
@@ -647,7 +843,8 @@ qesb_status launch_conv(const ConvIn &in, const ConvGeom &g, int sign, const __n
   return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));
 }
 
-int g_conv_path = 0;  // 0: direct kernel where it applies, 1: implicit GEMM only
+int g_conv_path = 0;  // 0: z-marching / direct kernels where they apply, 1: implicit GEMM only,
+                      // 2: direct kernel (not the z-marching one), 3 / 4: z-marching with 2 / 4 rows per CTA
 
 template <int N>
 qesb_status launch_conv_direct(const ConvIn &in, const ConvGeom &g, int sign, const __nv_bfloat16 *Bm, int Kp,
@@ -664,6 +861,61 @@ qesb_status launch_conv_direct(const ConvIn &in, const ConvGeom &g, int sign, co
   }
   const dim3 grid(g.W / 128, (g.H + kDirTY - 1) / kDirTY, (g.D + kDirTZ - 1) / kDirTZ);
   k_conv_direct<N><<<grid, 128, smem, s>>>(in, g, sign, Bm, Kp, out, err);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled()
+{
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess && p &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+template <int N, int TY>
+qesb_status launch_conv_zdirect(const ConvIn &in, const ConvGeom &g, const __nv_bfloat16 *Bm, int Kp,
+                                const ConvOut &out, int *err, cudaStream_t s)
+{
+  constexpr int smem = (int)zd_smem_bytes<N, TY>();
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  static bool attr[64] = {};
+  if (!attr[dev & 63]) {
+    cudaError_t e = cudaFuncSetAttribute(k_conv_zdirect<N, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv attr: %s", cudaGetErrorString(e));
+    attr[dev & 63] = true;
+  }
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return qesb_fail(QESB_ERR_CUDA, "cuTensorMapEncodeTiled not available");
+  // the input as a 4-D tensor (channel, x, y, z over all items), boxes of
+  // 8 channels x 130 voxels x (TY + 2) rows x 1 plane; zeros outside
+  const cuuint64_t dims[4] = {16, (cuuint64_t)g.W, (cuuint64_t)g.H, (cuuint64_t)g.D};
+  const cuuint64_t strides[3] = {32, (cuuint64_t)g.W * 32, (cuuint64_t)g.W * g.H * 32};
+  const cuuint32_t box[4] = {8, (cuuint32_t)kZdX, (cuuint32_t)(TY + 2), 1}, one[4] = {1, 1, 1, 1};
+  CUtensorMap map;
+  const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(in.x1), dims, strides,
+                         box, one, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return qesb_fail(QESB_ERR_CUDA, "conv tensor map: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  // z chunks: whole items unless that leaves fewer than two CTAs per SM slot
+  const int per_sm = smem <= 110 * 1024 ? 2 : 1;
+  const long xy = (long)(g.W / 128) * ((g.H + TY - 1) / TY), items = g.D / g.Dc;
+  int zc = g.Dc;
+  while (zc > 2 && xy * items * ((g.Dc + zc - 1) / zc) < 2L * sms * per_sm) zc = (zc + 1) / 2;
+  const dim3 grid(g.W / 128, (g.H + TY - 1) / TY, (unsigned)(items * ((g.Dc + zc - 1) / zc)));
+  k_conv_zdirect<N, TY><<<grid, 128, smem, s>>>(map, g, zc, Bm, Kp, out, err);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));
 }
@@ -747,7 +999,15 @@ extern "C" qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const 
             static_cast<const __nv_bfloat16 *>(mask)};
   const auto *B = static_cast<const __nv_bfloat16 *>(Bm);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (g_conv_path == 0 && W % 128 == 0 && (N == 16 || N == 32)) {
+  const bool zd = (g_conv_path == 0 || g_conv_path == 3 || g_conv_path == 4) && W % 128 == 0 &&
+                  (N == 16 || N == 32) && c1 == 16 && c2 == 0 && !up1 && sign == 1 && !mask &&
+                  reinterpret_cast<uintptr_t>(x1) % 16 == 0;
+  if (zd) {
+    if (g_conv_path == 3)
+      return N == 16 ? launch_conv_zdirect<16, 2>(in, g, B, Kp, o, err, s) : launch_conv_zdirect<32, 2>(in, g, B, Kp, o, err, s);
+    return N == 16 ? launch_conv_zdirect<16, 4>(in, g, B, Kp, o, err, s) : launch_conv_zdirect<32, 4>(in, g, B, Kp, o, err, s);
+  }
+  if ((g_conv_path == 0 || g_conv_path >= 2) && W % 128 == 0 && (N == 16 || N == 32)) {
     if (N == 16) return launch_conv_direct<16>(in, g, sign, B, Kp, o, err, s);
     return launch_conv_direct<32>(in, g, sign, B, Kp, o, err, s);
   }
@@ -768,7 +1028,7 @@ extern "C" qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *
 
 extern "C" qesb_status qesb_net_set_conv_path(int path)
 {
-  if (path != 0 && path != 1) return qesb_fail(QESB_ERR_ARG, "qesb_net_set_conv_path: path must be 0 or 1");
+  if (path < 0 || path > 4) return qesb_fail(QESB_ERR_ARG, "qesb_net_set_conv_path: path must be in [0, 4]");
   g_conv_path = path;
   return QESB_OK;
 }

@@ -1336,6 +1336,7 @@ qesb_status run_sweep_loop(const SweepVariant &sv, bool multi, const SweepArgs &
   const int per_it_us = std::max(1, (int)(cells / 4.0e5));
   int chunk = std::max(1, std::min(128, 2000 / per_it_us));
   if (wk > 0) chunk = wk * std::max(1, chunk / wk);
+  else chunk = std::max(1, std::min(chunk, itermax));  // a short fixed phase (a start stage) launches no empty tail
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   const dim3 wgrid(std::max(1, 4 * sms / std::max(1, nslots)), std::max(1, nslots));

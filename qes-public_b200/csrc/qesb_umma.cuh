@@ -136,6 +136,29 @@ __device__ __forceinline__ void mma_drain(uint64_t *drain, bool issuer, uint32_t
   mbar_wait(drain, 0, limit);
 }
 
+// Expect `bytes` of asynchronous copies on the mbarrier, counting this
+// thread's arrival; a plain arrival (no copies) for the same phase bookkeeping.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *mbar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *mbar)
+{
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
+
+// 4-D tiled tensor copy global -> shared through a tensor map (a
+// __grid_constant__ kernel parameter or global memory), completing on the
+// mbarrier; this GPU's own memory only (no multicast).
+__device__ __forceinline__ void tma_load4(void *dst, const void *map, int c0, int c1, int c2, int c3, uint64_t *mbar)
+{
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(mbar))
+      : "memory");
+}
+
 // 32 lanes x 8 consecutive 32-bit columns of TMEM into 8 registers per thread
 // (warp w of a warpgroup reads lanes 32*(w%4) .. +31).
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8])

@@ -21,9 +21,13 @@ Nx, Ny, Nz, SEED, NB, ITERMAX = 40, 32, 16, 2024, 5, 150
 
 
 def _run(tmp_path, calls, solver_type):
+    """One demo run. The reference's Solver_CPU_RB (type 1) runs on one OpenMP
+    thread: with more, the unsynchronised max_error reset inside its parallel
+    region (Solver_CPU_RB.cpp:166) can end a solve early, at random."""
     out = tmp_path / f"out_{solver_type}_{calls}.bin"
     r = subprocess.run([DEMO, str(out), str(Nx), str(Ny), str(Nz), str(SEED), str(NB), str(ITERMAX), "1e-9",
-                        str(calls), str(solver_type)], capture_output=True, text=True, timeout=300)
+                        str(calls), str(solver_type)], capture_output=True, text=True, timeout=300,
+                       env=dict(os.environ, OMP_NUM_THREADS="1"))
     return r, out
 
 

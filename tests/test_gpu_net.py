@@ -266,3 +266,41 @@ def test_conv3d_items_stack_along_z_without_crosstalk(D, H, W, c1, c2, co, up):
             xin = torch.cat([xin, x2[i].double()], 1)
         ref = torch.relu(torch.nn.functional.conv3d(xin, w.double(), b.double(), padding=1))
         np.testing.assert_allclose(out[i].numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.parametrize("path", [2, 3, 4])
+@pytest.mark.parametrize("items,D,H,W,co", [(1, 1, 5, 128, 16), (1, 3, 6, 256, 32), (3, 4, 7, 128, 16),
+                                            (2, 6, 4, 128, 32), (1, 17, 9, 128, 16)])
+def test_conv3d_zmarch_and_direct_paths_match_torch(conv_path, path, items, D, H, W, co):
+    """The z-marching direct convolution (tensor-map staging, planes through a
+    ring, MMAs of one plane overlapping the read-out of the last) with 2 and 4
+    rows per CTA, and the direct kernel, for 16-channel forward convolutions:
+    odd heights (partial row tiles), one-plane and many-plane items, stacked
+    items, both output widths; against torch per item."""
+    import torch
+    torch.manual_seed(items + D + H + W + co + path)
+    ci = 16
+    xs = [_bf16(torch.randn(1, ci, D, H, W)) for _ in range(items)]
+    w = _bf16(torch.randn(co, ci, 3, 3, 3) / (27 * ci) ** 0.5)
+    b = torch.randn(co)
+    bm, kp = _bm_forward(w)
+    dev = "cuda:0"
+    xd = torch.cat([_cl(t) for t in xs], 0).to(dev)
+    bmd, bd = bm.to(dev), b.float().to(dev)
+    conv_path(path)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    for relu, fp32 in ((1, True), (0, False)):
+        yf = torch.zeros(items * D * H * W * co, dtype=torch.float32, device=dev) if fp32 else None
+        y = None if fp32 else torch.zeros(items * D * H * W * co, dtype=torch.bfloat16, device=dev)
+        g = lambda t: t.data_ptr() if t is not None else None  # noqa: E731
+        qesb.check(qesb.lib().qesb_conv3d_items(g(xd), ci, 0, None, 0, items, D, H, W, 1, g(bmd), kp, co, g(y),
+                                                g(yf), g(bd), relu, None, g(err), None))
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0
+        out = (yf if fp32 else y.float()).view(items, D, H, W, co).cpu().double()
+        for i in range(items):
+            ref = torch.nn.functional.conv3d(xs[i].double(), w.double(), b.double(), padding=1)
+            if relu:
+                ref = torch.relu(ref)
+            tol = 1e-4 if fp32 else 1e-2
+            np.testing.assert_allclose(out[i].numpy(), _cl(ref).numpy(), rtol=tol, atol=tol)

@@ -366,9 +366,11 @@ qesb_status qesb_umma_selftest(const uint16_t *A, const uint16_t *B, float *C, i
  * (BF16) or yf (FP32); optional bias[N] (FP32), ReLU, and mask (BF16 [V][N]:
  * output zeroed where mask <= 0). N in {16, 32, 64, 128}. *err is set if a
  * kernel's tensor-core completion wait gives up. Grids with W a multiple of
- * 128 and N in {16, 32} run a direct kernel (each 16-channel input slice
- * staged once per tile, the 27 taps as shifted descriptors into it); the
- * others the implicit GEMM (per-tap gather). Small grids (fewer than about two
+ * 128 and N in {16, 32} run direct kernels (the 27 taps as shifted
+ * descriptors into staged input rows): forward convolutions of one 16-channel
+ * input without mask march along z, each input plane staged once by
+ * tensor-map copies; the others stage each 16-channel slice once per tile.
+ * The remaining grids run the implicit GEMM (per-tap gather). Small grids (fewer than about two
  * 128-voxel tiles per SM) split the K chunks over more CTAs and add FP32
  * partial sums in a scratch buffer kept per (device, stream), one slice per
  * split, allocated on the first such call on a stream and grown as needed (a
@@ -390,7 +392,7 @@ qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const void *x2, i
  * tensor-map copies, MMAs of one plane overlapping the read-out of the
  * previous; else the direct kernel where it applies; else the implicit GEMM),
  * 1 = implicit GEMM everywhere, 2 = the direct kernel but not the z-marching
- * one, 3 / 4 = the z-marching kernel with 2 / 4 output rows per CTA (4 is the
+ * one, 3 / 4 = the z-marching kernel with 2 / 4 output rows per CTA (2 is the
  * default's) - for comparison. */
 qesb_status qesb_net_set_conv_path(int path);
 /* Weight gradient dW[tap*(c1+c2) + c][n] += sum_v X[v + offset(tap)][c] * dY[v][n]

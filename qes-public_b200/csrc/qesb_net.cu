@@ -561,13 +561,26 @@ __global__ void __launch_bounds__(128, 1) k_conv_zdirect(const __grid_constant__
   bool ok = true;
   auto epilogue = [&](int t) {  // output plane z0 + t from accumulator set t % 2
     const int z = z0 + t, x = x0 + warp * 32 + lane;
+    const int ny = min(TY, g.H - y0);  // rows of this tile inside the grid
+    // every row's accumulators at once, then one wait: the loads overlap
+    uint32_t raw[TY][N];
+#pragma unroll
+    for (int r = 0; r < TY; ++r)
+#pragma unroll
+      for (int c0 = 0; c0 < N; c0 += 16)
+        if (r < ny)  // warp-uniform
+          umma::tmem_ld16_async(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((t & 1) * TY * N + r * N + c0),
+                                *reinterpret_cast<uint32_t(*)[16]>(&raw[r][c0]));
+    umma::tmem_wait_ld();
+#pragma unroll
     for (int r = 0; r < TY; ++r) {
-      const int y = y0 + r;
-      if (y >= g.H) break;  // warp-uniform
-      const long v = ((long)z * g.H + y) * g.W + x;
+      if (r >= ny) break;
+      const long v = ((long)z * g.H + y0 + r) * g.W + x;
+#pragma unroll
       for (int c0 = 0; c0 < N; c0 += 8) {
         float f[8];
-        umma::tmem_ld8(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((t & 1) * TY * N + r * N + c0), f);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) f[q] = __uint_as_float(raw[r][c0 + q]);
         if (out.bias) {
 #pragma unroll
           for (int q = 0; q < 8; ++q) f[q] += __ldg(out.bias + c0 + q);
@@ -1003,9 +1016,9 @@ extern "C" qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const 
                   (N == 16 || N == 32) && c1 == 16 && c2 == 0 && !up1 && sign == 1 && !mask &&
                   reinterpret_cast<uintptr_t>(x1) % 16 == 0;
   if (zd) {
-    if (g_conv_path == 3)
-      return N == 16 ? launch_conv_zdirect<16, 2>(in, g, B, Kp, o, err, s) : launch_conv_zdirect<32, 2>(in, g, B, Kp, o, err, s);
-    return N == 16 ? launch_conv_zdirect<16, 4>(in, g, B, Kp, o, err, s) : launch_conv_zdirect<32, 4>(in, g, B, Kp, o, err, s);
+    if (g_conv_path == 4)
+      return N == 16 ? launch_conv_zdirect<16, 4>(in, g, B, Kp, o, err, s) : launch_conv_zdirect<32, 4>(in, g, B, Kp, o, err, s);
+    return N == 16 ? launch_conv_zdirect<16, 2>(in, g, B, Kp, o, err, s) : launch_conv_zdirect<32, 2>(in, g, B, Kp, o, err, s);
   }
   if ((g_conv_path == 0 || g_conv_path >= 2) && W % 128 == 0 && (N == 16 || N == 32)) {
     if (N == 16) return launch_conv_direct<16>(in, g, sign, B, Kp, o, err, s);

@@ -114,6 +114,8 @@ def parse(argv=None):
                     help="QES-Fire solve pattern: this many fire steps warm-started from the previous lambda, exit")
     ap.add_argument("--profile-batch", action="store_true",
                     help="profiling driver: the headline batch once untimed, once more, exit")
+    ap.add_argument("--conv-path", type=int, default=0,
+                    help="network convolution kernels for --forward-only (qesb_net_set_conv_path)")
     ap.add_argument("--forward-only", type=int, default=0,
                     help="profiling driver: run this many warm-start forward passes on one domain, exit")
     return ap.parse_args(argv)
@@ -1223,6 +1225,7 @@ def run_forward_only(args):
 
     cities = [make_city(args.workload, SEED0 + i) for i in range(args.batch)]
     solvers = [qesb.Solver_B200(w.domain, TOL) for w in cities]
+    qesb.check(qesb.lib().qesb_net_set_conv_path(args.conv_path))
     net = ws.WarmNet(args.weights or ws.DEFAULT_WEIGHTS, device=0)
     try:
         for s, w in zip(solvers, cities):

@@ -17,9 +17,10 @@ pytestmark = pytest.mark.gpu
 
 # option "variant" index of bulk_w4_s3, the first bulk-copy sweep shape
 # (after the 5 fused tile shapes and the 13 streaming split shapes), and of
-# zmt_y4x2_b5, the first z-march shape staged by tensor-map copies
+# zmt_y4x2_b5, the first z-march shape staged by tensor-map copies, and of zmtb_y4x2_b5
 BULK_W4_S3 = 18
 ZMT_Y4X2_B5 = 51
+ZMTB_Y4X2_B5 = 59  # the same with equal plane-step shares per CTA
 
 
 def _city():
@@ -28,7 +29,7 @@ def _city():
     return d, qesb.city_build(d, c.buildings, c.inflow)
 
 
-@pytest.mark.parametrize("variant", [BULK_W4_S3, ZMT_Y4X2_B5])
+@pytest.mark.parametrize("variant", [BULK_W4_S3, ZMT_Y4X2_B5, ZMTB_Y4X2_B5])
 def test_stage_wait_timeout_is_an_error_status_and_the_handle_recovers(variant):
     d, w = _city()
     itermax = 60

@@ -114,6 +114,17 @@ def city_layout(dom, seed, max_buildings, fp=(10.0, 40.0), h=(10.0, 60.0)):
     return b[:n].copy(), inflow
 
 
+def city_flags(dom, buildings):
+    """The restatement's cell flags of a city (qo_city_flags): fluid 1, ground
+    plane 2, then each building's stair-step cells 0, in order."""
+    Nx, Ny, Nz = dom.base
+    flag = np.empty(dom.numCellCentered(), np.int32)
+    b = np.ascontiguousarray(buildings, np.float32)
+    _lib().qo_city_flags(Nx, Ny, Nz, dom.dx(), dom.dy(), _p(dom.dz_array), len(b), _p(b) if len(b) else None,
+                         _p(flag))
+    return flag
+
+
 def city_inputs(dom, buildings, inflow):
     """Inputs of a city: flags and inflow from the restatement, wall
     coefficients and solid faces from the reference build."""

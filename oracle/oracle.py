@@ -85,6 +85,8 @@ def ref() -> C.CDLL:
         L.qesref_wall_log_bc.restype = i
         L.qesref_set_threads.argtypes = [i]
         L.qesref_set_threads.restype = None
+        L.qr_rect_building_flags.argtypes = [i, i, i, f, f, _V, i, _V, _V, _V]
+        L.qr_rect_building_flags.restype = i
         L.qesref_set_threads(1)
         _ref = L
     return _ref
@@ -195,6 +197,18 @@ def ref_walls(dom, icellflag):
     outs = [np.zeros(nc, np.float32) for _ in range(6)]
     ref().qesref_walls(*_dims(dom), _p(dom.dz_array), _p(flag), *[_p(a) for a in outs])
     return (flag, *outs)
+
+
+def ref_rect_building_flags(dom, buildings, icellflag):
+    """The reference's own building rasterisation (RectangularBuilding::parseValues,
+    PolyBuilding::setPolyBuilding and setCellFlags, stair-step): buildings as rows of
+    (x_start, y_start, length, width, height, base height), rotation 0, applied in order
+    to a copy of icellflag; returns (icellflag, ibuilding_flag)."""
+    b = np.ascontiguousarray(np.asarray(buildings, np.float32).reshape(-1, 6))
+    flag = icellflag.astype(np.int32).copy()
+    ib = np.zeros_like(flag)
+    ref().qr_rect_building_flags(*_dims(dom), _p(dom.dz_array), len(b), _p(b), _p(flag), _p(ib))
+    return flag, ib
 
 
 def ref_set_velocity_zero(dom, icellflag, u0, v0, w0):

@@ -1,8 +1,9 @@
 // Test infrastructure: a C entry layer over the reference's OWN solver code.
 //
 // This file is compiled together with the reference sources where they lie
-// (src/winds/Solver.cpp, Solver_CPU.cpp, Solver_CPU_RB.cpp, Wall.cpp and
-// src/qes/Domain.cpp) by oracle/Makefile into oracle/_ref/libqesref.so.
+// (src/winds/Solver.cpp, Solver_CPU.cpp, Solver_CPU_RB.cpp, Wall.cpp,
+// PolyBuilding.cpp and src/qes/Domain.cpp) by oracle/Makefile into
+// oracle/_ref/libqesref.so.
 // Nothing in the product links it; only tests/ and bench.py's CPU-baseline
 // and reference legs load it, as the checker and the timed reference.
 //
@@ -16,10 +17,28 @@
 
 #include "qes/Domain.h"
 #include "WINDSGeneralData.h"
+#include "WINDSInputData.h"
 #include "Solver_CPU.h"
 #include "Solver_CPU_RB.h"
 #include "Wall.h"
+#include "RectangularBuilding.h"
+#include "CutBuilding.h"
 #include <iostream>
+
+// The cut-cell rasterisation (src/winds/CutBuilding.cpp) needs the full
+// WINDSGeneralData; PolyBuilding::setCellFlags calls it only for
+// meshTypeFlag 1, which the oracle never sets. An empty definition stands in,
+// as do the building parameterizations (upwind cavity, wakes, street canyon,
+// side wall, rooftop, mixing: their own reference files), which PolyBuilding's
+// virtual table names but the rasterisation never calls.
+void CutBuilding::setCutCellFlags(WINDSGeneralData *, const PolyBuilding *, int) {}
+void PolyBuilding::upwindCavity(const WINDSInputData *, WINDSGeneralData *) {}
+void PolyBuilding::polygonWake(const WINDSInputData *, WINDSGeneralData *, int) {}
+void PolyBuilding::streetCanyon(WINDSGeneralData *) {}
+void PolyBuilding::streetCanyonModified(WINDSGeneralData *) {}
+void PolyBuilding::sideWall(const WINDSInputData *, WINDSGeneralData *) {}
+void PolyBuilding::rooftop(const WINDSInputData *, WINDSGeneralData *) {}
+void PolyBuilding::NonLocalMixing(WINDSGeneralData *, TURBGeneralData *, int) {}
 
 namespace {
 
@@ -189,6 +208,47 @@ double qesref_solve(int kind, int Nx, int Ny, int Nz, float dx, float dy, const 
   std::memcpy(v, wgd.v.data(), sizeof(float) * nf);
   std::memcpy(w, wgd.w.data(), sizeof(float) * nf);
   return t;
+}
+
+// The reference's rectangular buildings on a cell-flag field: for each of the
+// nb buildings b[q] = (x_start, y_start, length, width, height, base height),
+// rotation 0, RectangularBuilding::parseValues builds its polygon
+// (src/winds/RectangularBuilding.h:62-112), then PolyBuilding::setPolyBuilding
+// and setCellFlags (src/winds/PolyBuilding.cpp:72-236) rasterise it with the
+// stair-step method, in building order. icellflag (cell layout) is the
+// field before the buildings on entry and after them on return;
+// ibuilding_flag (nullable) receives each cell's building index, -1 elsewhere.
+int qr_rect_building_flags(int Nx, int Ny, int Nz, float dx, float dy, const float *dz_array, int nb,
+                           const float *b, int *icellflag, int *ibuilding_flag)
+{
+  qes::Domain d = make_domain(Nx, Ny, Nz, dx, dy, dz_array);
+  WINDSGeneralData wgd(d);
+  const size_t nc = (size_t)(d.nx() - 1) * (d.ny() - 1) * (d.nz() - 1);
+  wgd.icellflag.assign(icellflag, icellflag + nc);
+  wgd.ibuilding_flag.assign(nc, -1);
+  wgd.icellflag_footprint.assign((size_t)(d.nx() - 1) * (d.ny() - 1), 1);
+  ShimSimParams sp;
+  WINDSInputData wid;
+  wid.simParams = &sp;
+  for (int q = 0; q < nb; ++q) {
+    const float *B = b + 6 * q;
+    auto &v = ParseInterface::shimValues();
+    v.clear();
+    v["xStart"] = B[0];
+    v["yStart"] = B[1];
+    v["length"] = B[2];
+    v["width"] = B[3];
+    v["height"] = B[4];
+    v["baseHeight"] = B[5];
+    v["buildingRotation"] = 0.0;
+    RectangularBuilding rb;
+    rb.parseValues();
+    rb.setPolyBuilding(&wgd);
+    rb.setCellFlags(&wid, &wgd, q);
+  }
+  std::memcpy(icellflag, wgd.icellflag.data(), sizeof(int) * nc);
+  if (ibuilding_flag) std::memcpy(ibuilding_flag, wgd.ibuilding_flag.data(), sizeof(int) * nc);
+  return 0;
 }
 
 }  // extern "C"

@@ -1,9 +1,10 @@
 // Test-infrastructure shim (oracle only).
 //
 // The reference's WINDSGeneralData drags in NetCDF, GDAL, OptiX and every
-// parameterization. The solver path (src/winds/Solver*.cpp) and the wall
-// routines (src/winds/Wall.cpp) only touch the members below, which carry
-// the same names and types as src/winds/WINDSGeneralData.h:201-320.
+// parameterization. The solver path (src/winds/Solver*.cpp), the wall
+// routines (src/winds/Wall.cpp) and the building rasterisation
+// (src/winds/PolyBuilding.cpp) only touch the members below, which carry the
+// same names and types as src/winds/WINDSGeneralData.h:201-320.
 #pragma once
 #include <utility>
 #include <vector>
@@ -22,6 +23,8 @@ public:
 
   std::vector<float> e, f, g, h, m, n;
   std::vector<int> icellflag;
+  std::vector<int> ibuilding_flag, icellflag_footprint;  // building rasterisation (PolyBuilding.cpp)
+  std::vector<float> base_height;
   std::vector<float> building_volume_frac;
   std::vector<float> ni, nj, nk, ti, tj, tk;
   std::vector<float> wall_distance;

@@ -37,6 +37,32 @@ def test_walls_and_solid_faces_match_reference(seed):
     np.testing.assert_array_equal(w0, w.w0)
 
 
+@pytest.mark.skipif(not O.ref_available(), reason="reference build oracle/_ref absent")
+@pytest.mark.parametrize("nx,ny,nz,seed,nb", [(36, 30, 18, 1, 7), (64, 48, 24, 2, 12), (100, 90, 30, 3, 20),
+                                              (128, 128, 64, 1001, 40)])
+def test_building_rasterisation_matches_reference_polybuilding(nx, ny, nz, seed, nb):
+    """The buildings' stair-step cells, from the product generator and from the
+    oracle's restatement, against the reference's own RectangularBuilding /
+    PolyBuilding code (PNPOLY cell-centre test, k range from z and z_face) run
+    on the same field before the buildings (fluid 1, ground plane 2)."""
+    from oracle import city as OC
+
+    d = qesb.Domain(nx, ny, nz, 2.0, 2.0, 1.0, qesb.city_dz(nz, 1.0, 1.03))
+    c = qesb.city_random(d, seed, nb, fp=(6, 16), h=(4, 24))
+    w = qesb.city_build(d, c.buildings, c.inflow)
+    b = np.array([[x.x_start, x.y_start, x.length, x.width, x.height, x.base_height] for x in c.buildings],
+                 np.float32)
+    assert len(b) > 0
+    X, Y, Z = nx, ny, nz + 1
+    before = np.ones((Z, Y, X), np.int32)
+    before[0] = 2
+    flag, ib = O.ref_rect_building_flags(d, b, before.ravel())
+    np.testing.assert_array_equal(w.icellflag, flag)
+    assert (ib[flag == 0] >= 0).all() and (ib[flag != 0] == -1).all()
+    od = OC.Domain(nx, ny, nz, 2.0, 2.0, d.dz_array)
+    np.testing.assert_array_equal(OC.city_flags(od, b), flag)
+
+
 def test_cuboid100_cells():
     """20x20x20 m cuboid at x, y in [40, 60] m: PNPOLY on cell centres puts
     cells 40..59 inside; heights 0..20 m give k = 1..20 (z[k] = k - 0.5)."""

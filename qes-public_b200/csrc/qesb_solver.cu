@@ -717,6 +717,10 @@ struct qesb_handle {
 
   // sweep kernels: this solve as a one-domain list
   SweepList list;
+  // batches led by this handle: their domain list and loop graphs, kept from
+  // batch to batch (no allocation, free or graph instantiation per batch once warm)
+  SweepList blist;
+  SweepGraph bgraph_start, bgraph_pre, bgraph;
   SweepCtl *h_ctl = nullptr;  // pinned
   SweepGraph sgraph;  // iteration-loop graph of the sweep kernels
 
@@ -1591,6 +1595,10 @@ void free_all(qesb_handle *h)
   for (void *p : ptrs)
     if (p) cudaFree(p);
   h->list.destroy();
+  h->blist.destroy();
+  h->bgraph_start.reset();
+  h->bgraph_pre.reset();
+  h->bgraph.reset();
   if (h->h_state) cudaFreeHost(h->h_state);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
   for (auto &e : h->ev)
@@ -2225,8 +2233,11 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     CKS(attach_tmaps(h, sv, doms[i], s));
     cells += (double)G.XY * G.Z;
   }
-  SweepList list;
-  CKS(list.create(n));
+  SweepList &list = h0->blist;
+  if (list.cap < n) {
+    list.destroy();
+    CKS(list.create(n));
+  }
   list.a.wait_limit = h0->opt_wait_limit;
   k_sweep_stamp<<<1, 1, 0, s>>>(list.a.ctl);  // the latencies (ms_sor) count from here
   qesb_status qs = QESB_OK;
@@ -2236,13 +2247,12 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     // the start stages of the pre-phases that have one, as a list of their own
     sweep_tiles(start, sv, true, h0->device);
     qs = list.upload(start, sv.unit, s);
-    SweepGraph gx;
     int smax = 0;
     for (int i : start_of) smax = std::max(smax, hs[i]->start_iters);
     int n1 = 0;
     if (qs == QESB_OK)
-      qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, smax, h0->opt_graph != 0, &gx, h0->h_ctl, &n1);
-    gx.reset();
+      qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, smax, h0->opt_graph != 0, &h0->bgraph_start,
+                          h0->h_ctl, &n1);
     pre_launched += n1;
     for (size_t q = 0; q < start_of.size() && qs == QESB_OK; ++q) {
       qesb_handle *h = hs[start_of[q]];
@@ -2261,13 +2271,12 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     // the over-relaxed pre-phase of the domains that have one, as a list of its own
     sweep_tiles(pre, sv, true, h0->device);
     qs = list.upload(pre, sv.unit, s);
-    SweepGraph gx;
     int pre_max = 0;
     for (int i : pre_of) pre_max = std::max(pre_max, hs[i]->pre_iters);
     int n2 = 0;
     if (qs == QESB_OK)
-      qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, pre_max, h0->opt_graph != 0, &gx, h0->h_ctl, &n2);
-    gx.reset();
+      qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, pre_max, h0->opt_graph != 0, &h0->bgraph_pre,
+                          h0->h_ctl, &n2);
     pre_launched += n2;
     for (size_t q = 0; q < pre_of.size() && qs == QESB_OK; ++q) {
       qesb_handle *h = hs[pre_of[q]];
@@ -2289,13 +2298,11 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
                           s) != cudaSuccess)
         qs = qesb_fail(QESB_ERR_CUDA, "qesb_solve_batch: window snapshot copy failed");
   if (qs == QESB_OK) {
-    SweepGraph gx;
     CK(cudaEventRecord(h0->evs[2], s));
     if (itermax > 0)
-      qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, itermax, h0->opt_graph != 0, &gx, h0->h_ctl,
+      qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, itermax, h0->opt_graph != 0, &h0->bgraph, h0->h_ctl,
                           &launched, h0->win_k, n);
     CK(cudaEventRecord(h0->evs[3], s));
-    gx.reset();
   }
   const unsigned long long t0 = h0->h_ctl->t0;
   CK(cudaEventRecord(h0->ev[2], s));
@@ -2313,7 +2320,6 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   }
   CK(cudaEventRecord(h0->ev[3], s));
   cudaError_t se = cudaStreamSynchronize(s);
-  list.destroy();
   if (qs != QESB_OK) return qs;
   if (se != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "batch: %s", cudaGetErrorString(se));
   float ms_all = 0, ms_pre = 0, ms_ref = 0;

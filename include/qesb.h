@@ -98,6 +98,15 @@ qesb_status qesb_reset_lambda(qesb_handle *h);
 qesb_status qesb_set_inputs(qesb_handle *h, const float *e, const float *f, const float *g,
                             const float *hc, const float *m, const float *n, const int *icellflag,
                             const float *u0, const float *v0, const float *w0);
+/* The same inputs when the coefficients are the stair-step walls of the flag
+ * field (the reference's default mesh: Wall::defineWalls then
+ * Wall::solverCoefficients, src/winds/Wall.cpp:44-350): icellflag, u0, v0, w0
+ * from the host (16 bytes per cell instead of 40), e..n computed from
+ * icellflag on the device by the reference's rules, bit for bit what
+ * Wall::solverCoefficients gives. Not for cut-cell coefficients (meshTypeFlag
+ * 1) or coefficients read from a file: pass those to qesb_set_inputs. */
+qesb_status qesb_set_inputs_flags(qesb_handle *h, const int *icellflag, const float *u0, const float *v0,
+                                  const float *w0);
 /* Same, from device pointers (reference layouts) already on the handle's device. */
 qesb_status qesb_set_inputs_device(qesb_handle *h, const float *e, const float *f, const float *g,
                                    const float *hc, const float *m, const float *n,

@@ -156,6 +156,23 @@ __global__ void k_city_winds(CityGrid G, const float *__restrict__ up, const flo
 
 }  // namespace
 
+qesb_status qesb_city_walls_dev(int Nx, int Ny, int Nz, float dx, const float *d_dz, const int *d_flag, float *e,
+                                float *f, float *g, float *hc, float *m, float *n, void *stream)
+{
+  CityGrid G;
+  G.nx = Nx + 1;
+  G.ny = Ny + 1;
+  G.nz = Nz + 2;
+  G.X = Nx;
+  G.XY = (long)Nx * Ny;
+  G.FX = Nx + 1;
+  G.FXY = (long)(Nx + 1) * (Ny + 1);
+  k_city_walls<<<dim3(1, G.ny - 1, G.nz - 1), 256, 0, static_cast<cudaStream_t>(stream)>>>(G, dx, d_dz, d_flag, e, f, g,
+                                                                                           hc, m, n);
+  const cudaError_t ce = cudaGetLastError();
+  return ce == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "wall coefficients: %s", cudaGetErrorString(ce));
+}
+
 extern "C" qesb_status qesb_city_build_device(const qesb_grid *grid, int n_buildings, const qesb_building *b,
                                               const qesb_inflow *in, int *icellflag, float *e, float *f,
                                               float *g, float *hc, float *m, float *n, float *u0, float *v0,

@@ -14,3 +14,9 @@ qesb_status qesb_fail(qesb_status s, const char *fmt, ...);
 
 // The handle's base grid counts and device (for the library's other parts).
 qesb_status qesb_handle_grid(qesb_handle *h, int *Nx, int *Ny, int *Nz, int *device);
+
+// Wall::defineWalls + Wall::solverCoefficients (stair-step walls) on the
+// device: e..n (cell arrays) from a flag field already on the device, on the
+// given stream; dz on the device (nz - 1 values, as the grid's dz_array).
+qesb_status qesb_city_walls_dev(int Nx, int Ny, int Nz, float dx, const float *d_dz, const int *d_flag, float *e,
+                                float *f, float *g, float *hc, float *m, float *n, void *stream);

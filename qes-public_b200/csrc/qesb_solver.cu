@@ -1759,6 +1759,32 @@ qesb_status qesb_set_inputs(qesb_handle *h, const float *e, const float *f, cons
   return QESB_OK;
 }
 
+qesb_status qesb_set_inputs_flags(qesb_handle *h, const int *icellflag, const float *u0, const float *v0,
+                                  const float *w0)
+{
+  if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
+  if (!icellflag || !u0 || !v0 || !w0) return qesb_fail(QESB_ERR_ARG, "qesb_set_inputs_flags: null input");
+  CK(cudaSetDevice(h->device));
+  CKS(ensure_own_inputs(h));
+  const size_t nc = (size_t)h->G.XY * h->G.Z, nf = (size_t)h->G.FXY * h->G.FZ;
+  cudaStream_t s = h->stream;
+  CK(cudaMemcpyAsync(h->d_own_flag, icellflag, nc * sizeof(int), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_own_u0, u0, nf * sizeof(float), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_own_v0, v0, nf * sizeof(float), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(h->d_own_w0, w0, nf * sizeof(float), cudaMemcpyHostToDevice, s));
+  CKS(qesb_city_walls_dev(h->G.X, h->G.Y, h->G.Z - 1, h->dx, h->d_dz, h->d_own_flag, h->d_own_in[0], h->d_own_in[1],
+                          h->d_own_in[2], h->d_own_in[3], h->d_own_in[4], h->d_own_in[5], s));
+  for (int q = 0; q < 6; ++q) h->d_in[q] = h->d_own_in[q];
+  h->d_flag = h->d_own_flag;
+  h->d_u0 = h->d_own_u0;
+  h->d_v0 = h->d_own_v0;
+  h->d_w0 = h->d_own_w0;
+  CKS(prepare_coefs(h));
+  CK(cudaStreamSynchronize(s));
+  h->have_inputs = true;
+  return QESB_OK;
+}
+
 qesb_status qesb_set_inputs_device(qesb_handle *h, const float *e, const float *f, const float *g,
                                    const float *hc, const float *m, const float *n,
                                    const int *icellflag, const float *u0, const float *v0,

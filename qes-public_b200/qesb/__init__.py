@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
             "qesb_set_tolerance": ([V, C.c_float], C.c_int),
             "qesb_set_prephase": ([V, C.c_float, C.c_float, C.c_int], C.c_int),
             "qesb_set_prephase_start": ([V, C.c_float, C.c_int], C.c_int),
+            "qesb_set_inputs_flags": ([V, V, V, V, V], C.c_int),
             "qesb_set_window_rule": ([V, C.c_int, C.c_double], C.c_int),
             "qesb_fp64_same_sor": ([V, V, C.c_float, C.c_int, C.c_int, V, V, V, V, C.POINTER(Fp64Report)],
                                    C.c_int),
@@ -366,6 +367,12 @@ class Solver_B200:
     def set_inputs(self, WGD: WINDSGeneralData):
         arrs = [np.ascontiguousarray(a) for a in WGD.inputs()]
         check(lib().qesb_set_inputs(self._h, *[_ptr(a) for a in arrs]))
+
+    def set_inputs_flags(self, WGD: WINDSGeneralData):
+        """qesb_set_inputs_flags: icellflag and u0, v0, w0 only; the stair-step
+        wall coefficients computed from the flags on the device."""
+        arrs = [np.ascontiguousarray(a) for a in (WGD.icellflag, WGD.u0, WGD.v0, WGD.w0)]
+        check(lib().qesb_set_inputs_flags(self._h, *[_ptr(a) for a in arrs]))
 
     def set_inputs_device(self, e, f, g, h, m, n, icellflag, u0, v0, w0):
         """Device pointers (ints) in the reference layouts."""

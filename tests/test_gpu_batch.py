@@ -205,3 +205,26 @@ def test_batch_autotune_keeps_lambda_and_results_exact():
     finally:
         for s in solvers:
             s.close()
+
+
+def test_flags_only_inputs_give_the_same_solve():
+    """qesb_set_inputs_flags (icellflag and the initial winds; the stair-step
+    wall coefficients computed on the device) gives the solve that
+    qesb_set_inputs gives from the reference's full arrays, bit for bit."""
+    for (nx, ny, nz, seed, nb) in [(70, 45, 21, 9, 8), (131, 40, 15, 3, 6)]:
+        d = qesb.Domain(nx, ny, nz, 2.0, 2.0, 1.0, qesb.city_dz(nz, 1.0, 1.03))
+        c = qesb.city_random(d, seed, nb, fp=(6, 18), h=(4, 16))
+        w = qesb.city_build(d, c.buildings, c.inflow)
+        out = []
+        for flags_only in (False, True):
+            with qesb.Solver_B200(d, 1.1e-3) as s:
+                if flags_only:
+                    s.set_inputs_flags(w)
+                else:
+                    s.set_inputs(w)
+                st = s.solve(w, 3000, set_inputs=False)
+                out.append((st["iterations"], st["max_divergence"], s.lambda_, w.u.copy(), w.w.copy()))
+        a, b = out
+        assert a[0] == b[0] and a[1] == b[1]
+        for x, y in zip(a[2:], b[2:]):
+            np.testing.assert_array_equal(x, y)

@@ -42,10 +42,14 @@ void Solver_B200::solve(WINDSGeneralData *WGD, const int &itermax)
   auto start = std::chrono::high_resolution_clock::now();
   std::cout << "[Solver]\t Running B200 Solver (GPU) ..." << std::endl;
   check(qesb_set_tolerance(handle_, tol), "qesb_set_tolerance");
-  check(qesb_set_inputs(handle_, WGD->e.data(), WGD->f.data(), WGD->g.data(), WGD->h.data(),
-                        WGD->m.data(), WGD->n.data(), WGD->icellflag.data(), WGD->u0.data(),
-                        WGD->v0.data(), WGD->w0.data()),
-        "qesb_set_inputs");
+  if (stair_)
+    check(qesb_set_inputs_flags(handle_, WGD->icellflag.data(), WGD->u0.data(), WGD->v0.data(), WGD->w0.data()),
+          "qesb_set_inputs_flags");
+  else
+    check(qesb_set_inputs(handle_, WGD->e.data(), WGD->f.data(), WGD->g.data(), WGD->h.data(),
+                          WGD->m.data(), WGD->n.data(), WGD->icellflag.data(), WGD->u0.data(),
+                          WGD->v0.data(), WGD->w0.data()),
+          "qesb_set_inputs");
   bool from_zero = true;  // a solve from lambda = 0: the first, or the first after resetLambda
   for (float x : lambda)
     if (x != 0.0f) {

@@ -32,6 +32,12 @@ public:
   // it. The network is the caller's (qesb_warmnet_load); nullptr turns it off.
   void useLearnedStart(qesb_warmnet *net) { net_ = net; }
 
+  // Stair-step inputs (qesb_set_inputs_flags): when the coefficients are the
+  // ones Wall::solverCoefficients gives for the flags (meshTypeFlag 0, not read
+  // from a file), each solve uploads only icellflag and u0, v0, w0 and the
+  // library recomputes e..n from the flags on the device, bit for bit.
+  void useStairStepInputs(bool on) { stair_ = on; }
+
 protected:
   // Solver::solve semantics (src/winds/Solver_CPU.cpp:42-238): reads e..n,
   // icellflag, u0 v0 w0 and writes u v w of WGD. lambda lives in the base
@@ -43,4 +49,5 @@ protected:
 private:
   qesb_handle *handle_ = nullptr;
   qesb_warmnet *net_ = nullptr;
+  bool stair_ = false;
 };

@@ -7,8 +7,11 @@
 // file for comparison.
 // With a weights file (type 5 only) every solve that starts from lambda = 0
 // uses the learned warm start (Solver_B200::useLearnedStart).
-//   solver_b200_demo <out.bin> <Nx> <Ny> <Nz> <seed> <nbuildings> <itermax> <tol> [calls] [type] [weights]
+//   solver_b200_demo <out.bin> <Nx> <Ny> <Nz> <seed> <nbuildings> <itermax> <tol> [calls] [type] [weights] [stair]
+// With "stair" as the last argument (type 5) the solves upload only the flags and initial winds
+// (Solver_B200::useStairStepInputs); a weights argument of "-" means no network.
 #include <cstdio>
+#include <cstring>
 #include <cstdlib>
 #include <vector>
 
@@ -51,7 +54,9 @@ int main(int argc, char **argv)
 
   Solver *solver = SolverFactory::create(type, wgd.domain, tol);
   qesb_warmnet *net = nullptr;
-  if (argc > 11 && type == B200_Type) {
+  if (argc > 12 && type == B200_Type && std::strcmp(argv[12], "stair") == 0)
+    static_cast<Solver_B200 *>(solver)->useStairStepInputs(true);
+  if (argc > 11 && type == B200_Type && std::strcmp(argv[11], "-") != 0) {
     if (qesb_warmnet_load(argv[11], 0, &net) != QESB_OK) {
       std::fprintf(stderr, "warm-start network: %s\n", qesb_last_error());
       return 1;

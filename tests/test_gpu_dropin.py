@@ -91,6 +91,24 @@ def test_dropin_type_5_through_the_reference_factory(tmp_path, calls):
 
 @needs_demo
 @pytest.mark.gpu
+def test_dropin_stair_step_inputs_from_cpp(tmp_path):
+    """Solver_B200::useStairStepInputs: the adaptor uploads only icellflag and the
+    initial winds (qesb_set_inputs_flags) and the library rebuilds e..n from the
+    flags; the result is the oracle's red-black result, as with the full arrays."""
+    out = tmp_path / "stair.bin"
+    r = subprocess.run([DEMO, str(out), str(Nx), str(Ny), str(Nz), str(SEED), str(NB), str(ITERMAX), "1e-9", "2",
+                        "5", "-", "stair"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    d, u, v, ww, lam = _read(out)
+    uo, vo, wo, L = _oracle(d, 2)
+    np.testing.assert_array_equal(lam, L)
+    np.testing.assert_array_equal(u, uo)
+    np.testing.assert_array_equal(v, vo)
+    np.testing.assert_array_equal(ww, wo)
+
+
+@needs_demo
+@pytest.mark.gpu
 def test_dropin_learned_warm_start_from_cpp(tmp_path):
     """Solver_B200::useLearnedStart through the reference factory: the C++
     caller's solves from lambda = 0 start from the network (qesb_warm_start).

@@ -402,7 +402,8 @@ qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const void *x2, i
  * previous; else the direct kernel where it applies; else the implicit GEMM),
  * 1 = implicit GEMM everywhere, 2 = the direct kernel but not the z-marching
  * one, 3 / 4 = the z-marching kernel with 2 / 4 output rows per CTA (2 is the
- * default's) - for comparison. */
+ * default's), 5 = the default with a four-stage implicit GEMM instead of
+ * three - for comparison. */
 qesb_status qesb_net_set_conv_path(int path);
 /* Weight gradient dW[tap*(c1+c2) + c][n] += sum_v X[v + offset(tap)][c] * dY[v][n]
  * (FP32, accumulated with atomics: zero it first); X as in qesb_conv3d,

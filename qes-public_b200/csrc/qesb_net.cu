@@ -19,6 +19,9 @@ using namespace qesb;
 namespace {
 
 constexpr uint32_t kWaitLimit = 1u << 26;  // mbarrier polls before a kernel gives up
+int g_conv_path = 0;  // 0: z-marching / direct kernels where they apply, 1: implicit GEMM only,
+                      // 2: direct kernel (not the z-marching one), 3 / 4: z-marching with 2 / 4 rows per CTA,
+                      // 5: as 0 with a four-stage implicit GEMM
 
 // Byte offset of element (r, k) in a canonical no-swizzle tile with KC = 64
 // columns of K and R rows (see qesb_umma.cuh).
@@ -148,6 +151,29 @@ __device__ __forceinline__ uint4 load_in8(const ConvIn &in, const ConvGeom &g, i
   return __ldg(reinterpret_cast<const uint4 *>(p));
 }
 
+// Address of load_in8's 16 bytes, and whether they lie inside the output
+// voxel's item (else the copy zero-fills and the address is only a placeholder).
+__device__ __forceinline__ const __nv_bfloat16 *in_addr8(const ConvIn &in, const ConvGeom &g, int zo, int z, int y,
+                                                         int x, int c, bool &valid)
+{
+  const int zb = zo - zo % g.Dc;
+  valid = !(z < zb || z >= zb + g.Dc || y < 0 || y >= g.H || x < 0 || x >= g.W);
+  if (!valid) return in.x1;
+  if (c < in.c1) {
+    if (in.up1) return in.x1 + ((((long)(z >> 1) * (g.H >> 1) + (y >> 1)) * (g.W >> 1) + (x >> 1)) * in.c1 + c);
+    return in.x1 + ((((long)z * g.H + y) * g.W + x) * in.c1 + c);
+  }
+  return in.x2 + ((((long)z * g.H + y) * g.W + x) * in.c2 + (c - in.c1));
+}
+
+// 16-byte asynchronous copy global -> shared; valid = false fills zeros and reads nothing.
+__device__ __forceinline__ void cp16_zfill(void *dst, const void *src, bool valid)
+{
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(umma::smem_u32(dst)), "l"(src),
+               "r"(valid ? 16 : 0)
+               : "memory");
+}
+
 __device__ __forceinline__ void tap_offset(int t, int &dz, int &dy, int &dx)
 {
   dz = t / 9 - 1;
@@ -168,9 +194,11 @@ struct ConvOut {
 // Y[v][n] = epilogue( sum_k A[v][k] * Bm[n][k] ), A the implicit im2col of
 // the input at taps v + sign*offset(t), k = t*cin + c, Bm [N][Kp] K-major
 // BF16 (Kp = roundup(27*cin, 64), zero-padded). One CTA of 128 threads per
-// 128 voxels; two shared-memory stages so the gather of chunk j+1 overlaps
-// the MMAs of chunk j; accumulator N FP32 columns of TMEM.
-template <int N>
+// 128 voxels; a ring of NSTAGES shared-memory stages filled by asynchronous
+// 16-byte copies (zero-filled outside the grid) NSTAGES - 2 K chunks ahead,
+// so the gathers of the next chunks are in flight while chunk j's MMAs run;
+// accumulator N FP32 columns of TMEM.
+template <int N, int NSTAGES>
 __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int sign, const __nv_bfloat16 *__restrict__ Bm,
                                                    int Kp, ConvOut out, int *err)
 {
@@ -178,9 +206,10 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
   // and stores its partial in slice y of out.acc; k_conv_finish adds the
   // slices in order and applies the epilogue (the same bits every run).
   constexpr uint32_t SA = 128 * 64 * 2, SB = N * 64 * 2, STAGE = SA + SB;
+  constexpr int NS = NSTAGES, DIST = NS - 2;  // chunk c's copies go out DIST iterations before its MMAs
   constexpr uint32_t NCOLS = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
   extern __shared__ __align__(1024) uint8_t sm[];
-  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ __align__(8) uint64_t mbar[NS];  // stage s: the MMAs of chunk c, c % NS == s
   __shared__ __align__(8) uint64_t mdrain;  // completion of every issued MMA, after a wait gave up
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -188,8 +217,7 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
   const long m0 = (long)blockIdx.x * 128;
   if (warp == 0) umma::tmem_alloc(&tmem_base, NCOLS);
   if (tid == 0) {
-    umma::mbar_init(&mbar[0], 1);
-    umma::mbar_init(&mbar[1], 1);
+    for (int q = 0; q < NS; ++q) umma::mbar_init(&mbar[q], 1);
     umma::mbar_init(&mdrain, 1);
     umma::fence_mbar_init();
   }
@@ -201,58 +229,86 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
 
   // this thread's 8 rows (m = tid/8 + 16 i) and fixed k-group g = tid % 8
   const int g8 = tid & 7;
-  int rz[8], ry[8], rx[8];
+  int rz[8], ry[8], rx[8], rzb[8];
+  long rvox[8];
   bool rv[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const long v = m0 + (tid >> 3) + 16 * i;
     rv[i] = v < g.V;
     const long vv = rv[i] ? v : 0;
+    rvox[i] = vv;
     rx[i] = (int)(vv % g.W);
     ry[i] = (int)((vv / g.W) % g.H);
     rz[i] = (int)(vv / ((long)g.W * g.H));
+    rzb[i] = rz[i] - rz[i] % g.Dc;  // the row's item starts at this depth
   }
   const int nk_all = Kp / 64, per = (nk_all + gridDim.y - 1) / gridDim.y;
   const int jb = blockIdx.y * per, je = min(nk_all, jb + per), nk = je > jb ? je - jb : 0;
-  bool ok = true;
-  for (int jl = 0; jl < nk && ok; ++jl) {
-    const int j = jb + jl, s = jl & 1;
-    if (jl >= 2) ok = umma::mbar_wait(&mbar[s], ((jl - 2) >> 1) & 1, kWaitLimit);
-    if (!ok) break;
-    uint8_t *sa = sm + s * STAGE, *sb = sa + SA;
-    // A: rows m = tid/8 + 16 i, k-group g8
-    {
+  // this thread's copies of local chunk jl into its stage (one commit group, empty past the range)
+  auto issue = [&](int jl) {
+    if (jl < nk) {
+      const int j = jb + jl;
+      uint8_t *sa = sm + (jl % NS) * STAGE, *sb = sa + SA;
+      // A: rows m = tid/8 + 16 i, k-group g8
       const int kk = j * 64 + 8 * g8;
       const int t = kk / cin, c = kk - t * cin;
       int dz = 0, dy = 0, dx = 0;
       if (t < 27) tap_offset(t, dz, dy, dx);
+      dz *= sign;
+      dy *= sign;
+      dx *= sign;
+      if (in.up1 && c < in.c1) {  // the upsampled input: its own index arithmetic
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        uint4 val = make_uint4(0, 0, 0, 0);
-        if (rv[i] && t < 27)
-          val = load_in8(in, g, rz[i], rz[i] + sign * dz, ry[i] + sign * dy, rx[i] + sign * dx, c);
-        *reinterpret_cast<uint4 *>(sa + off_kmajor((tid >> 3) + 16 * i, 8 * g8)) = val;
+        for (int i = 0; i < 8; ++i) {
+          bool valid = false;
+          const __nv_bfloat16 *src = in_addr8(in, g, rz[i], rz[i] + dz, ry[i] + dy, rx[i] + dx, c, valid);
+          cp16_zfill(sa + off_kmajor((tid >> 3) + 16 * i, 8 * g8), src, valid && rv[i] && t < 27);
+        }
+      } else {  // same-grid input: one voxel offset for the tap, bounds per row
+        const long dv = ((long)dz * g.H + dy) * g.W + dx;
+        const bool first = c < in.c1;
+        const __nv_bfloat16 *tb = first ? in.x1 + c : in.x2 + (c - in.c1);
+        const int cs = first ? in.c1 : in.c2;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int z = rz[i] + dz, y = ry[i] + dy, x = rx[i] + dx;
+          const bool valid = rv[i] && t < 27 && z >= rzb[i] && z < rzb[i] + g.Dc && (unsigned)y < (unsigned)g.H &&
+                             (unsigned)x < (unsigned)g.W;
+          cp16_zfill(sa + off_kmajor((tid >> 3) + 16 * i, 8 * g8), valid ? tb + (rvox[i] + dv) * cs : in.x1, valid);
+        }
+      }
+      // B: N rows x 8 k-groups
+      for (int idx = tid; idx < N * 8; idx += 128) {
+        const int n = idx >> 3, gg = idx & 7;
+        cp16_zfill(sb + off_kmajor(n, 8 * gg), Bm + (long)n * Kp + j * 64 + 8 * gg, true);
       }
     }
-    // B: N rows x 8 k-groups
-    for (int idx = tid; idx < N * 8; idx += 128) {
-      const int n = idx >> 3, gg = idx & 7;
-      *reinterpret_cast<uint4 *>(sb + off_kmajor(n, 8 * gg)) =
-          __ldg(reinterpret_cast<const uint4 *>(Bm + (long)n * Kp + j * 64 + 8 * gg));
-    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  bool ok = true;
+  for (int jl = 0; jl < DIST; ++jl) issue(jl);
+  for (int jl = 0; jl < nk && ok; ++jl) {
+    // refill the stage chunk jl + DIST - NS used (its MMAs were issued two iterations ago)
+    const int c = jl + DIST - NS;
+    if (c >= 0) ok = umma::mbar_wait(&mbar[c % NS], (c / NS) & 1, kWaitLimit);
+    if (!ok) break;
+    issue(jl + DIST);
+    asm volatile("cp.async.wait_group %0;" ::"n"(DIST) : "memory");  // chunk jl's copies (this thread's) landed
     umma::fence_smem_async();
-    __syncthreads();
+    __syncthreads();  // everyone's
     if (tid == 0) {
       umma::fence_after_sync();
-      const uint32_t a0 = umma::smem_u32(sa), b0 = umma::smem_u32(sb);
+      const uint32_t a0 = umma::smem_u32(sm + (jl % NS) * STAGE), b0 = a0 + SA;
 #pragma unroll
       for (int kk = 0; kk < 4; ++kk)
         umma::mma_bf16(tmem, umma::desc(a0 + kk * 256, 128, 1024), umma::desc(b0 + kk * 256, 128, 1024), idesc,
                        (jl > 0 || kk > 0) ? 1u : 0u);
-      umma::mma_commit(&mbar[s]);
+      umma::mma_commit(&mbar[jl % NS]);
     }
   }
-  if (ok && nk > 0) ok = umma::mbar_wait(&mbar[(nk - 1) & 1], ((nk - 1) >> 1) & 1, kWaitLimit);
+  asm volatile("cp.async.wait_group 0;" ::: "memory");  // no copy outlives the CTA's shared memory
+  if (ok && nk > 0) ok = umma::mbar_wait(&mbar[(nk - 1) % NS], ((nk - 1) / NS) & 1, kWaitLimit);
   umma::fence_after_sync();
   if (!ok) {
     if (lane == 0) atomicExch(err, 1);
@@ -326,12 +382,6 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
 // TMEM. sign = -1 flips the taps (input gradient with the transposed weights).
 constexpr int kDirTY = 2, kDirTZ = 2, kDirNR = (kDirTY + 2) * (kDirTZ + 2), kDirXW = 130;
 
-__device__ __forceinline__ void cp16_zfill(void *dst, const void *src, bool valid)
-{
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(umma::smem_u32(dst)), "l"(src),
-               "r"(valid ? 16 : 0)
-               : "memory");
-}
 
 // Address of the 8 channels c..c+7 of the input at voxel (z, y, x) (caller
 // checks the grid bounds).
@@ -826,14 +876,17 @@ template <int N>
 qesb_status launch_conv(const ConvIn &in, const ConvGeom &g, int sign, const __nv_bfloat16 *Bm, int Kp,
                         const ConvOut &out, int *err, cudaStream_t s)
 {
-  constexpr int smem = 2 * (128 * 64 * 2 + N * 64 * 2);
+  // three stages (gathers one chunk ahead, three CTAs per SM at N = 32), or four (two ahead) on conv path 5
+  const bool three = g_conv_path != 5;
+  const int smem = (three ? 3 : 4) * (128 * 64 * 2 + N * 64 * 2);
   int dev = 0;
   cudaGetDevice(&dev);
-  static bool attr[64] = {};
-  if (!attr[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(k_conv_igemm<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  static bool attr[64][2] = {};
+  if (!attr[dev & 63][three]) {
+    cudaError_t e = three ? cudaFuncSetAttribute(k_conv_igemm<N, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                          : cudaFuncSetAttribute(k_conv_igemm<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv attr: %s", cudaGetErrorString(e));
-    attr[dev & 63] = true;
+    attr[dev & 63][three] = true;
   }
   const unsigned blocks = (unsigned)((g.V + 127) / 128);
   // Small grids (fewer CTAs than about two per SM): split the K chunks over
@@ -847,7 +900,8 @@ qesb_status launch_conv(const ConvIn &in, const ConvGeom &g, int sign, const __n
     const qesb_status st = acc_buffer(dev, s, need, &o.acc);
     if (st != QESB_OK) return st;
   }
-  k_conv_igemm<N><<<dim3(blocks, split), 128, smem, s>>>(in, g, sign, Bm, Kp, o, err);
+  if (three) k_conv_igemm<N, 3><<<dim3(blocks, split), 128, smem, s>>>(in, g, sign, Bm, Kp, o, err);
+  else k_conv_igemm<N, 4><<<dim3(blocks, split), 128, smem, s>>>(in, g, sign, Bm, Kp, o, err);
   if (split > 1) {
     const long total = g.V * N;
     k_conv_finish<<<(unsigned)std::min<long>((total + 255) / 256, 148L * 16), 256, 0, s>>>(o.acc, split, g.V, N, out);
@@ -856,8 +910,6 @@ qesb_status launch_conv(const ConvIn &in, const ConvGeom &g, int sign, const __n
   return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));
 }
 
-int g_conv_path = 0;  // 0: z-marching / direct kernels where they apply, 1: implicit GEMM only,
-                      // 2: direct kernel (not the z-marching one), 3 / 4: z-marching with 2 / 4 rows per CTA
 
 template <int N>
 qesb_status launch_conv_direct(const ConvIn &in, const ConvGeom &g, int sign, const __nv_bfloat16 *Bm, int Kp,
@@ -1012,7 +1064,7 @@ extern "C" qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const 
             static_cast<const __nv_bfloat16 *>(mask)};
   const auto *B = static_cast<const __nv_bfloat16 *>(Bm);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const bool zd = (g_conv_path == 0 || g_conv_path == 3 || g_conv_path == 4) && W % 128 == 0 &&
+  const bool zd = (g_conv_path == 0 || g_conv_path >= 3) && W % 128 == 0 &&
                   (N == 16 || N == 32) && c1 == 16 && c2 == 0 && !up1 && sign == 1 && !mask &&
                   reinterpret_cast<uintptr_t>(x1) % 16 == 0;
   if (zd) {
@@ -1041,7 +1093,7 @@ extern "C" qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *
 
 extern "C" qesb_status qesb_net_set_conv_path(int path)
 {
-  if (path < 0 || path > 4) return qesb_fail(QESB_ERR_ARG, "qesb_net_set_conv_path: path must be in [0, 4]");
+  if (path < 0 || path > 5) return qesb_fail(QESB_ERR_ARG, "qesb_net_set_conv_path: path must be in [0, 5]");
   g_conv_path = path;
   return QESB_OK;
 }

@@ -19,9 +19,10 @@ using namespace qesb;
 namespace {
 
 constexpr uint32_t kWaitLimit = 1u << 26;  // mbarrier polls before a kernel gives up
-int g_conv_path = 0;  // 0: z-marching / direct kernels where they apply, 1: implicit GEMM only,
-                      // 2: direct kernel (not the z-marching one), 3 / 4: z-marching with 2 / 4 rows per CTA,
-                      // 5: as 0 with a four-stage implicit GEMM
+int g_conv_path = 0;  // 0: z-marching kernel for every forward convolution it takes (concatenated and
+                      // upsampled inputs, rows of 128, 64 or 32), else direct, else implicit GEMM;
+                      // 1: implicit GEMM only; 2: direct kernel, else implicit GEMM; 3 / 4: z-marching for
+                      // one 16-channel input only, 2 / 4 rows per CTA; 5: as 3 with a four-stage implicit GEMM
 
 // Byte offset of element (r, k) in a canonical no-swizzle tile with KC = 64
 // columns of K and R rows (see qesb_umma.cuh).
@@ -151,21 +152,6 @@ __device__ __forceinline__ uint4 load_in8(const ConvIn &in, const ConvGeom &g, i
   return __ldg(reinterpret_cast<const uint4 *>(p));
 }
 
-// Address of load_in8's 16 bytes, and whether they lie inside the output
-// voxel's item (else the copy zero-fills and the address is only a placeholder).
-__device__ __forceinline__ const __nv_bfloat16 *in_addr8(const ConvIn &in, const ConvGeom &g, int zo, int z, int y,
-                                                         int x, int c, bool &valid)
-{
-  const int zb = zo - zo % g.Dc;
-  valid = !(z < zb || z >= zb + g.Dc || y < 0 || y >= g.H || x < 0 || x >= g.W);
-  if (!valid) return in.x1;
-  if (c < in.c1) {
-    if (in.up1) return in.x1 + ((((long)(z >> 1) * (g.H >> 1) + (y >> 1)) * (g.W >> 1) + (x >> 1)) * in.c1 + c);
-    return in.x1 + ((((long)z * g.H + y) * g.W + x) * in.c1 + c);
-  }
-  return in.x2 + ((((long)z * g.H + y) * g.W + x) * in.c2 + (c - in.c1));
-}
-
 // 16-byte asynchronous copy global -> shared; valid = false fills zeros and reads nothing.
 __device__ __forceinline__ void cp16_zfill(void *dst, const void *src, bool valid)
 {
@@ -258,12 +244,16 @@ __global__ void __launch_bounds__(128) k_conv_igemm(ConvIn in, ConvGeom g, int s
       dz *= sign;
       dy *= sign;
       dx *= sign;
-      if (in.up1 && c < in.c1) {  // the upsampled input: its own index arithmetic
+      if (in.up1 && c < in.c1) {  // the upsampled input: the coarse voxel of each fine one
+        const int Hc = g.H >> 1, Wc = g.W >> 1;
+        const __nv_bfloat16 *tb = in.x1 + c;
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-          bool valid = false;
-          const __nv_bfloat16 *src = in_addr8(in, g, rz[i], rz[i] + dz, ry[i] + dy, rx[i] + dx, c, valid);
-          cp16_zfill(sa + off_kmajor((tid >> 3) + 16 * i, 8 * g8), src, valid && rv[i] && t < 27);
+          const int z = rz[i] + dz, y = ry[i] + dy, x = rx[i] + dx;
+          const bool valid = rv[i] && t < 27 && z >= rzb[i] && z < rzb[i] + g.Dc && (unsigned)y < (unsigned)g.H &&
+                             (unsigned)x < (unsigned)g.W;
+          const long cv = ((long)(z >> 1) * Hc + (y >> 1)) * Wc + (x >> 1);
+          cp16_zfill(sa + off_kmajor((tid >> 3) + 16 * i, 8 * g8), valid ? tb + cv * in.c1 : in.x1, valid);
         }
       } else {  // same-grid input: one voxel offset for the tap, bounds per row
         const long dv = ((long)dz * g.H + dy) * g.W + dx;
@@ -514,73 +504,130 @@ __global__ void __launch_bounds__(128) k_conv_direct(ConvIn in, ConvGeom g, int 
   }
 }
 
-// z-marching direct convolution for 16-channel inputs on grids whose x rows
-// are multiples of 128 voxels (the network's half-resolution level 0). A CTA
-// owns 128 consecutive x positions of TY output rows and marches along z
-// through up to ZC output planes of one item. Each input plane of
-// (TY + 2) rows x 130 voxels (the x and y halos) arrives once, by two
-// tensor-map copies (channels 0-7 and 8-15; zeros outside the grid), into a
-// ring of four plane slots laid out as
-//     byte cg * CG + (r * 130 + xi) * 16,   cg = channel group of 8,
-// so that, as in k_conv_direct, every tap (dz, dy, dx) of output row r is a
-// canonical K-major 128 x 16 A operand starting at row r + 1 + dy, voxel
-// 1 + dx of the slot of plane z + dz (SBO 128 B, LBO CG). Taps reaching past
-// the item's z faces are not issued (zero padding). Lane 0 of warp r issues
-// the 27 MMAs of output row r of a plane into one of two TMEM accumulator
-// sets and commits them to that set's mbarrier (TY arrivals); while they run,
-// thread 0 refills the slot the previous plane's MMAs have released (two
-// planes ahead) and the four warps read the previous plane's accumulators out
-// (bias, ReLU, store). Every wait is bounded; a CTA that gives up lets its
-// copies and MMAs finish, flags *err and stops.
-constexpr int kZdX = 130;  // staged voxels per row: x0 - 1 .. x0 + 128
+// z-marching direct convolution. A CTA owns XT consecutive x positions
+// (XT = 128, or the whole row when W is 64 or 32) of TY output rows and
+// marches along z through up to ZC output planes of one item. Each input
+// plane of (TY + 2) rows x (XT + 2) voxels (the x and y halos) arrives once,
+// by one tensor-map copy per group of 8 channels (zeros outside the grid),
+// into a ring of NS plane slots laid out as
+//     byte q * CGB + p * 16,   q = channel group, p = r * (XT + 2) + xi,
+// i.e. the staged rows one after the other as one flat row of voxels. The
+// output positions use the same flattening (output row r, column x at
+// p = r * (XT + 2) + x), so tap (dz, dy, dx) of a window of 128 consecutive
+// output positions starting at s is a canonical K-major 128 x 16 A operand
+// starting at staged position s + (1 + dy) * (XT + 2) + 1 + dx of the slot of
+// plane z + dz (SBO 128 B, LBO CGB; the next 16 channels 2 * CGB further).
+// With XT = 128 a window is one output row (s = r * 130); with XT < 128 the
+// windows tile the flattened rows (s = 128 c) and the positions that fall on
+// halo columns (x >= XT) are computed and dropped. Taps reaching past the
+// item's z faces are not issued (zero padding). The staged channels may come
+// from two inputs (a concatenation): kg1 groups of x1, then kg - kg1 of x2.
+//
+// Six warps, each role on its own mbarriers so that copies, MMAs and the
+// read-out of different planes overlap:
+//  * warp 4, one lane: copies plane i into slot i % NS once the MMAs of the
+//    step that last read the slot's previous plane have completed (empty);
+//  * warp 5, one lane: for output plane t, once planes t - 1 .. t + 1 have
+//    landed (full) and the read-out of plane t - 2 has left accumulator set
+//    t % 2 (acce), issues the C windows' 27 x KS MMAs into that set, then
+//    commits them to accf[t % 2] and to empty[slot of plane t - 1];
+//  * warps 0-3 (their TMEM lanes): read plane t's accumulators out when
+//    accf[t % 2] completes, free the set (acce), then bias, ReLU and stores
+//    (or, for a convolution split over its input channels, plain FP32 stores
+//    into the launch's slice of out.acc).
+// Every wait is bounded and also ends when another role has given up; a CTA
+// that gives up lets its copies and MMAs finish, flags *err and stops.
+struct ZfIn {
+  int kg1, kg;  // channel groups of 8 staged per plane: kg1 from x1, kg - kg1 from x2 (kg even)
+  int ch1, ch2; // first staged channel of x1 / of x2
+  int c1, cin;  // channels of x1 and of the concatenation (the weights' K index is tap * cin + channel)
+  int ns;       // plane slots in the ring (>= 4)
+};
 
-template <int TY>
-__host__ __device__ constexpr uint32_t zd_cg_bytes()
+template <int XT, int TY>
+struct Zf {
+  static constexpr int RWD = XT + 2;                                 // staged voxels per row
+  static constexpr int S = XT == 128 ? RWD : 128;                    // output positions between windows
+  static constexpr int C = XT == 128 ? TY : (TY * RWD + 127) / 128;  // windows (128-row MMAs) per plane
+  static constexpr int STAGED = (TY + 2) * RWD;                      // positions one copy writes
+  static constexpr int READ = (C - 1) * S + 128 + 2 * RWD + 2;       // positions the windows' taps read
+  static constexpr uint32_t CGB = ((STAGED > READ ? STAGED : READ) * 16 + 127) / 128 * 128;
+  static constexpr uint32_t BOX_TX = (uint32_t)STAGED * 16;          // bytes of one channel group's copy
+  static_assert(C <= 4, "at most four windows per plane");
+};
+
+template <int N, int XT, int TY>
+__host__ __device__ constexpr uint32_t zf_smem_bytes(int kg, int ns)
 {
-  return ((TY + 2) * kZdX * 16 + 127) / 128 * 128;
+  return (uint32_t)ns * (uint32_t)kg * Zf<XT, TY>::CGB + 27u * (uint32_t)(kg / 2) * N * 32u;
 }
 
-template <int N, int TY>
-__host__ __device__ constexpr uint32_t zd_smem_bytes()
+// Bounded wait that also gives up as soon as another role of the CTA has
+// (*abort set); sets *abort itself when its own polls run out.
+__device__ __forceinline__ bool zf_wait(uint64_t *bar, uint32_t parity, volatile int *abort)
 {
-  return 4 * 2 * zd_cg_bytes<TY>() + 27 * N * 32;
+  for (uint32_t n = 0; n < kWaitLimit / 64; ++n) {
+    if (umma::mbar_wait(bar, parity, 64)) return true;
+    if (*abort) return false;
+  }
+  *abort = 1;
+  return false;
 }
 
-template <int N, int TY>
-__global__ void __launch_bounds__(128, 1) k_conv_zdirect(const __grid_constant__ CUtensorMap xmap, ConvGeom g, int ZC,
-                                                         const __nv_bfloat16 *__restrict__ Bm, int Kp, ConvOut out,
-                                                         int *err)
+template <int N, int XT, int TY>
+__global__ void __launch_bounds__(192, 1) k_conv_zflat(const __grid_constant__ CUtensorMap map1,
+                                                       const __grid_constant__ CUtensorMap map2, ZfIn zi, ConvGeom g,
+                                                       int ZC, const __nv_bfloat16 *__restrict__ Bm, int Kp,
+                                                       ConvOut out, int slice, int *err)
 {
-  constexpr uint32_t CG = zd_cg_bytes<TY>(), SLOT = 2 * CG, PLANE_TX = 2u * (TY + 2) * kZdX * 16;
-  constexpr uint32_t NCOLS = 2 * TY * N <= 32 ? 32 : 2 * TY * N <= 64 ? 64 : 2 * TY * N <= 128 ? 128 : 256;
-  static_assert(2 * TY * N <= 256, "two accumulator sets exceed the TMEM columns allocated");
+  using Z = Zf<XT, TY>;
+  constexpr int C = Z::C, RWD = Z::RWD;
+  constexpr uint32_t CGB = Z::CGB;
+  constexpr uint32_t NCOLS = 2 * C * N <= 32 ? 32 : 2 * C * N <= 64 ? 64 : 2 * C * N <= 128 ? 128 : 2 * C * N <= 256 ? 256 : 512;
+  static_assert(2 * C * N <= 512, "two accumulator sets exceed the TMEM columns");
+  constexpr int kMaxNS = 8;
   extern __shared__ __align__(1024) uint8_t sm[];
-  __shared__ __align__(8) uint64_t full[4];  // plane slot s: its copies (or a plain arrival) of plane i, i % 4 == s
-  __shared__ __align__(8) uint64_t mmab[2];  // accumulator set b: the MMAs of plane step t, t % 2 == b (TY issuers)
+  __shared__ __align__(8) uint64_t full[kMaxNS];   // slot s: the copies (or a plain arrival) of its current plane
+  __shared__ __align__(8) uint64_t empty[kMaxNS];  // slot s: the MMAs that read its current plane last are done
+  __shared__ __align__(8) uint64_t accf[2];        // accumulator set b: the MMAs of plane t, t % 2 == b, are done
+  __shared__ __align__(8) uint64_t acce[2];        // accumulator set b: plane t's read-out is done (4 warps)
   __shared__ __align__(8) uint64_t mdrain;
   __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag, n_issued, n_landed, n_mma;
+  volatile int *abort = &abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int KG = zi.kg, KS = KG >> 1, NS = zi.ns;
+  const uint32_t SLOT = (uint32_t)KG * CGB;
   const int nzc = (g.Dc + ZC - 1) / ZC;
   const int item = blockIdx.z / nzc, zlo = item * g.Dc, zhi = zlo + g.Dc;
   const int z0 = zlo + (blockIdx.z % nzc) * ZC, z1 = min(z0 + ZC, zhi), nz = z1 - z0;
-  const int x0 = blockIdx.x * 128, y0 = blockIdx.y * TY;
-  uint8_t *sb = sm + 4 * SLOT;
-  if (umma::smem_u32(sm) & 127u) {  // tensor copies need 128-byte aligned slots
+  const int x0 = blockIdx.x * XT, y0 = blockIdx.y * TY;
+  uint8_t *sb = sm + (uint32_t)NS * SLOT;
+  if ((umma::smem_u32(sm) & 127u) || NS < 4 || NS > kMaxNS) {  // copies need 128-byte aligned slots
     if (tid == 0) atomicExch(err, 1);
     return;
   }
   if (warp == 0) umma::tmem_alloc(&tmem_base, NCOLS);
   if (tid == 0) {
-    for (int q = 0; q < 4; ++q) umma::mbar_init(&full[q], 1);
-    umma::mbar_init(&mmab[0], TY);
-    umma::mbar_init(&mmab[1], TY);
-    umma::mbar_init(&mdrain, TY);
+    for (int q = 0; q < NS; ++q) {
+      umma::mbar_init(&full[q], 1);
+      umma::mbar_init(&empty[q], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      umma::mbar_init(&accf[b], 1);
+      umma::mbar_init(&acce[b], 4);
+    }
+    umma::mbar_init(&mdrain, 1);
     umma::fence_mbar_init();
+    abort_flag = 0;
+    n_issued = n_landed = n_mma = 0;
   }
-  // the weights of the 27 taps (K = 16), canonical K-major: tap t, row n, k-group kg
-  for (int idx = tid; idx < 27 * N * 2; idx += 128) {
-    const int t = idx / (N * 2), rem = idx - t * N * 2, n = rem >> 1, kg = rem & 1;
-    cp16_zfill(sb + t * N * 32 + (n >> 3) * 256 + kg * 128 + (n & 7) * 16, Bm + (long)n * Kp + t * 16 + 8 * kg, true);
+  // the weights, canonical K-major blocks of N rows x 16 channels, block (ks, tap) at (ks * 27 + tap) * N * 32
+  for (int idx = tid; idx < 27 * KS * N * 2; idx += 192) {
+    const int blk = idx / (N * 2), rem = idx - blk * N * 2, n = rem >> 1, kl = rem & 1;
+    const int ks = blk / 27, t = blk - ks * 27, q = 2 * ks + kl;
+    const int cc = q < zi.kg1 ? zi.ch1 + 8 * q : zi.c1 + zi.ch2 + 8 * (q - zi.kg1);
+    cp16_zfill(sb + blk * N * 32 + (n >> 3) * 256 + kl * 128 + (n & 7) * 16, Bm + (long)n * Kp + t * zi.cin + cc, true);
   }
   asm volatile("cp.async.commit_group;" ::: "memory");
   asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -589,133 +636,158 @@ __global__ void __launch_bounds__(128, 1) k_conv_zdirect(const __grid_constant__
   __syncthreads();
   umma::fence_after_sync();
   const uint32_t tmem = tmem_base;
-  constexpr uint32_t idesc = umma::idesc_bf16(128, N, 0, 0);
-  const uint32_t a0 = umma::smem_u32(sm), b0 = umma::smem_u32(sb);
-  // plane index i is z = z0 - 1 + i, in slot i % 4; planes outside the item
-  // (or past z1) get a plain arrival instead of copies
-  int issued = 0, landed = 0;
-  auto issue = [&](int i) {
-    const int z = z0 - 1 + i;
-    uint64_t *bar = &full[i & 3];
-    if (z < zlo || z >= zhi || z > z1) {
-      umma::mbar_arrive(bar);
-    } else {
-      umma::mbar_expect_tx(bar, PLANE_TX);
-      uint8_t *dst = sm + (i & 3) * SLOT;
-      umma::tma_load4(dst, &xmap, 0, x0 - 1, y0 - 1, z, bar);
-      umma::tma_load4(dst + CG, &xmap, 8, x0 - 1, y0 - 1, z, bar);
-    }
-  };
-  if (tid == 0)
-    for (; issued < 3; ++issued) issue(issued);
-  bool ok = true;
-  auto epilogue = [&](int t) {  // output plane z0 + t from accumulator set t % 2
-    const int z = z0 + t, x = x0 + warp * 32 + lane;
-    const int ny = min(TY, g.H - y0);  // rows of this tile inside the grid
-    // every row's accumulators at once, then one wait: the loads overlap
-    uint32_t raw[TY][N];
-#pragma unroll
-    for (int r = 0; r < TY; ++r)
-#pragma unroll
-      for (int c0 = 0; c0 < N; c0 += 16)
-        if (r < ny)  // warp-uniform
-          umma::tmem_ld16_async(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((t & 1) * TY * N + r * N + c0),
-                                *reinterpret_cast<uint32_t(*)[16]>(&raw[r][c0]));
-    umma::tmem_wait_ld();
-#pragma unroll
-    for (int r = 0; r < TY; ++r) {
-      if (r >= ny) break;
-      const long v = ((long)z * g.H + y0 + r) * g.W + x;
-#pragma unroll
-      for (int c0 = 0; c0 < N; c0 += 8) {
-        float f[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) f[q] = __uint_as_float(raw[r][c0 + q]);
-        if (out.bias) {
-#pragma unroll
-          for (int q = 0; q < 8; ++q) f[q] += __ldg(out.bias + c0 + q);
-        }
-        if (out.relu) {
-#pragma unroll
-          for (int q = 0; q < 8; ++q) f[q] = fmaxf(f[q], 0.0f);
-        }
-        if (out.yf) {
-          float4 *dst = reinterpret_cast<float4 *>(out.yf + v * N + c0);
-          dst[0] = make_float4(f[0], f[1], f[2], f[3]);
-          dst[1] = make_float4(f[4], f[5], f[6], f[7]);
+
+  if (warp == 4) {
+    // ---- producer: plane index i is z = z0 - 1 + i (i = 0 .. nz + 1); planes
+    // outside the item get a plain arrival instead of copies
+    if (lane == 0) {
+      int i = 0;
+      for (; i <= nz + 1; ++i) {
+        const int s = i % NS, k = i / NS;
+        if (k >= 1 && !zf_wait(&empty[s], (uint32_t)(k - 1) & 1u, abort)) break;
+        const int z = z0 - 1 + i;
+        if (z < zlo || z >= zhi) {
+          umma::mbar_arrive(&full[s]);
         } else {
-          uint4 pk;
-          __nv_bfloat162 *h2 = reinterpret_cast<__nv_bfloat162 *>(&pk);
-#pragma unroll
-          for (int q = 0; q < 4; ++q) h2[q] = __floats2bfloat162_rn(f[2 * q], f[2 * q + 1]);
-          *reinterpret_cast<uint4 *>(out.y + v * N + c0) = pk;
+          umma::mbar_expect_tx(&full[s], (uint32_t)KG * Z::BOX_TX);
+          uint8_t *dst = sm + (uint32_t)s * SLOT;
+          for (int q = 0; q < zi.kg1; ++q)
+            umma::tma_load4(dst + q * CGB, &map1, zi.ch1 + 8 * q, x0 - 1, y0 - 1, z, &full[s]);
+          for (int q = zi.kg1; q < KG; ++q)
+            umma::tma_load4(dst + q * CGB, &map2, zi.ch2 + 8 * (q - zi.kg1), x0 - 1, y0 - 1, z, &full[s]);
         }
       }
+      n_issued = i;
     }
-  };
-  const bool issuer = warp < TY && lane == 0;  // issues output row r = warp
-  // descriptors of the tap (dz, dy, dx) = (0, -1, -1) of row `warp` in slot 0 and of tap 0's weights;
-  // the other taps and slots are fixed offsets from them (16-byte units in the address field)
-  const uint64_t ad0 = umma::desc(a0 + (uint32_t)(warp * kZdX) * 16, CG, 128);
-  const uint64_t bd0 = umma::desc(b0, 128, 256);
-  for (int t = 0; t < nz; ++t) {
-    const int z = z0 + t;
-    if (issuer) {
-      for (; ok && landed <= t + 2; ++landed) ok = umma::mbar_wait(&full[landed & 3], (landed >> 2) & 1, kWaitLimit);
-      if (ok) {
+  } else if (warp == 5) {
+    // ---- MMA issuer
+    if (lane == 0) {
+      constexpr uint32_t idesc = umma::idesc_bf16(128, N, 0, 0);
+      const uint32_t a0 = umma::smem_u32(sm), b0 = umma::smem_u32(sb);
+      const uint64_t ad0 = umma::desc(a0, CGB, 128);  // tap (0, -1, -1), first K step, window 0, slot 0
+      const uint64_t bd0 = umma::desc(b0, 128, 256);  // weights block (0, 0)
+      int landed = 0, t = 0;
+      for (; t < nz; ++t) {
+        bool ok = true;
+        for (; ok && landed <= t + 2; ++landed) ok = zf_wait(&full[landed % NS], (uint32_t)(landed / NS) & 1u, abort);
+        if (ok && t >= 2) ok = zf_wait(&acce[t & 1], (uint32_t)((t - 2) >> 1) & 1u, abort);
+        if (!ok) break;
         umma::fence_after_sync();
-        const uint32_t acc = tmem + (uint32_t)((t & 1) * TY * N + warp * N);
-        uint32_t first = 1;
-        int tap = 0;
-        for (int dz = -1; dz <= 1; ++dz) {
-          if (z + dz < zlo || z + dz >= zhi) {
-            tap += 9;
+        const int z = z0 + t;
+        uint64_t sofs[3];  // slot offsets of planes z - 1, z, z + 1 (16-byte units)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) sofs[d] = (uint64_t)((t + d) % NS) * (SLOT >> 4);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const uint32_t acc = tmem + (uint32_t)((t & 1) * C * N + c * N);
+          const uint64_t adc = ad0 + (uint64_t)(c * Z::S);
+          uint32_t accum = 0;
+          for (int ks = 0; ks < KS; ++ks) {
+            const uint64_t aks = adc + (uint64_t)ks * (2 * CGB >> 4), bks = bd0 + (uint64_t)(ks * 27 * N * 2);
+#pragma unroll
+            for (int dz = -1; dz <= 1; ++dz) {
+              if (z + dz < zlo || z + dz >= zhi) continue;
+              const uint64_t as = aks + sofs[dz + 1];
+#pragma unroll
+              for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+                for (int dx = 0; dx < 3; ++dx) {
+                  constexpr int kN2 = N * 2;  // one block of N x 16 weights, 16-byte units
+                  umma::mma_bf16(acc, as + (uint64_t)(dy * RWD + dx),
+                                 bks + (uint64_t)(((dz + 1) * 9 + dy * 3 + dx) * kN2), idesc, accum);
+                  accum = 1;
+                }
+            }
+          }
+        }
+        umma::mma_commit(&accf[t & 1]);
+        // plane index t (z - 1) is read by no later step: free its slot if a later plane needs it
+        if (t + NS <= nz + 1) umma::mma_commit(&empty[t % NS]);
+      }
+      n_landed = landed;
+      n_mma = t;
+    }
+  } else {
+    // ---- read-out: warps 0-3, TMEM lanes 32 warp .. 32 warp + 31
+    const int ny = min(TY, g.H - y0);  // rows of this tile inside the grid
+    constexpr int WB = C * N <= 64 ? C : 64 / N > 0 ? 64 / N : 1;  // windows per TMEM wait (<= 64 registers)
+    for (int t = 0; t < nz; ++t) {
+      if (!zf_wait(&accf[t & 1], (uint32_t)(t >> 1) & 1u, abort)) break;
+      umma::fence_after_sync();
+      const int z = z0 + t;
+#pragma unroll
+      for (int c = 0; c < C; c += WB) {
+        uint32_t raw[WB][N];
+#pragma unroll
+        for (int w = 0; w < WB; ++w)
+#pragma unroll
+          for (int c0 = 0; c0 < N; c0 += 16)
+            if (c + w < C)
+              umma::tmem_ld16_async(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((t & 1) * C * N + (c + w) * N + c0),
+                                    *reinterpret_cast<uint32_t(*)[16]>(&raw[w][c0]));
+        umma::tmem_wait_ld();
+        if (c + WB >= C) {  // this warp's lanes of set t % 2 are all read
+          umma::fence_before_sync();
+          if (lane == 0) umma::mbar_arrive(&acce[t & 1]);
+        }
+#pragma unroll
+        for (int w = 0; w < WB; ++w) {
+          if (c + w >= C) break;
+          const int p = (c + w) * Z::S + warp * 32 + lane, r = p / RWD, x = p - r * RWD;
+          if (r >= ny || x >= XT) continue;
+          const long v = ((long)z * g.H + y0 + r) * g.W + x0 + x;
+          if (slice >= 0) {  // FP32 partial sum of this launch's channels
+            float4 *dst = reinterpret_cast<float4 *>(out.acc + ((long)slice * g.V + v) * N);
+#pragma unroll
+            for (int c0 = 0; c0 < N; c0 += 4)
+              dst[c0 / 4] = make_float4(__uint_as_float(raw[w][c0]), __uint_as_float(raw[w][c0 + 1]),
+                                        __uint_as_float(raw[w][c0 + 2]), __uint_as_float(raw[w][c0 + 3]));
             continue;
           }
-          const uint64_t as = ad0 + (uint64_t)(((t + 1 + dz) & 3) * (SLOT >> 4));
-          for (int dy = 0; dy < 3; ++dy)
-            for (int dx = 0; dx < 3; ++dx, ++tap) {
-              const uint64_t ad = as + (uint64_t)((dy * kZdX + dx) * 1);  // 16-byte units: one voxel
-              const uint64_t bd = bd0 + (uint64_t)(tap * N * 2);          // tap * N * 32 bytes
-              umma::mma_bf16(acc, ad, bd, idesc, first ? 0u : 1u);
-              first = 0;
+#pragma unroll
+          for (int c0 = 0; c0 < N; c0 += 8) {
+            float f[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) f[q] = __uint_as_float(raw[w][c0 + q]);
+            if (out.bias) {
+#pragma unroll
+              for (int q = 0; q < 8; ++q) f[q] += __ldg(out.bias + c0 + q);
             }
+            if (out.relu) {
+#pragma unroll
+              for (int q = 0; q < 8; ++q) f[q] = fmaxf(f[q], 0.0f);
+            }
+            if (out.yf) {
+              float4 *dst = reinterpret_cast<float4 *>(out.yf + v * N + c0);
+              dst[0] = make_float4(f[0], f[1], f[2], f[3]);
+              dst[1] = make_float4(f[4], f[5], f[6], f[7]);
+            } else {
+              uint4 pk;
+              __nv_bfloat162 *h2 = reinterpret_cast<__nv_bfloat162 *>(&pk);
+#pragma unroll
+              for (int q = 0; q < 4; ++q) h2[q] = __floats2bfloat162_rn(f[2 * q], f[2 * q + 1]);
+              *reinterpret_cast<uint4 *>(out.y + v * N + c0) = pk;
+            }
+          }
         }
-        umma::mma_commit(&mmab[t & 1]);
       }
     }
-    // thread 0 refills the slot step t - 1's MMAs read last (plane index t - 1) with plane index t + 3
-    if (tid == 0 && ok && issued <= nz + 1) {
-      if (t >= 1) ok = umma::mbar_wait(&mmab[(t - 1) & 1], ((t - 1) >> 1) & 1, kWaitLimit);
-      if (ok) issue(issued++);
-    }
-    if (t >= 1 && ok) {
-      ok = umma::mbar_wait(&mmab[(t - 1) & 1], ((t - 1) >> 1) & 1, kWaitLimit);
-      umma::fence_after_sync();
-      if (ok) epilogue(t - 1);
-    }
-    umma::fence_before_sync();
-    if (__syncthreads_or(!ok)) {
-      ok = false;
-      break;
-    }
-    umma::fence_after_sync();
-  }
-  if (ok && nz > 0) {
-    ok = umma::mbar_wait(&mmab[(nz - 1) & 1], ((nz - 1) >> 1) & 1, kWaitLimit);
-    umma::fence_after_sync();
-    if (ok) epilogue(nz - 1);
-  }
-  if (__syncthreads_or(!ok)) {
-    // a wait gave up: let every issued copy land and every issued MMA finish before TMEM and the slots go
-    if (tid == 0) {
-      atomicExch(err, 1);
-      for (; landed < issued; ++landed) umma::mbar_wait(&full[landed & 3], (landed >> 2) & 1, kWaitLimit);
-    }
-    umma::mma_drain(&mdrain, issuer, kWaitLimit);
   }
   umma::fence_before_sync();
   __syncthreads();
+  umma::fence_after_sync();
+  if (abort_flag) {
+    // a wait gave up: let every issued copy land and every issued MMA finish before TMEM and the slots go
+    if (tid == 0) atomicExch(err, 1);
+    if (tid == 160) {  // the issuer's thread: its MMAs tracked by one more commit
+      umma::mma_commit(&mdrain);
+      umma::mbar_wait(&mdrain, 0, kWaitLimit);
+      for (int i = n_landed; i < n_issued; ++i) umma::mbar_wait(&full[i % NS], (uint32_t)(i / NS) & 1u, kWaitLimit);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+  }
   if (warp == 0) {
     umma::fence_after_sync();
     umma::tmem_dealloc(tmem, NCOLS);
@@ -835,12 +907,56 @@ __global__ void k_conv_finish(const float *__restrict__ acc, int split, long V, 
   for (long i = threadIdx.x + (long)blockIdx.x * blockDim.x; i < V * N; i += (long)gridDim.x * blockDim.x) {
     float a = acc[i];
     for (int y = 1; y < split; ++y) a += acc[(long)y * V * N + i];
-    if (out.bias) a += __ldg(out.bias + (int)(i % N));
+    if (out.bias) a += __ldg(out.bias + (int)(i & (N - 1)));
     if (out.relu) a = fmaxf(a, 0.0f);
     if (out.mask && !(__bfloat162float(out.mask[i]) > 0.0f)) a = 0.0f;
     if (out.yf) out.yf[i] = a;
     else out.y[i] = __float2bfloat16_rn(a);
   }
+}
+
+// The same, four consecutive elements per thread (16-byte aligned outputs):
+// the same sums in the same order.
+__global__ void k_conv_finish4(const float *__restrict__ acc, int split, long V, int N, ConvOut out)
+{
+  const long n4 = V * N / 4, slice4 = V * N / 4;
+  const float4 *a4 = reinterpret_cast<const float4 *>(acc);
+  for (long i = threadIdx.x + (long)blockIdx.x * blockDim.x; i < n4; i += (long)gridDim.x * blockDim.x) {
+    float4 a = a4[i];
+    for (int y = 1; y < split; ++y) {
+      const float4 b = a4[(long)y * slice4 + i];
+      a.x += b.x;
+      a.y += b.y;
+      a.z += b.z;
+      a.w += b.w;
+    }
+    float f[4] = {a.x, a.y, a.z, a.w};
+    const int n0 = (int)((i * 4) & (N - 1));
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (out.bias) f[q] += __ldg(out.bias + n0 + q);
+      if (out.relu) f[q] = fmaxf(f[q], 0.0f);
+      if (out.mask && !(__bfloat162float(out.mask[i * 4 + q]) > 0.0f)) f[q] = 0.0f;
+    }
+    if (out.yf) {
+      reinterpret_cast<float4 *>(out.yf)[i] = make_float4(f[0], f[1], f[2], f[3]);
+    } else {
+      uint2 pk;
+      __nv_bfloat162 *h2 = reinterpret_cast<__nv_bfloat162 *>(&pk);
+      h2[0] = __floats2bfloat162_rn(f[0], f[1]);
+      h2[1] = __floats2bfloat162_rn(f[2], f[3]);
+      reinterpret_cast<uint2 *>(out.y)[i] = pk;
+    }
+  }
+}
+
+void launch_finish(const float *acc, int split, long V, int N, const ConvOut &out, cudaStream_t s)
+{
+  const bool vec = out.yf ? reinterpret_cast<uintptr_t>(out.yf) % 16 == 0 : reinterpret_cast<uintptr_t>(out.y) % 8 == 0;
+  const long total = vec ? V * N / 4 : V * N;
+  const unsigned blocks = (unsigned)std::min<long>((total + 255) / 256, 148L * 16);
+  if (vec) k_conv_finish4<<<blocks, 256, 0, s>>>(acc, split, V, N, out);
+  else k_conv_finish<<<blocks, 256, 0, s>>>(acc, split, V, N, out);
 }
 
 // FP32 partial-sum buffers of the split-K convolutions, one per (device,
@@ -903,8 +1019,7 @@ qesb_status launch_conv(const ConvIn &in, const ConvGeom &g, int sign, const __n
   if (three) k_conv_igemm<N, 3><<<dim3(blocks, split), 128, smem, s>>>(in, g, sign, Bm, Kp, o, err);
   else k_conv_igemm<N, 4><<<dim3(blocks, split), 128, smem, s>>>(in, g, sign, Bm, Kp, o, err);
   if (split > 1) {
-    const long total = g.V * N;
-    k_conv_finish<<<(unsigned)std::min<long>((total + 255) / 256, 148L * 16), 256, 0, s>>>(o.acc, split, g.V, N, out);
+    launch_finish(o.acc, split, g.V, N, out, s);
   }
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));
@@ -948,41 +1063,143 @@ EncodeTiledFn encode_tiled()
   return fn;
 }
 
-template <int N, int TY>
-qesb_status launch_conv_zdirect(const ConvIn &in, const ConvGeom &g, const __nv_bfloat16 *Bm, int Kp,
-                                const ConvOut &out, int *err, cudaStream_t s)
+// An input as a 4-D tensor (channel, x, y, z over all items), boxes of 8
+// channels x (XT + 2) voxels x (TY + 2) rows x 1 plane; zeros outside.
+qesb_status zf_map(CUtensorMap *map, const __nv_bfloat16 *x, int c, const ConvGeom &g, int XT, int TY)
 {
-  constexpr int smem = (int)zd_smem_bytes<N, TY>();
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return qesb_fail(QESB_ERR_CUDA, "cuTensorMapEncodeTiled not available");
+  const cuuint64_t cb = (cuuint64_t)c * 2;
+  const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)g.W, (cuuint64_t)g.H, (cuuint64_t)g.D};
+  const cuuint64_t st[3] = {cb, (cuuint64_t)g.W * cb, (cuuint64_t)g.W * g.H * cb};
+  const cuuint32_t box[4] = {8, (cuuint32_t)(XT + 2), (cuuint32_t)(TY + 2), 1}, one[4] = {1, 1, 1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(x), dims, st, box, one,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return qesb_fail(QESB_ERR_CUDA, "conv tensor map: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return QESB_OK;
+}
+
+int max_dyn_smem()
+{
+  int dev = 0, v = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return v - 1024;  // room for the kernel's static shared memory
+}
+
+// Launches (channel splits) the z-marching convolution needs for cin input
+// channels: the fewest whose 16-channel K steps, shared out evenly, fit the
+// shared memory; 0 when even one step does not fit.
+template <int N, int XT, int TY>
+int zf_splits(int cin)
+{
+  const int steps = cin / 16, lim = max_dyn_smem();
+  for (int P = 1; P <= steps; ++P)
+    if ((int)zf_smem_bytes<N, XT, TY>(2 * ((steps + P - 1) / P), 4) <= lim) return P;
+  return 0;
+}
+
+// z-marching convolution of x1 (c1 channels) concatenated with x2 (c2), both
+// on the output grid. Split over its input channels when the weights and the
+// plane ring do not fit one CTA's shared memory: each launch stores its FP32
+// partial sums in its own slice, k_conv_finish adds them in launch order and
+// applies the epilogue.
+template <int N, int XT, int TY>
+qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, const __nv_bfloat16 *x2, int c2, const ConvGeom &g,
+                              const __nv_bfloat16 *Bm, int Kp, const ConvOut &out, int *err, cudaStream_t s)
+{
+  const int cin = c1 + c2, steps = cin / 16, P = zf_splits<N, XT, TY>(cin);
+  if (P == 0) return qesb_fail(QESB_ERR_ARG, "qesb_conv3d: %d channels do not fit the z-marching kernel", cin);
+  const int per = (steps + P - 1) / P;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  static bool attr[64] = {};
-  if (!attr[dev & 63]) {
-    cudaError_t e = cudaFuncSetAttribute(k_conv_zdirect<N, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  // plane slots: four when two CTAs fit an SM, else as many as fit (at most eight)
+  const int lim = max_dyn_smem();
+  int ns = 4;
+  if (2 * ((int)zf_smem_bytes<N, XT, TY>(2 * per, 4) + 1024) > lim + 1024)
+    while (ns < 8 && (int)zf_smem_bytes<N, XT, TY>(2 * per, ns + 1) <= lim) ++ns;
+  static int attr[64] = {};  // dynamic shared memory allowed so far, per device
+  const int need = (int)zf_smem_bytes<N, XT, TY>(2 * per, ns);
+  if (attr[dev & 63] < need) {
+    cudaError_t e = cudaFuncSetAttribute(k_conv_zflat<N, XT, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, need);
     if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv attr: %s", cudaGetErrorString(e));
-    attr[dev & 63] = true;
+    attr[dev & 63] = need;
   }
-  EncodeTiledFn enc = encode_tiled();
-  if (!enc) return qesb_fail(QESB_ERR_CUDA, "cuTensorMapEncodeTiled not available");
-  // the input as a 4-D tensor (channel, x, y, z over all items), boxes of
-  // 8 channels x 130 voxels x (TY + 2) rows x 1 plane; zeros outside
-  const cuuint64_t dims[4] = {16, (cuuint64_t)g.W, (cuuint64_t)g.H, (cuuint64_t)g.D};
-  const cuuint64_t strides[3] = {32, (cuuint64_t)g.W * 32, (cuuint64_t)g.W * g.H * 32};
-  const cuuint32_t box[4] = {8, (cuuint32_t)kZdX, (cuuint32_t)(TY + 2), 1}, one[4] = {1, 1, 1, 1};
-  CUtensorMap map;
-  const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(in.x1), dims, strides,
-                         box, one, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return qesb_fail(QESB_ERR_CUDA, "conv tensor map: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  CUtensorMap map1, map2;
+  qesb_status st = zf_map(&map1, x1, c1, g, XT, TY);
+  if (st != QESB_OK) return st;
+  map2 = map1;
+  if (c2 && (st = zf_map(&map2, x2, c2, g, XT, TY)) != QESB_OK) return st;
+  ConvOut o = out;
+  if (P > 1 && (st = acc_buffer(dev, s, (size_t)P * g.V * N, &o.acc)) != QESB_OK) return st;
   // z chunks: whole items unless that leaves fewer than two CTAs per SM slot
-  const int per_sm = smem <= 110 * 1024 ? 2 : 1;
-  const long xy = (long)(g.W / 128) * ((g.H + TY - 1) / TY), items = g.D / g.Dc;
+  const int per_sm = std::max(1, (max_dyn_smem() + 1024) / (need + 1024));
+  const long xy = (long)(g.W / XT) * ((g.H + TY - 1) / TY), items = g.D / g.Dc;
   int zc = g.Dc;
   while (zc > 2 && xy * items * ((g.Dc + zc - 1) / zc) < 2L * sms * per_sm) zc = (zc + 1) / 2;
-  const dim3 grid(g.W / 128, (g.H + TY - 1) / TY, (unsigned)(items * ((g.Dc + zc - 1) / zc)));
-  k_conv_zdirect<N, TY><<<grid, 128, smem, s>>>(map, g, zc, Bm, Kp, out, err);
+  const dim3 grid(g.W / XT, (g.H + TY - 1) / TY, (unsigned)(items * ((g.Dc + zc - 1) / zc)));
+  for (int p = 0; p < P; ++p) {
+    const int a = p * per, b = std::min(steps, a + per);  // K steps (16 channels) [a, b) of the concatenation
+    ZfIn zi;
+    zi.kg = 2 * (b - a);
+    zi.kg1 = std::max(0, std::min(zi.kg, (c1 - 16 * a) / 8));
+    zi.ch1 = std::min(16 * a, c1);
+    zi.ch2 = std::max(0, 16 * a - c1);
+    zi.c1 = c1;
+    zi.cin = cin;
+    zi.ns = ns;
+    const int smem = (int)zf_smem_bytes<N, XT, TY>(zi.kg, ns);
+    k_conv_zflat<N, XT, TY><<<grid, 192, smem, s>>>(map1, map2, zi, g, zc, Bm, Kp, o, P > 1 ? p : -1, err);
+  }
+  if (P > 1) {
+    launch_finish(o.acc, P, g.V, N, out, s);
+  }
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));
+}
+
+// Nearest-neighbour x2 upsampling of a coarse grid (D/2 x H/2 x W/2, c
+// channels) onto the output grid, 16 bytes (8 channels) per thread.
+__global__ void k_up2(const __nv_bfloat16 *__restrict__ x, ConvGeom g, int c, __nv_bfloat16 *__restrict__ y)
+{
+  const int cg = c / 8, n = g.W * cg;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int xq = i / cg, q = i - xq * cg;
+  for (long row = blockIdx.y; row < (long)g.D * g.H; row += gridDim.y) {
+    const int zq = (int)(row / g.H), yq = (int)(row - (long)zq * g.H);
+    const long cv = ((long)(zq >> 1) * (g.H >> 1) + (yq >> 1)) * (g.W >> 1) + (xq >> 1);
+    reinterpret_cast<uint4 *>(y)[row * n + i] = __ldg(reinterpret_cast<const uint4 *>(x) + cv * cg + q);
+  }
+}
+
+// Upsampled-input buffers, one per (device, stream) like the split-K ones.
+struct UpBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+};
+std::mutex g_up_mu;
+std::map<std::pair<int, cudaStream_t>, UpBuf> g_up;
+
+qesb_status up_buffer(int dev, cudaStream_t s, size_t bytes, void **out)
+{
+  std::lock_guard<std::mutex> lk(g_up_mu);
+  UpBuf &b = g_up[{dev, s}];
+  if (b.cap < bytes) {
+    if (b.p) {
+      cudaStreamSynchronize(s);  // the old buffer may still be read by this stream's work
+      cudaFree(b.p);
+    }
+    b.p = nullptr;
+    b.cap = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv upsampling buffer: %s", cudaGetErrorString(e));
+    b.cap = bytes;
+  }
+  *out = b.p;
+  return QESB_OK;
 }
 
 template <int N>
@@ -1064,13 +1281,53 @@ extern "C" qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const 
             static_cast<const __nv_bfloat16 *>(mask)};
   const auto *B = static_cast<const __nv_bfloat16 *>(Bm);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const bool zd = (g_conv_path == 0 || g_conv_path >= 3) && W % 128 == 0 &&
-                  (N == 16 || N == 32) && c1 == 16 && c2 == 0 && !up1 && sign == 1 && !mask &&
-                  reinterpret_cast<uintptr_t>(x1) % 16 == 0;
-  if (zd) {
+  const auto aligned = [](const void *p) { return reinterpret_cast<uintptr_t>(p) % 16 == 0; };
+  const bool fwd = sign == 1 && !mask && aligned(x1) && (!c2 || aligned(x2));
+  if (fwd && g_conv_path == 0 && N <= 64) {
+    // the z-marching kernel: rows of 128 (two output rows per CTA, one when
+    // the channels of two do not fit unsplit), or whole rows of 64 or 32
+    int xt = 0, ty = 0;
+    const int cin = c1 + c2;
+    if (W % 128 == 0) {
+      xt = 128;
+      const int p2 = N == 16 ? zf_splits<16, 128, 2>(cin) : N == 32 ? zf_splits<32, 128, 2>(cin) : zf_splits<64, 128, 2>(cin);
+      const int p1 = N == 16 ? zf_splits<16, 128, 1>(cin) : N == 32 ? zf_splits<32, 128, 1>(cin) : zf_splits<64, 128, 1>(cin);
+      ty = p2 == 1 || p1 != 1 ? 2 : 1;
+    } else if (W == 64) {
+      xt = 64, ty = 4;
+    } else if (W == 32) {
+      xt = 32, ty = 8;
+    }
+    if (xt) {
+      const __nv_bfloat16 *xa = in.x1;
+      if (up1) {  // the upsampled input on the output grid first
+        void *u = nullptr;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        qesb_status st = up_buffer(dev, s, (size_t)g.V * c1 * 2, &u);
+        if (st != QESB_OK) return st;
+        const int n = W * (c1 / 8);
+        const dim3 grid((unsigned)((n + 255) / 256), (unsigned)std::min<long>((long)g.D * H, 65535L));
+        k_up2<<<grid, 256, 0, s>>>(in.x1, g, c1, static_cast<__nv_bfloat16 *>(u));
+        xa = static_cast<const __nv_bfloat16 *>(u);
+      }
+      const __nv_bfloat16 *xb = in.x2;
+#define QESB_ZF(NN, XT_, TY_) launch_conv_zflat<NN, XT_, TY_>(xa, c1, xb, c2, g, B, Kp, o, err, s)
+      if (xt == 128 && ty == 2) return N == 16 ? QESB_ZF(16, 128, 2) : N == 32 ? QESB_ZF(32, 128, 2) : QESB_ZF(64, 128, 2);
+      if (xt == 128) return N == 16 ? QESB_ZF(16, 128, 1) : N == 32 ? QESB_ZF(32, 128, 1) : QESB_ZF(64, 128, 1);
+      if (xt == 64) return N == 16 ? QESB_ZF(16, 64, 4) : N == 32 ? QESB_ZF(32, 64, 4) : QESB_ZF(64, 64, 4);
+      return N == 16 ? QESB_ZF(16, 32, 8) : N == 32 ? QESB_ZF(32, 32, 8) : QESB_ZF(64, 32, 8);
+#undef QESB_ZF
+    }
+  }
+  // paths 3, 4, 5: the z-marching kernel for one 16-channel input only (4 rows per CTA on path 4, else 2)
+  if (fwd && g_conv_path >= 3 && W % 128 == 0 && (N == 16 || N == 32) && c1 == 16 && c2 == 0 &&
+      !up1) {
     if (g_conv_path == 4)
-      return N == 16 ? launch_conv_zdirect<16, 4>(in, g, B, Kp, o, err, s) : launch_conv_zdirect<32, 4>(in, g, B, Kp, o, err, s);
-    return N == 16 ? launch_conv_zdirect<16, 2>(in, g, B, Kp, o, err, s) : launch_conv_zdirect<32, 2>(in, g, B, Kp, o, err, s);
+      return N == 16 ? launch_conv_zflat<16, 128, 4>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s)
+                     : launch_conv_zflat<32, 128, 4>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s);
+    return N == 16 ? launch_conv_zflat<16, 128, 2>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s)
+                   : launch_conv_zflat<32, 128, 2>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s);
   }
   if ((g_conv_path == 0 || g_conv_path >= 2) && W % 128 == 0 && (N == 16 || N == 32)) {
     if (N == 16) return launch_conv_direct<16>(in, g, sign, B, Kp, o, err, s);

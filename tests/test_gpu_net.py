@@ -304,3 +304,56 @@ def test_conv3d_zmarch_and_direct_paths_match_torch(conv_path, path, items, D, H
                 ref = torch.relu(ref)
             tol = 1e-4 if fp32 else 1e-2
             np.testing.assert_allclose(out[i].numpy(), _cl(ref).numpy(), rtol=tol, atol=tol)
+
+
+@pytest.mark.parametrize("items,D,H,W,c1,c2,up,co", [
+    (2, 4, 6, 64, 16, 0, 0, 32),     # rows of 64, a partial row tile
+    (1, 5, 9, 64, 32, 0, 0, 32),
+    (2, 4, 8, 64, 64, 32, 1, 32),    # upsampled + concatenated input, split over its channels
+    (2, 4, 8, 32, 32, 0, 0, 64),     # rows of 32
+    (1, 4, 10, 32, 64, 0, 0, 64),    # rows of 32 that would need a split: the implicit GEMM instead
+    (1, 4, 6, 128, 32, 16, 1, 16),   # rows of 128, one output row per CTA (48 channels unsplit)
+    (2, 2, 3, 128, 16, 0, 0, 32),
+    (1, 4, 4, 256, 16, 16, 0, 16),   # two row tiles, a concatenation without upsampling
+    (1, 2, 4, 64, 128, 64, 1, 64),   # twelve channel splits
+])
+def test_conv3d_zmarch_flat_windows_match_torch(conv_path, items, D, H, W, c1, c2, up, co):
+    """The default forward path: the z-marching kernel with flattened 128-row
+    windows (rows of 64 and 32 voxels), concatenated and upsampled inputs
+    (the upsampling done on the output grid first), and channel splits whose
+    FP32 partial sums are added in launch order; stacked items, partial row
+    tiles; against torch per item and against the implicit GEMM."""
+    import torch
+    torch.manual_seed(items + D + H + W + c1 + c2 + co)
+    ci = c1 + c2
+    x1 = [_bf16(torch.randn(1, c1, D // 2, H // 2, W // 2) if up else torch.randn(1, c1, D, H, W))
+          for _ in range(items)]
+    x2 = [_bf16(torch.randn(1, c2, D, H, W)) for _ in range(items)] if c2 else None
+    w = _bf16(torch.randn(co, ci, 3, 3, 3) / (27 * ci) ** 0.5)
+    b = torch.randn(co)
+    bm, kp = _bm_forward(w)
+    dev = "cuda:0"
+    x1d = torch.cat([_cl(t) for t in x1], 0).to(dev)
+    x2d = torch.cat([_cl(t) for t in x2], 0).to(dev) if c2 else None
+    bmd, bd = bm.to(dev), b.float().to(dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    g = lambda t: t.data_ptr() if t is not None else None  # noqa: E731
+
+    def run():
+        yf = torch.zeros(items * D * H * W * co, dtype=torch.float32, device=dev)
+        qesb.check(qesb.lib().qesb_conv3d_items(g(x1d), c1, up, g(x2d), c2, items, D, H, W, 1, g(bmd), kp, co,
+                                                None, g(yf), g(bd), 1, None, g(err), None))
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0
+        return yf.view(items, D, H, W, co).cpu().double()
+
+    conv_path(0)
+    out = run()
+    for i in range(items):
+        xin = torch.nn.functional.interpolate(x1[i].double(), scale_factor=2, mode="nearest") if up else x1[i].double()
+        if c2:
+            xin = torch.cat([xin, x2[i].double()], 1)
+        ref = torch.relu(torch.nn.functional.conv3d(xin, w.double(), b.double(), padding=1))
+        np.testing.assert_allclose(out[i].numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)
+    conv_path(1)
+    np.testing.assert_allclose(out.numpy(), run().numpy(), rtol=1e-5, atol=1e-5)

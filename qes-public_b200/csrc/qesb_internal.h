@@ -20,3 +20,8 @@ qesb_status qesb_handle_grid(qesb_handle *h, int *Nx, int *Ny, int *Nz, int *dev
 // given stream; dz on the device (nz - 1 values, as the grid's dz_array).
 qesb_status qesb_city_walls_dev(int Nx, int Ny, int Nz, float dx, const float *d_dz, const int *d_flag, float *e,
                                 float *f, float *g, float *hc, float *m, float *n, void *stream);
+
+// Forward convolution of one input whose output channel 0 alone is stored:
+// y0 FP32 [V] (the network's head; arguments as qesb_conv3d_items).
+qesb_status qesb_conv3d_head(const void *x1, int c1, int items, int D, int H, int W, const void *Bm, int Kp, int N,
+                             float *y0, const float *bias, int relu, int *err, void *stream);

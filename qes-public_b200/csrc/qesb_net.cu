@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <mutex>
 #include <map>
+#include <tuple>
 
 #include <algorithm>
 #include <cstdint>
@@ -175,6 +176,7 @@ struct ConvOut {
   const __nv_bfloat16 *mask;  // [V][N] (nullable): zero where mask <= 0 (gradient through a ReLU)
   float *acc;             // split-K: [split][V][N] FP32 partial sums, one slice per K split (plain
                           // stores), summed in split order by k_conv_finish with the epilogue
+  int ch0 = 0;            // yf holds output channel 0 alone, FP32 [V] (the z-marching kernel and the sums)
 };
 
 // Y[v][n] = epilogue( sum_k A[v][k] * Bm[n][k] ), A the implicit im2col of
@@ -757,7 +759,9 @@ __global__ void __launch_bounds__(192, 1) k_conv_zflat(const __grid_constant__ C
 #pragma unroll
               for (int q = 0; q < 8; ++q) f[q] = fmaxf(f[q], 0.0f);
             }
-            if (out.yf) {
+            if (out.ch0) {
+              if (c0 == 0) out.yf[v] = f[0];
+            } else if (out.yf) {
               float4 *dst = reinterpret_cast<float4 *>(out.yf + v * N + c0);
               dst[0] = make_float4(f[0], f[1], f[2], f[3]);
               dst[1] = make_float4(f[4], f[5], f[6], f[7]);
@@ -910,8 +914,13 @@ __global__ void k_conv_finish(const float *__restrict__ acc, int split, long V, 
     if (out.bias) a += __ldg(out.bias + (int)(i & (N - 1)));
     if (out.relu) a = fmaxf(a, 0.0f);
     if (out.mask && !(__bfloat162float(out.mask[i]) > 0.0f)) a = 0.0f;
-    if (out.yf) out.yf[i] = a;
-    else out.y[i] = __float2bfloat16_rn(a);
+    if (out.ch0) {
+      if ((i & (N - 1)) == 0) out.yf[i / N] = a;
+    } else if (out.yf) {
+      out.yf[i] = a;
+    } else {
+      out.y[i] = __float2bfloat16_rn(a);
+    }
   }
 }
 
@@ -938,7 +947,9 @@ __global__ void k_conv_finish4(const float *__restrict__ acc, int split, long V,
       if (out.relu) f[q] = fmaxf(f[q], 0.0f);
       if (out.mask && !(__bfloat162float(out.mask[i * 4 + q]) > 0.0f)) f[q] = 0.0f;
     }
-    if (out.yf) {
+    if (out.ch0) {
+      if (n0 == 0) out.yf[i * 4 / N] = f[0];
+    } else if (out.yf) {
       reinterpret_cast<float4 *>(out.yf)[i] = make_float4(f[0], f[1], f[2], f[3]);
     } else {
       uint2 pk;
@@ -952,40 +963,51 @@ __global__ void k_conv_finish4(const float *__restrict__ acc, int split, long V,
 
 void launch_finish(const float *acc, int split, long V, int N, const ConvOut &out, cudaStream_t s)
 {
-  const bool vec = out.yf ? reinterpret_cast<uintptr_t>(out.yf) % 16 == 0 : reinterpret_cast<uintptr_t>(out.y) % 8 == 0;
+  const bool vec = out.ch0 || (out.yf ? reinterpret_cast<uintptr_t>(out.yf) % 16 == 0 : reinterpret_cast<uintptr_t>(out.y) % 8 == 0);
   const long total = vec ? V * N / 4 : V * N;
   const unsigned blocks = (unsigned)std::min<long>((total + 255) / 256, 148L * 16);
   if (vec) k_conv_finish4<<<blocks, 256, 0, s>>>(acc, split, V, N, out);
   else k_conv_finish<<<blocks, 256, 0, s>>>(acc, split, V, N, out);
 }
 
-// FP32 partial-sum buffers of the split-K convolutions, one per (device,
-// stream) so that convolutions on different streams never share one; grown on
-// demand (the network's small levels: a few MB) and kept for the process.
-struct AccBuf {
-  float *p = nullptr;
+// Scratch buffers of the convolutions, one per (kind, device, stream) so that
+// convolutions on different streams never share one; grown on demand and
+// kept for the process. Kinds: FP32 partial sums of split convolutions, the
+// upsampled input on the output grid, a full head output whose channel 0 is
+// taken.
+enum { kScratchAcc = 0, kScratchUp = 1, kScratchHead = 2 };
+struct ScratchBuf {
+  void *p = nullptr;
   size_t cap = 0;
 };
-std::mutex g_acc_mu;
-std::map<std::pair<int, cudaStream_t>, AccBuf> g_acc;
+std::mutex g_scratch_mu;
+std::map<std::tuple<int, int, cudaStream_t>, ScratchBuf> g_scratch;
 
-qesb_status acc_buffer(int dev, cudaStream_t s, size_t need, float **out)
+qesb_status scratch_buffer(int kind, int dev, cudaStream_t s, size_t bytes, void **out)
 {
-  std::lock_guard<std::mutex> lk(g_acc_mu);
-  AccBuf &b = g_acc[{dev, s}];
-  if (b.cap < need) {
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  ScratchBuf &b = g_scratch[{kind, dev, s}];
+  if (b.cap < bytes) {
     if (b.p) {
       cudaStreamSynchronize(s);  // the old buffer may still be read by this stream's work
       cudaFree(b.p);
     }
     b.p = nullptr;
     b.cap = 0;
-    cudaError_t e = cudaMalloc((void **)&b.p, need * sizeof(float));
-    if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv split-K buffer: %s", cudaGetErrorString(e));
-    b.cap = need;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv scratch buffer: %s", cudaGetErrorString(e));
+    b.cap = bytes;
   }
   *out = b.p;
   return QESB_OK;
+}
+
+qesb_status acc_buffer(int dev, cudaStream_t s, size_t need, float **out)
+{
+  void *p = nullptr;
+  const qesb_status st = scratch_buffer(kScratchAcc, dev, s, need * sizeof(float), &p);
+  *out = static_cast<float *>(p);
+  return st;
 }
 
 template <int N>
@@ -1175,33 +1197,6 @@ __global__ void k_up2(const __nv_bfloat16 *__restrict__ x, ConvGeom g, int c, __
   }
 }
 
-// Upsampled-input buffers, one per (device, stream) like the split-K ones.
-struct UpBuf {
-  void *p = nullptr;
-  size_t cap = 0;
-};
-std::mutex g_up_mu;
-std::map<std::pair<int, cudaStream_t>, UpBuf> g_up;
-
-qesb_status up_buffer(int dev, cudaStream_t s, size_t bytes, void **out)
-{
-  std::lock_guard<std::mutex> lk(g_up_mu);
-  UpBuf &b = g_up[{dev, s}];
-  if (b.cap < bytes) {
-    if (b.p) {
-      cudaStreamSynchronize(s);  // the old buffer may still be read by this stream's work
-      cudaFree(b.p);
-    }
-    b.p = nullptr;
-    b.cap = 0;
-    cudaError_t e = cudaMalloc(&b.p, bytes);
-    if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv upsampling buffer: %s", cudaGetErrorString(e));
-    b.cap = bytes;
-  }
-  *out = b.p;
-  return QESB_OK;
-}
-
 template <int N>
 qesb_status launch_wgrad(const ConvIn &in, const ConvGeom &g, const __nv_bfloat16 *dY, long vchunk, float *dW,
                          int *err, cudaStream_t s)
@@ -1268,12 +1263,22 @@ bool conv_args_ok(int c1, int c2, int N, int D, int H, int W, int up1)
 }
 }  // namespace
 
-extern "C" qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const void *x2, int c2, int items, int D,
-                                         int H, int W, int sign, const void *Bm, int Kp, int N, void *y, void *yf,
-                                         const float *bias, int relu, const void *mask, int *err, void *stream)
+namespace {
+
+// Output channel 0 of an FP32 [V][N] tensor.
+__global__ void k_take_ch0(const float *__restrict__ src, int N, long V, float *__restrict__ dst)
+{
+  for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < V; v += (long)gridDim.x * blockDim.x)
+    dst[v] = src[v * N];
+}
+
+qesb_status conv_items(const void *x1, int c1, int up1, const void *x2, int c2, int items, int D, int H, int W,
+                       int sign, const void *Bm, int Kp, int N, void *y, void *yf, const float *bias, int relu,
+                       const void *mask, int *err, void *stream, int ch0)
 {
   if (!conv_args_ok(c1, c2, N, D, H, W, up1) || items < 1 || (items > 1 && D % 2) || !x1 || (c2 && !x2) ||
-      !Bm || (!y && !yf) || !err || (sign != 1 && sign != -1) || Kp < 27 * (c1 + c2) || Kp % 64)
+      !Bm || (!y && !yf) || !err || (sign != 1 && sign != -1) || Kp < 27 * (c1 + c2) || Kp % 64 ||
+      (ch0 && (!yf || y)))
     return qesb_fail(QESB_ERR_ARG, "qesb_conv3d: bad arguments");
   ConvIn in{static_cast<const __nv_bfloat16 *>(x1), static_cast<const __nv_bfloat16 *>(x2), c1, c2, up1};
   ConvGeom g{items * D, H, W, (long)items * D * H * W, D};
@@ -1281,6 +1286,8 @@ extern "C" qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const 
             static_cast<const __nv_bfloat16 *>(mask)};
   const auto *B = static_cast<const __nv_bfloat16 *>(Bm);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int dev = 0;
+  cudaGetDevice(&dev);
   const auto aligned = [](const void *p) { return reinterpret_cast<uintptr_t>(p) % 16 == 0; };
   const bool fwd = sign == 1 && !mask && aligned(x1) && (!c2 || aligned(x2));
   if (fwd && g_conv_path == 0 && N <= 64) {
@@ -1302,9 +1309,7 @@ extern "C" qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const 
       const __nv_bfloat16 *xa = in.x1;
       if (up1) {  // the upsampled input on the output grid first
         void *u = nullptr;
-        int dev = 0;
-        cudaGetDevice(&dev);
-        qesb_status st = up_buffer(dev, s, (size_t)g.V * c1 * 2, &u);
+        qesb_status st = scratch_buffer(kScratchUp, dev, s, (size_t)g.V * c1 * 2, &u);
         if (st != QESB_OK) return st;
         const int n = W * (c1 / 8);
         const dim3 grid((unsigned)((n + 255) / 256), (unsigned)std::min<long>((long)g.D * H, 65535L));
@@ -1312,6 +1317,7 @@ extern "C" qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const 
         xa = static_cast<const __nv_bfloat16 *>(u);
       }
       const __nv_bfloat16 *xb = in.x2;
+      o.ch0 = ch0;
 #define QESB_ZF(NN, XT_, TY_) launch_conv_zflat<NN, XT_, TY_>(xa, c1, xb, c2, g, B, Kp, o, err, s)
       if (xt == 128 && ty == 2) return N == 16 ? QESB_ZF(16, 128, 2) : N == 32 ? QESB_ZF(32, 128, 2) : QESB_ZF(64, 128, 2);
       if (xt == 128) return N == 16 ? QESB_ZF(16, 128, 1) : N == 32 ? QESB_ZF(32, 128, 1) : QESB_ZF(64, 128, 1);
@@ -1320,25 +1326,55 @@ extern "C" qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const 
 #undef QESB_ZF
     }
   }
-  // paths 3, 4, 5: the z-marching kernel for one 16-channel input only (4 rows per CTA on path 4, else 2)
-  if (fwd && g_conv_path >= 3 && W % 128 == 0 && (N == 16 || N == 32) && c1 == 16 && c2 == 0 &&
-      !up1) {
-    if (g_conv_path == 4)
-      return N == 16 ? launch_conv_zflat<16, 128, 4>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s)
-                     : launch_conv_zflat<32, 128, 4>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s);
-    return N == 16 ? launch_conv_zflat<16, 128, 2>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s)
-                   : launch_conv_zflat<32, 128, 2>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s);
+  float *full = nullptr;  // channel 0 alone from the other kernels: their full output first
+  if (ch0) {
+    void *p = nullptr;
+    qesb_status st = scratch_buffer(kScratchHead, dev, s, (size_t)g.V * N * sizeof(float), &p);
+    if (st != QESB_OK) return st;
+    full = static_cast<float *>(p);
+    o.yf = full;
   }
-  if ((g_conv_path == 0 || g_conv_path >= 2) && W % 128 == 0 && (N == 16 || N == 32)) {
-    if (N == 16) return launch_conv_direct<16>(in, g, sign, B, Kp, o, err, s);
-    return launch_conv_direct<32>(in, g, sign, B, Kp, o, err, s);
-  }
-  switch (N) {
-    case 16: return launch_conv<16>(in, g, sign, B, Kp, o, err, s);
-    case 32: return launch_conv<32>(in, g, sign, B, Kp, o, err, s);
-    case 64: return launch_conv<64>(in, g, sign, B, Kp, o, err, s);
-    default: return launch_conv<128>(in, g, sign, B, Kp, o, err, s);
-  }
+  auto others = [&]() -> qesb_status {
+    // paths 3, 4, 5: the z-marching kernel for one 16-channel input only (4 rows per CTA on path 4, else 2)
+    if (fwd && g_conv_path >= 3 && W % 128 == 0 && (N == 16 || N == 32) && c1 == 16 && c2 == 0 && !up1) {
+      if (g_conv_path == 4)
+        return N == 16 ? launch_conv_zflat<16, 128, 4>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s)
+                       : launch_conv_zflat<32, 128, 4>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s);
+      return N == 16 ? launch_conv_zflat<16, 128, 2>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s)
+                     : launch_conv_zflat<32, 128, 2>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s);
+    }
+    if ((g_conv_path == 0 || g_conv_path >= 2) && W % 128 == 0 && (N == 16 || N == 32)) {
+      if (N == 16) return launch_conv_direct<16>(in, g, sign, B, Kp, o, err, s);
+      return launch_conv_direct<32>(in, g, sign, B, Kp, o, err, s);
+    }
+    switch (N) {
+      case 16: return launch_conv<16>(in, g, sign, B, Kp, o, err, s);
+      case 32: return launch_conv<32>(in, g, sign, B, Kp, o, err, s);
+      case 64: return launch_conv<64>(in, g, sign, B, Kp, o, err, s);
+      default: return launch_conv<128>(in, g, sign, B, Kp, o, err, s);
+    }
+  };
+  const qesb_status st = others();
+  if (st != QESB_OK || !ch0) return st;
+  k_take_ch0<<<(unsigned)std::min<long>((g.V + 255) / 256, 148L * 16), 256, 0, s>>>(full, N, g.V, static_cast<float *>(yf));
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));
+}
+
+}  // namespace
+
+extern "C" qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const void *x2, int c2, int items, int D,
+                                         int H, int W, int sign, const void *Bm, int Kp, int N, void *y, void *yf,
+                                         const float *bias, int relu, const void *mask, int *err, void *stream)
+{
+  return conv_items(x1, c1, up1, x2, c2, items, D, H, W, sign, Bm, Kp, N, y, yf, bias, relu, mask, err, stream, 0);
+}
+
+qesb_status qesb_conv3d_head(const void *x1, int c1, int items, int D, int H, int W, const void *Bm, int Kp, int N,
+                             float *y0, const float *bias, int relu, int *err, void *stream)
+{
+  return conv_items(x1, c1, 0, nullptr, 0, items, D, H, W, 1, Bm, Kp, N, nullptr, y0, bias, relu, nullptr, err,
+                    stream, 1);
 }
 
 extern "C" qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *x2, int c2, int D, int H, int W,
@@ -1395,6 +1431,39 @@ __global__ void k_pool2(const __nv_bfloat16 *__restrict__ x, __nv_bfloat16 *__re
       s += __bfloat162float(x[src]);
     }
     y[i] = __float2bfloat16_rn(s * 0.125f);
+  }
+}
+
+// The same, one thread per output voxel and group of 8 channels (16-byte
+// loads and stores; the same sums in the same order). One block row per
+// output row (zz, yy).
+__global__ void k_pool2v(const __nv_bfloat16 *__restrict__ x, __nv_bfloat16 *__restrict__ y, int D, int H, int W,
+                         int C)
+{
+  const int h = H / 2, w = W / 2, cg = C / 8, n = w * cg;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int xx = i / cg, q8 = i - xx * cg;
+  for (long row = blockIdx.y; row < (long)(D / 2) * h; row += gridDim.y) {
+    const int zz = (int)(row / h), yy = (int)(row - (long)zz * h);
+    float acc[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const long src = (((long)(2 * zz + (q >> 2)) * H + 2 * yy + ((q >> 1) & 1)) * W + 2 * xx + (q & 1)) * C + 8 * q8;
+      const uint4 v = __ldg(reinterpret_cast<const uint4 *>(x + src));
+      const __nv_bfloat162 *b2 = reinterpret_cast<const __nv_bfloat162 *>(&v);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float2 f = __bfloat1622float2(b2[e]);
+        acc[2 * e] += f.x;
+        acc[2 * e + 1] += f.y;
+      }
+    }
+    uint4 pk;
+    __nv_bfloat162 *o2 = reinterpret_cast<__nv_bfloat162 *>(&pk);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) o2[e] = __floats2bfloat162_rn(acc[2 * e] * 0.125f, acc[2 * e + 1] * 0.125f);
+    *reinterpret_cast<uint4 *>(y + (row * w + xx) * C + 8 * q8) = pk;
   }
 }
 
@@ -1588,8 +1657,14 @@ extern "C" {
 qesb_status qesb_net_pool2(const void *x, void *y, int D, int H, int W, int C, void *stream)
 {
   if (!x || !y || D % 2 || H % 2 || W % 2 || C <= 0) return qesb_fail(QESB_ERR_ARG, "qesb_net_pool2: bad arguments");
-  const long n = (long)(D / 2) * (H / 2) * (W / 2) * C;
-  k_pool2<<<gs_blocks(n), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)x, (__nv_bfloat16 *)y, D, H, W, C);
+  if (C % 8 == 0 && reinterpret_cast<uintptr_t>(x) % 16 == 0 && reinterpret_cast<uintptr_t>(y) % 16 == 0) {
+    const int n = (W / 2) * (C / 8);
+    const dim3 grid((unsigned)((n + 127) / 128), (unsigned)std::min<long>((long)(D / 2) * (H / 2), 65535L));
+    k_pool2v<<<grid, 128, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)x, (__nv_bfloat16 *)y, D, H, W, C);
+  } else {
+    const long n = (long)(D / 2) * (H / 2) * (W / 2) * C;
+    k_pool2<<<gs_blocks(n), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)x, (__nv_bfloat16 *)y, D, H, W, C);
+  }
   NET_CK(cudaGetLastError());
   return QESB_OK;
 }

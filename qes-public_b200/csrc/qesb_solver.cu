@@ -195,6 +195,46 @@ __global__ void k_divergence(DevGrid G, const float *__restrict__ e, const float
   }
 }
 
+// The same from the packed wall mask: on the updated cells every coefficient
+// is exactly 0 or its layer's value (the packed path's precondition), so
+// reading the 1-byte mask instead of the six arrays gives the same R bit for
+// bit; the boundary cells, which have no mask, read the arrays.
+__global__ void k_divergence_packed(DevGrid G, const uint8_t *__restrict__ mask, const float *__restrict__ val,
+                                    const float *__restrict__ e, const float *__restrict__ f,
+                                    const float *__restrict__ g, const float *__restrict__ h,
+                                    const float *__restrict__ m, const float *__restrict__ n,
+                                    const float *__restrict__ u0, const float *__restrict__ v0,
+                                    const float *__restrict__ w0, const float *__restrict__ dz,
+                                    float dx, float dy, float *__restrict__ R)
+{
+  const int j = blockIdx.y, k = blockIdx.z + 1;  // k in [1, nz-3]
+  const bool row_in = j >= 1 && j <= G.Y - 2;
+  float lv[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) lv[q] = __ldg(val + q * G.Z + k);
+  const float dzk = dz[k], dzp = dz[k + 1], dzm = dz[k - 1];
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < G.X; i += gridDim.x * blockDim.x) {
+    const long c = G.cell(i, j, k), fc = G.face(i, j, k);
+    float ce, cf, cg, ch, cm, cn;
+    if (row_in && i >= 1 && i <= G.X - 2) {
+      const unsigned mb = mask[G.pad(i, j, k)];
+      ce = mb & 1u ? lv[0] : 0.0f;
+      cf = mb & 2u ? lv[1] : 0.0f;
+      cg = mb & 4u ? lv[2] : 0.0f;
+      ch = mb & 8u ? lv[3] : 0.0f;
+      cm = mb & 16u ? lv[4] : 0.0f;
+      cn = mb & 32u ? lv[5] : 0.0f;
+    } else {
+      ce = e[c], cf = f[c], cg = g[c], ch = h[c], cm = m[c], cn = n[c];
+    }
+    const float xt = (ce * u0[fc + 1] - cf * u0[fc]) * dx;
+    const float yt = (cg * v0[fc + G.FX] - ch * v0[fc]) * dy;
+    const double mt = (double)(cm * dzk) * 0.5 * (double)(dzk + dzp) * (double)w0[fc + G.FXY];
+    const float nt = cn * dzk * 0.5f * (dzk + dzm) * w0[fc];
+    R[G.pad(i, j, k)] = (float)(-2.0 * ((double)(xt + yt) + (mt - (double)nt)));
+  }
+}
+
 // Natural <-> padded lambda.
 __global__ void k_lambda_to_pad(DevGrid G, const float *__restrict__ src, float *__restrict__ dst)
 {
@@ -405,13 +445,10 @@ __global__ void k_correct(DevGrid G, const float *__restrict__ L, const float *_
 //   4: height of the cell centre / domain height     5..C-1: 0
 __global__ void k_absmax_R(DevGrid G, const float *__restrict__ R, unsigned *__restrict__ out)
 {
+  // one block per updated (row j, layer k), threads along x
+  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
   float mx = 0.0f;
-  const long per = (long)(G.X - 2) * (G.Y - 2) * (G.Z - 2);
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < per; t += (long)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(t % (G.X - 2)), j = 1 + (int)((t / (G.X - 2)) % (G.Y - 2)),
-              k = 1 + (int)(t / ((long)(G.X - 2) * (G.Y - 2)));
-    mx = fmaxf(mx, fabsf(R[G.pad(i, j, k)]));
-  }
+  for (int i = 1 + threadIdx.x; i <= G.X - 2; i += blockDim.x) mx = fmaxf(mx, fabsf(R[G.pad(i, j, k)]));
   mx = warp_max_f(mx);
   if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(mx));
 }
@@ -814,6 +851,21 @@ qesb_status ensure_err(qesb_handle *h, int itermax)
   CKS(dalloc(&h->d_err, (size_t)cap));
   h->err_cap = cap;
   return QESB_OK;
+}
+
+// R of the handle's inputs into d_R: from the packed wall mask when the
+// coefficients are stair-step, else from the six arrays (the same bits).
+void launch_divergence(qesb_handle *h, cudaStream_t s)
+{
+  const DevGrid &G = h->G;
+  if (h->packed)
+    k_divergence_packed<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(
+        G, h->d_mask, h->d_val, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_u0,
+        h->d_v0, h->d_w0, h->d_dz, h->dx, h->dy, h->d_R);
+  else
+    k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3],
+                                                                 h->d_in[4], h->d_in[5], h->d_u0, h->d_v0, h->d_w0,
+                                                                 h->d_dz, h->dx, h->dy, h->d_R);
 }
 
 // Inspect coefficients; build mask + tables when stair-step, else padded copies.
@@ -1495,9 +1547,7 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   const int nerr = err_slots(h, itermax);
   CKS(ensure_err(h, nerr));
   CK(cudaEventRecord(h->ev[0], s));
-  k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(
-      G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_u0, h->d_v0,
-      h->d_w0, h->d_dz, h->dx, h->dy, h->d_R);
+  launch_divergence(h, s);
   CK(cudaGetLastError());
   CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * nerr, s));
   CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
@@ -1925,9 +1975,7 @@ qesb_status qesb_compute_divergence(qesb_handle *h)
   if (!h->have_inputs) return qesb_fail(QESB_ERR_STATE, "qesb_compute_divergence before qesb_set_inputs");
   CK(cudaSetDevice(h->device));
   const DevGrid &G = h->G;
-  k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, h->stream>>>(
-      G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_u0, h->d_v0, h->d_w0,
-      h->d_dz, h->dx, h->dy, h->d_R);
+  launch_divergence(h, h->stream);
   CK(cudaGetLastError());
   return QESB_OK;
 }
@@ -1938,7 +1986,7 @@ qesb_status qesb_warm_input(qesb_handle *h, void *x, int C, unsigned *scale)
   CK(cudaSetDevice(h->device));
   const DevGrid &G = h->G;
   CK(cudaMemsetAsync(scale, 0, sizeof(unsigned), h->stream));
-  k_absmax_R<<<148 * 4, 256, 0, h->stream>>>(G, h->d_R, scale);
+  k_absmax_R<<<dim3(1, G.Y - 2, G.Z - 2), 128, 0, h->stream>>>(G, h->d_R, scale);
   double dzs = 0.0, height = 0.0;
   for (int k = 1; k < G.Z; ++k) dzs += h->dz[k];
   for (int k = 1; k < G.Z - 1; ++k) height += h->dz[k];
@@ -1956,7 +2004,7 @@ qesb_status qesb_warm_input_half(qesb_handle *h, void *x, int C, unsigned *scale
     return qesb_fail(QESB_ERR_ARG, "qesb_warm_input_half: the net grid (Nz x Ny x Nx) must have even sizes");
   CK(cudaSetDevice(h->device));
   CK(cudaMemsetAsync(scale, 0, sizeof(unsigned), h->stream));
-  k_absmax_R<<<148 * 4, 256, 0, h->stream>>>(G, h->d_R, scale);
+  k_absmax_R<<<dim3(1, G.Y - 2, G.Z - 2), 128, 0, h->stream>>>(G, h->d_R, scale);
   double dzs = 0.0, height = 0.0;
   for (int k = 1; k < G.Z; ++k) dzs += h->dz[k];
   for (int k = 1; k < G.Z - 1; ++k) height += h->dz[k];
@@ -2135,9 +2183,7 @@ qesb_status qesb_autotune_batch(qesb_handle *const *hs, int n, int *best, float 
   for (int i = 0; i < n; ++i) {
     qesb_handle *h = hs[i];
     const DevGrid &G = h->G;
-    k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(
-        G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_u0, h->d_v0, h->d_w0,
-        h->d_dz, h->dx, h->dy, h->d_R);
+    launch_divergence(h, s);
     k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam, h->d_lam_s);
     k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_R, h->d_R_s);
   }
@@ -2233,9 +2279,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     const bool pre_on = prephase_on(h) && itermax > 0;
     const int nerr = err_slots(h, itermax);
     CKS(ensure_err(h, nerr));
-    k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(
-        G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_u0, h->d_v0,
-        h->d_w0, h->d_dz, h->dx, h->dy, h->d_R);
+    launch_divergence(h, s);
     CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * nerr, s));
     h->last_pre_iterations = 0;
     if (pre_on) {

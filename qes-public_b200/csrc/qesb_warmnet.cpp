@@ -103,7 +103,7 @@ struct qesb_warmnet {
     void *p = nullptr;
     CKS_FWD(alloc(&p, V(0) * kInCh * 2));
     b.x = static_cast<uint16_t *>(p);
-    CKS_FWD(alloc(&p, V(0) * kHeadN * 4));
+    CKS_FWD(alloc(&p, V(0) * 4));  // the head's prediction channel
     b.y = static_cast<float *>(p);
     b.ea.resize(nlev);
     b.e.resize(nlev);
@@ -156,7 +156,9 @@ struct qesb_warmnet {
       CKS_FWD(conv(layers[index('d', l, true)], below, b.e[l], items, Dl, Hl, Wl, b.da[l], nullptr, s));
       CKS_FWD(conv(layers[index('d', l, false)], b.da[l], nullptr, items, Dl, Hl, Wl, b.d[l], nullptr, s));
     }
-    return conv(layers[index('h', 0, false)], b.d[0], nullptr, items, D, H, W, nullptr, b.y, s);
+    // the head: its prediction channel alone, FP32 [V]
+    const Layer &L = layers[index('h', 0, false)];
+    return qesb_conv3d_head(b.d[0], L.c1, items, D, H, W, L.Bm, L.Kp, L.cout, b.y, L.bias, L.relu, d_err, s);
   }
 
   qesb_status ensure_scales(int n)
@@ -318,10 +320,10 @@ qesb_status qesb_warm_start_batch(qesb_handle *const *hs, int n, qesb_warmnet *n
   }
   CKS_FWD(net->forward(*b, n, D, H, W, s));
   for (int i = 0; i < n; ++i) {
-    const float *y = b->y + V0 * kHeadN * i;
+    const float *y = b->y + V0 * i;
     CKS_FWD(join(s, st[i]));
-    CKS_FWD(net->res == 1 ? qesb_warm_apply(hs[i], y, kHeadN, net->d_scale + i)
-                          : qesb_warm_apply_up2(hs[i], y, kHeadN, net->d_scale + i));
+    CKS_FWD(net->res == 1 ? qesb_warm_apply(hs[i], y, 1, net->d_scale + i)
+                          : qesb_warm_apply_up2(hs[i], y, 1, net->d_scale + i));
   }
   int err = 0;
   if (cudaMemcpyAsync(&err, net->d_err, sizeof err, cudaMemcpyDeviceToHost, (cudaStream_t)s) != cudaSuccess ||

@@ -268,6 +268,35 @@ def test_cabi_warm_start_matches_the_python_network():
     np.testing.assert_array_equal(lc2, lc)
 
 
+def test_cabi_warm_start_same_on_every_convolution_path():
+    """The C layer loop on the default z-marching kernels (the head storing its
+    prediction channel alone) and on the implicit GEMM and older paths (the
+    head's full output, then channel 0): the same start to the rounding of
+    BF16 activations summed in other orders."""
+    from qesb import warmstart as ws
+
+    if not os.path.exists(ws.DEFAULT_WEIGHTS):
+        pytest.skip("no trained weights committed")
+    w, _ = qesb.random_city("city128", 900011)
+    cnet = ws.WarmNet(ws.DEFAULT_WEIGHTS, device=0)
+    starts = {}
+    try:
+        with qesb.Solver_B200(w.domain, RULE_TOL) as s:
+            s.set_inputs(w)
+            for path in (0, 1, 3):
+                qesb.check(qesb.lib().qesb_net_set_conv_path(path))
+                s.resetLambda()
+                cnet.warm_start(s)
+                starts[path] = s.lambda_
+    finally:
+        qesb.check(qesb.lib().qesb_net_set_conv_path(0))
+        cnet.close()
+    ref = np.abs(starts[1]).max()
+    assert ref > 0
+    for path in (0, 3):
+        assert np.abs(starts[path] - starts[1]).max() <= 2e-2 * ref, path
+
+
 def test_cabi_warm_start_batch_matches_single_starts():
     """qesb_warm_start_batch: three cities' inputs stacked along z, one
     forward pass, each start the single call's (to the summation order of

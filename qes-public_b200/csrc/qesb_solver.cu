@@ -89,51 +89,64 @@ __global__ void k_layer_max(DevGrid G, const float *__restrict__ e, const float 
                             const float *__restrict__ m, const float *__restrict__ n,
                             unsigned *__restrict__ vmax, int *__restrict__ bad)
 {
-  const int k = blockIdx.y + 1;
+  // one block per 8 updated rows j of layer k, threads along x; one atomic per block and coefficient
+  const int k = blockIdx.y + 1, j0 = 1 + blockIdx.x * 8;
   const float *cf[6] = {e, f, g, h, m, n};
   float mx[6] = {0, 0, 0, 0, 0, 0};
-  const long per = (long)(G.X - 2) * (G.Y - 2);
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < per; t += (long)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(t % (G.X - 2)), j = 1 + (int)(t / (G.X - 2));
-    const long c = G.cell(i, j, k);
+  bool b = false;
+  for (int j = j0; j < min(j0 + 8, G.Y - 1); ++j)
+    for (int i = 1 + threadIdx.x; i <= G.X - 2; i += blockDim.x) {
+      const long c = G.cell(i, j, k);
 #pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      float v = cf[q][c];
-      if (!(v >= 0.0f) || isinf(v)) atomicExch(bad, 1);  // negative, NaN or Inf: no packing
-      mx[q] = fmaxf(mx[q], v);
+      for (int q = 0; q < 6; ++q) {
+        const float v = cf[q][c];
+        b |= !(v >= 0.0f) || isinf(v);  // negative, NaN or Inf: no packing
+        mx[q] = fmaxf(mx[q], v);
+      }
     }
-  }
+  if (__syncthreads_or(b) && threadIdx.x == 0) atomicExch(bad, 1);
+  __shared__ float red[6][8];
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
-    float v = warp_max_f(mx[q]);
-    if ((threadIdx.x & 31) == 0) atomicMax(&vmax[q * G.Z + k], __float_as_uint(v));
+    const float v = warp_max_f(mx[q]);
+    if ((threadIdx.x & 31) == 0) red[q][w] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    float v = 0.0f;
+    for (int q = 0; q < nw; ++q) v = fmaxf(v, red[threadIdx.x][q]);
+    atomicMax(&vmax[threadIdx.x * G.Z + k], __float_as_uint(v));
   }
 }
 
 // Builds the 6-bit wall mask (bit q set when coefficient q is non-zero) and
-// flags any value that is neither 0 nor its layer's value.
+// flags any value that is neither 0 nor its layer's value. One block per
+// updated (row j, layer k), threads along x.
 __global__ void k_build_mask(DevGrid G, const float *__restrict__ e, const float *__restrict__ f,
                              const float *__restrict__ g, const float *__restrict__ h,
                              const float *__restrict__ m, const float *__restrict__ n,
                              const unsigned *__restrict__ vmax, uint8_t *__restrict__ mask,
                              int *__restrict__ bad)
 {
-  const int k = blockIdx.y + 1;
+  const int j = blockIdx.x + 1, k = blockIdx.y + 1;
   const float *cf[6] = {e, f, g, h, m, n};
-  const long per = (long)(G.X - 2) * (G.Y - 2);
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < per; t += (long)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(t % (G.X - 2)), j = 1 + (int)(t / (G.X - 2));
+  float ref[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) ref[q] = __uint_as_float(vmax[q * G.Z + k]);
+  bool b = false;
+  for (int i = 1 + threadIdx.x; i <= G.X - 2; i += blockDim.x) {
     const long c = G.cell(i, j, k);
     unsigned bits = 0;
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
       const float v = cf[q][c];
-      const float ref = __uint_as_float(vmax[q * G.Z + k]);
-      if (v == ref && v != 0.0f) bits |= 1u << q;
-      else if (v != 0.0f) atomicExch(bad, 1);
+      if (v == ref[q] && v != 0.0f) bits |= 1u << q;
+      else if (v != 0.0f) b = true;
     }
     mask[G.pad(i, j, k)] = (uint8_t)bits;
   }
+  if (__syncthreads_or(b) && threadIdx.x == 0) atomicExch(bad, 1);
 }
 
 // inv[k*64 + bits] = omega / (e + f + g + h + m + n) with absent terms 0,
@@ -445,12 +458,19 @@ __global__ void k_correct(DevGrid G, const float *__restrict__ L, const float *_
 //   4: height of the cell centre / domain height     5..C-1: 0
 __global__ void k_absmax_R(DevGrid G, const float *__restrict__ R, unsigned *__restrict__ out)
 {
-  // one block per updated (row j, layer k), threads along x
-  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  // one block per 8 updated rows j of layer k, threads along x; one atomic per block
+  const int k = blockIdx.y + 1, j0 = 1 + blockIdx.x * 8;
   float mx = 0.0f;
-  for (int i = 1 + threadIdx.x; i <= G.X - 2; i += blockDim.x) mx = fmaxf(mx, fabsf(R[G.pad(i, j, k)]));
+  for (int j = j0; j < min(j0 + 8, G.Y - 1); ++j)
+    for (int i = 1 + threadIdx.x; i <= G.X - 2; i += blockDim.x) mx = fmaxf(mx, fabsf(R[G.pad(i, j, k)]));
+  __shared__ float red[8];
   mx = warp_max_f(mx);
-  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(mx));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) mx = fmaxf(mx, red[q]);
+    atomicMax(out, __float_as_uint(mx));
+  }
 }
 
 __device__ __forceinline__ uint32_t bf16_bits_rne(float f)
@@ -708,6 +728,7 @@ struct qesb_handle {
 
   bool have_inputs = false;
   bool packed = false;
+  bool pc_ready = false;  // d_pc holds the current inputs' padded coefficients
   int opt_path = 1;
   int opt_k = 0;
   int opt_graph = 1;
@@ -868,6 +889,19 @@ void launch_divergence(qesb_handle *h, cudaStream_t s)
                                                                  h->d_dz, h->dx, h->dy, h->d_R);
 }
 
+// Padded copies of the six coefficients for the full-coefficient sweep.
+qesb_status ensure_padded_coefs(qesb_handle *h)
+{
+  if (h->pc_ready) return QESB_OK;
+  const DevGrid &G = h->G;
+  k_pad_coefs<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, h->stream>>>(
+      G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_pc[0], h->d_pc[1], h->d_pc[2],
+      h->d_pc[3], h->d_pc[4], h->d_pc[5]);
+  CK(cudaGetLastError());
+  h->pc_ready = true;
+  return QESB_OK;
+}
+
 // Inspect coefficients; build mask + tables when stair-step, else padded copies.
 qesb_status prepare_coefs(qesb_handle *h)
 {
@@ -877,12 +911,11 @@ qesb_status prepare_coefs(qesb_handle *h)
   if (h->opt_path != 0) {
     CK(cudaMemsetAsync(h->d_vmax, 0, sizeof(unsigned) * 6 * G.Z, s));
     CK(cudaMemsetAsync(h->d_bad, 0, sizeof(int), s));
-    dim3 grid(std::max(1, std::min(64, (int)(((long)(G.X - 2) * (G.Y - 2) + 255) / 256))), G.Z - 2);
-    k_layer_max<<<grid, 256, 0, s>>>(G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4],
-                                     h->d_in[5], h->d_vmax, h->d_bad);
+    k_layer_max<<<dim3((G.Y - 2 + 7) / 8, G.Z - 2), 256, 0, s>>>(G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3],
+                                                                h->d_in[4], h->d_in[5], h->d_vmax, h->d_bad);
     CK(cudaGetLastError());
-    k_build_mask<<<grid, 256, 0, s>>>(G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4],
-                                      h->d_in[5], h->d_vmax, h->d_mask, h->d_bad);
+    k_build_mask<<<dim3(G.Y - 2, G.Z - 2), 256, 0, s>>>(G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3],
+                                                         h->d_in[4], h->d_in[5], h->d_vmax, h->d_mask, h->d_bad);
     CK(cudaGetLastError());
     int bad = 1;
     CK(cudaMemcpyAsync(&bad, h->d_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -896,17 +929,17 @@ qesb_status prepare_coefs(qesb_handle *h)
       h->packed = true;
     }
   }
-  // The full-coefficient path is always prepared: it is the sweep for
-  // non-stair-step inputs and the fallback the packed path is tested against.
-  k_pad_coefs<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(
-      G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3], h->d_in[4], h->d_in[5], h->d_pc[0],
-      h->d_pc[1], h->d_pc[2], h->d_pc[3], h->d_pc[4], h->d_pc[5]);
-  CK(cudaGetLastError());
+  // The full-coefficient path (the sweep for non-stair-step inputs, and the
+  // one the packed path is tested against) gets its padded copies here when
+  // it is the only path, else at its first use.
+  h->pc_ready = false;
+  if (!h->packed) CKS(ensure_padded_coefs(h));
   return QESB_OK;
 }
 
 qesb_status run_iterations_full(qesb_handle *h, int itermax)
 {
+  CKS(ensure_padded_coefs(h));
   const DevGrid &G = h->G;
   cudaStream_t s = h->stream;
   const int nthr = 128;
@@ -1986,7 +2019,7 @@ qesb_status qesb_warm_input(qesb_handle *h, void *x, int C, unsigned *scale)
   CK(cudaSetDevice(h->device));
   const DevGrid &G = h->G;
   CK(cudaMemsetAsync(scale, 0, sizeof(unsigned), h->stream));
-  k_absmax_R<<<dim3(1, G.Y - 2, G.Z - 2), 128, 0, h->stream>>>(G, h->d_R, scale);
+  k_absmax_R<<<dim3((G.Y - 2 + 7) / 8, G.Z - 2), 256, 0, h->stream>>>(G, h->d_R, scale);
   double dzs = 0.0, height = 0.0;
   for (int k = 1; k < G.Z; ++k) dzs += h->dz[k];
   for (int k = 1; k < G.Z - 1; ++k) height += h->dz[k];
@@ -2004,7 +2037,7 @@ qesb_status qesb_warm_input_half(qesb_handle *h, void *x, int C, unsigned *scale
     return qesb_fail(QESB_ERR_ARG, "qesb_warm_input_half: the net grid (Nz x Ny x Nx) must have even sizes");
   CK(cudaSetDevice(h->device));
   CK(cudaMemsetAsync(scale, 0, sizeof(unsigned), h->stream));
-  k_absmax_R<<<dim3(1, G.Y - 2, G.Z - 2), 128, 0, h->stream>>>(G, h->d_R, scale);
+  k_absmax_R<<<dim3((G.Y - 2 + 7) / 8, G.Z - 2), 256, 0, h->stream>>>(G, h->d_R, scale);
   double dzs = 0.0, height = 0.0;
   for (int k = 1; k < G.Z; ++k) dzs += h->dz[k];
   for (int k = 1; k < G.Z - 1; ++k) height += h->dz[k];

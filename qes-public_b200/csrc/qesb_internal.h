@@ -25,3 +25,8 @@ qesb_status qesb_city_walls_dev(int Nx, int Ny, int Nz, float dx, const float *d
 // y0 FP32 [V] (the network's head; arguments as qesb_conv3d_items).
 qesb_status qesb_conv3d_head(const void *x1, int c1, int items, int D, int H, int W, const void *Bm, int Kp, int N,
                              float *y0, const float *bias, int relu, int *err, void *stream);
+
+// A small transfer run as a kernel on `stream` (no copy engine): dst and src
+// device memory or the device alias of mapped pinned host memory, bytes a
+// multiple of 4. The caller waits for the stream before reading dst.
+qesb_status qesb_copy_small(void *dst, const void *src, size_t bytes, void *stream);

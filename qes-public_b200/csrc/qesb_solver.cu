@@ -630,16 +630,83 @@ __global__ void k_warm_apply_up2(DevGrid G, int Dn, const float *__restrict__ yh
 // ---------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------
+// Small transfers on a solve's critical path (state polls, domain lists,
+// snapshots) run as kernels, between device memory and mapped pinned host
+// memory, not as copies: a copy waits in the copy engine's queue behind any
+// large transfer running for another stream (a batch's winds on their way to
+// the host, the next batch's inputs on their way in), and the solve's host
+// loop would wait with it. Words of [skip_lo, skip_hi) are left as they are.
+__global__ void k_words(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst, int n, int skip_lo, int skip_hi)
+{
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < n; i += gridDim.x * blockDim.x)
+    if (i < skip_lo || i >= skip_hi) dst[i] = src[i];
+  __threadfence_system();
+}
+
+__global__ void k_copy4(const float *__restrict__ src, float *__restrict__ dst, long n)
+{
+  const long n4 = n / 4;
+  const float4 *s4 = reinterpret_cast<const float4 *>(src);
+  float4 *d4 = reinterpret_cast<float4 *>(dst);
+  for (long i = threadIdx.x + blockIdx.x * (long)blockDim.x; i < n4; i += (long)gridDim.x * blockDim.x) d4[i] = s4[i];
+  for (long i = 4 * n4 + threadIdx.x + blockIdx.x * (long)blockDim.x; i < n; i += (long)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+// dst, src: device memory or the device alias of mapped pinned memory; bytes a multiple of 4
+qesb_status copy_words(void *dst, const void *src, size_t bytes, cudaStream_t s, size_t skip_lo = 0, size_t skip_hi = 0)
+{
+  const int n = (int)(bytes / 4);
+  k_words<<<std::max(1, std::min(148, (n + 255) / 256)), 256, 0, s>>>(
+      static_cast<const uint32_t *>(src), static_cast<uint32_t *>(dst), n, (int)(skip_lo / 4), (int)(skip_hi / 4));
+  CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+qesb_status qesb_copy_small(void *dst, const void *src, size_t bytes, void *stream)
+{
+  return copy_words(dst, src, bytes, static_cast<cudaStream_t>(stream));
+}
+
+// device -> device copy of n floats (16-byte aligned pointers)
+qesb_status copy_floats(float *dst, const float *src, long n, cudaStream_t s)
+{
+  k_copy4<<<148 * 4, 256, 0, s>>>(src, dst, n);
+  CK(cudaGetLastError());
+  return QESB_OK;
+}
+
+constexpr size_t kIoBytes = 256;  // a handle's scratch for small reads
+
+// Pinned host memory mapped into the device's address space, and its device alias.
+template <class T>
+qesb_status host_mapped(T **host, T **dev, size_t bytes)
+{
+  *host = nullptr;
+  *dev = nullptr;
+  if (cudaHostAlloc((void **)host, bytes, cudaHostAllocMapped) != cudaSuccess)
+    return qesb_fail(QESB_ERR_NOMEM, "cudaHostAlloc (mapped) of %zu bytes failed", bytes);
+  std::memset(*host, 0, bytes);
+  if (cudaHostGetDevicePointer((void **)dev, *host, 0) != cudaSuccess)
+    return qesb_fail(QESB_ERR_CUDA, "cudaHostGetDevicePointer failed");
+  return QESB_OK;
+}
+
 // Device-side domain list for the sweep kernels: descriptors, control
 // block, active list and unit offsets in one allocation of capacity n.
 struct SweepList {
   unsigned char *blk = nullptr;
+  unsigned char *stage = nullptr, *stage_dev = nullptr;  // mapped pinned image of blk, written by the host
+  size_t bytes = 0;
   int cap = 0;
   SweepArgs a{};
   qesb_status create(int n)
   {
-    const size_t bytes = sizeof(SweepDomain) * n + sizeof(SweepCtl) + sizeof(int) * (2 * n + 1);
+    static_assert(sizeof(SweepDomain) % 4 == 0 && sizeof(SweepCtl) % 8 == 0, "word copies of the list block");
+    bytes = sizeof(SweepDomain) * n + sizeof(SweepCtl) + sizeof(int) * (2 * n + 1);
+    bytes = (bytes + 3) / 4 * 4;
     CK(cudaMalloc((void **)&blk, bytes));
+    CKS(host_mapped(&stage, &stage_dev, bytes));
     cap = n;
     a.dom = reinterpret_cast<SweepDomain *>(blk);
     a.ctl = reinterpret_cast<SweepCtl *>(blk + sizeof(SweepDomain) * n);
@@ -659,18 +726,25 @@ struct SweepList {
       uoff[i + 1] = uoff[i] + sweep_units(doms[i], unit);
     }
     const SweepCtl ctl{0u, n, 0, 0, 0ull};
-    CK(cudaMemcpyAsync((void *)a.dom, doms.data(), sizeof(SweepDomain) * n, cudaMemcpyHostToDevice, s));
+    // the image in the staging buffer (the previous upload's copy has finished: it returned after it)
+    const size_t o_ctl = (size_t)((unsigned char *)a.ctl - blk), o_act = (size_t)((unsigned char *)a.active - blk),
+                 o_uoff = (size_t)((unsigned char *)a.uoff - blk);
+    std::memcpy(stage, doms.data(), sizeof(SweepDomain) * n);
+    std::memcpy(stage + o_ctl, &ctl, sizeof ctl);
+    std::memcpy(stage + o_act, active.data(), sizeof(int) * n);
+    std::memcpy(stage + o_uoff, uoff.data(), sizeof(int) * (n + 1));
     // everything but t0, the batch's start stamp (k_sweep_stamp), which outlives the pre-phase's list
-    CK(cudaMemcpyAsync(a.ctl, &ctl, offsetof(SweepCtl, t0), cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(a.active, active.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(a.uoff, uoff.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
+    const size_t used = o_uoff + sizeof(int) * (n + 1);
+    CKS(copy_words(blk, stage_dev, (used + 3) / 4 * 4, s, o_ctl + offsetof(SweepCtl, t0), o_ctl + sizeof(SweepCtl)));
     CK(cudaStreamSynchronize(s));
     return QESB_OK;
   }
   void destroy()
   {
     if (blk) cudaFree(blk);
+    if (stage) cudaFreeHost(stage);
     blk = nullptr;
+    stage = stage_dev = nullptr;
     cap = 0;
   }
 };
@@ -719,7 +793,7 @@ struct qesb_handle {
   double *d_err = nullptr;
   int err_cap = 0;
   SolveState *d_state = nullptr;
-  SolveState *h_state = nullptr;  // pinned
+  SolveState *h_state = nullptr, *h_state_dev = nullptr;  // mapped pinned, and its device alias
   double *d_div = nullptr;        // final divergence check (FP64)
   float *d_u = nullptr, *d_v = nullptr, *d_w = nullptr;  // output staging for host solves
   cudaEvent_t ev[4] = {};
@@ -779,7 +853,8 @@ struct qesb_handle {
   // batch to batch (no allocation, free or graph instantiation per batch once warm)
   SweepList blist;
   SweepGraph bgraph_start, bgraph_pre, bgraph;
-  SweepCtl *h_ctl = nullptr;  // pinned
+  SweepCtl *h_ctl = nullptr, *h_ctl_dev = nullptr;  // mapped pinned, and its device alias
+  unsigned char *h_io = nullptr, *h_io_dev = nullptr;  // mapped pinned scratch for small reads (kIoBytes)
   SweepGraph sgraph;  // iteration-loop graph of the sweep kernels
 
   // iteration-loop graphs of the tiled path, one per (variant, starting buffer)
@@ -948,7 +1023,7 @@ qesb_status run_iterations_full(qesb_handle *h, int itermax)
   const int chunk = 64;
   const long n4 = (long)pad_cells(G) / 4;
   if (h->win_k > 0)  // the first window starts from lambda as the loop begins
-    CK(cudaMemcpyAsync(h->d_snap, h->d_lam, sizeof(float) * pad_cells(G), cudaMemcpyDeviceToDevice, s));
+    CKS(copy_floats(h->d_snap, h->d_lam, (long)pad_cells(G), s));
   for (int base = 0; base < itermax; base += chunk) {
     const int n = std::min(chunk, itermax - base);
     for (int t = 0; t < n; ++t) {
@@ -965,7 +1040,7 @@ qesb_status run_iterations_full(qesb_handle *h, int itermax)
       }
     }
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CKS(copy_words(h->h_state_dev, h->d_state, sizeof(SolveState), s));
     CK(cudaStreamSynchronize(s));
     if (h->h_state->done) break;
   }
@@ -1062,7 +1137,7 @@ qesb_status run_iterations_tiled(qesb_handle *h, const Variant &v, int itermax)
       CKS(enqueue_chunk(h, v, 0, chunk, itermax));
     }
     launched += chunk;
-    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CKS(copy_words(h->h_state_dev, h->d_state, sizeof(SolveState), s));
     CK(cudaStreamSynchronize(s));
     if (h->h_state->done) break;
   }
@@ -1417,7 +1492,8 @@ void launch_window(int unit, bool multi, dim3 grid, cudaStream_t s, const SweepA
 // follows every wk-th black launch; chunks are then whole windows, so the
 // checks fall on iterations wk, 2 wk, ... of the loop for every domain.
 qesb_status run_sweep_loop(const SweepVariant &sv, bool multi, const SweepArgs &a, int device, cudaStream_t s,
-                           double cells, int itermax, bool graph, SweepGraph *cache, SweepCtl *h_ctl, int *launched,
+                           double cells, int itermax, bool graph, SweepGraph *cache, SweepCtl *h_ctl,
+                           SweepCtl *h_ctl_dev, int *launched,
                            int wk = 0, int nslots = 1)
 {
   CKS(sweep_prepare(sv));
@@ -1469,7 +1545,7 @@ qesb_status run_sweep_loop(const SweepVariant &sv, bool multi, const SweepArgs &
       CK(enqueue());
     }
     *launched += chunk;
-    CK(cudaMemcpyAsync(h_ctl, a.ctl, sizeof(SweepCtl), cudaMemcpyDeviceToHost, s));
+    CKS(copy_words(h_ctl_dev, a.ctl, sizeof(SweepCtl), s));
     CK(cudaStreamSynchronize(s));
     if (h_ctl->fault) return qesb_fail(QESB_ERR_CUDA, "sweep stage wait gave up");
     if (h_ctl->nactive == 0) break;
@@ -1501,9 +1577,9 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
     a.wait_limit = h->opt_wait_limit;
     int n1 = 0;
     CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, h->start_iters, h->opt_graph != 0,
-                       &h->sgraph_start, h->h_ctl, &n1));
+                       &h->sgraph_start, h->h_ctl, h->h_ctl_dev, &n1));
     pre_launched += n1;
-    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CKS(copy_words(h->h_state_dev, h->d_state, sizeof(SolveState), s));
     CK(cudaStreamSynchronize(s));
     if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the pre-phase's start stage");
     h->last_pre_iterations = h->h_state->it;
@@ -1523,9 +1599,9 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
     a.wait_limit = h->opt_wait_limit;
     int n2 = 0;
     CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, h->pre_iters, h->opt_graph != 0,
-                       &h->sgraph_pre, h->h_ctl, &n2));
+                       &h->sgraph_pre, h->h_ctl, h->h_ctl_dev, &n2));
     pre_launched += n2;
-    CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CKS(copy_words(h->h_state_dev, h->d_state, sizeof(SolveState), s));
     CK(cudaStreamSynchronize(s));
     if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the pre-phase");
     h->last_pre_iterations += h->h_state->it;
@@ -1541,10 +1617,10 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
   a.one = one[0];
   a.wait_limit = h->opt_wait_limit;
   if (h->win_k > 0)  // the first window starts from lambda as the reference loop begins
-    CK(cudaMemcpyAsync(h->d_snap, h->d_lam_s, sizeof(float) * 2 * h->S.CS, cudaMemcpyDeviceToDevice, s));
+    CKS(copy_floats(h->d_snap, h->d_lam_s, 2L * h->S.CS, s));
   CK(cudaEventRecord(h->evs[2], s));
   CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, itermax, h->opt_graph != 0, &h->sgraph,
-                     h->h_ctl, &launched, h->win_k, 1));
+                     h->h_ctl, h->h_ctl_dev, &launched, h->win_k, 1));
   CK(cudaEventRecord(h->evs[3], s));
   h->sweeps_timed = true;
   h->last_launches = 2 * (launched + pre_launched) + (h->win_k > 0 ? launched / h->win_k : 0);
@@ -1612,9 +1688,10 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   const bool check = u && v && w;
   if (check) CKS(enqueue_divergence_check(h, u, v, w, s));
   double div = -1.0;
-  if (check) CK(cudaMemcpyAsync(&div, h->d_div, sizeof(double), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(h->h_state, h->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+  if (check) CKS(copy_words(h->h_io_dev, h->d_div, sizeof(double), s));
+  CKS(copy_words(h->h_state_dev, h->d_state, sizeof(SolveState), s));
   CK(cudaStreamSynchronize(s));
+  if (check) std::memcpy(&div, h->h_io, sizeof div);
   if (st) {
     st->max_divergence = div;
     float a = 0, b = 0;
@@ -1684,6 +1761,7 @@ void free_all(qesb_handle *h)
   h->bgraph.reset();
   if (h->h_state) cudaFreeHost(h->h_state);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
+  if (h->h_io) cudaFreeHost(h->h_io);
   for (auto &e : h->ev)
     if (e) cudaEventDestroy(e);
   for (auto &e : h->evs)
@@ -1755,9 +1833,9 @@ qesb_status qesb_create(const qesb_grid *grid, float tol, int device, qesb_handl
   TRY(dalloc(&h->d_div, 1));
   TRY(h->list.create(1));
   TRY(ensure_err(h, 1024));
-  if (cudaMallocHost((void **)&h->h_state, sizeof(SolveState)) != cudaSuccess ||
-      cudaMallocHost((void **)&h->h_ctl, sizeof(SweepCtl)) != cudaSuccess)
-    return fail(qesb_fail(QESB_ERR_NOMEM, "cudaMallocHost failed"));
+  TRY(host_mapped(&h->h_state, &h->h_state_dev, sizeof(SolveState)));
+  TRY(host_mapped(&h->h_ctl, &h->h_ctl_dev, sizeof(SweepCtl)));
+  TRY(host_mapped(&h->h_io, &h->h_io_dev, kIoBytes));
   for (auto &e : h->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaEventCreate failed"));
   for (auto &e : h->evs)
@@ -2355,13 +2433,14 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     int n1 = 0;
     if (qs == QESB_OK)
       qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, smax, h0->opt_graph != 0, &h0->bgraph_start,
-                          h0->h_ctl, &n1);
+                          h0->h_ctl, h0->h_ctl_dev, &n1);
     pre_launched += n1;
+    for (size_t q = 0; q < start_of.size() && qs == QESB_OK; ++q)
+      qs = copy_words(hs[start_of[q]]->h_state_dev, hs[start_of[q]]->d_state, sizeof(SolveState), s);
+    if (qs == QESB_OK) CK(cudaStreamSynchronize(s));
     for (size_t q = 0; q < start_of.size() && qs == QESB_OK; ++q) {
       qesb_handle *h = hs[start_of[q]];
-      SolveState sp;
-      CK(cudaMemcpyAsync(&sp, h->d_state, sizeof sp, cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
+      const SolveState sp = *h->h_state;
       if (sp.nan)
         qs = qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d during the pre-phase's start stage",
                        start_of[q]);
@@ -2379,13 +2458,14 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     int n2 = 0;
     if (qs == QESB_OK)
       qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, pre_max, h0->opt_graph != 0, &h0->bgraph_pre,
-                          h0->h_ctl, &n2);
+                          h0->h_ctl, h0->h_ctl_dev, &n2);
     pre_launched += n2;
+    for (size_t q = 0; q < pre_of.size() && qs == QESB_OK; ++q)
+      qs = copy_words(hs[pre_of[q]]->h_state_dev, hs[pre_of[q]]->d_state, sizeof(SolveState), s);
+    if (qs == QESB_OK) CK(cudaStreamSynchronize(s));
     for (size_t q = 0; q < pre_of.size() && qs == QESB_OK; ++q) {
       qesb_handle *h = hs[pre_of[q]];
-      SolveState sp;
-      CK(cudaMemcpyAsync(&sp, h->d_state, sizeof sp, cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
+      const SolveState sp = *h->h_state;
       if (sp.nan) qs = qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d during the pre-phase", pre_of[q]);
       h->last_pre_iterations += sp.it;
       CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
@@ -2397,14 +2477,12 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   if (qs == QESB_OK) qs = list.upload(doms, sv.unit, s);
   if (qs == QESB_OK && h0->win_k > 0)  // each domain's first window starts from lambda as the loop begins
     for (int i = 0; i < n && qs == QESB_OK; ++i)
-      if (cudaMemcpyAsync(hs[i]->d_snap, hs[i]->d_lam_s, sizeof(float) * 2 * hs[i]->S.CS, cudaMemcpyDeviceToDevice,
-                          s) != cudaSuccess)
-        qs = qesb_fail(QESB_ERR_CUDA, "qesb_solve_batch: window snapshot copy failed");
+      qs = copy_floats(hs[i]->d_snap, hs[i]->d_lam_s, 2L * hs[i]->S.CS, s);
   if (qs == QESB_OK) {
     CK(cudaEventRecord(h0->evs[2], s));
     if (itermax > 0)
       qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, itermax, h0->opt_graph != 0, &h0->bgraph, h0->h_ctl,
-                          &launched, h0->win_k, n);
+                          h0->h_ctl_dev, &launched, h0->win_k, n);
     CK(cudaEventRecord(h0->evs[3], s));
   }
   const unsigned long long t0 = h0->h_ctl->t0;
@@ -2422,6 +2500,11 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     if (qs == QESB_OK && u && v && w && u[i] && v[i] && w[i]) qs = enqueue_divergence_check(h, u[i], v[i], w[i], s);
   }
   CK(cudaEventRecord(h0->ev[3], s));
+  // every domain's final state and divergence into its mapped buffers, then one wait
+  for (int i = 0; i < n && qs == QESB_OK; ++i) {
+    qs = copy_words(hs[i]->h_state_dev, hs[i]->d_state, sizeof(SolveState), s);
+    if (qs == QESB_OK) qs = copy_words(hs[i]->h_io_dev, hs[i]->d_div, sizeof(double), s);
+  }
   cudaError_t se = cudaStreamSynchronize(s);
   if (qs != QESB_OK) return qs;
   if (se != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "batch: %s", cudaGetErrorString(se));
@@ -2431,10 +2514,9 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   CK(cudaEventElapsedTime(&ms_ref, h0->evs[2], h0->evs[3]));
   int nan_at = -1;
   for (int i = 0; i < n; ++i) {
-    SolveState sti;
-    CK(cudaMemcpy(&sti, hs[i]->d_state, sizeof sti, cudaMemcpyDeviceToHost));
+    const SolveState sti = *hs[i]->h_state;
     double div = -1.0;
-    if (u && v && w && u[i] && v[i] && w[i]) CK(cudaMemcpy(&div, hs[i]->d_div, sizeof div, cudaMemcpyDeviceToHost));
+    if (u && v && w && u[i] && v[i] && w[i]) std::memcpy(&div, hs[i]->h_io, sizeof div);
     if (st) st[i].max_divergence = div;
     if (sti.nan && nan_at < 0) nan_at = i;
     if (st) {

@@ -67,6 +67,7 @@ struct qesb_warmnet {
   std::vector<int> ch;
   std::vector<Layer> layers;  // file order
   int *d_err = nullptr;
+  int *h_err = nullptr, *h_err_dev = nullptr;  // mapped pinned copy of *d_err, and its device alias
   unsigned *d_scale = nullptr;    // [nscale] max|R| per item of a call
   int nscale = 0;
   cudaEvent_t ev = nullptr;       // orders a batch's per-handle streams with the forward's stream
@@ -178,6 +179,8 @@ struct qesb_warmnet {
     ev = nullptr;
     for (void *p : owned) cudaFree(p);
     owned.clear();
+    if (h_err) cudaFreeHost(h_err);
+    h_err = h_err_dev = nullptr;
     bufs.clear();
   }
 };
@@ -259,6 +262,9 @@ qesb_status qesb_warmnet_load(const char *path, int device, qesb_warmnet **out)
   }
   if ((s = net->alloc(&p, sizeof(int))) != QESB_OK) return fail(s);
   net->d_err = static_cast<int *>(p);
+  if (cudaHostAlloc((void **)&net->h_err, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer((void **)&net->h_err_dev, net->h_err, 0) != cudaSuccess)
+    return fail(qesb_fail(QESB_ERR_CUDA, "qesb_warmnet_load: mapped host memory"));
   if ((s = net->ensure_scales(1)) != QESB_OK) return fail(s);
   if (cudaEventCreateWithFlags(&net->ev, cudaEventDisableTiming) != cudaSuccess)
     return fail(qesb_fail(QESB_ERR_CUDA, "qesb_warmnet_load: cudaEventCreate"));
@@ -325,10 +331,11 @@ qesb_status qesb_warm_start_batch(qesb_handle *const *hs, int n, qesb_warmnet *n
     CKS_FWD(net->res == 1 ? qesb_warm_apply(hs[i], y, 1, net->d_scale + i)
                           : qesb_warm_apply_up2(hs[i], y, 1, net->d_scale + i));
   }
-  int err = 0;
-  if (cudaMemcpyAsync(&err, net->d_err, sizeof err, cudaMemcpyDeviceToHost, (cudaStream_t)s) != cudaSuccess ||
-      cudaStreamSynchronize((cudaStream_t)s) != cudaSuccess)
+  // the error flag through mapped memory (a copy would queue behind other streams' transfers)
+  CKS_FWD(qesb_copy_small(net->h_err_dev, net->d_err, sizeof(int), s));
+  if (cudaStreamSynchronize((cudaStream_t)s) != cudaSuccess)
     return qesb_fail(QESB_ERR_CUDA, "qesb_warm_start: %s", cudaGetErrorString(cudaGetLastError()));
+  const int err = *net->h_err;
   for (int i = 0; i < n; ++i)
     if (st[i] != s && cudaStreamSynchronize((cudaStream_t)st[i]) != cudaSuccess)
       return qesb_fail(QESB_ERR_CUDA, "qesb_warm_start: %s", cudaGetErrorString(cudaGetLastError()));

@@ -286,6 +286,9 @@ qesb_status qesb_autotune_batch(qesb_handle *const *handles, int n, int *best, f
  *   "sweeps_per_launch"  iterations fused per sweep launch (0 = autotuned)
  *   "path"               0 = force full coefficients, 1 = allow the packed mask (default)
  *   "graph"              1 = run the iteration loop as a CUDA graph (default), 0 = plain launches
+ *   "pdl"                1 = z-march list sweeps and window checks as programmatic dependent launches,
+ *                        each grid's CTAs scheduled while the previous grid finishes; 0 = off (default:
+ *                        inside the CUDA-graph chunks it measured 0.6 % slower on the headline batch)
  *   "variant"            sweep variant index (-1 = autotuned / default), see qesb_num_variants
  *   "batch_variant"      sweep shape for qesb_solve_batch led by this handle (-1 = from "variant");
  *                        set by qesb_autotune_batch

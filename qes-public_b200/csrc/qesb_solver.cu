@@ -668,6 +668,24 @@ qesb_status qesb_copy_small(void *dst, const void *src, size_t bytes, void *stre
   return copy_words(dst, src, bytes, static_cast<cudaStream_t>(stream));
 }
 
+__global__ void k_zero(uint32_t *__restrict__ p, long n, bool vec)
+{
+  const long n4 = vec ? n / 4 : 0;
+  uint4 *p4 = reinterpret_cast<uint4 *>(p);
+  for (long i = threadIdx.x + blockIdx.x * (long)blockDim.x; i < n4; i += (long)gridDim.x * blockDim.x)
+    p4[i] = make_uint4(0, 0, 0, 0);
+  for (long i = 4 * n4 + threadIdx.x + blockIdx.x * (long)blockDim.x; i < n; i += (long)gridDim.x * blockDim.x) p[i] = 0;
+}
+
+// Zeroes `bytes` (a multiple of 4) of device memory with a kernel, like the copies above.
+cudaError_t zero_async(void *p, size_t bytes, cudaStream_t s)
+{
+  const long n = (long)(bytes / 4);
+  k_zero<<<(unsigned)std::max<long>(1, std::min<long>((n / 4 + 255) / 256, 148L * 4)), 256, 0, s>>>(
+      static_cast<uint32_t *>(p), n, reinterpret_cast<uintptr_t>(p) % 16 == 0);
+  return cudaGetLastError();
+}
+
 // device -> device copy of n floats (16-byte aligned pointers)
 qesb_status copy_floats(float *dst, const float *src, long n, cudaStream_t s)
 {
@@ -755,6 +773,7 @@ struct SweepGraph {
   int variant = -1, chunk = 0;
   int wk = 0, nslots = 0;  // window checks captured: every wk launches, over nslots list slots
   bool multi = false;
+  bool pdl = false;  // captured with programmatic dependent launches
   SweepArgs args{};
   cudaStream_t stream = nullptr;
   void reset()
@@ -806,6 +825,7 @@ struct qesb_handle {
   int opt_path = 1;
   int opt_k = 0;
   int opt_graph = 1;
+  int opt_pdl = 0;  // programmatic dependent launches between z-march list kernels (measured: no gain)
   int opt_variant = -1;
   int opt_batch_variant = -1;  // sweep shape for batches led by this handle (qesb_autotune_batch)
   int opt_autotune = 0;
@@ -984,8 +1004,8 @@ qesb_status prepare_coefs(qesb_handle *h)
   cudaStream_t s = h->stream;
   h->packed = false;
   if (h->opt_path != 0) {
-    CK(cudaMemsetAsync(h->d_vmax, 0, sizeof(unsigned) * 6 * G.Z, s));
-    CK(cudaMemsetAsync(h->d_bad, 0, sizeof(int), s));
+    CK(zero_async(h->d_vmax, sizeof(unsigned) * 6 * G.Z, s));
+    CK(zero_async(h->d_bad, sizeof(int), s));
     k_layer_max<<<dim3((G.Y - 2 + 7) / 8, G.Z - 2), 256, 0, s>>>(G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3],
                                                                 h->d_in[4], h->d_in[5], h->d_vmax, h->d_bad);
     CK(cudaGetLastError());
@@ -1471,18 +1491,34 @@ int err_slots(const qesb_handle *h, int itermax)
 }
 
 // Window check launch for a list of kernels of work-unit kind `unit`.
-void launch_window(int unit, bool multi, dim3 grid, cudaStream_t s, const SweepArgs &a)
+// A list kernel launch, as a programmatic dependent launch when pdl is set
+// (the kernel starts with pdl_wait_release()).
+cudaError_t launch_list(void (*k)(SweepArgs), dim3 grid, dim3 block, size_t smem, cudaStream_t s, const SweepArgs &a,
+                        bool pdl)
 {
-  if (unit == kUnitTile) {
-    if (multi) k_window_check<kUnitTile, true><<<grid, 256, 0, s>>>(a);
-    else k_window_check<kUnitTile, false><<<grid, 256, 0, s>>>(a);
-  } else if (unit == kUnitSpan) {
-    if (multi) k_window_check<kUnitSpan, true><<<grid, 256, 0, s>>>(a);
-    else k_window_check<kUnitSpan, false><<<grid, 256, 0, s>>>(a);
-  } else {
-    if (multi) k_window_check<kUnitRow, true><<<grid, 256, 0, s>>>(a);
-    else k_window_check<kUnitRow, false><<<grid, 256, 0, s>>>(a);
+  if (!pdl) {
+    k<<<grid, block, smem, s>>>(a);
+    return cudaGetLastError();
   }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, a);
+}
+
+void launch_window(int unit, bool multi, dim3 grid, cudaStream_t s, const SweepArgs &a, bool pdl = false)
+{
+  void (*k)(SweepArgs) = unit == kUnitTile   ? (multi ? k_window_check<kUnitTile, true> : k_window_check<kUnitTile, false>)
+                         : unit == kUnitSpan ? (multi ? k_window_check<kUnitSpan, true> : k_window_check<kUnitSpan, false>)
+                                             : (multi ? k_window_check<kUnitRow, true> : k_window_check<kUnitRow, false>);
+  launch_list(k, grid, dim3(256), 0, s, a, pdl);
 }
 
 // The iteration loop over a domain list: CUDA-graph chunks of (red, black)
@@ -1494,7 +1530,7 @@ void launch_window(int unit, bool multi, dim3 grid, cudaStream_t s, const SweepA
 qesb_status run_sweep_loop(const SweepVariant &sv, bool multi, const SweepArgs &a, int device, cudaStream_t s,
                            double cells, int itermax, bool graph, SweepGraph *cache, SweepCtl *h_ctl,
                            SweepCtl *h_ctl_dev, int *launched,
-                           int wk = 0, int nslots = 1)
+                           int wk = 0, int nslots = 1, bool pdl = false)
 {
   CKS(sweep_prepare(sv));
   const dim3 grid(sweep_ctas(sv, multi, device)), block(32, sv.block_y);
@@ -1506,20 +1542,24 @@ qesb_status run_sweep_loop(const SweepVariant &sv, bool multi, const SweepArgs &
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   const dim3 wgrid(std::max(1, 4 * sms / std::max(1, nslots)), std::max(1, nslots));
   auto red = multi ? sv.red_m : sv.red, black = multi ? sv.black_m : sv.black;
+  // programmatic dependent launches between the z-march list kernels (the
+  // first of a chunk waits for the chunk before it in the usual way)
+  const bool chain = pdl && sv.tile_rows > 0;
   auto enqueue = [&]() {
-    for (int c = 0; c < chunk; ++c) {
-      red<<<grid, block, sv.smem, s>>>(a);
-      black<<<grid, block, sv.smem, s>>>(a);
-      if (wk > 0 && (c + 1) % wk == 0) launch_window(sv.unit, multi, wgrid, s, a);
+    cudaError_t e = cudaSuccess;
+    for (int c = 0; c < chunk && e == cudaSuccess; ++c) {
+      e = launch_list(red, grid, block, sv.smem, s, a, chain && c > 0);
+      if (e == cudaSuccess) e = launch_list(black, grid, block, sv.smem, s, a, chain);
+      if (e == cudaSuccess && wk > 0 && (c + 1) % wk == 0) launch_window(sv.unit, multi, wgrid, s, a, chain);
     }
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
   };
   const int vid = (int)(&sv - kSweepVariants);
   *launched = 0;
   while (*launched < itermax) {
     if (graph) {
       const bool hit = cache->exec && cache->variant == vid && cache->chunk == chunk && cache->multi == multi &&
-                       cache->wk == wk && cache->nslots == nslots && cache->stream == s &&
+                       cache->wk == wk && cache->nslots == nslots && cache->stream == s && cache->pdl == chain &&
                        std::memcmp(&cache->args, &a, sizeof a) == 0;
       if (!hit) {
         cache->reset();
@@ -1537,6 +1577,7 @@ qesb_status run_sweep_loop(const SweepVariant &sv, bool multi, const SweepArgs &
         cache->wk = wk;
         cache->nslots = nslots;
         cache->multi = multi;
+        cache->pdl = chain;
         cache->stream = s;
         std::memcpy(&cache->args, &a, sizeof a);
       }
@@ -1577,14 +1618,14 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
     a.wait_limit = h->opt_wait_limit;
     int n1 = 0;
     CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, h->start_iters, h->opt_graph != 0,
-                       &h->sgraph_start, h->h_ctl, h->h_ctl_dev, &n1));
+                       &h->sgraph_start, h->h_ctl, h->h_ctl_dev, &n1, 0, 1, h->opt_pdl != 0));
     pre_launched += n1;
     CKS(copy_words(h->h_state_dev, h->d_state, sizeof(SolveState), s));
     CK(cudaStreamSynchronize(s));
     if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the pre-phase's start stage");
     h->last_pre_iterations = h->h_state->it;
-    CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * err_slots(h, itermax), s));
-    CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+    CK(zero_async(h->d_err, sizeof(double) * err_slots(h, itermax), s));
+    CK(zero_async(h->d_state, sizeof(SolveState), s));
   }
   if (prephase_on(h)) {
     // over-relaxed pre-phase from the current lambda; its state and error
@@ -1599,14 +1640,14 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
     a.wait_limit = h->opt_wait_limit;
     int n2 = 0;
     CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, h->pre_iters, h->opt_graph != 0,
-                       &h->sgraph_pre, h->h_ctl, h->h_ctl_dev, &n2));
+                       &h->sgraph_pre, h->h_ctl, h->h_ctl_dev, &n2, 0, 1, h->opt_pdl != 0));
     pre_launched += n2;
     CKS(copy_words(h->h_state_dev, h->d_state, sizeof(SolveState), s));
     CK(cudaStreamSynchronize(s));
     if (h->h_state->nan) return qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda during the pre-phase");
     h->last_pre_iterations += h->h_state->it;
-    CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
-    CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+    CK(zero_async(h->d_err, sizeof(double) * std::max(itermax, 1), s));
+    CK(zero_async(h->d_state, sizeof(SolveState), s));
   }
   CK(cudaEventRecord(h->evs[1], s));
   std::vector<SweepDomain> one{sweep_domain(h, itermax, (double)h->tol)};
@@ -1620,7 +1661,7 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
     CKS(copy_floats(h->d_snap, h->d_lam_s, 2L * h->S.CS, s));
   CK(cudaEventRecord(h->evs[2], s));
   CKS(run_sweep_loop(sv, false, a, h->device, s, (double)G.XY * G.Z, itermax, h->opt_graph != 0, &h->sgraph,
-                     h->h_ctl, h->h_ctl_dev, &launched, h->win_k, 1));
+                     h->h_ctl, h->h_ctl_dev, &launched, h->win_k, 1, h->opt_pdl != 0));
   CK(cudaEventRecord(h->evs[3], s));
   h->sweeps_timed = true;
   h->last_launches = 2 * (launched + pre_launched) + (h->win_k > 0 ? launched / h->win_k : 0);
@@ -1635,7 +1676,7 @@ qesb_status run_iterations_sweep(qesb_handle *h, const SweepVariant &sv, int ite
 qesb_status enqueue_divergence_check(qesb_handle *h, const float *u, const float *v, const float *w, cudaStream_t s)
 {
   const DevGrid &G = h->G;
-  CK(cudaMemsetAsync(h->d_div, 0, sizeof(double), s));
+  CK(zero_async(h->d_div, sizeof(double), s));
   const int kmax = G.FZ - 4;
   if (kmax >= 1) {
     k_max_divergence<<<dim3((G.X + 255) / 256, G.Y - 2, kmax), 256, 0, s>>>(G, h->d_flag, u, v, w, h->d_dz, h->dx,
@@ -1658,8 +1699,8 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   CK(cudaEventRecord(h->ev[0], s));
   launch_divergence(h, s);
   CK(cudaGetLastError());
-  CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * nerr, s));
-  CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+  CK(zero_async(h->d_err, sizeof(double) * nerr, s));
+  CK(zero_async(h->d_state, sizeof(SolveState), s));
   CK(cudaEventRecord(h->ev[1], s));
   const bool packed = h->packed && h->opt_path == 1;
   if (packed && h->opt_autotune && h->opt_variant < 0 && tuned_variant(G) < 0) {
@@ -1873,9 +1914,9 @@ qesb_status qesb_reset_lambda(qesb_handle *h)
   if (!h) return qesb_fail(QESB_ERR_ARG, "null handle");
   CK(cudaSetDevice(h->device));
   const size_t np = pad_alloc(h->G);
-  CK(cudaMemsetAsync(h->d_lam, 0, np * sizeof(float), h->stream));
-  CK(cudaMemsetAsync(h->d_lam2, 0, np * sizeof(float), h->stream));
-  CK(cudaMemsetAsync(h->d_R, 0, np * sizeof(float), h->stream));
+  CK(zero_async(h->d_lam, np * sizeof(float), h->stream));
+  CK(zero_async(h->d_lam2, np * sizeof(float), h->stream));
+  CK(zero_async(h->d_R, np * sizeof(float), h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return QESB_OK;
 }
@@ -1980,7 +2021,7 @@ qesb_status qesb_wall_log_law(qesb_handle *h, float z0, float dz, float *u, floa
     CK(cudaMalloc((void **)&h->d_wbits, (size_t)G.XY * G.Z));
     CK(cudaMalloc((void **)&h->d_wcut, sizeof(int)));
   }
-  CK(cudaMemsetAsync(h->d_wcut, 0, sizeof(int), s));
+  CK(zero_async(h->d_wcut, sizeof(int), s));
   const dim3 grid((G.X + 127) / 128, G.Y, G.Z - 2), block(128);
   k_wall_bits<<<grid, block, 0, s>>>(G, h->d_flag, h->d_wbits, h->d_wcut);
   // the reference's distances: getDomainSize() is (dx, dx, dz) (Domain.h:104),
@@ -2096,7 +2137,7 @@ qesb_status qesb_warm_input(qesb_handle *h, void *x, int C, unsigned *scale)
   if (!h || !x || !scale || C < 8 || C % 8) return qesb_fail(QESB_ERR_ARG, "qesb_warm_input: bad arguments");
   CK(cudaSetDevice(h->device));
   const DevGrid &G = h->G;
-  CK(cudaMemsetAsync(scale, 0, sizeof(unsigned), h->stream));
+  CK(zero_async(scale, sizeof(unsigned), h->stream));
   k_absmax_R<<<dim3((G.Y - 2 + 7) / 8, G.Z - 2), 256, 0, h->stream>>>(G, h->d_R, scale);
   double dzs = 0.0, height = 0.0;
   for (int k = 1; k < G.Z; ++k) dzs += h->dz[k];
@@ -2114,7 +2155,7 @@ qesb_status qesb_warm_input_half(qesb_handle *h, void *x, int C, unsigned *scale
   if (G.X % 2 || G.Y % 2 || (G.Z - 1) % 2)
     return qesb_fail(QESB_ERR_ARG, "qesb_warm_input_half: the net grid (Nz x Ny x Nx) must have even sizes");
   CK(cudaSetDevice(h->device));
-  CK(cudaMemsetAsync(scale, 0, sizeof(unsigned), h->stream));
+  CK(zero_async(scale, sizeof(unsigned), h->stream));
   k_absmax_R<<<dim3((G.Y - 2 + 7) / 8, G.Z - 2), 256, 0, h->stream>>>(G, h->d_R, scale);
   double dzs = 0.0, height = 0.0;
   for (int k = 1; k < G.Z; ++k) dzs += h->dz[k];
@@ -2176,7 +2217,7 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
     CKS(sweep_prepare(sv));
     CKS(ensure_err(h, n + 1));
     cudaStream_t s = h->stream;
-    CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+    CK(zero_async(h->d_state, sizeof(SolveState), s));
     std::vector<SweepDomain> one{sweep_domain(h, 1 << 30, -1.0)};  // tol < 0: every launch runs
     CKS(attach_tmaps(h, sv, one[0], s));
     sweep_tiles(one, sv, false, h->device);
@@ -2203,7 +2244,7 @@ qesb_status qesb_time_sweeps(qesb_handle *h, int n, float *ms, int *k)
   CKS(set_smem_attr(v));
   CKS(ensure_err(h, v.K));
   cudaStream_t s = h->stream;
-  CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+  CK(zero_async(h->d_state, sizeof(SolveState), s));
   float *buf[2] = {h->d_lam, h->d_lam2};
   const dim3 grid = tiled_grid(h->G, v);
   CK(cudaEventRecord(h->ev[0], s));
@@ -2316,8 +2357,8 @@ qesb_status qesb_autotune_batch(qesb_handle *const *hs, int n, int *best, float 
       for (int i = 0; i < n && qs == QESB_OK; ++i) {
         qs = ensure_err(hs[i], reps + 1);
         if (qs != QESB_OK) break;
-        if (cudaMemsetAsync(hs[i]->d_err, 0, sizeof(double) * (reps + 1), s) != cudaSuccess ||
-            cudaMemsetAsync(hs[i]->d_state, 0, sizeof(SolveState), s) != cudaSuccess)
+        if (zero_async(hs[i]->d_err, sizeof(double) * (reps + 1), s) != cudaSuccess ||
+            zero_async(hs[i]->d_state, sizeof(SolveState), s) != cudaSuccess)
           qs = qesb_fail(QESB_ERR_CUDA, "qesb_autotune_batch: memset");
         doms[i] = sweep_domain(hs[i], 1 << 30, -1.0);  // tol < 0: every launch runs
         if (qs == QESB_OK) qs = attach_tmaps(hs[i], sv, doms[i], s);
@@ -2391,7 +2432,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     const int nerr = err_slots(h, itermax);
     CKS(ensure_err(h, nerr));
     launch_divergence(h, s);
-    CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * nerr, s));
+    CK(zero_async(h->d_err, sizeof(double) * nerr, s));
     h->last_pre_iterations = 0;
     if (pre_on) {
       SweepDomain p;
@@ -2406,7 +2447,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
         start_of.push_back(i);
       }
     }
-    CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+    CK(zero_async(h->d_state, sizeof(SolveState), s));
     k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam, h->d_lam_s);
     k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_R, h->d_R_s);
     CK(cudaGetLastError());
@@ -2433,7 +2474,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     int n1 = 0;
     if (qs == QESB_OK)
       qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, smax, h0->opt_graph != 0, &h0->bgraph_start,
-                          h0->h_ctl, h0->h_ctl_dev, &n1);
+                          h0->h_ctl, h0->h_ctl_dev, &n1, 0, 1, h0->opt_pdl != 0);
     pre_launched += n1;
     for (size_t q = 0; q < start_of.size() && qs == QESB_OK; ++q)
       qs = copy_words(hs[start_of[q]]->h_state_dev, hs[start_of[q]]->d_state, sizeof(SolveState), s);
@@ -2445,8 +2486,8 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
         qs = qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d during the pre-phase's start stage",
                        start_of[q]);
       h->last_pre_iterations = sp.it;
-      CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * err_slots(h, itermax), s));
-      CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+      CK(zero_async(h->d_err, sizeof(double) * err_slots(h, itermax), s));
+      CK(zero_async(h->d_state, sizeof(SolveState), s));
     }
   }
   if (!pre.empty() && qs == QESB_OK) {
@@ -2458,7 +2499,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     int n2 = 0;
     if (qs == QESB_OK)
       qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, pre_max, h0->opt_graph != 0, &h0->bgraph_pre,
-                          h0->h_ctl, h0->h_ctl_dev, &n2);
+                          h0->h_ctl, h0->h_ctl_dev, &n2, 0, 1, h0->opt_pdl != 0);
     pre_launched += n2;
     for (size_t q = 0; q < pre_of.size() && qs == QESB_OK; ++q)
       qs = copy_words(hs[pre_of[q]]->h_state_dev, hs[pre_of[q]]->d_state, sizeof(SolveState), s);
@@ -2468,8 +2509,8 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
       const SolveState sp = *h->h_state;
       if (sp.nan) qs = qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d during the pre-phase", pre_of[q]);
       h->last_pre_iterations += sp.it;
-      CK(cudaMemsetAsync(h->d_err, 0, sizeof(double) * std::max(itermax, 1), s));
-      CK(cudaMemsetAsync(h->d_state, 0, sizeof(SolveState), s));
+      CK(zero_async(h->d_err, sizeof(double) * std::max(itermax, 1), s));
+      CK(zero_async(h->d_state, sizeof(SolveState), s));
     }
   }
   CK(cudaEventRecord(h0->evs[1], s));
@@ -2482,7 +2523,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     CK(cudaEventRecord(h0->evs[2], s));
     if (itermax > 0)
       qs = run_sweep_loop(sv, true, list.a, h0->device, s, cells, itermax, h0->opt_graph != 0, &h0->bgraph, h0->h_ctl,
-                          h0->h_ctl_dev, &launched, h0->win_k, n);
+                          h0->h_ctl_dev, &launched, h0->win_k, n, h0->opt_pdl != 0);
     CK(cudaEventRecord(h0->evs[3], s));
   }
   const unsigned long long t0 = h0->h_ctl->t0;
@@ -2604,10 +2645,10 @@ qesb_status qesb_fp64_same_sor(qesb_handle *h, const float *lambda0, float pre_o
     ok(cudaMemcpyAsync(tmp, lambda0, nc * sizeof(float), cudaMemcpyHostToDevice, s));
     k_widen64<<<(unsigned)((nc + 255) / 256), 256, 0, s>>>(tmp, L, (long)nc);
   } else {
-    ok(cudaMemsetAsync(L, 0, nc * sizeof(double), s));
+    ok(zero_async(L, nc * sizeof(double), s));
   }
-  ok(cudaMemsetAsync(R, 0, nc * sizeof(double), s));
-  ok(cudaMemsetAsync(acc, 0, 4 * sizeof(double), s));
+  ok(zero_async(R, nc * sizeof(double), s));
+  ok(zero_async(acc, 4 * sizeof(double), s));
   ok(cudaEventRecord(h->ev[0], s));
   k_div64<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3],
                                                           h->d_in[4], h->d_in[5], h->d_u0, h->d_v0, h->d_w0,
@@ -2685,6 +2726,8 @@ qesb_status qesb_set_option(qesb_handle *h, const char *key, int value)
     h->opt_path = value;
   } else if (k == "graph") {
     h->opt_graph = value ? 1 : 0;
+  } else if (k == "pdl") {
+    h->opt_pdl = value ? 1 : 0;
   } else if (k == "autotune") {
     h->opt_autotune = value ? 1 : 0;
   } else if (k == "variant") {

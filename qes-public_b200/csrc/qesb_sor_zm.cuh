@@ -252,6 +252,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_sor_zm(SweepArgs b)
   constexpr int TR = TY * RW, NT = 32 * TY, NSO = zm_other_slots(DIST), NSW = zm_own_slots(DIST);
   constexpr int OSTR = zm_oslot_floats<TR, TMA>();
   static_assert(DIST == 1 || DIST == 2, "copies run one or two planes ahead");
+  pdl_wait_release();
   const int na = b.ctl->nactive;
   if (na <= 0) return;
   extern __shared__ __align__(128) unsigned char zm_raw[];

@@ -48,6 +48,17 @@ struct SweepDomain {
   const TmaDesc *tm;  // [kTmCount] device tensor maps (TMA z-march shapes), or null
 };
 
+// Programmatic dependent launch: a list kernel launched while the previous
+// one still runs waits here until that grid has completed and its memory is
+// visible (a no-op for a plain launch), then lets the next kernel's CTAs be
+// scheduled as its own CTAs finish. Every list kernel reads the control block
+// and lambda the previous one wrote, so this is its first statement.
+__device__ __forceinline__ void pdl_wait_release()
+{
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 struct SweepCtl {
   unsigned blocks_done;   // CTAs of the current black launch that have finished
   int nactive;            // domains still iterating
@@ -209,6 +220,7 @@ __device__ __forceinline__ void sweep_finish_black(const SweepArgs &b, int na)
 template <int UNIT, bool MULTI>
 __global__ void __launch_bounds__(256) k_window_check(SweepArgs b)
 {
+  pdl_wait_release();
   const int na = b.ctl->nactive;
   const int slot = blockIdx.y;
   double dmax = 0.0;

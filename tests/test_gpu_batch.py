@@ -19,13 +19,14 @@ def _cities():
     return out
 
 
-def _batch(ws, tol, itermax, lam0s, variant=-1):
+def _batch(ws, tol, itermax, lam0s, variant=-1, pdl=1):
     import torch
 
     solvers = [qesb.Solver_B200(w.domain, tol) for w in ws]
     try:
         if variant >= 0:
             solvers[0].set_option("variant", variant)
+        solvers[0].set_option("pdl", pdl)
         for s, w, l0 in zip(solvers, ws, lam0s):
             s.set_inputs(w)
             if l0 is not None:
@@ -41,13 +42,16 @@ def _batch(ws, tol, itermax, lam0s, variant=-1):
             s.close()
 
 
-@pytest.mark.parametrize("variant", [-1, 18, 21, 23, 26, 40, 41, 42, 44, 46, 48, 50])
-def test_batch_matches_oracle_per_domain(variant):
+@pytest.mark.parametrize("variant,pdl", [(-1, 1), (18, 1), (21, 1), (23, 1), (26, 1), (40, 1), (41, 1), (42, 1),
+                                         (44, 1), (46, 1), (48, 1), (50, 1), (57, 1), (59, 1), (59, 0)])
+def test_batch_matches_oracle_per_domain(variant, pdl):
+    """Per domain the oracle's bits; z-march list shapes with and without
+    programmatic dependent launches between the list kernels."""
     ws = _cities()
     rng = np.random.default_rng(11)
     lam0s = [None, rng.standard_normal(ws[1].domain.numCellCentered()).astype(np.float32), None, None]
     tol = 1.1e-3
-    st, lams, winds = _batch(ws, tol, 3000, lam0s, variant)
+    st, lams, winds = _batch(ws, tol, 3000, lam0s, variant, pdl)
     for w, l0, s, L, (u, v, ww) in zip(ws, lam0s, st, lams, winds):
         d = w.domain
         Lo, it, fe, _ = O.sor(d, w, O.divergence(d, w), tol, 3000, ordering=1, err_fp64=True, lam=l0)

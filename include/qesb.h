@@ -398,15 +398,18 @@ qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *x2, int c2,
 qesb_status qesb_conv3d_items(const void *x1, int c1, int up1, const void *x2, int c2, int items, int D,
                               int H, int W, int sign, const void *Bm, int Kp, int N, void *y, void *yf,
                               const float *bias, int relu, const void *mask, int *err, void *stream);
-/* Process-wide choice of the qesb_conv3d kernel: 0 = the default (the
- * z-marching direct kernel for forward convolutions of one 16-channel input
- * without mask on grids with W a multiple of 128: input planes staged once by
- * tensor-map copies, MMAs of one plane overlapping the read-out of the
- * previous; else the direct kernel where it applies; else the implicit GEMM),
- * 1 = implicit GEMM everywhere, 2 = the direct kernel but not the z-marching
- * one, 3 / 4 = the z-marching kernel with 2 / 4 output rows per CTA (2 is the
- * default's), 5 = the default with a four-stage implicit GEMM instead of
- * three - for comparison. */
+/* Process-wide choice of the qesb_conv3d kernel: 0 = the default: forward
+ * convolutions without mask on rows of 128 (or a multiple), 64 or 32 voxels
+ * run the z-marching kernel (input planes staged once by tensor-map copies,
+ * copies, MMAs and read-out of different planes overlapping on their own
+ * warps; concatenated inputs; an upsampled input first written on the output
+ * grid; split over input channels when the weights and planes do not fit one
+ * CTA), with three output planes per MMA up to 32 output channels; else the
+ * direct kernel where it applies; else the implicit GEMM. 1 = implicit GEMM
+ * everywhere, 2 = the direct kernel, else the implicit GEMM, 3 / 4 = the
+ * z-marching kernel for one 16-channel input only, 2 / 4 output rows per CTA,
+ * 5 = as 3 with a four-stage implicit GEMM, 6 = as 0 with one output plane per
+ * MMA - for comparison. */
 qesb_status qesb_net_set_conv_path(int path);
 /* Weight gradient dW[tap*(c1+c2) + c][n] += sum_v X[v + offset(tap)][c] * dY[v][n]
  * (FP32, accumulated with atomics: zero it first); X as in qesb_conv3d,

@@ -21,9 +21,11 @@ namespace {
 
 constexpr uint32_t kWaitLimit = 1u << 26;  // mbarrier polls before a kernel gives up
 int g_conv_path = 0;  // 0: z-marching kernel for every forward convolution it takes (concatenated and
-                      // upsampled inputs, rows of 128, 64 or 32), else direct, else implicit GEMM;
-                      // 1: implicit GEMM only; 2: direct kernel, else implicit GEMM; 3 / 4: z-marching for
-                      // one 16-channel input only, 2 / 4 rows per CTA; 5: as 3 with a four-stage implicit GEMM
+                      // upsampled inputs, rows of 128, 64 or 32; three output planes per MMA up to 32
+                      // output channels), else direct, else implicit GEMM; 1: implicit GEMM only;
+                      // 2: direct kernel, else implicit GEMM; 3 / 4: z-marching for one 16-channel input
+                      // only, 2 / 4 rows per CTA; 5: as 3 with a four-stage implicit GEMM; 6: as 0 with
+                      // one output plane per MMA
 
 // Byte offset of element (r, k) in a canonical no-swizzle tile with KC = 64
 // columns of K and R rows (see qesb_umma.cuh).
@@ -798,6 +800,273 @@ __global__ void __launch_bounds__(192, 1) k_conv_zflat(const __grid_constant__ C
   }
 }
 
+// The same convolution with each input plane read once per tap (dy, dx): the
+// MMAs march over input planes, and the one of input plane i and tap (dy, dx)
+// multiplies its window by [W(dz=+1) | W(dz=0) | W(dz=-1)] (N = 3 x cout),
+// adding into the accumulators of output planes i - 2, i - 1 and i at once
+// (input plane index i is z = z0 - 1 + i, output index t is z = z0 + t). A
+// window's operand then leaves shared memory 9 x KS times per output plane
+// instead of 27 x KS, which bounds these small-N MMAs. The accumulators of an
+// output live in a TMEM ring of R slots per window (slot t % R): output t is
+// complete after input plane t + 2, is read out, and its slot is written again
+// by output t + R. Where the three outputs' slots wrap around the ring, and on
+// the first tap of a plane (whose newest output starts from zero, as do all
+// three on the item's first plane), the MMA is split into pieces of 1 or 2
+// outputs. Roles as in k_conv_zflat; each input plane is read by one step, so
+// its slot is freed right after that step's MMAs.
+template <int C, int N>
+__host__ __device__ constexpr int zf3_ring()
+{
+  return C * 8 * N <= 256 ? 8 : C * 5 * N <= 256 ? 5 : C * 4 * N <= 256 ? 4 : C * 8 * N <= 512 ? 8 : C * 5 * N <= 512 ? 5 : 4;
+}
+
+template <int N, int XT, int TY>
+__global__ void __launch_bounds__(192, 1) k_conv_zflat3(const __grid_constant__ CUtensorMap map1,
+                                                        const __grid_constant__ CUtensorMap map2, ZfIn zi, ConvGeom g,
+                                                        int ZC, const __nv_bfloat16 *__restrict__ Bm, int Kp,
+                                                        ConvOut out, int slice, int *err)
+{
+  using Z = Zf<XT, TY>;
+  constexpr int C = Z::C, RWD = Z::RWD, R = zf3_ring<C, N>();
+  constexpr uint32_t CGB = Z::CGB;
+  constexpr uint32_t NCOLS = C * R * N <= 32 ? 32 : C * R * N <= 64 ? 64 : C * R * N <= 128 ? 128 : C * R * N <= 256 ? 256 : 512;
+  static_assert(C * R * N <= 512 && R >= 4, "the output ring exceeds the TMEM columns");
+  constexpr int kMaxNS = 8;
+  extern __shared__ __align__(1024) uint8_t sm[];
+  __shared__ __align__(8) uint64_t full[kMaxNS];   // plane slot s: the copies (or a plain arrival) of its plane
+  __shared__ __align__(8) uint64_t empty[kMaxNS];  // plane slot s: the MMAs of its plane are done
+  __shared__ __align__(8) uint64_t accf[8];        // ring slot r: output t (t % R == r) is complete
+  __shared__ __align__(8) uint64_t acce[8];        // ring slot r: output t is read out (4 warps)
+  __shared__ __align__(8) uint64_t mdrain;
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag, n_issued, n_landed;
+  volatile int *abort = &abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int KG = zi.kg, KS = KG >> 1, NS = zi.ns;
+  const uint32_t SLOT = (uint32_t)KG * CGB;
+  const int nzc = (g.Dc + ZC - 1) / ZC;
+  const int item = blockIdx.z / nzc, zlo = item * g.Dc, zhi = zlo + g.Dc;
+  const int z0 = zlo + (blockIdx.z % nzc) * ZC, z1 = min(z0 + ZC, zhi), nz = z1 - z0;
+  const int x0 = blockIdx.x * XT, y0 = blockIdx.y * TY;
+  uint8_t *sb = sm + (uint32_t)NS * SLOT;
+  if ((umma::smem_u32(sm) & 127u) || NS < 2 || NS > kMaxNS) {  // copies need 128-byte aligned slots
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+  if (warp == 0) umma::tmem_alloc(&tmem_base, NCOLS);
+  if (tid == 0) {
+    for (int q = 0; q < NS; ++q) {
+      umma::mbar_init(&full[q], 1);
+      umma::mbar_init(&empty[q], 1);
+    }
+    for (int r = 0; r < R; ++r) {
+      umma::mbar_init(&accf[r], 1);
+      umma::mbar_init(&acce[r], 4);
+    }
+    umma::mbar_init(&mdrain, 1);
+    umma::fence_mbar_init();
+    abort_flag = 0;
+    n_issued = n_landed = 0;
+  }
+  // the weights: block (ks, dy, dx) of 3N rows x 16 channels, rows p * N + n holding tap dz = 1 - p
+  for (int idx = tid; idx < 27 * KS * N * 2; idx += 192) {
+    const int blk = idx / (6 * N), rem = idx - blk * 6 * N, np = rem >> 1, kl = rem & 1;
+    const int ks = blk / 9, yx = blk - ks * 9, part = np / N, n = np - part * N, q = 2 * ks + kl;
+    const int t = (2 - part) * 9 + yx;  // tap (dz, dy, dx) = (1 - part, yx / 3 - 1, yx % 3 - 1)
+    const int cc = q < zi.kg1 ? zi.ch1 + 8 * q : zi.c1 + zi.ch2 + 8 * (q - zi.kg1);
+    cp16_zfill(sb + blk * 3 * N * 32 + (np >> 3) * 256 + kl * 128 + (np & 7) * 16, Bm + (long)n * Kp + t * zi.cin + cc,
+               true);
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  umma::fence_smem_async();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = tmem_base;
+
+  if (warp == 4) {
+    // ---- producer: plane i (i = 0 .. nz + 1) into slot i % NS; planes outside the item get a plain arrival
+    if (lane == 0) {
+      int i = 0;
+      for (; i <= nz + 1; ++i) {
+        const int s = i % NS, k = i / NS;
+        if (k >= 1 && !zf_wait(&empty[s], (uint32_t)(k - 1) & 1u, abort)) break;
+        const int z = z0 - 1 + i;
+        if (z < zlo || z >= zhi) {
+          umma::mbar_arrive(&full[s]);
+        } else {
+          umma::mbar_expect_tx(&full[s], (uint32_t)KG * Z::BOX_TX);
+          uint8_t *dst = sm + (uint32_t)s * SLOT;
+          for (int q = 0; q < zi.kg1; ++q)
+            umma::tma_load4(dst + q * CGB, &map1, zi.ch1 + 8 * q, x0 - 1, y0 - 1, z, &full[s]);
+          for (int q = zi.kg1; q < KG; ++q)
+            umma::tma_load4(dst + q * CGB, &map2, zi.ch2 + 8 * (q - zi.kg1), x0 - 1, y0 - 1, z, &full[s]);
+        }
+      }
+      n_issued = i;
+    }
+  } else if (warp == 5) {
+    // ---- MMA issuer: one step per input plane
+    if (lane == 0) {
+      const uint32_t idesc1 = umma::idesc_bf16(128, N, 0, 0), idesc2 = umma::idesc_bf16(128, 2 * N, 0, 0),
+                     idesc3 = umma::idesc_bf16(128, 3 * N, 0, 0);
+      const uint32_t a0 = umma::smem_u32(sm), b0 = umma::smem_u32(sb);
+      const uint64_t ad0 = umma::desc(a0, CGB, 128);  // tap (dy, dx) = (-1, -1), first K step, window 0, slot 0
+      const uint64_t bd0 = umma::desc(b0, 128, 256);  // weights block (0, 0, 0), row 0
+      int i = 0;
+      for (; i <= nz + 1; ++i) {
+        bool ok = zf_wait(&full[i % NS], (uint32_t)(i / NS) & 1u, abort);
+        const int prev = i - R;  // the output that held output i's ring slot
+        if (ok && prev >= 0 && prev < nz) ok = zf_wait(&acce[prev % R], (uint32_t)(prev / R) & 1u, abort);
+        if (!ok) break;
+        umma::fence_after_sync();
+        const int z = z0 - 1 + i;
+        if (z >= zlo && z < zhi) {
+          const bool first_in_item = z == zlo;  // outputs i - 2, i - 1, i all start here
+          // the step's pieces of consecutive outputs (part pa.. of i - 2, i - 1, i, at ring slot sl): split
+          // where the ring wraps; on the first tap also before output i (which starts from zero there)
+          const int s0 = ((i - 2) % R + R) % R, wr = s0 + 3 <= R ? 3 : R - s0;  // parts before the wrap
+          int npo = 1, pao[2] = {0, wr}, lno[2] = {wr, 3 - wr}, slo[2] = {s0, 0};
+          if (wr < 3) npo = 2;
+          int npf = 0, paf[3], lnf[3], slf[3];
+          uint32_t acf[3];
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            if (k >= npo) break;
+            const int a = pao[k], e = a + lno[k];  // parts [a, e)
+            if (!first_in_item && a < 2 && e == 3) {  // split before part 2
+              paf[npf] = a, lnf[npf] = 2 - a, slf[npf] = slo[k], acf[npf] = 1u, ++npf;
+              paf[npf] = 2, lnf[npf] = 1, slf[npf] = slo[k] + 2 - a, acf[npf] = 0u, ++npf;
+            } else {
+              paf[npf] = a, lnf[npf] = e - a, slf[npf] = slo[k], acf[npf] = first_in_item || a == 2 ? 0u : 1u, ++npf;
+            }
+          }
+          const uint64_t as = ad0 + (uint64_t)((i % NS) * (SLOT >> 4));
+#pragma unroll
+          for (int c = 0; c < C; ++c) {
+            const uint64_t adc = as + (uint64_t)(c * Z::S);
+            const uint32_t colc = tmem + (uint32_t)(c * R * N);
+            for (int ks = 0; ks < KS; ++ks) {
+              const uint64_t aks = adc + (uint64_t)ks * (2 * CGB >> 4);
+              const uint64_t bks = bd0 + (uint64_t)(ks * 9 * 3 * N * 2);  // 16-byte units
+#pragma unroll
+              for (int yx = 0; yx < 9; ++yx) {
+                constexpr int kN2 = N * 2;
+                const uint64_t ad = aks + (uint64_t)((yx / 3) * RWD + yx % 3);
+                const uint64_t bd = bks + (uint64_t)(yx * 3 * kN2);
+                if (ks == 0 && yx == 0) {
+#pragma unroll
+                  for (int k = 0; k < 3; ++k)
+                    if (k < npf)
+                      umma::mma_bf16(colc + (uint32_t)(slf[k] * N), ad, bd + (uint64_t)(paf[k] * kN2),
+                                     lnf[k] == 1 ? idesc1 : lnf[k] == 2 ? idesc2 : idesc3, acf[k]);
+                } else {
+#pragma unroll
+                  for (int k = 0; k < 2; ++k)
+                    if (k < npo)
+                      umma::mma_bf16(colc + (uint32_t)(slo[k] * N), ad, bd + (uint64_t)(pao[k] * kN2),
+                                     lno[k] == 1 ? idesc1 : lno[k] == 2 ? idesc2 : idesc3, 1u);
+                }
+              }
+            }
+          }
+        }
+        // plane i is read by no later step: free its slot if a later plane needs it
+        if (i + NS <= nz + 1) umma::mma_commit(&empty[i % NS]);
+        if (i - 2 >= 0 && i - 2 < nz) umma::mma_commit(&accf[(i - 2) % R]);  // output i - 2 is complete
+      }
+      n_landed = i;
+    }
+  } else {
+    // ---- read-out: warps 0-3, TMEM lanes 32 warp .. 32 warp + 31
+    const int ny = min(TY, g.H - y0);  // rows of this tile inside the grid
+    constexpr int WB = C * N <= 64 ? C : 64 / N > 0 ? 64 / N : 1;  // windows per TMEM wait (<= 64 registers)
+    for (int t = 0; t < nz; ++t) {
+      if (!zf_wait(&accf[t % R], (uint32_t)(t / R) & 1u, abort)) break;
+      umma::fence_after_sync();
+      const int z = z0 + t;
+#pragma unroll
+      for (int c = 0; c < C; c += WB) {
+        uint32_t raw[WB][N];
+#pragma unroll
+        for (int w = 0; w < WB; ++w)
+#pragma unroll
+          for (int c0 = 0; c0 < N; c0 += 16)
+            if (c + w < C)
+              umma::tmem_ld16_async(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((c + w) * R * N + (t % R) * N + c0),
+                                    *reinterpret_cast<uint32_t(*)[16]>(&raw[w][c0]));
+        umma::tmem_wait_ld();
+        if (c + WB >= C) {  // this warp's lanes of output t are all read
+          umma::fence_before_sync();
+          if (lane == 0) umma::mbar_arrive(&acce[t % R]);
+        }
+#pragma unroll
+        for (int w = 0; w < WB; ++w) {
+          if (c + w >= C) break;
+          const int p = (c + w) * Z::S + warp * 32 + lane, r = p / RWD, x = p - r * RWD;
+          if (r >= ny || x >= XT) continue;
+          const long v = ((long)z * g.H + y0 + r) * g.W + x0 + x;
+          if (slice >= 0) {  // FP32 partial sum of this launch's channels
+            float4 *dst = reinterpret_cast<float4 *>(out.acc + ((long)slice * g.V + v) * N);
+#pragma unroll
+            for (int c0 = 0; c0 < N; c0 += 4)
+              dst[c0 / 4] = make_float4(__uint_as_float(raw[w][c0]), __uint_as_float(raw[w][c0 + 1]),
+                                        __uint_as_float(raw[w][c0 + 2]), __uint_as_float(raw[w][c0 + 3]));
+            continue;
+          }
+#pragma unroll
+          for (int c0 = 0; c0 < N; c0 += 8) {
+            float f[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) f[q] = __uint_as_float(raw[w][c0 + q]);
+            if (out.bias) {
+#pragma unroll
+              for (int q = 0; q < 8; ++q) f[q] += __ldg(out.bias + c0 + q);
+            }
+            if (out.relu) {
+#pragma unroll
+              for (int q = 0; q < 8; ++q) f[q] = fmaxf(f[q], 0.0f);
+            }
+            if (out.ch0) {
+              if (c0 == 0) out.yf[v] = f[0];
+            } else if (out.yf) {
+              float4 *dst = reinterpret_cast<float4 *>(out.yf + v * N + c0);
+              dst[0] = make_float4(f[0], f[1], f[2], f[3]);
+              dst[1] = make_float4(f[4], f[5], f[6], f[7]);
+            } else {
+              uint4 pk;
+              __nv_bfloat162 *h2 = reinterpret_cast<__nv_bfloat162 *>(&pk);
+#pragma unroll
+              for (int q = 0; q < 4; ++q) h2[q] = __floats2bfloat162_rn(f[2 * q], f[2 * q + 1]);
+              *reinterpret_cast<uint4 *>(out.y + v * N + c0) = pk;
+            }
+          }
+        }
+      }
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  if (abort_flag) {
+    // a wait gave up: let every issued copy land and every issued MMA finish before TMEM and the slots go
+    if (tid == 0) atomicExch(err, 1);
+    if (tid == 160) {  // the issuer's thread: its MMAs tracked by one more commit
+      umma::mma_commit(&mdrain);
+      umma::mbar_wait(&mdrain, 0, kWaitLimit);
+      for (int i = n_landed; i < n_issued; ++i) umma::mbar_wait(&full[i % NS], (uint32_t)(i / NS) & 1u, kWaitLimit);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+  }
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tmem, NCOLS);
+  }
+}
+
 // Weight gradient: dW[t*cin + c][n] += sum_v X[v + off(t)][c] * dY[v][n] over
 // this CTA's voxel range. M-tile = 128 rows of (t, c); K = voxels in chunks
 // of 64; both operands MN-major (channels contiguous). Partial sums from the
@@ -1137,17 +1406,30 @@ qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, const __nv_bfloat
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // one output plane per MMA, or three (k_conv_zflat3, off on conv path 6) where its output ring fits
+  // 256 TMEM columns (two CTAs per SM stay possible; measured slower otherwise)
+  constexpr int C = Zf<XT, TY>::C;
+  constexpr bool kThreeOk = N <= 32 && C * zf3_ring<C, (N <= 32 ? N : 16)>() * N <= 256;
+  const bool three = kThreeOk && g_conv_path == 0;
+  void (*kern)(CUtensorMap, CUtensorMap, ZfIn, ConvGeom, int, const __nv_bfloat16 *, int, ConvOut, int, int *) =
+      k_conv_zflat<N, XT, TY>;
+  if constexpr (kThreeOk)
+    if (three) kern = k_conv_zflat3<N, XT, TY>;
+  // TMEM columns one CTA allocates: a CTA that needs all 512 must have its SM alone
+  constexpr int kCols3 = C * zf3_ring<C, (kThreeOk ? N : 16)>() * N, kCols1 = 2 * C * N;
+  const bool whole_sm = (three ? kCols3 : kCols1) > 256;
   // plane slots: four when two CTAs fit an SM, else as many as fit (at most eight)
   const int lim = max_dyn_smem();
   int ns = 4;
-  if (2 * ((int)zf_smem_bytes<N, XT, TY>(2 * per, 4) + 1024) > lim + 1024)
+  if (whole_sm || 2 * ((int)zf_smem_bytes<N, XT, TY>(2 * per, 4) + 1024) > lim + 1024)
     while (ns < 8 && (int)zf_smem_bytes<N, XT, TY>(2 * per, ns + 1) <= lim) ++ns;
-  static int attr[64] = {};  // dynamic shared memory allowed so far, per device
-  const int need = (int)zf_smem_bytes<N, XT, TY>(2 * per, ns);
-  if (attr[dev & 63] < need) {
-    cudaError_t e = cudaFuncSetAttribute(k_conv_zflat<N, XT, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, need);
+  int need = (int)zf_smem_bytes<N, XT, TY>(2 * per, ns);
+  if (whole_sm) need = std::max(need, (lim + 1024) / 2 + 1024);  // keeps a second CTA off the SM
+  static int attr[64][2] = {};  // dynamic shared memory allowed so far, per device and kernel
+  if (attr[dev & 63][three] < need) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, need);
     if (e != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "conv attr: %s", cudaGetErrorString(e));
-    attr[dev & 63] = need;
+    attr[dev & 63][three] = need;
   }
   CUtensorMap map1, map2;
   qesb_status st = zf_map(&map1, x1, c1, g, XT, TY);
@@ -1172,8 +1454,9 @@ qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, const __nv_bfloat
     zi.c1 = c1;
     zi.cin = cin;
     zi.ns = ns;
-    const int smem = (int)zf_smem_bytes<N, XT, TY>(zi.kg, ns);
-    k_conv_zflat<N, XT, TY><<<grid, 192, smem, s>>>(map1, map2, zi, g, zc, Bm, Kp, o, P > 1 ? p : -1, err);
+    int smem = (int)zf_smem_bytes<N, XT, TY>(zi.kg, ns);
+    if (whole_sm) smem = std::max(smem, (lim + 1024) / 2 + 1024);
+    kern<<<grid, 192, smem, s>>>(map1, map2, zi, g, zc, Bm, Kp, o, P > 1 ? p : -1, err);
   }
   if (P > 1) {
     launch_finish(o.acc, P, g.V, N, out, s);
@@ -1290,7 +1573,7 @@ qesb_status conv_items(const void *x1, int c1, int up1, const void *x2, int c2, 
   cudaGetDevice(&dev);
   const auto aligned = [](const void *p) { return reinterpret_cast<uintptr_t>(p) % 16 == 0; };
   const bool fwd = sign == 1 && !mask && aligned(x1) && (!c2 || aligned(x2));
-  if (fwd && g_conv_path == 0 && N <= 64) {
+  if (fwd && (g_conv_path == 0 || g_conv_path == 6) && N <= 64) {
     // the z-marching kernel: rows of 128 (two output rows per CTA, one when
     // the channels of two do not fit unsplit), or whole rows of 64 or 32
     int xt = 0, ty = 0;
@@ -1386,7 +1669,7 @@ extern "C" qesb_status qesb_conv3d(const void *x1, int c1, int up1, const void *
 
 extern "C" qesb_status qesb_net_set_conv_path(int path)
 {
-  if (path < 0 || path > 5) return qesb_fail(QESB_ERR_ARG, "qesb_net_set_conv_path: path must be in [0, 5]");
+  if (path < 0 || path > 6) return qesb_fail(QESB_ERR_ARG, "qesb_net_set_conv_path: path must be in [0, 6]");
   g_conv_path = path;
   return QESB_OK;
 }

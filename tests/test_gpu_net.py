@@ -268,15 +268,16 @@ def test_conv3d_items_stack_along_z_without_crosstalk(D, H, W, c1, c2, co, up):
         np.testing.assert_allclose(out[i].numpy(), _cl(ref).numpy(), rtol=1e-4, atol=1e-4)
 
 
-@pytest.mark.parametrize("path", [2, 3, 4])
+@pytest.mark.parametrize("path", [0, 2, 3, 4, 6])
 @pytest.mark.parametrize("items,D,H,W,co", [(1, 1, 5, 128, 16), (1, 3, 6, 256, 32), (3, 4, 7, 128, 16),
-                                            (2, 6, 4, 128, 32), (1, 17, 9, 128, 16)])
+                                            (2, 6, 4, 128, 32), (1, 17, 9, 128, 16), (2, 10, 6, 64, 32)])
 def test_conv3d_zmarch_and_direct_paths_match_torch(conv_path, path, items, D, H, W, co):
-    """The z-marching direct convolution (tensor-map staging, planes through a
-    ring, MMAs of one plane overlapping the read-out of the last) with 2 and 4
-    rows per CTA, and the direct kernel, for 16-channel forward convolutions:
-    odd heights (partial row tiles), one-plane and many-plane items, stacked
-    items, both output widths; against torch per item."""
+    """The z-marching convolutions (tensor-map staging, planes through a ring,
+    copies, MMAs and read-out of different planes overlapping): three output
+    planes per MMA (path 0) and one (path 6), 2 and 4 rows per CTA (paths 3,
+    4), and the direct kernel, for 16-channel forward convolutions: odd heights
+    (partial row tiles), one-plane and many-plane items cut into z chunks,
+    stacked items, rows of 256, 128 and 64; against torch per item."""
     import torch
     torch.manual_seed(items + D + H + W + co + path)
     ci = 16

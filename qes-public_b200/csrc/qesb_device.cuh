@@ -83,11 +83,12 @@ __device__ __forceinline__ void block_max_to(double *dst, double v)
 {
   __shared__ double s_part[32];
   v = warp_max_d(v);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int lane = tid & 31, wid = tid >> 5;
   if (lane == 0) s_part[wid] = v;
   __syncthreads();
   if (wid == 0) {
-    const int nw = (blockDim.x + 31) >> 5;
+    const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
     double x = lane < nw ? s_part[lane] : 0.0;
     x = warp_max_d(x);
     if (lane == 0 && x != 0.0) atomic_max_nonneg(dst, x);

@@ -387,10 +387,11 @@ __global__ void k_max_divergence(DevGrid G, const int *__restrict__ flag, const 
                                  const float *__restrict__ v, const float *__restrict__ w,
                                  const float *__restrict__ dz, float dx, float dy, int kmax, double *out)
 {
-  const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+  // a warp per row j of layer k (eight rows per block), lanes along x; one atomic per block
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z + 1;
   double mx = 0.0;
   if (j <= G.Y - 2 && k <= kmax) {
-    for (int i = 1 + blockIdx.x * blockDim.x + threadIdx.x; i <= G.X - 2; i += gridDim.x * blockDim.x) {
+    for (int i = 1 + threadIdx.x; i <= G.X - 2; i += blockDim.x) {
       if (flag[G.cell(i, j, k)] != 1) continue;
       const long fc = G.face(i, j, k);
       const double d = ((double)u[fc + 1] - u[fc]) / dx + ((double)v[fc + G.FX] - v[fc]) / dy +
@@ -685,6 +686,54 @@ cudaError_t zero_async(void *p, size_t bytes, cudaStream_t s)
       static_cast<uint32_t *>(p), n, reinterpret_cast<uintptr_t>(p) % 16 == 0);
   return cudaGetLastError();
 }
+
+// Several small copies or zero fills (src null) in one launch, one op per grid row.
+constexpr int kMaxWordOps = 32;
+struct WordOps {
+  const uint32_t *src[kMaxWordOps];
+  uint32_t *dst[kMaxWordOps];
+  int n[kMaxWordOps];
+  int count;
+};
+
+__global__ void k_word_ops(WordOps ops)
+{
+  const int q = blockIdx.y;
+  if (q >= ops.count) return;
+  const uint32_t *src = ops.src[q];
+  uint32_t *dst = ops.dst[q];
+  for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < ops.n[q]; i += gridDim.x * blockDim.x)
+    dst[i] = src ? src[i] : 0u;
+  __threadfence_system();
+}
+
+// Collects small copies and fills (bytes multiples of 4) and launches them together on flush().
+struct WordBatch {
+  WordOps ops{};
+  int maxn = 0;
+  cudaStream_t s;
+  explicit WordBatch(cudaStream_t st) : s(st) {}
+  qesb_status add(void *dst, const void *src, size_t bytes)
+  {
+    if (ops.count == kMaxWordOps) CKS(flush());
+    ops.src[ops.count] = static_cast<const uint32_t *>(src);
+    ops.dst[ops.count] = static_cast<uint32_t *>(dst);
+    ops.n[ops.count] = (int)(bytes / 4);
+    maxn = std::max(maxn, ops.n[ops.count]);
+    ++ops.count;
+    return QESB_OK;
+  }
+  qesb_status zero(void *dst, size_t bytes) { return add(dst, nullptr, bytes); }
+  qesb_status flush()
+  {
+    if (ops.count == 0) return QESB_OK;
+    k_word_ops<<<dim3(std::max(1, std::min(148, (maxn + 255) / 256)), ops.count), 256, 0, s>>>(ops);
+    ops.count = 0;
+    maxn = 0;
+    CK(cudaGetLastError());
+    return QESB_OK;
+  }
+};
 
 // device -> device copy of n floats (16-byte aligned pointers)
 qesb_status copy_floats(float *dst, const float *src, long n, cudaStream_t s)
@@ -1679,8 +1728,8 @@ qesb_status enqueue_divergence_check(qesb_handle *h, const float *u, const float
   CK(zero_async(h->d_div, sizeof(double), s));
   const int kmax = G.FZ - 4;
   if (kmax >= 1) {
-    k_max_divergence<<<dim3((G.X + 255) / 256, G.Y - 2, kmax), 256, 0, s>>>(G, h->d_flag, u, v, w, h->d_dz, h->dx,
-                                                                           h->dy, kmax, h->d_div);
+    k_max_divergence<<<dim3(1, (G.Y - 2 + 7) / 8, kmax), dim3(32, 8), 0, s>>>(G, h->d_flag, u, v, w, h->d_dz, h->dx,
+                                                                             h->dy, kmax, h->d_div);
     CK(cudaGetLastError());
   }
   return QESB_OK;
@@ -2425,6 +2474,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     if (hs[i]->win_k != h0->win_k)
       return qesb_fail(QESB_ERR_ARG, "qesb_solve_batch: handles %d and 0 have different window lengths (%d, %d)", i,
                        hs[i]->win_k, h0->win_k);
+  WordBatch wb(s);  // the domains' small fills and state reads, one launch per group
   for (int i = 0; i < n; ++i) {
     qesb_handle *h = hs[i];
     const DevGrid &G = h->G;
@@ -2432,7 +2482,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     const int nerr = err_slots(h, itermax);
     CKS(ensure_err(h, nerr));
     launch_divergence(h, s);
-    CK(zero_async(h->d_err, sizeof(double) * nerr, s));
+    CKS(wb.zero(h->d_err, sizeof(double) * nerr));
     h->last_pre_iterations = 0;
     if (pre_on) {
       SweepDomain p;
@@ -2447,7 +2497,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
         start_of.push_back(i);
       }
     }
-    CK(zero_async(h->d_state, sizeof(SolveState), s));
+    CKS(wb.zero(h->d_state, sizeof(SolveState)));
     k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_lam, h->d_lam_s);
     k_pad_to_split<<<row_grid(G, G.Y, G.Z, G.X), 256, 0, s>>>(G, h->S, h->d_R, h->d_R_s);
     CK(cudaGetLastError());
@@ -2455,6 +2505,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     CKS(attach_tmaps(h, sv, doms[i], s));
     cells += (double)G.XY * G.Z;
   }
+  CKS(wb.flush());
   SweepList &list = h0->blist;
   if (list.cap < n) {
     list.destroy();
@@ -2477,7 +2528,8 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
                           h0->h_ctl, h0->h_ctl_dev, &n1, 0, 1, h0->opt_pdl != 0);
     pre_launched += n1;
     for (size_t q = 0; q < start_of.size() && qs == QESB_OK; ++q)
-      qs = copy_words(hs[start_of[q]]->h_state_dev, hs[start_of[q]]->d_state, sizeof(SolveState), s);
+      qs = wb.add(hs[start_of[q]]->h_state_dev, hs[start_of[q]]->d_state, sizeof(SolveState));
+    if (qs == QESB_OK) qs = wb.flush();
     if (qs == QESB_OK) CK(cudaStreamSynchronize(s));
     for (size_t q = 0; q < start_of.size() && qs == QESB_OK; ++q) {
       qesb_handle *h = hs[start_of[q]];
@@ -2486,9 +2538,10 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
         qs = qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d during the pre-phase's start stage",
                        start_of[q]);
       h->last_pre_iterations = sp.it;
-      CK(zero_async(h->d_err, sizeof(double) * err_slots(h, itermax), s));
-      CK(zero_async(h->d_state, sizeof(SolveState), s));
+      if (qs == QESB_OK) qs = wb.zero(h->d_err, sizeof(double) * err_slots(h, itermax));
+      if (qs == QESB_OK) qs = wb.zero(h->d_state, sizeof(SolveState));
     }
+    if (qs == QESB_OK) qs = wb.flush();
   }
   if (!pre.empty() && qs == QESB_OK) {
     // the over-relaxed pre-phase of the domains that have one, as a list of its own
@@ -2502,16 +2555,18 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
                           h0->h_ctl, h0->h_ctl_dev, &n2, 0, 1, h0->opt_pdl != 0);
     pre_launched += n2;
     for (size_t q = 0; q < pre_of.size() && qs == QESB_OK; ++q)
-      qs = copy_words(hs[pre_of[q]]->h_state_dev, hs[pre_of[q]]->d_state, sizeof(SolveState), s);
+      qs = wb.add(hs[pre_of[q]]->h_state_dev, hs[pre_of[q]]->d_state, sizeof(SolveState));
+    if (qs == QESB_OK) qs = wb.flush();
     if (qs == QESB_OK) CK(cudaStreamSynchronize(s));
     for (size_t q = 0; q < pre_of.size() && qs == QESB_OK; ++q) {
       qesb_handle *h = hs[pre_of[q]];
       const SolveState sp = *h->h_state;
       if (sp.nan) qs = qesb_fail(QESB_ERR_NUMERIC, "NaN in lambda of batch domain %d during the pre-phase", pre_of[q]);
       h->last_pre_iterations += sp.it;
-      CK(zero_async(h->d_err, sizeof(double) * std::max(itermax, 1), s));
-      CK(zero_async(h->d_state, sizeof(SolveState), s));
+      if (qs == QESB_OK) qs = wb.zero(h->d_err, sizeof(double) * std::max(itermax, 1));
+      if (qs == QESB_OK) qs = wb.zero(h->d_state, sizeof(SolveState));
     }
+    if (qs == QESB_OK) qs = wb.flush();
   }
   CK(cudaEventRecord(h0->evs[1], s));
   sweep_tiles(doms, sv, true, h0->device);
@@ -2543,9 +2598,10 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
   CK(cudaEventRecord(h0->ev[3], s));
   // every domain's final state and divergence into its mapped buffers, then one wait
   for (int i = 0; i < n && qs == QESB_OK; ++i) {
-    qs = copy_words(hs[i]->h_state_dev, hs[i]->d_state, sizeof(SolveState), s);
-    if (qs == QESB_OK) qs = copy_words(hs[i]->h_io_dev, hs[i]->d_div, sizeof(double), s);
+    qs = wb.add(hs[i]->h_state_dev, hs[i]->d_state, sizeof(SolveState));
+    if (qs == QESB_OK) qs = wb.add(hs[i]->h_io_dev, hs[i]->d_div, sizeof(double));
   }
+  if (qs == QESB_OK) qs = wb.flush();
   cudaError_t se = cudaStreamSynchronize(s);
   if (qs != QESB_OK) return qs;
   if (se != cudaSuccess) return qesb_fail(QESB_ERR_CUDA, "batch: %s", cudaGetErrorString(se));

@@ -871,6 +871,10 @@ struct qesb_handle {
   bool have_inputs = false;
   bool packed = false;
   bool pc_ready = false;  // d_pc holds the current inputs' padded coefficients
+  // R of the current inputs: inputs_gen counts input changes, R_gen the inputs d_R was computed from
+  // (0: none, or inputs in caller-owned memory that may change behind the handle); ev_R follows it
+  unsigned long long inputs_gen = 0, R_gen = 0;
+  cudaEvent_t ev_R = nullptr;
   int opt_path = 1;
   int opt_k = 0;
   int opt_graph = 1;
@@ -1031,6 +1035,9 @@ void launch_divergence(qesb_handle *h, cudaStream_t s)
     k_divergence<<<row_grid(G, G.Y, G.Z - 2, G.X), 256, 0, s>>>(G, h->d_in[0], h->d_in[1], h->d_in[2], h->d_in[3],
                                                                  h->d_in[4], h->d_in[5], h->d_u0, h->d_v0, h->d_w0,
                                                                  h->d_dz, h->dx, h->dy, h->d_R);
+  // remembered for the next solve unless the inputs live in caller-owned memory
+  h->R_gen = h->d_u0 == h->d_own_u0 && h->d_in[0] == h->d_own_in[0] ? h->inputs_gen : 0;
+  cudaEventRecord(h->ev_R, s);
 }
 
 // Padded copies of the six coefficients for the full-coefficient sweep.
@@ -1046,9 +1053,18 @@ qesb_status ensure_padded_coefs(qesb_handle *h)
   return QESB_OK;
 }
 
+// R for a solve: the R already computed from the same inputs (a warm start
+// computes it first), ordered after its computation, or a new one.
+void ensure_divergence(qesb_handle *h, cudaStream_t s)
+{
+  if (h->R_gen != 0 && h->R_gen == h->inputs_gen) cudaStreamWaitEvent(s, h->ev_R, 0);
+  else launch_divergence(h, s);
+}
+
 // Inspect coefficients; build mask + tables when stair-step, else padded copies.
 qesb_status prepare_coefs(qesb_handle *h)
 {
+  ++h->inputs_gen;  // new inputs: any R computed before is stale
   const DevGrid &G = h->G;
   cudaStream_t s = h->stream;
   h->packed = false;
@@ -1746,7 +1762,7 @@ qesb_status solve_impl(qesb_handle *h, int itermax, float *u, float *v, float *w
   const int nerr = err_slots(h, itermax);
   CKS(ensure_err(h, nerr));
   CK(cudaEventRecord(h->ev[0], s));
-  launch_divergence(h, s);
+  ensure_divergence(h, s);
   CK(cudaGetLastError());
   CK(zero_async(h->d_err, sizeof(double) * nerr, s));
   CK(zero_async(h->d_state, sizeof(SolveState), s));
@@ -1856,6 +1872,7 @@ void free_all(qesb_handle *h)
     if (e) cudaEventDestroy(e);
   for (auto &e : h->evs)
     if (e) cudaEventDestroy(e);
+  if (h->ev_R) cudaEventDestroy(h->ev_R);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
 }
 
@@ -1930,6 +1947,8 @@ qesb_status qesb_create(const qesb_grid *grid, float tol, int device, qesb_handl
     if (cudaEventCreate(&e) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaEventCreate failed"));
   for (auto &e : h->evs)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaEventCreate failed"));
+  if (cudaEventCreateWithFlags(&h->ev_R, cudaEventDisableTiming) != cudaSuccess)
+    return fail(qesb_fail(QESB_ERR_CUDA, "cudaEventCreate failed"));
   for (void *p : {(void *)h->d_lam, (void *)h->d_lam2, (void *)h->d_R})
     if (cudaMemset(p, 0, np * sizeof(float)) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaMemset failed"));
   if (cudaMemset(h->d_mask, 0, np) != cudaSuccess) return fail(qesb_fail(QESB_ERR_CUDA, "cudaMemset failed"));
@@ -1966,6 +1985,7 @@ qesb_status qesb_reset_lambda(qesb_handle *h)
   CK(zero_async(h->d_lam, np * sizeof(float), h->stream));
   CK(zero_async(h->d_lam2, np * sizeof(float), h->stream));
   CK(zero_async(h->d_R, np * sizeof(float), h->stream));
+  h->R_gen = 0;  // R is recomputed by the next solve
   CK(cudaStreamSynchronize(h->stream));
   return QESB_OK;
 }
@@ -2481,7 +2501,7 @@ qesb_status qesb_solve_batch(qesb_handle *const *hs, int n, int itermax, float *
     const bool pre_on = prephase_on(h) && itermax > 0;
     const int nerr = err_slots(h, itermax);
     CKS(ensure_err(h, nerr));
-    launch_divergence(h, s);
+    ensure_divergence(h, s);
     CKS(wb.zero(h->d_err, sizeof(double) * nerr));
     h->last_pre_iterations = 0;
     if (pre_on) {

@@ -371,3 +371,35 @@ def test_half_resolution_input_equals_full_input_then_pooling():
         torch.cuda.synchronize()
     assert int(scale[0]) == int(scale[1]) != 0
     assert torch.equal(half.view(torch.int16), pooled.view(torch.int16))
+
+
+def test_solve_after_learned_start_matches_oracle_and_new_inputs_recompute_R():
+    """A solve after the learned start reuses the R the start computed from
+    the same inputs (no second divergence pass) and still gives the oracle's
+    bits from that start; after new inputs (other initial winds) the next
+    solve computes R again and matches the oracle for them."""
+    from oracle import oracle as O
+    from qesb import warmstart as ws
+
+    if not os.path.exists(ws.DEFAULT_WEIGHTS):
+        pytest.skip("no trained weights committed")
+    w, _ = qesb.random_city("city128", 900021)
+    cnet = ws.WarmNet(ws.DEFAULT_WEIGHTS, device=0)
+    try:
+        with qesb.Solver_B200(w.domain, 1.1e-3) as s:
+            s.set_inputs(w)
+            cnet.warm_start(s)
+            lam0 = s.lambda_
+            st = s.solve(w, 3000, set_inputs=False)
+            d = w.domain
+            Lo, it, *_ = O.sor(d, w, O.divergence(d, w), 1.1e-3, 3000, lam=lam0)
+            assert st["iterations"] == it
+            np.testing.assert_array_equal(s.lambda_, Lo)
+            w.w0 = (w.w0 * 1.25).astype(np.float32)  # new inputs: R must follow them
+            s.resetLambda()
+            st2 = s.solve(w, 3000)
+            Lo2, it2, *_ = O.sor(d, w, O.divergence(d, w), 1.1e-3, 3000)
+            assert st2["iterations"] == it2
+            np.testing.assert_array_equal(s.lambda_, Lo2)
+    finally:
+        cnet.close()

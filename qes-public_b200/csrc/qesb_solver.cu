@@ -609,22 +609,27 @@ __global__ void k_warm_apply_up2(DevGrid G, int Dn, const float *__restrict__ yh
   float tz, ty;
   up2_axis(kk, D2, z0, z1, tz);
   up2_axis(j, H2, y0, y1, ty);
+  // the four coarse rows this fine row interpolates between (per block)
+  const float *r00 = yhead + ((long)z0 * H2 + y0) * W2 * N, *r01 = yhead + ((long)z0 * H2 + y1) * W2 * N;
+  const float *r10 = yhead + ((long)z1 * H2 + y0) * W2 * N, *r11 = yhead + ((long)z1 * H2 + y1) * W2 * N;
+  const bool row_upd = j >= 1 && j <= G.Y - 2 && kk >= 1 && kk <= G.Z - 2 && kk < Dn;
+  float *Lrow = L + G.pad(0, j, k);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G.X; i += gridDim.x * blockDim.x) {
-    const bool upd = i >= 1 && i <= G.X - 2 && j >= 1 && j <= G.Y - 2 && kk >= 1 && kk <= G.Z - 2 && kk < Dn;
+    const bool upd = row_upd && i >= 1 && i <= G.X - 2;
     float v = 0.0f;
     if (upd) {
       int x0, x1;
       float tx;
       up2_axis(i, W2, x0, x1, tx);
-      auto at = [&](int z, int y, int x) { return yhead[(((long)z * H2 + y) * W2 + x) * N]; };
-      const float c00 = at(z0, y0, x0) * (1.0f - tx) + at(z0, y0, x1) * tx;
-      const float c01 = at(z0, y1, x0) * (1.0f - tx) + at(z0, y1, x1) * tx;
-      const float c10 = at(z1, y0, x0) * (1.0f - tx) + at(z1, y0, x1) * tx;
-      const float c11 = at(z1, y1, x0) * (1.0f - tx) + at(z1, y1, x1) * tx;
+      const int a = x0 * N, b = x1 * N;
+      const float c00 = r00[a] * (1.0f - tx) + r00[b] * tx;
+      const float c01 = r01[a] * (1.0f - tx) + r01[b] * tx;
+      const float c10 = r10[a] * (1.0f - tx) + r10[b] * tx;
+      const float c11 = r11[a] * (1.0f - tx) + r11[b] * tx;
       const float c0 = c00 * (1.0f - ty) + c01 * ty, c1 = c10 * (1.0f - ty) + c11 * ty;
       v = s * (c0 * (1.0f - tz) + c1 * tz);
     }
-    L[G.pad(i, j, k)] = v;
+    Lrow[i] = v;
   }
 }
 

@@ -1379,15 +1379,30 @@ int max_dyn_smem()
   return v - 1024;  // room for the kernel's static shared memory
 }
 
+// Whether a launch shape runs k_conv_zflat3 (three output planes per MMA):
+// up to 32 output channels, an output ring within 256 TMEM columns (two CTAs
+// per SM stay possible; measured slower otherwise), the default conv path.
+template <int N, int XT, int TY>
+constexpr bool zf_three_ok()
+{
+  return N <= 32 && Zf<XT, TY>::C * zf3_ring<Zf<XT, TY>::C, (N <= 32 ? N : 16)>() * N <= 256;
+}
+
+template <int N, int XT, int TY>
+bool zf_uses_three()
+{
+  return zf_three_ok<N, XT, TY>() && g_conv_path == 0;
+}
+
 // Launches (channel splits) the z-marching convolution needs for cin input
 // channels: the fewest whose 16-channel K steps, shared out evenly, fit the
 // shared memory; 0 when even one step does not fit.
 template <int N, int XT, int TY>
 int zf_splits(int cin)
 {
-  const int steps = cin / 16, lim = max_dyn_smem();
+  const int steps = cin / 16, lim = max_dyn_smem(), ns = zf_uses_three<N, XT, TY>() ? 3 : 4;
   for (int P = 1; P <= steps; ++P)
-    if ((int)zf_smem_bytes<N, XT, TY>(2 * ((steps + P - 1) / P), 4) <= lim) return P;
+    if ((int)zf_smem_bytes<N, XT, TY>(2 * ((steps + P - 1) / P), ns) <= lim) return P;
   return 0;
 }
 
@@ -1406,11 +1421,10 @@ qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, const __nv_bfloat
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // one output plane per MMA, or three (k_conv_zflat3, off on conv path 6) where its output ring fits
-  // 256 TMEM columns (two CTAs per SM stay possible; measured slower otherwise)
+  // one output plane per MMA, or three (k_conv_zflat3; not on conv path 6)
   constexpr int C = Zf<XT, TY>::C;
-  constexpr bool kThreeOk = N <= 32 && C * zf3_ring<C, (N <= 32 ? N : 16)>() * N <= 256;
-  const bool three = kThreeOk && g_conv_path == 0;
+  constexpr bool kThreeOk = zf_three_ok<N, XT, TY>();
+  const bool three = zf_uses_three<N, XT, TY>();
   void (*kern)(CUtensorMap, CUtensorMap, ZfIn, ConvGeom, int, const __nv_bfloat16 *, int, ConvOut, int, int *) =
       k_conv_zflat<N, XT, TY>;
   if constexpr (kThreeOk)
@@ -1418,10 +1432,12 @@ qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, const __nv_bfloat
   // TMEM columns one CTA allocates: a CTA that needs all 512 must have its SM alone
   constexpr int kCols3 = C * zf3_ring<C, (kThreeOk ? N : 16)>() * N, kCols1 = 2 * C * N;
   const bool whole_sm = (three ? kCols3 : kCols1) > 256;
-  // plane slots: four when two CTAs fit an SM, else as many as fit (at most eight)
+  // plane slots: four when two CTAs fit an SM (three-plane kernel: three when four do not fit), else as
+  // many as fit (at most eight)
   const int lim = max_dyn_smem();
   int ns = 4;
-  if (whole_sm || 2 * ((int)zf_smem_bytes<N, XT, TY>(2 * per, 4) + 1024) > lim + 1024)
+  if (three && (int)zf_smem_bytes<N, XT, TY>(2 * per, 4) > lim) ns = 3;
+  if (whole_sm || 2 * ((int)zf_smem_bytes<N, XT, TY>(2 * per, ns) + 1024) > lim + 1024)
     while (ns < 8 && (int)zf_smem_bytes<N, XT, TY>(2 * per, ns + 1) <= lim) ++ns;
   int need = (int)zf_smem_bytes<N, XT, TY>(2 * per, ns);
   if (whole_sm) need = std::max(need, (lim + 1024) / 2 + 1024);  // keeps a second CTA off the SM
@@ -1584,7 +1600,7 @@ qesb_status conv_items(const void *x1, int c1, int up1, const void *x2, int c2, 
       const int p1 = N == 16 ? zf_splits<16, 128, 1>(cin) : N == 32 ? zf_splits<32, 128, 1>(cin) : zf_splits<64, 128, 1>(cin);
       ty = p2 == 1 || p1 != 1 ? 2 : 1;
     } else if (W == 64) {
-      xt = 64, ty = 4;
+      xt = 64, ty = 4;  // (two rows per CTA with three output planes per MMA measured 10-20 % slower)
     } else if (W == 32) {
       xt = 32, ty = 8;
     }

@@ -403,3 +403,59 @@ def test_solve_after_learned_start_matches_oracle_and_new_inputs_recompute_R():
             np.testing.assert_array_equal(s.lambda_, Lo2)
     finally:
         cnet.close()
+
+
+def test_learned_start_beats_the_prephase_alone_in_the_batch():
+    """The benchmark's comparison, on its batch of eight held-out 256x256x64
+    cities solved together to the window rule: the learned start (batched
+    forward pass) followed by the pre-phase with its start stage takes less
+    time per batch than the pre-phase alone from lambda = 0 (best of three
+    steps each, after a warm-up), and both arms' solves stop with their winds
+    computed."""
+    import time
+
+    import torch
+    from qesb import warmstart as ws
+
+    if not os.path.exists(ws.DEFAULT_WEIGHTS):
+        pytest.skip("no trained weights committed")
+    cities = [qesb.random_city("city256", 500000 + i)[0] for i in range(8)]
+    solvers = [qesb.Solver_B200(w.domain, RULE_TOL) for w in cities]
+    cnet = ws.WarmNet(ws.DEFAULT_WEIGHTS, device=0)
+    nf = cities[0].domain.numFaceCentered()
+    outs = [[torch.empty(nf, dtype=torch.float32, device="cuda") for _ in range(3)] for _ in cities]
+    ptrs = [[o[q].data_ptr() for o in outs] for q in range(3)]
+    try:
+        for s, w in zip(solvers, cities):
+            s.set_inputs(w)
+            s.set_window_rule(RULE_WINDOW, RULE_WINDOW_TOL)
+        bv, _ = qesb.autotune_batch(solvers)
+        solvers[0].set_option("batch_variant", bv)
+
+        def step(learned):
+            for s in solvers:
+                s.set_prephase(1.97, 2e-3, 10000)
+                s.set_prephase_start(*((1.8, 8) if learned else (0.0, 0)))
+            t0 = time.perf_counter()
+            if learned:
+                cnet.warm_start_batch(solvers)
+            else:
+                for s in solvers:
+                    s.resetLambda()
+            st = qesb.solve_batch(solvers, 10000, *ptrs)
+            torch.cuda.synchronize()
+            return time.perf_counter() - t0, st
+
+        best = {}
+        for learned in (False, True, False, True):
+            times = []
+            for _ in range(3):
+                dt, st = step(learned)
+                times.append(dt)
+                assert all(x["iterations"] < 10000 and x["max_divergence"] >= 0 for x in st)
+            best[learned] = min(best.get(learned, 1e9), min(times))
+    finally:
+        cnet.close()
+        for s in solvers:
+            s.close()
+    assert best[True] < best[False], best

@@ -633,16 +633,22 @@ def run_b200(args):
             s.set_prephase(PRE_OMEGA if use_pre else 0.0, PRE_TOL, ITERMAX)
             s.set_prephase_start(*start_stage(use_net, use_pre))
 
-    def batch_step(use_net, use_pre, sset=None, ptrs=None, strm=None):
+    def start_batch(sset, use_net, use_pre):
+        # the arm's settings and start (the learned start, or lambda = 0) of a batch
+        set_arm(sset, use_net, use_pre)
+        if use_net:
+            cnet.warm_start_batch(sset)
+        else:
+            for s in sset:
+                s.resetLambda()
+
+    def batch_step(use_net, use_pre, sset=None, ptrs=None, strm=None, started=False):
+        # started: the batch's start is already in place (a pipeline prepared it)
         sset, ptrs, strm = sset or solvers, ptrs or uvw, strm or stream
 
         def step():
-            set_arm(sset, use_net, use_pre)
-            if use_net:
-                cnet.warm_start_batch(sset)
-            else:
-                for s in sset:
-                    s.resetLambda()
+            if not started:
+                start_batch(sset, use_net, use_pre)
             st = qesb.solve_batch(sset, ITERMAX, *ptrs)
             return st, (launches_per_net if use_net else 0) + 6 * B + st[0]["launches"]
         return step
@@ -752,14 +758,16 @@ def run_b200(args):
     set_uvw = [uvw, [[o[q].data_ptr() for o in outs2] for q in range(3)]]
     host_out2 = [[torch.empty(nf, dtype=torch.float32, pin_memory=True) for _ in range(3)] for _ in range(B)]
     set_host_out = [host_out, host_out2]
-    steps_of_set = [batch_step(use_net, use_pre, sets[k], set_uvw[k], streams[k]) for k in range(2)]
+    steps_of_set = [batch_step(use_net, use_pre, sets[k], set_uvw[k], streams[k], started=True) for k in range(2)]
 
     def load(k, flags_only):
+        # a batch's inputs, then its start: on the loading thread, while the other batch solves
         for s_, ins in zip(sets[k], host_in):
             if flags_only:  # the stair-step coefficients computed from the flags on the device
                 qesb.check(qesb.lib().qesb_set_inputs_flags(s_._h, *[a.ctypes.data for a in ins[FLAGS_ONLY]]))
             else:
                 qesb.check(qesb.lib().qesb_set_inputs(s_._h, *[a.ctypes.data for a in ins]))
+        start_batch(sets[k], use_net, use_pre)
 
     def solve_read(k):
         st_, _ = steps_of_set[k]()
@@ -1004,8 +1012,8 @@ def run_b200(args):
                     "how": "public API from pinned host arrays: qesb_set_inputs_flags (icellflag, u0, v0, w0; the "
                            "stair-step wall coefficients, the reference's default mesh, computed from the flags on "
                            "the device), the batched learned start, qesb_solve_batch, winds read back to pinned "
-                           "host memory; two solver sets, the next batch's inputs loading on a second host thread "
-                           "while the current batch solves; device-timed over the steps",
+                           "host memory; two solver sets: while one batch solves, a second host thread loads the "
+                           "next batch's inputs and runs its learned start; device-timed over the steps",
                     "full_arrays_value": ms_e2e_full / B, "full_arrays_h2d_bytes_per_step": h2d_full,
                     "full_arrays_how": "the same with qesb_set_inputs and the reference's full input arrays "
                                        "(e, f, g, h, m, n, icellflag, u0, v0, w0)",

@@ -546,6 +546,7 @@ struct ZfIn {
   int ch1, ch2; // first staged channel of x1 / of x2
   int c1, cin;  // channels of x1 and of the concatenation (the weights' K index is tap * cin + channel)
   int ns;       // plane slots in the ring (>= 4)
+  int up1;      // x1 is the coarse grid (D/2 x H/2 x W/2): its planes are staged and upsampled in the CTA
 };
 
 template <int XT, int TY>
@@ -560,10 +561,22 @@ struct Zf {
   static_assert(C <= 4, "at most four windows per plane");
 };
 
+// The coarse planes of an upsampled input (k_conv_zflat3, up1): rows and
+// columns of the coarse grid under a tile's staged rows, bytes per channel group.
+template <int XT, int TY>
+struct ZfUp {
+  static constexpr int CR = TY / 2 + 2, CC = XT / 2 + 2;
+  static constexpr uint32_t CCB = ((uint32_t)CR * CC * 16 + 127) / 128 * 128;
+  static constexpr uint32_t BOX_TX = (uint32_t)CR * CC * 16;
+};
+
+// Shared memory of a launch: ns plane slots of kg channel groups, the
+// weights, and (upsampled input) two coarse plane slots of up_kg groups.
 template <int N, int XT, int TY>
-__host__ __device__ constexpr uint32_t zf_smem_bytes(int kg, int ns)
+__host__ __device__ constexpr uint32_t zf_smem_bytes(int kg, int ns, int up_kg = 0)
 {
-  return (uint32_t)ns * (uint32_t)kg * Zf<XT, TY>::CGB + 27u * (uint32_t)(kg / 2) * N * 32u;
+  return (uint32_t)ns * (uint32_t)kg * Zf<XT, TY>::CGB + 27u * (uint32_t)(kg / 2) * N * 32u +
+         2u * (uint32_t)up_kg * ZfUp<XT, TY>::CCB;
 }
 
 // Bounded wait that also gives up as soon as another role of the CTA has
@@ -837,6 +850,7 @@ __global__ void __launch_bounds__(192, 1) k_conv_zflat3(const __grid_constant__ 
   __shared__ __align__(8) uint64_t empty[kMaxNS];  // plane slot s: the MMAs of its plane are done
   __shared__ __align__(8) uint64_t accf[8];        // ring slot r: output t (t % R == r) is complete
   __shared__ __align__(8) uint64_t acce[8];        // ring slot r: output t is read out (4 warps)
+  __shared__ __align__(8) uint64_t cfull[2];       // coarse slot b: the copies of its coarse plane (up1)
   __shared__ __align__(8) uint64_t mdrain;
   __shared__ uint32_t tmem_base;
   __shared__ int abort_flag, n_issued, n_landed;
@@ -863,6 +877,8 @@ __global__ void __launch_bounds__(192, 1) k_conv_zflat3(const __grid_constant__ 
       umma::mbar_init(&accf[r], 1);
       umma::mbar_init(&acce[r], 4);
     }
+    umma::mbar_init(&cfull[0], 1);
+    umma::mbar_init(&cfull[1], 1);
     umma::mbar_init(&mdrain, 1);
     umma::fence_mbar_init();
     abort_flag = 0;
@@ -885,7 +901,76 @@ __global__ void __launch_bounds__(192, 1) k_conv_zflat3(const __grid_constant__ 
   umma::fence_after_sync();
   const uint32_t tmem = tmem_base;
 
-  if (warp == 4) {
+  if (warp == 4 && zi.up1) {
+    // ---- producer with an upsampled x1 (the whole warp): each coarse plane under the tile arrives once
+    // by tensor-map copies into one of two coarse slots, one coarse plane ahead; the lanes expand it
+    // (nearest neighbour) into the x1 channel groups of the fine slots of both fine planes it covers,
+    // then lane 0 adds the copies of x2's groups and the plane's arrival
+    using U = ZfUp<XT, TY>;
+    uint8_t *cbuf = sb + 27u * (uint32_t)KS * N * 32u;
+    const int cx0 = x0 / 2 - 1, cy0 = (y0 + 1) / 2 - 1;  // first coarse column and row (floor of (v - 1) / 2)
+    const int czlo = zlo / 2, czmax = min(zhi / 2 - 1, z1 / 2);
+    unsigned cis[2] = {0u, 0u}, cwt[2] = {0u, 0u};  // coarse loads issued / waited per slot (lane 0)
+    int cnext = 0, chave = -1;
+    int i = 0;
+    for (; i <= nz + 1; ++i) {
+      const int s = i % NS, k = i / NS;
+      bool ok = true;
+      if (lane == 0 && k >= 1) ok = zf_wait(&empty[s], (uint32_t)(k - 1) & 1u, abort);
+      if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+      const int z = z0 - 1 + i;
+      if (z < zlo || z >= zhi) {
+        if (lane == 0) umma::mbar_arrive(&full[s]);
+        continue;
+      }
+      const int c = z / 2;  // z >= zlo >= 0
+      if (c != chave) {
+        if (lane == 0) {
+          if (cnext < c) cnext = c;
+          for (; cnext <= c + 1 && cnext <= czmax && cnext >= czlo; ++cnext) {  // this plane and the next
+            const int b = cnext & 1;
+            umma::mbar_expect_tx(&cfull[b], (uint32_t)zi.kg1 * U::BOX_TX);
+            for (int q = 0; q < zi.kg1; ++q)
+              umma::tma_load4(cbuf + ((uint32_t)b * zi.kg1 + q) * U::CCB, &map1, zi.ch1 + 8 * q, cx0, cy0, cnext,
+                              &cfull[b]);
+            ++cis[b];
+          }
+          ok = zf_wait(&cfull[c & 1], cwt[c & 1] & 1u, abort);
+          ++cwt[c & 1];
+        }
+        if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+        chave = c;
+      }
+      const uint8_t *cb = cbuf + (uint32_t)(c & 1) * zi.kg1 * U::CCB;
+      uint8_t *dst = sm + (uint32_t)s * SLOT;
+      for (int q = 0; q < zi.kg1; ++q)
+#pragma unroll
+        for (int ry = 0; ry < TY + 2; ++ry) {
+          // staged row ry is fine row y0 - 1 + ry, coarse row floor((y0 + ry - 1) / 2) - cy0; staged column
+          // rx is fine column x0 - 1 + rx, coarse column (rx + 1) / 2 - (x0 even)
+          const uint4 *crow = reinterpret_cast<const uint4 *>(cb + q * U::CCB) + ((y0 + ry + 1) / 2 - 1 - cy0) * U::CC;
+          uint4 *frow = reinterpret_cast<uint4 *>(dst + q * CGB) + ry * RWD;
+          for (int rx = lane; rx < RWD; rx += 32) frow[rx] = crow[(rx + 1) >> 1];
+        }
+      umma::fence_smem_async();  // the expanded groups to the MMAs, the coarse slot's reads before its refill
+      __syncwarp();
+      if (lane == 0) {
+        if (KG > zi.kg1) {
+          umma::mbar_expect_tx(&full[s], (uint32_t)(KG - zi.kg1) * Z::BOX_TX);
+          for (int q = zi.kg1; q < KG; ++q)
+            umma::tma_load4(dst + q * CGB, &map2, zi.ch2 + 8 * (q - zi.kg1), x0 - 1, y0 - 1, z, &full[s]);
+        } else {
+          umma::mbar_arrive(&full[s]);
+        }
+      }
+    }
+    if (lane == 0) {
+      n_issued = i;
+      if (*abort)  // let the coarse copies in flight land before the CTA's memory goes
+        for (int b = 0; b < 2; ++b)
+          for (; cwt[b] < cis[b]; ++cwt[b]) umma::mbar_wait(&cfull[b], cwt[b] & 1u, kWaitLimit);
+    }
+  } else if (warp == 4) {
     // ---- producer: plane i (i = 0 .. nz + 1) into slot i % NS; planes outside the item get a plain arrival
     if (lane == 0) {
       int i = 0;
@@ -1371,6 +1456,23 @@ qesb_status zf_map(CUtensorMap *map, const __nv_bfloat16 *x, int c, const ConvGe
   return QESB_OK;
 }
 
+// The coarse grid under an upsampled input (D/2 x H/2 x W/2, c channels),
+// boxes of 8 channels x cc columns x cr rows x 1 plane; zeros outside.
+qesb_status zf_map_coarse(CUtensorMap *map, const __nv_bfloat16 *x, int c, const ConvGeom &g, int cc, int cr)
+{
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return qesb_fail(QESB_ERR_CUDA, "cuTensorMapEncodeTiled not available");
+  const cuuint64_t cb = (cuuint64_t)c * 2, W2 = (cuuint64_t)g.W / 2, H2 = (cuuint64_t)g.H / 2;
+  const cuuint64_t dims[4] = {(cuuint64_t)c, W2, H2, (cuuint64_t)g.D / 2};
+  const cuuint64_t st[3] = {cb, W2 * cb, W2 * H2 * cb};
+  const cuuint32_t box[4] = {8, (cuuint32_t)cc, (cuuint32_t)cr, 1}, one[4] = {1, 1, 1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(x), dims, st, box, one,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return qesb_fail(QESB_ERR_CUDA, "conv tensor map: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return QESB_OK;
+}
+
 int max_dyn_smem()
 {
   int dev = 0, v = 0;
@@ -1406,14 +1508,30 @@ int zf_splits(int cin)
   return 0;
 }
 
+// Nearest-neighbour x2 upsampling of a coarse grid (D/2 x H/2 x W/2, c
+// channels) onto the output grid, 16 bytes (8 channels) per thread.
+__global__ void k_up2(const __nv_bfloat16 *__restrict__ x, ConvGeom g, int c, __nv_bfloat16 *__restrict__ y)
+{
+  const int cg = c / 8, n = g.W * cg;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int xq = i / cg, q = i - xq * cg;
+  for (long row = blockIdx.y; row < (long)g.D * g.H; row += gridDim.y) {
+    const int zq = (int)(row / g.H), yq = (int)(row - (long)zq * g.H);
+    const long cv = ((long)(zq >> 1) * (g.H >> 1) + (yq >> 1)) * (g.W >> 1) + (xq >> 1);
+    reinterpret_cast<uint4 *>(y)[row * n + i] = __ldg(reinterpret_cast<const uint4 *>(x) + cv * cg + q);
+  }
+}
+
 // z-marching convolution of x1 (c1 channels) concatenated with x2 (c2), both
 // on the output grid. Split over its input channels when the weights and the
 // plane ring do not fit one CTA's shared memory: each launch stores its FP32
 // partial sums in its own slice, k_conv_finish adds them in launch order and
 // applies the epilogue.
 template <int N, int XT, int TY>
-qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, const __nv_bfloat16 *x2, int c2, const ConvGeom &g,
-                              const __nv_bfloat16 *Bm, int Kp, const ConvOut &out, int *err, cudaStream_t s)
+qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, int up1, const __nv_bfloat16 *x2, int c2,
+                              const ConvGeom &g, const __nv_bfloat16 *Bm, int Kp, const ConvOut &out, int *err,
+                              cudaStream_t s)
 {
   const int cin = c1 + c2, steps = cin / 16, P = zf_splits<N, XT, TY>(cin);
   if (P == 0) return qesb_fail(QESB_ERR_ARG, "qesb_conv3d: %d channels do not fit the z-marching kernel", cin);
@@ -1421,6 +1539,22 @@ qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, const __nv_bfloat
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // an upsampled x1: staged from the coarse grid and expanded in the CTA (three-plane kernel, unsplit,
+  // with three plane slots and the coarse slots fitting), else first written on the output grid
+  int up_kg = 0;
+  if (up1) {
+    if (zf_uses_three<N, XT, TY>() && P == 1 && (int)zf_smem_bytes<N, XT, TY>(2 * steps, 3, c1 / 8) <= max_dyn_smem()) {
+      up_kg = c1 / 8;
+    } else {
+      void *u = nullptr;
+      qesb_status st = scratch_buffer(kScratchUp, dev, s, (size_t)g.V * c1 * 2, &u);
+      if (st != QESB_OK) return st;
+      const int n = g.W * (c1 / 8);
+      const dim3 grid((unsigned)((n + 255) / 256), (unsigned)std::min<long>((long)g.D * g.H, 65535L));
+      k_up2<<<grid, 256, 0, s>>>(x1, g, c1, static_cast<__nv_bfloat16 *>(u));
+      x1 = static_cast<const __nv_bfloat16 *>(u);
+    }
+  }
   // one output plane per MMA, or three (k_conv_zflat3; not on conv path 6)
   constexpr int C = Zf<XT, TY>::C;
   constexpr bool kThreeOk = zf_three_ok<N, XT, TY>();
@@ -1436,10 +1570,10 @@ qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, const __nv_bfloat
   // many as fit (at most eight)
   const int lim = max_dyn_smem();
   int ns = 4;
-  if (three && (int)zf_smem_bytes<N, XT, TY>(2 * per, 4) > lim) ns = 3;
-  if (whole_sm || 2 * ((int)zf_smem_bytes<N, XT, TY>(2 * per, ns) + 1024) > lim + 1024)
-    while (ns < 8 && (int)zf_smem_bytes<N, XT, TY>(2 * per, ns + 1) <= lim) ++ns;
-  int need = (int)zf_smem_bytes<N, XT, TY>(2 * per, ns);
+  if (three && (int)zf_smem_bytes<N, XT, TY>(2 * per, 4, up_kg) > lim) ns = 3;
+  if (whole_sm || 2 * ((int)zf_smem_bytes<N, XT, TY>(2 * per, ns, up_kg) + 1024) > lim + 1024)
+    while (ns < 8 && (int)zf_smem_bytes<N, XT, TY>(2 * per, ns + 1, up_kg) <= lim) ++ns;
+  int need = (int)zf_smem_bytes<N, XT, TY>(2 * per, ns, up_kg);
   if (whole_sm) need = std::max(need, (lim + 1024) / 2 + 1024);  // keeps a second CTA off the SM
   static int attr[64][2] = {};  // dynamic shared memory allowed so far, per device and kernel
   if (attr[dev & 63][three] < need) {
@@ -1448,7 +1582,7 @@ qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, const __nv_bfloat
     attr[dev & 63][three] = need;
   }
   CUtensorMap map1, map2;
-  qesb_status st = zf_map(&map1, x1, c1, g, XT, TY);
+  qesb_status st = up_kg ? zf_map_coarse(&map1, x1, c1, g, XT / 2 + 2, TY / 2 + 2) : zf_map(&map1, x1, c1, g, XT, TY);
   if (st != QESB_OK) return st;
   map2 = map1;
   if (c2 && (st = zf_map(&map2, x2, c2, g, XT, TY)) != QESB_OK) return st;
@@ -1470,7 +1604,8 @@ qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, const __nv_bfloat
     zi.c1 = c1;
     zi.cin = cin;
     zi.ns = ns;
-    int smem = (int)zf_smem_bytes<N, XT, TY>(zi.kg, ns);
+    zi.up1 = up_kg > 0;
+    int smem = (int)zf_smem_bytes<N, XT, TY>(zi.kg, ns, up_kg);
     if (whole_sm) smem = std::max(smem, (lim + 1024) / 2 + 1024);
     kern<<<grid, 192, smem, s>>>(map1, map2, zi, g, zc, Bm, Kp, o, P > 1 ? p : -1, err);
   }
@@ -1481,20 +1616,6 @@ qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, const __nv_bfloat
   return e == cudaSuccess ? QESB_OK : qesb_fail(QESB_ERR_CUDA, "conv launch: %s", cudaGetErrorString(e));
 }
 
-// Nearest-neighbour x2 upsampling of a coarse grid (D/2 x H/2 x W/2, c
-// channels) onto the output grid, 16 bytes (8 channels) per thread.
-__global__ void k_up2(const __nv_bfloat16 *__restrict__ x, ConvGeom g, int c, __nv_bfloat16 *__restrict__ y)
-{
-  const int cg = c / 8, n = g.W * cg;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int xq = i / cg, q = i - xq * cg;
-  for (long row = blockIdx.y; row < (long)g.D * g.H; row += gridDim.y) {
-    const int zq = (int)(row / g.H), yq = (int)(row - (long)zq * g.H);
-    const long cv = ((long)(zq >> 1) * (g.H >> 1) + (yq >> 1)) * (g.W >> 1) + (xq >> 1);
-    reinterpret_cast<uint4 *>(y)[row * n + i] = __ldg(reinterpret_cast<const uint4 *>(x) + cv * cg + q);
-  }
-}
 
 template <int N>
 qesb_status launch_wgrad(const ConvIn &in, const ConvGeom &g, const __nv_bfloat16 *dY, long vchunk, float *dW,
@@ -1605,19 +1726,9 @@ qesb_status conv_items(const void *x1, int c1, int up1, const void *x2, int c2, 
       xt = 32, ty = 8;
     }
     if (xt) {
-      const __nv_bfloat16 *xa = in.x1;
-      if (up1) {  // the upsampled input on the output grid first
-        void *u = nullptr;
-        qesb_status st = scratch_buffer(kScratchUp, dev, s, (size_t)g.V * c1 * 2, &u);
-        if (st != QESB_OK) return st;
-        const int n = W * (c1 / 8);
-        const dim3 grid((unsigned)((n + 255) / 256), (unsigned)std::min<long>((long)g.D * H, 65535L));
-        k_up2<<<grid, 256, 0, s>>>(in.x1, g, c1, static_cast<__nv_bfloat16 *>(u));
-        xa = static_cast<const __nv_bfloat16 *>(u);
-      }
-      const __nv_bfloat16 *xb = in.x2;
+      const __nv_bfloat16 *xa = in.x1, *xb = in.x2;
       o.ch0 = ch0;
-#define QESB_ZF(NN, XT_, TY_) launch_conv_zflat<NN, XT_, TY_>(xa, c1, xb, c2, g, B, Kp, o, err, s)
+#define QESB_ZF(NN, XT_, TY_) launch_conv_zflat<NN, XT_, TY_>(xa, c1, up1, xb, c2, g, B, Kp, o, err, s)
       if (xt == 128 && ty == 2) return N == 16 ? QESB_ZF(16, 128, 2) : N == 32 ? QESB_ZF(32, 128, 2) : QESB_ZF(64, 128, 2);
       if (xt == 128) return N == 16 ? QESB_ZF(16, 128, 1) : N == 32 ? QESB_ZF(32, 128, 1) : QESB_ZF(64, 128, 1);
       if (xt == 64) return N == 16 ? QESB_ZF(16, 64, 4) : N == 32 ? QESB_ZF(32, 64, 4) : QESB_ZF(64, 64, 4);
@@ -1637,10 +1748,10 @@ qesb_status conv_items(const void *x1, int c1, int up1, const void *x2, int c2, 
     // paths 3, 4, 5: the z-marching kernel for one 16-channel input only (4 rows per CTA on path 4, else 2)
     if (fwd && g_conv_path >= 3 && W % 128 == 0 && (N == 16 || N == 32) && c1 == 16 && c2 == 0 && !up1) {
       if (g_conv_path == 4)
-        return N == 16 ? launch_conv_zflat<16, 128, 4>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s)
-                       : launch_conv_zflat<32, 128, 4>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s);
-      return N == 16 ? launch_conv_zflat<16, 128, 2>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s)
-                     : launch_conv_zflat<32, 128, 2>(in.x1, 16, nullptr, 0, g, B, Kp, o, err, s);
+        return N == 16 ? launch_conv_zflat<16, 128, 4>(in.x1, 16, 0, nullptr, 0, g, B, Kp, o, err, s)
+                       : launch_conv_zflat<32, 128, 4>(in.x1, 16, 0, nullptr, 0, g, B, Kp, o, err, s);
+      return N == 16 ? launch_conv_zflat<16, 128, 2>(in.x1, 16, 0, nullptr, 0, g, B, Kp, o, err, s)
+                     : launch_conv_zflat<32, 128, 2>(in.x1, 16, 0, nullptr, 0, g, B, Kp, o, err, s);
     }
     if ((g_conv_path == 0 || g_conv_path >= 2) && W % 128 == 0 && (N == 16 || N == 32)) {
       if (N == 16) return launch_conv_direct<16>(in, g, sign, B, Kp, o, err, s);

@@ -1588,11 +1588,16 @@ qesb_status launch_conv_zflat(const __nv_bfloat16 *x1, int c1, int up1, const __
   if (c2 && (st = zf_map(&map2, x2, c2, g, XT, TY)) != QESB_OK) return st;
   ConvOut o = out;
   if (P > 1 && (st = acc_buffer(dev, s, (size_t)P * g.V * N, &o.acc)) != QESB_OK) return st;
-  // z chunks: whole items unless that leaves fewer than two CTAs per SM slot
+  // z chunks: the length that minimises waves x (planes per CTA + ~3 planes of pipeline fill and weights)
   const int per_sm = std::max(1, (max_dyn_smem() + 1024) / (need + 1024));
-  const long xy = (long)(g.W / XT) * ((g.H + TY - 1) / TY), items = g.D / g.Dc;
+  const long xy = (long)(g.W / XT) * ((g.H + TY - 1) / TY), items = g.D / g.Dc, slots = (long)sms * per_sm;
   int zc = g.Dc;
-  while (zc > 2 && xy * items * ((g.Dc + zc - 1) / zc) < 2L * sms * per_sm) zc = (zc + 1) / 2;
+  long best = -1;
+  for (int c = g.Dc; c >= 2; c = (c + 1) / 2) {
+    const long waves = (xy * items * ((g.Dc + c - 1) / c) + slots - 1) / slots, cost = waves * (c + 3);
+    if (best < 0 || cost < best) best = cost, zc = c;
+    if (c == 2) break;
+  }
   const dim3 grid(g.W / XT, (g.H + TY - 1) / TY, (unsigned)(items * ((g.Dc + zc - 1) / zc)));
   for (int p = 0; p < P; ++p) {
     const int a = p * per, b = std::min(steps, a + per);  // K steps (16 channels) [a, b) of the concatenation
